@@ -1,0 +1,673 @@
+"""cfd_b200: B200-native pressure-correction solver (host-side mirror of ``cfd::gpu``).
+
+Python front end (ctypes) of ``libcfdb.so``, the C ABI declared in ``include/cfdb.h``. The
+names, argument meaning and error behaviour mirror the reference's accelerator interface
+(Yipexnn/CFD ``src/gpu/include/cfd/gpu/krylov.hpp``):
+
+* :func:`solve` / :func:`solve_amg_cg` / :func:`assemble_convection_diffusion`
+* :class:`DeviceSolver` (``DeviceSolver(const LduPattern&)``, ``set_amg``, ``solve``)
+* :func:`backend_name` / :func:`device_available` / :func:`device_description`
+
+Errors: invalid arguments raise :class:`InvalidArgument` (a ``ValueError``, the reference's
+``std::invalid_argument``); device failures raise :class:`CudaError` (a ``RuntimeError``, the
+reference's ``std::runtime_error("CUDA ...")``). Non-convergence is reported in
+:class:`SolveStats`, never raised. There is no CPU fallback: without the built library the import
+fails, and without a GPU every compute call raises :class:`NoDevice`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcfdb.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"cfd_b200: {LIB_PATH} is missing; build it with `python -m cfd_b200.build`")
+_lib = C.CDLL(LIB_PATH)
+
+_i, _d, _sz = C.c_int, C.c_double, C.c_size_t
+_pi, _pd = C.POINTER(C.c_int), C.POINTER(C.c_double)
+_vp = C.c_void_p
+
+
+class CsrStruct(C.Structure):
+    _fields_ = [("n", _i), ("nnz", _i), ("row_ptr", _pi), ("col", _pi), ("val", _pd)]
+
+
+class AmgLevelStruct(C.Structure):
+    _fields_ = [("a", CsrStruct), ("p", CsrStruct), ("r", CsrStruct)]
+
+
+class AmgViewStruct(C.Structure):
+    _fields_ = [("n_levels", _i), ("levels", C.POINTER(AmgLevelStruct)), ("coarse_inverse", _pd),
+                ("smooth_sweeps", _i), ("jacobi_weight", _d)]
+
+
+class ControlStruct(C.Structure):
+    _fields_ = [("abs_tolerance", _d), ("max_iterations", _i)]
+
+
+class StatsStruct(C.Structure):
+    _fields_ = [("iterations", _i), ("residual", _d), ("converged", _i), ("on_device", _i),
+                ("true_residual", _d)]
+
+
+class PatternStruct(C.Structure):
+    _fields_ = [("n", _i), ("n_faces", _i), ("nnz", _i), ("row_ptr", _pi), ("col", _pi),
+                ("diag_pos", _pi), ("upper_pos", _pi), ("lower_pos", _pi)]
+
+
+class AmgSettingsStruct(C.Structure):
+    _fields_ = [("strength_threshold", _d), ("max_levels", _i), ("coarse_size", _i),
+                ("smooth_sweeps", _i), ("jacobi_weight", _d)]
+
+
+def _proto(name, args, res=_i):
+    f = getattr(_lib, name)
+    f.argtypes = args
+    f.restype = res
+    return f
+
+
+_P = C.POINTER
+_proto("cfdb_backend_name", [C.c_char_p, _sz])
+_proto("cfdb_device_available", [])
+_proto("cfdb_device_description", [C.c_char_p, _sz])
+_proto("cfdb_last_error", [C.c_char_p, _sz])
+_proto("cfdb_default_amg_settings", [_P(AmgSettingsStruct)], None)
+_proto("cfdb_assemble", [_i, _i, _pi, _pi, _pd, _pd, _pd, _d, _pd, _pd, _pd, _pd])
+_proto("cfdb_assemble_device", [_i, _i, _vp, _vp, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp])
+_proto("cfdb_solve", [_P(CsrStruct), _pd, _pd, _i, _P(ControlStruct), _P(StatsStruct)])
+_proto("cfdb_solve_amg_cg", [_P(AmgViewStruct), _pd, _pd, _P(ControlStruct), _P(StatsStruct)])
+_proto("cfdb_build_pattern", [_i, _i, _pi, _pi, _pi, _pi, _pi, _pi, _pi, _pi])
+_proto("cfdb_amg_setup", [_P(CsrStruct), _P(AmgSettingsStruct), _P(_vp)])
+_proto("cfdb_hierarchy_destroy", [_vp])
+_proto("cfdb_hierarchy_levels", [_vp, _pi])
+_proto("cfdb_hierarchy_level", [_vp, _i, _i, _pi, _pi, _P(CsrStruct)])
+_proto("cfdb_hierarchy_aggregates", [_vp, _i, _P(_pi), _pi])
+_proto("cfdb_hierarchy_coarse_inverse", [_vp, _P(_pd), _pi])
+_proto("cfdb_hierarchy_view", [_vp, _i, _d, _P(AmgViewStruct)])
+_proto("cfdb_hierarchy_operator_complexity", [_vp, _pd])
+_proto("cfdb_system_create", [_P(PatternStruct), _P(_vp)])
+_proto("cfdb_system_create_mesh", [_i, _i, _pi, _pi, _P(_vp)])
+_proto("cfdb_system_destroy", [_vp])
+_proto("cfdb_system_on_device", [_vp])
+_proto("cfdb_system_set_amg", [_vp, _P(AmgViewStruct)])
+_proto("cfdb_system_setup_amg", [_vp, _pd, _pd, _pd, _P(AmgSettingsStruct)])
+_proto("cfdb_system_set_precision", [_vp, _i])
+_proto("cfdb_system_solve", [_vp, _pd, _pd, _pd, _pd, _pd, _i, _i, _P(ControlStruct),
+                             _P(StatsStruct)])
+_proto("cfdb_system_solve_device", [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _P(ControlStruct),
+                                    _P(StatsStruct)])
+_proto("cfdb_system_assemble_device", [_vp, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp])
+_proto("cfdb_system_apply_amg", [_vp, _pd, _pd])
+_proto("cfdb_system_stream", [_vp, _P(_vp)])
+_proto("cfdb_system_device_bytes", [_vp, _P(_sz)])
+# synthetic workloads (include/cfdb_synth.h)
+_proto("cfdb_mesh_box", [_i, _i, _i, _pd, _pd, _pd, _P(_vp)])
+_proto("cfdb_mesh_tet", [_i, _i, _i, _pd, _pd, _pd, _d, C.c_uint64, _P(_vp)])
+_proto("cfdb_mesh_destroy", [_vp])
+_proto("cfdb_mesh_sizes", [_vp, _pi, _pi, _pi, _pi])
+_proto("cfdb_mesh_addressing", [_vp, _P(_pi), _P(_pi)])
+_proto("cfdb_mesh_geometry", [_vp, _P(_pd), _P(_pd), _P(_pd), _P(_pd), _P(_pd)])
+_proto("cfdb_mesh_faces", [_vp, _P(_pi), _P(_pi)])
+_proto("cfdb_mesh_fv", [_vp, _P(_pd), _P(_pd)])
+_proto("cfdb_synth_pressure_inputs", [_vp, _d, _i, _i, _i, C.c_uint64, _pd, _pd, _pd])
+_proto("cfdb_positions_graded", [_i, _d, _pd])
+_proto("cfdb_positions_two_sided", [_i, _d, _pd])
+
+
+# -------------------------------------------------------------------------------------------
+# errors
+# -------------------------------------------------------------------------------------------
+
+class CfdbError(Exception):
+    code = 0
+
+
+class InvalidArgument(CfdbError, ValueError):
+    code = 1
+
+
+class CudaError(CfdbError, RuntimeError):
+    code = 2
+
+
+class OutOfMemory(CfdbError, MemoryError):
+    code = 3
+
+
+class NoDevice(CfdbError, RuntimeError):
+    code = 4
+
+
+class NotReady(CfdbError, RuntimeError):
+    code = 5
+
+
+class Timeout(CfdbError, RuntimeError):
+    code = 6
+
+
+_ERRORS = {1: InvalidArgument, 2: CudaError, 3: OutOfMemory, 4: NoDevice, 5: NotReady, 6: Timeout}
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(4096)
+    _lib.cfdb_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise _ERRORS.get(rc, CfdbError)(last_error())
+
+
+# -------------------------------------------------------------------------------------------
+# array helpers
+# -------------------------------------------------------------------------------------------
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_pi)
+
+
+def _dp(a):
+    return a.ctypes.data_as(_pd)
+
+
+def _out_f64(a, name):
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+        raise InvalidArgument(f"{name} must be a C-contiguous float64 numpy array (updated in place)")
+    return a
+
+
+def _devptr(t):
+    """Device pointer of a torch CUDA tensor / object with data_ptr(), or a raw int."""
+    if isinstance(t, int):
+        return t
+    if hasattr(t, "data_ptr"):
+        return int(t.data_ptr())
+    raise InvalidArgument("expected a device tensor or a raw device pointer")
+
+
+# -------------------------------------------------------------------------------------------
+# reference-mirroring types (krylov.hpp)
+# -------------------------------------------------------------------------------------------
+
+class Method(enum.IntEnum):
+    Cg = 0
+    BiCgStab = 1
+
+
+class Precision(enum.IntEnum):
+    FP64 = 0
+    MIXED = 1
+
+
+@dataclass
+class SolveControl:
+    abs_tolerance: float = 1e-10
+    max_iterations: int = 1000
+
+    def _c(self):
+        return ControlStruct(float(self.abs_tolerance), int(self.max_iterations))
+
+
+@dataclass
+class SolveStats:
+    iterations: int = 0
+    residual: float = 0.0
+    converged: bool = False
+    on_device: bool = False
+    true_residual: float = 0.0
+
+    @staticmethod
+    def _from(s: StatsStruct) -> "SolveStats":
+        return SolveStats(s.iterations, s.residual, bool(s.converged), bool(s.on_device),
+                          s.true_residual)
+
+
+@dataclass
+class CsrView:
+    """krylov.hpp:10-16: square (or rectangular: n rows) CSR matrix."""
+    n: int
+    row_ptr: np.ndarray
+    col: np.ndarray
+    val: np.ndarray
+
+    def __post_init__(self):
+        self.row_ptr = _i32(self.row_ptr)
+        self.col = _i32(self.col)
+        self.val = _f64(self.val)
+
+    @property
+    def nnz(self):
+        return int(self.row_ptr[-1]) if len(self.row_ptr) else 0
+
+    def _c(self):
+        return CsrStruct(int(self.n), self.nnz, _ip(self.row_ptr), _ip(self.col), _dp(self.val))
+
+
+def _empty_csr():
+    return CsrStruct(0, 0, None, None, None)
+
+
+@dataclass
+class AmgLevelView:
+    a: CsrView | None = None
+    p: CsrView | None = None
+    r: CsrView | None = None
+
+
+@dataclass
+class AmgView:
+    """krylov.hpp:48-58."""
+    levels: list = field(default_factory=list)
+    coarse_inverse: np.ndarray | None = None
+    smooth_sweeps: int = 2
+    jacobi_weight: float = 0.7
+
+    def _c(self):
+        L = len(self.levels)
+        arr = (AmgLevelStruct * max(L, 1))()
+        for l, lv in enumerate(self.levels):
+            arr[l].a = lv.a._c() if lv.a is not None else _empty_csr()
+            arr[l].p = lv.p._c() if lv.p is not None else _empty_csr()
+            arr[l].r = lv.r._c() if lv.r is not None else _empty_csr()
+        ci = _f64(self.coarse_inverse) if self.coarse_inverse is not None else None
+        v = AmgViewStruct(L, arr, _dp(ci) if ci is not None else None, int(self.smooth_sweeps),
+                          float(self.jacobi_weight))
+        v._keep = (arr, ci)
+        return v
+
+
+@dataclass
+class LduPattern:
+    """krylov.hpp:68-77."""
+    n: int
+    n_faces: int
+    row_ptr: np.ndarray
+    col: np.ndarray
+    diag_pos: np.ndarray
+    upper_pos: np.ndarray
+    lower_pos: np.ndarray
+
+    def __post_init__(self):
+        for k in ("row_ptr", "col", "diag_pos", "upper_pos", "lower_pos"):
+            setattr(self, k, _i32(getattr(self, k)))
+
+    @property
+    def nnz(self):
+        return int(self.row_ptr[-1])
+
+    def _c(self):
+        return PatternStruct(int(self.n), int(self.n_faces), self.nnz, _ip(self.row_ptr),
+                             _ip(self.col), _ip(self.diag_pos), _ip(self.upper_pos),
+                             _ip(self.lower_pos))
+
+
+# -------------------------------------------------------------------------------------------
+# backend queries (krylov.hpp:118-123)
+# -------------------------------------------------------------------------------------------
+
+def backend_name() -> str:
+    buf = C.create_string_buffer(64)
+    _check(_lib.cfdb_backend_name(buf, len(buf)))
+    return buf.value.decode()
+
+
+def device_available() -> bool:
+    return bool(_lib.cfdb_device_available())
+
+
+def device_description() -> str:
+    buf = C.create_string_buffer(512)
+    _check(_lib.cfdb_device_description(buf, len(buf)))
+    return buf.value.decode()
+
+
+# -------------------------------------------------------------------------------------------
+# one-shot calls
+# -------------------------------------------------------------------------------------------
+
+def assemble_convection_diffusion(n_cells, n_faces, owner, neighbour, flux, gamma, delta_coeff,
+                                  convection, upper, lower, diag, divergence) -> None:
+    """krylov.hpp:105-116; upper/lower/diag/divergence are numpy float64 arrays updated in
+    place (diag and divergence accumulated)."""
+    own, nei = _i32(owner[:n_faces]), _i32(neighbour[:n_faces])
+    flux, gamma, delta = _f64(flux), _f64(gamma), _f64(delta_coeff)
+    for a, nm in ((upper, "upper"), (lower, "lower"), (diag, "diag"), (divergence, "divergence")):
+        _out_f64(a, nm)
+    if min(len(own), len(nei), len(flux), len(gamma), len(delta), len(upper), len(lower)) < n_faces \
+            or min(len(diag), len(divergence)) < n_cells:
+        raise InvalidArgument("array shorter than n_faces / n_cells")
+    _check(_lib.cfdb_assemble(int(n_cells), int(n_faces), _ip(own), _ip(nei), _dp(flux),
+                              _dp(gamma), _dp(delta), float(convection), _dp(upper), _dp(lower),
+                              _dp(diag), _dp(divergence)))
+
+
+def assemble_convection_diffusion_device(n_cells, n_faces, owner, neighbour, flux, gamma,
+                                         delta_coeff, convection, upper, lower, diag,
+                                         divergence) -> None:
+    """Same on device arrays (torch CUDA tensors or raw device pointers)."""
+    _check(_lib.cfdb_assemble_device(int(n_cells), int(n_faces), _devptr(owner),
+                                     _devptr(neighbour), _devptr(flux), _devptr(gamma),
+                                     _devptr(delta_coeff), float(convection), _devptr(upper),
+                                     _devptr(lower), _devptr(diag), _devptr(divergence)))
+
+
+def solve(a: CsrView, b, x, method: Method, control: SolveControl) -> SolveStats:
+    """krylov.hpp:37-38 (Jacobi-preconditioned CG); x: float64 array, initial guess in and
+    solution out."""
+    b = _f64(b)
+    _out_f64(x, "x")
+    st = StatsStruct()
+    cs, ctl = a._c(), control._c()
+    _check(_lib.cfdb_solve(C.byref(cs), _dp(b), _dp(x), int(method), C.byref(ctl), C.byref(st)))
+    return SolveStats._from(st)
+
+
+def solve_amg_cg(amg: AmgView, b, x, control: SolveControl) -> SolveStats:
+    """krylov.hpp:61-62: AMG-preconditioned CG, A = amg.levels[0].a."""
+    b = _f64(b)
+    _out_f64(x, "x")
+    st = StatsStruct()
+    v, ctl = amg._c(), control._c()
+    _check(_lib.cfdb_solve_amg_cg(C.byref(v), _dp(b), _dp(x), C.byref(ctl), C.byref(st)))
+    return SolveStats._from(st)
+
+
+def build_csr_pattern(n, owner, neighbour) -> LduPattern:
+    """fv::build_csr_pattern (ldu_matrix.cpp:572-612) from internal-face addressing."""
+    nei = _i32(neighbour)
+    nf = len(nei)
+    own = _i32(owner[:nf])
+    rp = np.zeros(n + 1, np.int32)
+    col = np.zeros(n + 2 * nf, np.int32)
+    dp, up, lp = np.zeros(n, np.int32), np.zeros(nf, np.int32), np.zeros(nf, np.int32)
+    nnz = C.c_int()
+    _check(_lib.cfdb_build_pattern(int(n), nf, _ip(own), _ip(nei), _ip(rp), _ip(col), _ip(dp),
+                                   _ip(up), _ip(lp), C.byref(nnz)))
+    return LduPattern(n, nf, rp, col[:nnz.value].copy(), dp, up, lp)
+
+
+# -------------------------------------------------------------------------------------------
+# AMG hierarchy (fv::AmgPreconditioner::setup, host)
+# -------------------------------------------------------------------------------------------
+
+@dataclass
+class AmgSettings:
+    strength_threshold: float = 0.08
+    max_levels: int = 25
+    coarse_size: int = 400
+    smooth_sweeps: int = 2
+    jacobi_weight: float = 0.7
+
+    def _c(self):
+        return AmgSettingsStruct(float(self.strength_threshold), int(self.max_levels),
+                                 int(self.coarse_size), int(self.smooth_sweeps),
+                                 float(self.jacobi_weight))
+
+
+class AmgHierarchy:
+    """Smoothed-aggregation hierarchy built on the host by the library (amg.cpp:122-190)."""
+
+    def __init__(self, a: CsrView, settings: AmgSettings | None = None):
+        self.settings = settings or AmgSettings()
+        h = _vp()
+        cs, ss = a._c(), self.settings._c()
+        _check(_lib.cfdb_amg_setup(C.byref(cs), C.byref(ss), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.cfdb_hierarchy_destroy(h)
+            self._h = None
+
+    def levels(self) -> int:
+        n = C.c_int()
+        _check(_lib.cfdb_hierarchy_levels(self._h, C.byref(n)))
+        return n.value
+
+    def _csr(self, level, which):
+        nr, nc, m = C.c_int(), C.c_int(), CsrStruct()
+        _check(_lib.cfdb_hierarchy_level(self._h, level, which, C.byref(nr), C.byref(nc), C.byref(m)))
+        nnz = m.nnz
+        rp = np.ctypeslib.as_array(m.row_ptr, (nr.value + 1,)).copy()
+        ci = np.ctypeslib.as_array(m.col, (max(nnz, 1),))[:nnz].copy() if nnz else np.zeros(0, np.int32)
+        va = np.ctypeslib.as_array(m.val, (max(nnz, 1),))[:nnz].copy() if nnz else np.zeros(0)
+        return CsrView(nr.value, rp, ci, va), nc.value
+
+    def level_matrix(self, level) -> CsrView:
+        return self._csr(level, 0)[0]
+
+    def level_prolongation(self, level) -> CsrView:
+        return self._csr(level, 1)[0]
+
+    def level_restriction(self, level) -> CsrView:
+        return self._csr(level, 2)[0]
+
+    def level_size(self, level) -> int:
+        return self.level_matrix(level).n
+
+    def aggregates(self, level):
+        p, n = _pi(), C.c_int()
+        _check(_lib.cfdb_hierarchy_aggregates(self._h, level, C.byref(p), C.byref(n)))
+        return np.ctypeslib.as_array(p, (self.level_size(level),)).copy(), n.value
+
+    def coarse_inverse(self) -> np.ndarray:
+        p, n = _pd(), C.c_int()
+        _check(_lib.cfdb_hierarchy_coarse_inverse(self._h, C.byref(p), C.byref(n)))
+        return np.ctypeslib.as_array(p, (n.value * n.value,)).copy()
+
+    def operator_complexity(self) -> float:
+        v = C.c_double()
+        _check(_lib.cfdb_hierarchy_operator_complexity(self._h, C.byref(v)))
+        return v.value
+
+    def view(self) -> AmgView:
+        L = self.levels()
+        lv = []
+        for l in range(L):
+            a = self.level_matrix(l)
+            p = self.level_prolongation(l) if l + 1 < L else None
+            r = self.level_restriction(l) if l + 1 < L else None
+            lv.append(AmgLevelView(a, p, r))
+        return AmgView(lv, self.coarse_inverse(), self.settings.smooth_sweeps,
+                       self.settings.jacobi_weight)
+
+
+# -------------------------------------------------------------------------------------------
+# persistent system (DeviceSolver)
+# -------------------------------------------------------------------------------------------
+
+class DeviceSolver:
+    """krylov.hpp:83-103: persistent solver for repeated solves on one LDU pattern."""
+
+    def __init__(self, pattern: LduPattern | None = None, *, mesh=None):
+        h = _vp()
+        if pattern is not None:
+            self.pattern = pattern
+            ps = pattern._c()
+            _check(_lib.cfdb_system_create(C.byref(ps), C.byref(h)))
+            self.n, self.n_faces = pattern.n, pattern.n_faces
+        elif mesh is not None:
+            n, own, nei = mesh
+            nei = _i32(nei)
+            own = _i32(own[:len(nei)])
+            _check(_lib.cfdb_system_create_mesh(int(n), len(nei), _ip(own), _ip(nei), C.byref(h)))
+            self.n, self.n_faces = int(n), len(nei)
+            self.pattern = None
+        else:
+            raise InvalidArgument("DeviceSolver needs a pattern or mesh addressing")
+        self._h = h
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.cfdb_system_destroy(h)
+            self._h = None
+
+    __del__ = close
+
+    def on_device(self) -> bool:
+        return bool(_lib.cfdb_system_on_device(self._h))
+
+    def set_amg(self, amg: AmgView) -> None:
+        v = amg._c()
+        _check(_lib.cfdb_system_set_amg(self._h, C.byref(v)))
+
+    def setup_amg(self, diag, upper, lower, settings: AmgSettings | None = None) -> None:
+        s = (settings or AmgSettings())._c()
+        _check(_lib.cfdb_system_setup_amg(self._h, _dp(_f64(diag)), _dp(_f64(upper)),
+                                          _dp(_f64(lower)), C.byref(s)))
+
+    def set_precision(self, precision: Precision) -> None:
+        _check(_lib.cfdb_system_set_precision(self._h, int(precision)))
+
+    def solve(self, diag, upper, lower, b, x, method: Method = Method.Cg, use_amg: bool = True,
+              control: SolveControl | None = None) -> SolveStats:
+        diag, upper, lower, b = _f64(diag), _f64(upper), _f64(lower), _f64(b)
+        _out_f64(x, "x")
+        if len(diag) != self.n or len(b) != self.n or len(x) != self.n or \
+                len(upper) != self.n_faces or len(lower) != self.n_faces:
+            raise InvalidArgument("array sizes do not match the pattern")
+        st = StatsStruct()
+        ctl = (control or SolveControl())._c()
+        _check(_lib.cfdb_system_solve(self._h, _dp(diag), _dp(upper), _dp(lower), _dp(b), _dp(x),
+                                      int(method), 1 if use_amg else 0, C.byref(ctl),
+                                      C.byref(st)))
+        return SolveStats._from(st)
+
+    def solve_device(self, diag, upper, lower, b, x, method: Method = Method.Cg,
+                     use_amg: bool = True, control: SolveControl | None = None) -> SolveStats:
+        """All arrays device-resident (torch CUDA float64 tensors or raw pointers)."""
+        st = StatsStruct()
+        ctl = (control or SolveControl())._c()
+        _check(_lib.cfdb_system_solve_device(self._h, _devptr(diag), _devptr(upper),
+                                             _devptr(lower), _devptr(b), _devptr(x), int(method),
+                                             1 if use_amg else 0, C.byref(ctl), C.byref(st)))
+        return SolveStats._from(st)
+
+    def assemble_device(self, flux, gamma, delta, convection, upper, lower, diag, div) -> None:
+        _check(_lib.cfdb_system_assemble_device(self._h, _devptr(flux), _devptr(gamma),
+                                                _devptr(delta), float(convection),
+                                                _devptr(upper), _devptr(lower), _devptr(diag),
+                                                _devptr(div)))
+
+    def apply_amg(self, r) -> np.ndarray:
+        """One V-cycle z = M^-1 r on the installed hierarchy (AmgPreconditioner::apply)."""
+        r = _f64(r)
+        z = np.zeros(self.n)
+        _check(_lib.cfdb_system_apply_amg(self._h, _dp(r), _dp(z)))
+        return z
+
+    def stream(self) -> int:
+        s = _vp()
+        _check(_lib.cfdb_system_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def device_bytes(self) -> int:
+        b = C.c_size_t()
+        _check(_lib.cfdb_system_device_bytes(self._h, C.byref(b)))
+        return b.value
+
+
+# -------------------------------------------------------------------------------------------
+# synthetic workloads (include/cfdb_synth.h)
+# -------------------------------------------------------------------------------------------
+
+def positions_graded(n: int, grading: float) -> np.ndarray:
+    out = np.zeros(n + 1)
+    _check(_lib.cfdb_positions_graded(n, float(grading), _dp(out)))
+    return out
+
+
+def positions_two_sided(n: int, ratio: float) -> np.ndarray:
+    out = np.zeros(n + 1)
+    _check(_lib.cfdb_positions_two_sided(n, float(ratio), _dp(out)))
+    return out
+
+
+class Mesh:
+    """Box (hex) or jittered 6-tet mesh in the reference's face ordering, with geometry."""
+
+    def __init__(self, h, nx, ny, nz):
+        self._h = h
+        self.shape = (nx, ny, nz)
+        nc, nf, ni, npn = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(_lib.cfdb_mesh_sizes(h, C.byref(nc), C.byref(nf), C.byref(ni), C.byref(npn)))
+        self.n_cells, self.n_faces, self.n_internal_faces, self.n_points = (
+            nc.value, nf.value, ni.value, npn.value)
+        o, n = _pi(), _pi()
+        _check(_lib.cfdb_mesh_addressing(h, C.byref(o), C.byref(n)))
+        self.owner = np.ctypeslib.as_array(o, (self.n_faces,)).copy()
+        self.neighbour = np.ctypeslib.as_array(n, (self.n_internal_faces,)).copy()
+        pts, fc, sf, cc, vol = _pd(), _pd(), _pd(), _pd(), _pd()
+        _check(_lib.cfdb_mesh_geometry(h, C.byref(pts), C.byref(fc), C.byref(sf), C.byref(cc),
+                                       C.byref(vol)))
+        self.points = np.ctypeslib.as_array(pts, (self.n_points, 3)).copy()
+        self.face_centres = np.ctypeslib.as_array(fc, (self.n_faces, 3)).copy()
+        self.face_areas = np.ctypeslib.as_array(sf, (self.n_faces, 3)).copy()
+        self.cell_centres = np.ctypeslib.as_array(cc, (self.n_cells, 3)).copy()
+        self.cell_volumes = np.ctypeslib.as_array(vol, (self.n_cells,)).copy()
+        dl, w = _pd(), _pd()
+        _check(_lib.cfdb_mesh_fv(h, C.byref(dl), C.byref(w)))
+        self.delta = np.ctypeslib.as_array(dl, (self.n_internal_faces,)).copy()
+        self.weights = np.ctypeslib.as_array(w, (self.n_internal_faces,)).copy()
+        fo, fn = _pi(), _pi()
+        _check(_lib.cfdb_mesh_faces(h, C.byref(fo), C.byref(fn)))
+        self.face_offsets = np.ctypeslib.as_array(fo, (self.n_faces + 1,)).copy()
+        self.face_nodes = np.ctypeslib.as_array(fn, (int(self.face_offsets[-1]),)).copy()
+
+    @staticmethod
+    def box(nx, ny, nz, xs=None, ys=None, zs=None) -> "Mesh":
+        xs = _f64(xs if xs is not None else np.linspace(0, 1, nx + 1))
+        ys = _f64(ys if ys is not None else np.linspace(0, 1, ny + 1))
+        zs = _f64(zs if zs is not None else np.linspace(0, 1, nz + 1))
+        h = _vp()
+        _check(_lib.cfdb_mesh_box(nx, ny, nz, _dp(xs), _dp(ys), _dp(zs), C.byref(h)))
+        return Mesh(h, nx, ny, nz)
+
+    @staticmethod
+    def tet(nx, ny, nz, jitter=0.2, seed=0, xs=None, ys=None, zs=None) -> "Mesh":
+        xs = _f64(xs if xs is not None else np.linspace(0, 1, nx + 1))
+        ys = _f64(ys if ys is not None else np.linspace(0, 1, ny + 1))
+        zs = _f64(zs if zs is not None else np.linspace(0, 1, nz + 1))
+        h = _vp()
+        _check(_lib.cfdb_mesh_tet(nx, ny, nz, _dp(xs), _dp(ys), _dp(zs), float(jitter),
+                                  int(seed), C.byref(h)))
+        return Mesh(h, nx, ny, nz)
+
+    def pressure_inputs(self, sigma=0.0, unit_rau=False, flux_kind=0, rhs_kind=1, seed=0):
+        """(gamma, flux, source) of a pressure system on this mesh."""
+        g = np.zeros(self.n_internal_faces)
+        f = np.zeros(self.n_internal_faces)
+        s = np.zeros(self.n_cells)
+        _check(_lib.cfdb_synth_pressure_inputs(self._h, float(sigma), 1 if unit_rau else 0,
+                                               int(flux_kind), int(rhs_kind), int(seed), _dp(g),
+                                               _dp(f), _dp(s)))
+        return g, f, s
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.cfdb_mesh_destroy(h)
+            self._h = None
+
+
+from . import workloads  # noqa: E402,F401  (configs of the pressure systems)

@@ -1,0 +1,763 @@
+// C ABI of the cfdb library (declared in include/cfdb.h).
+#include "../../include/cfdb.h"
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "engine.hpp"
+#include "host_algos.hpp"
+
+using namespace cfdb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+template <class F> int guarded(F&& f) {
+    try {
+        f();
+        return CFDB_OK;
+    } catch (const Error& e) {
+        return set_error(e.code, e.what());
+    } catch (const std::bad_alloc&) {
+        return set_error(CFDB_ERR_OOM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return set_error(CFDB_ERR_INTERNAL, e.what());
+    }
+}
+
+int copy_str(const std::string& s, char* buf, size_t len) {
+    if (buf == nullptr || len == 0) return set_error(CFDB_ERR_BAD_ARG, "null buffer");
+    const size_t n = std::min(len - 1, s.size());
+    std::memcpy(buf, s.data(), n);
+    buf[n] = '\0';
+    return CFDB_OK;
+}
+
+void require_device() {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        (void)cudaGetLastError();
+        fail(CFDB_ERR_NO_DEVICE, "no CUDA device: this library has no host fallback");
+    }
+}
+
+HostCsr csr_from(const cfdb_csr& v, int n_cols) {
+    HostCsr m;
+    m.n_rows = v.n;
+    m.n_cols = n_cols;
+    if (v.n < 0 || v.nnz < 0) fail(CFDB_ERR_BAD_ARG, "negative CSR size");
+    if (v.n > 0 && (v.row_ptr == nullptr || (v.nnz > 0 && (v.col == nullptr || v.val == nullptr)))) {
+        fail(CFDB_ERR_BAD_ARG, "CSR view with null arrays");
+    }
+    m.rp.assign(v.row_ptr, v.row_ptr + v.n + 1);
+    if (m.rp[0] != 0 || m.rp[v.n] != v.nnz) fail(CFDB_ERR_BAD_ARG, "CSR row_ptr inconsistent with nnz");
+    for (int i = 0; i < v.n; ++i)
+        if (m.rp[i + 1] < m.rp[i]) fail(CFDB_ERR_BAD_ARG, "CSR row_ptr not monotone");
+    m.ci.assign(v.col, v.col + v.nnz);
+    m.va.assign(v.val, v.val + v.nnz);
+    for (int c : m.ci)
+        if (c < 0 || c >= n_cols) fail(CFDB_ERR_BAD_ARG, "CSR column index out of range");
+    return m;
+}
+
+// Copies an AmgView into a host hierarchy; level 0's operator is optional (skip_a0).
+std::shared_ptr<Hierarchy> hierarchy_from(const cfdb_amg_view& v, int n0, bool skip_a0) {
+    if (v.n_levels <= 0 || v.levels == nullptr) fail(CFDB_ERR_BAD_ARG, "empty hierarchy");
+    auto h = std::make_shared<Hierarchy>();
+    const int L = v.n_levels;
+    std::vector<int> n(L);
+    n[0] = n0;
+    for (int l = 1; l < L; ++l) n[l] = v.levels[l].a.n;
+    for (int l = 0; l < L; ++l) {
+        if (l == 0 && skip_a0) {
+            h->a.emplace_back();
+            h->a.back().n_rows = h->a.back().n_cols = n0;
+        } else {
+            h->a.push_back(csr_from(v.levels[l].a, n[l]));
+        }
+        if (l + 1 < L) {
+            h->p.push_back(csr_from(v.levels[l].p, n[l + 1]));
+            h->r.push_back(csr_from(v.levels[l].r, n[l]));
+        }
+    }
+    h->n_c = n[L - 1];
+    if (v.coarse_inverse == nullptr) fail(CFDB_ERR_BAD_ARG, "hierarchy without coarse inverse");
+    h->coarse_inverse.assign(v.coarse_inverse, v.coarse_inverse + static_cast<size_t>(h->n_c) * h->n_c);
+    h->ldlt_ok = true;
+    return h;
+}
+
+} // namespace
+
+// ------------------------------------------------------------------------------------------------
+// system object
+// ------------------------------------------------------------------------------------------------
+
+struct cfdb_system {
+    int device = 0;
+    LduPatternHost pat;
+    std::vector<int> owner, neighbour; // kept when created from mesh addressing
+    std::unique_ptr<Engine> eng;
+    std::shared_ptr<const Hierarchy> h;
+    int sweeps = 2;
+    double weight = 0.7;
+    int precision = CFDB_PRECISION_FP64;
+    bool dirty = true;
+    // value map of the level-0 CSR entries into [diag | upper | lower]
+    std::vector<int> src;
+    std::vector<int> diag_src;
+    // device copies for the fused face assembly
+    DeviceArena asm_arena;
+    int* d_owner = nullptr;
+    int* d_cf_ptr = nullptr;
+    int* d_cf_face = nullptr;
+};
+
+namespace {
+
+void build_value_map(cfdb_system* s) {
+    const LduPatternHost& p = s->pat;
+    s->src.assign(static_cast<size_t>(p.nnz()), -1);
+    for (int i = 0; i < p.n; ++i) s->src[p.diag_pos[i]] = i;
+    for (int f = 0; f < p.n_faces; ++f) {
+        s->src[p.upper_pos[f]] = p.n + f;
+        s->src[p.lower_pos[f]] = p.n + p.n_faces + f;
+    }
+    s->diag_src.resize(static_cast<size_t>(p.n));
+    for (int i = 0; i < p.n; ++i) s->diag_src[i] = i;
+}
+
+void ensure_engine(cfdb_system* s) {
+    if (!s->dirty && s->eng) return;
+    CFDB_CUDA(cudaSetDevice(s->device));
+    if (!s->eng) s->eng = std::make_unique<Engine>(s->device);
+    SystemSpec sp;
+    sp.n = s->pat.n;
+    sp.rp = s->pat.row_ptr.data();
+    sp.ci = s->pat.col.data();
+    sp.src = s->src;
+    sp.diag_src = s->diag_src;
+    sp.vs_len = s->pat.n + 2 * s->pat.n_faces;
+    sp.h = s->h;
+    const bool mixed = s->precision == CFDB_PRECISION_MIXED;
+    std::vector<SystemSpec> v;
+    v.push_back(std::move(sp));
+    s->eng->build(std::move(v), s->sweeps, s->weight, /*need64=*/!mixed, /*need32=*/mixed);
+    s->dirty = false;
+}
+
+void validate_pattern(const cfdb_ldu_pattern& p) {
+    if (p.n <= 0 || p.n_faces < 0 || p.nnz < p.n) fail(CFDB_ERR_BAD_ARG, "invalid pattern sizes");
+    if (p.row_ptr == nullptr || p.col == nullptr || p.diag_pos == nullptr ||
+        (p.n_faces > 0 && (p.upper_pos == nullptr || p.lower_pos == nullptr))) {
+        fail(CFDB_ERR_BAD_ARG, "pattern with null arrays");
+    }
+    if (p.row_ptr[0] != 0 || p.row_ptr[p.n] != p.nnz) fail(CFDB_ERR_BAD_ARG, "pattern row_ptr inconsistent");
+    for (int i = 0; i < p.n; ++i) {
+        if (p.row_ptr[i + 1] < p.row_ptr[i]) fail(CFDB_ERR_BAD_ARG, "pattern row_ptr not monotone");
+        if (p.diag_pos[i] < p.row_ptr[i] || p.diag_pos[i] >= p.row_ptr[i + 1])
+            fail(CFDB_ERR_BAD_ARG, "diag_pos outside its row");
+    }
+    for (int k = 0; k < p.nnz; ++k)
+        if (p.col[k] < 0 || p.col[k] >= p.n) fail(CFDB_ERR_BAD_ARG, "pattern column out of range");
+    for (int f = 0; f < p.n_faces; ++f) {
+        if (p.upper_pos[f] < 0 || p.upper_pos[f] >= p.nnz || p.lower_pos[f] < 0 || p.lower_pos[f] >= p.nnz)
+            fail(CFDB_ERR_BAD_ARG, "face position out of range");
+    }
+}
+
+// Cell -> face lists in ascending face order (owner and neighbour faces merged).
+void cell_faces(int n, int nf, const int* own, const int* nei, std::vector<int>& ptr, std::vector<int>& face) {
+    ptr.assign(static_cast<size_t>(n) + 1, 0);
+    for (int f = 0; f < nf; ++f) {
+        ++ptr[own[f] + 1];
+        ++ptr[nei[f] + 1];
+    }
+    for (int c = 0; c < n; ++c) ptr[c + 1] += ptr[c];
+    face.resize(static_cast<size_t>(ptr[n]));
+    std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+    for (int f = 0; f < nf; ++f) {
+        face[fill[own[f]]++] = f;
+        face[fill[nei[f]]++] = f;
+    }
+}
+
+SolveResult run_single(cfdb_system* s, const double* diag, const double* upper, const double* lower,
+                       const double* b, double* x, int method, int use_amg, const cfdb_control* c, bool dev) {
+    if (c == nullptr) fail(CFDB_ERR_BAD_ARG, "null control");
+    if (method != CFDB_METHOD_CG && method != CFDB_METHOD_BICGSTAB) fail(CFDB_ERR_BAD_ARG, "unknown method");
+    if (method == CFDB_METHOD_BICGSTAB) {
+        fail(CFDB_ERR_BAD_ARG, "BiCGStab is not provided by this library (pressure path: CG)");
+    }
+    if (diag == nullptr || b == nullptr || x == nullptr || (s->pat.n_faces > 0 && (upper == nullptr || lower == nullptr)))
+        fail(CFDB_ERR_BAD_ARG, "null array");
+    ensure_engine(s);
+    Engine& e = *s->eng;
+    const int n = s->pat.n, nf = s->pat.n_faces;
+    if (dev) {
+        e.set_values_device(diag, upper, lower, n, n + nf);
+    } else {
+        std::vector<double> vs(static_cast<size_t>(n) + 2 * static_cast<size_t>(nf));
+        std::memcpy(vs.data(), diag, sizeof(double) * n);
+        if (nf > 0) {
+            std::memcpy(vs.data() + n, upper, sizeof(double) * nf);
+            std::memcpy(vs.data() + n + nf, lower, sizeof(double) * nf);
+        }
+        e.upload_values({vs.data()});
+        CFDB_CUDA(cudaStreamSynchronize(e.stream()));
+    }
+    e.set_rhs(0, b, dev);
+    e.set_guess(0, x, dev);
+    Mode mode = Mode::Jacobi;
+    if (use_amg && s->h) mode = s->precision == CFDB_PRECISION_MIXED ? Mode::AmgMixed : Mode::AmgFp64;
+    if (mode == Mode::Jacobi && s->precision == CFDB_PRECISION_MIXED) {
+        // Jacobi CG runs on the FP64 level-0 operator, which exists in every precision.
+    }
+    SolveRequest rq;
+    rq.tol = c->abs_tolerance;
+    rq.max_it = c->max_iterations;
+    const auto res = e.solve(mode, {rq});
+    e.get_solution(0, x, dev);
+    CFDB_CUDA(cudaStreamSynchronize(e.stream()));
+    return res[0];
+}
+
+void put_stats(cfdb_stats* st, const SolveResult& r) {
+    if (st == nullptr) return;
+    st->iterations = r.iterations;
+    st->residual = r.residual;
+    st->converged = r.converged ? 1 : 0;
+    st->on_device = 1;
+    st->true_residual = r.true_residual;
+}
+
+} // namespace
+
+extern "C" {
+
+int cfdb_backend_name(char* buf, size_t len) { return copy_str("cuda", buf, len); }
+
+int cfdb_device_available(void) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    return count > 0 ? 1 : 0;
+}
+
+int cfdb_device_description(char* buf, size_t len) {
+    std::string s = "cuda";
+    int dev = 0;
+    cudaDeviceProp prop{};
+    if (cfdb_device_available() && cudaGetDevice(&dev) == cudaSuccess &&
+        cudaGetDeviceProperties(&prop, dev) == cudaSuccess) {
+        s += std::string(" (device: ") + prop.name + ", sm_" + std::to_string(prop.major) +
+             std::to_string(prop.minor) + ")";
+    } else {
+        (void)cudaGetLastError();
+        s += " (no CUDA device)";
+    }
+    return copy_str(s, buf, len);
+}
+
+int cfdb_last_error(char* buf, size_t len) { return copy_str(g_last_error, buf, len); }
+
+void cfdb_default_amg_settings(cfdb_amg_settings* s) {
+    if (s == nullptr) return;
+    s->strength_threshold = 0.08;
+    s->max_levels = 25;
+    s->coarse_size = 400;
+    s->smooth_sweeps = 2;
+    s->jacobi_weight = 0.7;
+}
+
+int cfdb_build_pattern(int n, int n_faces, const int* owner, const int* neighbour, int* row_ptr, int* col,
+                       int* diag_pos, int* upper_pos, int* lower_pos, int* nnz) {
+    return guarded([&] {
+        if (n <= 0 || n_faces < 0 || (n_faces > 0 && (owner == nullptr || neighbour == nullptr)) ||
+            row_ptr == nullptr || col == nullptr || diag_pos == nullptr || nnz == nullptr)
+            fail(CFDB_ERR_BAD_ARG, "cfdb_build_pattern: bad arguments");
+        const LduPatternHost p = build_pattern(n, n_faces, owner, neighbour);
+        std::memcpy(row_ptr, p.row_ptr.data(), sizeof(int) * (n + 1));
+        std::memcpy(col, p.col.data(), sizeof(int) * p.col.size());
+        std::memcpy(diag_pos, p.diag_pos.data(), sizeof(int) * n);
+        if (n_faces > 0) {
+            std::memcpy(upper_pos, p.upper_pos.data(), sizeof(int) * n_faces);
+            std::memcpy(lower_pos, p.lower_pos.data(), sizeof(int) * n_faces);
+        }
+        *nnz = p.nnz();
+    });
+}
+
+// ---- assembly ----
+
+static int assemble_impl(int n_cells, int n_faces, const int* owner, const int* neighbour, const double* flux,
+                         const double* gamma, const double* delta, double convection, double* upper,
+                         double* lower, double* diag, double* div, bool dev) {
+    return guarded([&] {
+        require_device();
+        if (n_cells < 0 || n_faces < 0) fail(CFDB_ERR_BAD_ARG, "negative size");
+        if (n_faces == 0) return; // reference: nothing to do (krylov_cuda.cu:705-707)
+        if (!owner || !neighbour || !flux || !gamma || !delta || !upper || !lower || !diag || !div)
+            fail(CFDB_ERR_BAD_ARG, "null array");
+        std::vector<int> h_own, h_nei;
+        const int* own_h = owner;
+        const int* nei_h = neighbour;
+        if (dev) {
+            h_own.resize(n_faces);
+            h_nei.resize(n_faces);
+            CFDB_CUDA(cudaMemcpy(h_own.data(), owner, sizeof(int) * n_faces, cudaMemcpyDeviceToHost));
+            CFDB_CUDA(cudaMemcpy(h_nei.data(), neighbour, sizeof(int) * n_faces, cudaMemcpyDeviceToHost));
+            own_h = h_own.data();
+            nei_h = h_nei.data();
+        }
+        for (int f = 0; f < n_faces; ++f) {
+            if (own_h[f] < 0 || own_h[f] >= n_cells || nei_h[f] < 0 || nei_h[f] >= n_cells)
+                fail(CFDB_ERR_BAD_ARG, "face addresses a cell out of range");
+        }
+        std::vector<int> ptr, face;
+        cell_faces(n_cells, n_faces, own_h, nei_h, ptr, face);
+        cudaStream_t st = nullptr;
+        CFDB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        struct StreamGuard {
+            cudaStream_t s;
+            ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+        } guard{st};
+        DeviceArena ar;
+        const int* d_ptr = ar.upload(ptr, st);
+        const int* d_face = ar.upload(face, st);
+        const int* d_own;
+        const double *d_flux, *d_gamma, *d_delta;
+        double *d_up, *d_lo, *d_diag, *d_div;
+        if (dev) {
+            d_own = owner;
+            d_flux = flux;
+            d_gamma = gamma;
+            d_delta = delta;
+            d_up = upper;
+            d_lo = lower;
+            d_diag = diag;
+            d_div = div;
+        } else {
+            int* o = ar.alloc<int>(n_faces);
+            double* buf = ar.alloc<double>(5 * static_cast<size_t>(n_faces) + 2 * static_cast<size_t>(n_cells));
+            CFDB_CUDA(cudaMemcpyAsync(o, owner, sizeof(int) * n_faces, cudaMemcpyHostToDevice, st));
+            double* fl = buf;
+            double* ga = fl + n_faces;
+            double* de = ga + n_faces;
+            d_up = de + n_faces;
+            d_lo = d_up + n_faces;
+            d_diag = d_lo + n_faces;
+            d_div = d_diag + n_cells;
+            CFDB_CUDA(cudaMemcpyAsync(fl, flux, sizeof(double) * n_faces, cudaMemcpyHostToDevice, st));
+            CFDB_CUDA(cudaMemcpyAsync(ga, gamma, sizeof(double) * n_faces, cudaMemcpyHostToDevice, st));
+            CFDB_CUDA(cudaMemcpyAsync(de, delta, sizeof(double) * n_faces, cudaMemcpyHostToDevice, st));
+            CFDB_CUDA(cudaMemcpyAsync(d_diag, diag, sizeof(double) * n_cells, cudaMemcpyHostToDevice, st));
+            CFDB_CUDA(cudaMemcpyAsync(d_div, div, sizeof(double) * n_cells, cudaMemcpyHostToDevice, st));
+            d_own = o;
+            d_flux = fl;
+            d_gamma = ga;
+            d_delta = de;
+        }
+        k_assemble_faces<<<(n_faces + 255) / 256, 256, 0, st>>>(n_faces, d_flux, d_gamma, d_delta, convection, d_up,
+                                                               d_lo);
+        k_assemble_cells<<<(n_cells + 255) / 256, 256, 0, st>>>(n_cells, d_ptr, d_face, d_flux, d_gamma, d_delta, d_own,
+                                                               convection, d_diag, d_div);
+        CFDB_CUDA(cudaGetLastError());
+        if (!dev) {
+            CFDB_CUDA(cudaMemcpyAsync(upper, d_up, sizeof(double) * n_faces, cudaMemcpyDeviceToHost, st));
+            CFDB_CUDA(cudaMemcpyAsync(lower, d_lo, sizeof(double) * n_faces, cudaMemcpyDeviceToHost, st));
+            CFDB_CUDA(cudaMemcpyAsync(diag, d_diag, sizeof(double) * n_cells, cudaMemcpyDeviceToHost, st));
+            CFDB_CUDA(cudaMemcpyAsync(div, d_div, sizeof(double) * n_cells, cudaMemcpyDeviceToHost, st));
+        }
+        CFDB_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+int cfdb_assemble(int n_cells, int n_faces, const int* owner, const int* neighbour, const double* flux,
+                  const double* gamma, const double* delta_coeff, double convection, double* upper, double* lower,
+                  double* diag, double* divergence) {
+    return assemble_impl(n_cells, n_faces, owner, neighbour, flux, gamma, delta_coeff, convection, upper, lower,
+                         diag, divergence, false);
+}
+
+int cfdb_assemble_device(int n_cells, int n_faces, const int* owner, const int* neighbour, const double* flux,
+                         const double* gamma, const double* delta_coeff, double convection, double* upper,
+                         double* lower, double* diag, double* divergence) {
+    return assemble_impl(n_cells, n_faces, owner, neighbour, flux, gamma, delta_coeff, convection, upper, lower,
+                         diag, divergence, true);
+}
+
+// ---- one-shot solves ----
+
+int cfdb_solve(const cfdb_csr* a, const double* b, double* x, int method, const cfdb_control* control,
+               cfdb_stats* stats) {
+    return guarded([&] {
+        require_device();
+        if (a == nullptr || b == nullptr || x == nullptr || control == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
+        if (method == CFDB_METHOD_BICGSTAB) fail(CFDB_ERR_BAD_ARG, "BiCGStab is not provided by this library");
+        if (method != CFDB_METHOD_CG) fail(CFDB_ERR_BAD_ARG, "unknown method");
+        if (a->n == 0) {
+            put_stats(stats, SolveResult{0, 0.0, true, 0.0});
+            return;
+        }
+        const HostCsr m = csr_from(*a, a->n);
+        int dev = 0;
+        CFDB_CUDA(cudaGetDevice(&dev));
+        Engine e(dev);
+        SystemSpec sp;
+        sp.n = m.n_rows;
+        sp.rp = m.rp.data();
+        sp.ci = m.ci.data();
+        sp.src.resize(m.nnz());
+        for (int k = 0; k < m.nnz(); ++k) sp.src[k] = k;
+        sp.diag_src.assign(m.n_rows, -1);
+        for (int i = 0; i < m.n_rows; ++i)
+            for (int k = m.rp[i]; k < m.rp[i + 1]; ++k)
+                if (m.ci[k] == i && m.va[k] != 0.0) sp.diag_src[i] = k;
+        sp.vs_len = m.nnz();
+        std::vector<SystemSpec> v;
+        v.push_back(std::move(sp));
+        e.build(std::move(v), 2, 0.7, true, false);
+        e.upload_values({m.va.data()});
+        e.set_rhs(0, b, false);
+        e.set_guess(0, x, false);
+        const auto r = e.solve(Mode::Jacobi, {SolveRequest{control->abs_tolerance, control->max_iterations}});
+        e.get_solution(0, x, false);
+        put_stats(stats, r[0]);
+    });
+}
+
+int cfdb_solve_amg_cg(const cfdb_amg_view* amg, const double* b, double* x, const cfdb_control* control,
+                      cfdb_stats* stats) {
+    return guarded([&] {
+        require_device();
+        if (amg == nullptr || amg->n_levels <= 0 || amg->levels == nullptr)
+            fail(CFDB_ERR_BAD_ARG, "solve_amg_cg: empty hierarchy");
+        if (b == nullptr || x == nullptr || control == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
+        const int n0 = amg->levels[0].a.n;
+        auto h = hierarchy_from(*amg, n0, false);
+        const HostCsr& m = h->a[0];
+        int dev = 0;
+        CFDB_CUDA(cudaGetDevice(&dev));
+        Engine e(dev);
+        SystemSpec sp;
+        sp.n = m.n_rows;
+        sp.rp = m.rp.data();
+        sp.ci = m.ci.data();
+        sp.src.resize(m.nnz());
+        for (int k = 0; k < m.nnz(); ++k) sp.src[k] = k;
+        sp.diag_src.assign(m.n_rows, -1);
+        for (int i = 0; i < m.n_rows; ++i)
+            for (int k = m.rp[i]; k < m.rp[i + 1]; ++k)
+                if (m.ci[k] == i && m.va[k] != 0.0) sp.diag_src[i] = k;
+        sp.vs_len = m.nnz();
+        sp.h = h;
+        std::vector<SystemSpec> v;
+        v.push_back(std::move(sp));
+        e.build(std::move(v), amg->smooth_sweeps, amg->jacobi_weight, true, false);
+        e.upload_values({m.va.data()});
+        e.set_rhs(0, b, false);
+        e.set_guess(0, x, false);
+        const auto r = e.solve(Mode::AmgFp64, {SolveRequest{control->abs_tolerance, control->max_iterations}});
+        e.get_solution(0, x, false);
+        put_stats(stats, r[0]);
+    });
+}
+
+// ---- hierarchy ----
+
+struct cfdb_hierarchy {
+    Hierarchy h;
+    std::vector<cfdb_amg_level> view_levels;
+};
+
+int cfdb_amg_setup(const cfdb_csr* a, const cfdb_amg_settings* settings, cfdb_hierarchy** out) {
+    return guarded([&] {
+        if (a == nullptr || out == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
+        AmgSettings s;
+        if (settings != nullptr) {
+            s.theta = settings->strength_threshold;
+            s.max_levels = settings->max_levels;
+            s.coarse_size = settings->coarse_size;
+            s.sweeps = settings->smooth_sweeps;
+            s.weight = settings->jacobi_weight;
+        }
+        if (s.max_levels < 1) fail(CFDB_ERR_BAD_ARG, "max_levels must be >= 1");
+        const HostCsr m = csr_from(*a, a->n);
+        auto* h = new cfdb_hierarchy;
+        try {
+            h->h = amg_setup(m, s);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int cfdb_hierarchy_destroy(cfdb_hierarchy* h) {
+    delete h;
+    return CFDB_OK;
+}
+
+int cfdb_hierarchy_levels(const cfdb_hierarchy* h, int* n_levels) {
+    if (h == nullptr || n_levels == nullptr) return set_error(CFDB_ERR_BAD_ARG, "null argument");
+    *n_levels = h->h.levels();
+    return CFDB_OK;
+}
+
+static cfdb_csr view_of(const HostCsr& m) {
+    return cfdb_csr{m.n_rows, m.nnz(), m.rp.data(), m.ci.data(), m.va.data()};
+}
+
+int cfdb_hierarchy_level(const cfdb_hierarchy* h, int level, int which, int* n_rows, int* n_cols, cfdb_csr* m) {
+    if (h == nullptr || m == nullptr) return set_error(CFDB_ERR_BAD_ARG, "null argument");
+    if (level < 0 || level >= h->h.levels()) return set_error(CFDB_ERR_BAD_ARG, "level out of range");
+    const HostCsr* src = nullptr;
+    if (which == 0) src = &h->h.a[level];
+    else if (level + 1 < h->h.levels()) src = which == 1 ? &h->h.p[level] : &h->h.r[level];
+    if (src == nullptr) return set_error(CFDB_ERR_BAD_ARG, "no such operator on this level");
+    *m = view_of(*src);
+    if (n_rows) *n_rows = src->n_rows;
+    if (n_cols) *n_cols = src->n_cols;
+    return CFDB_OK;
+}
+
+int cfdb_hierarchy_aggregates(const cfdb_hierarchy* h, int level, const int** agg, int* n_aggregates) {
+    if (h == nullptr || agg == nullptr) return set_error(CFDB_ERR_BAD_ARG, "null argument");
+    if (level < 0 || level + 1 >= h->h.levels()) return set_error(CFDB_ERR_BAD_ARG, "level has no aggregates");
+    *agg = h->h.agg[level].data();
+    if (n_aggregates) *n_aggregates = h->h.n_agg[level];
+    return CFDB_OK;
+}
+
+int cfdb_hierarchy_coarse_inverse(const cfdb_hierarchy* h, const double** inv, int* n_c) {
+    if (h == nullptr || inv == nullptr) return set_error(CFDB_ERR_BAD_ARG, "null argument");
+    *inv = h->h.coarse_inverse.data();
+    if (n_c) *n_c = h->h.n_c;
+    return CFDB_OK;
+}
+
+int cfdb_hierarchy_view(cfdb_hierarchy* h, int smooth_sweeps, double jacobi_weight, cfdb_amg_view* view) {
+    if (h == nullptr || view == nullptr) return set_error(CFDB_ERR_BAD_ARG, "null argument");
+    const int L = h->h.levels();
+    h->view_levels.assign(L, cfdb_amg_level{});
+    for (int l = 0; l < L; ++l) {
+        h->view_levels[l].a = view_of(h->h.a[l]);
+        if (l + 1 < L) {
+            h->view_levels[l].p = view_of(h->h.p[l]);
+            h->view_levels[l].r = view_of(h->h.r[l]);
+        }
+    }
+    view->n_levels = L;
+    view->levels = h->view_levels.data();
+    view->coarse_inverse = h->h.coarse_inverse.data();
+    view->smooth_sweeps = smooth_sweeps;
+    view->jacobi_weight = jacobi_weight;
+    return CFDB_OK;
+}
+
+int cfdb_hierarchy_operator_complexity(const cfdb_hierarchy* h, double* oc) {
+    if (h == nullptr || oc == nullptr) return set_error(CFDB_ERR_BAD_ARG, "null argument");
+    *oc = h->h.operator_complexity();
+    return CFDB_OK;
+}
+
+// ---- persistent system ----
+
+int cfdb_system_create(const cfdb_ldu_pattern* pattern, cfdb_system** out) {
+    return guarded([&] {
+        require_device();
+        if (pattern == nullptr || out == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
+        validate_pattern(*pattern);
+        auto s = std::make_unique<cfdb_system>();
+        CFDB_CUDA(cudaGetDevice(&s->device));
+        LduPatternHost& p = s->pat;
+        p.n = pattern->n;
+        p.n_faces = pattern->n_faces;
+        p.row_ptr.assign(pattern->row_ptr, pattern->row_ptr + pattern->n + 1);
+        p.col.assign(pattern->col, pattern->col + pattern->nnz);
+        p.diag_pos.assign(pattern->diag_pos, pattern->diag_pos + pattern->n);
+        if (pattern->n_faces > 0) {
+            p.upper_pos.assign(pattern->upper_pos, pattern->upper_pos + pattern->n_faces);
+            p.lower_pos.assign(pattern->lower_pos, pattern->lower_pos + pattern->n_faces);
+        }
+        build_value_map(s.get());
+        ensure_engine(s.get());
+        *out = s.release();
+    });
+}
+
+int cfdb_system_create_mesh(int n_cells, int n_faces, const int* owner, const int* neighbour, cfdb_system** out) {
+    return guarded([&] {
+        require_device();
+        if (out == nullptr || n_cells <= 0 || n_faces < 0 || (n_faces > 0 && (!owner || !neighbour)))
+            fail(CFDB_ERR_BAD_ARG, "bad arguments");
+        auto s = std::make_unique<cfdb_system>();
+        CFDB_CUDA(cudaGetDevice(&s->device));
+        s->pat = build_pattern(n_cells, n_faces, owner, neighbour);
+        s->owner.assign(owner, owner + n_faces);
+        s->neighbour.assign(neighbour, neighbour + n_faces);
+        build_value_map(s.get());
+        std::vector<int> ptr, face;
+        cell_faces(n_cells, n_faces, owner, neighbour, ptr, face);
+        CFDB_CUDA(cudaSetDevice(s->device));
+        s->d_owner = s->asm_arena.upload(s->owner, nullptr);
+        s->d_cf_ptr = s->asm_arena.upload(ptr, nullptr);
+        s->d_cf_face = s->asm_arena.upload(face, nullptr);
+        CFDB_CUDA(cudaDeviceSynchronize());
+        ensure_engine(s.get());
+        *out = s.release();
+    });
+}
+
+int cfdb_system_destroy(cfdb_system* sys) {
+    return guarded([&] {
+        if (sys == nullptr) return;
+        cudaSetDevice(sys->device);
+        delete sys;
+    });
+}
+
+int cfdb_system_on_device(const cfdb_system* sys) { return sys != nullptr && sys->eng ? 1 : 0; }
+
+int cfdb_system_set_amg(cfdb_system* sys, const cfdb_amg_view* amg) {
+    return guarded([&] {
+        if (sys == nullptr || amg == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
+        if (amg->n_levels <= 0 || amg->levels == nullptr)
+            fail(CFDB_ERR_BAD_ARG, "DeviceSolver::set_amg: empty hierarchy");
+        sys->h = hierarchy_from(*amg, sys->pat.n, /*skip_a0=*/true);
+        sys->sweeps = amg->smooth_sweeps;
+        sys->weight = amg->jacobi_weight;
+        sys->dirty = true;
+        ensure_engine(sys);
+    });
+}
+
+int cfdb_system_setup_amg(cfdb_system* sys, const double* diag, const double* upper, const double* lower,
+                          const cfdb_amg_settings* settings) {
+    return guarded([&] {
+        if (sys == nullptr || diag == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
+        const LduPatternHost& p = sys->pat;
+        HostCsr a;
+        a.n_rows = a.n_cols = p.n;
+        a.rp = p.row_ptr;
+        a.ci = p.col;
+        a.va.assign(static_cast<size_t>(p.nnz()), 0.0);
+        for (int i = 0; i < p.n; ++i) a.va[p.diag_pos[i]] = diag[i];
+        for (int f = 0; f < p.n_faces; ++f) {
+            a.va[p.upper_pos[f]] = upper[f];
+            a.va[p.lower_pos[f]] = lower[f];
+        }
+        AmgSettings s;
+        if (settings != nullptr) {
+            s.theta = settings->strength_threshold;
+            s.max_levels = settings->max_levels;
+            s.coarse_size = settings->coarse_size;
+            s.sweeps = settings->smooth_sweeps;
+            s.weight = settings->jacobi_weight;
+        }
+        auto h = std::make_shared<Hierarchy>(amg_setup(a, s));
+        if (h->levels() <= 1) {
+            // ldu_matrix.cpp:358: a single-level hierarchy runs Jacobi CG instead of AMG
+            sys->h.reset();
+        } else {
+            sys->h = h;
+        }
+        sys->sweeps = s.sweeps;
+        sys->weight = s.weight;
+        sys->dirty = true;
+        ensure_engine(sys);
+    });
+}
+
+int cfdb_system_set_precision(cfdb_system* sys, int precision) {
+    return guarded([&] {
+        if (sys == nullptr) fail(CFDB_ERR_BAD_ARG, "null system");
+        if (precision != CFDB_PRECISION_FP64 && precision != CFDB_PRECISION_MIXED)
+            fail(CFDB_ERR_BAD_ARG, "unknown precision");
+        if (sys->precision != precision) {
+            sys->precision = precision;
+            sys->dirty = true;
+            ensure_engine(sys);
+        }
+    });
+}
+
+int cfdb_system_solve(cfdb_system* sys, const double* diag, const double* upper, const double* lower, const double* b,
+                      double* x, int method, int use_amg, const cfdb_control* control, cfdb_stats* stats) {
+    return guarded([&] {
+        if (sys == nullptr) fail(CFDB_ERR_BAD_ARG, "null system");
+        CFDB_CUDA(cudaSetDevice(sys->device));
+        put_stats(stats, run_single(sys, diag, upper, lower, b, x, method, use_amg, control, false));
+    });
+}
+
+int cfdb_system_solve_device(cfdb_system* sys, const double* diag, const double* upper, const double* lower,
+                             const double* b, double* x, int method, int use_amg, const cfdb_control* control,
+                             cfdb_stats* stats) {
+    return guarded([&] {
+        if (sys == nullptr) fail(CFDB_ERR_BAD_ARG, "null system");
+        CFDB_CUDA(cudaSetDevice(sys->device));
+        put_stats(stats, run_single(sys, diag, upper, lower, b, x, method, use_amg, control, true));
+    });
+}
+
+int cfdb_system_assemble_device(cfdb_system* sys, const double* flux, const double* gamma, const double* delta,
+                                double convection, double* upper, double* lower, double* diag, double* div) {
+    return guarded([&] {
+        if (sys == nullptr) fail(CFDB_ERR_BAD_ARG, "null system");
+        if (sys->d_cf_ptr == nullptr) fail(CFDB_ERR_BAD_ARG, "system was not created from mesh addressing");
+        if (!flux || !gamma || !delta || !upper || !lower || !diag || !div) fail(CFDB_ERR_BAD_ARG, "null array");
+        CFDB_CUDA(cudaSetDevice(sys->device));
+        ensure_engine(sys);
+        cudaStream_t st = sys->eng->stream();
+        const int n = sys->pat.n, nf = sys->pat.n_faces;
+        if (nf > 0) {
+            k_assemble_faces<<<(nf + 255) / 256, 256, 0, st>>>(nf, flux, gamma, delta, convection, upper, lower);
+        }
+        k_assemble_cells<<<(n + 255) / 256, 256, 0, st>>>(n, sys->d_cf_ptr, sys->d_cf_face, flux, gamma, delta,
+                                                          sys->d_owner, convection, diag, div);
+        CFDB_CUDA(cudaGetLastError());
+        CFDB_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+int cfdb_system_apply_amg(cfdb_system* sys, const double* r, double* z) {
+    return guarded([&] {
+        if (sys == nullptr || r == nullptr || z == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
+        if (!sys->h) fail(CFDB_ERR_NOT_READY, "apply_amg: no hierarchy installed");
+        CFDB_CUDA(cudaSetDevice(sys->device));
+        ensure_engine(sys);
+        const Mode mode = sys->precision == CFDB_PRECISION_MIXED ? Mode::AmgMixed : Mode::AmgFp64;
+        sys->eng->set_residual(0, r, false);
+        sys->eng->apply_vcycle(mode, {0});
+        sys->eng->get_precond(0, z, false, mode);
+    });
+}
+
+int cfdb_system_stream(const cfdb_system* sys, void** stream) {
+    if (sys == nullptr || stream == nullptr || !sys->eng) return set_error(CFDB_ERR_BAD_ARG, "null argument");
+    *stream = sys->eng->stream();
+    return CFDB_OK;
+}
+
+int cfdb_system_device_bytes(const cfdb_system* sys, size_t* bytes) {
+    if (sys == nullptr || bytes == nullptr) return set_error(CFDB_ERR_BAD_ARG, "null argument");
+    *bytes = (sys->eng ? sys->eng->device_bytes() : 0) + sys->asm_arena.bytes();
+    return CFDB_OK;
+}
+
+} // extern "C"

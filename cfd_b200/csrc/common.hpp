@@ -1,0 +1,98 @@
+// Shared host-side utilities of the cfdb library: error propagation to the C ABI, device
+// buffers and the host sparse-matrix type used for patterns and AMG hierarchies.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+namespace cfdb {
+
+// Error carrying a cfdb_status code; the C ABI converts it into a return value + message.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(int code, const std::string& msg);
+void check_cuda(cudaError_t e, const char* what);
+#define CFDB_CUDA(call) ::cfdb::check_cuda((call), #call)
+
+// Host CSR matrix (int32 indices, FP64 values).
+struct HostCsr {
+    int n_rows = 0;
+    int n_cols = 0;
+    std::vector<int> rp{0};
+    std::vector<int> ci;
+    std::vector<double> va;
+    [[nodiscard]] int nnz() const { return rp.empty() ? 0 : rp.back(); }
+    [[nodiscard]] bool empty() const { return n_rows == 0; }
+};
+
+// Owning device allocation (256-byte aligned by cudaMalloc).
+class DeviceBuffer {
+public:
+    DeviceBuffer() = default;
+    explicit DeviceBuffer(size_t bytes) { allocate(bytes); }
+    ~DeviceBuffer() { release(); }
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr_(o.ptr_), bytes_(o.bytes_) {
+        o.ptr_ = nullptr;
+        o.bytes_ = 0;
+    }
+    DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+        if (this != &o) {
+            release();
+            ptr_ = o.ptr_;
+            bytes_ = o.bytes_;
+            o.ptr_ = nullptr;
+            o.bytes_ = 0;
+        }
+        return *this;
+    }
+    void allocate(size_t bytes);
+    void release();
+    [[nodiscard]] void* get() const { return ptr_; }
+    template <class T> [[nodiscard]] T* as() const { return static_cast<T*>(ptr_); }
+    [[nodiscard]] size_t bytes() const { return bytes_; }
+
+private:
+    void* ptr_ = nullptr;
+    size_t bytes_ = 0;
+};
+
+// Device arrays are grouped in an arena per engine so their footprint can be reported.
+class DeviceArena {
+public:
+    template <class T> T* alloc(size_t count) {
+        bufs_.emplace_back(sizeof(T) * (count > 0 ? count : 1));
+        total_ += bufs_.back().bytes();
+        return bufs_.back().as<T>();
+    }
+    template <class T> T* upload(const std::vector<T>& h, cudaStream_t s) {
+        T* d = alloc<T>(h.size());
+        if (!h.empty()) {
+            CFDB_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
+        }
+        return d;
+    }
+    [[nodiscard]] size_t bytes() const { return total_; }
+    void clear() {
+        bufs_.clear();
+        total_ = 0;
+    }
+
+private:
+    std::vector<DeviceBuffer> bufs_;
+    size_t total_ = 0;
+};
+
+inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
+inline int ceil_div(int v, int m) { return (v + m - 1) / m; }
+
+} // namespace cfdb

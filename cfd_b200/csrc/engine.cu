@@ -1,0 +1,805 @@
+#include "engine.hpp"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace cfdb {
+
+namespace {
+
+constexpr int kTargetTiles = 148 * 8; // 148 SMs x 8 resident 256-thread CTAs
+
+// SELL-32 under construction on the host.
+struct SellBuild {
+    std::vector<int> slice{0};
+    std::vector<int> col;
+    std::vector<double> val;
+    std::vector<int> src;
+    bool with_src = false;
+};
+
+// Appends rows [0, n_rows) of a CSR block (n_pad >= n_rows, multiple of 32) whose first row has
+// global index row0. Column indices are shifted by col_off; padding slots read column pad_col
+// with value 0. src_of (optional): value-source index per CSR entry (shifted by src_off).
+void sell_append(SellBuild& sb, int n_rows, int n_pad, const int* rp, const int* ci,
+                 const double* va, const int* src_of, int col_off, int src_off, int pad_col) {
+    for (int s0 = 0; s0 < n_pad; s0 += 32) {
+        int width = 0;
+        for (int i = s0; i < s0 + 32 && i < n_rows; ++i) width = std::max(width, rp[i + 1] - rp[i]);
+        const int base = sb.slice.back();
+        const size_t slots = static_cast<size_t>(width) * 32;
+        sb.col.resize(base + slots, pad_col);
+        sb.val.resize(base + slots, 0.0);
+        if (sb.with_src) sb.src.resize(base + slots, -1);
+        for (int lane = 0; lane < 32; ++lane) {
+            const int i = s0 + lane;
+            if (i >= n_rows) continue;
+            const int len = rp[i + 1] - rp[i];
+            for (int k = 0; k < len; ++k) {
+                const size_t slot = base + static_cast<size_t>(k) * 32 + lane;
+                const int e = rp[i] + k;
+                sb.col[slot] = ci[e] + col_off;
+                sb.val[slot] = va != nullptr ? va[e] : 0.0;
+                if (sb.with_src) sb.src[slot] = src_of != nullptr ? src_of[e] + src_off : -1;
+            }
+        }
+        if (static_cast<long long>(base) + static_cast<long long>(slots) > INT_MAX) {
+            fail(1, "operator too large for 32-bit slot offsets");
+        }
+        sb.slice.push_back(base + static_cast<int>(slots));
+    }
+}
+
+std::vector<float> to_float(const std::vector<double>& v) {
+    std::vector<float> f(v.size());
+    for (size_t i = 0; i < v.size(); ++i) f[i] = static_cast<float>(v[i]);
+    return f;
+}
+
+// krylov_openmp.cpp:147-157 / krylov_cuda.cu:345-352: last nonzero diagonal entry, default 1.
+std::vector<double> inverse_diagonal(const HostCsr& a) {
+    std::vector<double> d(static_cast<size_t>(a.n_rows), 1.0);
+    for (int i = 0; i < a.n_rows; ++i)
+        for (int k = a.rp[i]; k < a.rp[i + 1]; ++k)
+            if (a.ci[k] == i && a.va[k] != 0.0) d[i] = 1.0 / a.va[k];
+    return d;
+}
+
+int grid_of(long long n) { return static_cast<int>(std::max<long long>(1, (n + 255) / 256)); }
+
+} // namespace
+
+Engine::Engine(int device) : device_(device) {
+    CFDB_CUDA(cudaSetDevice(device));
+    CFDB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    CFDB_CUDA(cudaMallocHost(&h_pinned_, 4 * sizeof(int)));
+}
+
+Engine::~Engine() {
+    cudaSetDevice(device_);
+    release_graphs();
+    if (stream_ != nullptr) {
+        cudaStreamSynchronize(stream_);
+        cudaStreamDestroy(stream_);
+    }
+    if (h_pinned_ != nullptr) cudaFreeHost(h_pinned_);
+    arena_.clear();
+}
+
+void Engine::release_graphs() {
+    for (auto& g : graphs_)
+        for (auto& e : g)
+            if (e != nullptr) {
+                cudaGraphExecDestroy(e);
+                e = nullptr;
+            }
+}
+
+int Engine::level_rows(int l) const { return l < n_levels_ ? lv_[l].n_rows : 0; }
+
+long long Engine::level_slots(int l) const { return l < n_levels_ ? lv_[l].a.slots : 0; }
+
+void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, bool need64,
+                   bool need32) {
+    CFDB_CUDA(cudaSetDevice(device_));
+    CFDB_CUDA(cudaStreamSynchronize(stream_));
+    release_graphs();
+    arena_.clear();
+    lv_.clear();
+    n_sys_ = static_cast<int>(systems.size());
+    if (n_sys_ == 0) fail(1, "engine: no systems");
+    if (sweeps < 0) fail(1, "engine: negative smoothing sweeps");
+    sweeps_ = sweeps;
+    weight_ = weight;
+    need64_ = need64;
+    need32_ = need32;
+    has_amg_ = true;
+    for (const auto& s : systems) {
+        if (!s.h) has_amg_ = false;
+        if (s.n <= 0) fail(1, "engine: empty system");
+    }
+    if (!has_amg_) {
+        for (auto& s : systems) s.h.reset();
+    }
+    std::vector<int> L(n_sys_);
+    for (int s = 0; s < n_sys_; ++s) L[s] = systems[s].h ? systems[s].h->levels() : 1;
+    perm_.resize(n_sys_);
+    std::iota(perm_.begin(), perm_.end(), 0);
+    std::stable_sort(perm_.begin(), perm_.end(), [&](int a, int b) { return L[a] > L[b]; });
+    rank_.assign(n_sys_, 0);
+    for (int k = 0; k < n_sys_; ++k) rank_[perm_[k]] = k;
+    n_levels_ = L[perm_[0]];
+    n_of_.resize(n_sys_);
+    for (int s = 0; s < n_sys_; ++s) n_of_[s] = systems[s].n;
+    auto rows_at = [&](int s, int l) { return l == 0 ? systems[s].n : systems[s].h->a[l].n_rows; };
+    for (int s = 0; s < n_sys_; ++s) {
+        if (systems[s].h && systems[s].h->a.size() > 0 && !systems[s].h->a[0].empty() &&
+            systems[s].h->a[0].n_rows != systems[s].n) {
+            fail(1, "engine: hierarchy level 0 does not match the system size");
+        }
+        if (systems[s].h) {
+            const auto& h = *systems[s].h;
+            for (int l = 0; l + 1 < h.levels(); ++l) {
+                const int nl = rows_at(s, l), nc = h.a[l + 1].n_rows;
+                if (h.p[l].n_rows != nl || h.p[l].n_cols != nc || h.r[l].n_rows != nc ||
+                    h.r[l].n_cols != nl) {
+                    fail(1, "engine: transfer operator sizes do not match level " + std::to_string(l));
+                }
+            }
+            if (h.n_c != rows_at(s, h.levels() - 1) ||
+                h.coarse_inverse.size() != static_cast<size_t>(h.n_c) * h.n_c) {
+                fail(1, "engine: coarse inverse size does not match the coarsest level");
+            }
+        }
+    }
+    // value-source offsets in batch order
+    vs_off_.assign(n_sys_, 0);
+    vs_total_ = 0;
+    for (int k = 0; k < n_sys_; ++k) {
+        vs_off_[perm_[k]] = vs_total_;
+        vs_total_ += systems[perm_[k]].vs_len;
+    }
+    // per-level offsets
+    std::vector<std::vector<int>> off(n_levels_, std::vector<int>(n_sys_, -1));
+    lv_.resize(n_levels_);
+    for (int l = 0; l < n_levels_; ++l) {
+        DevLevel& d = lv_[l];
+        int cursor = 0;
+        d.n_rows_nc = -1;
+        for (int k = 0; k < n_sys_; ++k) {
+            const int s = perm_[k];
+            if (L[s] <= l) continue;
+            if (L[s] - 1 == l && d.n_rows_nc < 0) d.n_rows_nc = cursor;
+            off[l][s] = cursor;
+            cursor += round_up(rows_at(s, l), 32);
+        }
+        d.n_rows = cursor;
+        if (d.n_rows_nc < 0) d.n_rows_nc = cursor;
+    }
+    off0_.resize(n_sys_);
+    for (int s = 0; s < n_sys_; ++s) off0_[s] = off[0][s];
+    cudaStream_t st = stream_;
+    // tiles
+    std::vector<int> sys_tile0(n_sys_ + 1, 0);
+    for (int l = 0; l < n_levels_; ++l) {
+        DevLevel& d = lv_[l];
+        const int base = std::max(256, round_up(ceil_div(std::max(d.n_rows, 1), kTargetTiles), 256));
+        std::vector<int> trow, tsys;
+        int nc_tiles = -1;
+        for (int k = 0; k < n_sys_; ++k) {
+            const int s = perm_[k];
+            if (L[s] <= l) continue;
+            if (L[s] - 1 == l && nc_tiles < 0) nc_tiles = static_cast<int>(tsys.size());
+            if (l == 0) sys_tile0[k] = static_cast<int>(tsys.size());
+            const int pad = round_up(rows_at(s, l), 32);
+            for (int r = 0; r < pad; r += base) {
+                trow.push_back(off[l][s] + r);
+                tsys.push_back(k);
+            }
+        }
+        if (l == 0) sys_tile0[n_sys_] = static_cast<int>(tsys.size());
+        trow.push_back(d.n_rows);
+        d.n_tiles = static_cast<int>(tsys.size());
+        d.n_tiles_nc = nc_tiles < 0 ? d.n_tiles : nc_tiles;
+        d.tiles.row = arena_.upload(trow, st);
+        d.tiles.sys = arena_.upload(tsys, st);
+    }
+    // level-0 operator (values filled per solve) + value maps
+    {
+        SellBuild sb;
+        sb.with_src = true;
+        std::vector<int> dsrc(static_cast<size_t>(lv_[0].n_rows), -1);
+        for (int k = 0; k < n_sys_; ++k) {
+            const int s = perm_[k];
+            const SystemSpec& sp = systems[s];
+            if (static_cast<int>(sp.src.size()) != sp.rp[sp.n] ||
+                static_cast<int>(sp.diag_src.size()) != sp.n) {
+                fail(1, "engine: level-0 value map size mismatch");
+            }
+            sell_append(sb, sp.n, round_up(sp.n, 32), sp.rp, sp.ci, nullptr, sp.src.data(), off[0][s],
+                        vs_off_[s], off[0][s]);
+            for (int i = 0; i < sp.n; ++i)
+                dsrc[off[0][s] + i] = sp.diag_src[i] >= 0 ? sp.diag_src[i] + vs_off_[s] : -1;
+        }
+        DevLevel& d = lv_[0];
+        d.a.n_slices = static_cast<int>(sb.slice.size()) - 1;
+        d.a.slots = sb.slice.back();
+        const int* dslice = arena_.upload(sb.slice, st);
+        const int* dcol = arena_.upload(sb.col, st);
+        d.a.s64 = {dslice, dcol, arena_.alloc<double>(d.a.slots)};
+        if (need32_) d.a.s32 = {dslice, dcol, arena_.alloc<float>(d.a.slots)};
+        src0_ = arena_.upload(sb.src, st);
+        diag_src0_ = arena_.upload(dsrc, st);
+        d.wd64 = arena_.alloc<double>(d.n_rows);
+        if (need32_) d.wd32 = arena_.alloc<float>(d.n_rows);
+        dinv0_ = arena_.alloc<double>(d.n_rows);
+    }
+    // coarser levels, transfers
+    for (int l = 0; l < n_levels_; ++l) {
+        DevLevel& d = lv_[l];
+        if (l > 0) {
+            SellBuild sb;
+            std::vector<double> wd(static_cast<size_t>(d.n_rows_nc), weight_);
+            for (int k = 0; k < n_sys_; ++k) {
+                const int s = perm_[k];
+                if (L[s] - 1 <= l) continue; // only systems with a coarser level need A_l here
+                const HostCsr& a = systems[s].h->a[l];
+                sell_append(sb, a.n_rows, round_up(a.n_rows, 32), a.rp.data(), a.ci.data(), a.va.data(),
+                            nullptr, off[l][s], 0, off[l][s]);
+                const std::vector<double> dinv = inverse_diagonal(a);
+                for (int i = 0; i < a.n_rows; ++i) wd[off[l][s] + i] = weight_ * dinv[i];
+            }
+            d.a.n_slices = static_cast<int>(sb.slice.size()) - 1;
+            d.a.slots = sb.slice.back();
+            const int* dslice = arena_.upload(sb.slice, st);
+            const int* dcol = arena_.upload(sb.col, st);
+            if (need64_) {
+                d.a.s64 = {dslice, dcol, arena_.upload(sb.val, st)};
+                d.wd64 = arena_.upload(wd, st);
+            }
+            if (need32_) {
+                d.a.s32 = {dslice, dcol, arena_.upload(to_float(sb.val), st)};
+                d.wd32 = arena_.upload(to_float(wd), st);
+            }
+        }
+        if (l + 1 < n_levels_) {
+            SellBuild sp, sr;
+            for (int k = 0; k < n_sys_; ++k) {
+                const int s = perm_[k];
+                if (L[s] - 1 <= l) continue;
+                const HostCsr& p = systems[s].h->p[l];
+                const HostCsr& r = systems[s].h->r[l];
+                sell_append(sp, p.n_rows, round_up(p.n_rows, 32), p.rp.data(), p.ci.data(), p.va.data(),
+                            nullptr, off[l + 1][s], 0, off[l + 1][s]);
+                sell_append(sr, r.n_rows, round_up(r.n_rows, 32), r.rp.data(), r.ci.data(), r.va.data(),
+                            nullptr, off[l][s], 0, off[l][s]);
+            }
+            auto up = [&](SellBuild& b, DevSell64_32& m) {
+                m.n_slices = static_cast<int>(b.slice.size()) - 1;
+                m.slots = b.slice.back();
+                const int* ds = arena_.upload(b.slice, st);
+                const int* dc = arena_.upload(b.col, st);
+                if (need64_) m.s64 = {ds, dc, arena_.upload(b.val, st)};
+                if (need32_) m.s32 = {ds, dc, arena_.upload(to_float(b.val), st)};
+            };
+            up(sp, d.p);
+            up(sr, d.r);
+        }
+        // vectors (zero-initialised)
+        auto vec64 = [&](int n) {
+            double* p = arena_.alloc<double>(n);
+            CFDB_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * std::max(n, 1), st));
+            return p;
+        };
+        auto vec32 = [&](int n) {
+            float* p = arena_.alloc<float>(n);
+            CFDB_CUDA(cudaMemsetAsync(p, 0, sizeof(float) * std::max(n, 1), st));
+            return p;
+        };
+        if (need64_ || l == 0) {
+            d.x64 = vec64(d.n_rows);
+            d.y64 = vec64(d.n_rows);
+            d.t64 = vec64(d.n_rows);
+            if (l > 0) d.b64 = vec64(d.n_rows);
+        }
+        if (need32_) {
+            d.x32 = vec32(d.n_rows);
+            d.y32 = vec32(d.n_rows);
+            d.t32 = vec32(d.n_rows);
+            if (l > 0) d.b32 = vec32(d.n_rows);
+        }
+    }
+    // Krylov vectors and state
+    {
+        const int n0 = lv_[0].n_rows;
+        auto vec64 = [&](int n) {
+            double* p = arena_.alloc<double>(n);
+            CFDB_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * std::max(n, 1), st));
+            return p;
+        };
+        b_ = vec64(n0);
+        x_ = vec64(n0);
+        r_ = vec64(n0);
+        p_ = vec64(n0);
+        q_ = vec64(n0);
+        vs_ = arena_.alloc<double>(std::max(vs_total_, 1));
+        st_ = arena_.alloc<SysState>(n_sys_);
+        CFDB_CUDA(cudaMemsetAsync(st_, 0, sizeof(SysState) * n_sys_, st));
+        partials_ = arena_.alloc<double>(2 * static_cast<size_t>(lv_[0].n_tiles));
+        counters_ = arena_.alloc<int>(n_sys_);
+        CFDB_CUDA(cudaMemsetAsync(counters_, 0, sizeof(int) * n_sys_, st));
+        sys_tile0_ = arena_.upload(sys_tile0, st);
+        n_active_ = arena_.alloc<int>(1);
+        error_ = arena_.alloc<int>(1);
+        CFDB_CUDA(cudaMemsetAsync(error_, 0, sizeof(int), st));
+    }
+    // coarse blocks
+    n_blocks_ = 0;
+    fused_final_ = has_amg_ && sweeps_ > 0;
+    if (has_amg_) {
+        std::vector<int> bsys, brow, bn, blevel;
+        std::vector<long long> moff;
+        std::vector<double> mt;
+        size_t max_n = 0;
+        for (int k = 0; k < n_sys_; ++k) {
+            const int s = perm_[k];
+            const Hierarchy& h = *systems[s].h;
+            const int c = h.levels() - 1;
+            if (c == 0) fused_final_ = false;
+            const int n = h.n_c;
+            bsys.push_back(k);
+            brow.push_back(off[c][s]);
+            bn.push_back(n);
+            blevel.push_back(c);
+            moff.push_back(static_cast<long long>(mt.size()));
+            const size_t o = mt.size();
+            mt.resize(o + static_cast<size_t>(n) * n);
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j)
+                    mt[o + static_cast<size_t>(j) * n + i] = h.coarse_inverse[static_cast<size_t>(i) * n + j];
+            max_n = std::max(max_n, static_cast<size_t>(round_up(n, 32)));
+        }
+        n_blocks_ = static_cast<int>(bsys.size());
+        n_single_ = 0;
+        for (int k = 0; k < n_sys_; ++k)
+            if (systems[perm_[k]].h->levels() == 1) ++n_single_;
+        cb_.sys = arena_.upload(bsys, st);
+        cb_.row = arena_.upload(brow, st);
+        cb_.n = arena_.upload(bn, st);
+        cb_.m_off = arena_.upload(moff, st);
+        cb_.mt = arena_.upload(mt, st);
+        block_level_ = arena_.upload(blevel, st);
+        coarse_smem64_ = max_n * sizeof(double);
+        coarse_smem32_ = max_n * sizeof(float);
+        if (coarse_smem64_ > 200 * 1024) fail(1, "coarsest level too large for the dense solve (> 25600 rows)");
+        std::vector<double*> bl64(n_levels_), xl64(n_levels_);
+        std::vector<float*> bl32(n_levels_), xl32(n_levels_);
+        for (int l = 0; l < n_levels_; ++l) {
+            bl64[l] = l == 0 ? r_ : lv_[l].b64;
+            xl64[l] = lv_[l].x64;
+            bl32[l] = lv_[l].b32; // level 0 (single-level systems) handled by the FP64 kernel
+            xl32[l] = lv_[l].x32;
+        }
+        b_level64_ = arena_.upload(bl64, st);
+        x_level64_ = arena_.upload(xl64, st);
+        b_level32_ = arena_.upload(bl32, st);
+        x_level32_ = arena_.upload(xl32, st);
+        if (coarse_smem64_ > 48 * 1024) {
+            CFDB_CUDA(cudaFuncSetAttribute(k_vc_coarse<double, double>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(coarse_smem64_)));
+            CFDB_CUDA(cudaFuncSetAttribute(k_vc_coarse<double, float>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(coarse_smem64_)));
+            CFDB_CUDA(cudaFuncSetAttribute(k_vc_coarse<float, float>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(coarse_smem32_)));
+        }
+    }
+    CFDB_CUDA(cudaStreamSynchronize(st));
+}
+
+void Engine::set_values_device(const double* p0, const double* p1, const double* p2, int n1, int n2) {
+    const DevLevel& d = lv_[0];
+    ValueSource vs{p0, p1, p2, n1, n2};
+    const long long n = std::max<long long>(d.a.slots, d.n_rows);
+    k_fill_level0<<<grid_of(n), 256, 0, stream_>>>(static_cast<int>(d.a.slots), d.n_rows, src0_, diag_src0_, vs,
+                                                   weight_, d.a.s64.val ? const_cast<double*>(d.a.s64.val) : nullptr,
+                                                   d.a.s32.val ? const_cast<float*>(d.a.s32.val) : nullptr, d.wd64,
+                                                   d.wd32);
+    // plain inverse diagonal for Jacobi preconditioning: weight 1
+    k_fill_level0<<<grid_of(d.n_rows), 256, 0, stream_>>>(0, d.n_rows, src0_, diag_src0_, vs, 1.0, nullptr,
+                                                          nullptr, dinv0_, nullptr);
+    CFDB_CUDA(cudaGetLastError());
+}
+
+void Engine::upload_values(const std::vector<const double*>& host_src) {
+    // host_src[s]: the value source of original system s
+    std::vector<int> lens(n_sys_);
+    for (int k = 0; k < n_sys_; ++k) {
+        const int s = perm_[k];
+        const int next = k + 1 < n_sys_ ? vs_off_[perm_[k + 1]] : vs_total_;
+        lens[s] = next - vs_off_[s];
+    }
+    for (int s = 0; s < n_sys_; ++s) {
+        if (lens[s] > 0) {
+            CFDB_CUDA(cudaMemcpyAsync(vs_ + vs_off_[s], host_src[s], sizeof(double) * lens[s],
+                                      cudaMemcpyHostToDevice, stream_));
+        }
+    }
+    set_values_device(vs_, vs_, vs_, INT_MAX, INT_MAX);
+}
+
+void Engine::upload_values_device_concat(const std::vector<const double*>& dev_src) {
+    std::vector<int> lens(n_sys_);
+    for (int k = 0; k < n_sys_; ++k) {
+        const int s = perm_[k];
+        const int next = k + 1 < n_sys_ ? vs_off_[perm_[k + 1]] : vs_total_;
+        lens[s] = next - vs_off_[s];
+    }
+    for (int s = 0; s < n_sys_; ++s) {
+        if (lens[s] > 0) {
+            CFDB_CUDA(cudaMemcpyAsync(vs_ + vs_off_[s], dev_src[s], sizeof(double) * lens[s],
+                                      cudaMemcpyDeviceToDevice, stream_));
+        }
+    }
+    set_values_device(vs_, vs_, vs_, INT_MAX, INT_MAX);
+}
+
+void Engine::set_rhs(int s, const double* b, bool dev) {
+    CFDB_CUDA(cudaMemcpyAsync(b_ + off0_[s], b, sizeof(double) * n_of_[s],
+                              dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
+}
+
+void Engine::set_guess(int s, const double* x, bool dev) {
+    CFDB_CUDA(cudaMemcpyAsync(x_ + off0_[s], x, sizeof(double) * n_of_[s],
+                              dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
+}
+
+void Engine::get_solution(int s, double* x, bool dev) {
+    CFDB_CUDA(cudaMemcpyAsync(x, x_ + off0_[s], sizeof(double) * n_of_[s],
+                              dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream_));
+    if (!dev) CFDB_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Engine::set_residual(int s, const double* r, bool dev) {
+    CFDB_CUDA(cudaMemcpyAsync(r_ + off0_[s], r, sizeof(double) * n_of_[s],
+                              dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
+}
+
+void Engine::get_precond(int s, double* z, bool dev, Mode mode) {
+    CFDB_CUDA(cudaStreamSynchronize(stream_));
+    const int n = n_of_[s];
+    if (mode == Mode::AmgMixed) {
+        std::vector<float> tmp(n);
+        CFDB_CUDA(cudaMemcpy(tmp.data(), lv_[0].x32 + off0_[s], sizeof(float) * n, cudaMemcpyDeviceToHost));
+        if (dev) fail(1, "get_precond: device output not supported for FP32");
+        for (int i = 0; i < n; ++i) z[i] = tmp[i];
+    } else {
+        CFDB_CUDA(cudaMemcpy(z, lv_[0].x64 + off0_[s], sizeof(double) * n,
+                             dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost));
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// V-cycle enqueue
+// ---------------------------------------------------------------------------------------------
+
+namespace {
+template <class T> T* vx(double* a, float* b);
+template <> double* vx<double>(double* a, float*) { return a; }
+template <> float* vx<float>(double*, float* b) { return b; }
+template <class T> Sell<T> vs_sel(const Sell<double>& a, const Sell<float>& b);
+template <> Sell<double> vs_sel<double>(const Sell<double>& a, const Sell<float>&) { return a; }
+template <> Sell<float> vs_sel<float>(const Sell<double>&, const Sell<float>& b) { return b; }
+} // namespace
+
+template <class T>
+void Engine::enqueue_vcycle_t(bool fused_final, int flexible) {
+    cudaStream_t s = stream_;
+    const SysState* stv = st_;
+    const int L = n_levels_;
+    // final pre-smoothing buffer so that after `sweeps_` post sweeps the iterate lands in x
+    const int writes_pre = sweeps_ >= 2 ? sweeps_ - 1 : sweeps_;
+    auto X = [&](int l) { return vx<T>(lv_[l].x64, lv_[l].x32); };
+    auto Y = [&](int l) { return vx<T>(lv_[l].y64, lv_[l].y32); };
+    auto Tv = [&](int l) { return vx<T>(lv_[l].t64, lv_[l].t32); };
+    auto Bv = [&](int l) { return vx<T>(lv_[l].b64, lv_[l].b32); };
+    auto WD = [&](int l) -> const T* {
+        if constexpr (sizeof(T) == 8) return lv_[l].wd64;
+        else return lv_[l].wd32;
+    };
+    auto A = [&](int l) { return vs_sel<T>(lv_[l].a.s64, lv_[l].a.s32); };
+    auto P = [&](int l) { return vs_sel<T>(lv_[l].p.s64, lv_[l].p.s32); };
+    auto R = [&](int l) { return vs_sel<T>(lv_[l].r.s64, lv_[l].r.s32); };
+
+    std::vector<T*> cur(L, nullptr);
+    // ---- down ----
+    for (int l = 0; l + 1 < L; ++l) {
+        const DevLevel& d = lv_[l];
+        const int g = d.n_tiles_nc;
+        if (g == 0) continue;
+        T* x = X(l);
+        T* y = Y(l);
+        T* target = (sweeps_ % 2 == 0) ? x : y;
+        T* start = (writes_pre % 2 == 1) ? target : (target == x ? y : x);
+        if (sweeps_ == 0) {
+            CFDB_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * d.n_rows_nc, s));
+            cur[l] = x;
+        } else {
+            if (l == 0) {
+                k_vc_first<T, double><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, WD(l), r_, start, sweeps_ >= 2);
+            } else {
+                k_vc_first<T, T><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, WD(l), Bv(l), start, sweeps_ >= 2);
+            }
+            T* c = start;
+            for (int k = 2; k < sweeps_; ++k) {
+                T* o = c == x ? y : x;
+                if (l == 0) k_vc_jacobi<T, double><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, WD(l), r_, c, o);
+                else k_vc_jacobi<T, T><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, WD(l), Bv(l), c, o);
+                c = o;
+            }
+            cur[l] = c;
+        }
+        if (l == 0) k_vc_residual<T, double><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, r_, cur[l], Tv(l));
+        else k_vc_residual<T, T><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, Bv(l), cur[l], Tv(l));
+        const DevLevel& nx = lv_[l + 1];
+        k_vc_spmv<T><<<nx.n_tiles, kBlock, 0, s>>>(R(l), nx.tiles, stv, Tv(l), Bv(l + 1));
+    }
+    // ---- coarsest blocks ----
+    // Systems are in descending level count, so single-level systems (coarsest level 0, whose
+    // right-hand side is the FP64 Krylov residual) form the last n_single_ blocks.
+    const int first0 = n_blocks_ - n_single_;
+    const Control ctl{n_active_, error_};
+    if (first0 > 0) {
+        if constexpr (sizeof(T) == 8) {
+            k_vc_coarse<double, double><<<first0, kBlock, coarse_smem64_, s>>>(cb_, stv, b_level64_, x_level64_,
+                                                                               block_level_, ctl);
+        } else {
+            k_vc_coarse<float, float><<<first0, kBlock, coarse_smem32_, s>>>(cb_, stv, b_level32_, x_level32_,
+                                                                             block_level_, ctl);
+        }
+    }
+    if (first0 < n_blocks_) {
+        CoarseBlocks tail = cb_;
+        tail.sys += first0;
+        tail.row += first0;
+        tail.n += first0;
+        tail.m_off += first0;
+        if constexpr (sizeof(T) == 8) {
+            k_vc_coarse<double, double><<<n_blocks_ - first0, kBlock, coarse_smem64_, s>>>(
+                tail, stv, b_level64_, x_level64_, block_level_ + first0, ctl);
+        } else {
+            k_vc_coarse<double, float><<<n_blocks_ - first0, kBlock, coarse_smem64_, s>>>(
+                tail, stv, b_level64_, x_level32_, block_level_ + first0, ctl);
+        }
+    }
+    // ---- up ----
+    for (int l = L - 2; l >= 0; --l) {
+        const DevLevel& d = lv_[l];
+        const int g = d.n_tiles_nc;
+        if (g == 0) continue;
+        T* x = X(l);
+        T* y = Y(l);
+        T* c = cur[l];
+        k_vc_prolong<T><<<g, kBlock, 0, s>>>(P(l), d.tiles, stv, X(l + 1), c);
+        for (int k = 0; k < sweeps_; ++k) {
+            T* o = c == x ? y : x;
+            const bool last = k + 1 == sweeps_;
+            if (l == 0 && last && fused_final) {
+                k_vc_jacobi_final<T><<<g, kBlock, 0, s>>>(A(0), d.tiles, st_, WD(0), r_, c, o, q_, partials_,
+                                                          counters_, sys_tile0_, Control{n_active_, error_},
+                                                          flexible);
+            } else if (l == 0) {
+                k_vc_jacobi<T, double><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, WD(l), r_, c, o);
+            } else {
+                k_vc_jacobi<T, T><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, WD(l), Bv(l), c, o);
+            }
+            c = o;
+        }
+    }
+}
+
+void Engine::enqueue_vcycle(Mode mode, bool fused_final, int flexible) {
+    if (mode == Mode::AmgMixed) enqueue_vcycle_t<float>(fused_final, flexible);
+    else enqueue_vcycle_t<double>(fused_final, flexible);
+}
+
+// Preconditioner output z (level-0 iterate) in the precision of the mode.
+void Engine::enqueue_init(Mode mode) {
+    const DevLevel& d = lv_[0];
+    const Control ctl{n_active_, error_};
+    k_cg_init<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, r_, partials_, counters_,
+                                                  sys_tile0_, ctl);
+    const int flexible = mode == Mode::AmgMixed ? 1 : 0;
+    if (mode == Mode::Jacobi) {
+        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, q_, partials_,
+                                                           counters_, sys_tile0_, ctl, 0);
+        return;
+    }
+    enqueue_vcycle(mode, fused_final_, flexible);
+    if (!fused_final_) {
+        if (mode == Mode::AmgMixed) {
+            k_cg_rz<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x32, nullptr, q_, partials_,
+                                                              counters_, sys_tile0_, ctl, flexible);
+        } else {
+            k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, nullptr, q_, partials_,
+                                                               counters_, sys_tile0_, ctl, flexible);
+        }
+    }
+}
+
+void Engine::enqueue_iteration(Mode mode) {
+    const DevLevel& d = lv_[0];
+    const Control ctl{n_active_, error_};
+    if (mode == Mode::AmgMixed) {
+        k_cg_pupdate<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, d.x32, p_);
+    } else {
+        k_cg_pupdate<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, d.x64, p_);
+    }
+    k_cg_spmv_pq<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, p_, q_, partials_, counters_,
+                                                     sys_tile0_, ctl);
+    k_cg_xr<<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, x_, r_, p_, q_, partials_, counters_, sys_tile0_,
+                                                ctl, mode == Mode::AmgMixed ? 1 : 0);
+    if (mode == Mode::AmgMixed) {
+        k_cg_true_check<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, r_, partials_,
+                                                            counters_, sys_tile0_, ctl);
+    }
+    const int flexible = mode == Mode::AmgMixed ? 1 : 0;
+    if (mode == Mode::Jacobi) {
+        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, q_, partials_,
+                                                           counters_, sys_tile0_, ctl, 0);
+        return;
+    }
+    enqueue_vcycle(mode, fused_final_, flexible);
+    if (!fused_final_) {
+        if (mode == Mode::AmgMixed) {
+            k_cg_rz<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x32, nullptr, q_, partials_,
+                                                              counters_, sys_tile0_, ctl, flexible);
+        } else {
+            k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, nullptr, q_, partials_,
+                                                               counters_, sys_tile0_, ctl, flexible);
+        }
+    }
+}
+
+void Engine::capture_graphs(Mode mode) {
+    const int m = static_cast<int>(mode);
+    if (graphs_[m][0] != nullptr) return;
+    for (int which = 0; which < 2; ++which) {
+        cudaGraph_t g = nullptr;
+        CFDB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        try {
+            if (which == 0) enqueue_init(mode);
+            else enqueue_iteration(mode);
+        } catch (...) {
+            cudaStreamEndCapture(stream_, &g);
+            if (g != nullptr) cudaGraphDestroy(g);
+            throw;
+        }
+        CFDB_CUDA(cudaStreamEndCapture(stream_, &g));
+        cudaGraphExec_t e = nullptr;
+        const cudaError_t err = cudaGraphInstantiate(&e, g, 0);
+        cudaGraphDestroy(g);
+        CFDB_CUDA(err);
+        graphs_[m][which] = e;
+    }
+}
+
+std::vector<SolveResult> Engine::solve(Mode mode, const std::vector<SolveRequest>& req) {
+    CFDB_CUDA(cudaSetDevice(device_));
+    if (static_cast<int>(req.size()) != n_sys_) fail(1, "solve: one request per system expected");
+    if (mode != Mode::Jacobi && !has_amg_) fail(5, "solve: no AMG hierarchy set");
+    if (mode == Mode::AmgMixed && !need32_) fail(5, "solve: mixed precision needs the FP32 hierarchy");
+    if (mode == Mode::AmgFp64 && !need64_) fail(5, "solve: FP64 AMG needs the FP64 hierarchy");
+    std::vector<SysState> hs(n_sys_);
+    int max_it = 0;
+    for (int s = 0; s < n_sys_; ++s) {
+        SysState& t = hs[rank_[s]];
+        std::memset(&t, 0, sizeof(t));
+        t.tol = req[s].tol;
+        t.max_it = req[s].max_it;
+        t.active = 1;
+        t.first = 1;
+        max_it = std::max(max_it, req[s].max_it);
+    }
+    capture_graphs(mode);
+    CFDB_CUDA(cudaMemcpyAsync(st_, hs.data(), sizeof(SysState) * n_sys_, cudaMemcpyHostToDevice, stream_));
+    const int n_act = n_sys_;
+    CFDB_CUDA(cudaMemcpyAsync(n_active_, &n_act, sizeof(int), cudaMemcpyHostToDevice, stream_));
+    CFDB_CUDA(cudaGraphLaunch(graphs_[static_cast<int>(mode)][0], stream_));
+    // Iterations: keep one graph launch in flight ahead of the convergence readback.
+    cudaEvent_t ev[2];
+    CFDB_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    CFDB_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    volatile int* flag = h_pinned_;
+    int launched = 0;
+    bool done = false;
+    const int cap = max_it + 2;
+    while (!done && launched < cap) {
+        CFDB_CUDA(cudaGraphLaunch(graphs_[static_cast<int>(mode)][1], stream_));
+        CFDB_CUDA(cudaMemcpyAsync(h_pinned_ + 2 * (launched & 1), n_active_, sizeof(int), cudaMemcpyDeviceToHost,
+                                  stream_));
+        CFDB_CUDA(cudaMemcpyAsync(h_pinned_ + 2 * (launched & 1) + 1, error_, sizeof(int), cudaMemcpyDeviceToHost,
+                                  stream_));
+        CFDB_CUDA(cudaEventRecord(ev[launched & 1], stream_));
+        ++launched;
+        if (launched >= 2) {
+            const int prev = (launched - 2) & 1;
+            CFDB_CUDA(cudaEventSynchronize(ev[prev]));
+            if (flag[2 * prev] <= 0 || flag[2 * prev + 1] != 0) done = true;
+        }
+    }
+    CFDB_CUDA(cudaStreamSynchronize(stream_));
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    int err = 0;
+    CFDB_CUDA(cudaMemcpy(&err, error_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err != 0) {
+        CFDB_CUDA(cudaMemset(error_, 0, sizeof(int)));
+        fail(6, "solve: a bounded device wait expired (coarse-level staging)");
+    }
+    // true residual for reporting
+    const DevLevel& d = lv_[0];
+    k_true_residual<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, partials_, counters_,
+                                                        sys_tile0_);
+    CFDB_CUDA(cudaGetLastError());
+    CFDB_CUDA(cudaMemcpyAsync(hs.data(), st_, sizeof(SysState) * n_sys_, cudaMemcpyDeviceToHost, stream_));
+    CFDB_CUDA(cudaStreamSynchronize(stream_));
+    std::vector<SolveResult> out(n_sys_);
+    for (int s = 0; s < n_sys_; ++s) {
+        const SysState& t = hs[rank_[s]];
+        SolveResult& o = out[s];
+        o.iterations = t.active ? t.max_it : t.iters_out;
+        o.residual = t.res;
+        o.converged = t.converged != 0;
+        o.true_residual = t.true_res;
+    }
+    return out;
+}
+
+void Engine::apply_vcycle(Mode mode, const std::vector<int>&) {
+    if (!has_amg_) fail(5, "apply_vcycle: no hierarchy");
+    // run with all systems treated as active (state pointer null) and no Krylov bookkeeping
+    SysState* keep = st_;
+    st_ = nullptr;
+    try {
+        if (mode == Mode::AmgMixed) enqueue_vcycle_t<float>(false, 0);
+        else enqueue_vcycle_t<double>(false, 0);
+    } catch (...) {
+        st_ = keep;
+        throw;
+    }
+    st_ = keep;
+    CFDB_CUDA(cudaGetLastError());
+    CFDB_CUDA(cudaStreamSynchronize(stream_));
+}
+
+double Engine::time_level0_sweep(bool fp32, int reps) {
+    const DevLevel& d = lv_[0];
+    cudaEvent_t a, b;
+    CFDB_CUDA(cudaEventCreate(&a));
+    CFDB_CUDA(cudaEventCreate(&b));
+    CFDB_CUDA(cudaEventRecord(a, stream_));
+    for (int i = 0; i < reps; ++i) {
+        if (fp32) {
+            k_vc_jacobi<float, double><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s32, d.tiles, nullptr, d.wd32, r_,
+                                                                         d.x32, d.y32);
+        } else {
+            k_vc_jacobi<double, double><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, nullptr, d.wd64, r_,
+                                                                          d.x64, d.y64);
+        }
+    }
+    CFDB_CUDA(cudaEventRecord(b, stream_));
+    CFDB_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CFDB_CUDA(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms / reps;
+}
+
+} // namespace cfdb

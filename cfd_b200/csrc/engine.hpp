@@ -1,0 +1,161 @@
+// Solver engine: one plan over a batch of independent pressure systems (a single solve is a
+// batch of one). Owns the device hierarchy in SELL-32, the Krylov vectors, per-system state
+// and the captured CUDA graphs of the iteration.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "common.hpp"
+#include "host_algos.hpp"
+#include "kernels.cuh"
+
+namespace cfdb {
+
+enum class Mode { AmgFp64 = 0, AmgMixed = 1, Jacobi = 2 };
+
+struct SystemSpec {
+    int n = 0;                        // level-0 rows
+    const int* rp = nullptr;          // level-0 CSR pattern (host, sorted columns)
+    const int* ci = nullptr;
+    std::vector<int> src;             // per pattern entry: index into this system's value source
+    std::vector<int> diag_src;        // per row: value-source index of the diagonal, or -1
+    int vs_len = 0;                   // length of this system's value source
+    std::shared_ptr<const Hierarchy> h; // levels >= 1, transfers, coarse inverse (null: none)
+};
+
+struct SolveRequest {
+    double tol = 1e-10;
+    int max_it = 1000;
+};
+
+struct SolveResult {
+    int iterations = 0;
+    double residual = 0.0;
+    bool converged = false;
+    double true_residual = 0.0;
+};
+
+class Engine {
+public:
+    explicit Engine(int device);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    // Builds the device plan. need64 / need32: keep FP64 / FP32 copies of the V-cycle levels.
+    void build(std::vector<SystemSpec> systems, int sweeps, double weight, bool need64,
+               bool need32);
+    [[nodiscard]] bool built() const { return n_sys_ > 0; }
+    [[nodiscard]] int n_systems() const { return n_sys_; }
+    [[nodiscard]] bool has_amg() const { return has_amg_; }
+    [[nodiscard]] bool has32() const { return need32_; }
+    [[nodiscard]] bool has64() const { return need64_; }
+    [[nodiscard]] size_t device_bytes() const { return arena_.bytes(); }
+    [[nodiscard]] cudaStream_t stream() const { return stream_; }
+    [[nodiscard]] int device() const { return device_; }
+    [[nodiscard]] int levels() const { return n_levels_; }
+    [[nodiscard]] int level_rows(int l) const;
+    [[nodiscard]] long long level_slots(int l) const;
+
+    // Level-0 values from a value source. For one system: three device arrays (diag, upper,
+    // lower) addressed by the source indices [0,n1) [n1,n2) [n2,..). upload_values copies a host
+    // value source (concatenated per system in batch order) first.
+    void set_values_device(const double* p0, const double* p1, const double* p2, int n1, int n2);
+    void upload_values(const std::vector<const double*>& host_src);
+    void upload_values_device_concat(const std::vector<const double*>& dev_src);
+
+    // Right-hand side / initial guess of system s (original batch index), host or device.
+    void set_rhs(int s, const double* b, bool device_ptr);
+    void set_guess(int s, const double* x, bool device_ptr);
+    void get_solution(int s, double* x, bool device_ptr);
+
+    // Runs the solve for all systems on the engine stream; blocks until done.
+    std::vector<SolveResult> solve(Mode mode, const std::vector<SolveRequest>& req);
+
+    // Launch the pieces of one V-cycle application z = M^-1 r for system-batch inputs that are
+    // already in the level-0 residual vector (used by the parity tests).
+    void apply_vcycle(Mode mode, const std::vector<int>& sys_rhs_ready);
+    void set_residual(int s, const double* r, bool device_ptr);
+    void get_precond(int s, double* z, bool device_ptr, Mode mode);
+
+    // Kernel timing probe: average device time (ms) of the level-0 FP64/FP32 smoother sweep.
+    double time_level0_sweep(bool fp32, int reps);
+
+private:
+    struct DevSell64_32 {
+        Sell<double> s64{};
+        Sell<float> s32{};
+        int n_slices = 0;
+        long long slots = 0;
+    };
+    struct DevLevel {
+        int n_rows = 0;     // all present systems (padded)
+        int n_rows_nc = 0;  // prefix of systems that continue to a coarser level
+        int n_tiles = 0;
+        int n_tiles_nc = 0;
+        Tiles tiles{};
+        DevSell64_32 a, p, r;
+        double* wd64 = nullptr;
+        float* wd32 = nullptr;
+        double *x64 = nullptr, *y64 = nullptr, *t64 = nullptr, *b64 = nullptr;
+        float *x32 = nullptr, *y32 = nullptr, *t32 = nullptr, *b32 = nullptr;
+        int final_in_y = 0; // after post-smoothing the iterate lives in y
+    };
+
+    void capture_graphs(Mode mode);
+    void enqueue_vcycle(Mode mode, bool fused_final, int flexible);
+    template <class T> void enqueue_vcycle_t(bool fused_final, int flexible);
+    void enqueue_init(Mode mode);
+    void enqueue_iteration(Mode mode);
+    void release_graphs();
+
+    int device_;
+    cudaStream_t stream_ = nullptr;
+    DeviceArena arena_;
+    int n_sys_ = 0;
+    int n_levels_ = 0;
+    int sweeps_ = 2;
+    double weight_ = 0.7;
+    bool need64_ = true;
+    bool need32_ = false;
+    bool has_amg_ = false;
+    bool fused_final_ = true;
+
+    // batch order: perm_[k] = original index of the k-th system (sorted by level count)
+    std::vector<int> perm_, rank_;
+    std::vector<int> n_of_;          // level-0 rows per original system
+    std::vector<int> off0_;          // level-0 row offset per original system
+    std::vector<int> vs_off_;        // value-source offset per original system (batch order)
+    int vs_total_ = 0;
+    std::vector<DevLevel> lv_;
+    // level-0 value map
+    int* src0_ = nullptr;
+    int* diag_src0_ = nullptr;
+    double* vs_ = nullptr;
+    double* dinv0_ = nullptr;
+    // Krylov vectors (level 0)
+    double *b_ = nullptr, *x_ = nullptr, *r_ = nullptr, *p_ = nullptr, *q_ = nullptr;
+    // state
+    SysState* st_ = nullptr;
+    double* partials_ = nullptr;
+    int* counters_ = nullptr;
+    int* sys_tile0_ = nullptr;
+    int* n_active_ = nullptr;
+    int* error_ = nullptr;
+    int* h_pinned_ = nullptr; // [0] n_active, [1] error
+    // coarse blocks
+    int n_blocks_ = 0;
+    int n_single_ = 0; // systems whose hierarchy has one level (dense solve on level 0)
+    CoarseBlocks cb_{};
+    int* block_level_ = nullptr;
+    double** b_level64_ = nullptr;
+    double** x_level64_ = nullptr;
+    float** b_level32_ = nullptr;
+    float** x_level32_ = nullptr;
+    size_t coarse_smem64_ = 0, coarse_smem32_ = 0;
+    // graphs per mode: [mode][0] init, [mode][1] iteration
+    cudaGraphExec_t graphs_[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+};
+
+} // namespace cfdb

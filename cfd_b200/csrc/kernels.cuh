@@ -1,0 +1,676 @@
+// Device kernels of the pressure solve (sm_100a).
+//
+// Layout: every sparse operator (level operators A_l, prolongations P_l, restrictions R_l) is
+// stored in SELL-32: rows in slices of 32, a slice's entries column-major (slot = base + k*32 +
+// lane), so a warp reads 32 consecutive values and 32 consecutive column indices per step.
+// Within a row, entries keep the CSR column order, so every row sum is accumulated in exactly
+// the order of the reference's CSR SpMV (krylov_cuda.cu:24-34 / krylov_kernels.inc:12-24).
+// The FP64 kernels are compiled without FMA contraction: every product and sum is rounded as
+// in the reference's host path, so V-cycles are bit-reproducible against the CPU oracle.
+//
+// Work decomposition: each level's rows are concatenated over the systems of a batch (a single
+// solve is a batch of one), each system's block padded to a multiple of 32 rows. A tile is a
+// run of whole slices of ONE system; one CTA of 256 threads processes one tile. Tiles carry
+// their system id so converged systems are skipped and reductions stay per system.
+//
+// Reductions (CG dot products) are deterministic: each tile writes its partial sums, the last
+// CTA of a system to finish (atomic ticket) adds that system's partials in a fixed order and
+// runs the scalar part of the Krylov step (alpha, beta, convergence tests) for that system.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cfdb {
+
+constexpr int kBlock = 256;
+
+template <class T> struct Sell {
+    const int* slice; // n_slices + 1 slot offsets
+    const int* col;
+    const T* val;
+};
+
+struct Tiles {
+    const int* row; // n_tiles + 1 first rows
+    const int* sys; // n_tiles system ids
+};
+
+// Per-system Krylov state (device resident; host reads it only at the end of a solve).
+struct SysState {
+    double tol;       // absolute tolerance on |r|_2
+    double res;       // last |r|_2
+    double rz;        // r . z
+    double pq;        // p . q
+    double alpha;
+    double beta;
+    double true_res;  // |b - A x|_2 recomputed after the solve
+    int it;           // current iteration number (1-based, as the reference loop counter)
+    int max_it;
+    int iters_out;    // reported iterations
+    int active;
+    int converged;
+    int first;        // next p-update is p = z
+    int phase;        // 0: initial preconditioning, 1: inside the loop
+    int check;        // mixed precision: recursive residual met the target, verify in FP64
+    int breakdown;    // p.q == 0 or rho == 0 style exits
+    int pad;
+};
+
+struct Control {
+    int* n_active;   // number of active systems (device)
+    int* error;      // device error flag (bounded waits)
+};
+
+// ---------------------------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of two values; result valid in thread 0. Fixed tree: deterministic.
+__device__ __forceinline__ void block_sum2(double& a, double& b) {
+    __shared__ double sa[kBlock / 32], sb[kBlock / 32];
+    a = warp_sum(a);
+    b = warp_sum(b);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        sa[w] = a;
+        sb[w] = b;
+    }
+    __syncthreads();
+    if (w == 0) {
+        a = l < kBlock / 32 ? sa[l] : 0.0;
+        b = l < kBlock / 32 ? sb[l] : 0.0;
+        a = warp_sum(a);
+        b = warp_sum(b);
+    }
+    __syncthreads();
+}
+
+// Writes this tile's partials; returns true in every thread of the system's last CTA, whose
+// thread 0 then holds the system totals in (a, b).
+__device__ __forceinline__ bool reduce_system(double& a, double& b, int tile, int s,
+                                              double* partials, int* counters,
+                                              const int* sys_tile0) {
+    __shared__ int last;
+    block_sum2(a, b);
+    if (threadIdx.x == 0) {
+        partials[2 * tile] = a;
+        partials[2 * tile + 1] = b;
+        __threadfence();
+        const int n_tiles = sys_tile0[s + 1] - sys_tile0[s];
+        const int ticket = atomicAdd(&counters[s], 1);
+        last = ticket == n_tiles - 1;
+        if (last) counters[s] = 0;
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    a = 0.0;
+    b = 0.0;
+    for (int t = sys_tile0[s] + threadIdx.x; t < sys_tile0[s + 1]; t += kBlock) {
+        a += __ldcg(&partials[2 * t]);
+        b += __ldcg(&partials[2 * t + 1]);
+    }
+    block_sum2(a, b);
+    return true;
+}
+
+__device__ __forceinline__ void deactivate(SysState& st, Control c) {
+    st.active = 0;
+    atomicSub(c.n_active, 1);
+}
+
+// Row sum of a SELL row: sum_k val[k] * x[col[k]] in CSR order.
+template <class T, class X>
+__device__ __forceinline__ T sell_row(const Sell<T>& m, int row, const X* __restrict__ x) {
+    const int slice = row >> 5;
+    const int lane = row & 31;
+    int k = __ldg(&m.slice[slice]) + lane;
+    const int end = __ldg(&m.slice[slice + 1]);
+    T s = T(0);
+#pragma unroll 4
+    for (; k < end; k += 32) {
+        const T v = __ldg(&m.val[k]);
+        const int c = __ldg(&m.col[k]);
+        if constexpr (sizeof(T) == 8) {
+            s = __dadd_rn(s, __dmul_rn(v, static_cast<T>(x[c])));
+        } else {
+            s = fmaf(v, static_cast<T>(x[c]), s);
+        }
+    }
+    return s;
+}
+
+// Tile bookkeeping shared by all tiled kernels.
+struct TileCtx {
+    int tile, s, r0, r1;
+};
+
+__device__ __forceinline__ bool tile_begin(const Tiles& t, const SysState* st, TileCtx& c) {
+    c.tile = blockIdx.x;
+    c.s = __ldg(&t.sys[c.tile]);
+    c.r0 = __ldg(&t.row[c.tile]);
+    c.r1 = __ldg(&t.row[c.tile + 1]);
+    return st == nullptr || *((volatile const int*)&st[c.s].active) != 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// level-0 values from the LDU (or CSR) source arrays
+// ---------------------------------------------------------------------------------------------
+
+// src indexes a virtual array [seg0 | seg1 | seg2]; -1 marks padding. For a single system the
+// three segments are diag (n), upper (nf), lower (nf); for a batch all sources are one array.
+struct ValueSource {
+    const double* p0;
+    const double* p1;
+    const double* p2;
+    int n1; // first index of seg1
+    int n2; // first index of seg2
+};
+
+__device__ __forceinline__ double vs_load(const ValueSource& v, int i) {
+    if (i < v.n1) return v.p0[i];
+    if (i < v.n2) return v.p1[i - v.n1];
+    return v.p2[i - v.n2];
+}
+
+// val[s] = source value of slot s; wd[i] = w * (diag_i != 0 ? 1/diag_i : 1)
+// (krylov_cuda.cu:541-562: assemble_diag / assemble_faces / inv_diag kernels, fused).
+static __global__ void k_fill_level0(int n_slots, int n_rows, const int* __restrict__ src,
+                              const int* __restrict__ diag_src, ValueSource vs, double weight,
+                              double* __restrict__ val64, float* __restrict__ val32,
+                              double* __restrict__ wd64, float* __restrict__ wd32) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n_slots) {
+        const int s = __ldg(&src[i]);
+        const double v = s >= 0 ? vs_load(vs, s) : 0.0;
+        if (val64 != nullptr) val64[i] = v;
+        if (val32 != nullptr) val32[i] = static_cast<float>(v);
+    }
+    if (i < n_rows) {
+        const int s = __ldg(&diag_src[i]);
+        const double d = s >= 0 ? vs_load(vs, s) : 0.0;
+        const double dinv = d != 0.0 ? 1.0 / d : 1.0;
+        const double wd = weight * dinv;
+        if (wd64 != nullptr) wd64[i] = wd;
+        if (wd32 != nullptr) wd32[i] = static_cast<float>(wd);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// V-cycle kernels (krylov_kernels.inc:182-238, krylov_cuda.cu:392-408)
+// T: arithmetic of the cycle (double: reference, float: mixed). B: type of the right-hand side
+// (level 0 reads the FP64 Krylov residual directly in both modes).
+// ---------------------------------------------------------------------------------------------
+
+template <class T> __device__ __forceinline__ T jac_update(T x, T wd, T b, T ax) {
+    if constexpr (sizeof(T) == 8) {
+        return __dadd_rn(x, __dmul_rn(wd, __dsub_rn(b, ax)));
+    } else {
+        return fmaf(wd, b - ax, x);
+    }
+}
+
+// First smoothing step from x = 0: x1 = 0 + wd * b (t = A*0 = 0), and when fused2 also the
+// second sweep y = x1 + wd (b - A x1) with x1 of the neighbours recomputed on the fly.
+template <class T, class B>
+static __global__ void __launch_bounds__(kBlock) k_vc_first(Sell<T> a, Tiles tiles, const SysState* st,
+                                                     const T* __restrict__ wd,
+                                                     const B* __restrict__ b, T* __restrict__ y,
+                                                     int fused2) {
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
+        const T wdi = wd[row];
+        const T bi = static_cast<T>(b[row]);
+        T x1;
+        if constexpr (sizeof(T) == 8) x1 = __dadd_rn(0.0, __dmul_rn(wdi, bi));
+        else x1 = wdi * bi;
+        if (!fused2) {
+            y[row] = x1;
+            continue;
+        }
+        const int slice = row >> 5, lane = row & 31;
+        const int end = __ldg(&a.slice[slice + 1]);
+        T s = T(0);
+        for (int k = __ldg(&a.slice[slice]) + lane; k < end; k += 32) {
+            const int j = __ldg(&a.col[k]);
+            const T v = __ldg(&a.val[k]);
+            if constexpr (sizeof(T) == 8) {
+                const T xj = __dadd_rn(0.0, __dmul_rn(wd[j], static_cast<T>(b[j])));
+                s = __dadd_rn(s, __dmul_rn(v, xj));
+            } else {
+                s = fmaf(v, wd[j] * static_cast<T>(b[j]), s);
+            }
+        }
+        y[row] = jac_update<T>(x1, wdi, bi, s);
+    }
+}
+
+// y = x + wd (b - A x)
+template <class T, class B>
+static __global__ void __launch_bounds__(kBlock) k_vc_jacobi(Sell<T> a, Tiles tiles, const SysState* st,
+                                                      const T* __restrict__ wd,
+                                                      const B* __restrict__ b,
+                                                      const T* __restrict__ x, T* __restrict__ y) {
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
+        const T s = sell_row(a, row, x);
+        y[row] = jac_update<T>(x[row], wd[row], static_cast<T>(b[row]), s);
+    }
+}
+
+// t = b - A x
+template <class T, class B>
+static __global__ void __launch_bounds__(kBlock) k_vc_residual(Sell<T> a, Tiles tiles, const SysState* st,
+                                                        const B* __restrict__ b,
+                                                        const T* __restrict__ x,
+                                                        T* __restrict__ t) {
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
+        const T s = sell_row(a, row, x);
+        if constexpr (sizeof(T) == 8) t[row] = __dsub_rn(static_cast<T>(b[row]), s);
+        else t[row] = static_cast<T>(b[row]) - s;
+    }
+}
+
+// y = M x (restriction into the next level's right-hand side)
+template <class T>
+static __global__ void __launch_bounds__(kBlock) k_vc_spmv(Sell<T> m, Tiles tiles, const SysState* st,
+                                                    const T* __restrict__ x, T* __restrict__ y) {
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) y[row] = sell_row(m, row, x);
+}
+
+// x += P xc
+template <class T>
+static __global__ void __launch_bounds__(kBlock) k_vc_prolong(Sell<T> p, Tiles tiles, const SysState* st,
+                                                       const T* __restrict__ xc,
+                                                       T* __restrict__ x) {
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
+        const T s = sell_row(p, row, xc);
+        if constexpr (sizeof(T) == 8) x[row] = __dadd_rn(x[row], s);
+        else x[row] = x[row] + s;
+    }
+}
+
+// ---- coarsest level: x = M b with the dense FP64 inverse (krylov_cuda.cu:298-307) ----
+// One CTA per coarse block. b is staged into shared memory with a TMA bulk copy (1-D,
+// cp.async.bulk, no multicast); every thread computes rows with a column-major (transposed)
+// inverse, so a warp's loads of one column are coalesced and each row sum keeps the reference
+// order j = 0..n-1.
+
+struct CoarseBlocks {
+    const int* sys;      // system of each block
+    const int* row;      // first row of the block in its level's vectors
+    const int* n;        // block size
+    const long long* m_off; // offset of the block's transposed inverse in `mt`
+    const double* mt;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+template <class TB, class TX>
+static __global__ void __launch_bounds__(kBlock) k_vc_coarse(CoarseBlocks cb, const SysState* st,
+                                                      const TB* const* __restrict__ b_level,
+                                                      TX* const* __restrict__ x_level,
+                                                      const int* __restrict__ block_level,
+                                                      Control ctl) {
+    using T = TB;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    const int blk = blockIdx.x;
+    const int s = cb.sys[blk];
+    if (st != nullptr && *((volatile const int*)&st[s].active) == 0) return;
+    const int lvl = block_level[blk];
+    const int r0 = cb.row[blk];
+    const int n = cb.n[blk];
+    const T* b = b_level[lvl] + r0;
+    TX* x = x_level[lvl] + r0;
+    T* bs = reinterpret_cast<T*>(smem_raw);
+    // bytes: the block is padded to 32 rows, so this is a multiple of 128 and 16-aligned.
+    const uint32_t bytes = static_cast<uint32_t>(((n + 31) / 32) * 32 * sizeof(T));
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&bar)),
+                     "r"(bytes)
+                     : "memory");
+        uint32_t done = 0;
+        while (done < bytes) {
+            const uint32_t chunk = bytes - done < 32768u ? bytes - done : 32768u;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_u32(reinterpret_cast<unsigned char*>(bs) + done)),
+                "l"(reinterpret_cast<const unsigned char*>(b) + done), "r"(chunk), "r"(smem_u32(&bar))
+                : "memory");
+            done += chunk;
+        }
+    }
+    // bounded wait on phase 0
+    uint32_t ok = 0;
+    for (int spin = 0; spin < (1 << 22) && !ok; ++spin) {
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(smem_u32(&bar)), "r"(0)
+            : "memory");
+    }
+    if (!ok) {
+        if (threadIdx.x == 0) atomicExch(ctl.error, 1);
+        return;
+    }
+    const double* mt = cb.mt + cb.m_off[blk];
+    for (int i = threadIdx.x; i < n; i += kBlock) {
+        double acc = 0.0;
+        for (int j = 0; j < n; ++j) {
+            acc = __dadd_rn(acc, __dmul_rn(__ldg(&mt[static_cast<long long>(j) * n + i]),
+                                           static_cast<double>(bs[j])));
+        }
+        x[i] = static_cast<TX>(acc);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Krylov kernels (krylov_kernels.inc:240-301 / krylov_cuda.cu:462-507), level-0 FP64
+// ---------------------------------------------------------------------------------------------
+
+// r = b - A x ; |r|_2 ; stop if already converged (iterations = 0)
+static __global__ void __launch_bounds__(kBlock) k_cg_init(Sell<double> a, Tiles tiles, SysState* st,
+                                                    const double* __restrict__ b,
+                                                    const double* __restrict__ x,
+                                                    double* __restrict__ r, double* partials,
+                                                    int* counters, const int* sys_tile0,
+                                                    Control ctl) {
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    double rr = 0.0, unused = 0.0;
+    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
+        const double ri = __dsub_rn(b[row], sell_row(a, row, x));
+        r[row] = ri;
+        rr = __dadd_rn(rr, __dmul_rn(ri, ri));
+    }
+    if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+        SysState& s = st[c.s];
+        s.res = sqrt(rr);
+        s.phase = 0;
+        s.first = 1;
+        s.check = 0;
+        s.it = 0;
+        if (s.res <= s.tol) {
+            s.converged = 1;
+            s.iters_out = 0;
+            deactivate(s, ctl);
+        }
+    }
+}
+
+// p = z (first) or p = z + beta p
+template <class Z>
+static __global__ void __launch_bounds__(kBlock) k_cg_pupdate(Tiles tiles, const SysState* st,
+                                                       const Z* __restrict__ z,
+                                                       double* __restrict__ p) {
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    const bool first = st[c.s].first != 0;
+    const double beta = st[c.s].beta;
+    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
+        const double zi = static_cast<double>(z[row]);
+        p[row] = first ? zi : __dadd_rn(zi, __dmul_rn(beta, p[row]));
+    }
+}
+
+// q = A p ; p.q ; alpha = rz / pq (break if pq == 0)
+static __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(Sell<double> a, Tiles tiles, SysState* st,
+                                                       const double* __restrict__ p,
+                                                       double* __restrict__ q, double* partials,
+                                                       int* counters, const int* sys_tile0,
+                                                       Control ctl) {
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    double pq = 0.0, unused = 0.0;
+    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
+        const double qi = sell_row(a, row, p);
+        q[row] = qi;
+        pq = __dadd_rn(pq, __dmul_rn(p[row], qi));
+    }
+    if (reduce_system(pq, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+        SysState& s = st[c.s];
+        s.first = 0;
+        s.pq = pq;
+        if (pq == 0.0) {
+            s.iters_out = s.it;
+            s.breakdown = 1;
+            deactivate(s, ctl);
+        } else {
+            s.alpha = s.rz / pq;
+        }
+    }
+}
+
+// x += alpha p ; r -= alpha q ; |r|_2 ; converged?
+// verify_true: mixed mode marks the system for an FP64 true-residual check instead.
+static __global__ void __launch_bounds__(kBlock) k_cg_xr(Tiles tiles, SysState* st,
+                                                  double* __restrict__ x, double* __restrict__ r,
+                                                  const double* __restrict__ p,
+                                                  const double* __restrict__ q, double* partials,
+                                                  int* counters, const int* sys_tile0,
+                                                  Control ctl, int verify_true) {
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    const double alpha = st[c.s].alpha;
+    double rr = 0.0, unused = 0.0;
+    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
+        x[row] = __dadd_rn(x[row], __dmul_rn(alpha, p[row]));
+        const double ri = __dsub_rn(r[row], __dmul_rn(alpha, q[row]));
+        r[row] = ri;
+        rr = __dadd_rn(rr, __dmul_rn(ri, ri));
+    }
+    if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+        SysState& s = st[c.s];
+        s.res = sqrt(rr);
+        if (s.res <= s.tol) {
+            if (verify_true) {
+                s.check = 1;
+            } else {
+                s.converged = 1;
+                s.iters_out = s.it;
+                deactivate(s, ctl);
+            }
+        }
+    }
+}
+
+// Mixed precision: for systems whose recursive residual met the target, recompute
+// r = b - A x in FP64; converged if |r| <= tol, else restart the search direction.
+static __global__ void __launch_bounds__(kBlock) k_cg_true_check(Sell<double> a, Tiles tiles, SysState* st,
+                                                          const double* __restrict__ b,
+                                                          const double* __restrict__ x,
+                                                          double* __restrict__ r, double* partials,
+                                                          int* counters, const int* sys_tile0,
+                                                          Control ctl) {
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    if (st[c.s].check == 0) return;
+    double rr = 0.0, unused = 0.0;
+    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
+        const double ri = __dsub_rn(b[row], sell_row(a, row, x));
+        r[row] = ri;
+        rr = __dadd_rn(rr, __dmul_rn(ri, ri));
+    }
+    if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+        SysState& s = st[c.s];
+        s.check = 0;
+        s.res = sqrt(rr);
+        if (s.res <= s.tol) {
+            s.converged = 1;
+            s.iters_out = s.it;
+            deactivate(s, ctl);
+        } else {
+            s.first = 1;
+        }
+    }
+}
+
+// Scalar tail of the preconditioning step for one system (last CTA, thread 0):
+// rz_new (and zq = z.q for the flexible variant) -> beta, iteration counter.
+__device__ __forceinline__ void precond_tail(SysState& s, double rz_new, double zq, int flexible,
+                                             Control ctl) {
+    if (s.phase == 0) {
+        s.phase = 1;
+        s.rz = rz_new;
+        s.it = 1;
+    } else {
+        if (!s.first) {
+            // reference: beta = rz_new / rz; flexible CG (Notay): beta = -(z . q) / (p . q)
+            s.beta = flexible ? -(zq / s.pq) : rz_new / s.rz;
+        }
+        s.rz = rz_new;
+        s.it += 1;
+    }
+    if (s.it > s.max_it) {
+        s.iters_out = s.max_it;
+        deactivate(s, ctl);
+    }
+}
+
+// Last post-smoothing sweep of level 0 fused with r.z (and z.q): z = x + wd (b - A x).
+template <class T>
+static __global__ void __launch_bounds__(kBlock) k_vc_jacobi_final(Sell<T> a, Tiles tiles, SysState* st,
+                                                            const T* __restrict__ wd,
+                                                            const double* __restrict__ r,
+                                                            const T* __restrict__ x,
+                                                            T* __restrict__ z,
+                                                            const double* __restrict__ q,
+                                                            double* partials, int* counters,
+                                                            const int* sys_tile0, Control ctl,
+                                                            int flexible) {
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    double rz = 0.0, zq = 0.0;
+    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
+        const T s = sell_row(a, row, x);
+        const double ri = r[row];
+        const T zi = jac_update<T>(x[row], wd[row], static_cast<T>(ri), s);
+        z[row] = zi;
+        const double zd = static_cast<double>(zi);
+        rz = __dadd_rn(rz, __dmul_rn(ri, zd));
+        if (flexible) zq = __dadd_rn(zq, __dmul_rn(zd, q[row]));
+    }
+    if (reduce_system(rz, zq, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+        precond_tail(st[c.s], rz, zq, flexible, ctl);
+    }
+}
+
+// Unfused r.z (and z.q) when the preconditioner output is not produced by a smoothing sweep
+// (no smoothing, single-level systems, Jacobi preconditioning: z = dinv * r when jac != null).
+template <class Z>
+static __global__ void __launch_bounds__(kBlock) k_cg_rz(Tiles tiles, SysState* st,
+                                                  const double* __restrict__ r,
+                                                  Z* __restrict__ z, const double* __restrict__ jac,
+                                                  const double* __restrict__ q, double* partials,
+                                                  int* counters, const int* sys_tile0,
+                                                  Control ctl, int flexible) {
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    double rz = 0.0, zq = 0.0;
+    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
+        const double ri = r[row];
+        double zd;
+        if (jac != nullptr) {
+            zd = __dmul_rn(ri, jac[row]);
+            z[row] = static_cast<Z>(zd);
+        } else {
+            zd = static_cast<double>(z[row]);
+        }
+        rz = __dadd_rn(rz, __dmul_rn(ri, zd));
+        if (flexible) zq = __dadd_rn(zq, __dmul_rn(zd, q[row]));
+    }
+    if (reduce_system(rz, zq, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+        precond_tail(st[c.s], rz, zq, flexible, ctl);
+    }
+}
+
+// |b - A x|_2 per system into st.true_res (reporting only; all systems).
+static __global__ void __launch_bounds__(kBlock) k_true_residual(Sell<double> a, Tiles tiles, SysState* st,
+                                                          const double* __restrict__ b,
+                                                          const double* __restrict__ x,
+                                                          double* partials, int* counters,
+                                                          const int* sys_tile0) {
+    TileCtx c;
+    tile_begin(tiles, nullptr, c);
+    double rr = 0.0, unused = 0.0;
+    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
+        const double ri = __dsub_rn(b[row], sell_row(a, row, x));
+        rr = __dadd_rn(rr, __dmul_rn(ri, ri));
+    }
+    if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+        st[c.s].true_res = sqrt(rr);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Face-loop assembly (krylov_cuda.cu:681-697 / krylov_openmp.cpp:289-300), atomic-free.
+// Each cell gathers its faces in ascending face order, which reproduces the serial loop's
+// accumulation order bit for bit. cf_face[k] holds the face, cf_sign[k] 0 when the cell owns it.
+// ---------------------------------------------------------------------------------------------
+static __global__ void k_assemble_faces(int nf, const double* __restrict__ flux,
+                                 const double* __restrict__ gamma,
+                                 const double* __restrict__ delta, double convection,
+                                 double* __restrict__ upper, double* __restrict__ lower) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const double fl = flux[f];
+    const double g = __dmul_rn(gamma[f], delta[f]);
+    const double pos = fl > 0.0 ? __dmul_rn(convection, fl) : 0.0;
+    const double neg = fl < 0.0 ? __dmul_rn(convection, fl) : 0.0;
+    upper[f] = __dsub_rn(neg, g);
+    lower[f] = __dsub_rn(-pos, g);
+}
+
+static __global__ void k_assemble_cells(int n, const int* __restrict__ cf_ptr,
+                                 const int* __restrict__ cf_face, const double* __restrict__ flux,
+                                 const double* __restrict__ gamma,
+                                 const double* __restrict__ delta, const int* __restrict__ owner,
+                                 double convection, double* __restrict__ diag,
+                                 double* __restrict__ div) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    double d = diag[c];
+    double v = div[c];
+    const int end = cf_ptr[c + 1];
+    for (int k = cf_ptr[c]; k < end; ++k) {
+        const int f = cf_face[k];
+        const double fl = flux[f];
+        const double g = __dmul_rn(gamma[f], delta[f]);
+        const double pos = fl > 0.0 ? __dmul_rn(convection, fl) : 0.0;
+        const double neg = fl < 0.0 ? __dmul_rn(convection, fl) : 0.0;
+        if (owner[f] == c) {
+            d = __dadd_rn(d, __dadd_rn(pos, g));
+            v = __dadd_rn(v, fl);
+        } else {
+            d = __dadd_rn(d, __dadd_rn(-neg, g));
+            v = __dsub_rn(v, fl);
+        }
+    }
+    diag[c] = d;
+    div[c] = v;
+}
+
+} // namespace cfdb

@@ -1,0 +1,202 @@
+/*
+ * cfdb: B200-native (sm_100a) pressure-correction solver -- the C ABI.
+ *
+ * Drop-in for the accelerator call surface of Yipexnn/CFD (namespace cfd::gpu,
+ * src/gpu/include/cfd/gpu/krylov.hpp), the path selected by "solver": {"device": "gpu"}.
+ * Each entry point names the reference interface it replaces. Plain C types only: host
+ * pointers unless the name ends in _device (then every array argument is a device pointer on
+ * the system's GPU). All calls return a cfdb_status; on failure cfdb_last_error() gives the
+ * message of the calling thread's last error. Non-convergence is not an error (stats).
+ */
+#ifndef CFDB_H
+#define CFDB_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    CFDB_OK = 0,
+    CFDB_ERR_BAD_ARG = 1,   /* reference: std::invalid_argument */
+    CFDB_ERR_CUDA = 2,      /* reference: std::runtime_error("CUDA <what>: <msg>") */
+    CFDB_ERR_OOM = 3,       /* device allocation failed / admission over budget */
+    CFDB_ERR_NO_DEVICE = 4, /* no CUDA device: this library has no host fallback */
+    CFDB_ERR_NOT_READY = 5, /* e.g. AMG solve requested before a hierarchy was set */
+    CFDB_ERR_TIMEOUT = 6,   /* a bounded device wait expired */
+    CFDB_ERR_INTERNAL = 7
+} cfdb_status;
+
+/* krylov.hpp:10-16 CsrView: square or rectangular CSR (0-based). */
+typedef struct {
+    int n;   /* rows */
+    int nnz;
+    const int* row_ptr; /* n + 1 */
+    const int* col;     /* nnz */
+    const double* val;  /* nnz */
+} cfdb_csr;
+
+/* krylov.hpp:48-52 AmgLevelView: a (n_l x n_l), p (n_l x n_{l+1}), r (n_{l+1} x n_l). */
+typedef struct {
+    cfdb_csr a;
+    cfdb_csr p;
+    cfdb_csr r;
+} cfdb_amg_level;
+
+/* krylov.hpp:53-58 AmgView. coarse_inverse: dense row-major inverse of the coarsest a. */
+typedef struct {
+    int n_levels;
+    const cfdb_amg_level* levels;
+    const double* coarse_inverse;
+    int smooth_sweeps;    /* reference default 2 */
+    double jacobi_weight; /* reference default 0.7 */
+} cfdb_amg_view;
+
+/* krylov.hpp:21-24 SolveControl. */
+typedef struct {
+    double abs_tolerance; /* stop when |r|_2 <= abs_tolerance */
+    int max_iterations;
+} cfdb_control;
+
+/* krylov.hpp:26-31 SolveStats (+ the true residual recomputed in FP64 after the solve). */
+typedef struct {
+    int iterations;
+    double residual; /* |r|_2 of the solver's residual at exit (reference semantics) */
+    int converged;
+    int on_device;
+    double true_residual; /* |b - A x|_2 recomputed in FP64 from the returned x */
+} cfdb_stats;
+
+/* krylov.hpp:68-77 LduPattern: CSR pattern + positions of diag / upper / lower values. */
+typedef struct {
+    int n;
+    int n_faces;
+    int nnz;
+    const int* row_ptr;
+    const int* col;
+    const int* diag_pos;
+    const int* upper_pos;
+    const int* lower_pos;
+} cfdb_ldu_pattern;
+
+typedef enum { CFDB_METHOD_CG = 0, CFDB_METHOD_BICGSTAB = 1 } cfdb_method;
+
+/* Arithmetic of the AMG V-cycle. FP64: the reference algorithm. MIXED: hierarchy and V-cycle
+ * in FP32 (FP32 accumulation) inside an FP64 flexible CG; the outer residual recompute, dots
+ * and the coarsest-level inverse stay FP64. */
+typedef enum { CFDB_PRECISION_FP64 = 0, CFDB_PRECISION_MIXED = 1 } cfdb_precision;
+
+/* amg.hpp:17-23 AmgSettings (+ the AmgView smoother defaults). */
+typedef struct {
+    double strength_threshold; /* 0.08 */
+    int max_levels;            /* 25 */
+    int coarse_size;           /* 400 */
+    int smooth_sweeps;         /* 2 */
+    double jacobi_weight;      /* 0.7 */
+} cfdb_amg_settings;
+
+/* ---- backend queries: krylov.hpp:118-123 ---- */
+int cfdb_backend_name(char* buf, size_t len);        /* backend_name(): "cuda" */
+int cfdb_device_available(void);                    /* device_available() */
+int cfdb_device_description(char* buf, size_t len); /* device_description() */
+int cfdb_last_error(char* buf, size_t len);          /* message of the last failed call */
+void cfdb_default_amg_settings(cfdb_amg_settings* s);
+
+/* ---- one-shot calls ---- */
+
+/* assemble_convection_diffusion (krylov.hpp:105-116; CUDA krylov_cuda.cu:701-741).
+ * upper = min(cF,0) - G, lower = -max(cF,0) - G, diag[own] += max(cF,0) + G,
+ * diag[nei] += -min(cF,0) + G, div[own] += F, div[nei] -= F, G = gamma*delta, c = convection.
+ * diag and divergence are accumulated (not cleared). Atomic-free, bit-identical to the
+ * reference's serial loop (each cell adds its faces in ascending face order). */
+int cfdb_assemble(int n_cells, int n_faces, const int* owner, const int* neighbour,
+                  const double* flux, const double* gamma, const double* delta_coeff,
+                  double convection, double* upper, double* lower, double* diag,
+                  double* divergence);
+/* Same on device arrays (no host copies), on the calling thread's library stream. */
+int cfdb_assemble_device(int n_cells, int n_faces, const int* owner, const int* neighbour,
+                         const double* flux, const double* gamma, const double* delta_coeff,
+                         double convection, double* upper, double* lower, double* diag,
+                         double* divergence);
+
+/* solve (krylov.hpp:37-38): Jacobi-preconditioned CG / BiCGStab on a host CSR matrix. */
+int cfdb_solve(const cfdb_csr* a, const double* b, double* x, int method,
+               const cfdb_control* control, cfdb_stats* stats);
+
+/* solve_amg_cg (krylov.hpp:61-62): AMG-preconditioned CG, A = levels[0].a. */
+int cfdb_solve_amg_cg(const cfdb_amg_view* amg, const double* b, double* x,
+                      const cfdb_control* control, cfdb_stats* stats);
+
+/* ---- CSR pattern: fv::build_csr_pattern (src/fv/src/ldu_matrix.cpp:572-612) ----
+ * col, upper_pos, lower_pos sized n + 2*n_faces / n_faces; returns nnz in *nnz. */
+int cfdb_build_pattern(int n, int n_faces, const int* owner, const int* neighbour,
+                       int* row_ptr, int* col, int* diag_pos, int* upper_pos, int* lower_pos,
+                       int* nnz);
+
+/* ---- host AMG setup: fv::AmgPreconditioner::setup (src/fv/src/amg.cpp:122-190) ---- */
+typedef struct cfdb_hierarchy cfdb_hierarchy;
+int cfdb_amg_setup(const cfdb_csr* a, const cfdb_amg_settings* settings,
+                   cfdb_hierarchy** out);
+int cfdb_hierarchy_destroy(cfdb_hierarchy* h);
+/* levels() / level_matrix / level_prolongation / level_restriction (amg.hpp:37-54);
+ * which: 0 = a, 1 = p, 2 = r. Pointers stay valid while h lives. */
+int cfdb_hierarchy_levels(const cfdb_hierarchy* h, int* n_levels);
+int cfdb_hierarchy_level(const cfdb_hierarchy* h, int level, int which, int* n_rows,
+                         int* n_cols, cfdb_csr* m);
+int cfdb_hierarchy_aggregates(const cfdb_hierarchy* h, int level, const int** agg,
+                              int* n_aggregates);
+/* coarse_inverse() (amg.cpp:227-240), dense row-major. */
+int cfdb_hierarchy_coarse_inverse(const cfdb_hierarchy* h, const double** inv, int* n_c);
+/* AmgView of the hierarchy with the given smoother; levels storage owned by h. */
+int cfdb_hierarchy_view(cfdb_hierarchy* h, int smooth_sweeps, double jacobi_weight,
+                        cfdb_amg_view* view);
+int cfdb_hierarchy_operator_complexity(const cfdb_hierarchy* h, double* oc);
+
+/* ---- persistent system: DeviceSolver (krylov.hpp:83-103; krylov_cuda.cu:566-677) ---- */
+typedef struct cfdb_system cfdb_system;
+
+/* DeviceSolver(const LduPattern&): the pattern is copied; the GPU is the current device. */
+int cfdb_system_create(const cfdb_ldu_pattern* pattern, cfdb_system** out);
+/* Same from mesh addressing (builds the pattern; keeps owner/neighbour for the fused
+ * face-data assembly below). */
+int cfdb_system_create_mesh(int n_cells, int n_faces, const int* owner, const int* neighbour,
+                            cfdb_system** out);
+int cfdb_system_destroy(cfdb_system* sys);                 /* ~DeviceSolver() */
+int cfdb_system_on_device(const cfdb_system* sys);         /* on_device() */
+/* set_amg(const AmgView&): levels[0].a is ignored (assembled on the device). */
+int cfdb_system_set_amg(cfdb_system* sys, const cfdb_amg_view* amg);
+/* Builds the hierarchy from LDU coefficients on the host (AmgPreconditioner::setup) and
+ * installs it, as LduMatrix::solve_persistent does on an AMG rebuild (ldu_matrix.cpp:314-353).*/
+int cfdb_system_setup_amg(cfdb_system* sys, const double* diag, const double* upper,
+                          const double* lower, const cfdb_amg_settings* settings);
+int cfdb_system_set_precision(cfdb_system* sys, int precision);
+/* solve(diag, upper, lower, b, x, method, use_amg, control): assembles A from LDU on the
+ * device and solves A x = b; x is the initial guess in and the solution out. */
+int cfdb_system_solve(cfdb_system* sys, const double* diag, const double* upper,
+                      const double* lower, const double* b, double* x, int method, int use_amg,
+                      const cfdb_control* control, cfdb_stats* stats);
+/* Same with device-resident arrays (no host transfers): the HBM-resident hot path. */
+int cfdb_system_solve_device(cfdb_system* sys, const double* diag, const double* upper,
+                             const double* lower, const double* b, double* x, int method,
+                             int use_amg, const cfdb_control* control, cfdb_stats* stats);
+/* Fused pressure assembly on device arrays (flow_solver.cpp:757-783 with the face loop of
+ * krylov_cuda.cu:681-697): from face flux / gamma / delta (n_faces) builds the device matrix
+ * directly and returns upper, lower (n_faces) and diag, divergence (n_cells, accumulated)
+ * like cfdb_assemble. Requires cfdb_system_create_mesh. */
+int cfdb_system_assemble_device(cfdb_system* sys, const double* flux, const double* gamma,
+                                const double* delta_coeff, double convection, double* upper,
+                                double* lower, double* diag, double* divergence);
+/* AmgPreconditioner::apply (amg.hpp:33; accelerator V-cycle krylov_kernels.inc:209-238): one
+ * V-cycle z = M^-1 r with zero initial guess on the installed hierarchy and the current
+ * matrix (set by the last solve), in the system's precision. Host arrays. */
+int cfdb_system_apply_amg(cfdb_system* sys, const double* r, double* z);
+/* Stream of the system (cudaStream_t as void*), for callers that order their own work. */
+int cfdb_system_stream(const cfdb_system* sys, void** stream);
+/* Device bytes held by the system (pattern, hierarchy, work vectors). */
+int cfdb_system_device_bytes(const cfdb_system* sys, size_t* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,86 @@
+"""Build recipe for the CPU oracle (test infrastructure only).
+
+* ``oracle/_build/liboracle.so``: the C restatement in ``oracle/oracle.c`` (gcc, no FMA
+  contraction so roundings match the reference's x86-64 host build).
+* ``oracle/_ref/libcfdref.so``: the reference's own host sources, compiled unchanged where
+  they lie under the reference checkout, plus ``oracle/ref_shim.cpp``. Only built when the
+  reference checkout is present; the built library is git-ignored and travels with the tree.
+
+Run ``python -m oracle.build`` (or call :func:`build_all`).
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD_DIR = os.path.join(HERE, "_build")
+REF_DIR = os.path.join(HERE, "_ref")
+ORACLE_SO = os.path.join(BUILD_DIR, "liboracle.so")
+REF_SO = os.path.join(REF_DIR, "libcfdref.so")
+
+# Where the reference checkout lives in the build container (read-only).
+REFERENCE_ROOT = os.environ.get("CFD_REFERENCE_ROOT", "/root/reference")
+REF_SOURCES = [
+    "src/gpu/src/krylov_openmp.cpp",
+    "src/gpu/src/device_solver.cpp",
+    "src/gpu/src/dispatch.cpp",
+]
+
+
+def _stale(target: str, sources: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources if os.path.exists(s))
+
+
+def build_oracle(force: bool = False) -> str:
+    src = os.path.join(HERE, "oracle.c")
+    hdr = os.path.join(HERE, "oracle.h")
+    if force or _stale(ORACLE_SO, [src, hdr]):
+        os.makedirs(BUILD_DIR, exist_ok=True)
+        tmp = ORACLE_SO + f".tmp{os.getpid()}"
+        cmd = ["gcc", "-std=c11", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC",
+               "-shared", src, "-o", tmp, "-lm"]
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, ORACLE_SO)
+    return ORACLE_SO
+
+
+def reference_available() -> bool:
+    return all(os.path.exists(os.path.join(REFERENCE_ROOT, s)) for s in REF_SOURCES)
+
+
+def build_ref(force: bool = False) -> str | None:
+    """Compile the reference's host path (unchanged sources) + our shim into oracle/_ref."""
+    if not reference_available():
+        return REF_SO if os.path.exists(REF_SO) else None
+    srcs = [os.path.join(REFERENCE_ROOT, s) for s in REF_SOURCES]
+    shim = os.path.join(HERE, "ref_shim.cpp")
+    deps = srcs + [shim, os.path.join(REFERENCE_ROOT, "src/gpu/src/krylov_kernels.inc"),
+                   os.path.join(REFERENCE_ROOT, "src/gpu/include/cfd/gpu/krylov.hpp")]
+    if force or _stale(REF_SO, deps):
+        if shutil.which("g++") is None:
+            return None
+        os.makedirs(REF_DIR, exist_ok=True)
+        tmp = REF_SO + f".tmp{os.getpid()}"
+        # No -march: plain x86-64 has no FMA, so the host path rounds every product and sum.
+        cmd = ["g++", "-std=c++20", "-O3", "-fopenmp", "-fPIC", "-shared",
+               "-I", os.path.join(REFERENCE_ROOT, "src/gpu/include"), *srcs, shim, "-o", tmp]
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, REF_SO)
+    return REF_SO
+
+
+def build_all(force: bool = False) -> None:
+    build_oracle(force)
+    build_ref(force)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv)
+    print(ORACLE_SO)
+    print(REF_SO if os.path.exists(REF_SO) else "(reference not built)")

@@ -106,6 +106,18 @@ _proto("cfdb_system_solve_device", [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _P(Con
                                     _P(StatsStruct)])
 _proto("cfdb_system_assemble_device", [_vp, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp])
 _proto("cfdb_system_apply_amg", [_vp, _pd, _pd])
+_proto("cfdb_system_set_ordered", [_vp, _i])
+_proto("cfdb_system_assemble", [_vp, _pd, _pd, _pd, _d, _pd, _pd, _pd, _pd])
+_proto("cfdb_system_assemble_pressure_device", [_vp, _vp, _vp, _vp, _vp, _vp, _i, _d, _vp, _vp,
+                                                _vp, _vp])
+_proto("cfdb_system_kernel_launches", [_vp, _P(C.c_ulonglong)])
+
+
+class KernelRecordStruct(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("level", _i), ("ms", _d), ("bytes", _d)]
+
+
+_proto("cfdb_system_profile", [_vp, _i, _i, _P(KernelRecordStruct), _i, _pi])
 _proto("cfdb_system_stream", [_vp, _P(_vp)])
 _proto("cfdb_system_device_bytes", [_vp, _P(_sz)])
 # synthetic workloads (include/cfdb_synth.h)
@@ -575,6 +587,42 @@ class DeviceSolver:
         z = np.zeros(self.n)
         _check(_lib.cfdb_system_apply_amg(self._h, _dp(r), _dp(z)))
         return z
+
+    def assemble(self, flux, gamma, delta, convection, upper, lower, diag, div) -> None:
+        """assemble_convection_diffusion on the system's mesh with host arrays (in place)."""
+        for a, nm in ((upper, "upper"), (lower, "lower"), (diag, "diag"), (div, "div")):
+            _out_f64(a, nm)
+        flux, gamma, delta = _f64(flux), _f64(gamma), _f64(delta)
+        _check(_lib.cfdb_system_assemble(self._h, _dp(flux), _dp(gamma), _dp(delta),
+                                         float(convection), _dp(upper), _dp(lower), _dp(diag),
+                                         _dp(div)))
+
+    def assemble_pressure_device(self, flux, gamma, delta, source0, upper, lower, diag, source,
+                                 diag0=None, ref_cell=0, ref_value=0.0) -> None:
+        """Pressure-equation assembly on device arrays (flow_solver.cpp:757-796)."""
+        _check(_lib.cfdb_system_assemble_pressure_device(
+            self._h, _devptr(flux), _devptr(gamma), _devptr(delta),
+            _devptr(diag0) if diag0 is not None else None, _devptr(source0), int(ref_cell),
+            float(ref_value), _devptr(upper), _devptr(lower), _devptr(diag), _devptr(source)))
+
+    def kernel_launches(self) -> int:
+        c = C.c_ulonglong()
+        _check(_lib.cfdb_system_kernel_launches(self._h, C.byref(c)))
+        return c.value
+
+    def set_ordered(self, ordered: bool) -> None:
+        """Bit-reproducible FP64 V-cycles (thread-per-row sums in CSR order on every level)."""
+        _check(_lib.cfdb_system_set_ordered(self._h, 1 if ordered else 0))
+
+    def profile(self, use_amg: bool = True, reps: int = 5) -> list:
+        """Per-kernel device time (ms) and algorithmic bytes of the initial preconditioning and
+        one iteration, in launch order: [(name, level, ms, bytes), ...]."""
+        recs = (KernelRecordStruct * 512)()
+        n = C.c_int()
+        _check(_lib.cfdb_system_profile(self._h, 1 if use_amg else 0, int(reps), recs, 512,
+                                        C.byref(n)))
+        return [(recs[i].name.decode(), recs[i].level, recs[i].ms, recs[i].bytes)
+                for i in range(n.value)]
 
     def stream(self) -> int:
         s = _vp()

@@ -121,6 +121,8 @@ struct cfdb_system {
     int* d_owner = nullptr;
     int* d_cf_ptr = nullptr;
     int* d_cf_face = nullptr;
+    double* h_asm = nullptr; // device staging of cfdb_system_assemble (host-array variant)
+    unsigned long long launches = 0;
 };
 
 namespace {
@@ -727,9 +729,11 @@ int cfdb_system_assemble_device(cfdb_system* sys, const double* flux, const doub
         const int n = sys->pat.n, nf = sys->pat.n_faces;
         if (nf > 0) {
             k_assemble_faces<<<(nf + 255) / 256, 256, 0, st>>>(nf, flux, gamma, delta, convection, upper, lower);
+            ++sys->launches;
         }
         k_assemble_cells<<<(n + 255) / 256, 256, 0, st>>>(n, sys->d_cf_ptr, sys->d_cf_face, flux, gamma, delta,
                                                           sys->d_owner, convection, diag, div);
+        ++sys->launches;
         CFDB_CUDA(cudaGetLastError());
         CFDB_CUDA(cudaStreamSynchronize(st));
     });
@@ -746,6 +750,117 @@ int cfdb_system_apply_amg(cfdb_system* sys, const double* r, double* z) {
         sys->eng->apply_vcycle(mode, {0});
         sys->eng->get_precond(0, z, false, mode);
     });
+}
+
+int cfdb_system_set_ordered(cfdb_system* sys, int ordered) {
+    return guarded([&] {
+        if (sys == nullptr) fail(CFDB_ERR_BAD_ARG, "null system");
+        CFDB_CUDA(cudaSetDevice(sys->device));
+        ensure_engine(sys);
+        if (sys->eng->ordered() != (ordered != 0)) {
+            sys->eng->set_ordered(ordered != 0);
+            sys->dirty = true;
+            ensure_engine(sys);
+        }
+    });
+}
+
+int cfdb_system_profile(cfdb_system* sys, int use_amg, int reps, cfdb_kernel_record* records, int max_records,
+                        int* n_records) {
+    return guarded([&] {
+        if (sys == nullptr || records == nullptr || n_records == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
+        CFDB_CUDA(cudaSetDevice(sys->device));
+        ensure_engine(sys);
+        Mode mode = Mode::Jacobi;
+        if (use_amg && sys->h) mode = sys->precision == CFDB_PRECISION_MIXED ? Mode::AmgMixed : Mode::AmgFp64;
+        const auto recs = sys->eng->profile(mode, reps);
+        const int n = std::min<int>(static_cast<int>(recs.size()), max_records);
+        for (int i = 0; i < n; ++i) {
+            std::memcpy(records[i].name, recs[i].name, sizeof(records[i].name));
+            records[i].level = recs[i].level;
+            records[i].ms = recs[i].ms;
+            records[i].bytes = recs[i].bytes;
+        }
+        *n_records = n;
+    });
+}
+
+int cfdb_system_assemble(cfdb_system* sys, const double* flux, const double* gamma, const double* delta,
+                         double convection, double* upper, double* lower, double* diag, double* div) {
+    return guarded([&] {
+        if (sys == nullptr) fail(CFDB_ERR_BAD_ARG, "null system");
+        if (sys->d_cf_ptr == nullptr) fail(CFDB_ERR_BAD_ARG, "system was not created from mesh addressing");
+        if (!flux || !gamma || !delta || !upper || !lower || !diag || !div) fail(CFDB_ERR_BAD_ARG, "null array");
+        CFDB_CUDA(cudaSetDevice(sys->device));
+        ensure_engine(sys);
+        cudaStream_t st = sys->eng->stream();
+        const int n = sys->pat.n, nf = sys->pat.n_faces;
+        if (sys->h_asm == nullptr) {
+            sys->h_asm = sys->asm_arena.alloc<double>(5 * static_cast<size_t>(nf) + 2 * static_cast<size_t>(n));
+        }
+        double* d_fl = sys->h_asm;
+        double* d_ga = d_fl + nf;
+        double* d_de = d_ga + nf;
+        double* d_up = d_de + nf;
+        double* d_lo = d_up + nf;
+        double* d_dg = d_lo + nf;
+        double* d_dv = d_dg + n;
+        const size_t bf = sizeof(double) * nf, bc = sizeof(double) * n;
+        if (nf > 0) {
+            CFDB_CUDA(cudaMemcpyAsync(d_fl, flux, bf, cudaMemcpyHostToDevice, st));
+            CFDB_CUDA(cudaMemcpyAsync(d_ga, gamma, bf, cudaMemcpyHostToDevice, st));
+            CFDB_CUDA(cudaMemcpyAsync(d_de, delta, bf, cudaMemcpyHostToDevice, st));
+        }
+        CFDB_CUDA(cudaMemcpyAsync(d_dg, diag, bc, cudaMemcpyHostToDevice, st));
+        CFDB_CUDA(cudaMemcpyAsync(d_dv, div, bc, cudaMemcpyHostToDevice, st));
+        if (nf > 0) {
+            k_assemble_faces<<<(nf + 255) / 256, 256, 0, st>>>(nf, d_fl, d_ga, d_de, convection, d_up, d_lo);
+            ++sys->launches;
+        }
+        k_assemble_cells<<<(n + 255) / 256, 256, 0, st>>>(n, sys->d_cf_ptr, sys->d_cf_face, d_fl, d_ga, d_de,
+                                                          sys->d_owner, convection, d_dg, d_dv);
+        ++sys->launches;
+        CFDB_CUDA(cudaGetLastError());
+        if (nf > 0) {
+            CFDB_CUDA(cudaMemcpyAsync(upper, d_up, bf, cudaMemcpyDeviceToHost, st));
+            CFDB_CUDA(cudaMemcpyAsync(lower, d_lo, bf, cudaMemcpyDeviceToHost, st));
+        }
+        CFDB_CUDA(cudaMemcpyAsync(diag, d_dg, bc, cudaMemcpyDeviceToHost, st));
+        CFDB_CUDA(cudaMemcpyAsync(div, d_dv, bc, cudaMemcpyDeviceToHost, st));
+        CFDB_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+int cfdb_system_assemble_pressure_device(cfdb_system* sys, const double* flux, const double* gamma,
+                                         const double* delta, const double* diag0, const double* source0,
+                                         int ref_cell, double ref_value, double* upper, double* lower,
+                                         double* diag, double* source) {
+    return guarded([&] {
+        if (sys == nullptr) fail(CFDB_ERR_BAD_ARG, "null system");
+        if (sys->d_cf_ptr == nullptr) fail(CFDB_ERR_BAD_ARG, "system was not created from mesh addressing");
+        if (!flux || !gamma || !delta || !source0 || !upper || !lower || !diag || !source)
+            fail(CFDB_ERR_BAD_ARG, "null array");
+        if (ref_cell >= sys->pat.n) fail(CFDB_ERR_BAD_ARG, "reference cell out of range");
+        CFDB_CUDA(cudaSetDevice(sys->device));
+        ensure_engine(sys);
+        cudaStream_t st = sys->eng->stream();
+        const int n = sys->pat.n, nf = sys->pat.n_faces;
+        if (nf > 0) {
+            k_assemble_faces<<<(nf + 255) / 256, 256, 0, st>>>(nf, flux, gamma, delta, 0.0, upper, lower);
+            ++sys->launches;
+        }
+        k_assemble_pressure_cells<<<(n + 255) / 256, 256, 0, st>>>(n, sys->d_cf_ptr, sys->d_cf_face, flux, gamma,
+                                                                   delta, sys->d_owner, diag0, source0, ref_cell,
+                                                                   ref_value, diag, source);
+        ++sys->launches;
+        CFDB_CUDA(cudaGetLastError());
+    });
+}
+
+int cfdb_system_kernel_launches(const cfdb_system* sys, unsigned long long* count) {
+    if (sys == nullptr || count == nullptr) return set_error(CFDB_ERR_BAD_ARG, "null argument");
+    *count = sys->launches + (sys->eng ? sys->eng->kernel_launches() : 0);
+    return CFDB_OK;
 }
 
 int cfdb_system_stream(const cfdb_system* sys, void** stream) {

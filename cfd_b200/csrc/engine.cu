@@ -4,6 +4,7 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <cstdio>
 #include <numeric>
 
 namespace cfdb {
@@ -11,6 +12,7 @@ namespace cfdb {
 namespace {
 
 constexpr int kTargetTiles = 148 * 8; // 148 SMs x 8 resident 256-thread CTAs
+constexpr int kWideRow = 24;          // average entries per row above which CSR/warp-per-row is used
 
 // SELL-32 under construction on the host.
 struct SellBuild {
@@ -50,6 +52,26 @@ void sell_append(SellBuild& sb, int n_rows, int n_pad, const int* rp, const int*
             fail(1, "operator too large for 32-bit slot offsets");
         }
         sb.slice.push_back(base + static_cast<int>(slots));
+    }
+}
+
+// CSR under construction on the host (global rows of a level; padding rows are empty).
+struct CsrBuild {
+    std::vector<int> rp{0};
+    std::vector<int> col;
+    std::vector<double> val;
+};
+
+void csr_append(CsrBuild& cb, int n_rows, int n_pad, const int* rp, const int* ci, const double* va, int col_off) {
+    for (int i = 0; i < n_pad; ++i) {
+        if (i < n_rows) {
+            for (int k = rp[i]; k < rp[i + 1]; ++k) {
+                cb.col.push_back(ci[k] + col_off);
+                cb.val.push_back(va[k]);
+            }
+        }
+        if (cb.col.size() > static_cast<size_t>(INT_MAX)) fail(1, "operator too large for 32-bit offsets");
+        cb.rp.push_back(static_cast<int>(cb.col.size()));
     }
 }
 
@@ -206,6 +228,24 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         d.n_tiles_nc = nc_tiles < 0 ? d.n_tiles : nc_tiles;
         d.tiles.row = arena_.upload(trow, st);
         d.tiles.sys = arena_.upload(tsys, st);
+        // fine tiles: one row per warp, for the warp-per-row (CSR) operators
+        std::vector<int> frow, fsys;
+        int nc_fine = -1;
+        for (int k = 0; k < n_sys_; ++k) {
+            const int s = perm_[k];
+            if (L[s] <= l) continue;
+            if (L[s] - 1 == l && nc_fine < 0) nc_fine = static_cast<int>(fsys.size());
+            const int pad = round_up(rows_at(s, l), 32);
+            for (int r = 0; r < pad; r += kFineRows) {
+                frow.push_back(off[l][s] + r);
+                fsys.push_back(k);
+            }
+        }
+        frow.push_back(d.n_rows);
+        d.n_tiles_f = static_cast<int>(fsys.size());
+        d.n_tiles_f_nc = nc_fine < 0 ? d.n_tiles_f : nc_fine;
+        d.tiles_f.row = arena_.upload(frow, st);
+        d.tiles_f.sys = arena_.upload(fsys, st);
     }
     // level-0 operator (values filled per solve) + value maps
     {
@@ -229,8 +269,11 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         d.a.slots = sb.slice.back();
         const int* dslice = arena_.upload(sb.slice, st);
         const int* dcol = arena_.upload(sb.col, st);
-        d.a.s64 = {dslice, dcol, arena_.alloc<double>(d.a.slots)};
-        if (need32_) d.a.s32 = {dslice, dcol, arena_.alloc<float>(d.a.slots)};
+        d.a.s64 = {dslice, dcol, arena_.alloc<double>(d.a.slots), kFmtSell};
+        if (need32_) d.a.s32 = {dslice, dcol, arena_.alloc<float>(d.a.slots), kFmtSell};
+        long long nnz0 = 0;
+        for (int s = 0; s < n_sys_; ++s) nnz0 += systems[s].rp[systems[s].n];
+        d.a.nnz = nnz0;
         src0_ = arena_.upload(sb.src, st);
         diag_src0_ = arena_.upload(dsrc, st);
         d.wd64 = arena_.alloc<double>(d.n_rows);
@@ -240,53 +283,71 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
     // coarser levels, transfers
     for (int l = 0; l < n_levels_; ++l) {
         DevLevel& d = lv_[l];
+        // One operator over the systems that continue past level l: rows of each block from
+        // `pick(s)`, columns shifted into the target level's concatenated index space. Wide
+        // operators (more than kWideRow entries per row on average) are stored as CSR for the
+        // warp-per-row kernels unless the engine is in ordered (bit-reproducible) mode.
+        auto build_op = [&](auto pick, int col_level, DevSell64_32& m) {
+            long long nnz = 0, rows = 0;
+            for (int k = 0; k < n_sys_; ++k) {
+                const int s = perm_[k];
+                if (L[s] - 1 <= l) continue;
+                nnz += pick(s).nnz();
+                rows += pick(s).n_rows;
+            }
+            // lanes per row: about six entries per lane, 8..32 lanes
+            const double avg = rows > 0 ? static_cast<double>(nnz) / static_cast<double>(rows) : 0.0;
+            const int lanes = avg > 128.0 ? 32 : avg > 64.0 ? 16 : 8;
+            const bool wide = !ordered_ && rows > 0 && avg > kWideRow;
+            if (wide) {
+                CsrBuild cbd;
+                for (int k = 0; k < n_sys_; ++k) {
+                    const int s = perm_[k];
+                    if (L[s] - 1 <= l) continue;
+                    const HostCsr& a = pick(s);
+                    csr_append(cbd, a.n_rows, round_up(a.n_rows, 32), a.rp.data(), a.ci.data(), a.va.data(),
+                               off[col_level][s]);
+                }
+                m.n_slices = static_cast<int>(cbd.rp.size()) - 1;
+                m.slots = cbd.rp.back();
+                const int* dp = arena_.upload(cbd.rp, st);
+                const int* dc = arena_.upload(cbd.col, st);
+                if (need64_) m.s64 = {dp, dc, arena_.upload(cbd.val, st), lanes};
+                if (need32_) m.s32 = {dp, dc, arena_.upload(to_float(cbd.val), st), lanes};
+            } else {
+                SellBuild sb;
+                for (int k = 0; k < n_sys_; ++k) {
+                    const int s = perm_[k];
+                    if (L[s] - 1 <= l) continue;
+                    const HostCsr& a = pick(s);
+                    sell_append(sb, a.n_rows, round_up(a.n_rows, 32), a.rp.data(), a.ci.data(), a.va.data(),
+                                nullptr, off[col_level][s], 0, off[col_level][s]);
+                }
+                m.n_slices = static_cast<int>(sb.slice.size()) - 1;
+                m.slots = sb.slice.back();
+                const int* dp = arena_.upload(sb.slice, st);
+                const int* dc = arena_.upload(sb.col, st);
+                if (need64_) m.s64 = {dp, dc, arena_.upload(sb.val, st), kFmtSell};
+                if (need32_) m.s32 = {dp, dc, arena_.upload(to_float(sb.val), st), kFmtSell};
+            }
+            m.nnz = nnz;
+        };
         if (l > 0) {
-            SellBuild sb;
             std::vector<double> wd(static_cast<size_t>(d.n_rows_nc), weight_);
             for (int k = 0; k < n_sys_; ++k) {
                 const int s = perm_[k];
                 if (L[s] - 1 <= l) continue; // only systems with a coarser level need A_l here
                 const HostCsr& a = systems[s].h->a[l];
-                sell_append(sb, a.n_rows, round_up(a.n_rows, 32), a.rp.data(), a.ci.data(), a.va.data(),
-                            nullptr, off[l][s], 0, off[l][s]);
                 const std::vector<double> dinv = inverse_diagonal(a);
                 for (int i = 0; i < a.n_rows; ++i) wd[off[l][s] + i] = weight_ * dinv[i];
             }
-            d.a.n_slices = static_cast<int>(sb.slice.size()) - 1;
-            d.a.slots = sb.slice.back();
-            const int* dslice = arena_.upload(sb.slice, st);
-            const int* dcol = arena_.upload(sb.col, st);
-            if (need64_) {
-                d.a.s64 = {dslice, dcol, arena_.upload(sb.val, st)};
-                d.wd64 = arena_.upload(wd, st);
-            }
-            if (need32_) {
-                d.a.s32 = {dslice, dcol, arena_.upload(to_float(sb.val), st)};
-                d.wd32 = arena_.upload(to_float(wd), st);
-            }
+            build_op([&](int s) -> const HostCsr& { return systems[s].h->a[l]; }, l, d.a);
+            if (need64_) d.wd64 = arena_.upload(wd, st);
+            if (need32_) d.wd32 = arena_.upload(to_float(wd), st);
         }
         if (l + 1 < n_levels_) {
-            SellBuild sp, sr;
-            for (int k = 0; k < n_sys_; ++k) {
-                const int s = perm_[k];
-                if (L[s] - 1 <= l) continue;
-                const HostCsr& p = systems[s].h->p[l];
-                const HostCsr& r = systems[s].h->r[l];
-                sell_append(sp, p.n_rows, round_up(p.n_rows, 32), p.rp.data(), p.ci.data(), p.va.data(),
-                            nullptr, off[l + 1][s], 0, off[l + 1][s]);
-                sell_append(sr, r.n_rows, round_up(r.n_rows, 32), r.rp.data(), r.ci.data(), r.va.data(),
-                            nullptr, off[l][s], 0, off[l][s]);
-            }
-            auto up = [&](SellBuild& b, DevSell64_32& m) {
-                m.n_slices = static_cast<int>(b.slice.size()) - 1;
-                m.slots = b.slice.back();
-                const int* ds = arena_.upload(b.slice, st);
-                const int* dc = arena_.upload(b.col, st);
-                if (need64_) m.s64 = {ds, dc, arena_.upload(b.val, st)};
-                if (need32_) m.s32 = {ds, dc, arena_.upload(to_float(b.val), st)};
-            };
-            up(sp, d.p);
-            up(sr, d.r);
+            build_op([&](int s) -> const HostCsr& { return systems[s].h->p[l]; }, l + 1, d.p);
+            build_op([&](int s) -> const HostCsr& { return systems[s].h->r[l]; }, l, d.r);
         }
         // vectors (zero-initialised)
         auto vec64 = [&](int n) {
@@ -342,7 +403,8 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
     if (has_amg_) {
         std::vector<int> bsys, brow, bn, blevel;
         std::vector<long long> moff;
-        std::vector<double> mt;
+        std::vector<double> mt, mr;
+        std::vector<int> tblk, trow;
         size_t max_n = 0;
         for (int k = 0; k < n_sys_; ++k) {
             const int s = perm_[k];
@@ -360,9 +422,20 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
             for (int i = 0; i < n; ++i)
                 for (int j = 0; j < n; ++j)
                     mt[o + static_cast<size_t>(j) * n + i] = h.coarse_inverse[static_cast<size_t>(i) * n + j];
+            mr.insert(mr.end(), h.coarse_inverse.begin(), h.coarse_inverse.end());
+            for (int i = 0; i < n; i += kCoarseRows) {
+                tblk.push_back(static_cast<int>(bsys.size()) - 1);
+                trow.push_back(i);
+            }
             max_n = std::max(max_n, static_cast<size_t>(round_up(n, 32)));
         }
         n_blocks_ = static_cast<int>(bsys.size());
+        coarse_bytes_ = 0.0;
+        coarse_rows_ = 0.0;
+        for (int b = 0; b < n_blocks_; ++b) {
+            coarse_bytes_ += 8.0 * bn[b] * static_cast<double>(bn[b]);
+            coarse_rows_ += bn[b];
+        }
         n_single_ = 0;
         for (int k = 0; k < n_sys_; ++k)
             if (systems[perm_[k]].h->levels() == 1) ++n_single_;
@@ -371,6 +444,13 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         cb_.n = arena_.upload(bn, st);
         cb_.m_off = arena_.upload(moff, st);
         cb_.mt = arena_.upload(mt, st);
+        cb_.mr = arena_.upload(mr, st);
+        cb_.tile_blk = arena_.upload(tblk, st);
+        cb_.tile_row = arena_.upload(trow, st);
+        n_ctiles_ = static_cast<int>(tblk.size());
+        n_ctiles_single_ = 0;
+        for (size_t t = 0; t < tblk.size(); ++t)
+            if (tblk[t] >= n_blocks_ - n_single_) ++n_ctiles_single_;
         block_level_ = arena_.upload(blevel, st);
         coarse_smem64_ = max_n * sizeof(double);
         coarse_smem32_ = max_n * sizeof(float);
@@ -413,6 +493,7 @@ void Engine::set_values_device(const double* p0, const double* p1, const double*
     // plain inverse diagonal for Jacobi preconditioning: weight 1
     k_fill_level0<<<grid_of(d.n_rows), 256, 0, stream_>>>(0, d.n_rows, src0_, diag_src0_, vs, 1.0, nullptr,
                                                           nullptr, dinv0_, nullptr);
+    launches_ += 2;
     CFDB_CUDA(cudaGetLastError());
 }
 
@@ -516,12 +597,31 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible) {
     auto P = [&](int l) { return vs_sel<T>(lv_[l].p.s64, lv_[l].p.s32); };
     auto R = [&](int l) { return vs_sel<T>(lv_[l].r.s64, lv_[l].r.s32); };
 
+    const double sv = sizeof(T);
+    const double sb0 = 8.0; // level-0 right-hand side: the FP64 Krylov residual
+    auto spmv_b = [&](const DevSell64_32& m, double rows, double cols) {
+        return static_cast<double>(m.nnz) * (sv + 4.0) + 4.0 * (rows + 1.0) + sv * cols + sv * rows;
+    };
+    // tiles of an operator: one row per warp for CSR operators, slice runs for SELL ones
+    struct Launch {
+        Tiles first;
+        int second; // grid
+        int block;
+    };
+    auto TL = [&](int l, const DevSell64_32& m, bool nc) -> Launch {
+        const DevLevel& d = lv_[l];
+        const int fmt = sizeof(T) == 8 ? m.s64.fmt : m.s32.fmt;
+        if (fmt != kFmtSell) return {d.tiles_f, nc ? d.n_tiles_f_nc : d.n_tiles_f, kFineRows * fmt};
+        return {d.tiles, nc ? d.n_tiles_nc : d.n_tiles, kBlock};
+    };
     std::vector<T*> cur(L, nullptr);
     // ---- down ----
     for (int l = 0; l + 1 < L; ++l) {
         const DevLevel& d = lv_[l];
         const int g = d.n_tiles_nc;
         if (g == 0) continue;
+        const double n = d.n_rows_nc;
+        const double sb = l == 0 ? sb0 : sv;
         T* x = X(l);
         T* y = Y(l);
         T* target = (sweeps_ % 2 == 0) ? x : y;
@@ -530,62 +630,76 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible) {
             CFDB_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * d.n_rows_nc, s));
             cur[l] = x;
         } else {
+            const auto ta = TL(l, d.a, true);
             if (l == 0) {
-                k_vc_first<T, double><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, WD(l), r_, start, sweeps_ >= 2);
+                k_vc_first<T, double><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, start, sweeps_ >= 2);
             } else {
-                k_vc_first<T, T><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, WD(l), Bv(l), start, sweeps_ >= 2);
+                k_vc_first<T, T><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), start, sweeps_ >= 2);
             }
+            mark("smooth_first", l,
+                 sweeps_ >= 2 ? spmv_b(d.a, n, n) - sv * n + sv * n + sb * n : 2.0 * sv * n + sb * n);
             T* c = start;
             for (int k = 2; k < sweeps_; ++k) {
                 T* o = c == x ? y : x;
-                if (l == 0) k_vc_jacobi<T, double><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, WD(l), r_, c, o);
-                else k_vc_jacobi<T, T><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, WD(l), Bv(l), c, o);
+                if (l == 0) k_vc_jacobi<T, double><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, c, o);
+                else k_vc_jacobi<T, T><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), c, o);
+                mark("smooth", l, spmv_b(d.a, n, n) + sv * n + sb * n);
                 c = o;
             }
             cur[l] = c;
         }
-        if (l == 0) k_vc_residual<T, double><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, r_, cur[l], Tv(l));
-        else k_vc_residual<T, T><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, Bv(l), cur[l], Tv(l));
+        const auto tr = TL(l, d.a, true);
+        if (l == 0) k_vc_residual<T, double><<<tr.second, tr.block, 0, s>>>(A(l), tr.first, stv, r_, cur[l], Tv(l));
+        else k_vc_residual<T, T><<<tr.second, tr.block, 0, s>>>(A(l), tr.first, stv, Bv(l), cur[l], Tv(l));
+        mark("residual", l, spmv_b(d.a, n, n) + sb * n);
         const DevLevel& nx = lv_[l + 1];
-        k_vc_spmv<T><<<nx.n_tiles, kBlock, 0, s>>>(R(l), nx.tiles, stv, Tv(l), Bv(l + 1));
+        const auto tq = TL(l + 1, d.r, false);
+        k_vc_spmv<T><<<tq.second, tq.block, 0, s>>>(R(l), tq.first, stv, Tv(l), Bv(l + 1));
+        mark("restrict", l, spmv_b(d.r, nx.n_rows, n));
     }
     // ---- coarsest blocks ----
     // Systems are in descending level count, so single-level systems (coarsest level 0, whose
     // right-hand side is the FP64 Krylov residual) form the last n_single_ blocks.
-    const int first0 = n_blocks_ - n_single_;
+    const int first0 = n_ctiles_ - n_ctiles_single_;
     const Control ctl{n_active_, error_};
+    const int ord = ordered_ ? 1 : 0;
     if (first0 > 0) {
         if constexpr (sizeof(T) == 8) {
             k_vc_coarse<double, double><<<first0, kBlock, coarse_smem64_, s>>>(cb_, stv, b_level64_, x_level64_,
-                                                                               block_level_, ctl);
+                                                                               block_level_, ctl, ord);
         } else {
             k_vc_coarse<float, float><<<first0, kBlock, coarse_smem32_, s>>>(cb_, stv, b_level32_, x_level32_,
-                                                                             block_level_, ctl);
+                                                                             block_level_, ctl, ord);
         }
+        mark("coarse", L - 1, coarse_bytes_ + 2.0 * sv * coarse_rows_);
     }
-    if (first0 < n_blocks_) {
+    if (first0 < n_ctiles_) {
         CoarseBlocks tail = cb_;
-        tail.sys += first0;
-        tail.row += first0;
-        tail.n += first0;
-        tail.m_off += first0;
+        tail.tile_blk += first0;
+        tail.tile_row += first0;
         if constexpr (sizeof(T) == 8) {
-            k_vc_coarse<double, double><<<n_blocks_ - first0, kBlock, coarse_smem64_, s>>>(
-                tail, stv, b_level64_, x_level64_, block_level_ + first0, ctl);
+            k_vc_coarse<double, double><<<n_ctiles_ - first0, kBlock, coarse_smem64_, s>>>(
+                tail, stv, b_level64_, x_level64_, block_level_, ctl, ord);
         } else {
-            k_vc_coarse<double, float><<<n_blocks_ - first0, kBlock, coarse_smem64_, s>>>(
-                tail, stv, b_level64_, x_level32_, block_level_ + first0, ctl);
+            k_vc_coarse<double, float><<<n_ctiles_ - first0, kBlock, coarse_smem64_, s>>>(
+                tail, stv, b_level64_, x_level32_, block_level_, ctl, ord);
         }
+        mark("coarse0", 0, 0.0);
     }
     // ---- up ----
     for (int l = L - 2; l >= 0; --l) {
         const DevLevel& d = lv_[l];
         const int g = d.n_tiles_nc;
         if (g == 0) continue;
+        const double n = d.n_rows_nc;
+        const double sb = l == 0 ? sb0 : sv;
         T* x = X(l);
         T* y = Y(l);
         T* c = cur[l];
-        k_vc_prolong<T><<<g, kBlock, 0, s>>>(P(l), d.tiles, stv, X(l + 1), c);
+        const auto tp = TL(l, d.p, true);
+        k_vc_prolong<T><<<tp.second, tp.block, 0, s>>>(P(l), tp.first, stv, X(l + 1), c);
+        const auto ta = TL(l, d.a, true);
+        mark("prolong", l, spmv_b(d.p, n, lv_[l + 1].n_rows) + sv * n);
         for (int k = 0; k < sweeps_; ++k) {
             T* o = c == x ? y : x;
             const bool last = k + 1 == sweeps_;
@@ -593,10 +707,13 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible) {
                 k_vc_jacobi_final<T><<<g, kBlock, 0, s>>>(A(0), d.tiles, st_, WD(0), r_, c, o, q_, partials_,
                                                           counters_, sys_tile0_, Control{n_active_, error_},
                                                           flexible);
+                mark("smooth_dot", l, spmv_b(d.a, n, n) + sv * n + sb * n + (flexible ? 8.0 * n : 0.0));
             } else if (l == 0) {
-                k_vc_jacobi<T, double><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, WD(l), r_, c, o);
+                k_vc_jacobi<T, double><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, c, o);
+                mark("smooth", l, spmv_b(d.a, n, n) + sv * n + sb * n);
             } else {
-                k_vc_jacobi<T, T><<<g, kBlock, 0, s>>>(A(l), d.tiles, stv, WD(l), Bv(l), c, o);
+                k_vc_jacobi<T, T><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), c, o);
+                mark("smooth", l, spmv_b(d.a, n, n) + sv * n + sb * n);
             }
             c = o;
         }
@@ -612,58 +729,132 @@ void Engine::enqueue_vcycle(Mode mode, bool fused_final, int flexible) {
 void Engine::enqueue_init(Mode mode) {
     const DevLevel& d = lv_[0];
     const Control ctl{n_active_, error_};
+    const double n = d.n_rows;
+    const double a0 = static_cast<double>(d.a.nnz) * 12.0 + 4.0 * (n + 1.0) + 16.0 * n;
     k_cg_init<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, r_, partials_, counters_,
                                                   sys_tile0_, ctl);
+    mark("cg_init", 0, a0 + 16.0 * n);
     const int flexible = mode == Mode::AmgMixed ? 1 : 0;
     if (mode == Mode::Jacobi) {
         k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, q_, partials_,
                                                            counters_, sys_tile0_, ctl, 0);
+        mark("cg_rz", 0, 24.0 * n);
         return;
     }
     enqueue_vcycle(mode, fused_final_, flexible);
-    if (!fused_final_) {
-        if (mode == Mode::AmgMixed) {
-            k_cg_rz<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x32, nullptr, q_, partials_,
-                                                              counters_, sys_tile0_, ctl, flexible);
-        } else {
-            k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, nullptr, q_, partials_,
-                                                               counters_, sys_tile0_, ctl, flexible);
-        }
+    if (!fused_final_) enqueue_rz(mode, flexible);
+}
+
+void Engine::enqueue_rz(Mode mode, int flexible) {
+    const DevLevel& d = lv_[0];
+    const Control ctl{n_active_, error_};
+    const double n = d.n_rows;
+    if (mode == Mode::AmgMixed) {
+        k_cg_rz<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x32, nullptr, q_, partials_,
+                                                          counters_, sys_tile0_, ctl, flexible);
+        mark("cg_rz", 0, 12.0 * n + (flexible ? 8.0 * n : 0.0));
+    } else {
+        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, nullptr, q_, partials_,
+                                                           counters_, sys_tile0_, ctl, flexible);
+        mark("cg_rz", 0, 16.0 * n + (flexible ? 8.0 * n : 0.0));
     }
 }
 
 void Engine::enqueue_iteration(Mode mode) {
     const DevLevel& d = lv_[0];
     const Control ctl{n_active_, error_};
+    const double n = d.n_rows;
+    const double a0 = static_cast<double>(d.a.nnz) * 12.0 + 4.0 * (n + 1.0) + 16.0 * n;
     if (mode == Mode::AmgMixed) {
         k_cg_pupdate<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, d.x32, p_);
+        mark("cg_p_update", 0, 20.0 * n);
     } else {
         k_cg_pupdate<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, d.x64, p_);
+        mark("cg_p_update", 0, 24.0 * n);
     }
     k_cg_spmv_pq<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, p_, q_, partials_, counters_,
                                                      sys_tile0_, ctl);
+    mark("cg_spmv_pq", 0, a0);
     k_cg_xr<<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, x_, r_, p_, q_, partials_, counters_, sys_tile0_,
                                                 ctl, mode == Mode::AmgMixed ? 1 : 0);
+    mark("cg_xr", 0, 48.0 * n);
     if (mode == Mode::AmgMixed) {
         k_cg_true_check<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, r_, partials_,
                                                             counters_, sys_tile0_, ctl);
+        mark("cg_true_check", 0, 0.0);
     }
     const int flexible = mode == Mode::AmgMixed ? 1 : 0;
     if (mode == Mode::Jacobi) {
         k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, q_, partials_,
                                                            counters_, sys_tile0_, ctl, 0);
+        mark("cg_rz", 0, 24.0 * n);
         return;
     }
     enqueue_vcycle(mode, fused_final_, flexible);
-    if (!fused_final_) {
-        if (mode == Mode::AmgMixed) {
-            k_cg_rz<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x32, nullptr, q_, partials_,
-                                                              counters_, sys_tile0_, ctl, flexible);
-        } else {
-            k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, nullptr, q_, partials_,
-                                                               counters_, sys_tile0_, ctl, flexible);
+    if (!fused_final_) enqueue_rz(mode, flexible);
+}
+
+void Engine::mark(const char* name, int level, double bytes) {
+    if (prof_ == nullptr) return;
+    cudaEvent_t e = nullptr;
+    CFDB_CUDA(cudaEventCreate(&e));
+    CFDB_CUDA(cudaEventRecord(e, stream_));
+    ProfRecord r{};
+    std::snprintf(r.name, sizeof(r.name), "%s", name);
+    r.level = level;
+    r.bytes = bytes;
+    prof_->push_back({r, e});
+}
+
+std::vector<ProfRecord> Engine::profile(Mode mode, int reps) {
+    CFDB_CUDA(cudaSetDevice(device_));
+    if (mode != Mode::Jacobi && !has_amg_) fail(5, "profile: no AMG hierarchy set");
+    std::vector<ProfRecord> out;
+    std::vector<int> count;
+    for (int rep = 0; rep < std::max(reps, 1); ++rep) {
+        // every system active, never converging: the profiled kernels do all their work
+        std::vector<SysState> hs(n_sys_);
+        for (auto& t : hs) {
+            std::memset(&t, 0, sizeof(t));
+            t.tol = -1.0;
+            t.max_it = 1 << 30;
+            t.active = 1;
+            t.first = 1;
         }
+        CFDB_CUDA(cudaMemcpyAsync(st_, hs.data(), sizeof(SysState) * n_sys_, cudaMemcpyHostToDevice, stream_));
+        const int n_act = n_sys_;
+        CFDB_CUDA(cudaMemcpyAsync(n_active_, &n_act, sizeof(int), cudaMemcpyHostToDevice, stream_));
+        std::vector<std::pair<ProfRecord, cudaEvent_t>> ev;
+        prof_ = &ev;
+        try {
+            mark("start", 0, 0.0);
+            enqueue_init(mode);
+            mark("iteration_start", 0, 0.0);
+            enqueue_iteration(mode);
+        } catch (...) {
+            prof_ = nullptr;
+            for (auto& e : ev) cudaEventDestroy(e.second);
+            throw;
+        }
+        prof_ = nullptr;
+        CFDB_CUDA(cudaStreamSynchronize(stream_));
+        if (rep == 0) {
+            for (size_t i = 1; i < ev.size(); ++i) out.push_back(ev[i].first);
+            count.assign(out.size(), 0);
+        }
+        for (size_t i = 1; i < ev.size() && i - 1 < out.size(); ++i) {
+            float ms = 0.f;
+            CFDB_CUDA(cudaEventElapsedTime(&ms, ev[i - 1].second, ev[i].second));
+            if (rep > 0 || reps == 1) {
+                out[i - 1].ms += ms;
+                ++count[i - 1];
+            }
+        }
+        for (auto& e : ev) cudaEventDestroy(e.second);
     }
+    for (size_t i = 0; i < out.size(); ++i)
+        if (count[i] > 0) out[i].ms /= count[i];
+    return out;
 }
 
 void Engine::capture_graphs(Mode mode) {
@@ -681,6 +872,17 @@ void Engine::capture_graphs(Mode mode) {
             throw;
         }
         CFDB_CUDA(cudaStreamEndCapture(stream_, &g));
+        size_t n_nodes = 0;
+        CFDB_CUDA(cudaGraphGetNodes(g, nullptr, &n_nodes));
+        std::vector<cudaGraphNode_t> nodes(n_nodes);
+        CFDB_CUDA(cudaGraphGetNodes(g, nodes.data(), &n_nodes));
+        int kernels = 0;
+        for (auto nd : nodes) {
+            cudaGraphNodeType t;
+            CFDB_CUDA(cudaGraphNodeGetType(nd, &t));
+            if (t == cudaGraphNodeTypeKernel) ++kernels;
+        }
+        graph_kernels_[m][which] = kernels;
         cudaGraphExec_t e = nullptr;
         const cudaError_t err = cudaGraphInstantiate(&e, g, 0);
         cudaGraphDestroy(g);
@@ -711,6 +913,7 @@ std::vector<SolveResult> Engine::solve(Mode mode, const std::vector<SolveRequest
     const int n_act = n_sys_;
     CFDB_CUDA(cudaMemcpyAsync(n_active_, &n_act, sizeof(int), cudaMemcpyHostToDevice, stream_));
     CFDB_CUDA(cudaGraphLaunch(graphs_[static_cast<int>(mode)][0], stream_));
+    launches_ += graph_kernels_[static_cast<int>(mode)][0];
     // Iterations: keep one graph launch in flight ahead of the convergence readback.
     cudaEvent_t ev[2];
     CFDB_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
@@ -721,6 +924,7 @@ std::vector<SolveResult> Engine::solve(Mode mode, const std::vector<SolveRequest
     const int cap = max_it + 2;
     while (!done && launched < cap) {
         CFDB_CUDA(cudaGraphLaunch(graphs_[static_cast<int>(mode)][1], stream_));
+        launches_ += graph_kernels_[static_cast<int>(mode)][1];
         CFDB_CUDA(cudaMemcpyAsync(h_pinned_ + 2 * (launched & 1), n_active_, sizeof(int), cudaMemcpyDeviceToHost,
                                   stream_));
         CFDB_CUDA(cudaMemcpyAsync(h_pinned_ + 2 * (launched & 1) + 1, error_, sizeof(int), cudaMemcpyDeviceToHost,
@@ -746,6 +950,7 @@ std::vector<SolveResult> Engine::solve(Mode mode, const std::vector<SolveRequest
     const DevLevel& d = lv_[0];
     k_true_residual<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, partials_, counters_,
                                                         sys_tile0_);
+    ++launches_;
     CFDB_CUDA(cudaGetLastError());
     CFDB_CUDA(cudaMemcpyAsync(hs.data(), st_, sizeof(SysState) * n_sys_, cudaMemcpyDeviceToHost, stream_));
     CFDB_CUDA(cudaStreamSynchronize(stream_));

@@ -29,6 +29,14 @@ struct SolveRequest {
     int max_it = 1000;
 };
 
+// One profiled kernel launch: algorithmic bytes and average device time.
+struct ProfRecord {
+    char name[32];
+    int level;
+    double ms;
+    double bytes;
+};
+
 struct SolveResult {
     int iterations = 0;
     double residual = 0.0;
@@ -82,19 +90,36 @@ public:
     // Kernel timing probe: average device time (ms) of the level-0 FP64/FP32 smoother sweep.
     double time_level0_sweep(bool fp32, int reps);
 
+    // Runs the initial preconditioning and one full iteration eagerly with CUDA events around
+    // every kernel (all systems kept active); returns per-kernel device time averaged over reps
+    // (the first repetition is a warm-up when reps > 1) with the algorithmic bytes of each.
+    std::vector<ProfRecord> profile(Mode mode, int reps);
+
+    // Ordered mode: every operator in SELL with thread-per-row sums in CSR order, so FP64
+    // V-cycles are bit-identical to the reference's sequential host arithmetic. Takes effect
+    // at the next build().
+    void set_ordered(bool on) { ordered_ = on; }
+    // Kernels launched by this engine so far (graph kernel nodes counted per graph launch).
+    [[nodiscard]] unsigned long long kernel_launches() const { return launches_; }
+    [[nodiscard]] bool ordered() const { return ordered_; }
+
 private:
     struct DevSell64_32 {
         Sell<double> s64{};
         Sell<float> s32{};
-        int n_slices = 0;
-        long long slots = 0;
+        int n_slices = 0;     // SELL slices, or CSR rows
+        long long slots = 0;  // stored entries (SELL: with padding)
+        long long nnz = 0;    // algorithmic nonzeros
     };
     struct DevLevel {
         int n_rows = 0;     // all present systems (padded)
         int n_rows_nc = 0;  // prefix of systems that continue to a coarser level
         int n_tiles = 0;
         int n_tiles_nc = 0;
-        Tiles tiles{};
+        Tiles tiles{};       // runs of whole slices (SELL operators, reductions)
+        int n_tiles_f = 0;   // one row per warp (CSR operators)
+        int n_tiles_f_nc = 0;
+        Tiles tiles_f{};
         DevSell64_32 a, p, r;
         double* wd64 = nullptr;
         float* wd32 = nullptr;
@@ -108,6 +133,8 @@ private:
     template <class T> void enqueue_vcycle_t(bool fused_final, int flexible);
     void enqueue_init(Mode mode);
     void enqueue_iteration(Mode mode);
+    void enqueue_rz(Mode mode, int flexible);
+    void mark(const char* name, int level, double bytes);
     void release_graphs();
 
     int device_;
@@ -121,6 +148,9 @@ private:
     bool need32_ = false;
     bool has_amg_ = false;
     bool fused_final_ = true;
+    bool ordered_ = false;
+    std::vector<std::pair<ProfRecord, cudaEvent_t>>* prof_ = nullptr;
+    double coarse_bytes_ = 0.0, coarse_rows_ = 0.0;
 
     // batch order: perm_[k] = original index of the k-th system (sorted by level count)
     std::vector<int> perm_, rank_;
@@ -147,6 +177,7 @@ private:
     // coarse blocks
     int n_blocks_ = 0;
     int n_single_ = 0; // systems whose hierarchy has one level (dense solve on level 0)
+    int n_ctiles_ = 0, n_ctiles_single_ = 0; // coarse-solve tiles (all / single-level suffix)
     CoarseBlocks cb_{};
     int* block_level_ = nullptr;
     double** b_level64_ = nullptr;
@@ -156,6 +187,8 @@ private:
     size_t coarse_smem64_ = 0, coarse_smem32_ = 0;
     // graphs per mode: [mode][0] init, [mode][1] iteration
     cudaGraphExec_t graphs_[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+    int graph_kernels_[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    unsigned long long launches_ = 0;
 };
 
 } // namespace cfdb

@@ -98,6 +98,12 @@ HostCsr spgemm(const HostCsr& a, const HostCsr& b) {
             len[i] = cnt;
         }
     }
+    long long total = 0;
+    for (int i = 0; i < n; ++i) total += len[i];
+    if (total > 0x7fffffffLL) {
+        fail(1, "amg setup: a Galerkin product exceeds 2^31 nonzeros (coarse operators densify; "
+                "lower strength_threshold)");
+    }
     for (int i = 0; i < n; ++i) c.rp[i + 1] = c.rp[i] + len[i];
     c.ci.resize(static_cast<size_t>(c.rp[n]));
     c.va.resize(static_cast<size_t>(c.rp[n]));

@@ -25,10 +25,20 @@ namespace cfdb {
 
 constexpr int kBlock = 256;
 
+// Storage of one sparse operator of a level, selected by `fmt`:
+//  0 (kFmtSell): SELL-32, one thread per row; `slice` = slice offsets. Row sums keep the CSR
+//     order.
+//  G in {2, 4, 8, 16, 32}: CSR with G lanes per row; `slice` = row offsets. Used for wide
+//     coarse-level rows (tens to hundreds of entries), where one thread per row would serialise
+//     long load chains; lanes sum strided entries and combine them with a fixed butterfly
+//     (deterministic, but not the sequential CSR order).
+enum : int { kFmtSell = 0 };
+
 template <class T> struct Sell {
-    const int* slice; // n_slices + 1 slot offsets
+    const int* slice; // SELL: n_slices + 1 slot offsets; CSR: n_rows + 1 row offsets
     const int* col;
     const T* val;
+    int fmt;
 };
 
 struct Tiles {
@@ -126,25 +136,136 @@ __device__ __forceinline__ void deactivate(SysState& st, Control c) {
     atomicSub(c.n_active, 1);
 }
 
-// Row sum of a SELL row: sum_k val[k] * x[col[k]] in CSR order.
-template <class T, class X>
-__device__ __forceinline__ T sell_row(const Sell<T>& m, int row, const X* __restrict__ x) {
+// s + a*b: FP64 rounds the product and the sum separately (reference rounding); FP32 fuses.
+template <class T> __device__ __forceinline__ T madd(T s, T a, T b) {
+    if constexpr (sizeof(T) == 8) return __dadd_rn(s, __dmul_rn(a, b));
+    else return fmaf(a, b, s);
+}
+
+// Row sum of a SELL row: sum_k val[k] * xa(col[k]) in CSR order. Four entries are loaded
+// before they are accumulated so that several loads are in flight per thread.
+template <class T, class XA>
+__device__ __forceinline__ T sell_row_sum(const Sell<T>& m, int row, XA xa) {
     const int slice = row >> 5;
     const int lane = row & 31;
     int k = __ldg(&m.slice[slice]) + lane;
     const int end = __ldg(&m.slice[slice + 1]);
     T s = T(0);
-#pragma unroll 4
-    for (; k < end; k += 32) {
-        const T v = __ldg(&m.val[k]);
-        const int c = __ldg(&m.col[k]);
-        if constexpr (sizeof(T) == 8) {
-            s = __dadd_rn(s, __dmul_rn(v, static_cast<T>(x[c])));
-        } else {
-            s = fmaf(v, static_cast<T>(x[c]), s);
+    for (; k + 96 < end; k += 128) {
+        T v[4], xv[4];
+        int c[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            v[u] = __ldg(&m.val[k + 32 * u]);
+            c[u] = __ldg(&m.col[k + 32 * u]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) xv[u] = xa(c[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s = madd<T>(s, v[u], xv[u]);
+    }
+    for (; k < end; k += 32) s = madd<T>(s, __ldg(&m.val[k]), xa(__ldg(&m.col[k])));
+    return s;
+}
+
+// Two SELL rows of one thread with their loads interleaved (twice the loads in flight); each
+// row is still accumulated in its own CSR order.
+template <class T, class XA>
+__device__ __forceinline__ void sell_row_sum2(const Sell<T>& m, int ra, int rb, XA xa, T& sa, T& sb) {
+    const int la = ra & 31, lb = rb & 31;
+    int ka = __ldg(&m.slice[ra >> 5]) + la;
+    const int ea = __ldg(&m.slice[(ra >> 5) + 1]);
+    int kb = __ldg(&m.slice[rb >> 5]) + lb;
+    const int eb = __ldg(&m.slice[(rb >> 5) + 1]);
+    sa = T(0);
+    sb = T(0);
+    for (; ka + 96 < ea && kb + 96 < eb; ka += 128, kb += 128) {
+        T va[4], vb[4], xa4[4], xb4[4];
+        int ca[4], cb[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            va[u] = __ldg(&m.val[ka + 32 * u]);
+            ca[u] = __ldg(&m.col[ka + 32 * u]);
+            vb[u] = __ldg(&m.val[kb + 32 * u]);
+            cb[u] = __ldg(&m.col[kb + 32 * u]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            xa4[u] = xa(ca[u]);
+            xb4[u] = xa(cb[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            sa = madd<T>(sa, va[u], xa4[u]);
+            sb = madd<T>(sb, vb[u], xb4[u]);
         }
     }
+    for (; ka < ea && kb < eb; ka += 32, kb += 32) {
+        const T v0 = __ldg(&m.val[ka]), v1 = __ldg(&m.val[kb]);
+        const int c0 = __ldg(&m.col[ka]), c1 = __ldg(&m.col[kb]);
+        const T x0 = xa(c0), x1 = xa(c1);
+        sa = madd<T>(sa, v0, x0);
+        sb = madd<T>(sb, v1, x1);
+    }
+    for (; ka < ea; ka += 32) sa = madd<T>(sa, __ldg(&m.val[ka]), xa(__ldg(&m.col[ka])));
+    for (; kb < eb; kb += 32) sb = madd<T>(sb, __ldg(&m.val[kb]), xa(__ldg(&m.col[kb])));
+}
+
+template <class T, class X>
+__device__ __forceinline__ T sell_row(const Sell<T>& m, int row, const X* __restrict__ x) {
+    return sell_row_sum(m, row, [x](int j) { return static_cast<T>(x[j]); });
+}
+
+// CSR row sum by a group of G lanes (G a power of two dividing 32): lane `sub` of the group
+// takes entries sub, sub+G, ..., two at a time; partial sums are combined with a fixed
+// butterfly over the group. Every lane of the group returns the same total. All lanes of the
+// warp must call it (the shuffles use the full mask).
+template <class T, class XA>
+__device__ __forceinline__ T csr_group_sum(const Sell<T>& m, int row, bool valid, int sub, int G, XA xa) {
+    T s = T(0);
+    if (valid) {
+        const int b = __ldg(&m.slice[row]);
+        const int e = __ldg(&m.slice[row + 1]);
+        int k = b + sub;
+        for (; k + G < e; k += 2 * G) {
+            const T v0 = __ldg(&m.val[k]), v1 = __ldg(&m.val[k + G]);
+            const int c0 = __ldg(&m.col[k]), c1 = __ldg(&m.col[k + G]);
+            const T x0 = xa(c0), x1 = xa(c1);
+            s = madd<T>(s, v0, x0);
+            s = madd<T>(s, v1, x1);
+        }
+        if (k < e) s = madd<T>(s, __ldg(&m.val[k]), xa(__ldg(&m.col[k])));
+    }
+    for (int o = G >> 1; o > 0; o >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, o);
     return s;
+}
+
+struct TileCtx;
+
+// Rows of a fine tile (CSR operators): one group of G = fmt lanes per row, blockDim = 8 * G.
+constexpr int kFineRows = 8;
+
+// Calls f(row, sum_j a_row,j xa(j)) for every row of the tile, in the operator's format.
+// SELL: one thread per row, two rows per pass; CSR: one lane group per row.
+template <class T, class XA, class F>
+__device__ __forceinline__ void visit_rows(const Sell<T>& m, int r0, int r1, XA xa, F f) {
+    if (m.fmt == kFmtSell) {
+        int row = r0 + threadIdx.x;
+        for (; row + kBlock < r1; row += 2 * kBlock) {
+            T s0, s1;
+            sell_row_sum2(m, row, row + kBlock, xa, s0, s1);
+            f(row, s0);
+            f(row + kBlock, s1);
+        }
+        if (row < r1) f(row, sell_row_sum(m, row, xa));
+    } else {
+        const int G = m.fmt;
+        const int row = r0 + static_cast<int>(threadIdx.x) / G;
+        const int sub = static_cast<int>(threadIdx.x) & (G - 1);
+        const bool valid = row < r1;
+        const T s = csr_group_sum(m, row, valid, sub, G, xa);
+        if (valid && sub == 0) f(row, s);
+    }
 }
 
 // Tile bookkeeping shared by all tiled kernels.
@@ -226,31 +347,17 @@ static __global__ void __launch_bounds__(kBlock) k_vc_first(Sell<T> a, Tiles til
                                                      int fused2) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
-    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
-        const T wdi = wd[row];
-        const T bi = static_cast<T>(b[row]);
-        T x1;
-        if constexpr (sizeof(T) == 8) x1 = __dadd_rn(0.0, __dmul_rn(wdi, bi));
-        else x1 = wdi * bi;
-        if (!fused2) {
-            y[row] = x1;
-            continue;
-        }
-        const int slice = row >> 5, lane = row & 31;
-        const int end = __ldg(&a.slice[slice + 1]);
-        T s = T(0);
-        for (int k = __ldg(&a.slice[slice]) + lane; k < end; k += 32) {
-            const int j = __ldg(&a.col[k]);
-            const T v = __ldg(&a.val[k]);
-            if constexpr (sizeof(T) == 8) {
-                const T xj = __dadd_rn(0.0, __dmul_rn(wd[j], static_cast<T>(b[j])));
-                s = __dadd_rn(s, __dmul_rn(v, xj));
-            } else {
-                s = fmaf(v, wd[j] * static_cast<T>(b[j]), s);
-            }
-        }
-        y[row] = jac_update<T>(x1, wdi, bi, s);
+    auto x1 = [&](int j) -> T {
+        if constexpr (sizeof(T) == 8) return __dadd_rn(0.0, __dmul_rn(wd[j], static_cast<T>(b[j])));
+        else return wd[j] * static_cast<T>(b[j]);
+    };
+    if (!fused2) {
+        for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) y[row] = x1(row);
+        return;
     }
+    visit_rows(a, c.r0, c.r1, x1, [&](int row, T s) {
+        y[row] = jac_update<T>(x1(row), wd[row], static_cast<T>(b[row]), s);
+    });
 }
 
 // y = x + wd (b - A x)
@@ -261,10 +368,9 @@ static __global__ void __launch_bounds__(kBlock) k_vc_jacobi(Sell<T> a, Tiles ti
                                                       const T* __restrict__ x, T* __restrict__ y) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
-    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
-        const T s = sell_row(a, row, x);
+    visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
         y[row] = jac_update<T>(x[row], wd[row], static_cast<T>(b[row]), s);
-    }
+    });
 }
 
 // t = b - A x
@@ -275,11 +381,10 @@ static __global__ void __launch_bounds__(kBlock) k_vc_residual(Sell<T> a, Tiles 
                                                         T* __restrict__ t) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
-    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
-        const T s = sell_row(a, row, x);
+    visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
         if constexpr (sizeof(T) == 8) t[row] = __dsub_rn(static_cast<T>(b[row]), s);
         else t[row] = static_cast<T>(b[row]) - s;
-    }
+    });
 }
 
 // y = M x (restriction into the next level's right-hand side)
@@ -288,7 +393,7 @@ static __global__ void __launch_bounds__(kBlock) k_vc_spmv(Sell<T> m, Tiles tile
                                                     const T* __restrict__ x, T* __restrict__ y) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
-    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) y[row] = sell_row(m, row, x);
+    visit_rows(m, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) { y[row] = s; });
 }
 
 // x += P xc
@@ -298,25 +403,33 @@ static __global__ void __launch_bounds__(kBlock) k_vc_prolong(Sell<T> p, Tiles t
                                                        T* __restrict__ x) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
-    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
-        const T s = sell_row(p, row, xc);
+    visit_rows(p, c.r0, c.r1, [xc](int j) { return xc[j]; }, [&](int row, T s) {
         if constexpr (sizeof(T) == 8) x[row] = __dadd_rn(x[row], s);
         else x[row] = x[row] + s;
-    }
+    });
 }
 
 // ---- coarsest level: x = M b with the dense FP64 inverse (krylov_cuda.cu:298-307) ----
-// One CTA per coarse block. b is staged into shared memory with a TMA bulk copy (1-D,
-// cp.async.bulk, no multicast); every thread computes rows with a column-major (transposed)
-// inverse, so a warp's loads of one column are coalesced and each row sum keeps the reference
-// order j = 0..n-1.
+// Work is split into tiles of kCoarseRows rows of one coarse block, one CTA each. Each CTA
+// stages its block's right-hand side into shared memory with a TMA bulk copy (1-D
+// cp.async.bulk, no multicast) and then
+//  * ordered mode: one thread per row walks j = 0..n-1 in the reference order over the
+//    column-major copy of the inverse (a warp's loads of one column are coalesced), eight
+//    columns loaded ahead of the dependent sum;
+//  * default: one warp per row over the row-major inverse (lanes stride the row, coalesced),
+//    partial sums combined with a fixed butterfly.
+
+constexpr int kCoarseRows = kBlock / 32;
 
 struct CoarseBlocks {
-    const int* sys;      // system of each block
-    const int* row;      // first row of the block in its level's vectors
-    const int* n;        // block size
-    const long long* m_off; // offset of the block's transposed inverse in `mt`
-    const double* mt;
+    const int* sys;          // system of each block
+    const int* row;          // first row of the block in its level's vectors
+    const int* n;            // block size
+    const long long* m_off;  // offset of the block's inverse in `mt` / `mr`
+    const double* mt;        // column-major (transposed) inverses
+    const double* mr;        // row-major inverses
+    const int* tile_blk;     // block of each tile
+    const int* tile_row;     // first row (within the block) of each tile
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -328,16 +441,17 @@ static __global__ void __launch_bounds__(kBlock) k_vc_coarse(CoarseBlocks cb, co
                                                       const TB* const* __restrict__ b_level,
                                                       TX* const* __restrict__ x_level,
                                                       const int* __restrict__ block_level,
-                                                      Control ctl) {
+                                                      Control ctl, int ordered) {
     using T = TB;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar;
-    const int blk = blockIdx.x;
+    const int blk = cb.tile_blk[blockIdx.x];
     const int s = cb.sys[blk];
     if (st != nullptr && *((volatile const int*)&st[s].active) == 0) return;
     const int lvl = block_level[blk];
     const int r0 = cb.row[blk];
     const int n = cb.n[blk];
+    const int i0 = cb.tile_row[blockIdx.x];
     const T* b = b_level[lvl] + r0;
     TX* x = x_level[lvl] + r0;
     T* bs = reinterpret_cast<T*>(smem_raw);
@@ -376,14 +490,32 @@ static __global__ void __launch_bounds__(kBlock) k_vc_coarse(CoarseBlocks cb, co
         if (threadIdx.x == 0) atomicExch(ctl.error, 1);
         return;
     }
-    const double* mt = cb.mt + cb.m_off[blk];
-    for (int i = threadIdx.x; i < n; i += kBlock) {
+    if (ordered) {
+        const int i = i0 + threadIdx.x;
+        if (threadIdx.x >= kCoarseRows || i >= n) return;
+        const double* mt = cb.mt + cb.m_off[blk];
         double acc = 0.0;
-        for (int j = 0; j < n; ++j) {
-            acc = __dadd_rn(acc, __dmul_rn(__ldg(&mt[static_cast<long long>(j) * n + i]),
-                                           static_cast<double>(bs[j])));
+        int j = 0;
+        for (; j + 8 <= n; j += 8) {
+            double m[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) m[u] = __ldg(&mt[static_cast<long long>(j + u) * n + i]);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) acc = __dadd_rn(acc, __dmul_rn(m[u], static_cast<double>(bs[j + u])));
         }
+        for (; j < n; ++j)
+            acc = __dadd_rn(acc, __dmul_rn(__ldg(&mt[static_cast<long long>(j) * n + i]), static_cast<double>(bs[j])));
         x[i] = static_cast<TX>(acc);
+    } else {
+        const int i = i0 + (threadIdx.x >> 5);
+        const int lane = threadIdx.x & 31;
+        if (i >= n) return;
+        const double* mr = cb.mr + cb.m_off[blk] + static_cast<long long>(i) * n;
+        double acc = 0.0;
+        for (int j = lane; j < n; j += 32) acc = __dadd_rn(acc, __dmul_rn(__ldg(&mr[j]), static_cast<double>(bs[j])));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xffffffffu, acc, o));
+        if (lane == 0) x[i] = static_cast<TX>(acc);
     }
 }
 
@@ -401,11 +533,11 @@ static __global__ void __launch_bounds__(kBlock) k_cg_init(Sell<double> a, Tiles
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     double rr = 0.0, unused = 0.0;
-    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
-        const double ri = __dsub_rn(b[row], sell_row(a, row, x));
+    visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, double ax) {
+        const double ri = __dsub_rn(b[row], ax);
         r[row] = ri;
         rr = __dadd_rn(rr, __dmul_rn(ri, ri));
-    }
+    });
     if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
         SysState& s = st[c.s];
         s.res = sqrt(rr);
@@ -445,11 +577,10 @@ static __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(Sell<double> a, Ti
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     double pq = 0.0, unused = 0.0;
-    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
-        const double qi = sell_row(a, row, p);
+    visit_rows(a, c.r0, c.r1, [p](int j) { return p[j]; }, [&](int row, double qi) {
         q[row] = qi;
         pq = __dadd_rn(pq, __dmul_rn(p[row], qi));
-    }
+    });
     if (reduce_system(pq, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
         SysState& s = st[c.s];
         s.first = 0;
@@ -509,11 +640,11 @@ static __global__ void __launch_bounds__(kBlock) k_cg_true_check(Sell<double> a,
     if (!tile_begin(tiles, st, c)) return;
     if (st[c.s].check == 0) return;
     double rr = 0.0, unused = 0.0;
-    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
-        const double ri = __dsub_rn(b[row], sell_row(a, row, x));
+    visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, double ax) {
+        const double ri = __dsub_rn(b[row], ax);
         r[row] = ri;
         rr = __dadd_rn(rr, __dmul_rn(ri, ri));
-    }
+    });
     if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
         SysState& s = st[c.s];
         s.check = 0;
@@ -564,15 +695,14 @@ static __global__ void __launch_bounds__(kBlock) k_vc_jacobi_final(Sell<T> a, Ti
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     double rz = 0.0, zq = 0.0;
-    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
-        const T s = sell_row(a, row, x);
+    visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
         const double ri = r[row];
         const T zi = jac_update<T>(x[row], wd[row], static_cast<T>(ri), s);
         z[row] = zi;
         const double zd = static_cast<double>(zi);
         rz = __dadd_rn(rz, __dmul_rn(ri, zd));
         if (flexible) zq = __dadd_rn(zq, __dmul_rn(zd, q[row]));
-    }
+    });
     if (reduce_system(rz, zq, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
         precond_tail(st[c.s], rz, zq, flexible, ctl);
     }
@@ -616,10 +746,10 @@ static __global__ void __launch_bounds__(kBlock) k_true_residual(Sell<double> a,
     TileCtx c;
     tile_begin(tiles, nullptr, c);
     double rr = 0.0, unused = 0.0;
-    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
-        const double ri = __dsub_rn(b[row], sell_row(a, row, x));
+    visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, double ax) {
+        const double ri = __dsub_rn(b[row], ax);
         rr = __dadd_rn(rr, __dmul_rn(ri, ri));
-    }
+    });
     if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
         st[c.s].true_res = sqrt(rr);
     }
@@ -642,6 +772,41 @@ static __global__ void k_assemble_faces(int nf, const double* __restrict__ flux,
     const double neg = fl < 0.0 ? __dmul_rn(convection, fl) : 0.0;
     upper[f] = __dsub_rn(neg, g);
     lower[f] = __dsub_rn(-pos, g);
+}
+
+// Pressure assembly epilogue fused into the cell gather (flow_solver.cpp:768-770 and 794-796):
+// diag = diag0 + sum of face coefficients, source = source0 - div(flux), then
+// set_reference(ref_cell, ref_value): source += diag * value, diag += diag.
+static __global__ void k_assemble_pressure_cells(int n, const int* __restrict__ cf_ptr,
+                                                 const int* __restrict__ cf_face,
+                                                 const double* __restrict__ flux,
+                                                 const double* __restrict__ gamma,
+                                                 const double* __restrict__ delta,
+                                                 const int* __restrict__ owner,
+                                                 const double* __restrict__ diag0,
+                                                 const double* __restrict__ source0, int ref_cell,
+                                                 double ref_value, double* __restrict__ diag,
+                                                 double* __restrict__ source) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    double d = diag0 != nullptr ? diag0[c] : 0.0;
+    double v = 0.0;
+    const int end = cf_ptr[c + 1];
+    for (int k = cf_ptr[c]; k < end; ++k) {
+        const int f = cf_face[k];
+        const double fl = flux[f];
+        const double g = __dmul_rn(gamma[f], delta[f]);
+        d = __dadd_rn(d, __dadd_rn(0.0, g));
+        if (owner[f] == c) v = __dadd_rn(v, fl);
+        else v = __dsub_rn(v, fl);
+    }
+    double src = __dsub_rn(source0[c], v);
+    if (c == ref_cell) {
+        src = __dadd_rn(src, __dmul_rn(d, ref_value));
+        d = __dadd_rn(d, d);
+    }
+    diag[c] = d;
+    source[c] = src;
 }
 
 static __global__ void k_assemble_cells(int n, const int* __restrict__ cf_ptr,

@@ -191,6 +191,40 @@ int cfdb_system_assemble_device(cfdb_system* sys, const double* flux, const doub
  * V-cycle z = M^-1 r with zero initial guess on the installed hierarchy and the current
  * matrix (set by the last solve), in the system's precision. Host arrays. */
 int cfdb_system_apply_amg(cfdb_system* sys, const double* r, double* z);
+/* Ordered arithmetic: every level operator stored for thread-per-row sums in the CSR column
+ * order, so FP64 V-cycles are bit-identical to the reference's sequential host arithmetic
+ * (slower on wide coarse levels). Default off: wide coarse rows use warp-per-row sums. */
+int cfdb_system_set_ordered(cfdb_system* sys, int ordered);
+
+/* Per-kernel device time of the initial preconditioning plus one iteration (events around
+ * every kernel, averaged over reps after one warm-up), with each kernel's algorithmic bytes. */
+typedef struct {
+    char name[32];
+    int level;
+    double ms;
+    double bytes;
+} cfdb_kernel_record;
+int cfdb_system_profile(cfdb_system* sys, int use_amg, int reps, cfdb_kernel_record* records,
+                        int max_records, int* n_records);
+
+/* cfdb_system_assemble_device with host arrays (the reference's assemble call on a persistent
+ * mesh: inputs copied to the device, results copied back). */
+int cfdb_system_assemble(cfdb_system* sys, const double* flux, const double* gamma,
+                         const double* delta_coeff, double convection, double* upper,
+                         double* lower, double* diag, double* divergence);
+/* The whole pressure-equation assembly of FlowSolver::pressure_correction for internal faces
+ * on device arrays (flow_solver.cpp:757-796, convection 0): upper = lower = -gamma*delta,
+ * diag = diag0 + sum of gamma*delta (diag0 may be NULL: zero), source = source0 - div(flux),
+ * then set_reference(ref_cell, ref_value) unless ref_cell < 0. Requires
+ * cfdb_system_create_mesh. */
+int cfdb_system_assemble_pressure_device(cfdb_system* sys, const double* flux,
+                                         const double* gamma, const double* delta_coeff,
+                                         const double* diag0, const double* source0,
+                                         int ref_cell, double ref_value, double* upper,
+                                         double* lower, double* diag, double* source);
+/* Number of this library's kernels the system has launched so far (graph nodes included). */
+int cfdb_system_kernel_launches(const cfdb_system* sys, unsigned long long* count);
+
 /* Stream of the system (cudaStream_t as void*), for callers that order their own work. */
 int cfdb_system_stream(const cfdb_system* sys, void** stream);
 /* Device bytes held by the system (pattern, hierarchy, work vectors). */

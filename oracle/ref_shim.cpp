@@ -127,6 +127,61 @@ int ref_device_solver_solve(int n, int nf, int nnz, const int* row_ptr, const in
     }
 }
 
+// Persistent cfd::gpu::DeviceSolver, as LduMatrix::solve_persistent keeps it in its AmgCache
+// (ldu_matrix.cpp:302-312): created once per pattern, hierarchy installed on (re)build, then
+// solve() per pressure solve.
+void* ref_ds_create(int n, int nf, int nnz, const int* row_ptr, const int* col, const int* diag_pos,
+                    const int* upper_pos, const int* lower_pos) {
+    try {
+        const cfd::gpu::LduPattern pt{n, nf, nnz, row_ptr, col, diag_pos, upper_pos, lower_pos};
+        return new cfd::gpu::DeviceSolver(pt);
+    } catch (const std::exception&) {
+        return nullptr;
+    }
+}
+
+int ref_ds_set_amg(void* h, int n_levels, const RefCsr* a, const RefCsr* p, const RefCsr* r,
+                   const double* coarse_inverse, int sweeps, double weight) {
+    try {
+        cfd::gpu::AmgView v;
+        for (int l = 0; l < n_levels; ++l) {
+            cfd::gpu::AmgLevelView lv;
+            lv.a = l == 0 ? cfd::gpu::CsrView{} : view(a[l]);
+            if (l + 1 < n_levels) {
+                lv.p = view(p[l]);
+                lv.r = view(r[l]);
+            }
+            v.levels.push_back(lv);
+        }
+        v.coarse_inverse = coarse_inverse;
+        v.smooth_sweeps = sweeps;
+        v.jacobi_weight = weight;
+        static_cast<cfd::gpu::DeviceSolver*>(h)->set_amg(v);
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
+int ref_ds_solve(void* h, const double* diag, const double* upper, const double* lower,
+                 const double* b, double* x, int method, int use_amg, double tol, int max_iter,
+                 int* iters, double* res, int* conv) {
+    try {
+        const auto st = static_cast<cfd::gpu::DeviceSolver*>(h)->solve(
+            diag, upper, lower, b, x,
+            method == 0 ? cfd::gpu::Method::Cg : cfd::gpu::Method::BiCgStab, use_amg != 0,
+            {tol, max_iter});
+        put(st, iters, res, conv);
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
+void ref_ds_destroy(void* h) {
+    delete static_cast<cfd::gpu::DeviceSolver*>(h);
+}
+
 int ref_backend_is_host() {
     return cfd::gpu::backend_name() == "host" ? 1 : 0;
 }

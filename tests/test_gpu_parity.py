@@ -96,6 +96,7 @@ def test_vcycle_bitwise(gpu, make):
     up, lo, diag, src = _assembled(case)
     pat, a, h = _hierarchy(case, up, lo, diag)
     ds = cb.DeviceSolver(_pattern(cb, pat))
+    ds.set_ordered(True)
     ds.set_amg(_view(cb, h))
     x = np.zeros(case.n)
     ds.solve(diag, up, lo, src, x, cb.Method.Cg, True, cb.SolveControl(1e300, 1))  # installs A
@@ -124,6 +125,23 @@ def test_amg_pcg_matches_oracle(gpu, make):
     assert tr <= 1.05 * tol and abs(tr - st.true_residual) <= 1e-6 * tol
     # solutions agree to the solver tolerance (relative to the solution scale)
     assert np.linalg.norm(x - xo) <= 1e-5 * np.linalg.norm(xo)
+
+
+@pytest.mark.parametrize("make", CASES, ids=["cavity12", "graded16", "tet8"])
+def test_vcycle_fast_mode_close(gpu, make):
+    """Default (warp-per-row sums on wide coarse levels): V-cycle agrees to FP64 round-off."""
+    cb = gpu
+    case = make()
+    up, lo, diag, src = _assembled(case)
+    pat, a, h = _hierarchy(case, up, lo, diag)
+    ds = cb.DeviceSolver(_pattern(cb, pat))
+    ds.set_amg(_view(cb, h))
+    x = np.zeros(case.n)
+    ds.solve(diag, up, lo, src, x, cb.Method.Cg, True, cb.SolveControl(1e300, 1))
+    r = np.random.default_rng(8).standard_normal(case.n)
+    z = ds.apply_amg(r)
+    zr = O.vcycle_apply(h.a, h.p, h.r, h.coarse_inverse, r, 2, 0.7)
+    assert np.linalg.norm(z - zr) <= 1e-12 * np.linalg.norm(zr)
 
 
 def test_solve_amg_cg_oneshot(gpu):

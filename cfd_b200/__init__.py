@@ -85,6 +85,8 @@ _proto("cfdb_assemble_device", [_i, _i, _vp, _vp, _vp, _vp, _vp, _d, _vp, _vp, _
 _proto("cfdb_solve", [_P(CsrStruct), _pd, _pd, _i, _P(ControlStruct), _P(StatsStruct)])
 _proto("cfdb_solve_amg_cg", [_P(AmgViewStruct), _pd, _pd, _P(ControlStruct), _P(StatsStruct)])
 _proto("cfdb_build_pattern", [_i, _i, _pi, _pi, _pi, _pi, _pi, _pi, _pi, _pi])
+_proto("cfdb_solve_device_noalloc", [_P(CsrStruct), _vp, _vp, _i, _P(ControlStruct),
+                                     _P(StatsStruct)])
 _proto("cfdb_amg_setup", [_P(CsrStruct), _P(AmgSettingsStruct), _P(_vp)])
 _proto("cfdb_hierarchy_destroy", [_vp])
 _proto("cfdb_hierarchy_levels", [_vp, _pi])
@@ -399,6 +401,20 @@ def solve_amg_cg(amg: AmgView, b, x, control: SolveControl) -> SolveStats:
     st = StatsStruct()
     v, ctl = amg._c(), control._c()
     _check(_lib.cfdb_solve_amg_cg(C.byref(v), _dp(b), _dp(x), C.byref(ctl), C.byref(st)))
+    return SolveStats._from(st)
+
+
+def solve_device_noalloc(n, nnz, row_ptr, col, val, b, x, method: Method,
+                         control: SolveControl) -> SolveStats:
+    """Jacobi-preconditioned CG that allocates no device memory: every array is the caller's
+    device memory (torch CUDA tensors or raw pointers), work vectors live in the library's
+    static device array (at most 65,536 rows). For callers that cannot call cudaMalloc."""
+    cs = CsrStruct(int(n), int(nnz), C.cast(_devptr(row_ptr), _pi), C.cast(_devptr(col), _pi),
+                   C.cast(_devptr(val), _pd))
+    st = StatsStruct()
+    ctl = control._c()
+    _check(_lib.cfdb_solve_device_noalloc(C.byref(cs), _devptr(b), _devptr(x), int(method),
+                                          C.byref(ctl), C.byref(st)))
     return SolveStats._from(st)
 
 

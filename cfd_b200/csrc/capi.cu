@@ -99,6 +99,11 @@ std::shared_ptr<Hierarchy> hierarchy_from(const cfdb_amg_view& v, int n0, bool s
 
 } // namespace
 
+namespace cfdb {
+// Records the calling thread's last error message (used by entry points in other files).
+void set_thread_error(const std::string& msg) { g_last_error = msg; }
+} // namespace cfdb
+
 // ------------------------------------------------------------------------------------------------
 // system object
 // ------------------------------------------------------------------------------------------------

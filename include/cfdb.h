@@ -128,6 +128,18 @@ int cfdb_solve(const cfdb_csr* a, const double* b, double* x, int method,
 int cfdb_solve_amg_cg(const cfdb_amg_view* amg, const double* b, double* x,
                       const cfdb_control* control, cfdb_stats* stats);
 
+/* Allocation-free Jacobi-preconditioned CG (no counterpart in the reference). For callers that
+ * cannot call cudaMalloc -- a host application that owns all device memory through its own
+ * pool, or a latency-critical loop that must not stall on the allocator. The matrix (CSR),
+ * b and x (initial guess in, solution out) are the caller's device arrays; the work vectors
+ * live in one static device array of the library, so at most 65,536 rows (larger n is
+ * rejected with CFDB_ERR_BAD_ARG). The first call on each device resolves that array's address
+ * and should come before any stream capture. Calls share the array: calls that overlap on the
+ * GPU race. Same iteration and stopping rule as cfdb_solve; runs on the legacy default
+ * stream and returns when the solve is done. */
+int cfdb_solve_device_noalloc(const cfdb_csr* a, const double* b, double* x, int method,
+                              const cfdb_control* control, cfdb_stats* stats);
+
 /* ---- CSR pattern: fv::build_csr_pattern (src/fv/src/ldu_matrix.cpp:572-612) ----
  * col, upper_pos, lower_pos sized n + 2*n_faces / n_faces; returns nnz in *nnz. */
 int cfdb_build_pattern(int n, int n_faces, const int* owner, const int* neighbour,

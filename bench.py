@@ -235,6 +235,7 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
     import torch
 
     import cfd_b200 as cb
+    from cfd_b200.multi import replica_summary
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -298,10 +299,7 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
             ms = e0.elapsed_time(e1)
             launches = ds.kernel_launches() - launches0
             clocks = sampler.stop() if sampler else None
-        if world > 1:
-            tm = torch.tensor([ms], device=dev)
-            torch.distributed.all_reduce(tm, op=torch.distributed.ReduceOp.MAX)
-            ms = float(tm.item())
+        ms, _ = replica_summary(ms, args.steps, world)
         worst = max(s.true_residual for s in stats) / bnorm_ref
         assert all(s.converged for s in stats) and worst <= 1e-8, (k, worst)
         results[k] = dict(ms=ms, stats=stats, launches=launches, clocks=clocks,

@@ -62,6 +62,10 @@ class PatternStruct(C.Structure):
                 ("diag_pos", _pi), ("upper_pos", _pi), ("lower_pos", _pi)]
 
 
+class KernelRecordStruct(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("level", _i), ("ms", _d), ("bytes", _d)]
+
+
 class AmgSettingsStruct(C.Structure):
     _fields_ = [("strength_threshold", _d), ("max_levels", _i), ("coarse_size", _i),
                 ("smooth_sweeps", _i), ("jacobi_weight", _d)]
@@ -115,8 +119,27 @@ _proto("cfdb_system_assemble_pressure_device", [_vp, _vp, _vp, _vp, _vp, _vp, _i
 _proto("cfdb_system_kernel_launches", [_vp, _P(C.c_ulonglong)])
 
 
-class KernelRecordStruct(C.Structure):
-    _fields_ = [("name", C.c_char * 32), ("level", _i), ("ms", _d), ("bytes", _d)]
+class TuningStruct(C.Structure):
+    _fields_ = [("target_tiles", _i), ("wide_row", _i), ("lanes_div", _i), ("fuse_first", _i)]
+
+
+_proto("cfdb_default_tuning", [_P(TuningStruct)], None)
+_proto("cfdb_system_set_tuning", [_vp, _P(TuningStruct)])
+_proto("cfdb_batch_create", [_i, _pi, _pi, _pi, _pi, _P(_vp)])
+_proto("cfdb_batch_destroy", [_vp])
+_proto("cfdb_batch_sizes", [_vp, _P(C.c_longlong), _P(C.c_longlong)])
+_proto("cfdb_batch_setup_amg", [_vp, _pd, _pd, _pd, _P(AmgSettingsStruct)])
+_proto("cfdb_batch_set_precision", [_vp, _i])
+_proto("cfdb_batch_set_tuning", [_vp, _P(TuningStruct)])
+_proto("cfdb_batch_assemble_pressure_device", [_vp, _vp, _vp, _vp, _vp, _pi, _d, _vp, _vp, _vp,
+                                               _vp])
+_proto("cfdb_batch_solve_device", [_vp, _vp, _vp, _vp, _vp, _vp, _i, _P(ControlStruct),
+                                   _P(StatsStruct)])
+_proto("cfdb_batch_profile", [_vp, _i, _P(KernelRecordStruct), _i, _pi])
+_proto("cfdb_batch_stream", [_vp, _P(_vp)])
+_proto("cfdb_batch_device_bytes", [_vp, _P(_sz)])
+_proto("cfdb_batch_kernel_launches", [_vp, _P(C.c_ulonglong)])
+
 
 
 _proto("cfdb_system_profile", [_vp, _i, _i, _P(KernelRecordStruct), _i, _pi])
@@ -649,6 +672,105 @@ class DeviceSolver:
         b = C.c_size_t()
         _check(_lib.cfdb_system_device_bytes(self._h, C.byref(b)))
         return b.value
+
+
+@dataclass
+class Tuning:
+    """Launch-shape / schedule knobs of the device plan (cfdb_tuning)."""
+    target_tiles: int = 148 * 8
+    wide_row: int = 24
+    lanes_div: int = 6
+    fuse_first: int = 1
+
+    def _c(self):
+        return TuningStruct(int(self.target_tiles), int(self.wide_row), int(self.lanes_div),
+                            int(self.fuse_first))
+
+
+def _set_system_tuning(self, t: Tuning) -> None:
+    ts = t._c()
+    _check(_lib.cfdb_system_set_tuning(self._h, C.byref(ts)))
+
+
+DeviceSolver.set_tuning = _set_system_tuning
+
+
+def _profile_records(fn, handle, *args):
+    recs = (KernelRecordStruct * 1024)()
+    n = C.c_int()
+    _check(fn(handle, *args, recs, 1024, C.byref(n)))
+    return [(recs[i].name.decode(), recs[i].level, recs[i].ms, recs[i].bytes) for i in range(n.value)]
+
+
+class Batch:
+    """Many independent pressure systems of uneven size solved in one device plan: every
+    kernel launch covers all systems, with per-system convergence and dot products. Arrays
+    are concatenated in system order (cells of system 0, then 1, ...; faces likewise);
+    owner / neighbour hold local cell indices."""
+
+    def __init__(self, n_cells, n_faces, owner, neighbour):
+        nc, nf = _i32(n_cells), _i32(n_faces)
+        own, nei = _i32(owner), _i32(neighbour)
+        if len(nc) != len(nf) or len(own) != int(nf.sum()) or len(nei) != int(nf.sum()):
+            raise InvalidArgument("batch: inconsistent sizes")
+        h = _vp()
+        _check(_lib.cfdb_batch_create(len(nc), _ip(nc), _ip(nf), _ip(own), _ip(nei), C.byref(h)))
+        self._h = h
+        self.n_systems = len(nc)
+        self.n_cells, self.n_faces = nc, nf
+        self.total_cells, self.total_faces = int(nc.sum()), int(nf.sum())
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.cfdb_batch_destroy(h)
+            self._h = None
+
+    __del__ = close
+
+    def setup_amg(self, diag, upper, lower, settings: AmgSettings | None = None) -> None:
+        s = (settings or AmgSettings())._c()
+        _check(_lib.cfdb_batch_setup_amg(self._h, _dp(_f64(diag)), _dp(_f64(upper)),
+                                         _dp(_f64(lower)), C.byref(s)))
+
+    def set_precision(self, precision: Precision) -> None:
+        _check(_lib.cfdb_batch_set_precision(self._h, int(precision)))
+
+    def set_tuning(self, t: Tuning) -> None:
+        ts = t._c()
+        _check(_lib.cfdb_batch_set_tuning(self._h, C.byref(ts)))
+
+    def assemble_pressure_device(self, flux, gamma, delta, source0, upper, lower, diag, source,
+                                 ref_cells=None, ref_value=0.0) -> None:
+        refs = _i32(ref_cells if ref_cells is not None else np.zeros(self.n_systems))
+        _check(_lib.cfdb_batch_assemble_pressure_device(
+            self._h, _devptr(flux), _devptr(gamma), _devptr(delta), _devptr(source0), _ip(refs),
+            float(ref_value), _devptr(upper), _devptr(lower), _devptr(diag), _devptr(source)))
+
+    def solve_device(self, diag, upper, lower, rhs, x, controls, use_amg=True):
+        ctl = (ControlStruct * self.n_systems)(*[c._c() for c in controls])
+        st = (StatsStruct * self.n_systems)()
+        _check(_lib.cfdb_batch_solve_device(self._h, _devptr(diag), _devptr(upper), _devptr(lower),
+                                            _devptr(rhs), _devptr(x), 1 if use_amg else 0, ctl, st))
+        return [SolveStats._from(st[i]) for i in range(self.n_systems)]
+
+    def profile(self, reps: int = 3) -> list:
+        return _profile_records(_lib.cfdb_batch_profile, self._h, int(reps))
+
+    def stream(self) -> int:
+        s = _vp()
+        _check(_lib.cfdb_batch_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def device_bytes(self) -> int:
+        b = C.c_size_t()
+        _check(_lib.cfdb_batch_device_bytes(self._h, C.byref(b)))
+        return b.value
+
+    def kernel_launches(self) -> int:
+        c = C.c_ulonglong()
+        _check(_lib.cfdb_batch_kernel_launches(self._h, C.byref(c)))
+        return c.value
 
 
 # -------------------------------------------------------------------------------------------

@@ -856,7 +856,7 @@ int cfdb_system_assemble_pressure_device(cfdb_system* sys, const double* flux, c
         }
         k_assemble_pressure_cells<<<(n + 255) / 256, 256, 0, st>>>(n, sys->d_cf_ptr, sys->d_cf_face, flux, gamma,
                                                                    delta, sys->d_owner, diag0, source0, ref_cell,
-                                                                   ref_value, diag, source);
+                                                                   nullptr, ref_value, diag, source);
         ++sys->launches;
         CFDB_CUDA(cudaGetLastError());
     });
@@ -866,6 +866,34 @@ int cfdb_system_kernel_launches(const cfdb_system* sys, unsigned long long* coun
     if (sys == nullptr || count == nullptr) return set_error(CFDB_ERR_BAD_ARG, "null argument");
     *count = sys->launches + (sys->eng ? sys->eng->kernel_launches() : 0);
     return CFDB_OK;
+}
+
+void cfdb_default_tuning(cfdb_tuning* t) {
+    if (t == nullptr) return;
+    const Tuning d{};
+    t->target_tiles = d.target_tiles;
+    t->wide_row = d.wide_row;
+    t->lanes_div = d.lanes_div;
+    t->fuse_first = d.fuse_first;
+}
+
+static Tuning tuning_from(const cfdb_tuning* t) {
+    if (t == nullptr) fail(CFDB_ERR_BAD_ARG, "null tuning");
+    if (t->target_tiles < 1 || t->wide_row < 0 || t->lanes_div < 1)
+        fail(CFDB_ERR_BAD_ARG, "tuning values out of range");
+    return Tuning{t->target_tiles, t->wide_row, t->lanes_div, t->fuse_first != 0 ? 1 : 0};
+}
+
+int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t) {
+    return guarded([&] {
+        if (sys == nullptr) fail(CFDB_ERR_BAD_ARG, "null system");
+        const Tuning tu = tuning_from(t);
+        CFDB_CUDA(cudaSetDevice(sys->device));
+        ensure_engine(sys);
+        sys->eng->set_tuning(tu);
+        sys->dirty = true;
+        ensure_engine(sys);
+    });
 }
 
 int cfdb_system_stream(const cfdb_system* sys, void** stream) {

@@ -11,8 +11,6 @@ namespace cfdb {
 
 namespace {
 
-constexpr int kTargetTiles = 148 * 8; // 148 SMs x 8 resident 256-thread CTAs
-constexpr int kWideRow = 24;          // average entries per row above which CSR/warp-per-row is used
 
 // SELL-32 under construction on the host.
 struct SellBuild {
@@ -208,7 +206,7 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
     std::vector<int> sys_tile0(n_sys_ + 1, 0);
     for (int l = 0; l < n_levels_; ++l) {
         DevLevel& d = lv_[l];
-        const int base = std::max(256, round_up(ceil_div(std::max(d.n_rows, 1), kTargetTiles), 256));
+        const int base = std::max(256, round_up(ceil_div(std::max(d.n_rows, 1), std::max(tuning_.target_tiles, 1)), 256));
         std::vector<int> trow, tsys;
         int nc_tiles = -1;
         for (int k = 0; k < n_sys_; ++k) {
@@ -259,10 +257,10 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
                 static_cast<int>(sp.diag_src.size()) != sp.n) {
                 fail(1, "engine: level-0 value map size mismatch");
             }
-            sell_append(sb, sp.n, round_up(sp.n, 32), sp.rp, sp.ci, nullptr, sp.src.data(), off[0][s],
-                        vs_off_[s], off[0][s]);
-            for (int i = 0; i < sp.n; ++i)
-                dsrc[off[0][s] + i] = sp.diag_src[i] >= 0 ? sp.diag_src[i] + vs_off_[s] : -1;
+            const int so = sp.absolute_src ? 0 : vs_off_[s];
+            sell_append(sb, sp.n, round_up(sp.n, 32), sp.rp, sp.ci, nullptr, sp.src.data(), off[0][s], so,
+                        off[0][s]);
+            for (int i = 0; i < sp.n; ++i) dsrc[off[0][s] + i] = sp.diag_src[i] >= 0 ? sp.diag_src[i] + so : -1;
         }
         DevLevel& d = lv_[0];
         d.a.n_slices = static_cast<int>(sb.slice.size()) - 1;
@@ -276,6 +274,14 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         d.a.nnz = nnz0;
         src0_ = arena_.upload(sb.src, st);
         diag_src0_ = arena_.upload(dsrc, st);
+        std::vector<int> rmap(static_cast<size_t>(lv_[0].n_rows), -1);
+        long long uo = 0;
+        for (int s = 0; s < n_sys_; ++s) {
+            for (int i = 0; i < systems[s].n; ++i) rmap[off[0][s] + i] = static_cast<int>(uo + i);
+            uo += systems[s].n;
+        }
+        user_rows_ = uo;
+        row_map_ = arena_.upload(rmap, st);
         d.wd64 = arena_.alloc<double>(d.n_rows);
         if (need32_) d.wd32 = arena_.alloc<float>(d.n_rows);
         dinv0_ = arena_.alloc<double>(d.n_rows);
@@ -297,8 +303,9 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
             }
             // lanes per row: about six entries per lane, 8..32 lanes
             const double avg = rows > 0 ? static_cast<double>(nnz) / static_cast<double>(rows) : 0.0;
-            const int lanes = avg > 128.0 ? 32 : avg > 64.0 ? 16 : 8;
-            const bool wide = !ordered_ && rows > 0 && avg > kWideRow;
+            int lanes = 4;
+            while (lanes < 32 && lanes * std::max(tuning_.lanes_div, 1) < avg) lanes *= 2;
+            const bool wide = !ordered_ && rows > 0 && avg > tuning_.wide_row;
             if (wide) {
                 CsrBuild cbd;
                 for (int k = 0; k < n_sys_; ++k) {
@@ -397,7 +404,8 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         error_ = arena_.alloc<int>(1);
         CFDB_CUDA(cudaMemsetAsync(error_, 0, sizeof(int), st));
     }
-    // coarse blocks
+    // coarse blocks (one per system with two or more levels; single-level systems are
+    // Jacobi-preconditioned and have none)
     n_blocks_ = 0;
     fused_final_ = has_amg_ && sweeps_ > 0;
     if (has_amg_) {
@@ -410,7 +418,10 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
             const int s = perm_[k];
             const Hierarchy& h = *systems[s].h;
             const int c = h.levels() - 1;
-            if (c == 0) fused_final_ = false;
+            if (c == 0) {
+                fused_final_ = false; // their r.z comes from k_cg_rz
+                continue;
+            }
             const int n = h.n_c;
             bsys.push_back(k);
             brow.push_back(off[c][s]);
@@ -439,6 +450,8 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         n_single_ = 0;
         for (int k = 0; k < n_sys_; ++k)
             if (systems[perm_[k]].h->levels() == 1) ++n_single_;
+        single_.assign(n_sys_, 0);
+        for (int s = 0; s < n_sys_; ++s) single_[s] = systems[s].h->levels() == 1 ? 1 : 0;
         cb_.sys = arena_.upload(bsys, st);
         cb_.row = arena_.upload(brow, st);
         cb_.n = arena_.upload(bn, st);
@@ -448,9 +461,6 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         cb_.tile_blk = arena_.upload(tblk, st);
         cb_.tile_row = arena_.upload(trow, st);
         n_ctiles_ = static_cast<int>(tblk.size());
-        n_ctiles_single_ = 0;
-        for (size_t t = 0; t < tblk.size(); ++t)
-            if (tblk[t] >= n_blocks_ - n_single_) ++n_ctiles_single_;
         block_level_ = arena_.upload(blevel, st);
         coarse_smem64_ = max_n * sizeof(double);
         coarse_smem32_ = max_n * sizeof(float);
@@ -530,6 +540,22 @@ void Engine::upload_values_device_concat(const std::vector<const double*>& dev_s
     set_values_device(vs_, vs_, vs_, INT_MAX, INT_MAX);
 }
 
+void Engine::set_rhs_guess_concat(const double* b, const double* x0) {
+    const int n = lv_[0].n_rows;
+    k_gather_rows<<<grid_of(n), 256, 0, stream_>>>(n, row_map_, b, b_);
+    k_gather_rows<<<grid_of(n), 256, 0, stream_>>>(n, row_map_, x0, x_);
+    launches_ += 2;
+    CFDB_CUDA(cudaGetLastError());
+}
+
+void Engine::get_solution_concat(double* x) {
+    const int n = lv_[0].n_rows;
+    k_scatter_rows<<<grid_of(n), 256, 0, stream_>>>(n, row_map_, x_, x);
+    ++launches_;
+    CFDB_CUDA(cudaGetLastError());
+    CFDB_CUDA(cudaStreamSynchronize(stream_));
+}
+
 void Engine::set_rhs(int s, const double* b, bool dev) {
     CFDB_CUDA(cudaMemcpyAsync(b_ + off0_[s], b, sizeof(double) * n_of_[s],
                               dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
@@ -584,7 +610,8 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible) {
     const SysState* stv = st_;
     const int L = n_levels_;
     // final pre-smoothing buffer so that after `sweeps_` post sweeps the iterate lands in x
-    const int writes_pre = sweeps_ >= 2 ? sweeps_ - 1 : sweeps_;
+    const bool fuse = sweeps_ >= 2 && tuning_.fuse_first != 0;
+    const int writes_pre = fuse ? sweeps_ - 1 : sweeps_;
     auto X = [&](int l) { return vx<T>(lv_[l].x64, lv_[l].x32); };
     auto Y = [&](int l) { return vx<T>(lv_[l].y64, lv_[l].y32); };
     auto Tv = [&](int l) { return vx<T>(lv_[l].t64, lv_[l].t32); };
@@ -632,14 +659,13 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible) {
         } else {
             const auto ta = TL(l, d.a, true);
             if (l == 0) {
-                k_vc_first<T, double><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, start, sweeps_ >= 2);
+                k_vc_first<T, double><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, start, fuse);
             } else {
-                k_vc_first<T, T><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), start, sweeps_ >= 2);
+                k_vc_first<T, T><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), start, fuse);
             }
-            mark("smooth_first", l,
-                 sweeps_ >= 2 ? spmv_b(d.a, n, n) - sv * n + sv * n + sb * n : 2.0 * sv * n + sb * n);
+            mark("smooth_first", l, fuse ? spmv_b(d.a, n, n) - sv * n + sv * n + sb * n : 2.0 * sv * n + sb * n);
             T* c = start;
-            for (int k = 2; k < sweeps_; ++k) {
+            for (int k = fuse ? 2 : 1; k < sweeps_; ++k) {
                 T* o = c == x ? y : x;
                 if (l == 0) k_vc_jacobi<T, double><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, c, o);
                 else k_vc_jacobi<T, T><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), c, o);
@@ -657,34 +683,18 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible) {
         k_vc_spmv<T><<<tq.second, tq.block, 0, s>>>(R(l), tq.first, stv, Tv(l), Bv(l + 1));
         mark("restrict", l, spmv_b(d.r, nx.n_rows, n));
     }
-    // ---- coarsest blocks ----
-    // Systems are in descending level count, so single-level systems (coarsest level 0, whose
-    // right-hand side is the FP64 Krylov residual) form the last n_single_ blocks.
-    const int first0 = n_ctiles_ - n_ctiles_single_;
+    // ---- coarsest blocks (dense inverse of each multi-level system's coarsest operator) ----
     const Control ctl{n_active_, error_};
     const int ord = ordered_ ? 1 : 0;
-    if (first0 > 0) {
+    if (n_ctiles_ > 0) {
         if constexpr (sizeof(T) == 8) {
-            k_vc_coarse<double, double><<<first0, kBlock, coarse_smem64_, s>>>(cb_, stv, b_level64_, x_level64_,
-                                                                               block_level_, ctl, ord);
+            k_vc_coarse<double, double><<<n_ctiles_, kBlock, coarse_smem64_, s>>>(cb_, stv, b_level64_, x_level64_,
+                                                                                  block_level_, ctl, ord);
         } else {
-            k_vc_coarse<float, float><<<first0, kBlock, coarse_smem32_, s>>>(cb_, stv, b_level32_, x_level32_,
-                                                                             block_level_, ctl, ord);
+            k_vc_coarse<float, float><<<n_ctiles_, kBlock, coarse_smem32_, s>>>(cb_, stv, b_level32_, x_level32_,
+                                                                                block_level_, ctl, ord);
         }
         mark("coarse", L - 1, coarse_bytes_ + 2.0 * sv * coarse_rows_);
-    }
-    if (first0 < n_ctiles_) {
-        CoarseBlocks tail = cb_;
-        tail.tile_blk += first0;
-        tail.tile_row += first0;
-        if constexpr (sizeof(T) == 8) {
-            k_vc_coarse<double, double><<<n_ctiles_ - first0, kBlock, coarse_smem64_, s>>>(
-                tail, stv, b_level64_, x_level64_, block_level_, ctl, ord);
-        } else {
-            k_vc_coarse<double, float><<<n_ctiles_ - first0, kBlock, coarse_smem64_, s>>>(
-                tail, stv, b_level64_, x_level32_, block_level_, ctl, ord);
-        }
-        mark("coarse0", 0, 0.0);
     }
     // ---- up ----
     for (int l = L - 2; l >= 0; --l) {
@@ -736,7 +746,7 @@ void Engine::enqueue_init(Mode mode) {
     mark("cg_init", 0, a0 + 16.0 * n);
     const int flexible = mode == Mode::AmgMixed ? 1 : 0;
     if (mode == Mode::Jacobi) {
-        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, q_, partials_,
+        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, nullptr, q_, partials_,
                                                            counters_, sys_tile0_, ctl, 0);
         mark("cg_rz", 0, 24.0 * n);
         return;
@@ -750,11 +760,11 @@ void Engine::enqueue_rz(Mode mode, int flexible) {
     const Control ctl{n_active_, error_};
     const double n = d.n_rows;
     if (mode == Mode::AmgMixed) {
-        k_cg_rz<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x32, nullptr, q_, partials_,
+        k_cg_rz<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x32, nullptr, dinv0_, q_, partials_,
                                                           counters_, sys_tile0_, ctl, flexible);
         mark("cg_rz", 0, 12.0 * n + (flexible ? 8.0 * n : 0.0));
     } else {
-        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, nullptr, q_, partials_,
+        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, nullptr, dinv0_, q_, partials_,
                                                            counters_, sys_tile0_, ctl, flexible);
         mark("cg_rz", 0, 16.0 * n + (flexible ? 8.0 * n : 0.0));
     }
@@ -766,10 +776,10 @@ void Engine::enqueue_iteration(Mode mode) {
     const double n = d.n_rows;
     const double a0 = static_cast<double>(d.a.nnz) * 12.0 + 4.0 * (n + 1.0) + 16.0 * n;
     if (mode == Mode::AmgMixed) {
-        k_cg_pupdate<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, d.x32, p_);
+        k_cg_pupdate<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, d.x32, r_, dinv0_, p_);
         mark("cg_p_update", 0, 20.0 * n);
     } else {
-        k_cg_pupdate<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, d.x64, p_);
+        k_cg_pupdate<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, d.x64, r_, dinv0_, p_);
         mark("cg_p_update", 0, 24.0 * n);
     }
     k_cg_spmv_pq<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, p_, q_, partials_, counters_,
@@ -785,7 +795,7 @@ void Engine::enqueue_iteration(Mode mode) {
     }
     const int flexible = mode == Mode::AmgMixed ? 1 : 0;
     if (mode == Mode::Jacobi) {
-        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, q_, partials_,
+        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, nullptr, q_, partials_,
                                                            counters_, sys_tile0_, ctl, 0);
         mark("cg_rz", 0, 24.0 * n);
         return;
@@ -814,12 +824,14 @@ std::vector<ProfRecord> Engine::profile(Mode mode, int reps) {
     for (int rep = 0; rep < std::max(reps, 1); ++rep) {
         // every system active, never converging: the profiled kernels do all their work
         std::vector<SysState> hs(n_sys_);
-        for (auto& t : hs) {
+        for (int s = 0; s < n_sys_; ++s) {
+            SysState& t = hs[rank_[s]];
             std::memset(&t, 0, sizeof(t));
             t.tol = -1.0;
             t.max_it = 1 << 30;
             t.active = 1;
             t.first = 1;
+            t.jacobi = mode != Mode::Jacobi && !single_.empty() && single_[s] ? 1 : 0;
         }
         CFDB_CUDA(cudaMemcpyAsync(st_, hs.data(), sizeof(SysState) * n_sys_, cudaMemcpyHostToDevice, stream_));
         const int n_act = n_sys_;
@@ -906,6 +918,7 @@ std::vector<SolveResult> Engine::solve(Mode mode, const std::vector<SolveRequest
         t.max_it = req[s].max_it;
         t.active = 1;
         t.first = 1;
+        t.jacobi = mode != Mode::Jacobi && !single_.empty() && single_[s] ? 1 : 0;
         max_it = std::max(max_it, req[s].max_it);
     }
     capture_graphs(mode);

@@ -21,7 +21,17 @@ struct SystemSpec {
     std::vector<int> src;             // per pattern entry: index into this system's value source
     std::vector<int> diag_src;        // per row: value-source index of the diagonal, or -1
     int vs_len = 0;                   // length of this system's value source
+    bool absolute_src = false;        // src already indexes the batch-wide value source
     std::shared_ptr<const Hierarchy> h; // levels >= 1, transfers, coarse inverse (null: none)
+};
+
+// Launch-shape and schedule knobs (no effect on the arithmetic of a row sum except that wide
+// operators switch between the ordered SELL sum and the lane-group CSR sum).
+struct Tuning {
+    int target_tiles = 148 * 8; // SELL tiles (CTAs of 256 threads) per level
+    int wide_row = 24;          // average row length above which CSR lane groups are used
+    int lanes_div = 6;          // lanes per CSR row ~ average row length / lanes_div (4..32)
+    int fuse_first = 1;         // first two smoothing sweeps in one kernel (x1 recomputed)
 };
 
 struct SolveRequest {
@@ -99,6 +109,15 @@ public:
     // V-cycles are bit-identical to the reference's sequential host arithmetic. Takes effect
     // at the next build().
     void set_ordered(bool on) { ordered_ = on; }
+    void set_tuning(const Tuning& t) { tuning_ = t; }
+    [[nodiscard]] const Tuning& tuning() const { return tuning_; }
+
+    // Batch vectors in the caller's order (systems concatenated, no padding), device arrays:
+    // gathers b and the initial guess (x0 == nullptr: zero) into the engine layout, scatters
+    // the solution back.
+    void set_rhs_guess_concat(const double* b, const double* x0);
+    void get_solution_concat(double* x);
+    [[nodiscard]] long long user_rows() const { return user_rows_; }
     // Kernels launched by this engine so far (graph kernel nodes counted per graph launch).
     [[nodiscard]] unsigned long long kernel_launches() const { return launches_; }
     [[nodiscard]] bool ordered() const { return ordered_; }
@@ -149,6 +168,9 @@ private:
     bool has_amg_ = false;
     bool fused_final_ = true;
     bool ordered_ = false;
+    Tuning tuning_{};
+    int* row_map_ = nullptr;       // per level-0 row: index in the caller's concatenated vectors, -1 padding
+    long long user_rows_ = 0;
     std::vector<std::pair<ProfRecord, cudaEvent_t>>* prof_ = nullptr;
     double coarse_bytes_ = 0.0, coarse_rows_ = 0.0;
 
@@ -176,8 +198,9 @@ private:
     int* h_pinned_ = nullptr; // [0] n_active, [1] error
     // coarse blocks
     int n_blocks_ = 0;
-    int n_single_ = 0; // systems whose hierarchy has one level (dense solve on level 0)
-    int n_ctiles_ = 0, n_ctiles_single_ = 0; // coarse-solve tiles (all / single-level suffix)
+    int n_single_ = 0;        // systems whose hierarchy has one level (Jacobi-preconditioned CG)
+    std::vector<int> single_; // per original system: 1 if its hierarchy has one level
+    int n_ctiles_ = 0;        // coarse-solve tiles
     CoarseBlocks cb_{};
     int* block_level_ = nullptr;
     double** b_level64_ = nullptr;

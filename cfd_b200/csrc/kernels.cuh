@@ -64,7 +64,8 @@ struct SysState {
     int phase;        // 0: initial preconditioning, 1: inside the loop
     int check;        // mixed precision: recursive residual met the target, verify in FP64
     int breakdown;    // p.q == 0 or rho == 0 style exits
-    int pad;
+    int jacobi;       // single-level hierarchy: Jacobi-preconditioned FP64 CG (z = r / diag), as
+                      // ldu_matrix.cpp:357 solves a system whose hierarchy has one level
 };
 
 struct Control {
@@ -324,6 +325,25 @@ static __global__ void k_fill_level0(int n_slots, int n_rows, const int* __restr
     }
 }
 
+// Engine layout <-> caller's concatenated vectors (map[i] = caller index of engine row i, or -1).
+static __global__ void k_gather_rows(int n, const int* __restrict__ map, const double* __restrict__ src,
+                                     double* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int s = map[i];
+        dst[i] = (s >= 0 && src != nullptr) ? src[s] : 0.0;
+    }
+}
+
+static __global__ void k_scatter_rows(int n, const int* __restrict__ map, const double* __restrict__ src,
+                                      double* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int s = map[i];
+        if (s >= 0) dst[s] = src[i];
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // V-cycle kernels (krylov_kernels.inc:182-238, krylov_cuda.cu:392-408)
 // T: arithmetic of the cycle (double: reference, float: mixed). B: type of the right-hand side
@@ -553,17 +573,21 @@ static __global__ void __launch_bounds__(kBlock) k_cg_init(Sell<double> a, Tiles
     }
 }
 
-// p = z (first) or p = z + beta p
+// p = z (first) or p = z + beta p. Jacobi systems recompute z = r * jac0 (r has not changed
+// since their r.z), which keeps their z in FP64 whatever the precision of `z`.
 template <class Z>
 static __global__ void __launch_bounds__(kBlock) k_cg_pupdate(Tiles tiles, const SysState* st,
                                                        const Z* __restrict__ z,
+                                                       const double* __restrict__ r,
+                                                       const double* __restrict__ jac0,
                                                        double* __restrict__ p) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     const bool first = st[c.s].first != 0;
+    const bool jsys = st[c.s].jacobi != 0;
     const double beta = st[c.s].beta;
     for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
-        const double zi = static_cast<double>(z[row]);
+        const double zi = jsys ? __dmul_rn(r[row], jac0[row]) : static_cast<double>(z[row]);
         p[row] = first ? zi : __dadd_rn(zi, __dmul_rn(beta, p[row]));
     }
 }
@@ -617,7 +641,7 @@ static __global__ void __launch_bounds__(kBlock) k_cg_xr(Tiles tiles, SysState* 
         SysState& s = st[c.s];
         s.res = sqrt(rr);
         if (s.res <= s.tol) {
-            if (verify_true) {
+            if (verify_true && !s.jacobi) {
                 s.check = 1;
             } else {
                 s.converged = 1;
@@ -709,16 +733,20 @@ static __global__ void __launch_bounds__(kBlock) k_vc_jacobi_final(Sell<T> a, Ti
 }
 
 // Unfused r.z (and z.q) when the preconditioner output is not produced by a smoothing sweep
-// (no smoothing, single-level systems, Jacobi preconditioning: z = dinv * r when jac != null).
+// (no smoothing; Jacobi preconditioning z = dinv * r for every system when jac != null, or for
+// the systems flagged `jacobi` (jac0, z not stored: k_cg_pupdate recomputes it)).
 template <class Z>
 static __global__ void __launch_bounds__(kBlock) k_cg_rz(Tiles tiles, SysState* st,
                                                   const double* __restrict__ r,
                                                   Z* __restrict__ z, const double* __restrict__ jac,
+                                                  const double* __restrict__ jac0,
                                                   const double* __restrict__ q, double* partials,
                                                   int* counters, const int* sys_tile0,
                                                   Control ctl, int flexible) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
+    const bool jsys = st[c.s].jacobi != 0;
+    const int flex = jsys ? 0 : flexible;
     double rz = 0.0, zq = 0.0;
     for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
         const double ri = r[row];
@@ -726,14 +754,16 @@ static __global__ void __launch_bounds__(kBlock) k_cg_rz(Tiles tiles, SysState* 
         if (jac != nullptr) {
             zd = __dmul_rn(ri, jac[row]);
             z[row] = static_cast<Z>(zd);
+        } else if (jsys) {
+            zd = __dmul_rn(ri, jac0[row]);
         } else {
             zd = static_cast<double>(z[row]);
         }
         rz = __dadd_rn(rz, __dmul_rn(ri, zd));
-        if (flexible) zq = __dadd_rn(zq, __dmul_rn(zd, q[row]));
+        if (flex) zq = __dadd_rn(zq, __dmul_rn(zd, q[row]));
     }
     if (reduce_system(rz, zq, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
-        precond_tail(st[c.s], rz, zq, flexible, ctl);
+        precond_tail(st[c.s], rz, zq, flex, ctl);
     }
 }
 
@@ -776,7 +806,8 @@ static __global__ void k_assemble_faces(int nf, const double* __restrict__ flux,
 
 // Pressure assembly epilogue fused into the cell gather (flow_solver.cpp:768-770 and 794-796):
 // diag = diag0 + sum of face coefficients, source = source0 - div(flux), then
-// set_reference(ref_cell, ref_value): source += diag * value, diag += diag.
+// set_reference(ref_cell, ref_value): source += diag * value, diag += diag (for the cell
+// ref_cell, or every cell flagged in ref_mask when batches carry one reference per system).
 static __global__ void k_assemble_pressure_cells(int n, const int* __restrict__ cf_ptr,
                                                  const int* __restrict__ cf_face,
                                                  const double* __restrict__ flux,
@@ -785,7 +816,8 @@ static __global__ void k_assemble_pressure_cells(int n, const int* __restrict__ 
                                                  const int* __restrict__ owner,
                                                  const double* __restrict__ diag0,
                                                  const double* __restrict__ source0, int ref_cell,
-                                                 double ref_value, double* __restrict__ diag,
+                                                 const int* __restrict__ ref_mask, double ref_value,
+                                                 double* __restrict__ diag,
                                                  double* __restrict__ source) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
@@ -801,7 +833,7 @@ static __global__ void k_assemble_pressure_cells(int n, const int* __restrict__ 
         else v = __dsub_rn(v, fl);
     }
     double src = __dsub_rn(source0[c], v);
-    if (c == ref_cell) {
+    if (c == ref_cell || (ref_mask != nullptr && ref_mask[c] != 0)) {
         src = __dadd_rn(src, __dmul_rn(d, ref_value));
         d = __dadd_rn(d, d);
     }

@@ -1,0 +1,415 @@
+// Serving loop for pressure solves (declared in include/cfdb_serve.h).
+//
+// Requests (a registered mesh, LDU coefficients, right-hand side) are queued at submit time and
+// taken by worker slots as soon as a slot is free: continuous batching at the request level.
+// Every mesh owns one resident persistent system (pattern, hierarchy, device copies of the last
+// matrix / right-hand side / solution, its own CUDA stream), so requests on different meshes run
+// concurrently and overlap on the GPU; requests on one mesh are serialised on its system.
+// Residency is bounded by an HBM budget: a system is admitted only when its (estimated, then
+// measured) device footprint fits next to the resident ones, evicting idle systems in
+// least-recently-used order; requests that do not fit wait in the queue until memory frees up.
+#include "../../include/cfdb_serve.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "common.hpp"
+
+namespace cfdb {
+void set_thread_error(const std::string& msg); // capi.cu
+}
+
+using cfdb::fail;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Mesh {
+    int n = 0, nf = 0;
+    std::vector<int> owner, neighbour;
+};
+
+struct Resident {
+    cfdb_system* sys = nullptr;
+    size_t bytes = 0;
+    double *d_diag = nullptr, *d_upper = nullptr, *d_lower = nullptr, *d_rhs = nullptr, *d_x = nullptr;
+    long long matrix_key = -1;   // key of the LDU values on the device
+    long long solution_key = -1; // key of the matrix the device solution belongs to
+    int age = 0;                 // solves since the hierarchy was built
+    bool busy = false;
+    Clock::time_point last_use{};
+};
+
+struct Request {
+    long long ticket = 0;
+    int mesh = 0;
+    long long key = 0;
+    bool warm = false;
+    double rel_tol = 1e-8;
+    int max_iter = 500;
+    std::vector<double> diag, upper, lower, rhs;
+    Clock::time_point submitted{}, started{}, finished{};
+    std::vector<double> x;
+    cfdb_stats stats{};
+    int status = CFDB_OK;
+    std::string error;
+    bool done = false;
+};
+
+} // namespace
+
+struct cfdb_server {
+    cfdb_server_config cfg{};
+    int device = 0;
+    Clock::time_point t0{};
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    bool stopping = false;
+    std::vector<Mesh> meshes;
+    std::unordered_map<int, std::unique_ptr<Resident>> resident;
+    size_t resident_bytes = 0;
+    std::deque<std::shared_ptr<Request>> queue;
+    std::map<long long, std::shared_ptr<Request>> tickets;
+    long long next_ticket = 1;
+    std::vector<std::thread> workers;
+    long long completed = 0;
+    long long evictions = 0;
+};
+
+namespace {
+
+size_t estimate_bytes(const cfdb_server& s, const Mesh& m) {
+    // measured footprint of the persistent systems: about 800 bytes per cell (hierarchy, SELL
+    // copies, Krylov vectors) plus the server's device copies of one matrix and three vectors
+    const size_t per_cell = s.cfg.precision == CFDB_PRECISION_MIXED ? 700 : 800;
+    return per_cell * static_cast<size_t>(m.n) + sizeof(double) * (static_cast<size_t>(m.n) * 3 + 2 * static_cast<size_t>(m.nf) + m.n);
+}
+
+void release(cfdb_server& s, Resident& r) {
+    if (r.sys != nullptr) cfdb_system_destroy(r.sys);
+    for (double* p : {r.d_diag, r.d_upper, r.d_lower, r.d_rhs, r.d_x})
+        if (p != nullptr) cudaFree(p);
+    s.resident_bytes -= std::min(s.resident_bytes, r.bytes);
+    r = Resident{};
+}
+
+// Frees idle resident systems (least recently used first) until `need` more bytes fit.
+// Called with the lock held. Returns whether the request fits now.
+bool make_room(cfdb_server& s, size_t need, int keep_mesh) {
+    const size_t budget = static_cast<size_t>(s.cfg.hbm_budget_bytes);
+    while (s.resident_bytes + need > budget) {
+        int victim = -1;
+        Clock::time_point oldest = Clock::time_point::max();
+        for (auto& kv : s.resident) {
+            if (kv.first == keep_mesh || kv.second->busy || kv.second->sys == nullptr) continue;
+            if (kv.second->last_use < oldest) {
+                oldest = kv.second->last_use;
+                victim = kv.first;
+            }
+        }
+        if (victim < 0) return false;
+        release(s, *s.resident[victim]);
+        s.resident.erase(victim);
+        ++s.evictions;
+    }
+    return true;
+}
+
+void check(int rc) {
+    if (rc != CFDB_OK) {
+        char buf[1024];
+        cfdb_last_error(buf, sizeof(buf));
+        throw cfdb::Error(rc, buf);
+    }
+}
+
+void dmalloc(double** p, size_t n) {
+    const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), sizeof(double) * std::max<size_t>(n, 1));
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        fail(CFDB_ERR_OOM, std::string("server: device allocation failed: ") + cudaGetErrorString(e));
+    }
+}
+
+// Runs one request on its (locked) resident system. No server lock held.
+void execute(cfdb_server& s, Resident& r, const Mesh& m, Request& q, bool created) {
+    cudaSetDevice(s.device);
+    if (created) {
+        check(cfdb_system_create_mesh(m.n, m.nf, m.owner.data(), m.neighbour.data(), &r.sys));
+        check(cfdb_system_set_precision(r.sys, s.cfg.precision));
+        dmalloc(&r.d_diag, m.n);
+        dmalloc(&r.d_upper, m.nf);
+        dmalloc(&r.d_lower, m.nf);
+        dmalloc(&r.d_rhs, m.n);
+        dmalloc(&r.d_x, m.n);
+    }
+    void* stream_v = nullptr;
+    check(cfdb_system_stream(r.sys, &stream_v));
+    cudaStream_t st = static_cast<cudaStream_t>(stream_v);
+    const bool new_matrix = r.matrix_key != q.key || q.key < 0;
+    if (created || (s.cfg.max_age > 0 && r.age >= s.cfg.max_age)) {
+        // hierarchy (re)build from this request's matrix, as the reference's AmgCache does
+        check(cfdb_system_setup_amg(r.sys, q.diag.data(), q.upper.data(), q.lower.data(), &s.cfg.settings));
+        r.age = 0;
+    }
+    if (new_matrix) {
+        CFDB_CUDA(cudaMemcpyAsync(r.d_diag, q.diag.data(), sizeof(double) * m.n, cudaMemcpyHostToDevice, st));
+        if (m.nf > 0) {
+            CFDB_CUDA(cudaMemcpyAsync(r.d_upper, q.upper.data(), sizeof(double) * m.nf, cudaMemcpyHostToDevice, st));
+            CFDB_CUDA(cudaMemcpyAsync(r.d_lower, q.lower.data(), sizeof(double) * m.nf, cudaMemcpyHostToDevice, st));
+        }
+        r.matrix_key = q.key;
+    }
+    CFDB_CUDA(cudaMemcpyAsync(r.d_rhs, q.rhs.data(), sizeof(double) * m.n, cudaMemcpyHostToDevice, st));
+    if (!(q.warm && r.solution_key == q.key && q.key >= 0)) {
+        CFDB_CUDA(cudaMemsetAsync(r.d_x, 0, sizeof(double) * m.n, st));
+    }
+    double bn = 0.0;
+    for (double v : q.rhs) bn += v * v;
+    const cfdb_control ctl{q.rel_tol * std::sqrt(bn), q.max_iter};
+    check(cfdb_system_solve_device(r.sys, r.d_diag, r.d_upper, r.d_lower, r.d_rhs, r.d_x, CFDB_METHOD_CG, 1, &ctl,
+                                   &q.stats));
+    r.solution_key = q.key;
+    ++r.age;
+    q.x.resize(m.n);
+    CFDB_CUDA(cudaMemcpyAsync(q.x.data(), r.d_x, sizeof(double) * m.n, cudaMemcpyDeviceToHost, st));
+    CFDB_CUDA(cudaStreamSynchronize(st));
+}
+
+void worker_loop(cfdb_server* sp) {
+    cfdb_server& s = *sp;
+    cudaSetDevice(s.device);
+    std::unique_lock<std::mutex> lk(s.mu);
+    for (;;) {
+        // first queued request whose mesh is idle and whose system is resident or fits
+        std::shared_ptr<Request> q;
+        Resident* r = nullptr;
+        bool created = false;
+        for (;;) {
+            if (s.stopping && s.queue.empty()) return;
+            for (auto it = s.queue.begin(); it != s.queue.end(); ++it) {
+                auto& cand = *it;
+                auto rit = s.resident.find(cand->mesh);
+                if (rit != s.resident.end()) {
+                    if (rit->second->busy) continue;
+                    r = rit->second.get();
+                    created = r->sys == nullptr;
+                } else {
+                    const size_t need = estimate_bytes(s, s.meshes[cand->mesh]);
+                    if (!make_room(s, need, cand->mesh)) continue;
+                    auto res = std::make_unique<Resident>();
+                    res->bytes = need;
+                    s.resident_bytes += need;
+                    r = res.get();
+                    s.resident[cand->mesh] = std::move(res);
+                    created = true;
+                }
+                q = cand;
+                s.queue.erase(it);
+                break;
+            }
+            if (q) break;
+            s.cv_work.wait(lk);
+        }
+        r->busy = true;
+        q->started = Clock::now();
+        lk.unlock();
+        try {
+            execute(s, *r, s.meshes[q->mesh], *q, created);
+        } catch (const cfdb::Error& e) {
+            q->status = e.code;
+            q->error = e.what();
+        } catch (const std::exception& e) {
+            q->status = CFDB_ERR_INTERNAL;
+            q->error = e.what();
+        }
+        q->finished = Clock::now();
+        lk.lock();
+        if (created && r->sys != nullptr) {
+            size_t b = 0;
+            cfdb_system_device_bytes(r->sys, &b);
+            const size_t actual = b + sizeof(double) * (3 * static_cast<size_t>(s.meshes[q->mesh].n) +
+                                                        2 * static_cast<size_t>(s.meshes[q->mesh].nf));
+            s.resident_bytes = s.resident_bytes - std::min(s.resident_bytes, r->bytes) + actual;
+            r->bytes = actual;
+        }
+        if (q->status != CFDB_OK && r->sys == nullptr) {
+            s.resident_bytes -= std::min(s.resident_bytes, r->bytes);
+            s.resident.erase(q->mesh);
+        } else {
+            r->busy = false;
+            r->last_use = Clock::now();
+        }
+        q->done = true;
+        ++s.completed;
+        s.cv_done.notify_all();
+        s.cv_work.notify_all();
+    }
+}
+
+template <class F> int guarded_s(F&& f) {
+    try {
+        f();
+        return CFDB_OK;
+    } catch (const cfdb::Error& e) {
+        cfdb::set_thread_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        cfdb::set_thread_error("host allocation failed");
+        return CFDB_ERR_OOM;
+    } catch (const std::exception& e) {
+        cfdb::set_thread_error(e.what());
+        return CFDB_ERR_INTERNAL;
+    }
+}
+
+double seconds(const cfdb_server& s, Clock::time_point t) {
+    return std::chrono::duration<double>(t - s.t0).count();
+}
+
+} // namespace
+
+extern "C" {
+
+void cfdb_default_server_config(cfdb_server_config* c) {
+    if (c == nullptr) return;
+    c->slots = 4;
+    c->hbm_budget_bytes = 150e9;
+    c->precision = CFDB_PRECISION_MIXED;
+    cfdb_default_amg_settings(&c->settings);
+    c->max_age = 0;
+}
+
+int cfdb_server_create(const cfdb_server_config* cfg, cfdb_server** out) {
+    return guarded_s([&] {
+        if (cfg == nullptr || out == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
+        if (cfg->slots < 1 || cfg->slots > 64) fail(CFDB_ERR_BAD_ARG, "slots must be in 1..64");
+        if (!(cfg->hbm_budget_bytes > 0)) fail(CFDB_ERR_BAD_ARG, "HBM budget must be positive");
+        if (!cfdb_device_available()) fail(CFDB_ERR_NO_DEVICE, "no CUDA device: this library has no host fallback");
+        auto s = std::make_unique<cfdb_server>();
+        s->cfg = *cfg;
+        CFDB_CUDA(cudaGetDevice(&s->device));
+        s->t0 = Clock::now();
+        for (int i = 0; i < cfg->slots; ++i) s->workers.emplace_back(worker_loop, s.get());
+        *out = s.release();
+    });
+}
+
+int cfdb_server_destroy(cfdb_server* s) {
+    if (s == nullptr) return CFDB_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stopping = true;
+    }
+    s->cv_work.notify_all();
+    for (auto& t : s->workers) t.join();
+    cudaSetDevice(s->device);
+    for (auto& kv : s->resident) release(*s, *kv.second);
+    delete s;
+    return CFDB_OK;
+}
+
+int cfdb_server_add_mesh(cfdb_server* s, int n_cells, int n_faces, const int* owner, const int* neighbour, int* mesh_id) {
+    return guarded_s([&] {
+        if (s == nullptr || mesh_id == nullptr || n_cells <= 0 || n_faces < 0 || (n_faces > 0 && (!owner || !neighbour)))
+            fail(CFDB_ERR_BAD_ARG, "cfdb_server_add_mesh: bad arguments");
+        for (int f = 0; f < n_faces; ++f)
+            if (owner[f] < 0 || owner[f] >= n_cells || neighbour[f] < 0 || neighbour[f] >= n_cells)
+                fail(CFDB_ERR_BAD_ARG, "cfdb_server_add_mesh: face addresses a cell out of range");
+        Mesh m;
+        m.n = n_cells;
+        m.nf = n_faces;
+        m.owner.assign(owner, owner + n_faces);
+        m.neighbour.assign(neighbour, neighbour + n_faces);
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->meshes.push_back(std::move(m));
+        *mesh_id = static_cast<int>(s->meshes.size()) - 1;
+    });
+}
+
+int cfdb_server_submit(cfdb_server* s, int mesh_id, long long matrix_key, const double* diag, const double* upper,
+                       const double* lower, const double* rhs, int warm_start, double rel_tol, int max_iterations,
+                       long long* ticket) {
+    return guarded_s([&] {
+        if (s == nullptr || ticket == nullptr || !diag || !rhs) fail(CFDB_ERR_BAD_ARG, "cfdb_server_submit: null argument");
+        auto q = std::make_shared<Request>();
+        q->submitted = Clock::now();
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (mesh_id < 0 || mesh_id >= static_cast<int>(s->meshes.size())) fail(CFDB_ERR_BAD_ARG, "unknown mesh");
+        }
+        const Mesh& m = s->meshes[mesh_id];
+        if (m.nf > 0 && (!upper || !lower)) fail(CFDB_ERR_BAD_ARG, "cfdb_server_submit: null face coefficients");
+        if (!(rel_tol > 0.0) || max_iterations < 0) fail(CFDB_ERR_BAD_ARG, "cfdb_server_submit: bad tolerance");
+        q->mesh = mesh_id;
+        q->key = matrix_key;
+        q->warm = warm_start != 0;
+        q->rel_tol = rel_tol;
+        q->max_iter = max_iterations;
+        q->diag.assign(diag, diag + m.n);
+        q->upper.assign(upper, upper + m.nf);
+        q->lower.assign(lower, lower + m.nf);
+        q->rhs.assign(rhs, rhs + m.n);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (s->stopping) fail(CFDB_ERR_BAD_ARG, "server is stopping");
+            if (estimate_bytes(*s, m) > static_cast<size_t>(s->cfg.hbm_budget_bytes))
+                fail(CFDB_ERR_OOM, "request can never fit the server's HBM budget");
+            q->ticket = s->next_ticket++;
+            s->tickets[q->ticket] = q;
+            s->queue.push_back(q);
+            *ticket = q->ticket;
+        }
+        s->cv_work.notify_one();
+    });
+}
+
+int cfdb_server_wait(cfdb_server* s, long long ticket, double* x, cfdb_stats* stats, double* times) {
+    return guarded_s([&] {
+        if (s == nullptr) fail(CFDB_ERR_BAD_ARG, "null server");
+        std::shared_ptr<Request> q;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            auto it = s->tickets.find(ticket);
+            if (it == s->tickets.end()) fail(CFDB_ERR_BAD_ARG, "unknown ticket");
+            q = it->second;
+            s->cv_done.wait(lk, [&] { return q->done; });
+            s->tickets.erase(it);
+        }
+        if (times != nullptr) {
+            times[0] = seconds(*s, q->submitted);
+            times[1] = seconds(*s, q->started);
+            times[2] = seconds(*s, q->finished);
+        }
+        if (q->status != CFDB_OK) fail(q->status, q->error);
+        if (x != nullptr) std::memcpy(x, q->x.data(), sizeof(double) * q->x.size());
+        if (stats != nullptr) *stats = q->stats;
+    });
+}
+
+int cfdb_server_info(cfdb_server* s, cfdb_server_info_t* info) {
+    if (s == nullptr || info == nullptr) return CFDB_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    info->resident_systems = static_cast<int>(s->resident.size());
+    info->resident_bytes = static_cast<double>(s->resident_bytes);
+    info->queued = static_cast<int>(s->queue.size());
+    info->completed = s->completed;
+    info->evictions = s->evictions;
+    return CFDB_OK;
+}
+
+} // extern "C"

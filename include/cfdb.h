@@ -237,10 +237,54 @@ int cfdb_system_assemble_pressure_device(cfdb_system* sys, const double* flux,
 /* Number of this library's kernels the system has launched so far (graph nodes included). */
 int cfdb_system_kernel_launches(const cfdb_system* sys, unsigned long long* count);
 
+/* Launch-shape / schedule knobs of the device plan (see cfd_b200/autotune.py). */
+typedef struct {
+    int target_tiles; /* SELL tiles (256-thread CTAs) per level, default 1184 = 148 SMs x 8 */
+    int wide_row;     /* average row length above which CSR lane groups are used, default 24 */
+    int lanes_div;    /* lanes per CSR row ~ average row length / lanes_div, default 6 */
+    int fuse_first;   /* first two smoothing sweeps in one kernel, default 1 */
+} cfdb_tuning;
+void cfdb_default_tuning(cfdb_tuning* t);
+int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t);
+
 /* Stream of the system (cudaStream_t as void*), for callers that order their own work. */
 int cfdb_system_stream(const cfdb_system* sys, void** stream);
 /* Device bytes held by the system (pattern, hierarchy, work vectors). */
 int cfdb_system_device_bytes(const cfdb_system* sys, size_t* bytes);
+
+/* ---- batches: many independent pressure systems of uneven size in one device plan ----
+ * (No counterpart in the reference, which solves systems one at a time through DeviceSolver.)
+ * Every level of every system is concatenated into one set of arrays; each kernel launch of the
+ * solve covers all systems (per-system convergence masks, per-system dot products), and the
+ * whole iteration is one captured CUDA graph. Arrays are concatenated in system order: cells
+ * of system 0, then system 1, ...; faces likewise; owner / neighbour hold LOCAL cell indices. */
+typedef struct cfdb_batch cfdb_batch;
+int cfdb_batch_create(int n_systems, const int* n_cells, const int* n_faces, const int* owner,
+                      const int* neighbour, cfdb_batch** out);
+int cfdb_batch_destroy(cfdb_batch* b);
+int cfdb_batch_sizes(const cfdb_batch* b, long long* total_cells, long long* total_faces);
+/* Hierarchies of all systems from host LDU arrays (AmgPreconditioner::setup per system,
+ * systems in parallel on the host). */
+int cfdb_batch_setup_amg(cfdb_batch* b, const double* diag, const double* upper,
+                         const double* lower, const cfdb_amg_settings* settings);
+int cfdb_batch_set_precision(cfdb_batch* b, int precision);
+int cfdb_batch_set_tuning(cfdb_batch* b, const cfdb_tuning* t);
+/* cfdb_system_assemble_pressure_device for every system (device arrays); ref_cell: host array
+ * of per-system local reference cells (-1: none). */
+int cfdb_batch_assemble_pressure_device(cfdb_batch* b, const double* flux, const double* gamma,
+                                        const double* delta_coeff, const double* source0,
+                                        const int* ref_cell, double ref_value, double* upper,
+                                        double* lower, double* diag, double* source);
+/* Solves every system (device arrays); x: initial guesses in, solutions out. controls and
+ * stats: one per system (host arrays). use_amg = 0 runs Jacobi-preconditioned CG. */
+int cfdb_batch_solve_device(cfdb_batch* b, const double* diag, const double* upper,
+                            const double* lower, const double* rhs, double* x, int use_amg,
+                            const cfdb_control* controls, cfdb_stats* stats);
+int cfdb_batch_profile(cfdb_batch* b, int reps, cfdb_kernel_record* records, int max_records,
+                       int* n_records);
+int cfdb_batch_stream(const cfdb_batch* b, void** stream);
+int cfdb_batch_device_bytes(const cfdb_batch* b, size_t* bytes);
+int cfdb_batch_kernel_launches(const cfdb_batch* b, unsigned long long* count);
 
 #ifdef __cplusplus
 }

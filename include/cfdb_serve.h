@@ -1,0 +1,61 @@
+/*
+ * cfdb serving loop: continuous batching of pressure solves on one GPU (no counterpart in the
+ * reference, which solves one system at a time inside its time loop).
+ *
+ * Requests are queued at submit and taken by worker slots as soon as a slot is free; each mesh
+ * keeps a resident persistent system (pattern, AMG hierarchy, the last matrix, right-hand side
+ * and solution on the device, its own CUDA stream), so requests on different meshes overlap on
+ * the GPU. Systems are admitted against an HBM budget (estimated footprint, then measured),
+ * evicting idle systems least-recently-used first; requests that cannot fit yet wait.
+ * matrix_key names a coefficient set: a request repeating the key of the matrix resident on its
+ * mesh skips the matrix upload, and with warm_start it starts from the resident solution.
+ */
+#ifndef CFDB_SERVE_H
+#define CFDB_SERVE_H
+
+#include "cfdb.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    int slots;                  /* concurrent worker slots (streams), default 4 */
+    double hbm_budget_bytes;    /* device bytes the resident systems may hold, default 150e9 */
+    int precision;              /* cfdb_precision of the solves, default MIXED */
+    cfdb_amg_settings settings; /* hierarchy settings */
+    int max_age;                /* rebuild the hierarchy after this many solves (0: never) */
+} cfdb_server_config;
+
+typedef struct {
+    int resident_systems;
+    double resident_bytes;
+    int queued;
+    long long completed;
+    long long evictions;
+} cfdb_server_info_t;
+
+typedef struct cfdb_server cfdb_server;
+
+void cfdb_default_server_config(cfdb_server_config* c);
+int cfdb_server_create(const cfdb_server_config* cfg, cfdb_server** out);
+/* Drains the queue, joins the workers, frees every resident system. */
+int cfdb_server_destroy(cfdb_server* s);
+/* Registers mesh addressing (internal faces); returns its id. */
+int cfdb_server_add_mesh(cfdb_server* s, int n_cells, int n_faces, const int* owner,
+                         const int* neighbour, int* mesh_id);
+/* Queues one solve A x = rhs to relative residual rel_tol (x0 = 0, or the resident solution of
+ * the same matrix_key with warm_start). Host arrays are copied at submit. */
+int cfdb_server_submit(cfdb_server* s, int mesh_id, long long matrix_key, const double* diag,
+                       const double* upper, const double* lower, const double* rhs,
+                       int warm_start, double rel_tol, int max_iterations, long long* ticket);
+/* Blocks until the ticket is done; x (n_cells, may be NULL) receives the solution, times (3
+ * doubles, may be NULL) the submit / start / finish times in seconds since server creation. */
+int cfdb_server_wait(cfdb_server* s, long long ticket, double* x, cfdb_stats* stats,
+                     double* times);
+int cfdb_server_info(cfdb_server* s, cfdb_server_info_t* info);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -10,6 +10,8 @@ separately). `value` is the mixed-precision path (FP32 V-cycle inside FP64 flexi
 plain FP64 path is reported beside it. Inputs are resident in HBM and larger than L2.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config graded|tet|cavity]
+  python bench.py --config batch    # 256 uneven boxes in one device plan, autotuned
+  python bench.py --config serve    # serving loop, Poisson arrivals, p50/p99
 
 Multi-GPU: the path does not shard (one pressure system per GPU); N ranks run independent
 replicas (weak scaling, no collective on the data path); value = total solves/s, time = max
@@ -39,7 +41,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="graded", choices=["graded", "tet", "cavity"])
+    ap.add_argument("--config", default="graded", choices=["graded", "tet", "cavity", "batch", "serve"])
+    ap.add_argument("--systems", type=int, default=256, help="batch: number of systems")
+    ap.add_argument("--tune-cache", default=None, help="batch: autotuner cache file")
+    ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serve: arrival rates (1/s)")
+    ap.add_argument("--requests", type=int, default=200, help="serve: requests per rate")
+    ap.add_argument("--slots", type=int, default=4, help="serve: worker slots")
     ap.add_argument("--size", type=int, default=0, help="override the mesh edge length")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -469,6 +476,213 @@ def cpu_baseline(case):
                 "kind": "reference", "sample": f"failed: {e}"}
 
 
+# ------------------------------------------------------------------------------------------
+# batched configuration: 256 boxes of uneven size in one device plan
+# ------------------------------------------------------------------------------------------
+
+BATCH_METRIC = "batched pressure solves/s (256 boxes, edge log-uniform 8-64, each to 1e-8, mixed)"
+
+
+def run_batch(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import cfd_b200 as cb
+    from cfd_b200 import workloads as W
+    from cfd_b200.autotune import tune
+    from cfd_b200.multi import replica_summary
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    edges = W.box_edges(args.systems)
+    cases = [W.batch_box(e, seed=W.SEED_BASE + 1000 + i) for i, e in enumerate(edges)]
+    nc, nf = [c.n for c in cases], [c.n_faces for c in cases]
+    tc, tf = sum(nc), sum(nf)
+    cat = lambda k: np.concatenate([getattr(c, k) for c in cases])  # noqa: E731
+    T = lambda a: torch.as_tensor(a, dtype=torch.float64, device=dev)  # noqa: E731
+    flux, gamma, delta, src0 = T(cat("flux")), T(cat("gamma")), T(cat("delta")), T(cat("source0"))
+    z = lambda m: torch.zeros(m, dtype=torch.float64, device=dev)  # noqa: E731
+    up, lo, dg, src, x = z(tf), z(tf), z(tc), z(tc), z(tc)
+    b = cb.Batch(nc, nf, cat("owner"), cat("neighbour"))
+    refs = [0] * len(cases)
+    b.assemble_pressure_device(flux, gamma, delta, src0, up, lo, dg, src, ref_cells=refs)
+    torch.cuda.synchronize()
+    h_dg, h_up, h_lo, h_src = dg.cpu().numpy(), up.cpu().numpy(), lo.cpu().numpy(), src.cpu().numpy()
+    t0 = time.perf_counter()
+    settings = cb.AmgSettings(strength_threshold=THETA)
+    b.setup_amg(h_dg, h_up, h_lo, settings)
+    setup_s = time.perf_counter() - t0
+    offs = np.concatenate([[0], np.cumsum(nc)])
+    tols = [1e-8 * float(np.linalg.norm(h_src[offs[i]:offs[i + 1]])) for i in range(len(cases))]
+    ctl = [cb.SolveControl(t, 500) for t in tols]
+    stream = torch.cuda.ExternalStream(b.stream(), device=dev)
+
+    def step():
+        b.assemble_pressure_device(flux, gamma, delta, src0, up, lo, dg, src, ref_cells=refs)
+        x.zero_()
+        return b.solve_device(dg, up, lo, src, x, ctl)
+
+    def run_iterations(k):
+        x.zero_()
+        b.solve_device(dg, up, lo, src, x, [cb.SolveControl(0.0, k)] * len(cases))
+
+    out = {}
+    tuning = None
+    for label, prec in (("mixed", cb.Precision.MIXED), ("fp64", cb.Precision.FP64)):
+        b.set_precision(prec)
+        if label == "mixed":
+            sig = f"batch:{len(cases)}:{tc}:{tf}:mixed"
+            with torch.cuda.stream(stream):
+                best, tuning = tune(b, run_iterations, b.stream(), sig, cache_path=args.tune_cache)
+        with torch.cuda.stream(stream):
+            for _ in range(max(args.warmup, 0)):
+                step()
+            torch.cuda.synchronize()
+            sampler = ClockSampler(local_rank) if label == "mixed" else None
+            if sampler:
+                sampler.start()
+            l0 = b.kernel_launches()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            stats = [step() for _ in range(args.steps)]
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            launches = b.kernel_launches() - l0
+            clocks = sampler.stop() if sampler else None
+        ms, _ = replica_summary(ms, args.steps, world)
+        xs = x.cpu().numpy()
+        assert all(st.converged for st in stats[-1]), label
+        it = [st.iterations for st in stats[-1]]
+        prof = b.profile(3)
+        ms_it = sum(r[2] for r in prof)
+        by_it = sum(r[3] for r in prof)
+        out[label] = {
+            "systems_per_s": world * len(cases) * args.steps / (ms / 1e3),
+            "ms_per_batch": ms / args.steps, "iterations_min": min(it), "iterations_max": max(it),
+            "true_rel_residual_max": max(st.true_residual / (t / 1e-8) for st, t in zip(stats[-1], tols)),
+            "profile_init_plus_iteration_ms": ms_it, "profile_bytes": by_it,
+            "profile_gbs": by_it / 1e9 / (ms_it / 1e3) if ms_it > 0 else None,
+            "gpu_launches": launches, "clocks": clocks, "device_bytes": b.device_bytes(),
+        }
+        del xs
+    # one system at a time, plain FP64 drop-in path (DeviceSolver per system), same solves
+    t_single = 0.0
+    it_single = []
+    for i, c in enumerate(cases):
+        ds = cb.DeviceSolver(mesh=(c.n, c.owner, c.neighbour))
+        s0, s1 = offs[i], offs[i + 1]
+        fo = sum(nf[:i])
+        d_i, u_i, l_i = h_dg[s0:s1], h_up[fo:fo + c.n_faces], h_lo[fo:fo + c.n_faces]
+        ds.setup_amg(d_i, u_i, l_i, settings)
+        ds.set_precision(cb.Precision.FP64)
+        bd, bu, bl, bs = T(d_i), T(u_i), T(l_i), T(h_src[s0:s1])
+        xi = z(c.n)
+        st_i = torch.cuda.ExternalStream(ds.stream(), device=dev)
+        with torch.cuda.stream(st_i):
+            ds.solve_device(bd, bu, bl, bs, xi, cb.Method.Cg, True, ctl[i])
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(st_i)
+            xi.zero_()
+            r = ds.solve_device(bd, bu, bl, bs, xi, cb.Method.Cg, True, ctl[i])
+            e1.record(st_i)
+            torch.cuda.synchronize()
+        t_single += e0.elapsed_time(e1)
+        it_single.append(r.iterations)
+        ds.close()
+    value = out["mixed"]["systems_per_s"]
+    line = {
+        "metric": BATCH_METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["mixed"]["ms_per_batch"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64+f32 (FP64 outer, FP32 V-cycle)", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"batch{len(cases)} boxes", "systems": len(cases), "cells": tc,
+                   "internal_faces": tf, "edge_min": min(edges), "edge_max": max(edges),
+                   "strength_threshold": THETA, "step": "batched device assembly + solve of all systems",
+                   "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+        "mixed": out["mixed"], "fp64": out["fp64"],
+        "one_at_a_time_fp64": {"systems_per_s": len(cases) / (t_single / 1e3), "ms_total": t_single,
+                               "iterations_max": max(it_single)},
+        "batched_mixed_vs_one_at_a_time_fp64": value / (len(cases) / (t_single / 1e3)),
+        "setup_s_host": setup_s, "tuning": tuning, "clocks": out["mixed"]["clocks"],
+        "gpu_launches": out["mixed"]["gpu_launches"],
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    b.close()
+
+
+# ------------------------------------------------------------------------------------------
+# serving loop: Poisson arrivals over a pool of box and tet meshes
+# ------------------------------------------------------------------------------------------
+
+SERVE_METRIC = "served pressure solves/s at saturation (box/tet mix, 1e-8, mixed, warm starts)"
+
+
+def run_serve(args, rank, world, local_rank):
+    import torch
+
+    import cfd_b200 as cb
+    from cfd_b200 import serving as S
+    from cfd_b200 import workloads as W
+
+    torch.cuda.set_device(local_rank)
+    pool_cases = W.serve_pool()
+    settings = cb.AmgSettings(strength_threshold=THETA)
+    rates = [float(r) for r in args.rates.split(",") if r]
+    n_req = args.requests
+    res = {}
+
+    def server(prec, slots):
+        srv = S.Server(slots=slots, hbm_budget_bytes=150e9, precision=prec, settings=settings)
+        pool = S.make_pool(srv, pool_cases, variants=3, seed=7)
+        t0 = time.perf_counter()
+        for e in pool:  # hierarchy builds (AmgCache setup), not timed below
+            srv.wait(srv.submit(e.mesh_id, 0, *e.matrices[0], e.rhs[0]))
+        return srv, pool, time.perf_counter() - t0
+
+    # plain FP64 drop-in, one request at a time, no warm start
+    srv, pool, setup = server(cb.Precision.FP64, 1)
+    S.run_load(srv, pool, 0.0, n_req // 2, seed=10, closed_loop=True, warm_start=False)
+    _, base = S.run_load(srv, pool, 0.0, n_req, seed=11, closed_loop=True, warm_start=False)
+    res["one_at_a_time_fp64"] = dict(base, setup_s=setup)
+    srv.close()
+    for label, prec in (("mixed", cb.Precision.MIXED), ("fp64", cb.Precision.FP64)):
+        srv, pool, setup = server(prec, args.slots)
+        S.run_load(srv, pool, 1e6, n_req, seed=10)  # warm-up: page-locked buffers, graphs
+        sampler = ClockSampler(local_rank) if label == "mixed" else None
+        if sampler:
+            sampler.start()
+        _, sat = S.run_load(srv, pool, 1e6, n_req, seed=11)  # all requests queued at once
+        sweep = [S.run_load(srv, pool, r, n_req, seed=12 + k)[1] for k, r in enumerate(rates)]
+        clocks = sampler.stop() if sampler else None
+        res[label] = {"saturated": sat, "sweep": sweep, "setup_s": setup, "clocks": clocks,
+                      "info": srv.info()}
+        srv.close()
+    value = res["mixed"]["saturated"]["solves_per_s"]
+    line = {
+        "metric": SERVE_METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+        "steps": n_req, "warmup": len(pool_cases),
+        "ms_per_step": 1e3 / value if value else None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32 (FP64 outer, FP32 V-cycle)",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": "serve box/tet pool", "box_edges": list(W.SERVE_BOX_EDGES),
+                   "tet_edges": list(W.SERVE_TET_EDGES), "tet_share": 0.25, "repeat_share": 0.3,
+                   "slots": args.slots, "hbm_budget_gb": 150, "rates_hz": rates,
+                   "requests_per_rate": n_req, "strength_threshold": THETA,
+                   "step": "one request: H2D of its matrix (new key) and rhs, AMG-PCG to 1e-8, D2H of x",
+                   "parallelism": f"replicas x{world}"},
+        "mixed": res["mixed"], "fp64": res["fp64"], "one_at_a_time_fp64": res["one_at_a_time_fp64"],
+        "served_mixed_vs_one_at_a_time_fp64": value / res["one_at_a_time_fp64"]["solves_per_s"],
+        "p50_ms": res["mixed"]["saturated"]["p50_ms"], "p99_ms": res["mixed"]["saturated"]["p99_ms"],
+        "clocks": res["mixed"]["clocks"],
+    }
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     args = parse()
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
@@ -479,6 +693,10 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
+        if args.config in ("batch", "serve"):
+            print(json.dumps({"impl": "reference", "unavailable": "the reference solves one system at a "
+                              "time; its host solver is timed per system by --config graded|tet|cavity"}))
+            return
         case, desc = make_case(args.config, size)
         run_reference(args, f"{args.config}{case.mesh.shape[0]}^3", case, desc)
         return
@@ -488,15 +706,24 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.config == "batch":
+        run_batch(args, rank, world, local_rank)
+    elif args.config == "serve":
+        run_serve(args, rank, world, local_rank)
+    else:
+        run_case(args, rank, world, local_rank, size)
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+def run_case(args, rank, world, local_rank, size):
     case, desc = make_case(args.config, size)
     cfg_name = f"{args.config}{case.mesh.shape[0]}^3"
     if args.profile_only:
         args.no_e2e = True
         args.no_cpu_baseline = True
     run_ours(args, rank, world, local_rank, cfg_name, case, desc)
-    if world > 1:
-        import torch
-        torch.distributed.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -1,0 +1,122 @@
+"""Autotuner for the device plan's launch shapes and smoother schedule.
+
+The knobs are those of `Tuning` (include/cfdb.h, cfdb_tuning):
+
+* target_tiles - CTAs per level operator (tile height follows from it),
+* wide_row     - average row length above which a level switches from SELL-32 rows to
+                 CSR lane groups,
+* lanes_div    - lanes per CSR row = average row length / lanes_div,
+* fuse_first   - first two Jacobi sweeps of the pre-smoothing fused into one kernel.
+
+The search is a coordinate descent from the defaults: each knob in turn is swept over its
+candidate values with the others fixed, the best value kept, and the pass repeated until no
+knob changes (at most `passes` passes). The objective is the device time of a fixed number of
+CG iterations (tolerance 0, so every system runs exactly `iterations` iterations) through the
+captured graphs of the real solve path, median of `reps` runs. Results are cached in a JSON
+file keyed by a workload signature.
+"""
+from __future__ import annotations
+
+import dataclasses
+import json
+import os
+import statistics
+from typing import Callable
+
+from . import Tuning
+
+CANDIDATES = {
+    "target_tiles": [148 * 4, 148 * 8, 148 * 16],
+    "wide_row": [16, 24, 32, 64],
+    "lanes_div": [3, 4, 6, 8],
+    "fuse_first": [0, 1],
+}
+
+
+def _key(t: Tuning) -> tuple:
+    return tuple(dataclasses.astuple(t))
+
+
+def coordinate_search(evaluate: Callable[[Tuning], float], start: Tuning | None = None,
+                      candidates: dict | None = None, passes: int = 2):
+    """Minimises evaluate(tuning) (milliseconds) by coordinate descent. Returns
+    (best tuning, best value, trace of (tuning dict, value))."""
+    cand = candidates or CANDIDATES
+    best = dataclasses.replace(start) if start is not None else Tuning()
+    seen = {}
+    trace = []
+
+    def ev(t):
+        k = _key(t)
+        if k not in seen:
+            seen[k] = float(evaluate(t))
+            trace.append((dataclasses.asdict(t), seen[k]))
+        return seen[k]
+
+    best_v = ev(best)
+    for _ in range(max(passes, 1)):
+        changed = False
+        for knob, values in cand.items():
+            for v in values:
+                if getattr(best, knob) == v:
+                    continue
+                t = dataclasses.replace(best, **{knob: v})
+                val = ev(t)
+                if val < best_v:
+                    best, best_v, changed = t, val, True
+        if not changed:
+            break
+    return best, best_v, trace
+
+
+def solve_timer(target, run_iterations: Callable[[int], None], stream_handle: int,
+                iterations: int = 6, reps: int = 3):
+    """An objective for coordinate_search: installs the tuning on `target` (a DeviceSolver or
+    Batch), then times run_iterations(iterations) with CUDA events on the target's stream."""
+    import torch
+
+    def evaluate(t: Tuning) -> float:
+        target.set_tuning(t)
+        stream = torch.cuda.ExternalStream(stream_handle)
+        run_iterations(iterations)  # warm: graph capture for the new plan
+        times = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            run_iterations(iterations)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return statistics.median(times)
+
+    return evaluate
+
+
+def tune(target, run_iterations, stream_handle, signature: str, cache_path: str | None = None,
+         iterations: int = 6, reps: int = 3, passes: int = 2):
+    """Tunes `target` for the workload named by `signature`, reusing a cached result when the
+    cache file holds one. Installs and returns the best tuning with its record."""
+    cache = {}
+    if cache_path and os.path.exists(cache_path):
+        try:
+            with open(cache_path) as f:
+                cache = json.load(f)
+        except (OSError, ValueError):
+            cache = {}
+    if signature in cache:
+        rec = cache[signature]
+        best = Tuning(**rec["tuning"])
+        target.set_tuning(best)
+        return best, dict(rec, cached=True)
+    evaluate = solve_timer(target, run_iterations, stream_handle, iterations, reps)
+    default_ms = evaluate(Tuning())
+    best, best_ms, trace = coordinate_search(evaluate, Tuning(), passes=passes)
+    target.set_tuning(best)
+    rec = {"tuning": dataclasses.asdict(best), "ms": best_ms, "default_ms": default_ms,
+           "iterations": iterations, "evaluations": len(trace), "trace": trace}
+    if cache_path:
+        cache[signature] = rec
+        with open(cache_path, "w") as f:
+            json.dump(cache, f, indent=1)
+    return best, dict(rec, cached=False)

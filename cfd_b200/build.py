@@ -32,7 +32,7 @@ def _sources():
 
 def _deps():
     return (glob.glob(os.path.join(CSRC, "*")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
-            + [os.path.abspath(__file__)])
+            + glob.glob(os.path.join(ROOT, "include", "*.hpp")) + [os.path.abspath(__file__)])
 
 
 def _stale(target, deps):

@@ -214,14 +214,8 @@ SolveResult run_single(cfdb_system* s, const double* diag, const double* upper, 
     if (dev) {
         e.set_values_device(diag, upper, lower, n, n + nf);
     } else {
-        std::vector<double> vs(static_cast<size_t>(n) + 2 * static_cast<size_t>(nf));
-        std::memcpy(vs.data(), diag, sizeof(double) * n);
-        if (nf > 0) {
-            std::memcpy(vs.data() + n, upper, sizeof(double) * nf);
-            std::memcpy(vs.data() + n + nf, lower, sizeof(double) * nf);
-        }
-        e.upload_values({vs.data()});
-        CFDB_CUDA(cudaStreamSynchronize(e.stream()));
+        // the caller's arrays are read by the copies before this call returns
+        e.upload_values_ldu(diag, upper, lower, n, nf);
     }
     e.set_rhs(0, b, dev);
     e.set_guess(0, x, dev);

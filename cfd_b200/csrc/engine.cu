@@ -524,6 +524,16 @@ void Engine::upload_values(const std::vector<const double*>& host_src) {
     set_values_device(vs_, vs_, vs_, INT_MAX, INT_MAX);
 }
 
+void Engine::upload_values_ldu(const double* diag, const double* upper, const double* lower, int n, int nf) {
+    if (n_sys_ != 1 || vs_total_ != static_cast<long long>(n) + 2LL * nf) fail(1, "upload_values_ldu: layout mismatch");
+    CFDB_CUDA(cudaMemcpyAsync(vs_, diag, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
+    if (nf > 0) {
+        CFDB_CUDA(cudaMemcpyAsync(vs_ + n, upper, sizeof(double) * nf, cudaMemcpyHostToDevice, stream_));
+        CFDB_CUDA(cudaMemcpyAsync(vs_ + n + nf, lower, sizeof(double) * nf, cudaMemcpyHostToDevice, stream_));
+    }
+    set_values_device(vs_, vs_, vs_, INT_MAX, INT_MAX);
+}
+
 void Engine::upload_values_device_concat(const std::vector<const double*>& dev_src) {
     std::vector<int> lens(n_sys_);
     for (int k = 0; k < n_sys_; ++k) {

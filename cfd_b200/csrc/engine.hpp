@@ -81,6 +81,8 @@ public:
     // value source (concatenated per system in batch order) first.
     void set_values_device(const double* p0, const double* p1, const double* p2, int n1, int n2);
     void upload_values(const std::vector<const double*>& host_src);
+    // Single system: LDU values straight from the caller's host arrays (no staging copy).
+    void upload_values_ldu(const double* diag, const double* upper, const double* lower, int n, int nf);
     void upload_values_device_concat(const std::vector<const double*>& dev_src);
 
     // Right-hand side / initial guess of system s (original batch index), host or device.

@@ -61,9 +61,10 @@ struct Request {
     bool warm = false;
     double rel_tol = 1e-8;
     int max_iter = 500;
-    std::vector<double> diag, upper, lower, rhs;
+    // borrowed from the caller until the ticket is waited for
+    const double *diag = nullptr, *upper = nullptr, *lower = nullptr, *rhs = nullptr;
+    double* x = nullptr;
     Clock::time_point submitted{}, started{}, finished{};
-    std::vector<double> x;
     cfdb_stats stats{};
     int status = CFDB_OK;
     std::string error;
@@ -79,7 +80,7 @@ struct cfdb_server {
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     bool stopping = false;
-    std::vector<Mesh> meshes;
+    std::deque<Mesh> meshes; // stable element addresses while meshes are added
     std::unordered_map<int, std::unique_ptr<Resident>> resident;
     size_t resident_bytes = 0;
     std::deque<std::shared_ptr<Request>> queue;
@@ -163,30 +164,29 @@ void execute(cfdb_server& s, Resident& r, const Mesh& m, Request& q, bool create
     const bool new_matrix = r.matrix_key != q.key || q.key < 0;
     if (created || (s.cfg.max_age > 0 && r.age >= s.cfg.max_age)) {
         // hierarchy (re)build from this request's matrix, as the reference's AmgCache does
-        check(cfdb_system_setup_amg(r.sys, q.diag.data(), q.upper.data(), q.lower.data(), &s.cfg.settings));
+        check(cfdb_system_setup_amg(r.sys, q.diag, q.upper, q.lower, &s.cfg.settings));
         r.age = 0;
     }
     if (new_matrix) {
-        CFDB_CUDA(cudaMemcpyAsync(r.d_diag, q.diag.data(), sizeof(double) * m.n, cudaMemcpyHostToDevice, st));
+        CFDB_CUDA(cudaMemcpyAsync(r.d_diag, q.diag, sizeof(double) * m.n, cudaMemcpyHostToDevice, st));
         if (m.nf > 0) {
-            CFDB_CUDA(cudaMemcpyAsync(r.d_upper, q.upper.data(), sizeof(double) * m.nf, cudaMemcpyHostToDevice, st));
-            CFDB_CUDA(cudaMemcpyAsync(r.d_lower, q.lower.data(), sizeof(double) * m.nf, cudaMemcpyHostToDevice, st));
+            CFDB_CUDA(cudaMemcpyAsync(r.d_upper, q.upper, sizeof(double) * m.nf, cudaMemcpyHostToDevice, st));
+            CFDB_CUDA(cudaMemcpyAsync(r.d_lower, q.lower, sizeof(double) * m.nf, cudaMemcpyHostToDevice, st));
         }
         r.matrix_key = q.key;
     }
-    CFDB_CUDA(cudaMemcpyAsync(r.d_rhs, q.rhs.data(), sizeof(double) * m.n, cudaMemcpyHostToDevice, st));
+    CFDB_CUDA(cudaMemcpyAsync(r.d_rhs, q.rhs, sizeof(double) * m.n, cudaMemcpyHostToDevice, st));
     if (!(q.warm && r.solution_key == q.key && q.key >= 0)) {
         CFDB_CUDA(cudaMemsetAsync(r.d_x, 0, sizeof(double) * m.n, st));
     }
     double bn = 0.0;
-    for (double v : q.rhs) bn += v * v;
+    for (int i = 0; i < m.n; ++i) bn += q.rhs[i] * q.rhs[i];
     const cfdb_control ctl{q.rel_tol * std::sqrt(bn), q.max_iter};
     check(cfdb_system_solve_device(r.sys, r.d_diag, r.d_upper, r.d_lower, r.d_rhs, r.d_x, CFDB_METHOD_CG, 1, &ctl,
                                    &q.stats));
     r.solution_key = q.key;
     ++r.age;
-    q.x.resize(m.n);
-    CFDB_CUDA(cudaMemcpyAsync(q.x.data(), r.d_x, sizeof(double) * m.n, cudaMemcpyDeviceToHost, st));
+    if (q.x != nullptr) CFDB_CUDA(cudaMemcpyAsync(q.x, r.d_x, sizeof(double) * m.n, cudaMemcpyDeviceToHost, st));
     CFDB_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -342,17 +342,19 @@ int cfdb_server_add_mesh(cfdb_server* s, int n_cells, int n_faces, const int* ow
 }
 
 int cfdb_server_submit(cfdb_server* s, int mesh_id, long long matrix_key, const double* diag, const double* upper,
-                       const double* lower, const double* rhs, int warm_start, double rel_tol, int max_iterations,
-                       long long* ticket) {
+                       const double* lower, const double* rhs, double* x, int warm_start, double rel_tol,
+                       int max_iterations, long long* ticket) {
     return guarded_s([&] {
         if (s == nullptr || ticket == nullptr || !diag || !rhs) fail(CFDB_ERR_BAD_ARG, "cfdb_server_submit: null argument");
         auto q = std::make_shared<Request>();
         q->submitted = Clock::now();
+        const Mesh* mp = nullptr;
         {
             std::lock_guard<std::mutex> lk(s->mu);
             if (mesh_id < 0 || mesh_id >= static_cast<int>(s->meshes.size())) fail(CFDB_ERR_BAD_ARG, "unknown mesh");
+            mp = &s->meshes[mesh_id];
         }
-        const Mesh& m = s->meshes[mesh_id];
+        const Mesh& m = *mp;
         if (m.nf > 0 && (!upper || !lower)) fail(CFDB_ERR_BAD_ARG, "cfdb_server_submit: null face coefficients");
         if (!(rel_tol > 0.0) || max_iterations < 0) fail(CFDB_ERR_BAD_ARG, "cfdb_server_submit: bad tolerance");
         q->mesh = mesh_id;
@@ -360,10 +362,11 @@ int cfdb_server_submit(cfdb_server* s, int mesh_id, long long matrix_key, const 
         q->warm = warm_start != 0;
         q->rel_tol = rel_tol;
         q->max_iter = max_iterations;
-        q->diag.assign(diag, diag + m.n);
-        q->upper.assign(upper, upper + m.nf);
-        q->lower.assign(lower, lower + m.nf);
-        q->rhs.assign(rhs, rhs + m.n);
+        q->diag = diag;
+        q->upper = upper;
+        q->lower = lower;
+        q->rhs = rhs;
+        q->x = x;
         {
             std::lock_guard<std::mutex> lk(s->mu);
             if (s->stopping) fail(CFDB_ERR_BAD_ARG, "server is stopping");
@@ -378,7 +381,7 @@ int cfdb_server_submit(cfdb_server* s, int mesh_id, long long matrix_key, const 
     });
 }
 
-int cfdb_server_wait(cfdb_server* s, long long ticket, double* x, cfdb_stats* stats, double* times) {
+int cfdb_server_wait(cfdb_server* s, long long ticket, cfdb_stats* stats, double* times) {
     return guarded_s([&] {
         if (s == nullptr) fail(CFDB_ERR_BAD_ARG, "null server");
         std::shared_ptr<Request> q;
@@ -396,7 +399,6 @@ int cfdb_server_wait(cfdb_server* s, long long ticket, double* x, cfdb_stats* st
             times[2] = seconds(*s, q->finished);
         }
         if (q->status != CFDB_OK) fail(q->status, q->error);
-        if (x != nullptr) std::memcpy(x, q->x.data(), sizeof(double) * q->x.size());
         if (stats != nullptr) *stats = q->stats;
     });
 }

@@ -40,8 +40,8 @@ _p("cfdb_default_server_config", [C.POINTER(ServerConfigStruct)], None)
 _p("cfdb_server_create", [C.POINTER(ServerConfigStruct), C.POINTER(_vp)])
 _p("cfdb_server_destroy", [_vp])
 _p("cfdb_server_add_mesh", [_vp, _i, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)])
-_p("cfdb_server_submit", [_vp, _i, _ll, _pd, _pd, _pd, _pd, _i, _d, _i, C.POINTER(_ll)])
-_p("cfdb_server_wait", [_vp, _ll, _pd, C.POINTER(StatsStruct), _pd])
+_p("cfdb_server_submit", [_vp, _i, _ll, _pd, _pd, _pd, _pd, _pd, _i, _d, _i, C.POINTER(_ll)])
+_p("cfdb_server_wait", [_vp, _ll, C.POINTER(StatsStruct), _pd])
 _p("cfdb_server_info", [_vp, C.POINTER(ServerInfoStruct)])
 
 
@@ -57,6 +57,7 @@ class Server:
         _check(_lib.cfdb_server_create(C.byref(cfg), C.byref(h)))
         self._h = h
         self.meshes = {}
+        self._borrowed = {}
 
     def close(self):
         h = getattr(self, "_h", None)
@@ -75,25 +76,36 @@ class Server:
         self.meshes[mid.value] = (int(n_cells), len(nei))
         return mid.value
 
-    def submit(self, mesh_id, matrix_key, diag, upper, lower, rhs, warm_start=False,
+    def submit(self, mesh_id, matrix_key, diag, upper, lower, rhs, x=None, warm_start=False,
                rel_tol=1e-8, max_iterations=500) -> int:
+        """Queues a solve. The arrays are borrowed until wait(ticket) returns (the server keeps
+        references); x (float64, n_cells) receives the solution, a new array when omitted."""
         n, nf = self.meshes[mesh_id]
         diag, upper, lower, rhs = _f64(diag), _f64(upper), _f64(lower), _f64(rhs)
         if len(diag) != n or len(rhs) != n or len(upper) != nf or len(lower) != nf:
             raise InvalidArgument("request arrays do not match the mesh")
+        if x is None:
+            x = np.zeros(n)
+        elif not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous
+                  and x.size == n):
+            raise InvalidArgument("x must be a contiguous float64 array of n_cells")
         t = _ll()
         _check(_lib.cfdb_server_submit(self._h, int(mesh_id), int(matrix_key), _dp(diag),
-                                       _dp(upper), _dp(lower), _dp(rhs), 1 if warm_start else 0,
-                                       float(rel_tol), int(max_iterations), C.byref(t)))
+                                       _dp(upper), _dp(lower), _dp(rhs), _dp(x),
+                                       1 if warm_start else 0, float(rel_tol),
+                                       int(max_iterations), C.byref(t)))
+        self._borrowed[t.value] = (diag, upper, lower, rhs, x)
         return t.value
 
-    def wait(self, ticket, n_cells=None):
-        x = np.zeros(n_cells) if n_cells else None
+    def wait(self, ticket):
+        """(x, SolveStats, (submit, start, finish) seconds since the server started)."""
         st = StatsStruct()
         times = (C.c_double * 3)()
-        _check(_lib.cfdb_server_wait(self._h, int(ticket), _dp(x) if x is not None else None,
-                                     C.byref(st), times))
-        return x, SolveStats._from(st), (times[0], times[1], times[2])
+        try:
+            _check(_lib.cfdb_server_wait(self._h, int(ticket), C.byref(st), times))
+        finally:
+            arrays = self._borrowed.pop(ticket, None)
+        return arrays[4], SolveStats._from(st), (times[0], times[1], times[2])
 
     def info(self) -> dict:
         i = ServerInfoStruct()
@@ -102,78 +114,139 @@ class Server:
                 "queued": i.queued, "completed": i.completed, "evictions": i.evictions}
 
 
+def _pinned(shape_or_array):
+    """Page-locked float64 numpy array (a copy of the array given, or zeros of a length)."""
+    import torch
+    if isinstance(shape_or_array, int):
+        return torch.zeros(shape_or_array, dtype=torch.float64).pin_memory().numpy()
+    a = np.ascontiguousarray(shape_or_array, dtype=np.float64)
+    return torch.from_numpy(a.copy()).pin_memory().numpy()
+
+
 @dataclass
 class MeshEntry:
+    """One pooled mesh: its server id, kind, size and page-locked request data: `variants`
+    coefficient sets (diag, upper, lower) and right-hand sides."""
     mesh_id: int
+    kind: str
     n: int
-    diag: np.ndarray
-    upper: np.ndarray
-    lower: np.ndarray
-    rhs: np.ndarray
+    matrices: list
+    rhs: list
+    free_x: list
 
 
-def run_load(server: Server, pool: list, rate_hz: float, duration_s: float, repeat_frac=0.3,
-             seed=0, coefficient_jitter=0.1, rel_tol=1e-8):
-    """Poisson arrivals at rate_hz for duration_s over the meshes in `pool` (MeshEntry). A
-    fraction repeat_frac repeats the previous matrix of its mesh with a warm start; the rest
-    carry new coefficients (the mesh's base matrix scaled per face by LogNormal(0, jitter)) and
-    a new right-hand side. Returns per-request records and summary statistics."""
+def make_pool(server: Server, pool_cases, variants=3, seed=0, coefficient_jitter=0.1,
+              x_buffers=4):
+    """Registers the meshes of `pool_cases` [(kind, case, diag, upper, lower, source)] and
+    prepares page-locked coefficient variants: the finalized matrix with its face coefficients
+    scaled by LogNormal(0, coefficient_jitter) (diagonal adjusted so row sums are kept) and
+    zero-mean random right-hand sides; `x_buffers` page-locked solution buffers per mesh (more
+    are allocated on demand when more requests of one mesh are in flight)."""
     rng = np.random.default_rng(seed)
-    arrivals = []
-    t = 0.0
-    while True:
-        t += rng.exponential(1.0 / rate_hz)
-        if t > duration_s:
-            break
-        arrivals.append(t)
-    last_key = {}
+    pool = []
+    for kind, c, d, u, l, b in pool_cases:
+        mid = server.add_mesh(c.n, c.owner, c.neighbour)
+        mats, rhs = [], []
+        for v in range(variants):
+            if v == 0:
+                dv, uv, lv = d, u, l
+            else:
+                sc = np.exp(coefficient_jitter * rng.standard_normal(len(u)))
+                uv, lv = u * sc, l * sc
+                dv = d.copy()
+                np.add.at(dv, c.owner, -(uv - u))
+                np.add.at(dv, c.neighbour, -(lv - l))
+            mats.append((_pinned(dv), _pinned(uv), _pinned(lv)))
+            r = b if v == 0 else rng.standard_normal(c.n)
+            rhs.append(_pinned(r - r.mean()))
+        pool.append(MeshEntry(mid, kind, c.n, mats, rhs, [_pinned(c.n) for _ in range(x_buffers)]))
+    return pool
+
+
+def run_load(server: Server, pool: list, rate_hz: float, n_requests: int, repeat_frac=0.3,
+             tet_frac=0.25, seed=0, rel_tol=1e-8, closed_loop=False, warm_start=True):
+    """Open-loop Poisson arrivals at rate_hz (closed_loop: each request submitted when the
+    previous one finished) of n_requests over the pool. A request picks tet meshes with
+    probability tet_frac, then a pool mesh of that kind uniformly. With probability repeat_frac
+    it repeats its mesh's previous matrix (same key: no re-upload) with a new right-hand side
+    and, if warm_start, starts from the resident solution; otherwise it carries the next
+    coefficient variant under a new key. Latency = finish - submit on the server clock."""
+    import queue as _q
+    rng = np.random.default_rng(seed)
+    by_kind = {}
+    for e in pool:
+        by_kind.setdefault(e.kind, []).append(e)
+    kinds = sorted(by_kind)
+    last = {}
     key_counter = [0]
     records = []
+    pending = _q.Queue()
     lock = threading.Lock()
-    pending = []
 
-    def waiter(ticket, meta):
-        _, st, times = server.wait(ticket)
-        with lock:
-            records.append(dict(meta, latency=times[2] - times[0], queue=times[1] - times[0],
-                                service=times[2] - times[1], iterations=st.iterations,
-                                converged=st.converged, true_residual=st.true_residual))
+    def collector():
+        while True:
+            item = pending.get()
+            if item is None:
+                return
+            ticket, e, x, meta = item
+            _, st, times = server.wait(ticket)
+            with lock:
+                e.free_x.append(x)
+                records.append(dict(meta, latency=times[2] - times[0], queue=times[1] - times[0],
+                                    service=times[2] - times[1], iterations=st.iterations,
+                                    converged=st.converged, residual=st.residual))
 
+    th = threading.Thread(target=collector, daemon=True)
+    th.start()
     t0 = time.perf_counter()
-    threads = []
-    for ta in arrivals:
-        now = time.perf_counter() - t0
-        if ta > now:
-            time.sleep(ta - now)
-        e = pool[int(rng.integers(len(pool)))]
-        repeat = e.mesh_id in last_key and rng.random() < repeat_frac
-        if repeat:
-            key, d, u, l, b = last_key[e.mesh_id]
-            warm = True
+    ta = 0.0
+    done_events = []
+    for i in range(n_requests):
+        if not closed_loop:
+            ta += rng.exponential(1.0 / rate_hz)
+            now = time.perf_counter() - t0
+            if ta > now:
+                time.sleep(ta - now)
+        kind = "tet" if ("tet" in by_kind and rng.random() < tet_frac) else \
+            ("box" if "box" in by_kind else kinds[0])
+        group = by_kind[kind]
+        e = group[int(rng.integers(len(group)))]
+        rep = e.mesh_id in last and rng.random() < repeat_frac
+        if rep:
+            key, mi = last[e.mesh_id]
         else:
             key_counter[0] += 1
             key = key_counter[0]
-            s = np.exp(coefficient_jitter * rng.standard_normal(len(e.upper)))
-            u, l = e.upper * s, e.lower * s
-            d = e.diag - (e.upper - u) - (e.lower - l)
-            b = rng.standard_normal(e.n)
-            b -= b.mean()
-            last_key[e.mesh_id] = (key, d, u, l, b)
-            warm = False
-        tk = server.submit(e.mesh_id, key, d, u, l, b, warm_start=warm, rel_tol=rel_tol)
-        th = threading.Thread(target=waiter, args=(tk, {"mesh": e.mesh_id, "n": e.n, "warm": warm,
-                                                        "arrival": ta}))
-        th.start()
-        threads.append(th)
-    for th in threads:
-        th.join()
+            mi = key % len(e.matrices)
+            last[e.mesh_id] = (key, mi)
+        bi = int(rng.integers(len(e.rhs)))
+        d, u, l = e.matrices[mi]
+        with lock:
+            x = e.free_x.pop() if e.free_x else _pinned(e.n)
+        ticket = server.submit(e.mesh_id, key, d, u, l, e.rhs[bi], x=x,
+                               warm_start=bool(rep and warm_start), rel_tol=rel_tol)
+        pending.put((ticket, e, x, {"mesh": e.mesh_id, "kind": e.kind, "n": e.n,
+                                    "repeat": bool(rep)}))
+        if closed_loop:
+            while True:
+                with lock:
+                    if len(records) == i + 1:
+                        break
+                time.sleep(0.0002)
+    pending.put(None)
+    th.join()
     wall = time.perf_counter() - t0
     lat = np.array([r["latency"] for r in records])
+    cells = sum(r["n"] for r in records)
     return records, {
-        "requests": len(records), "rate_hz": rate_hz, "wall_s": wall,
+        "requests": len(records), "rate_hz": None if closed_loop else rate_hz,
+        "closed_loop": closed_loop, "wall_s": wall,
         "solves_per_s": len(records) / wall if wall > 0 else 0.0,
+        "mcells_per_s": cells / wall / 1e6 if wall > 0 else 0.0,
         "p50_ms": float(np.percentile(lat, 50) * 1e3) if len(lat) else None,
         "p99_ms": float(np.percentile(lat, 99) * 1e3) if len(lat) else None,
         "mean_service_ms": float(np.mean([r["service"] for r in records]) * 1e3) if records else None,
+        "repeat_frac": float(np.mean([r["repeat"] for r in records])) if records else None,
+        "mean_iterations": float(np.mean([r["iterations"] for r in records])) if records else None,
         "all_converged": all(r["converged"] for r in records),
     }

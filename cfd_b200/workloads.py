@@ -84,3 +84,35 @@ def batch_box(edge, sigma=0.5, seed=0) -> PressureCase:
     from . import Mesh
     m = Mesh.box(edge, edge, edge)
     return _case(f"box{edge}", m, sigma=sigma, unit_rau=False, rhs_kind=1, seed=seed)
+
+
+# serving mix: box meshes with edge log-uniform in [16, 128] and jittered-tet meshes of 0.1-2M
+# cells, one tet request in four. The pool holds log-spaced sizes of each kind; a request picks
+# its kind, then a pool size uniformly (log-uniform in size).
+SERVE_BOX_EDGES = (16, 23, 32, 45, 64, 91, 128)
+SERVE_TET_EDGES = (26, 35, 46, 55, 69)  # 6 n^3 cells: 0.105M, 0.257M, 0.584M, 0.998M, 1.97M
+
+
+def serve_pool(seed=SEED_BASE + 4, box_edges=SERVE_BOX_EDGES, tet_edges=SERVE_TET_EDGES):
+    """Pressure cases of the serving pool, each with its finalized LDU coefficients:
+    [(kind, case, diag, upper, lower, source)]."""
+    from . import assemble_convection_diffusion
+    out = []
+    for i, e in enumerate(box_edges):
+        out.append(("box", graded_box(e, seed=seed + i)))
+    for i, e in enumerate(tet_edges):
+        out.append(("tet", tet(e, seed=seed + 100 + i)))
+    res = []
+    for kind, c in out:
+        up, lo = np.zeros(c.n_faces), np.zeros(c.n_faces)
+        dg, dv = np.zeros(c.n), np.zeros(c.n)
+        assemble_convection_diffusion(c.n, c.n_faces, c.owner, c.neighbour, c.flux, c.gamma,
+                                      c.delta, 0.0, up, lo, dg, dv)  # on the device
+        d, s = c.finalize(up, lo, dg, dv)
+        res.append((kind, c, d, up, lo, s))
+    return res
+
+
+def graded_box(edge, sigma=0.5, seed=0) -> PressureCase:
+    """Uniform box of the serving mix (rAU log-normal, random zero-mean source)."""
+    return batch_box(edge, sigma=sigma, seed=seed)

@@ -45,14 +45,16 @@ int cfdb_server_destroy(cfdb_server* s);
 int cfdb_server_add_mesh(cfdb_server* s, int n_cells, int n_faces, const int* owner,
                          const int* neighbour, int* mesh_id);
 /* Queues one solve A x = rhs to relative residual rel_tol (x0 = 0, or the resident solution of
- * the same matrix_key with warm_start). Host arrays are copied at submit. */
+ * the same matrix_key with warm_start). The host arrays are borrowed, as for an asynchronous
+ * copy: diag / upper / lower / rhs must stay valid and unchanged, and x (n_cells, may be NULL)
+ * receives the solution, by the time cfdb_server_wait returns for the ticket. Page-locked
+ * arrays are copied at full link speed. */
 int cfdb_server_submit(cfdb_server* s, int mesh_id, long long matrix_key, const double* diag,
-                       const double* upper, const double* lower, const double* rhs,
+                       const double* upper, const double* lower, const double* rhs, double* x,
                        int warm_start, double rel_tol, int max_iterations, long long* ticket);
-/* Blocks until the ticket is done; x (n_cells, may be NULL) receives the solution, times (3
- * doubles, may be NULL) the submit / start / finish times in seconds since server creation. */
-int cfdb_server_wait(cfdb_server* s, long long ticket, double* x, cfdb_stats* stats,
-                     double* times);
+/* Blocks until the ticket is done; times (3 doubles, may be NULL) receives the submit / start /
+ * finish times in seconds since server creation. */
+int cfdb_server_wait(cfdb_server* s, long long ticket, cfdb_stats* stats, double* times);
 int cfdb_server_info(cfdb_server* s, cfdb_server_info_t* info);
 
 #ifdef __cplusplus

@@ -29,7 +29,7 @@ def test_same_result_alone_and_in_the_mix(gpu):
     for case, d, u, l, b in cases:
         s = Server(slots=1)
         mid = s.add_mesh(case.n, case.owner, case.neighbour)
-        x, st, _ = s.wait(s.submit(mid, 1, d, u, l, b), case.n)
+        x, st, _ = s.wait(s.submit(mid, 1, d, u, l, b))
         assert st.converged
         alone.append(x)
         s.close()
@@ -37,7 +37,7 @@ def test_same_result_alone_and_in_the_mix(gpu):
     ids = [s.add_mesh(c.n, c.owner, c.neighbour) for c, *_ in cases]
     tickets = [s.submit(mid, 1, d, u, l, b) for mid, (c, d, u, l, b) in zip(ids, cases)]
     tickets += [s.submit(mid, 1, d, u, l, b) for mid, (c, d, u, l, b) in zip(ids, cases)]
-    outs = [s.wait(t, cases[i % len(cases)][0].n) for i, t in enumerate(tickets)]
+    outs = [s.wait(t) for t in tickets]
     for i, (x, st, times) in enumerate(outs):
         assert st.converged
         assert np.array_equal(x, alone[i % len(cases)])  # bit-identical alone and in the mix
@@ -54,11 +54,11 @@ def test_warm_start_and_budget_eviction(gpu):
     s = Server(slots=2, hbm_budget_bytes=2.5e6)
     ids = [s.add_mesh(c.n, c.owner, c.neighbour) for c, *_ in cases]
     (c0, d, u, l, b) = cases[0]
-    x1, st1, _ = s.wait(s.submit(ids[0], 7, d, u, l, b), c0.n)
-    x2, st2, _ = s.wait(s.submit(ids[0], 7, d, u, l, b, warm_start=True), c0.n)
+    x1, st1, _ = s.wait(s.submit(ids[0], 7, d, u, l, b))
+    x2, st2, _ = s.wait(s.submit(ids[0], 7, d, u, l, b, warm_start=True))
     assert st1.converged and st2.converged and st2.iterations <= 1 < st1.iterations
     for mid, (c, d, u, l, b) in zip(ids, cases):
-        x, st, _ = s.wait(s.submit(mid, 1, d, u, l, b), c.n)
+        x, st, _ = s.wait(s.submit(mid, 1, d, u, l, b))
         assert st.converged
         a = O.ldu_to_csr(O.build_pattern(c.n, c.owner, c.neighbour), d, u, l)
         assert np.linalg.norm(b - a.matvec(x)) <= 1.05e-8 * np.linalg.norm(b)

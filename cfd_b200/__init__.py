@@ -678,9 +678,9 @@ class DeviceSolver:
 class Tuning:
     """Launch-shape / schedule knobs of the device plan (cfdb_tuning)."""
     target_tiles: int = 148 * 8
-    wide_row: int = 24
-    lanes_div: int = 6
-    fuse_first: int = 1
+    wide_row: int = 48
+    lanes_div: int = 16
+    fuse_first: int = 0
 
     def _c(self):
         return TuningStruct(int(self.target_tiles), int(self.wide_row), int(self.lanes_div),

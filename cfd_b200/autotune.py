@@ -27,8 +27,8 @@ from . import Tuning
 
 CANDIDATES = {
     "target_tiles": [148 * 4, 148 * 8, 148 * 16],
-    "wide_row": [16, 24, 32, 64],
-    "lanes_div": [3, 4, 6, 8],
+    "wide_row": [24, 32, 48, 64],
+    "lanes_div": [8, 12, 16, 32],
     "fuse_first": [0, 1],
 }
 

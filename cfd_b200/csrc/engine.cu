@@ -19,6 +19,8 @@ struct SellBuild {
     std::vector<double> val;
     std::vector<int> src;
     bool with_src = false;
+    bool sort = false;      // reorder rows by length within aligned windows of kSellRows
+    std::vector<int> perm;  // row at each position (when sort)
 };
 
 // Appends rows [0, n_rows) of a CSR block (n_pad >= n_rows, multiple of 32) whose first row has
@@ -26,16 +28,29 @@ struct SellBuild {
 // with value 0. src_of (optional): value-source index per CSR entry (shifted by src_off).
 void sell_append(SellBuild& sb, int n_rows, int n_pad, const int* rp, const int* ci,
                  const double* va, const int* src_of, int col_off, int src_off, int pad_col) {
+    // order[q]: block row at block position q (identity unless sorting)
+    std::vector<int> order(static_cast<size_t>(n_pad));
+    std::iota(order.begin(), order.end(), 0);
+    auto len_of = [&](int i) { return i < n_rows ? rp[i + 1] - rp[i] : -1; };
+    if (sb.sort) {
+        for (int w0 = 0; w0 < n_pad; w0 += kSellRows) {
+            const int w1 = std::min(n_pad, w0 + kSellRows);
+            std::stable_sort(order.begin() + w0, order.begin() + w1,
+                             [&](int a, int b) { return len_of(a) > len_of(b); });
+        }
+        const int row0 = static_cast<int>(sb.perm.size());
+        for (int q = 0; q < n_pad; ++q) sb.perm.push_back(row0 + order[q]);
+    }
     for (int s0 = 0; s0 < n_pad; s0 += 32) {
         int width = 0;
-        for (int i = s0; i < s0 + 32 && i < n_rows; ++i) width = std::max(width, rp[i + 1] - rp[i]);
+        for (int q = s0; q < s0 + 32; ++q) width = std::max(width, len_of(order[q]));
         const int base = sb.slice.back();
         const size_t slots = static_cast<size_t>(width) * 32;
         sb.col.resize(base + slots, pad_col);
         sb.val.resize(base + slots, 0.0);
         if (sb.with_src) sb.src.resize(base + slots, -1);
         for (int lane = 0; lane < 32; ++lane) {
-            const int i = s0 + lane;
+            const int i = order[s0 + lane];
             if (i >= n_rows) continue;
             const int len = rp[i + 1] - rp[i];
             for (int k = 0; k < len; ++k) {
@@ -225,26 +240,32 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         d.n_tiles = static_cast<int>(tsys.size());
         d.n_tiles_nc = nc_tiles < 0 ? d.n_tiles : nc_tiles;
         d.tiles.row = arena_.upload(trow, st);
-        d.tiles.sys = arena_.upload(tsys, st);
-        // fine tiles: one row per warp, for the warp-per-row (CSR) operators
-        std::vector<int> frow, fsys;
-        int nc_fine = -1;
+        d.tiles.sys = n_sys_ > 1 ? arena_.upload(tsys, st) : nullptr;
+    }
+    // Launch tiles of one operator over the rows of `row_level` of the systems `include`
+    // selects (a prefix in batch order); `nc` marks the systems that continue past that level.
+    auto op_tiles = [&](DevSell64_32& m, int fmt, int row_level, auto include, auto nc) {
+        const int rpt = fmt == kFmtSell ? kSellRows : (fmt <= 32 ? kFineRows : kBlock / fmt);
+        m.block = fmt == kFmtSell ? kBlock : (fmt <= 32 ? kFineRows * fmt : kBlock);
+        std::vector<int> trow, tsys;
+        int n_nc = -1, end = 0;
         for (int k = 0; k < n_sys_; ++k) {
             const int s = perm_[k];
-            if (L[s] <= l) continue;
-            if (L[s] - 1 == l && nc_fine < 0) nc_fine = static_cast<int>(fsys.size());
-            const int pad = round_up(rows_at(s, l), 32);
-            for (int r = 0; r < pad; r += kFineRows) {
-                frow.push_back(off[l][s] + r);
-                fsys.push_back(k);
+            if (!include(s)) continue;
+            if (!nc(s) && n_nc < 0) n_nc = static_cast<int>(tsys.size());
+            const int pad = round_up(rows_at(s, row_level), 32);
+            for (int r = 0; r < pad; r += rpt) {
+                trow.push_back(off[row_level][s] + r);
+                tsys.push_back(k);
             }
+            end = off[row_level][s] + pad;
         }
-        frow.push_back(d.n_rows);
-        d.n_tiles_f = static_cast<int>(fsys.size());
-        d.n_tiles_f_nc = nc_fine < 0 ? d.n_tiles_f : nc_fine;
-        d.tiles_f.row = arena_.upload(frow, st);
-        d.tiles_f.sys = arena_.upload(fsys, st);
-    }
+        trow.push_back(end);
+        m.n_tiles = static_cast<int>(tsys.size());
+        m.n_tiles_nc = n_nc < 0 ? m.n_tiles : n_nc;
+        m.tiles.row = arena_.upload(trow, st);
+        m.tiles.sys = n_sys_ > 1 ? arena_.upload(tsys, st) : nullptr;
+    };
     // level-0 operator (values filled per solve) + value maps
     {
         SellBuild sb;
@@ -285,6 +306,7 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         d.wd64 = arena_.alloc<double>(d.n_rows);
         if (need32_) d.wd32 = arena_.alloc<float>(d.n_rows);
         dinv0_ = arena_.alloc<double>(d.n_rows);
+        op_tiles(d.a, kFmtSell, 0, [](int) { return true; }, [&](int s) { return L[s] > 1; });
     }
     // coarser levels, transfers
     for (int l = 0; l < n_levels_; ++l) {
@@ -293,7 +315,7 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         // `pick(s)`, columns shifted into the target level's concatenated index space. Wide
         // operators (more than kWideRow entries per row on average) are stored as CSR for the
         // warp-per-row kernels unless the engine is in ordered (bit-reproducible) mode.
-        auto build_op = [&](auto pick, int col_level, DevSell64_32& m) {
+        auto build_op = [&](auto pick, int col_level, int row_level, DevSell64_32& m) {
             long long nnz = 0, rows = 0;
             for (int k = 0; k < n_sys_; ++k) {
                 const int s = perm_[k];
@@ -301,11 +323,20 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
                 nnz += pick(s).nnz();
                 rows += pick(s).n_rows;
             }
-            // lanes per row: about six entries per lane, 8..32 lanes
+            // lanes per row: about lanes_div entries per lane, and enough lanes in all to keep
+            // ~150K threads busy on operators with few, long rows; never more than the row length
             const double avg = rows > 0 ? static_cast<double>(nnz) / static_cast<double>(rows) : 0.0;
+            constexpr double kFillThreads = 148.0 * 1024.0;
             int lanes = 4;
-            while (lanes < 32 && lanes * std::max(tuning_.lanes_div, 1) < avg) lanes *= 2;
-            const bool wide = !ordered_ && rows > 0 && avg > tuning_.wide_row;
+            while (lanes < 256 && 2.0 * lanes <= std::max(avg, 4.0) &&
+                   (lanes * std::max(tuning_.lanes_div, 1) < avg ||
+                    static_cast<double>(lanes) * static_cast<double>(rows) < kFillThreads)) {
+                lanes *= 2;
+            }
+            // CSR lane groups for long rows, and for operators too short to fill the GPU with one
+            // thread per row; SELL (rows sorted by length within 256-row windows) otherwise
+            const bool wide = !ordered_ && rows > 0 &&
+                              (avg > tuning_.wide_row || static_cast<double>(rows) < kFillThreads);
             if (wide) {
                 CsrBuild cbd;
                 for (int k = 0; k < n_sys_; ++k) {
@@ -317,16 +348,22 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
                 }
                 m.n_slices = static_cast<int>(cbd.rp.size()) - 1;
                 m.slots = cbd.rp.back();
+                // slack for the aligned quad loads of the last row
+                cbd.col.insert(cbd.col.end(), 4, 0);
+                cbd.val.insert(cbd.val.end(), 4, 0.0);
                 const int* dp = arena_.upload(cbd.rp, st);
                 const int* dc = arena_.upload(cbd.col, st);
                 if (need64_) m.s64 = {dp, dc, arena_.upload(cbd.val, st), lanes};
                 if (need32_) m.s32 = {dp, dc, arena_.upload(to_float(cbd.val), st), lanes};
+                op_tiles(m, lanes, row_level, [&](int s) { return L[s] - 1 > l; }, [](int) { return true; });
             } else {
                 SellBuild sb;
+                sb.sort = true;
                 for (int k = 0; k < n_sys_; ++k) {
                     const int s = perm_[k];
                     if (L[s] - 1 <= l) continue;
                     const HostCsr& a = pick(s);
+                    if (static_cast<int>(sb.perm.size()) != off[row_level][s]) fail(1, "engine: operator rows out of order");
                     sell_append(sb, a.n_rows, round_up(a.n_rows, 32), a.rp.data(), a.ci.data(), a.va.data(),
                                 nullptr, off[col_level][s], 0, off[col_level][s]);
                 }
@@ -334,8 +371,10 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
                 m.slots = sb.slice.back();
                 const int* dp = arena_.upload(sb.slice, st);
                 const int* dc = arena_.upload(sb.col, st);
-                if (need64_) m.s64 = {dp, dc, arena_.upload(sb.val, st), kFmtSell};
-                if (need32_) m.s32 = {dp, dc, arena_.upload(to_float(sb.val), st), kFmtSell};
+                const int* dperm = arena_.upload(sb.perm, st);
+                if (need64_) m.s64 = {dp, dc, arena_.upload(sb.val, st), kFmtSell, dperm};
+                if (need32_) m.s32 = {dp, dc, arena_.upload(to_float(sb.val), st), kFmtSell, dperm};
+                op_tiles(m, kFmtSell, row_level, [&](int s) { return L[s] - 1 > l; }, [](int) { return true; });
             }
             m.nnz = nnz;
         };
@@ -348,13 +387,13 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
                 const std::vector<double> dinv = inverse_diagonal(a);
                 for (int i = 0; i < a.n_rows; ++i) wd[off[l][s] + i] = weight_ * dinv[i];
             }
-            build_op([&](int s) -> const HostCsr& { return systems[s].h->a[l]; }, l, d.a);
+            build_op([&](int s) -> const HostCsr& { return systems[s].h->a[l]; }, l, l, d.a);
             if (need64_) d.wd64 = arena_.upload(wd, st);
             if (need32_) d.wd32 = arena_.upload(to_float(wd), st);
         }
         if (l + 1 < n_levels_) {
-            build_op([&](int s) -> const HostCsr& { return systems[s].h->p[l]; }, l + 1, d.p);
-            build_op([&](int s) -> const HostCsr& { return systems[s].h->r[l]; }, l, d.r);
+            build_op([&](int s) -> const HostCsr& { return systems[s].h->p[l]; }, l + 1, l, d.p);
+            build_op([&](int s) -> const HostCsr& { return systems[s].h->r[l]; }, l, l + 1, d.r);
         }
         // vectors (zero-initialised)
         auto vec64 = [&](int n) {
@@ -614,14 +653,42 @@ template <> Sell<double> vs_sel<double>(const Sell<double>& a, const Sell<float>
 template <> Sell<float> vs_sel<float>(const Sell<double>&, const Sell<float>& b) { return b; }
 } // namespace
 
+// Buffer holding the first pre-smoothing iterate of level l, chosen so that after the
+// remaining pre sweeps and the post sweeps the iterate lands in x.
+template <class T> T* Engine::start_buffer(int l) const {
+    T* x = vx<T>(lv_[l].x64, lv_[l].x32);
+    T* y = vx<T>(lv_[l].y64, lv_[l].y32);
+    const bool fuse = sweeps_ >= 2 && tuning_.fuse_first != 0;
+    const int writes_pre = fuse ? sweeps_ - 1 : sweeps_;
+    T* target = (sweeps_ % 2 == 0) ? x : y;
+    return (writes_pre % 2 == 1) ? target : (target == x ? y : x);
+}
+
+X1Out Engine::x1_out(Mode mode) const {
+    X1Out o{};
+    const bool fuse = sweeps_ >= 2 && tuning_.fuse_first != 0;
+    if (mode == Mode::Jacobi || !has_amg_ || sweeps_ == 0 || fuse || n_levels_ < 2) return o;
+    const DevLevel& d = lv_[0];
+    o.n = d.n_rows_nc;
+    if (mode == Mode::AmgMixed) {
+        o.wd32 = d.wd32;
+        o.x32 = start_buffer<float>(0);
+    } else {
+        o.wd64 = d.wd64;
+        o.x64 = start_buffer<double>(0);
+    }
+    return o;
+}
+
 template <class T>
-void Engine::enqueue_vcycle_t(bool fused_final, int flexible) {
+void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
     cudaStream_t s = stream_;
     const SysState* stv = st_;
     const int L = n_levels_;
     // final pre-smoothing buffer so that after `sweeps_` post sweeps the iterate lands in x
     const bool fuse = sweeps_ >= 2 && tuning_.fuse_first != 0;
-    const int writes_pre = fuse ? sweeps_ - 1 : sweeps_;
+    // unfused schedule: each restriction also writes the coarser level's first sweep
+    const bool x1_by_restrict = !fuse && sweeps_ > 0;
     auto X = [&](int l) { return vx<T>(lv_[l].x64, lv_[l].x32); };
     auto Y = [&](int l) { return vx<T>(lv_[l].y64, lv_[l].y32); };
     auto Tv = [&](int l) { return vx<T>(lv_[l].t64, lv_[l].t32); };
@@ -645,11 +712,8 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible) {
         int second; // grid
         int block;
     };
-    auto TL = [&](int l, const DevSell64_32& m, bool nc) -> Launch {
-        const DevLevel& d = lv_[l];
-        const int fmt = sizeof(T) == 8 ? m.s64.fmt : m.s32.fmt;
-        if (fmt != kFmtSell) return {d.tiles_f, nc ? d.n_tiles_f_nc : d.n_tiles_f, kFineRows * fmt};
-        return {d.tiles, nc ? d.n_tiles_nc : d.n_tiles, kBlock};
+    auto TL = [&](int, const DevSell64_32& m, bool nc) -> Launch {
+        return {m.tiles, nc ? m.n_tiles_nc : m.n_tiles, m.block};
     };
     std::vector<T*> cur(L, nullptr);
     // ---- down ----
@@ -661,11 +725,23 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible) {
         const double sb = l == 0 ? sb0 : sv;
         T* x = X(l);
         T* y = Y(l);
-        T* target = (sweeps_ % 2 == 0) ? x : y;
-        T* start = (writes_pre % 2 == 1) ? target : (target == x ? y : x);
+        T* start = start_buffer<T>(l);
+        const bool x1_ready = l == 0 ? x1_ready0 : x1_by_restrict;
         if (sweeps_ == 0) {
             CFDB_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * d.n_rows_nc, s));
             cur[l] = x;
+        } else if (x1_ready) {
+            // first sweep already in `start` (written with the right-hand side)
+            const auto ta = TL(l, d.a, true);
+            T* c = start;
+            for (int k = 1; k < sweeps_; ++k) {
+                T* o = c == x ? y : x;
+                if (l == 0) k_vc_jacobi<T, double><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, c, o);
+                else k_vc_jacobi<T, T><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), c, o);
+                mark("smooth", l, spmv_b(d.a, n, n) + sv * n + sb * n);
+                c = o;
+            }
+            cur[l] = c;
         } else {
             const auto ta = TL(l, d.a, true);
             if (l == 0) {
@@ -690,8 +766,12 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible) {
         mark("residual", l, spmv_b(d.a, n, n) + sb * n);
         const DevLevel& nx = lv_[l + 1];
         const auto tq = TL(l + 1, d.r, false);
-        k_vc_spmv<T><<<tq.second, tq.block, 0, s>>>(R(l), tq.first, stv, Tv(l), Bv(l + 1));
-        mark("restrict", l, spmv_b(d.r, nx.n_rows, n));
+        const bool next_x1 = x1_by_restrict && l + 2 < L && nx.n_rows_nc > 0;
+        k_vc_spmv<T><<<tq.second, tq.block, 0, s>>>(R(l), tq.first, stv, Tv(l), Bv(l + 1),
+                                                    next_x1 ? WD(l + 1) : nullptr,
+                                                    next_x1 ? start_buffer<T>(l + 1) : nullptr,
+                                                    next_x1 ? nx.n_rows_nc : 0);
+        mark("restrict", l, spmv_b(d.r, nx.n_rows, n) + (next_x1 ? 2.0 * sv * nx.n_rows_nc : 0.0));
     }
     // ---- coarsest blocks (dense inverse of each multi-level system's coarsest operator) ----
     const Control ctl{n_active_, error_};
@@ -740,9 +820,9 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible) {
     }
 }
 
-void Engine::enqueue_vcycle(Mode mode, bool fused_final, int flexible) {
-    if (mode == Mode::AmgMixed) enqueue_vcycle_t<float>(fused_final, flexible);
-    else enqueue_vcycle_t<double>(fused_final, flexible);
+void Engine::enqueue_vcycle(Mode mode, bool fused_final, int flexible, bool x1_ready0) {
+    if (mode == Mode::AmgMixed) enqueue_vcycle_t<float>(fused_final, flexible, x1_ready0);
+    else enqueue_vcycle_t<double>(fused_final, flexible, x1_ready0);
 }
 
 // Preconditioner output z (level-0 iterate) in the precision of the mode.
@@ -751,9 +831,11 @@ void Engine::enqueue_init(Mode mode) {
     const Control ctl{n_active_, error_};
     const double n = d.n_rows;
     const double a0 = static_cast<double>(d.a.nnz) * 12.0 + 4.0 * (n + 1.0) + 16.0 * n;
+    const X1Out x1o = x1_out(mode);
+    const double x1b = (mode == Mode::AmgMixed ? 8.0 : 16.0) * x1o.n;
     k_cg_init<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, r_, partials_, counters_,
-                                                  sys_tile0_, ctl);
-    mark("cg_init", 0, a0 + 16.0 * n);
+                                                  sys_tile0_, ctl, x1o);
+    mark("cg_init", 0, a0 + 16.0 * n + x1b);
     const int flexible = mode == Mode::AmgMixed ? 1 : 0;
     if (mode == Mode::Jacobi) {
         k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, nullptr, q_, partials_,
@@ -761,7 +843,7 @@ void Engine::enqueue_init(Mode mode) {
         mark("cg_rz", 0, 24.0 * n);
         return;
     }
-    enqueue_vcycle(mode, fused_final_, flexible);
+    enqueue_vcycle(mode, fused_final_, flexible, x1o.n > 0);
     if (!fused_final_) enqueue_rz(mode, flexible);
 }
 
@@ -795,12 +877,14 @@ void Engine::enqueue_iteration(Mode mode) {
     k_cg_spmv_pq<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, p_, q_, partials_, counters_,
                                                      sys_tile0_, ctl);
     mark("cg_spmv_pq", 0, a0);
+    const X1Out x1o = x1_out(mode);
+    const double x1b = (mode == Mode::AmgMixed ? 8.0 : 16.0) * x1o.n;
     k_cg_xr<<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, x_, r_, p_, q_, partials_, counters_, sys_tile0_,
-                                                ctl, mode == Mode::AmgMixed ? 1 : 0);
-    mark("cg_xr", 0, 48.0 * n);
+                                                ctl, mode == Mode::AmgMixed ? 1 : 0, x1o);
+    mark("cg_xr", 0, 48.0 * n + x1b);
     if (mode == Mode::AmgMixed) {
         k_cg_true_check<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, r_, partials_,
-                                                            counters_, sys_tile0_, ctl);
+                                                            counters_, sys_tile0_, ctl, x1o);
         mark("cg_true_check", 0, 0.0);
     }
     const int flexible = mode == Mode::AmgMixed ? 1 : 0;
@@ -810,7 +894,7 @@ void Engine::enqueue_iteration(Mode mode) {
         mark("cg_rz", 0, 24.0 * n);
         return;
     }
-    enqueue_vcycle(mode, fused_final_, flexible);
+    enqueue_vcycle(mode, fused_final_, flexible, x1o.n > 0);
     if (!fused_final_) enqueue_rz(mode, flexible);
 }
 
@@ -831,6 +915,14 @@ std::vector<ProfRecord> Engine::profile(Mode mode, int reps) {
     if (mode != Mode::Jacobi && !has_amg_) fail(5, "profile: no AMG hierarchy set");
     std::vector<ProfRecord> out;
     std::vector<int> count;
+    // b = 1 on every real row, x = 0: a nonzero residual whatever the engine held before (the
+    // right-hand side and the guess are overwritten by the next solve anyway)
+    {
+        const int n = lv_[0].n_rows;
+        k_fill_rows<<<grid_of(n), 256, 0, stream_>>>(n, row_map_, 1.0, b_);
+        CFDB_CUDA(cudaMemsetAsync(x_, 0, sizeof(double) * n, stream_));
+        launches_ += 1;
+    }
     for (int rep = 0; rep < std::max(reps, 1); ++rep) {
         // every system active, never converging: the profiled kernels do all their work
         std::vector<SysState> hs(n_sys_);
@@ -995,8 +1087,8 @@ void Engine::apply_vcycle(Mode mode, const std::vector<int>&) {
     SysState* keep = st_;
     st_ = nullptr;
     try {
-        if (mode == Mode::AmgMixed) enqueue_vcycle_t<float>(false, 0);
-        else enqueue_vcycle_t<double>(false, 0);
+        if (mode == Mode::AmgMixed) enqueue_vcycle_t<float>(false, 0, false);
+        else enqueue_vcycle_t<double>(false, 0, false);
     } catch (...) {
         st_ = keep;
         throw;

@@ -29,9 +29,10 @@ struct SystemSpec {
 // operators switch between the ordered SELL sum and the lane-group CSR sum).
 struct Tuning {
     int target_tiles = 148 * 8; // SELL tiles (CTAs of 256 threads) per level
-    int wide_row = 24;          // average row length above which CSR lane groups are used
-    int lanes_div = 6;          // lanes per CSR row ~ average row length / lanes_div (4..32)
-    int fuse_first = 1;         // first two smoothing sweeps in one kernel (x1 recomputed)
+    int wide_row = 48;          // average row length above which CSR lane groups are used
+    int lanes_div = 16;         // lanes per CSR row ~ average row length / lanes_div (4..256),
+                                // and at least enough lanes to give ~150K threads per operator
+    int fuse_first = 0;         // first two smoothing sweeps in one kernel (x1 recomputed)
 };
 
 struct SolveRequest {
@@ -131,16 +132,19 @@ private:
         int n_slices = 0;     // SELL slices, or CSR rows
         long long slots = 0;  // stored entries (SELL: with padding)
         long long nnz = 0;    // algorithmic nonzeros
+        // launch tiles of the operator's own row space: kSellRows rows (SELL), 8 rows (CSR,
+        // G <= 32) or 256 / G rows (CSR, G > 32); block = threads per CTA
+        Tiles tiles{};
+        int n_tiles = 0;
+        int n_tiles_nc = 0;   // tiles of systems that continue to a coarser level
+        int block = kBlock;
     };
     struct DevLevel {
         int n_rows = 0;     // all present systems (padded)
         int n_rows_nc = 0;  // prefix of systems that continue to a coarser level
         int n_tiles = 0;
         int n_tiles_nc = 0;
-        Tiles tiles{};       // runs of whole slices (SELL operators, reductions)
-        int n_tiles_f = 0;   // one row per warp (CSR operators)
-        int n_tiles_f_nc = 0;
-        Tiles tiles_f{};
+        Tiles tiles{};       // runs of whole slices (the reductions of the Krylov kernels)
         DevSell64_32 a, p, r;
         double* wd64 = nullptr;
         float* wd32 = nullptr;
@@ -150,8 +154,12 @@ private:
     };
 
     void capture_graphs(Mode mode);
-    void enqueue_vcycle(Mode mode, bool fused_final, int flexible);
-    template <class T> void enqueue_vcycle_t(bool fused_final, int flexible);
+    // x1_ready0: the level-0 first pre-smoothing sweep was written by the residual producer
+    void enqueue_vcycle(Mode mode, bool fused_final, int flexible, bool x1_ready0);
+    template <class T> void enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0);
+    template <class T> T* start_buffer(int l) const;
+    // where the residual producers of `mode` write the level-0 first sweep (n = 0: nowhere)
+    X1Out x1_out(Mode mode) const;
     void enqueue_init(Mode mode);
     void enqueue_iteration(Mode mode);
     void enqueue_rz(Mode mode, int flexible);

@@ -24,14 +24,19 @@
 namespace cfdb {
 
 constexpr int kBlock = 256;
+// Rows of a SELL tile of the V-cycle kernels (one row per thread); also the window within which
+// a SELL operator's rows may be reordered by length.
+constexpr int kSellRows = kBlock;
 
 // Storage of one sparse operator of a level, selected by `fmt`:
 //  0 (kFmtSell): SELL-32, one thread per row; `slice` = slice offsets. Row sums keep the CSR
 //     order.
-//  G in {2, 4, 8, 16, 32}: CSR with G lanes per row; `slice` = row offsets. Used for wide
-//     coarse-level rows (tens to hundreds of entries), where one thread per row would serialise
-//     long load chains; lanes sum strided entries and combine them with a fixed butterfly
-//     (deterministic, but not the sequential CSR order).
+//  G in {4, 8, 16, 32, 64, 128, 256}: CSR with G lanes per row; `slice` = row offsets. Used
+//     for wide coarse-level rows (tens to thousands of entries), where one thread per row would
+//     serialise long load chains; lanes sum strided entries and combine them with a fixed
+//     butterfly (and, above 32 lanes, a fixed-order sum over the row's warps): deterministic,
+//     but not the sequential CSR order. Tiles of a CSR operator hold 8 rows (G <= 32, blockDim
+//     8 G) or 256 / G rows (G > 32, blockDim 256).
 enum : int { kFmtSell = 0 };
 
 template <class T> struct Sell {
@@ -39,11 +44,14 @@ template <class T> struct Sell {
     const int* col;
     const T* val;
     int fmt;
+    // SELL only: row held at each position (rows sorted by length, longest first, within each
+    // aligned window of kSellRows positions, which cuts slice padding); null = identity
+    const int* perm = nullptr;
 };
 
 struct Tiles {
     const int* row; // n_tiles + 1 first rows
-    const int* sys; // n_tiles system ids
+    const int* sys; // n_tiles system ids (null when the plan holds one system: all 0)
 };
 
 // Per-system Krylov state (device resident; host reads it only at the end of a solve).
@@ -143,8 +151,10 @@ template <class T> __device__ __forceinline__ T madd(T s, T a, T b) {
     else return fmaf(a, b, s);
 }
 
-// Row sum of a SELL row: sum_k val[k] * xa(col[k]) in CSR order. Four entries are loaded
-// before they are accumulated so that several loads are in flight per thread.
+// Row sum of a SELL row: sum_k val[k] * xa(col[k]) in CSR order. Entries are taken in batches
+// of four, software-pipelined: the column / value loads of the next batch are issued before the
+// gathers of the current one, so a thread keeps two batches of the row in flight. Every row of
+// a slice has the slice's width, so the batch predicates are warp-uniform.
 template <class T, class XA>
 __device__ __forceinline__ T sell_row_sum(const Sell<T>& m, int row, XA xa) {
     const int slice = row >> 5;
@@ -152,20 +162,40 @@ __device__ __forceinline__ T sell_row_sum(const Sell<T>& m, int row, XA xa) {
     int k = __ldg(&m.slice[slice]) + lane;
     const int end = __ldg(&m.slice[slice + 1]);
     T s = T(0);
-    for (; k + 96 < end; k += 128) {
-        T v[4], xv[4];
-        int c[4];
+    if (k >= end) return s;
+    T v[4];
+    int c[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const bool ok = k + 32 * u < end;
+        v[u] = ok ? __ldg(&m.val[k + 32 * u]) : T(0);
+        c[u] = ok ? __ldg(&m.col[k + 32 * u]) : -1;
+    }
+    for (;;) {
+        const int kn = k + 128;
+        const bool more = kn < end;
+        T vn[4];
+        int cn[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            v[u] = __ldg(&m.val[k + 32 * u]);
-            c[u] = __ldg(&m.col[k + 32 * u]);
+            const bool ok = more && kn + 32 * u < end;
+            vn[u] = ok ? __ldg(&m.val[kn + 32 * u]) : T(0);
+            cn[u] = ok ? __ldg(&m.col[kn + 32 * u]) : -1;
         }
+        T xv[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) xv[u] = xa(c[u]);
+        for (int u = 0; u < 4; ++u) xv[u] = c[u] >= 0 ? xa(c[u]) : T(0);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) s = madd<T>(s, v[u], xv[u]);
+        for (int u = 0; u < 4; ++u)
+            if (c[u] >= 0) s = madd<T>(s, v[u], xv[u]);
+        if (!more) break;
+        k = kn;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            v[u] = vn[u];
+            c[u] = cn[u];
+        }
     }
-    for (; k < end; k += 32) s = madd<T>(s, __ldg(&m.val[k]), xa(__ldg(&m.col[k])));
     return s;
 }
 
@@ -217,34 +247,108 @@ __device__ __forceinline__ T sell_row(const Sell<T>& m, int row, const X* __rest
     return sell_row_sum(m, row, [x](int j) { return static_cast<T>(x[j]); });
 }
 
-// CSR row sum by a group of G lanes (G a power of two dividing 32): lane `sub` of the group
-// takes entries sub, sub+G, ..., two at a time; partial sums are combined with a fixed
-// butterfly over the group. Every lane of the group returns the same total. All lanes of the
-// warp must call it (the shuffles use the full mask).
+// Four consecutive values from a 16-byte aligned address.
+__device__ __forceinline__ void ld4(const float* p, float (&v)[4]) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = q.x;
+    v[1] = q.y;
+    v[2] = q.z;
+    v[3] = q.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&v)[4]) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = b.x;
+    v[3] = b.y;
+}
+
+// Partial CSR row sum of one lane. The row is read in aligned quads (16-byte vector loads of
+// columns and values): lane `sub` takes quads sub, sub + G, ... of the row's aligned span, two
+// quads per pass, and masks the entries outside [row begin, row end). CSR arrays carry four
+// entries of slack so the last quad never reads past them.
+template <class T, class XA>
+__device__ __forceinline__ T csr_lane_sum(const Sell<T>& m, int row, int sub, int G, XA xa) {
+    const int b = __ldg(&m.slice[row]);
+    const int e = __ldg(&m.slice[row + 1]);
+    T s = T(0);
+    for (int k = (b & ~3) + 4 * sub; k < e; k += 8 * G) {
+        const int k2 = k + 4 * G;
+        const bool two = k2 < e;
+        int c[8];
+        T v[8], xv[8];
+        {
+            const int4 q = __ldg(reinterpret_cast<const int4*>(m.col + k));
+            c[0] = q.x;
+            c[1] = q.y;
+            c[2] = q.z;
+            c[3] = q.w;
+            T t[4];
+            ld4(m.val + k, t);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = t[u];
+        }
+        if (two) {
+            const int4 q = __ldg(reinterpret_cast<const int4*>(m.col + k2));
+            c[4] = q.x;
+            c[5] = q.y;
+            c[6] = q.z;
+            c[7] = q.w;
+            T t[4];
+            ld4(m.val + k2, t);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[4 + u] = t[u];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int kk = (u < 4 ? k : k2) + (u & 3);
+            const bool ok = (u < 4 || two) && kk >= b && kk < e;
+            xv[u] = ok ? xa(c[u]) : T(0);
+            if (!ok) v[u] = T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) s = madd<T>(s, v[u], xv[u]);
+    }
+    return s;
+}
+
+// CSR row sum by a group of G lanes (G a power of two dividing 32); partial sums are combined
+// with a fixed butterfly over the group. Every lane of the group returns the same total. All
+// lanes of the warp must call it (the shuffles use the full mask).
 template <class T, class XA>
 __device__ __forceinline__ T csr_group_sum(const Sell<T>& m, int row, bool valid, int sub, int G, XA xa) {
-    T s = T(0);
-    if (valid) {
-        const int b = __ldg(&m.slice[row]);
-        const int e = __ldg(&m.slice[row + 1]);
-        int k = b + sub;
-        for (; k + G < e; k += 2 * G) {
-            const T v0 = __ldg(&m.val[k]), v1 = __ldg(&m.val[k + G]);
-            const int c0 = __ldg(&m.col[k]), c1 = __ldg(&m.col[k + G]);
-            const T x0 = xa(c0), x1 = xa(c1);
-            s = madd<T>(s, v0, x0);
-            s = madd<T>(s, v1, x1);
-        }
-        if (k < e) s = madd<T>(s, __ldg(&m.val[k]), xa(__ldg(&m.col[k])));
-    }
+    T s = valid ? csr_lane_sum(m, row, sub, G, xa) : T(0);
     for (int o = G >> 1; o > 0; o >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, o);
     return s;
 }
 
+// CSR row sum by G = 64..256 lanes (whole warps) of a 256-thread block holding 256 / G rows:
+// butterfly within each warp, then the row's warps are added in warp order. Returns the
+// total in the row's first lane. Every thread of the block must call it (__syncthreads).
+template <class T, class XA>
+__device__ __forceinline__ T csr_block_sum(const Sell<T>& m, int row, bool valid, int sub, int G, XA xa) {
+    __shared__ T red[kBlock / 32];
+    T s = valid ? csr_lane_sum(m, row, sub, G, xa) : T(0);
+    for (int o = 16; o > 0; o >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, o);
+    const int w = static_cast<int>(threadIdx.x) >> 5;
+    if ((threadIdx.x & 31) == 0) red[w] = s;
+    __syncthreads();
+    T t = T(0);
+    if (sub == 0) {
+        const int w0 = w;  // the row's first warp
+        for (int q = 0; q < G / 32; ++q) t = t + red[w0 + q];
+    }
+    __syncthreads();
+    return t;
+}
+
 struct TileCtx;
 
-// Rows of a fine tile (CSR operators): one group of G = fmt lanes per row, blockDim = 8 * G.
+// Rows of a fine tile (CSR operators with G <= 32): one group of G = fmt lanes per row,
+// blockDim = 8 * G. Wider groups take 256 / G rows per tile with blockDim 256.
 constexpr int kFineRows = 8;
+
 
 // Calls f(row, sum_j a_row,j xa(j)) for every row of the tile, in the operator's format.
 // SELL: one thread per row, two rows per pass; CSR: one lane group per row.
@@ -252,6 +356,11 @@ template <class T, class XA, class F>
 __device__ __forceinline__ void visit_rows(const Sell<T>& m, int r0, int r1, XA xa, F f) {
     if (m.fmt == kFmtSell) {
         int row = r0 + threadIdx.x;
+        if (m.perm != nullptr) {
+            // reordered operator: tiles are aligned windows, one position per thread
+            for (; row < r1; row += kBlock) f(__ldg(&m.perm[row]), sell_row_sum(m, row, xa));
+            return;
+        }
         for (; row + kBlock < r1; row += 2 * kBlock) {
             T s0, s1;
             sell_row_sum2(m, row, row + kBlock, xa, s0, s1);
@@ -264,8 +373,13 @@ __device__ __forceinline__ void visit_rows(const Sell<T>& m, int r0, int r1, XA 
         const int row = r0 + static_cast<int>(threadIdx.x) / G;
         const int sub = static_cast<int>(threadIdx.x) & (G - 1);
         const bool valid = row < r1;
-        const T s = csr_group_sum(m, row, valid, sub, G, xa);
-        if (valid && sub == 0) f(row, s);
+        if (G <= 32) {
+            const T s = csr_group_sum(m, row, valid, sub, G, xa);
+            if (valid && sub == 0) f(row, s);
+        } else {
+            const T s = csr_block_sum(m, row, valid, sub, G, xa);
+            if (valid && sub == 0) f(row, s);
+        }
     }
 }
 
@@ -276,7 +390,7 @@ struct TileCtx {
 
 __device__ __forceinline__ bool tile_begin(const Tiles& t, const SysState* st, TileCtx& c) {
     c.tile = blockIdx.x;
-    c.s = __ldg(&t.sys[c.tile]);
+    c.s = t.sys != nullptr ? __ldg(&t.sys[c.tile]) : 0;  // null: a single system
     c.r0 = __ldg(&t.row[c.tile]);
     c.r1 = __ldg(&t.row[c.tile + 1]);
     return st == nullptr || *((volatile const int*)&st[c.s].active) != 0;
@@ -335,6 +449,12 @@ static __global__ void k_gather_rows(int n, const int* __restrict__ map, const d
     }
 }
 
+// dst[i] = value on the caller's rows, 0 on padding rows.
+static __global__ void k_fill_rows(int n, const int* __restrict__ map, double value, double* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = map[i] >= 0 ? value : 0.0;
+}
+
 static __global__ void k_scatter_rows(int n, const int* __restrict__ map, const double* __restrict__ src,
                                       double* __restrict__ dst) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -358,6 +478,29 @@ template <class T> __device__ __forceinline__ T jac_update(T x, T wd, T b, T ax)
     }
 }
 
+// First Jacobi sweep from x = 0 (A*0 = 0): x1 = 0 + wd * b, in the arithmetic of T.
+template <class T, class B> __device__ __forceinline__ T first_sweep(T wd, B b) {
+    if constexpr (sizeof(T) == 8) return __dadd_rn(0.0, __dmul_rn(wd, static_cast<double>(b)));
+    else return wd * static_cast<T>(b);
+}
+
+// The first sweep of the next V-cycle's level-0 pre-smoothing, written by the kernels that
+// produce the Krylov residual r (so no separate sweep kernel reads r again): rows below n
+// (systems with a coarser level) get x1 = first_sweep(wd, r) in the V-cycle's precision.
+struct X1Out {
+    const float* wd32 = nullptr;
+    float* x32 = nullptr;
+    const double* wd64 = nullptr;
+    double* x64 = nullptr;
+    int n = 0;
+    __device__ __forceinline__ void put(int row, double r) const {
+        if (row < n) {
+            if (x32 != nullptr) x32[row] = first_sweep<float>(wd32[row], r);
+            if (x64 != nullptr) x64[row] = first_sweep<double>(wd64[row], r);
+        }
+    }
+};
+
 // First smoothing step from x = 0: x1 = 0 + wd * b (t = A*0 = 0), and when fused2 also the
 // second sweep y = x1 + wd (b - A x1) with x1 of the neighbours recomputed on the fly.
 template <class T, class B>
@@ -372,7 +515,7 @@ static __global__ void __launch_bounds__(kBlock) k_vc_first(Sell<T> a, Tiles til
         else return wd[j] * static_cast<T>(b[j]);
     };
     if (!fused2) {
-        for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) y[row] = x1(row);
+        for (int row = c.r0 + threadIdx.x; row < c.r1; row += blockDim.x) y[row] = x1(row);
         return;
     }
     visit_rows(a, c.r0, c.r1, x1, [&](int row, T s) {
@@ -410,10 +553,16 @@ static __global__ void __launch_bounds__(kBlock) k_vc_residual(Sell<T> a, Tiles 
 // y = M x (restriction into the next level's right-hand side)
 template <class T>
 static __global__ void __launch_bounds__(kBlock) k_vc_spmv(Sell<T> m, Tiles tiles, const SysState* st,
-                                                    const T* __restrict__ x, T* __restrict__ y) {
+                                                    const T* __restrict__ x, T* __restrict__ y,
+                                                    const T* __restrict__ wd1, T* __restrict__ x1,
+                                                    int n1) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
-    visit_rows(m, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) { y[row] = s; });
+    visit_rows(m, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
+        y[row] = s;
+        // restriction: also the first pre-smoothing sweep of the coarser level
+        if (x1 != nullptr && row < n1) x1[row] = first_sweep<T>(wd1[row], s);
+    });
 }
 
 // x += P xc
@@ -549,13 +698,14 @@ static __global__ void __launch_bounds__(kBlock) k_cg_init(Sell<double> a, Tiles
                                                     const double* __restrict__ x,
                                                     double* __restrict__ r, double* partials,
                                                     int* counters, const int* sys_tile0,
-                                                    Control ctl) {
+                                                    Control ctl, X1Out x1o) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     double rr = 0.0, unused = 0.0;
     visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, double ax) {
         const double ri = __dsub_rn(b[row], ax);
         r[row] = ri;
+        x1o.put(row, ri);
         rr = __dadd_rn(rr, __dmul_rn(ri, ri));
     });
     if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
@@ -626,7 +776,7 @@ static __global__ void __launch_bounds__(kBlock) k_cg_xr(Tiles tiles, SysState* 
                                                   const double* __restrict__ p,
                                                   const double* __restrict__ q, double* partials,
                                                   int* counters, const int* sys_tile0,
-                                                  Control ctl, int verify_true) {
+                                                  Control ctl, int verify_true, X1Out x1o) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     const double alpha = st[c.s].alpha;
@@ -635,6 +785,7 @@ static __global__ void __launch_bounds__(kBlock) k_cg_xr(Tiles tiles, SysState* 
         x[row] = __dadd_rn(x[row], __dmul_rn(alpha, p[row]));
         const double ri = __dsub_rn(r[row], __dmul_rn(alpha, q[row]));
         r[row] = ri;
+        x1o.put(row, ri);
         rr = __dadd_rn(rr, __dmul_rn(ri, ri));
     }
     if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
@@ -659,7 +810,7 @@ static __global__ void __launch_bounds__(kBlock) k_cg_true_check(Sell<double> a,
                                                           const double* __restrict__ x,
                                                           double* __restrict__ r, double* partials,
                                                           int* counters, const int* sys_tile0,
-                                                          Control ctl) {
+                                                          Control ctl, X1Out x1o) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     if (st[c.s].check == 0) return;
@@ -667,6 +818,7 @@ static __global__ void __launch_bounds__(kBlock) k_cg_true_check(Sell<double> a,
     visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, double ax) {
         const double ri = __dsub_rn(b[row], ax);
         r[row] = ri;
+        x1o.put(row, ri);
         rr = __dadd_rn(rr, __dmul_rn(ri, ri));
     });
     if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {

@@ -240,9 +240,10 @@ int cfdb_system_kernel_launches(const cfdb_system* sys, unsigned long long* coun
 /* Launch-shape / schedule knobs of the device plan (see cfd_b200/autotune.py). */
 typedef struct {
     int target_tiles; /* SELL tiles (256-thread CTAs) per level, default 1184 = 148 SMs x 8 */
-    int wide_row;     /* average row length above which CSR lane groups are used, default 24 */
-    int lanes_div;    /* lanes per CSR row ~ average row length / lanes_div, default 6 */
-    int fuse_first;   /* first two smoothing sweeps in one kernel, default 1 */
+    int wide_row;     /* average row length above which CSR lane groups are used, default 48 */
+    int lanes_div;    /* lanes per CSR row ~ average row length / lanes_div (4..256, and enough
+                         lanes for ~150K threads per operator), default 16 */
+    int fuse_first;   /* first two smoothing sweeps in one kernel, default 0 */
 } cfdb_tuning;
 void cfdb_default_tuning(cfdb_tuning* t);
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t);

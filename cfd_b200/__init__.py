@@ -120,7 +120,8 @@ _proto("cfdb_system_kernel_launches", [_vp, _P(C.c_ulonglong)])
 
 
 class TuningStruct(C.Structure):
-    _fields_ = [("target_tiles", _i), ("wide_row", _i), ("lanes_div", _i), ("fuse_first", _i)]
+    _fields_ = [("target_tiles", _i), ("wide_row", _i), ("lanes_div", _i), ("fuse_first", _i),
+                ("sell_rows", _i), ("krylov_pair", _i)]
 
 
 _proto("cfdb_default_tuning", [_P(TuningStruct)], None)
@@ -681,10 +682,12 @@ class Tuning:
     wide_row: int = 48
     lanes_div: int = 16
     fuse_first: int = 0
+    sell_rows: int = 256
+    krylov_pair: int = 1
 
     def _c(self):
         return TuningStruct(int(self.target_tiles), int(self.wide_row), int(self.lanes_div),
-                            int(self.fuse_first))
+                            int(self.fuse_first), int(self.sell_rows), int(self.krylov_pair))
 
 
 def _set_system_tuning(self, t: Tuning) -> None:

@@ -2,11 +2,13 @@
 
 The knobs are those of `Tuning` (include/cfdb.h, cfdb_tuning):
 
-* target_tiles - CTAs per level operator (tile height follows from it),
+* target_tiles - level-0 Krylov tiles (0: 256 rows each; else about this many CTAs),
 * wide_row     - average row length above which a level switches from SELL-32 rows to
                  CSR lane groups,
 * lanes_div    - lanes per CSR row = average row length / lanes_div,
-* fuse_first   - first two Jacobi sweeps of the pre-smoothing fused into one kernel.
+* fuse_first   - first two Jacobi sweeps of the pre-smoothing fused into one kernel,
+* sell_rows    - rows per CTA of SELL operators (one row per thread per pass),
+* krylov_pair  - level-0 Krylov SpMV kernels take two rows per thread per pass, or one.
 
 The search is a coordinate descent from the defaults: each knob in turn is swept over its
 candidate values with the others fixed, the best value kept, and the pass repeated until no
@@ -26,10 +28,12 @@ from typing import Callable
 from . import Tuning
 
 CANDIDATES = {
-    "target_tiles": [148 * 4, 148 * 8, 148 * 16],
+    "target_tiles": [0, 148 * 8, 148 * 16],
     "wide_row": [24, 32, 48, 64],
     "lanes_div": [8, 12, 16, 32],
     "fuse_first": [0, 1],
+    "sell_rows": [256, 512, 1024],
+    "krylov_pair": [0, 1],
 }
 
 

@@ -869,13 +869,18 @@ void cfdb_default_tuning(cfdb_tuning* t) {
     t->wide_row = d.wide_row;
     t->lanes_div = d.lanes_div;
     t->fuse_first = d.fuse_first;
+    t->sell_rows = d.sell_rows;
+    t->krylov_pair = d.krylov_pair;
 }
 
 static Tuning tuning_from(const cfdb_tuning* t) {
     if (t == nullptr) fail(CFDB_ERR_BAD_ARG, "null tuning");
-    if (t->target_tiles < 1 || t->wide_row < 0 || t->lanes_div < 1)
+    if (t->target_tiles < 0 || t->wide_row < 0 || t->lanes_div < 1)
         fail(CFDB_ERR_BAD_ARG, "tuning values out of range");
-    return Tuning{t->target_tiles, t->wide_row, t->lanes_div, t->fuse_first != 0 ? 1 : 0};
+    if (t->sell_rows < kSellRows || t->sell_rows % kSellRows != 0 || t->sell_rows > 16 * kSellRows)
+        fail(CFDB_ERR_BAD_ARG, "tuning: sell_rows must be a multiple of 256 in 256..4096");
+    return Tuning{t->target_tiles, t->wide_row, t->lanes_div, t->fuse_first != 0 ? 1 : 0, t->sell_rows,
+                  t->krylov_pair != 0 ? 1 : 0};
 }
 
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t) {

@@ -217,11 +217,14 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
     off0_.resize(n_sys_);
     for (int s = 0; s < n_sys_; ++s) off0_[s] = off[0][s];
     cudaStream_t st = stream_;
-    // tiles
+    // Krylov tiles of level 0 (the reductions): kSellRows rows, or a fixed tile count when
+    // target_tiles > 0; coarser levels use their operators' own tiles
     std::vector<int> sys_tile0(n_sys_ + 1, 0);
-    for (int l = 0; l < n_levels_; ++l) {
+    for (int l = 0; l < 1; ++l) {
         DevLevel& d = lv_[l];
-        const int base = std::max(256, round_up(ceil_div(std::max(d.n_rows, 1), std::max(tuning_.target_tiles, 1)), 256));
+        const int base = tuning_.target_tiles > 0
+                             ? std::max(kSellRows, round_up(ceil_div(std::max(d.n_rows, 1), tuning_.target_tiles), kSellRows))
+                             : kSellRows;
         std::vector<int> trow, tsys;
         int nc_tiles = -1;
         for (int k = 0; k < n_sys_; ++k) {
@@ -245,7 +248,8 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
     // Launch tiles of one operator over the rows of `row_level` of the systems `include`
     // selects (a prefix in batch order); `nc` marks the systems that continue past that level.
     auto op_tiles = [&](DevSell64_32& m, int fmt, int row_level, auto include, auto nc) {
-        const int rpt = fmt == kFmtSell ? kSellRows : (fmt <= 32 ? kFineRows : kBlock / fmt);
+        const int rpt = fmt == kFmtSell ? std::max(kSellRows, tuning_.sell_rows / kSellRows * kSellRows)
+                                        : (fmt <= 32 ? kFineRows : kBlock / fmt);
         m.block = fmt == kFmtSell ? kBlock : (fmt <= 32 ? kFineRows * fmt : kBlock);
         std::vector<int> trow, tsys;
         int n_nc = -1, end = 0;
@@ -435,10 +439,18 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         vs_ = arena_.alloc<double>(std::max(vs_total_, 1));
         st_ = arena_.alloc<SysState>(n_sys_);
         CFDB_CUDA(cudaMemsetAsync(st_, 0, sizeof(SysState) * n_sys_, st));
-        partials_ = arena_.alloc<double>(2 * static_cast<size_t>(lv_[0].n_tiles));
-        counters_ = arena_.alloc<int>(n_sys_);
-        CFDB_CUDA(cudaMemsetAsync(counters_, 0, sizeof(int) * n_sys_, st));
-        sys_tile0_ = arena_.upload(sys_tile0, st);
+        // two-level reduction: groups of kGroupTiles tiles within each system
+        std::vector<int> grp0(n_sys_ + 1, 0);
+        for (int k = 0; k < n_sys_; ++k) grp0[k + 1] = grp0[k] + ceil_div(sys_tile0[k + 1] - sys_tile0[k], kGroupTiles);
+        const int n_groups = std::max(grp0[n_sys_], 1);
+        red_.partials = arena_.alloc<double>(2 * static_cast<size_t>(std::max(lv_[0].n_tiles, 1)));
+        red_.gpartials = arena_.alloc<double>(2 * static_cast<size_t>(n_groups));
+        int* cnt = arena_.alloc<int>(n_sys_ + n_groups);
+        CFDB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (n_sys_ + n_groups), st));
+        red_.counters = cnt;
+        red_.gcounters = cnt + n_sys_;
+        red_.sys_tile0 = arena_.upload(sys_tile0, st);
+        red_.grp0 = arena_.upload(grp0, st);
         n_active_ = arena_.alloc<int>(1);
         error_ = arena_.alloc<int>(1);
         CFDB_CUDA(cudaMemsetAsync(error_, 0, sizeof(int), st));
@@ -651,6 +663,14 @@ template <> float* vx<float>(double*, float* b) { return b; }
 template <class T> Sell<T> vs_sel(const Sell<double>& a, const Sell<float>& b);
 template <> Sell<double> vs_sel<double>(const Sell<double>& a, const Sell<float>&) { return a; }
 template <> Sell<float> vs_sel<float>(const Sell<double>&, const Sell<float>& b) { return b; }
+
+// Calls fn with the visiting strategy v as a compile-time constant.
+template <class Fn> void with_visit(int v, Fn&& fn) {
+    if (v == kVisitSell2) fn(std::integral_constant<int, kVisitSell2>{});
+    else if (v == kVisitSell1) fn(std::integral_constant<int, kVisitSell1>{});
+    else if (v == kVisitWarp) fn(std::integral_constant<int, kVisitWarp>{});
+    else fn(std::integral_constant<int, kVisitBlock>{});
+}
 } // namespace
 
 // Buffer holding the first pre-smoothing iterate of level l, chosen so that after the
@@ -711,16 +731,16 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
         Tiles first;
         int second; // grid
         int block;
+        int visit;  // row-visiting strategy of the operator's kernels
     };
     auto TL = [&](int, const DevSell64_32& m, bool nc) -> Launch {
-        return {m.tiles, nc ? m.n_tiles_nc : m.n_tiles, m.block};
+        return {m.tiles, nc ? m.n_tiles_nc : m.n_tiles, m.block, visit_of(m.s64.val != nullptr ? m.s64.fmt : m.s32.fmt)};
     };
     std::vector<T*> cur(L, nullptr);
     // ---- down ----
     for (int l = 0; l + 1 < L; ++l) {
         const DevLevel& d = lv_[l];
-        const int g = d.n_tiles_nc;
-        if (g == 0) continue;
+        if (d.a.n_tiles_nc == 0) continue;  // no system continues past this level
         const double n = d.n_rows_nc;
         const double sb = l == 0 ? sb0 : sv;
         T* x = X(l);
@@ -736,8 +756,8 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
             T* c = start;
             for (int k = 1; k < sweeps_; ++k) {
                 T* o = c == x ? y : x;
-                if (l == 0) k_vc_jacobi<T, double><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, c, o);
-                else k_vc_jacobi<T, T><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), c, o);
+                if (l == 0) with_visit(ta.visit, [&](auto V) { k_vc_jacobi<T, double, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, c, o); });
+                else with_visit(ta.visit, [&](auto V) { k_vc_jacobi<T, T, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), c, o); });
                 mark("smooth", l, spmv_b(d.a, n, n) + sv * n + sb * n);
                 c = o;
             }
@@ -745,32 +765,33 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
         } else {
             const auto ta = TL(l, d.a, true);
             if (l == 0) {
-                k_vc_first<T, double><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, start, fuse);
+                with_visit(ta.visit, [&](auto V) { k_vc_first<T, double, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, start, fuse); });
             } else {
-                k_vc_first<T, T><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), start, fuse);
+                with_visit(ta.visit, [&](auto V) { k_vc_first<T, T, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), start, fuse); });
             }
             mark("smooth_first", l, fuse ? spmv_b(d.a, n, n) - sv * n + sv * n + sb * n : 2.0 * sv * n + sb * n);
             T* c = start;
             for (int k = fuse ? 2 : 1; k < sweeps_; ++k) {
                 T* o = c == x ? y : x;
-                if (l == 0) k_vc_jacobi<T, double><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, c, o);
-                else k_vc_jacobi<T, T><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), c, o);
+                if (l == 0) with_visit(ta.visit, [&](auto V) { k_vc_jacobi<T, double, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, c, o); });
+                else with_visit(ta.visit, [&](auto V) { k_vc_jacobi<T, T, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), c, o); });
                 mark("smooth", l, spmv_b(d.a, n, n) + sv * n + sb * n);
                 c = o;
             }
             cur[l] = c;
         }
         const auto tr = TL(l, d.a, true);
-        if (l == 0) k_vc_residual<T, double><<<tr.second, tr.block, 0, s>>>(A(l), tr.first, stv, r_, cur[l], Tv(l));
-        else k_vc_residual<T, T><<<tr.second, tr.block, 0, s>>>(A(l), tr.first, stv, Bv(l), cur[l], Tv(l));
+        if (l == 0) with_visit(tr.visit, [&](auto V) { k_vc_residual<T, double, decltype(V)::value><<<tr.second, tr.block, 0, s>>>(A(l), tr.first, stv, r_, cur[l], Tv(l)); });
+        else with_visit(tr.visit, [&](auto V) { k_vc_residual<T, T, decltype(V)::value><<<tr.second, tr.block, 0, s>>>(A(l), tr.first, stv, Bv(l), cur[l], Tv(l)); });
         mark("residual", l, spmv_b(d.a, n, n) + sb * n);
         const DevLevel& nx = lv_[l + 1];
         const auto tq = TL(l + 1, d.r, false);
         const bool next_x1 = x1_by_restrict && l + 2 < L && nx.n_rows_nc > 0;
-        k_vc_spmv<T><<<tq.second, tq.block, 0, s>>>(R(l), tq.first, stv, Tv(l), Bv(l + 1),
-                                                    next_x1 ? WD(l + 1) : nullptr,
-                                                    next_x1 ? start_buffer<T>(l + 1) : nullptr,
-                                                    next_x1 ? nx.n_rows_nc : 0);
+        with_visit(tq.visit, [&](auto V) {
+            k_vc_spmv<T, decltype(V)::value><<<tq.second, tq.block, 0, s>>>(
+                R(l), tq.first, stv, Tv(l), Bv(l + 1), next_x1 ? WD(l + 1) : nullptr,
+                next_x1 ? start_buffer<T>(l + 1) : nullptr, next_x1 ? nx.n_rows_nc : 0);
+        });
         mark("restrict", l, spmv_b(d.r, nx.n_rows, n) + (next_x1 ? 2.0 * sv * nx.n_rows_nc : 0.0));
     }
     // ---- coarsest blocks (dense inverse of each multi-level system's coarsest operator) ----
@@ -789,30 +810,32 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
     // ---- up ----
     for (int l = L - 2; l >= 0; --l) {
         const DevLevel& d = lv_[l];
-        const int g = d.n_tiles_nc;
-        if (g == 0) continue;
+        if (d.a.n_tiles_nc == 0) continue;  // no system continues past this level
         const double n = d.n_rows_nc;
         const double sb = l == 0 ? sb0 : sv;
         T* x = X(l);
         T* y = Y(l);
         T* c = cur[l];
         const auto tp = TL(l, d.p, true);
-        k_vc_prolong<T><<<tp.second, tp.block, 0, s>>>(P(l), tp.first, stv, X(l + 1), c);
+        with_visit(tp.visit, [&](auto V) {
+            k_vc_prolong<T, decltype(V)::value><<<tp.second, tp.block, 0, s>>>(P(l), tp.first, stv, X(l + 1), c);
+        });
         const auto ta = TL(l, d.a, true);
         mark("prolong", l, spmv_b(d.p, n, lv_[l + 1].n_rows) + sv * n);
         for (int k = 0; k < sweeps_; ++k) {
             T* o = c == x ? y : x;
             const bool last = k + 1 == sweeps_;
             if (l == 0 && last && fused_final) {
-                k_vc_jacobi_final<T><<<g, kBlock, 0, s>>>(A(0), d.tiles, st_, WD(0), r_, c, o, q_, partials_,
-                                                          counters_, sys_tile0_, Control{n_active_, error_},
-                                                          flexible);
+                with_visit(krylov_visit(), [&](auto V) {
+                    k_vc_jacobi_final<T, decltype(V)::value><<<d.n_tiles_nc, kBlock, 0, s>>>(
+                        A(0), d.tiles, st_, WD(0), r_, c, o, q_, red_, Control{n_active_, error_}, flexible);
+                });
                 mark("smooth_dot", l, spmv_b(d.a, n, n) + sv * n + sb * n + (flexible ? 8.0 * n : 0.0));
             } else if (l == 0) {
-                k_vc_jacobi<T, double><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, c, o);
+                with_visit(ta.visit, [&](auto V) { k_vc_jacobi<T, double, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, c, o); });
                 mark("smooth", l, spmv_b(d.a, n, n) + sv * n + sb * n);
             } else {
-                k_vc_jacobi<T, T><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), c, o);
+                with_visit(ta.visit, [&](auto V) { k_vc_jacobi<T, T, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), c, o); });
                 mark("smooth", l, spmv_b(d.a, n, n) + sv * n + sb * n);
             }
             c = o;
@@ -833,13 +856,13 @@ void Engine::enqueue_init(Mode mode) {
     const double a0 = static_cast<double>(d.a.nnz) * 12.0 + 4.0 * (n + 1.0) + 16.0 * n;
     const X1Out x1o = x1_out(mode);
     const double x1b = (mode == Mode::AmgMixed ? 8.0 : 16.0) * x1o.n;
-    k_cg_init<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, r_, partials_, counters_,
-                                                  sys_tile0_, ctl, x1o);
+    with_visit(krylov_visit(), [&](auto V) {
+        k_cg_init<decltype(V)::value><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, r_, red_, ctl, x1o);
+    });
     mark("cg_init", 0, a0 + 16.0 * n + x1b);
     const int flexible = mode == Mode::AmgMixed ? 1 : 0;
     if (mode == Mode::Jacobi) {
-        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, nullptr, q_, partials_,
-                                                           counters_, sys_tile0_, ctl, 0);
+        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, nullptr, q_, red_, ctl, 0);
         mark("cg_rz", 0, 24.0 * n);
         return;
     }
@@ -852,12 +875,10 @@ void Engine::enqueue_rz(Mode mode, int flexible) {
     const Control ctl{n_active_, error_};
     const double n = d.n_rows;
     if (mode == Mode::AmgMixed) {
-        k_cg_rz<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x32, nullptr, dinv0_, q_, partials_,
-                                                          counters_, sys_tile0_, ctl, flexible);
+        k_cg_rz<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x32, nullptr, dinv0_, q_, red_, ctl, flexible);
         mark("cg_rz", 0, 12.0 * n + (flexible ? 8.0 * n : 0.0));
     } else {
-        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, nullptr, dinv0_, q_, partials_,
-                                                           counters_, sys_tile0_, ctl, flexible);
+        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, nullptr, dinv0_, q_, red_, ctl, flexible);
         mark("cg_rz", 0, 16.0 * n + (flexible ? 8.0 * n : 0.0));
     }
 }
@@ -874,23 +895,25 @@ void Engine::enqueue_iteration(Mode mode) {
         k_cg_pupdate<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, d.x64, r_, dinv0_, p_);
         mark("cg_p_update", 0, 24.0 * n);
     }
-    k_cg_spmv_pq<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, p_, q_, partials_, counters_,
-                                                     sys_tile0_, ctl);
+    with_visit(krylov_visit(), [&](auto V) {
+        k_cg_spmv_pq<decltype(V)::value><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, p_, q_, red_, ctl);
+    });
     mark("cg_spmv_pq", 0, a0);
     const X1Out x1o = x1_out(mode);
     const double x1b = (mode == Mode::AmgMixed ? 8.0 : 16.0) * x1o.n;
-    k_cg_xr<<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, x_, r_, p_, q_, partials_, counters_, sys_tile0_,
+    k_cg_xr<<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, x_, r_, p_, q_, red_,
                                                 ctl, mode == Mode::AmgMixed ? 1 : 0, x1o);
     mark("cg_xr", 0, 48.0 * n + x1b);
     if (mode == Mode::AmgMixed) {
-        k_cg_true_check<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, r_, partials_,
-                                                            counters_, sys_tile0_, ctl, x1o);
+        with_visit(krylov_visit(), [&](auto V) {
+            k_cg_true_check<decltype(V)::value><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, r_,
+                                                                               red_, ctl, x1o);
+        });
         mark("cg_true_check", 0, 0.0);
     }
     const int flexible = mode == Mode::AmgMixed ? 1 : 0;
     if (mode == Mode::Jacobi) {
-        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, nullptr, q_, partials_,
-                                                           counters_, sys_tile0_, ctl, 0);
+        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, nullptr, q_, red_, ctl, 0);
         mark("cg_rz", 0, 24.0 * n);
         return;
     }
@@ -1063,8 +1086,9 @@ std::vector<SolveResult> Engine::solve(Mode mode, const std::vector<SolveRequest
     }
     // true residual for reporting
     const DevLevel& d = lv_[0];
-    k_true_residual<<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, partials_, counters_,
-                                                        sys_tile0_);
+    with_visit(krylov_visit(), [&](auto V) {
+        k_true_residual<decltype(V)::value><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, red_);
+    });
     ++launches_;
     CFDB_CUDA(cudaGetLastError());
     CFDB_CUDA(cudaMemcpyAsync(hs.data(), st_, sizeof(SysState) * n_sys_, cudaMemcpyDeviceToHost, stream_));
@@ -1106,10 +1130,10 @@ double Engine::time_level0_sweep(bool fp32, int reps) {
     CFDB_CUDA(cudaEventRecord(a, stream_));
     for (int i = 0; i < reps; ++i) {
         if (fp32) {
-            k_vc_jacobi<float, double><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s32, d.tiles, nullptr, d.wd32, r_,
+            k_vc_jacobi<float, double, kVisitSell2><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s32, d.tiles, nullptr, d.wd32, r_,
                                                                          d.x32, d.y32);
         } else {
-            k_vc_jacobi<double, double><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, nullptr, d.wd64, r_,
+            k_vc_jacobi<double, double, kVisitSell2><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, nullptr, d.wd64, r_,
                                                                           d.x64, d.y64);
         }
     }

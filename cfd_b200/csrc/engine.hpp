@@ -28,11 +28,13 @@ struct SystemSpec {
 // Launch-shape and schedule knobs (no effect on the arithmetic of a row sum except that wide
 // operators switch between the ordered SELL sum and the lane-group CSR sum).
 struct Tuning {
-    int target_tiles = 148 * 8; // SELL tiles (CTAs of 256 threads) per level
+    int target_tiles = 148 * 8; // level-0 Krylov tiles: about this many (0: 256 rows each)
     int wide_row = 48;          // average row length above which CSR lane groups are used
     int lanes_div = 16;         // lanes per CSR row ~ average row length / lanes_div (4..256),
                                 // and at least enough lanes to give ~150K threads per operator
     int fuse_first = 0;         // first two smoothing sweeps in one kernel (x1 recomputed)
+    int sell_rows = kSellRows;  // rows per CTA of SELL operators (multiple of kSellRows)
+    int krylov_pair = 1;        // level-0 Krylov SpMV kernels: two rows per thread per pass
 };
 
 struct SolveRequest {
@@ -158,6 +160,8 @@ private:
     void enqueue_vcycle(Mode mode, bool fused_final, int flexible, bool x1_ready0);
     template <class T> void enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0);
     template <class T> T* start_buffer(int l) const;
+    // rows per thread per pass of the level-0 Krylov SpMV kernels (two, or one)
+    int krylov_visit() const { return tuning_.krylov_pair ? kVisitSell2 : kVisitSell1; }
     // where the residual producers of `mode` write the level-0 first sweep (n = 0: nowhere)
     X1Out x1_out(Mode mode) const;
     void enqueue_init(Mode mode);
@@ -200,9 +204,7 @@ private:
     double *b_ = nullptr, *x_ = nullptr, *r_ = nullptr, *p_ = nullptr, *q_ = nullptr;
     // state
     SysState* st_ = nullptr;
-    double* partials_ = nullptr;
-    int* counters_ = nullptr;
-    int* sys_tile0_ = nullptr;
+    Reduce red_{};
     int* n_active_ = nullptr;
     int* error_ = nullptr;
     int* h_pinned_ = nullptr; // [0] n_active, [1] error

@@ -111,32 +111,66 @@ __device__ __forceinline__ void block_sum2(double& a, double& b) {
     __syncthreads();
 }
 
+// Per-tile partial sums and their tickets, reduced in two fixed-order levels: the last CTA of
+// each group of kGroupTiles consecutive tiles of a system sums the group's partials, and the
+// last group of the system sums the group totals. Deterministic, and no CTA sums more than
+// kGroupTiles or (tiles / kGroupTiles) values.
+constexpr int kGroupTiles = 64;
+struct Reduce {
+    double* partials;        // 2 per tile
+    double* gpartials;       // 2 per group
+    int* counters;           // per system: groups finished
+    int* gcounters;          // per group: tiles finished
+    const int* sys_tile0;    // n_systems + 1: first tile of each system
+    const int* grp0;         // n_systems + 1: first group of each system
+};
+
+// Sum of the pairs src[first..last) in index order by the block; valid in thread 0.
+__device__ __forceinline__ void sum_pairs(const double* src, int first, int last, double& a, double& b) {
+    a = 0.0;
+    b = 0.0;
+    for (int t = first + threadIdx.x; t < last; t += blockDim.x) {
+        a += __ldcg(&src[2 * t]);
+        b += __ldcg(&src[2 * t + 1]);
+    }
+    block_sum2(a, b);
+}
+
 // Writes this tile's partials; returns true in every thread of the system's last CTA, whose
 // thread 0 then holds the system totals in (a, b).
-__device__ __forceinline__ bool reduce_system(double& a, double& b, int tile, int s,
-                                              double* partials, int* counters,
-                                              const int* sys_tile0) {
+__device__ __forceinline__ bool reduce_system(double& a, double& b, int tile, int s, const Reduce& r) {
     __shared__ int last;
     block_sum2(a, b);
+    const int t0 = r.sys_tile0[s], t1 = r.sys_tile0[s + 1];
+    const int g = (tile - t0) / kGroupTiles;
+    const int gi = r.grp0[s] + g;
+    const int gf = t0 + g * kGroupTiles;
+    const int gl = min(t1, gf + kGroupTiles);
     if (threadIdx.x == 0) {
-        partials[2 * tile] = a;
-        partials[2 * tile + 1] = b;
+        r.partials[2 * tile] = a;
+        r.partials[2 * tile + 1] = b;
         __threadfence();
-        const int n_tiles = sys_tile0[s + 1] - sys_tile0[s];
-        const int ticket = atomicAdd(&counters[s], 1);
-        last = ticket == n_tiles - 1;
-        if (last) counters[s] = 0;
+        const int ticket = atomicAdd(&r.gcounters[gi], 1);
+        last = ticket == gl - gf - 1;
+        if (last) r.gcounters[gi] = 0;
     }
     __syncthreads();
     if (!last) return false;
     __threadfence();
-    a = 0.0;
-    b = 0.0;
-    for (int t = sys_tile0[s] + threadIdx.x; t < sys_tile0[s + 1]; t += kBlock) {
-        a += __ldcg(&partials[2 * t]);
-        b += __ldcg(&partials[2 * t + 1]);
+    sum_pairs(r.partials, gf, gl, a, b);
+    if (threadIdx.x == 0) {
+        r.gpartials[2 * gi] = a;
+        r.gpartials[2 * gi + 1] = b;
+        __threadfence();
+        const int n_groups = r.grp0[s + 1] - r.grp0[s];
+        const int ticket = atomicAdd(&r.counters[s], 1);
+        last = ticket == n_groups - 1;
+        if (last) r.counters[s] = 0;
     }
-    block_sum2(a, b);
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    sum_pairs(r.gpartials, r.grp0[s], r.grp0[s + 1], a, b);
     return true;
 }
 
@@ -199,47 +233,59 @@ __device__ __forceinline__ T sell_row_sum(const Sell<T>& m, int row, XA xa) {
     return s;
 }
 
-// Two SELL rows of one thread with their loads interleaved (twice the loads in flight); each
-// row is still accumulated in its own CSR order.
+// Predicated batch of four SELL entries starting at k (column -1 beyond the row end e).
+template <class T>
+__device__ __forceinline__ void sell_load4(const Sell<T>& m, int k, int e, T (&v)[4], int (&c)[4]) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const bool ok = k + 32 * u < e;
+        v[u] = ok ? __ldg(&m.val[k + 32 * u]) : T(0);
+        c[u] = ok ? __ldg(&m.col[k + 32 * u]) : -1;
+    }
+}
+
+template <class T, class XA>
+__device__ __forceinline__ void sell_acc4(T& s, const T (&v)[4], const int (&c)[4], XA xa) {
+    T xv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) xv[u] = c[u] >= 0 ? xa(c[u]) : T(0);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        if (c[u] >= 0) s = madd<T>(s, v[u], xv[u]);
+}
+
+// Two SELL rows of one thread, both software-pipelined as in sell_row_sum (up to four batches
+// in flight per thread); each row is still accumulated in its own CSR order.
 template <class T, class XA>
 __device__ __forceinline__ void sell_row_sum2(const Sell<T>& m, int ra, int rb, XA xa, T& sa, T& sb) {
-    const int la = ra & 31, lb = rb & 31;
-    int ka = __ldg(&m.slice[ra >> 5]) + la;
+    int ka = __ldg(&m.slice[ra >> 5]) + (ra & 31);
     const int ea = __ldg(&m.slice[(ra >> 5) + 1]);
-    int kb = __ldg(&m.slice[rb >> 5]) + lb;
+    int kb = __ldg(&m.slice[rb >> 5]) + (rb & 31);
     const int eb = __ldg(&m.slice[(rb >> 5) + 1]);
     sa = T(0);
     sb = T(0);
-    for (; ka + 96 < ea && kb + 96 < eb; ka += 128, kb += 128) {
-        T va[4], vb[4], xa4[4], xb4[4];
-        int ca[4], cb[4];
+    T va[4], vb[4];
+    int ca[4], cb[4];
+    sell_load4(m, ka, ea, va, ca);
+    sell_load4(m, kb, eb, vb, cb);
+    for (;;) {
+        ka += 128;
+        kb += 128;
+        T van[4], vbn[4];
+        int can[4], cbn[4];
+        sell_load4(m, ka, ea, van, can);
+        sell_load4(m, kb, eb, vbn, cbn);
+        sell_acc4(sa, va, ca, xa);
+        sell_acc4(sb, vb, cb, xa);
+        if (ka >= ea && kb >= eb) break;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            va[u] = __ldg(&m.val[ka + 32 * u]);
-            ca[u] = __ldg(&m.col[ka + 32 * u]);
-            vb[u] = __ldg(&m.val[kb + 32 * u]);
-            cb[u] = __ldg(&m.col[kb + 32 * u]);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            xa4[u] = xa(ca[u]);
-            xb4[u] = xa(cb[u]);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            sa = madd<T>(sa, va[u], xa4[u]);
-            sb = madd<T>(sb, vb[u], xb4[u]);
+            va[u] = van[u];
+            ca[u] = can[u];
+            vb[u] = vbn[u];
+            cb[u] = cbn[u];
         }
     }
-    for (; ka < ea && kb < eb; ka += 32, kb += 32) {
-        const T v0 = __ldg(&m.val[ka]), v1 = __ldg(&m.val[kb]);
-        const int c0 = __ldg(&m.col[ka]), c1 = __ldg(&m.col[kb]);
-        const T x0 = xa(c0), x1 = xa(c1);
-        sa = madd<T>(sa, v0, x0);
-        sb = madd<T>(sb, v1, x1);
-    }
-    for (; ka < ea; ka += 32) sa = madd<T>(sa, __ldg(&m.val[ka]), xa(__ldg(&m.col[ka])));
-    for (; kb < eb; kb += 32) sb = madd<T>(sb, __ldg(&m.val[kb]), xa(__ldg(&m.col[kb])));
 }
 
 template <class T, class X>
@@ -350,17 +396,19 @@ struct TileCtx;
 constexpr int kFineRows = 8;
 
 
-// Calls f(row, sum_j a_row,j xa(j)) for every row of the tile, in the operator's format.
-// SELL: one thread per row, two rows per pass; CSR: one lane group per row.
-template <class T, class XA, class F>
-__device__ __forceinline__ void visit_rows(const Sell<T>& m, int r0, int r1, XA xa, F f) {
-    if (m.fmt == kFmtSell) {
+// Row-visiting strategies of the tiled kernels, fixed at compile time so that each kernel
+// instance holds the registers of one strategy only:
+//  kVisitSell2  SELL, two rows per thread per pass (big tiles of the Krylov kernels);
+//  kVisitSell1  SELL, one row per thread per pass, rows optionally reordered (V-cycle kernels);
+//  kVisitWarp   CSR, G <= 32 lanes per row (8 rows per tile);
+//  kVisitBlock  CSR, G = 64..256 lanes per row (256 / G rows per tile).
+enum : int { kVisitSell2 = 0, kVisitSell1 = 1, kVisitWarp = 2, kVisitBlock = 3 };
+
+// Calls f(row, sum_j a_row,j xa(j)) for every row of the tile.
+template <int V, class T, class XA, class F>
+__device__ __forceinline__ void visit_rows_v(const Sell<T>& m, int r0, int r1, XA xa, F f) {
+    if constexpr (V == kVisitSell2) {
         int row = r0 + threadIdx.x;
-        if (m.perm != nullptr) {
-            // reordered operator: tiles are aligned windows, one position per thread
-            for (; row < r1; row += kBlock) f(__ldg(&m.perm[row]), sell_row_sum(m, row, xa));
-            return;
-        }
         for (; row + kBlock < r1; row += 2 * kBlock) {
             T s0, s1;
             sell_row_sum2(m, row, row + kBlock, xa, s0, s1);
@@ -368,12 +416,16 @@ __device__ __forceinline__ void visit_rows(const Sell<T>& m, int r0, int r1, XA 
             f(row + kBlock, s1);
         }
         if (row < r1) f(row, sell_row_sum(m, row, xa));
+    } else if constexpr (V == kVisitSell1) {
+        // reordered operators: tiles are aligned windows of positions
+        for (int row = r0 + threadIdx.x; row < r1; row += kBlock)
+            f(m.perm != nullptr ? __ldg(&m.perm[row]) : row, sell_row_sum(m, row, xa));
     } else {
         const int G = m.fmt;
         const int row = r0 + static_cast<int>(threadIdx.x) / G;
         const int sub = static_cast<int>(threadIdx.x) & (G - 1);
         const bool valid = row < r1;
-        if (G <= 32) {
+        if constexpr (V == kVisitWarp) {
             const T s = csr_group_sum(m, row, valid, sub, G, xa);
             if (valid && sub == 0) f(row, s);
         } else {
@@ -381,6 +433,11 @@ __device__ __forceinline__ void visit_rows(const Sell<T>& m, int r0, int r1, XA 
             if (valid && sub == 0) f(row, s);
         }
     }
+}
+
+// Strategy of an operator's V-cycle kernels.
+__host__ __device__ inline int visit_of(int fmt) {
+    return fmt == kFmtSell ? kVisitSell1 : (fmt <= 32 ? kVisitWarp : kVisitBlock);
 }
 
 // Tile bookkeeping shared by all tiled kernels.
@@ -503,7 +560,7 @@ struct X1Out {
 
 // First smoothing step from x = 0: x1 = 0 + wd * b (t = A*0 = 0), and when fused2 also the
 // second sweep y = x1 + wd (b - A x1) with x1 of the neighbours recomputed on the fly.
-template <class T, class B>
+template <class T, class B, int V>
 static __global__ void __launch_bounds__(kBlock) k_vc_first(Sell<T> a, Tiles tiles, const SysState* st,
                                                      const T* __restrict__ wd,
                                                      const B* __restrict__ b, T* __restrict__ y,
@@ -518,47 +575,47 @@ static __global__ void __launch_bounds__(kBlock) k_vc_first(Sell<T> a, Tiles til
         for (int row = c.r0 + threadIdx.x; row < c.r1; row += blockDim.x) y[row] = x1(row);
         return;
     }
-    visit_rows(a, c.r0, c.r1, x1, [&](int row, T s) {
+    visit_rows_v<V>(a, c.r0, c.r1, x1, [&](int row, T s) {
         y[row] = jac_update<T>(x1(row), wd[row], static_cast<T>(b[row]), s);
     });
 }
 
 // y = x + wd (b - A x)
-template <class T, class B>
+template <class T, class B, int V>
 static __global__ void __launch_bounds__(kBlock) k_vc_jacobi(Sell<T> a, Tiles tiles, const SysState* st,
                                                       const T* __restrict__ wd,
                                                       const B* __restrict__ b,
                                                       const T* __restrict__ x, T* __restrict__ y) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
-    visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
+    visit_rows_v<V>(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
         y[row] = jac_update<T>(x[row], wd[row], static_cast<T>(b[row]), s);
     });
 }
 
 // t = b - A x
-template <class T, class B>
+template <class T, class B, int V>
 static __global__ void __launch_bounds__(kBlock) k_vc_residual(Sell<T> a, Tiles tiles, const SysState* st,
                                                         const B* __restrict__ b,
                                                         const T* __restrict__ x,
                                                         T* __restrict__ t) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
-    visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
+    visit_rows_v<V>(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
         if constexpr (sizeof(T) == 8) t[row] = __dsub_rn(static_cast<T>(b[row]), s);
         else t[row] = static_cast<T>(b[row]) - s;
     });
 }
 
 // y = M x (restriction into the next level's right-hand side)
-template <class T>
+template <class T, int V>
 static __global__ void __launch_bounds__(kBlock) k_vc_spmv(Sell<T> m, Tiles tiles, const SysState* st,
                                                     const T* __restrict__ x, T* __restrict__ y,
                                                     const T* __restrict__ wd1, T* __restrict__ x1,
                                                     int n1) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
-    visit_rows(m, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
+    visit_rows_v<V>(m, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
         y[row] = s;
         // restriction: also the first pre-smoothing sweep of the coarser level
         if (x1 != nullptr && row < n1) x1[row] = first_sweep<T>(wd1[row], s);
@@ -566,13 +623,13 @@ static __global__ void __launch_bounds__(kBlock) k_vc_spmv(Sell<T> m, Tiles tile
 }
 
 // x += P xc
-template <class T>
+template <class T, int V>
 static __global__ void __launch_bounds__(kBlock) k_vc_prolong(Sell<T> p, Tiles tiles, const SysState* st,
                                                        const T* __restrict__ xc,
                                                        T* __restrict__ x) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
-    visit_rows(p, c.r0, c.r1, [xc](int j) { return xc[j]; }, [&](int row, T s) {
+    visit_rows_v<V>(p, c.r0, c.r1, [xc](int j) { return xc[j]; }, [&](int row, T s) {
         if constexpr (sizeof(T) == 8) x[row] = __dadd_rn(x[row], s);
         else x[row] = x[row] + s;
     });
@@ -693,22 +750,22 @@ static __global__ void __launch_bounds__(kBlock) k_vc_coarse(CoarseBlocks cb, co
 // ---------------------------------------------------------------------------------------------
 
 // r = b - A x ; |r|_2 ; stop if already converged (iterations = 0)
+template <int V>
 static __global__ void __launch_bounds__(kBlock) k_cg_init(Sell<double> a, Tiles tiles, SysState* st,
                                                     const double* __restrict__ b,
                                                     const double* __restrict__ x,
-                                                    double* __restrict__ r, double* partials,
-                                                    int* counters, const int* sys_tile0,
+                                                    double* __restrict__ r, Reduce red,
                                                     Control ctl, X1Out x1o) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     double rr = 0.0, unused = 0.0;
-    visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, double ax) {
+    visit_rows_v<V>(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, double ax) {
         const double ri = __dsub_rn(b[row], ax);
         r[row] = ri;
         x1o.put(row, ri);
         rr = __dadd_rn(rr, __dmul_rn(ri, ri));
     });
-    if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+    if (reduce_system(rr, unused, c.tile, c.s, red) && threadIdx.x == 0) {
         SysState& s = st[c.s];
         s.res = sqrt(rr);
         s.phase = 0;
@@ -736,26 +793,38 @@ static __global__ void __launch_bounds__(kBlock) k_cg_pupdate(Tiles tiles, const
     const bool first = st[c.s].first != 0;
     const bool jsys = st[c.s].jacobi != 0;
     const double beta = st[c.s].beta;
-    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
-        const double zi = jsys ? __dmul_rn(r[row], jac0[row]) : static_cast<double>(z[row]);
-        p[row] = first ? zi : __dadd_rn(zi, __dmul_rn(beta, p[row]));
+    // four rows per thread per pass: all loads of the pass are issued before any store
+    for (int r0 = c.r0 + threadIdx.x; r0 < c.r1; r0 += 4 * kBlock) {
+        double zi[4], pi[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = r0 + u * kBlock;
+            const bool ok = row < c.r1;
+            zi[u] = !ok ? 0.0 : (jsys ? __dmul_rn(r[row], jac0[row]) : static_cast<double>(z[row]));
+            pi[u] = ok && !first ? p[row] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = r0 + u * kBlock;
+            if (row < c.r1) p[row] = first ? zi[u] : __dadd_rn(zi[u], __dmul_rn(beta, pi[u]));
+        }
     }
 }
 
 // q = A p ; p.q ; alpha = rz / pq (break if pq == 0)
+template <int V>
 static __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(Sell<double> a, Tiles tiles, SysState* st,
                                                        const double* __restrict__ p,
-                                                       double* __restrict__ q, double* partials,
-                                                       int* counters, const int* sys_tile0,
+                                                       double* __restrict__ q, Reduce red,
                                                        Control ctl) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     double pq = 0.0, unused = 0.0;
-    visit_rows(a, c.r0, c.r1, [p](int j) { return p[j]; }, [&](int row, double qi) {
+    visit_rows_v<V>(a, c.r0, c.r1, [p](int j) { return p[j]; }, [&](int row, double qi) {
         q[row] = qi;
         pq = __dadd_rn(pq, __dmul_rn(p[row], qi));
     });
-    if (reduce_system(pq, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+    if (reduce_system(pq, unused, c.tile, c.s, red) && threadIdx.x == 0) {
         SysState& s = st[c.s];
         s.first = 0;
         s.pq = pq;
@@ -774,21 +843,36 @@ static __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(Sell<double> a, Ti
 static __global__ void __launch_bounds__(kBlock) k_cg_xr(Tiles tiles, SysState* st,
                                                   double* __restrict__ x, double* __restrict__ r,
                                                   const double* __restrict__ p,
-                                                  const double* __restrict__ q, double* partials,
-                                                  int* counters, const int* sys_tile0,
+                                                  const double* __restrict__ q, Reduce red,
                                                   Control ctl, int verify_true, X1Out x1o) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     const double alpha = st[c.s].alpha;
     double rr = 0.0, unused = 0.0;
-    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
-        x[row] = __dadd_rn(x[row], __dmul_rn(alpha, p[row]));
-        const double ri = __dsub_rn(r[row], __dmul_rn(alpha, q[row]));
-        r[row] = ri;
-        x1o.put(row, ri);
-        rr = __dadd_rn(rr, __dmul_rn(ri, ri));
+    // four rows per thread per pass: all loads of the pass are issued before any store
+    for (int r0 = c.r0 + threadIdx.x; r0 < c.r1; r0 += 4 * kBlock) {
+        double xi[4], pi[4], ri[4], qi[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = r0 + u * kBlock;
+            const bool ok = row < c.r1;
+            xi[u] = ok ? x[row] : 0.0;
+            pi[u] = ok ? p[row] : 0.0;
+            ri[u] = ok ? r[row] : 0.0;
+            qi[u] = ok ? q[row] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = r0 + u * kBlock;
+            if (row >= c.r1) continue;
+            x[row] = __dadd_rn(xi[u], __dmul_rn(alpha, pi[u]));
+            const double rn = __dsub_rn(ri[u], __dmul_rn(alpha, qi[u]));
+            r[row] = rn;
+            x1o.put(row, rn);
+            rr = __dadd_rn(rr, __dmul_rn(rn, rn));
+        }
     }
-    if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+    if (reduce_system(rr, unused, c.tile, c.s, red) && threadIdx.x == 0) {
         SysState& s = st[c.s];
         s.res = sqrt(rr);
         if (s.res <= s.tol) {
@@ -805,23 +889,23 @@ static __global__ void __launch_bounds__(kBlock) k_cg_xr(Tiles tiles, SysState* 
 
 // Mixed precision: for systems whose recursive residual met the target, recompute
 // r = b - A x in FP64; converged if |r| <= tol, else restart the search direction.
+template <int V>
 static __global__ void __launch_bounds__(kBlock) k_cg_true_check(Sell<double> a, Tiles tiles, SysState* st,
                                                           const double* __restrict__ b,
                                                           const double* __restrict__ x,
-                                                          double* __restrict__ r, double* partials,
-                                                          int* counters, const int* sys_tile0,
+                                                          double* __restrict__ r, Reduce red,
                                                           Control ctl, X1Out x1o) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     if (st[c.s].check == 0) return;
     double rr = 0.0, unused = 0.0;
-    visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, double ax) {
+    visit_rows_v<V>(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, double ax) {
         const double ri = __dsub_rn(b[row], ax);
         r[row] = ri;
         x1o.put(row, ri);
         rr = __dadd_rn(rr, __dmul_rn(ri, ri));
     });
-    if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+    if (reduce_system(rr, unused, c.tile, c.s, red) && threadIdx.x == 0) {
         SysState& s = st[c.s];
         s.check = 0;
         s.res = sqrt(rr);
@@ -858,20 +942,19 @@ __device__ __forceinline__ void precond_tail(SysState& s, double rz_new, double 
 }
 
 // Last post-smoothing sweep of level 0 fused with r.z (and z.q): z = x + wd (b - A x).
-template <class T>
+template <class T, int V>
 static __global__ void __launch_bounds__(kBlock) k_vc_jacobi_final(Sell<T> a, Tiles tiles, SysState* st,
                                                             const T* __restrict__ wd,
                                                             const double* __restrict__ r,
                                                             const T* __restrict__ x,
                                                             T* __restrict__ z,
                                                             const double* __restrict__ q,
-                                                            double* partials, int* counters,
-                                                            const int* sys_tile0, Control ctl,
+                                                            Reduce red, Control ctl,
                                                             int flexible) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     double rz = 0.0, zq = 0.0;
-    visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
+    visit_rows_v<V>(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
         const double ri = r[row];
         const T zi = jac_update<T>(x[row], wd[row], static_cast<T>(ri), s);
         z[row] = zi;
@@ -879,7 +962,7 @@ static __global__ void __launch_bounds__(kBlock) k_vc_jacobi_final(Sell<T> a, Ti
         rz = __dadd_rn(rz, __dmul_rn(ri, zd));
         if (flexible) zq = __dadd_rn(zq, __dmul_rn(zd, q[row]));
     });
-    if (reduce_system(rz, zq, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+    if (reduce_system(rz, zq, c.tile, c.s, red) && threadIdx.x == 0) {
         precond_tail(st[c.s], rz, zq, flexible, ctl);
     }
 }
@@ -892,47 +975,60 @@ static __global__ void __launch_bounds__(kBlock) k_cg_rz(Tiles tiles, SysState* 
                                                   const double* __restrict__ r,
                                                   Z* __restrict__ z, const double* __restrict__ jac,
                                                   const double* __restrict__ jac0,
-                                                  const double* __restrict__ q, double* partials,
-                                                  int* counters, const int* sys_tile0,
+                                                  const double* __restrict__ q, Reduce red,
                                                   Control ctl, int flexible) {
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     const bool jsys = st[c.s].jacobi != 0;
     const int flex = jsys ? 0 : flexible;
     double rz = 0.0, zq = 0.0;
-    for (int row = c.r0 + threadIdx.x; row < c.r1; row += kBlock) {
-        const double ri = r[row];
-        double zd;
-        if (jac != nullptr) {
-            zd = __dmul_rn(ri, jac[row]);
-            z[row] = static_cast<Z>(zd);
-        } else if (jsys) {
-            zd = __dmul_rn(ri, jac0[row]);
-        } else {
-            zd = static_cast<double>(z[row]);
+    // four rows per thread per pass: all loads of the pass are issued before the sums
+    for (int r0 = c.r0 + threadIdx.x; r0 < c.r1; r0 += 4 * kBlock) {
+        double ri[4], zd[4], qi[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = r0 + u * kBlock;
+            const bool ok = row < c.r1;
+            ri[u] = ok ? r[row] : 0.0;
+            if (!ok) {
+                zd[u] = 0.0;
+            } else if (jac != nullptr) {
+                zd[u] = __dmul_rn(ri[u], jac[row]);
+            } else if (jsys) {
+                zd[u] = __dmul_rn(ri[u], jac0[row]);
+            } else {
+                zd[u] = static_cast<double>(z[row]);
+            }
+            qi[u] = ok && flex ? q[row] : 0.0;
         }
-        rz = __dadd_rn(rz, __dmul_rn(ri, zd));
-        if (flex) zq = __dadd_rn(zq, __dmul_rn(zd, q[row]));
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = r0 + u * kBlock;
+            if (row >= c.r1) continue;
+            if (jac != nullptr) z[row] = static_cast<Z>(zd[u]);
+            rz = __dadd_rn(rz, __dmul_rn(ri[u], zd[u]));
+            if (flex) zq = __dadd_rn(zq, __dmul_rn(zd[u], qi[u]));
+        }
     }
-    if (reduce_system(rz, zq, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+    if (reduce_system(rz, zq, c.tile, c.s, red) && threadIdx.x == 0) {
         precond_tail(st[c.s], rz, zq, flex, ctl);
     }
 }
 
 // |b - A x|_2 per system into st.true_res (reporting only; all systems).
+template <int V>
 static __global__ void __launch_bounds__(kBlock) k_true_residual(Sell<double> a, Tiles tiles, SysState* st,
                                                           const double* __restrict__ b,
                                                           const double* __restrict__ x,
-                                                          double* partials, int* counters,
-                                                          const int* sys_tile0) {
+                                                          Reduce red) {
     TileCtx c;
     tile_begin(tiles, nullptr, c);
     double rr = 0.0, unused = 0.0;
-    visit_rows(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, double ax) {
+    visit_rows_v<V>(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, double ax) {
         const double ri = __dsub_rn(b[row], ax);
         rr = __dadd_rn(rr, __dmul_rn(ri, ri));
     });
-    if (reduce_system(rr, unused, c.tile, c.s, partials, counters, sys_tile0) && threadIdx.x == 0) {
+    if (reduce_system(rr, unused, c.tile, c.s, red) && threadIdx.x == 0) {
         st[c.s].true_res = sqrt(rr);
     }
 }

@@ -239,11 +239,16 @@ int cfdb_system_kernel_launches(const cfdb_system* sys, unsigned long long* coun
 
 /* Launch-shape / schedule knobs of the device plan (see cfd_b200/autotune.py). */
 typedef struct {
-    int target_tiles; /* SELL tiles (256-thread CTAs) per level, default 1184 = 148 SMs x 8 */
+    int target_tiles; /* level-0 Krylov tiles (reductions): about this many CTAs, default 1184 =
+                         148 SMs x 8; 0 = 256 rows per CTA */
     int wide_row;     /* average row length above which CSR lane groups are used, default 48 */
     int lanes_div;    /* lanes per CSR row ~ average row length / lanes_div (4..256, and enough
                          lanes for ~150K threads per operator), default 16 */
     int fuse_first;   /* first two smoothing sweeps in one kernel, default 0 */
+    int sell_rows;    /* rows per CTA of SELL operators (one row per thread per pass): a multiple
+                         of 256, default 256 */
+    int krylov_pair;  /* level-0 Krylov SpMV kernels take two rows per thread per pass (1) or one
+                         (0), default 1 */
 } cfdb_tuning;
 void cfdb_default_tuning(cfdb_tuning* t);
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t);

@@ -121,7 +121,7 @@ _proto("cfdb_system_kernel_launches", [_vp, _P(C.c_ulonglong)])
 
 class TuningStruct(C.Structure):
     _fields_ = [("target_tiles", _i), ("wide_row", _i), ("lanes_div", _i), ("fuse_first", _i),
-                ("sell_rows", _i), ("krylov_pair", _i)]
+                ("sell_rows", _i), ("krylov_pair", _i), ("tail_rows", _i)]
 
 
 _proto("cfdb_default_tuning", [_P(TuningStruct)], None)
@@ -684,10 +684,12 @@ class Tuning:
     fuse_first: int = 0
     sell_rows: int = 256
     krylov_pair: int = 1
+    tail_rows: int = 0
 
     def _c(self):
         return TuningStruct(int(self.target_tiles), int(self.wide_row), int(self.lanes_div),
-                            int(self.fuse_first), int(self.sell_rows), int(self.krylov_pair))
+                            int(self.fuse_first), int(self.sell_rows), int(self.krylov_pair),
+                            int(self.tail_rows))
 
 
 def _set_system_tuning(self, t: Tuning) -> None:

@@ -8,7 +8,8 @@ The knobs are those of `Tuning` (include/cfdb.h, cfdb_tuning):
 * lanes_div    - lanes per CSR row = average row length / lanes_div,
 * fuse_first   - first two Jacobi sweeps of the pre-smoothing fused into one kernel,
 * sell_rows    - rows per CTA of SELL operators (one row per thread per pass),
-* krylov_pair  - level-0 Krylov SpMV kernels take two rows per thread per pass, or one.
+* krylov_pair  - level-0 Krylov SpMV kernels take two rows per thread per pass, or one,
+* tail_rows    - coarse levels of at most this many rows run in one persistent kernel.
 
 The search is a coordinate descent from the defaults: each knob in turn is swept over its
 candidate values with the others fixed, the best value kept, and the pass repeated until no
@@ -34,6 +35,7 @@ CANDIDATES = {
     "fuse_first": [0, 1],
     "sell_rows": [256, 512, 1024],
     "krylov_pair": [0, 1],
+    "tail_rows": [0, 1024, 8192],
 }
 
 

@@ -12,6 +12,7 @@
 
 namespace cfdb {
 void set_thread_error(const std::string& msg); // capi.cu
+Tuning tuning_from(const cfdb_tuning* t);     // capi.cu
 }
 
 using namespace cfdb;
@@ -246,8 +247,7 @@ int cfdb_batch_set_precision(cfdb_batch* b, int precision) {
 int cfdb_batch_set_tuning(cfdb_batch* b, const cfdb_tuning* t) {
     return guarded_b([&] {
         if (b == nullptr || t == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
-        if (t->target_tiles < 1 || t->wide_row < 0 || t->lanes_div < 1) fail(CFDB_ERR_BAD_ARG, "tuning values out of range");
-        b->tuning = Tuning{t->target_tiles, t->wide_row, t->lanes_div, t->fuse_first != 0 ? 1 : 0};
+        b->tuning = tuning_from(t);
         b->dirty = true;
         ensure_batch_engine(b);
     });

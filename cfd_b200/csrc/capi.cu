@@ -102,6 +102,18 @@ std::shared_ptr<Hierarchy> hierarchy_from(const cfdb_amg_view& v, int n0, bool s
 namespace cfdb {
 // Records the calling thread's last error message (used by entry points in other files).
 void set_thread_error(const std::string& msg) { g_last_error = msg; }
+
+// Validated engine tuning from the C struct (shared with the batch API).
+Tuning tuning_from(const cfdb_tuning* t) {
+    if (t == nullptr) fail(CFDB_ERR_BAD_ARG, "null tuning");
+    if (t->target_tiles < 0 || t->wide_row < 0 || t->lanes_div < 1)
+        fail(CFDB_ERR_BAD_ARG, "tuning values out of range");
+    if (t->sell_rows < kSellRows || t->sell_rows % kSellRows != 0 || t->sell_rows > 16 * kSellRows)
+        fail(CFDB_ERR_BAD_ARG, "tuning: sell_rows must be a multiple of 256 in 256..4096");
+    return Tuning{t->target_tiles, t->wide_row, t->lanes_div, t->fuse_first != 0 ? 1 : 0, t->sell_rows,
+                  t->krylov_pair != 0 ? 1 : 0, std::max(t->tail_rows, 0)};
+}
+
 } // namespace cfdb
 
 // ------------------------------------------------------------------------------------------------
@@ -871,16 +883,7 @@ void cfdb_default_tuning(cfdb_tuning* t) {
     t->fuse_first = d.fuse_first;
     t->sell_rows = d.sell_rows;
     t->krylov_pair = d.krylov_pair;
-}
-
-static Tuning tuning_from(const cfdb_tuning* t) {
-    if (t == nullptr) fail(CFDB_ERR_BAD_ARG, "null tuning");
-    if (t->target_tiles < 0 || t->wide_row < 0 || t->lanes_div < 1)
-        fail(CFDB_ERR_BAD_ARG, "tuning values out of range");
-    if (t->sell_rows < kSellRows || t->sell_rows % kSellRows != 0 || t->sell_rows > 16 * kSellRows)
-        fail(CFDB_ERR_BAD_ARG, "tuning: sell_rows must be a multiple of 256 in 256..4096");
-    return Tuning{t->target_tiles, t->wide_row, t->lanes_div, t->fuse_first != 0 ? 1 : 0, t->sell_rows,
-                  t->krylov_pair != 0 ? 1 : 0};
+    t->tail_rows = d.tail_rows;
 }
 
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t) {

@@ -144,6 +144,10 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
     release_graphs();
     arena_.clear();
     lv_.clear();
+    tail32_ = nullptr;
+    tail64_ = nullptr;
+    tail_n32_ = tail_n64_ = tail_grid32_ = tail_grid64_ = 0;
+    tail_bar_ = nullptr;
     n_sys_ = static_cast<int>(systems.size());
     if (n_sys_ == 0) fail(1, "engine: no systems");
     if (sweeps < 0) fail(1, "engine: negative smoothing sweeps");
@@ -452,6 +456,8 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         red_.sys_tile0 = arena_.upload(sys_tile0, st);
         red_.grp0 = arena_.upload(grp0, st);
         n_active_ = arena_.alloc<int>(1);
+        tail_bar_ = arena_.alloc<unsigned>(2);
+        CFDB_CUDA(cudaMemsetAsync(tail_bar_, 0, 2 * sizeof(unsigned), st));
         error_ = arena_.alloc<int>(1);
         CFDB_CUDA(cudaMemsetAsync(error_, 0, sizeof(int), st));
     }
@@ -700,6 +706,154 @@ X1Out Engine::x1_out(Mode mode) const {
     return o;
 }
 
+// First level of the persistent tail, or n_levels_ when the tail is not used: the levels from
+// there down must all be small (<= tail_rows rows) lane-group CSR operators, the schedule the
+// unfused one (first sweeps written by the restrictions), and the engine not in ordered mode.
+int Engine::tail_level() const {
+    const bool fuse = sweeps_ >= 2 && tuning_.fuse_first != 0;
+    if (!has_amg_ || ordered_ || fuse || sweeps_ == 0 || tuning_.tail_rows <= 0 || n_levels_ < 3) return n_levels_;
+    int lt = n_levels_ - 1;
+    while (lt - 1 >= 1) {
+        const int l = lt - 1;
+        const DevLevel& d = lv_[l];
+        if (d.n_rows > tuning_.tail_rows) break;
+        auto csr = [](const DevSell64_32& m) { return m.s64.val != nullptr ? m.s64.fmt != kFmtSell : m.s32.fmt != kFmtSell; };
+        if (d.a.n_tiles > 0 && !csr(d.a)) break;
+        if (d.p.n_tiles > 0 && !csr(d.p)) break;
+        if (d.r.n_tiles > 0 && !csr(d.r)) break;
+        lt = l;
+    }
+    return lt <= n_levels_ - 2 ? lt : n_levels_;
+}
+
+// Phase list of the tail for precision T (uploaded before any graph capture that uses it).
+template <class T> void Engine::prepare_tail() {
+    TailPhase<T>*& dev = sizeof(T) == 8 ? reinterpret_cast<TailPhase<T>*&>(tail64_) : reinterpret_cast<TailPhase<T>*&>(tail32_);
+    int& count = sizeof(T) == 8 ? tail_n64_ : tail_n32_;
+    int& grid = sizeof(T) == 8 ? tail_grid64_ : tail_grid32_;
+    double& bytes = sizeof(T) == 8 ? tail_bytes64_ : tail_bytes32_;
+    if (dev != nullptr) return;
+    const int L = n_levels_;
+    const int lt = tail_level();
+    count = 0;
+    if (lt >= L) return;
+    auto X = [&](int l) { return vx<T>(lv_[l].x64, lv_[l].x32); };
+    auto Y = [&](int l) { return vx<T>(lv_[l].y64, lv_[l].y32); };
+    auto Tv = [&](int l) { return vx<T>(lv_[l].t64, lv_[l].t32); };
+    auto Bv = [&](int l) { return vx<T>(lv_[l].b64, lv_[l].b32); };
+    auto WD = [&](int l) -> const T* {
+        if constexpr (sizeof(T) == 8) return lv_[l].wd64;
+        else return lv_[l].wd32;
+    };
+    auto OP = [&](const DevSell64_32& m) { return vs_sel<T>(m.s64, m.s32); };
+    const double sv = sizeof(T);
+    auto csr_b = [&](const DevSell64_32& m, double rows, double cols) {
+        return static_cast<double>(m.nnz) * (sv + 4.0) + 4.0 * (rows + 1.0) + sv * cols + sv * rows;
+    };
+    std::vector<TailPhase<T>> ph;
+    bytes = 0.0;
+    int max_blocks = 1;
+    auto add = [&](int kind, const DevSell64_32& m, int n, const T* x, const T* b, const T* wd, T* y, T* x1, int n1,
+                   double by) {
+        TailPhase<T> p{};
+        p.kind = kind;
+        p.n = n;
+        p.m = OP(m);
+        p.x = x;
+        p.b = b;
+        p.wd = wd;
+        p.y = y;
+        p.x1 = x1;
+        p.n1 = n1;
+        ph.push_back(p);
+        bytes += by;
+        if (kind != kTailCoarse) max_blocks = std::max(max_blocks, ceil_div(n, kBlock / p.m.fmt));
+    };
+    std::vector<T*> cur(L, nullptr);
+    for (int l = lt; l + 1 < L; ++l) {
+        const DevLevel& d = lv_[l];
+        const double n = d.n_rows_nc;
+        T* x = X(l);
+        T* y = Y(l);
+        T* c = start_buffer<T>(l);
+        for (int k = 1; k < sweeps_; ++k) {
+            T* o = c == x ? y : x;
+            add(kTailJacobi, d.a, d.a.n_slices, c, Bv(l), WD(l), o, nullptr, 0, csr_b(d.a, n, n) + 3.0 * sv * n);
+            c = o;
+        }
+        cur[l] = c;
+        add(kTailResidual, d.a, d.a.n_slices, c, Bv(l), nullptr, Tv(l), nullptr, 0, csr_b(d.a, n, n) + sv * n);
+        const DevLevel& nx = lv_[l + 1];
+        const bool next_x1 = l + 2 < L && nx.n_rows_nc > 0;
+        add(kTailRestrict, d.r, d.r.n_slices, Tv(l), nullptr, next_x1 ? WD(l + 1) : nullptr, Bv(l + 1),
+            next_x1 ? start_buffer<T>(l + 1) : nullptr, next_x1 ? nx.n_rows_nc : 0,
+            csr_b(d.r, nx.n_rows, n) + (next_x1 ? 2.0 * sv * nx.n_rows_nc : 0.0));
+    }
+    {
+        TailPhase<T> p{};
+        p.kind = kTailCoarse;
+        ph.push_back(p);
+        bytes += coarse_bytes_ + 2.0 * sv * coarse_rows_;
+        max_blocks = std::max(max_blocks, n_ctiles_);
+    }
+    for (int l = L - 2; l >= lt; --l) {
+        const DevLevel& d = lv_[l];
+        const double n = d.n_rows_nc;
+        T* x = X(l);
+        T* y = Y(l);
+        T* c = cur[l];
+        add(kTailProlong, d.p, d.p.n_slices, X(l + 1), nullptr, nullptr, c, nullptr, 0,
+            csr_b(d.p, n, lv_[l + 1].n_rows) + sv * n);
+        for (int k = 0; k < sweeps_; ++k) {
+            T* o = c == x ? y : x;
+            add(kTailJacobi, d.a, d.a.n_slices, c, Bv(l), WD(l), o, nullptr, 0, csr_b(d.a, n, n) + 3.0 * sv * n);
+            c = o;
+        }
+    }
+    // grid: co-resident CTAs (cooperative launch), no more than the largest phase can use
+    const size_t smem = sizeof(T) == 8 ? coarse_smem64_ : coarse_smem32_;
+    CFDB_CUDA(cudaFuncSetAttribute(k_vc_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    int per_sm = 0, sms = 0;
+    CFDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vc_tail<T>, kBlock, smem));
+    CFDB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+    if (per_sm <= 0) return;  // cannot be co-resident: keep the separate kernels
+    grid = std::max(1, std::min(per_sm * sms, max_blocks));
+    TailPhase<T>* d = arena_.alloc<TailPhase<T>>(ph.size());
+    CFDB_CUDA(cudaMemcpyAsync(d, ph.data(), sizeof(TailPhase<T>) * ph.size(), cudaMemcpyHostToDevice, stream_));
+    CFDB_CUDA(cudaStreamSynchronize(stream_));
+    dev = d;
+    count = static_cast<int>(ph.size());
+}
+
+template <class T> void Engine::launch_tail(cudaStream_t s) {
+    const TailPhase<T>* ph = sizeof(T) == 8 ? reinterpret_cast<const TailPhase<T>*>(tail64_)
+                                            : reinterpret_cast<const TailPhase<T>*>(tail32_);
+    const int count = sizeof(T) == 8 ? tail_n64_ : tail_n32_;
+    const int grid = sizeof(T) == 8 ? tail_grid64_ : tail_grid32_;
+    T* const* b_lv;
+    T* const* x_lv;
+    if constexpr (sizeof(T) == 8) {
+        b_lv = b_level64_;
+        x_lv = x_level64_;
+    } else {
+        b_lv = b_level32_;
+        x_lv = x_level32_;
+    }
+    const size_t smem = sizeof(T) == 8 ? coarse_smem64_ : coarse_smem32_;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid));
+    cfg.blockDim = dim3(kBlock);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CFDB_CUDA(cudaLaunchKernelEx(&cfg, k_vc_tail<T>, ph, count, cb_, n_ctiles_, b_lv, x_lv,
+                                 static_cast<const int*>(block_level_), tail_bar_, error_));
+}
+
 template <class T>
 void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
     cudaStream_t s = stream_;
@@ -737,8 +891,11 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
         return {m.tiles, nc ? m.n_tiles_nc : m.n_tiles, m.block, visit_of(m.s64.val != nullptr ? m.s64.fmt : m.s32.fmt)};
     };
     std::vector<T*> cur(L, nullptr);
+    // levels lt and below run in the persistent tail kernel when its phases are prepared
+    const int tail_count = sizeof(T) == 8 ? tail_n64_ : tail_n32_;
+    const int lt = tail_count > 0 ? tail_level() : L;
     // ---- down ----
-    for (int l = 0; l + 1 < L; ++l) {
+    for (int l = 0; l + 1 < L && l < lt; ++l) {
         const DevLevel& d = lv_[l];
         if (d.a.n_tiles_nc == 0) continue;  // no system continues past this level
         const double n = d.n_rows_nc;
@@ -797,7 +954,10 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
     // ---- coarsest blocks (dense inverse of each multi-level system's coarsest operator) ----
     const Control ctl{n_active_, error_};
     const int ord = ordered_ ? 1 : 0;
-    if (n_ctiles_ > 0) {
+    if (lt < L) {
+        launch_tail<T>(s);
+        mark("tail", lt, sizeof(T) == 8 ? tail_bytes64_ : tail_bytes32_);
+    } else if (n_ctiles_ > 0) {
         if constexpr (sizeof(T) == 8) {
             k_vc_coarse<double, double><<<n_ctiles_, kBlock, coarse_smem64_, s>>>(cb_, stv, b_level64_, x_level64_,
                                                                                   block_level_, ctl, ord);
@@ -808,7 +968,7 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
         mark("coarse", L - 1, coarse_bytes_ + 2.0 * sv * coarse_rows_);
     }
     // ---- up ----
-    for (int l = L - 2; l >= 0; --l) {
+    for (int l = std::min(L - 2, lt - 1); l >= 0; --l) {
         const DevLevel& d = lv_[l];
         if (d.a.n_tiles_nc == 0) continue;  // no system continues past this level
         const double n = d.n_rows_nc;
@@ -936,6 +1096,8 @@ void Engine::mark(const char* name, int level, double bytes) {
 std::vector<ProfRecord> Engine::profile(Mode mode, int reps) {
     CFDB_CUDA(cudaSetDevice(device_));
     if (mode != Mode::Jacobi && !has_amg_) fail(5, "profile: no AMG hierarchy set");
+    if (mode == Mode::AmgMixed) prepare_tail<float>();
+    else if (mode == Mode::AmgFp64) prepare_tail<double>();
     std::vector<ProfRecord> out;
     std::vector<int> count;
     // b = 1 on every real row, x = 0: a nonzero residual whatever the engine held before (the
@@ -997,6 +1159,8 @@ std::vector<ProfRecord> Engine::profile(Mode mode, int reps) {
 void Engine::capture_graphs(Mode mode) {
     const int m = static_cast<int>(mode);
     if (graphs_[m][0] != nullptr) return;
+    if (mode == Mode::AmgMixed) prepare_tail<float>();
+    else if (mode == Mode::AmgFp64) prepare_tail<double>();
     for (int which = 0; which < 2; ++which) {
         cudaGraph_t g = nullptr;
         CFDB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -1107,6 +1271,8 @@ std::vector<SolveResult> Engine::solve(Mode mode, const std::vector<SolveRequest
 
 void Engine::apply_vcycle(Mode mode, const std::vector<int>&) {
     if (!has_amg_) fail(5, "apply_vcycle: no hierarchy");
+    if (mode == Mode::AmgMixed) prepare_tail<float>();
+    else prepare_tail<double>();
     // run with all systems treated as active (state pointer null) and no Krylov bookkeeping
     SysState* keep = st_;
     st_ = nullptr;

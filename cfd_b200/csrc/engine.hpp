@@ -35,6 +35,8 @@ struct Tuning {
     int fuse_first = 0;         // first two smoothing sweeps in one kernel (x1 recomputed)
     int sell_rows = kSellRows;  // rows per CTA of SELL operators (multiple of kSellRows)
     int krylov_pair = 1;        // level-0 Krylov SpMV kernels: two rows per thread per pass
+    int tail_rows = 0;          // coarse levels of at most this many rows (and everything below
+                                // them) run as one persistent tail kernel; 0 disables it
 };
 
 struct SolveRequest {
@@ -160,6 +162,10 @@ private:
     void enqueue_vcycle(Mode mode, bool fused_final, int flexible, bool x1_ready0);
     template <class T> void enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0);
     template <class T> T* start_buffer(int l) const;
+    // V-cycle tail (small coarse levels in one persistent kernel): first level, phases
+    int tail_level() const;
+    template <class T> void prepare_tail();
+    template <class T> void launch_tail(cudaStream_t s);
     // rows per thread per pass of the level-0 Krylov SpMV kernels (two, or one)
     int krylov_visit() const { return tuning_.krylov_pair ? kVisitSell2 : kVisitSell1; }
     // where the residual producers of `mode` write the level-0 first sweep (n = 0: nowhere)
@@ -213,6 +219,12 @@ private:
     int n_single_ = 0;        // systems whose hierarchy has one level (Jacobi-preconditioned CG)
     std::vector<int> single_; // per original system: 1 if its hierarchy has one level
     int n_ctiles_ = 0;        // coarse-solve tiles
+    // persistent tail: phase lists per precision (device), barrier words
+    TailPhase<float>* tail32_ = nullptr;
+    TailPhase<double>* tail64_ = nullptr;
+    int tail_n32_ = 0, tail_n64_ = 0, tail_grid32_ = 0, tail_grid64_ = 0;
+    double tail_bytes32_ = 0.0, tail_bytes64_ = 0.0;
+    unsigned* tail_bar_ = nullptr;
     CoarseBlocks cb_{};
     int* block_level_ = nullptr;
     double** b_level64_ = nullptr;

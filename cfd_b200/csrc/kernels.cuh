@@ -1118,4 +1118,135 @@ static __global__ void k_assemble_cells(int n, const int* __restrict__ cf_ptr,
     div[c] = v;
 }
 
+// ---------------------------------------------------------------------------------------------
+// V-cycle tail: the small coarse levels and the dense coarse solve in one persistent kernel.
+// Each coarse level costs six small kernels whose run time is launch and ramp latency; here
+// every phase is a grid-stride loop over the operator's rows, separated by a grid barrier.
+// The kernel is launched cooperatively (all CTAs co-resident) and every barrier wait is
+// bounded: on expiry the kernel sets the error flag and returns. It processes every system's
+// rows (no per-system activity test: the rows of converged systems are only level vectors).
+// Phase arithmetic is the same per row as the separate kernels (same lane sums and coarse
+// row products), so the results do not depend on which path ran.
+// ---------------------------------------------------------------------------------------------
+enum : int { kTailJacobi = 0, kTailResidual = 1, kTailRestrict = 2, kTailProlong = 3, kTailCoarse = 4 };
+
+template <class T> struct TailPhase {
+    int kind;
+    int n;          // rows of the operator
+    Sell<T> m;      // CSR operator (lane groups); unused by kTailCoarse
+    const T* x;     // gathered vector (A x, R t, P xc)
+    const T* b;     // right-hand side (jacobi, residual)
+    const T* wd;    // w/diag (jacobi), or of the coarser level (restriction's first sweep)
+    T* y;           // output (jacobi / residual / restriction), iterate (prolongation, in place)
+    T* x1;          // restriction: first sweep of the coarser level (rows < n1), or null
+    int n1;
+};
+
+constexpr int kTailSpinLimit = 1 << 22;
+
+// Grid-wide barrier over `nblocks` co-resident CTAs: bar[0] counts arrivals, bar[1] is the
+// generation. Bounded: returns false (error flag set) if the generation does not move.
+__device__ __forceinline__ bool tail_barrier(unsigned* bar, unsigned nblocks, int* error) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = bar + 1;
+        const unsigned g0 = *gen;
+        __threadfence();
+        int good = 1;
+        if (atomicAdd(&bar[0], 1u) + 1u == nblocks) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicAdd(&bar[1], 1u);
+        } else {
+            for (int spin = 0; *gen == g0; ++spin) {
+                if (spin >= kTailSpinLimit) {
+                    good = 0;
+                    atomicExch(error, 2);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// f(row, sum) for every row of a CSR lane-group operator, grid-stride over blocks of
+// kBlock / G rows (every thread of a block runs the same number of passes).
+template <class T, class XA, class F>
+__device__ __forceinline__ void tail_rows(const Sell<T>& m, int n, XA xa, F f) {
+    const int G = m.fmt;
+    const int rpb = kBlock / G;
+    const int sub = static_cast<int>(threadIdx.x) & (G - 1);
+    for (int base = blockIdx.x * rpb; base < n; base += gridDim.x * rpb) {
+        const int row = base + static_cast<int>(threadIdx.x) / G;
+        const bool valid = row < n;
+        T s;
+        if (G <= 32) s = csr_group_sum(m, row, valid, sub, G, xa);
+        else s = csr_block_sum(m, row, valid, sub, G, xa);
+        if (valid && sub == 0) f(row, s);
+    }
+}
+
+template <class T>
+static __global__ void __launch_bounds__(kBlock, 4) k_vc_tail(const TailPhase<T>* __restrict__ phases, int n_phases,
+                                                    CoarseBlocks cb, int n_ctiles, T* const* __restrict__ b_level,
+                                                    T* const* __restrict__ x_level,
+                                                    const int* __restrict__ block_level, unsigned* bar,
+                                                    int* error) {
+    extern __shared__ __align__(16) unsigned char tail_smem[];
+    for (int ph = 0; ph < n_phases; ++ph) {
+        const TailPhase<T> P = phases[ph];
+        if (P.kind == kTailCoarse) {
+            T* bs = reinterpret_cast<T*>(tail_smem);
+            for (int t = blockIdx.x; t < n_ctiles; t += gridDim.x) {
+                const int blk = cb.tile_blk[t];
+                const int n = cb.n[blk];
+                const int r0 = cb.row[blk];
+                const int lvl = block_level[blk];
+                const T* b = b_level[lvl] + r0;
+                T* x = x_level[lvl] + r0;
+                for (int j = threadIdx.x; j < n; j += kBlock) bs[j] = __ldcg(&b[j]);
+                __syncthreads();
+                const int i = cb.tile_row[t] + (threadIdx.x >> 5);
+                const int lane = threadIdx.x & 31;
+                if (i < n) {
+                    const double* mr = cb.mr + cb.m_off[blk] + static_cast<long long>(i) * n;
+                    double acc = 0.0;
+                    for (int j = lane; j < n; j += 32) acc = __dadd_rn(acc, __dmul_rn(__ldg(&mr[j]), static_cast<double>(bs[j])));
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xffffffffu, acc, o));
+                    if (lane == 0) x[i] = static_cast<T>(acc);
+                }
+                __syncthreads();
+            }
+        } else {
+            // vectors written by earlier phases of this kernel are read through L2 (ld.cg): the
+            // grid barrier orders the writes, and L2 is coherent across SMs. One row-sum
+            // instance serves every phase kind (the kind only selects the epilogue).
+            const T* x = P.x;
+            auto xa = [x](int j) { return __ldcg(&x[j]); };
+            tail_rows(P.m, P.n, xa, [&](int row, T s) {
+                if (P.kind == kTailJacobi) {
+                    P.y[row] = jac_update<T>(__ldcg(&x[row]), P.wd[row], __ldcg(&P.b[row]), s);
+                } else if (P.kind == kTailResidual) {
+                    if constexpr (sizeof(T) == 8) P.y[row] = __dsub_rn(__ldcg(&P.b[row]), s);
+                    else P.y[row] = __ldcg(&P.b[row]) - s;
+                } else if (P.kind == kTailRestrict) {
+                    P.y[row] = s;
+                    if (P.x1 != nullptr && row < P.n1) P.x1[row] = first_sweep<T>(P.wd[row], s);
+                } else {
+                    if constexpr (sizeof(T) == 8) P.y[row] = __dadd_rn(__ldcg(&P.y[row]), s);
+                    else P.y[row] = __ldcg(&P.y[row]) + s;
+                }
+            });
+        }
+        if (ph + 1 < n_phases && !tail_barrier(bar, gridDim.x, error)) return;
+    }
+}
+
 } // namespace cfdb

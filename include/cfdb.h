@@ -249,6 +249,8 @@ typedef struct {
                          of 256, default 256 */
     int krylov_pair;  /* level-0 Krylov SpMV kernels take two rows per thread per pass (1) or one
                          (0), default 1 */
+    int tail_rows;    /* coarse levels of at most this many rows, with all coarser ones, run as one
+                         persistent kernel; 0 (default) disables it */
 } cfdb_tuning;
 void cfdb_default_tuning(cfdb_tuning* t);
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t);

@@ -8,7 +8,7 @@ from cfd_b200.autotune import CANDIDATES, coordinate_search
 
 def test_coordinate_search_finds_separable_minimum():
     target = {"target_tiles": 148 * 16, "wide_row": 32, "lanes_div": 8, "fuse_first": 1, "sell_rows": 512,
-              "krylov_pair": 0}
+              "krylov_pair": 0, "tail_rows": 8192}
     calls = []
 
     def cost(t):

@@ -189,3 +189,26 @@ def test_mixed_precision_reaches_target(gpu, make):
     assert np.linalg.norm(src - a.matvec(x)) <= tol
     xo, so = O.amg_cg(h.a, h.p, h.r, h.coarse_inverse, src, abs_tol=tol, max_iterations=500)
     assert np.linalg.norm(x - xo) <= 1e-5 * np.linalg.norm(xo)
+
+
+@pytest.mark.parametrize("precision", ["FP64", "MIXED"])
+def test_persistent_tail_matches_separate_kernels(gpu, precision):
+    """The persistent tail kernel (small coarse levels + coarse solve in one cooperative launch)
+    computes every row exactly as the separate per-level kernels do."""
+    cb = gpu
+    case = W.graded(24)
+    up, lo, diag, src = _assembled(case)
+    ds = cb.DeviceSolver(cb.build_csr_pattern(case.n, case.owner, case.neighbour))
+    ds.set_precision(getattr(cb.Precision, precision))
+    ds.setup_amg(diag, up, lo, cb.AmgSettings(strength_threshold=0.04))
+    tol = 1e-10 * np.linalg.norm(src)
+    out = []
+    for tail in (0, 10**6):
+        ds.set_tuning(cb.Tuning(tail_rows=tail))
+        x = np.zeros(case.n)
+        st = ds.solve(diag, up, lo, src, x, cb.Method.Cg, True, cb.SolveControl(tol, 500))
+        z = ds.apply_amg(np.random.default_rng(3).standard_normal(case.n))
+        assert st.converged
+        out.append((x, st.iterations, z))
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][2], out[1][2])

@@ -111,7 +111,7 @@ Tuning tuning_from(const cfdb_tuning* t) {
     if (t->sell_rows < kSellRows || t->sell_rows % kSellRows != 0 || t->sell_rows > 16 * kSellRows)
         fail(CFDB_ERR_BAD_ARG, "tuning: sell_rows must be a multiple of 256 in 256..4096");
     return Tuning{t->target_tiles, t->wide_row, t->lanes_div, t->fuse_first != 0 ? 1 : 0, t->sell_rows,
-                  t->krylov_pair != 0 ? 1 : 0, std::max(t->tail_rows, 0)};
+                  t->krylov_pair != 0 ? 1 : 0, t->col16 != 0 ? 1 : 0, std::max(t->tail_rows, 0)};
 }
 
 } // namespace cfdb
@@ -215,9 +215,6 @@ SolveResult run_single(cfdb_system* s, const double* diag, const double* upper, 
                        const double* b, double* x, int method, int use_amg, const cfdb_control* c, bool dev) {
     if (c == nullptr) fail(CFDB_ERR_BAD_ARG, "null control");
     if (method != CFDB_METHOD_CG && method != CFDB_METHOD_BICGSTAB) fail(CFDB_ERR_BAD_ARG, "unknown method");
-    if (method == CFDB_METHOD_BICGSTAB) {
-        fail(CFDB_ERR_BAD_ARG, "BiCGStab is not provided by this library (pressure path: CG)");
-    }
     if (diag == nullptr || b == nullptr || x == nullptr || (s->pat.n_faces > 0 && (upper == nullptr || lower == nullptr)))
         fail(CFDB_ERR_BAD_ARG, "null array");
     ensure_engine(s);
@@ -231,15 +228,15 @@ SolveResult run_single(cfdb_system* s, const double* diag, const double* upper, 
     }
     e.set_rhs(0, b, dev);
     e.set_guess(0, x, dev);
+    // krylov_cuda.cu:659-669: with a hierarchy and use_amg the solve is AMG-CG whatever the
+    // method; otherwise Jacobi-preconditioned CG or BiCGStab on the FP64 level-0 operator
     Mode mode = Mode::Jacobi;
     if (use_amg && s->h) mode = s->precision == CFDB_PRECISION_MIXED ? Mode::AmgMixed : Mode::AmgFp64;
-    if (mode == Mode::Jacobi && s->precision == CFDB_PRECISION_MIXED) {
-        // Jacobi CG runs on the FP64 level-0 operator, which exists in every precision.
-    }
     SolveRequest rq;
     rq.tol = c->abs_tolerance;
     rq.max_it = c->max_iterations;
-    const auto res = e.solve(mode, {rq});
+    const auto res = (mode == Mode::Jacobi && method == CFDB_METHOD_BICGSTAB) ? std::vector<SolveResult>{e.solve_bicgstab(rq)}
+                                                                              : e.solve(mode, {rq});
     e.get_solution(0, x, dev);
     CFDB_CUDA(cudaStreamSynchronize(e.stream()));
     return res[0];
@@ -419,8 +416,7 @@ int cfdb_solve(const cfdb_csr* a, const double* b, double* x, int method, const 
     return guarded([&] {
         require_device();
         if (a == nullptr || b == nullptr || x == nullptr || control == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
-        if (method == CFDB_METHOD_BICGSTAB) fail(CFDB_ERR_BAD_ARG, "BiCGStab is not provided by this library");
-        if (method != CFDB_METHOD_CG) fail(CFDB_ERR_BAD_ARG, "unknown method");
+        if (method != CFDB_METHOD_CG && method != CFDB_METHOD_BICGSTAB) fail(CFDB_ERR_BAD_ARG, "unknown method");
         if (a->n == 0) {
             put_stats(stats, SolveResult{0, 0.0, true, 0.0});
             return;
@@ -446,9 +442,10 @@ int cfdb_solve(const cfdb_csr* a, const double* b, double* x, int method, const 
         e.upload_values({m.va.data()});
         e.set_rhs(0, b, false);
         e.set_guess(0, x, false);
-        const auto r = e.solve(Mode::Jacobi, {SolveRequest{control->abs_tolerance, control->max_iterations}});
+        const SolveRequest rq{control->abs_tolerance, control->max_iterations};
+        const SolveResult r = method == CFDB_METHOD_BICGSTAB ? e.solve_bicgstab(rq) : e.solve(Mode::Jacobi, {rq})[0];
         e.get_solution(0, x, false);
-        put_stats(stats, r[0]);
+        put_stats(stats, r);
     });
 }
 
@@ -884,6 +881,7 @@ void cfdb_default_tuning(cfdb_tuning* t) {
     t->sell_rows = d.sell_rows;
     t->krylov_pair = d.krylov_pair;
     t->tail_rows = d.tail_rows;
+    t->col16 = d.col16;
 }
 
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t) {

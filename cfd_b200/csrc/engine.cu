@@ -21,7 +21,40 @@ struct SellBuild {
     bool with_src = false;
     bool sort = false;      // reorder rows by length within aligned windows of kSellRows
     std::vector<int> perm;  // row at each position (when sort)
+    std::vector<char> pad;  // 1 for padding slots
 };
+
+// 16-bit column offsets of the groups [ptr[g], ptr[g+1]) of `col` (SELL slices or CSR rows):
+// base[g] = smallest real column of the group, c16[k] = col[k] - base[g]; padding entries
+// (pad[k] != 0) and entries outside every group get offset 0. False when some group spans
+// 65536 columns or more (the operator then keeps int32 columns).
+bool compress_cols(const std::vector<int>& ptr, const std::vector<int>& col, const std::vector<char>* pad,
+                   std::vector<uint16_t>& c16, std::vector<int>& base) {
+    const long long ng = static_cast<long long>(ptr.size()) - 1;
+    c16.assign(col.size(), 0);
+    base.assign(static_cast<size_t>(std::max(ng, 1LL)), 0);
+    int ok = 1;
+#pragma omp parallel for schedule(static) reduction(&& : ok)
+    for (long long g = 0; g < ng; ++g) {
+        int lo = INT_MAX, hi = INT_MIN;
+        for (int k = ptr[g]; k < ptr[g + 1]; ++k) {
+            if (pad != nullptr && (*pad)[k]) continue;
+            lo = std::min(lo, col[k]);
+            hi = std::max(hi, col[k]);
+        }
+        if (lo > hi) continue;  // padding only
+        if (static_cast<long long>(hi) - lo > 65535) {
+            ok = 0;
+            continue;
+        }
+        base[g] = lo;
+        for (int k = ptr[g]; k < ptr[g + 1]; ++k) {
+            if (pad != nullptr && (*pad)[k]) continue;
+            c16[k] = static_cast<uint16_t>(col[k] - lo);
+        }
+    }
+    return ok != 0;
+}
 
 // Appends rows [0, n_rows) of a CSR block (n_pad >= n_rows, multiple of 32) whose first row has
 // global index row0. Column indices are shifted by col_off; padding slots read column pad_col
@@ -48,6 +81,7 @@ void sell_append(SellBuild& sb, int n_rows, int n_pad, const int* rp, const int*
         const size_t slots = static_cast<size_t>(width) * 32;
         sb.col.resize(base + slots, pad_col);
         sb.val.resize(base + slots, 0.0);
+        sb.pad.resize(base + slots, 1);
         if (sb.with_src) sb.src.resize(base + slots, -1);
         for (int lane = 0; lane < 32; ++lane) {
             const int i = order[s0 + lane];
@@ -56,6 +90,7 @@ void sell_append(SellBuild& sb, int n_rows, int n_pad, const int* rp, const int*
             for (int k = 0; k < len; ++k) {
                 const size_t slot = base + static_cast<size_t>(k) * 32 + lane;
                 const int e = rp[i] + k;
+                sb.pad[slot] = 0;
                 sb.col[slot] = ci[e] + col_off;
                 sb.val[slot] = va != nullptr ? va[e] : 0.0;
                 if (sb.with_src) sb.src[slot] = src_of != nullptr ? src_of[e] + src_off : -1;
@@ -148,6 +183,7 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
     tail64_ = nullptr;
     tail_n32_ = tail_n64_ = tail_grid32_ = tail_grid64_ = 0;
     tail_bar_ = nullptr;
+    bcg_ = nullptr;
     n_sys_ = static_cast<int>(systems.size());
     if (n_sys_ == 0) fail(1, "engine: no systems");
     if (sweeps < 0) fail(1, "engine: negative smoothing sweeps");
@@ -297,7 +333,15 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         const int* dslice = arena_.upload(sb.slice, st);
         const int* dcol = arena_.upload(sb.col, st);
         d.a.s64 = {dslice, dcol, arena_.alloc<double>(d.a.slots), kFmtSell};
-        if (need32_) d.a.s32 = {dslice, dcol, arena_.alloc<float>(d.a.slots), kFmtSell};
+        if (need32_) {
+            d.a.s32 = {dslice, dcol, arena_.alloc<float>(d.a.slots), kFmtSell};
+            std::vector<uint16_t> c16;
+            std::vector<int> cbase;
+            if (tuning_.col16 && compress_cols(sb.slice, sb.col, &sb.pad, c16, cbase)) {
+                d.a.s32.c16 = arena_.upload(c16, st);
+                d.a.s32.cbase = arena_.upload(cbase, st);
+            }
+        }
         long long nnz0 = 0;
         for (int s = 0; s < n_sys_; ++s) nnz0 += systems[s].rp[systems[s].n];
         d.a.nnz = nnz0;
@@ -359,10 +403,19 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
                 // slack for the aligned quad loads of the last row
                 cbd.col.insert(cbd.col.end(), 4, 0);
                 cbd.val.insert(cbd.val.end(), 4, 0.0);
+                std::vector<uint16_t> c16;
+                std::vector<int> cbase;
+                const bool packed = need32_ && tuning_.col16 && compress_cols(cbd.rp, cbd.col, nullptr, c16, cbase);
                 const int* dp = arena_.upload(cbd.rp, st);
-                const int* dc = arena_.upload(cbd.col, st);
+                const int* dc = (need64_ || !packed) ? arena_.upload(cbd.col, st) : nullptr;
                 if (need64_) m.s64 = {dp, dc, arena_.upload(cbd.val, st), lanes};
-                if (need32_) m.s32 = {dp, dc, arena_.upload(to_float(cbd.val), st), lanes};
+                if (need32_) {
+                    m.s32 = {dp, dc, arena_.upload(to_float(cbd.val), st), lanes};
+                    if (packed) {
+                        m.s32.c16 = arena_.upload(c16, st);
+                        m.s32.cbase = arena_.upload(cbase, st);
+                    }
+                }
                 op_tiles(m, lanes, row_level, [&](int s) { return L[s] - 1 > l; }, [](int) { return true; });
             } else {
                 SellBuild sb;
@@ -377,11 +430,20 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
                 }
                 m.n_slices = static_cast<int>(sb.slice.size()) - 1;
                 m.slots = sb.slice.back();
+                std::vector<uint16_t> c16;
+                std::vector<int> cbase;
+                const bool packed = need32_ && tuning_.col16 && compress_cols(sb.slice, sb.col, &sb.pad, c16, cbase);
                 const int* dp = arena_.upload(sb.slice, st);
-                const int* dc = arena_.upload(sb.col, st);
+                const int* dc = (need64_ || !packed) ? arena_.upload(sb.col, st) : nullptr;
                 const int* dperm = arena_.upload(sb.perm, st);
                 if (need64_) m.s64 = {dp, dc, arena_.upload(sb.val, st), kFmtSell, dperm};
-                if (need32_) m.s32 = {dp, dc, arena_.upload(to_float(sb.val), st), kFmtSell, dperm};
+                if (need32_) {
+                    m.s32 = {dp, dc, arena_.upload(to_float(sb.val), st), kFmtSell, dperm};
+                    if (packed) {
+                        m.s32.c16 = arena_.upload(c16, st);
+                        m.s32.cbase = arena_.upload(cbase, st);
+                    }
+                }
                 op_tiles(m, kFmtSell, row_level, [&](int s) { return L[s] - 1 > l; }, [](int) { return true; });
             }
             m.nnz = nnz;
@@ -748,7 +810,8 @@ template <class T> void Engine::prepare_tail() {
     auto OP = [&](const DevSell64_32& m) { return vs_sel<T>(m.s64, m.s32); };
     const double sv = sizeof(T);
     auto csr_b = [&](const DevSell64_32& m, double rows, double cols) {
-        return static_cast<double>(m.nnz) * (sv + 4.0) + 4.0 * (rows + 1.0) + sv * cols + sv * rows;
+        const double cb = sizeof(T) == 4 && m.s32.c16 != nullptr ? 2.0 : 4.0;
+        return static_cast<double>(m.nnz) * (sv + cb) + 4.0 * (rows + 1.0) + sv * cols + sv * rows;
     };
     std::vector<TailPhase<T>> ph;
     bytes = 0.0;
@@ -878,7 +941,8 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
     const double sv = sizeof(T);
     const double sb0 = 8.0; // level-0 right-hand side: the FP64 Krylov residual
     auto spmv_b = [&](const DevSell64_32& m, double rows, double cols) {
-        return static_cast<double>(m.nnz) * (sv + 4.0) + 4.0 * (rows + 1.0) + sv * cols + sv * rows;
+        const double cb = sizeof(T) == 4 && m.s32.c16 != nullptr ? 2.0 : 4.0;
+        return static_cast<double>(m.nnz) * (sv + cb) + 4.0 * (rows + 1.0) + sv * cols + sv * rows;
     };
     // tiles of an operator: one row per warp for CSR operators, slice runs for SELL ones
     struct Launch {

@@ -35,6 +35,7 @@ struct Tuning {
     int fuse_first = 0;         // first two smoothing sweeps in one kernel (x1 recomputed)
     int sell_rows = kSellRows;  // rows per CTA of SELL operators (multiple of kSellRows)
     int krylov_pair = 1;        // level-0 Krylov SpMV kernels: two rows per thread per pass
+    int col16 = 1;              // FP32 operators store 16-bit column offsets where they fit
     int tail_rows = 0;          // coarse levels of at most this many rows (and everything below
                                 // them) run as one persistent tail kernel; 0 disables it
 };
@@ -97,6 +98,8 @@ public:
 
     // Runs the solve for all systems on the engine stream; blocks until done.
     std::vector<SolveResult> solve(Mode mode, const std::vector<SolveRequest>& req);
+    // Jacobi-preconditioned BiCGStab on the level-0 operator (single-system plans; bicgstab.cu).
+    SolveResult solve_bicgstab(const SolveRequest& req);
 
     // Launch the pieces of one V-cycle application z = M^-1 r for system-batch inputs that are
     // already in the level-0 residual vector (used by the parity tests).
@@ -206,6 +209,7 @@ private:
     int* diag_src0_ = nullptr;
     double* vs_ = nullptr;
     double* dinv0_ = nullptr;
+    double* bcg_ = nullptr;  // BiCGStab work vectors (allocated on first use)
     // Krylov vectors (level 0)
     double *b_ = nullptr, *x_ = nullptr, *r_ = nullptr, *p_ = nullptr, *q_ = nullptr;
     // state

@@ -47,6 +47,10 @@ template <class T> struct Sell {
     // SELL only: row held at each position (rows sorted by length, longest first, within each
     // aligned window of kSellRows positions, which cuts slice padding); null = identity
     const int* perm = nullptr;
+    // Compressed columns (FP32 copies whose every SELL slice / CSR row spans fewer than 65536
+    // columns): column = cbase[slice or row] + c16[k]; `col` is then unused. Null = int32 `col`.
+    const uint16_t* c16 = nullptr;
+    const int* cbase = nullptr;
 };
 
 struct Tiles {
@@ -185,62 +189,16 @@ template <class T> __device__ __forceinline__ T madd(T s, T a, T b) {
     else return fmaf(a, b, s);
 }
 
-// Row sum of a SELL row: sum_k val[k] * xa(col[k]) in CSR order. Entries are taken in batches
-// of four, software-pipelined: the column / value loads of the next batch are issued before the
-// gathers of the current one, so a thread keeps two batches of the row in flight. Every row of
-// a slice has the slice's width, so the batch predicates are warp-uniform.
-template <class T, class XA>
-__device__ __forceinline__ T sell_row_sum(const Sell<T>& m, int row, XA xa) {
-    const int slice = row >> 5;
-    const int lane = row & 31;
-    int k = __ldg(&m.slice[slice]) + lane;
-    const int end = __ldg(&m.slice[slice + 1]);
-    T s = T(0);
-    if (k >= end) return s;
-    T v[4];
-    int c[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const bool ok = k + 32 * u < end;
-        v[u] = ok ? __ldg(&m.val[k + 32 * u]) : T(0);
-        c[u] = ok ? __ldg(&m.col[k + 32 * u]) : -1;
-    }
-    for (;;) {
-        const int kn = k + 128;
-        const bool more = kn < end;
-        T vn[4];
-        int cn[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const bool ok = more && kn + 32 * u < end;
-            vn[u] = ok ? __ldg(&m.val[kn + 32 * u]) : T(0);
-            cn[u] = ok ? __ldg(&m.col[kn + 32 * u]) : -1;
-        }
-        T xv[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) xv[u] = c[u] >= 0 ? xa(c[u]) : T(0);
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-            if (c[u] >= 0) s = madd<T>(s, v[u], xv[u]);
-        if (!more) break;
-        k = kn;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            v[u] = vn[u];
-            c[u] = cn[u];
-        }
-    }
-    return s;
-}
-
-// Predicated batch of four SELL entries starting at k (column -1 beyond the row end e).
-template <class T>
-__device__ __forceinline__ void sell_load4(const Sell<T>& m, int k, int e, T (&v)[4], int (&c)[4]) {
+// Predicated batch of four SELL entries starting at k (column -1 beyond the row end e); C16:
+// compressed columns (the caller has checked m.c16).
+template <bool C16, class T>
+__device__ __forceinline__ void sell_load4(const Sell<T>& m, int k, int e, int base, T (&v)[4], int (&c)[4]) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
         const bool ok = k + 32 * u < e;
         v[u] = ok ? __ldg(&m.val[k + 32 * u]) : T(0);
-        c[u] = ok ? __ldg(&m.col[k + 32 * u]) : -1;
+        if constexpr (C16) c[u] = ok ? base + static_cast<int>(__ldg(&m.c16[k + 32 * u])) : -1;
+        else c[u] = ok ? __ldg(&m.col[k + 32 * u]) : -1;
     }
 }
 
@@ -254,27 +212,68 @@ __device__ __forceinline__ void sell_acc4(T& s, const T (&v)[4], const int (&c)[
         if (c[u] >= 0) s = madd<T>(s, v[u], xv[u]);
 }
 
+// Row sum of a SELL row: sum_k val[k] * xa(col[k]) in CSR order. Entries are taken in batches
+// of four, software-pipelined: the column / value loads of the next batch are issued before the
+// gathers of the current one, so a thread keeps two batches of the row in flight. Every row of
+// a slice has the slice's width, so the batch predicates are warp-uniform.
+template <bool C16, class T, class XA>
+__device__ __forceinline__ T sell_row_sum_c(const Sell<T>& m, int row, XA xa) {
+    const int slice = row >> 5;
+    const int lane = row & 31;
+    int k = __ldg(&m.slice[slice]) + lane;
+    const int end = __ldg(&m.slice[slice + 1]);
+    const int base = C16 ? __ldg(&m.cbase[slice]) : 0;
+    T s = T(0);
+    if (k >= end) return s;
+    T v[4];
+    int c[4];
+    sell_load4<C16>(m, k, end, base, v, c);
+    for (;;) {
+        k += 128;
+        T vn[4];
+        int cn[4];
+        sell_load4<C16>(m, k, end, base, vn, cn);
+        sell_acc4(s, v, c, xa);
+        if (k >= end) break;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            v[u] = vn[u];
+            c[u] = cn[u];
+        }
+    }
+    return s;
+}
+
+template <class T, class XA>
+__device__ __forceinline__ T sell_row_sum(const Sell<T>& m, int row, XA xa) {
+    if constexpr (sizeof(T) == 4) {
+        if (m.c16 != nullptr) return sell_row_sum_c<true>(m, row, xa);
+    }
+    return sell_row_sum_c<false>(m, row, xa);
+}
+
 // Two SELL rows of one thread, both software-pipelined as in sell_row_sum (up to four batches
 // in flight per thread); each row is still accumulated in its own CSR order.
-template <class T, class XA>
-__device__ __forceinline__ void sell_row_sum2(const Sell<T>& m, int ra, int rb, XA xa, T& sa, T& sb) {
+template <bool C16, class T, class XA>
+__device__ __forceinline__ void sell_row_sum2_c(const Sell<T>& m, int ra, int rb, XA xa, T& sa, T& sb) {
     int ka = __ldg(&m.slice[ra >> 5]) + (ra & 31);
     const int ea = __ldg(&m.slice[(ra >> 5) + 1]);
     int kb = __ldg(&m.slice[rb >> 5]) + (rb & 31);
     const int eb = __ldg(&m.slice[(rb >> 5) + 1]);
+    const int ba = C16 ? __ldg(&m.cbase[ra >> 5]) : 0, bb = C16 ? __ldg(&m.cbase[rb >> 5]) : 0;
     sa = T(0);
     sb = T(0);
     T va[4], vb[4];
     int ca[4], cb[4];
-    sell_load4(m, ka, ea, va, ca);
-    sell_load4(m, kb, eb, vb, cb);
+    sell_load4<C16>(m, ka, ea, ba, va, ca);
+    sell_load4<C16>(m, kb, eb, bb, vb, cb);
     for (;;) {
         ka += 128;
         kb += 128;
         T van[4], vbn[4];
         int can[4], cbn[4];
-        sell_load4(m, ka, ea, van, can);
-        sell_load4(m, kb, eb, vbn, cbn);
+        sell_load4<C16>(m, ka, ea, ba, van, can);
+        sell_load4<C16>(m, kb, eb, bb, vbn, cbn);
         sell_acc4(sa, va, ca, xa);
         sell_acc4(sb, vb, cb, xa);
         if (ka >= ea && kb >= eb) break;
@@ -286,6 +285,17 @@ __device__ __forceinline__ void sell_row_sum2(const Sell<T>& m, int ra, int rb, 
             cb[u] = cbn[u];
         }
     }
+}
+
+template <class T, class XA>
+__device__ __forceinline__ void sell_row_sum2(const Sell<T>& m, int ra, int rb, XA xa, T& sa, T& sb) {
+    if constexpr (sizeof(T) == 4) {
+        if (m.c16 != nullptr) {
+            sell_row_sum2_c<true>(m, ra, rb, xa, sa, sb);
+            return;
+        }
+    }
+    sell_row_sum2_c<false>(m, ra, rb, xa, sa, sb);
 }
 
 template <class T, class X>
@@ -310,6 +320,25 @@ __device__ __forceinline__ void ld4(const double* p, double (&v)[4]) {
     v[3] = b.y;
 }
 
+// Four consecutive CSR columns at an aligned index k into c[o..o+3] (8-byte loads when
+// compressed, 16-byte otherwise).
+template <class T>
+__device__ __forceinline__ void ld4col(const Sell<T>& m, int k, int base, int (&c)[8], int o) {
+    if (sizeof(T) == 4 && m.c16 != nullptr) {
+        const uint2 q = __ldg(reinterpret_cast<const uint2*>(m.c16 + k));
+        c[o] = base + static_cast<int>(q.x & 0xffffu);
+        c[o + 1] = base + static_cast<int>(q.x >> 16);
+        c[o + 2] = base + static_cast<int>(q.y & 0xffffu);
+        c[o + 3] = base + static_cast<int>(q.y >> 16);
+    } else {
+        const int4 q = __ldg(reinterpret_cast<const int4*>(m.col + k));
+        c[o] = q.x;
+        c[o + 1] = q.y;
+        c[o + 2] = q.z;
+        c[o + 3] = q.w;
+    }
+}
+
 // Partial CSR row sum of one lane. The row is read in aligned quads (16-byte vector loads of
 // columns and values): lane `sub` takes quads sub, sub + G, ... of the row's aligned span, two
 // quads per pass, and masks the entries outside [row begin, row end). CSR arrays carry four
@@ -318,6 +347,7 @@ template <class T, class XA>
 __device__ __forceinline__ T csr_lane_sum(const Sell<T>& m, int row, int sub, int G, XA xa) {
     const int b = __ldg(&m.slice[row]);
     const int e = __ldg(&m.slice[row + 1]);
+    const int base = sizeof(T) == 4 && m.c16 != nullptr ? __ldg(&m.cbase[row]) : 0;
     T s = T(0);
     for (int k = (b & ~3) + 4 * sub; k < e; k += 8 * G) {
         const int k2 = k + 4 * G;
@@ -325,22 +355,14 @@ __device__ __forceinline__ T csr_lane_sum(const Sell<T>& m, int row, int sub, in
         int c[8];
         T v[8], xv[8];
         {
-            const int4 q = __ldg(reinterpret_cast<const int4*>(m.col + k));
-            c[0] = q.x;
-            c[1] = q.y;
-            c[2] = q.z;
-            c[3] = q.w;
+            ld4col(m, k, base, c, 0);
             T t[4];
             ld4(m.val + k, t);
 #pragma unroll
             for (int u = 0; u < 4; ++u) v[u] = t[u];
         }
         if (two) {
-            const int4 q = __ldg(reinterpret_cast<const int4*>(m.col + k2));
-            c[4] = q.x;
-            c[5] = q.y;
-            c[6] = q.z;
-            c[7] = q.w;
+            ld4col(m, k2, base, c, 4);
             T t[4];
             ld4(m.val + k2, t);
 #pragma unroll
@@ -434,6 +456,11 @@ __device__ __forceinline__ void visit_rows_v(const Sell<T>& m, int r0, int r1, X
         }
     }
 }
+
+// CTAs per SM the V-cycle kernels are compiled for: the one-row SELL sweeps fit in 32
+// registers (full occupancy); the lane-group and two-row kernels hold more (FP64 most).
+template <class T, int V>
+constexpr int kMinBlocks = V == kVisitSell1 ? 8 : (sizeof(T) == 8 || V == kVisitSell2 ? 4 : 6);
 
 // Strategy of an operator's V-cycle kernels.
 __host__ __device__ inline int visit_of(int fmt) {
@@ -561,7 +588,7 @@ struct X1Out {
 // First smoothing step from x = 0: x1 = 0 + wd * b (t = A*0 = 0), and when fused2 also the
 // second sweep y = x1 + wd (b - A x1) with x1 of the neighbours recomputed on the fly.
 template <class T, class B, int V>
-static __global__ void __launch_bounds__(kBlock) k_vc_first(Sell<T> a, Tiles tiles, const SysState* st,
+static __global__ void __launch_bounds__(kBlock, (kMinBlocks<T, V>)) k_vc_first(Sell<T> a, Tiles tiles, const SysState* st,
                                                      const T* __restrict__ wd,
                                                      const B* __restrict__ b, T* __restrict__ y,
                                                      int fused2) {
@@ -582,7 +609,7 @@ static __global__ void __launch_bounds__(kBlock) k_vc_first(Sell<T> a, Tiles til
 
 // y = x + wd (b - A x)
 template <class T, class B, int V>
-static __global__ void __launch_bounds__(kBlock) k_vc_jacobi(Sell<T> a, Tiles tiles, const SysState* st,
+static __global__ void __launch_bounds__(kBlock, (kMinBlocks<T, V>)) k_vc_jacobi(Sell<T> a, Tiles tiles, const SysState* st,
                                                       const T* __restrict__ wd,
                                                       const B* __restrict__ b,
                                                       const T* __restrict__ x, T* __restrict__ y) {
@@ -595,7 +622,7 @@ static __global__ void __launch_bounds__(kBlock) k_vc_jacobi(Sell<T> a, Tiles ti
 
 // t = b - A x
 template <class T, class B, int V>
-static __global__ void __launch_bounds__(kBlock) k_vc_residual(Sell<T> a, Tiles tiles, const SysState* st,
+static __global__ void __launch_bounds__(kBlock, (kMinBlocks<T, V>)) k_vc_residual(Sell<T> a, Tiles tiles, const SysState* st,
                                                         const B* __restrict__ b,
                                                         const T* __restrict__ x,
                                                         T* __restrict__ t) {
@@ -609,7 +636,7 @@ static __global__ void __launch_bounds__(kBlock) k_vc_residual(Sell<T> a, Tiles 
 
 // y = M x (restriction into the next level's right-hand side)
 template <class T, int V>
-static __global__ void __launch_bounds__(kBlock) k_vc_spmv(Sell<T> m, Tiles tiles, const SysState* st,
+static __global__ void __launch_bounds__(kBlock, (kMinBlocks<T, V>)) k_vc_spmv(Sell<T> m, Tiles tiles, const SysState* st,
                                                     const T* __restrict__ x, T* __restrict__ y,
                                                     const T* __restrict__ wd1, T* __restrict__ x1,
                                                     int n1) {
@@ -624,7 +651,7 @@ static __global__ void __launch_bounds__(kBlock) k_vc_spmv(Sell<T> m, Tiles tile
 
 // x += P xc
 template <class T, int V>
-static __global__ void __launch_bounds__(kBlock) k_vc_prolong(Sell<T> p, Tiles tiles, const SysState* st,
+static __global__ void __launch_bounds__(kBlock, (kMinBlocks<T, V>)) k_vc_prolong(Sell<T> p, Tiles tiles, const SysState* st,
                                                        const T* __restrict__ xc,
                                                        T* __restrict__ x) {
     TileCtx c;

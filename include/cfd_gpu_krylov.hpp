@@ -8,8 +8,7 @@
 // Errors are thrown as the reference throws them: std::invalid_argument for bad arguments
 // (krylov.hpp callers rely on it for an empty hierarchy, device_solver.cpp:89) and
 // std::runtime_error("CUDA ...") for device failures (krylov_cuda.cu:18-22).
-// Not provided: solve_host / solve_amg_cg_host (the reference's host-thread path) and
-// Method::BiCgStab (the momentum solver; rejected with std::invalid_argument).
+// Not provided: solve_host / solve_amg_cg_host (the reference's host-thread path).
 #pragma once
 
 #include <memory>
@@ -44,7 +43,7 @@ struct SolveStats {
     bool on_device = false;
 };
 
-// krylov.hpp:37-38: Jacobi-preconditioned CG on a host CSR matrix, on the GPU.
+// krylov.hpp:37-38: Jacobi-preconditioned CG or BiCGStab on a host CSR matrix, on the GPU.
 SolveStats solve(const CsrView& a, const double* b, double* x, Method method,
                  const SolveControl& control);
 

@@ -17,7 +17,7 @@ def test_coordinate_search_finds_separable_minimum():
                    for k, v in target.items())
 
     best, val, trace = coordinate_search(cost)
-    assert dataclasses.asdict(best) == target
+    assert {k: v for k, v in dataclasses.asdict(best).items() if k in target} == target
     assert val == min(v for _, v in trace)
     assert len(calls) == len(set(calls))          # memoised
     assert trace[0][0] == dataclasses.asdict(Tuning())

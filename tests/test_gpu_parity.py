@@ -212,3 +212,27 @@ def test_persistent_tail_matches_separate_kernels(gpu, precision):
         out.append((x, st.iterations, z))
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][2], out[1][2])
+
+
+@pytest.mark.parametrize("make", [lambda: W.cavity(8), lambda: W.tet(5)], ids=["cavity8", "tet5"])
+def test_bicgstab_matches_oracle(gpu, make):
+    """Jacobi-preconditioned BiCGStab (krylov_kernels.inc:97-169): one-shot on a CSR matrix and
+    through the persistent system, iterations within 2 of the oracle, tolerance met."""
+    cb = gpu
+    case = make()
+    up, lo, diag, src = _assembled(case)
+    pat = O.build_pattern(case.n, case.owner, case.neighbour)
+    a = O.ldu_to_csr(pat, diag, up, lo)
+    tol = 1e-10 * np.linalg.norm(src)
+    xo, so = O.krylov(a, src, method=1, abs_tol=tol, max_iterations=5000)
+    assert so["converged"]
+    x = np.zeros(case.n)
+    st = cb.solve(cb.CsrView(a.n_rows, a.rp, a.ci, a.va), src, x, cb.Method.BiCgStab,
+                  cb.SolveControl(tol, 5000))
+    assert st.converged and abs(st.iterations - so["iterations"]) <= 2
+    assert np.linalg.norm(src - a.matvec(x)) <= 1.05 * tol
+    ds = cb.DeviceSolver(_pattern(cb, pat))
+    x2 = np.zeros(case.n)
+    st2 = ds.solve(diag, up, lo, src, x2, cb.Method.BiCgStab, False, cb.SolveControl(tol, 5000))
+    assert st2.converged and abs(st2.iterations - so["iterations"]) <= 2
+    assert np.linalg.norm(src - a.matvec(x2)) <= 1.05 * tol

@@ -79,10 +79,10 @@ HostCsr spgemm(const HostCsr& a, const HostCsr& b) {
     const int n = a.n_rows, m = b.n_cols;
     c.rp.assign(static_cast<size_t>(n) + 1, 0);
     std::vector<int> len(static_cast<size_t>(n), 0);
-#pragma omp parallel if (n > 20000)
+#pragma omp parallel if (n > 256)
     {
         std::vector<int> mark(static_cast<size_t>(std::max(m, 1)), -1);
-#pragma omp for schedule(dynamic, 512)
+#pragma omp for schedule(dynamic, 64)
         for (int i = 0; i < n; ++i) {
             int cnt = 0;
             for (int ka = a.rp[i]; ka < a.rp[i + 1]; ++ka) {
@@ -107,12 +107,12 @@ HostCsr spgemm(const HostCsr& a, const HostCsr& b) {
     for (int i = 0; i < n; ++i) c.rp[i + 1] = c.rp[i] + len[i];
     c.ci.resize(static_cast<size_t>(c.rp[n]));
     c.va.resize(static_cast<size_t>(c.rp[n]));
-#pragma omp parallel if (n > 20000)
+#pragma omp parallel if (n > 256)
     {
         std::vector<int> mark(static_cast<size_t>(std::max(m, 1)), -1);
         std::vector<double> acc(static_cast<size_t>(std::max(m, 1)));
         std::vector<int> list;
-#pragma omp for schedule(dynamic, 512)
+#pragma omp for schedule(dynamic, 64)
         for (int i = 0; i < n; ++i) {
             list.clear();
             for (int ka = a.rp[i]; ka < a.rp[i + 1]; ++ka) {
@@ -160,22 +160,55 @@ void prune_zeros(HostCsr& m) {
     m.va.resize(static_cast<size_t>(nnz));
 }
 
+// Rows of the transpose list their columns in ascending order (the order of the serial
+// fill), built in parallel: each thread takes a contiguous block of rows of `a`, and the
+// entries of its block follow those of the blocks before it in every output row.
 HostCsr transpose(const HostCsr& a) {
     HostCsr t;
     t.n_rows = a.n_cols;
     t.n_cols = a.n_rows;
-    t.rp.assign(static_cast<size_t>(t.n_rows) + 1, 0);
-    for (int k = 0; k < a.nnz(); ++k) ++t.rp[a.ci[k] + 1];
-    for (int j = 0; j < t.n_rows; ++j) t.rp[j + 1] += t.rp[j];
+    const int m = a.n_cols;
+    t.rp.assign(static_cast<size_t>(m) + 1, 0);
     t.ci.resize(static_cast<size_t>(a.nnz()));
     t.va.resize(static_cast<size_t>(a.nnz()));
-    std::vector<int> fill(t.rp.begin(), t.rp.end() - 1);
-    for (int i = 0; i < a.n_rows; ++i) {
-        for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) {
-            const int j = a.ci[k];
-            t.ci[fill[j]] = i;
-            t.va[fill[j]] = a.va[k];
-            ++fill[j];
+    const int nt = a.n_rows > 4096 ? omp_get_max_threads() : 1;
+    std::vector<std::vector<int>> cnt(static_cast<size_t>(nt));
+    auto block = [&](int tid, int& r0, int& r1) {
+        const long long n = a.n_rows;
+        r0 = static_cast<int>(n * tid / nt);
+        r1 = static_cast<int>(n * (tid + 1) / nt);
+    };
+#pragma omp parallel num_threads(nt) if (nt > 1)
+    {
+        const int tid = omp_get_thread_num();
+        int r0, r1;
+        block(tid, r0, r1);
+        std::vector<int>& c = cnt[static_cast<size_t>(tid)];
+        c.assign(static_cast<size_t>(m), 0);
+        for (int i = r0; i < r1; ++i)
+            for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) ++c[a.ci[k]];
+#pragma omp barrier
+#pragma omp single
+        {
+            // row lengths, then each thread's starting offset within every row
+            for (int j = 0; j < m; ++j) {
+                int len = 0;
+                for (int q = 0; q < nt; ++q) {
+                    const int v = cnt[static_cast<size_t>(q)][j];
+                    cnt[static_cast<size_t>(q)][j] = len;
+                    len += v;
+                }
+                t.rp[j + 1] = len;
+            }
+            for (int j = 0; j < m; ++j) t.rp[j + 1] += t.rp[j];
+        }
+        for (int i = r0; i < r1; ++i) {
+            for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) {
+                const int j = a.ci[k];
+                const int o = t.rp[j] + c[j]++;
+                t.ci[o] = i;
+                t.va[o] = a.va[k];
+            }
         }
     }
     return t;
@@ -375,7 +408,7 @@ Hierarchy amg_setup(const HostCsr& a0, const AmgSettings& s) {
         std::vector<double> inv(static_cast<size_t>(nl));
         for (int i = 0; i < nl; ++i) inv[i] = d[i] != 0.0 ? 1.0 / d[i] : 0.0;
         double rho = 0.0;
-#pragma omp parallel for reduction(max : rho) schedule(static) if (nl > 100000)
+#pragma omp parallel for reduction(max : rho) schedule(static) if (nl > 2048)
         for (int i = 0; i < nl; ++i) {
             double row = 0.0;
             for (int k = cur.rp[i]; k < cur.rp[i + 1]; ++k) row += std::fabs(cur.va[k]);
@@ -396,7 +429,7 @@ Hierarchy amg_setup(const HostCsr& a0, const AmgSettings& s) {
         pv_t.resize(static_cast<size_t>(nthreads));
         std::vector<int> row_start(static_cast<size_t>(nl));
         std::vector<int> row_tid(static_cast<size_t>(nl));
-#pragma omp parallel if (nl > 20000)
+#pragma omp parallel if (nl > 2048)
         {
             const int tid = omp_get_thread_num();
             std::vector<int> mark(static_cast<size_t>(n_agg), -1);
@@ -452,7 +485,7 @@ Hierarchy amg_setup(const HostCsr& a0, const AmgSettings& s) {
         p.ci.resize(static_cast<size_t>(p.rp[nl]));
         p.va.resize(static_cast<size_t>(p.rp[nl]));
         // gather the per-thread row buffers back in row order
-#pragma omp parallel for schedule(static) if (nl > 20000)
+#pragma omp parallel for schedule(static) if (nl > 2048)
         for (int i = 0; i < nl; ++i) {
             const int src = row_start[i];
             const int t = row_tid[i];

@@ -686,7 +686,7 @@ class Tuning:
     sell_rows: int = 256
     krylov_pair: int = 1
     tail_rows: int = 0
-    col16: int = 1
+    col16: int = 0
 
     def _c(self):
         return TuningStruct(int(self.target_tiles), int(self.wide_row), int(self.lanes_div),

@@ -59,6 +59,7 @@ bool compress_cols(const std::vector<int>& ptr, const std::vector<int>& col, con
 // Appends rows [0, n_rows) of a CSR block (n_pad >= n_rows, multiple of 32) whose first row has
 // global index row0. Column indices are shifted by col_off; padding slots read column pad_col
 // with value 0. src_of (optional): value-source index per CSR entry (shifted by src_off).
+// Slices are laid out serially (a prefix sum of their widths) and filled in parallel.
 void sell_append(SellBuild& sb, int n_rows, int n_pad, const int* rp, const int* ci,
                  const double* va, const int* src_of, int col_off, int src_off, int pad_col) {
     // order[q]: block row at block position q (identity unless sorting)
@@ -66,29 +67,45 @@ void sell_append(SellBuild& sb, int n_rows, int n_pad, const int* rp, const int*
     std::iota(order.begin(), order.end(), 0);
     auto len_of = [&](int i) { return i < n_rows ? rp[i + 1] - rp[i] : -1; };
     if (sb.sort) {
+#pragma omp parallel for schedule(dynamic, 16) if (n_pad > 65536)
         for (int w0 = 0; w0 < n_pad; w0 += kSellRows) {
             const int w1 = std::min(n_pad, w0 + kSellRows);
             std::stable_sort(order.begin() + w0, order.begin() + w1,
                              [&](int a, int b) { return len_of(a) > len_of(b); });
         }
         const int row0 = static_cast<int>(sb.perm.size());
-        for (int q = 0; q < n_pad; ++q) sb.perm.push_back(row0 + order[q]);
+        sb.perm.resize(static_cast<size_t>(row0) + n_pad);
+        for (int q = 0; q < n_pad; ++q) sb.perm[static_cast<size_t>(row0) + q] = row0 + order[q];
     }
-    for (int s0 = 0; s0 < n_pad; s0 += 32) {
-        int width = 0;
-        for (int q = s0; q < s0 + 32; ++q) width = std::max(width, len_of(order[q]));
-        const int base = sb.slice.back();
-        const size_t slots = static_cast<size_t>(width) * 32;
-        sb.col.resize(base + slots, pad_col);
-        sb.val.resize(base + slots, 0.0);
-        sb.pad.resize(base + slots, 1);
-        if (sb.with_src) sb.src.resize(base + slots, -1);
+    const int n_sl = n_pad / 32;
+    std::vector<long long> start(static_cast<size_t>(n_sl) + 1, 0);
+    const long long base0 = sb.slice.back();
+    start[0] = base0;
+    {
+        std::vector<int> width(static_cast<size_t>(n_sl), 0);
+#pragma omp parallel for schedule(static) if (n_sl > 4096)
+        for (int sl = 0; sl < n_sl; ++sl) {
+            int w = 0;
+            for (int q = sl * 32; q < sl * 32 + 32; ++q) w = std::max(w, len_of(order[q]));
+            width[sl] = w;
+        }
+        for (int sl = 0; sl < n_sl; ++sl) start[sl + 1] = start[sl] + 32LL * width[sl];
+    }
+    const long long total = start[n_sl];
+    if (total > INT_MAX) fail(1, "operator too large for 32-bit slot offsets");
+    sb.col.resize(static_cast<size_t>(total), pad_col);
+    sb.val.resize(static_cast<size_t>(total), 0.0);
+    sb.pad.resize(static_cast<size_t>(total), 1);
+    if (sb.with_src) sb.src.resize(static_cast<size_t>(total), -1);
+#pragma omp parallel for schedule(static) if (n_sl > 4096)
+    for (int sl = 0; sl < n_sl; ++sl) {
+        const long long base = start[sl];
         for (int lane = 0; lane < 32; ++lane) {
-            const int i = order[s0 + lane];
+            const int i = order[sl * 32 + lane];
             if (i >= n_rows) continue;
             const int len = rp[i + 1] - rp[i];
             for (int k = 0; k < len; ++k) {
-                const size_t slot = base + static_cast<size_t>(k) * 32 + lane;
+                const size_t slot = static_cast<size_t>(base + static_cast<long long>(k) * 32 + lane);
                 const int e = rp[i] + k;
                 sb.pad[slot] = 0;
                 sb.col[slot] = ci[e] + col_off;
@@ -96,11 +113,10 @@ void sell_append(SellBuild& sb, int n_rows, int n_pad, const int* rp, const int*
                 if (sb.with_src) sb.src[slot] = src_of != nullptr ? src_of[e] + src_off : -1;
             }
         }
-        if (static_cast<long long>(base) + static_cast<long long>(slots) > INT_MAX) {
-            fail(1, "operator too large for 32-bit slot offsets");
-        }
-        sb.slice.push_back(base + static_cast<int>(slots));
     }
+    const size_t s0 = sb.slice.size();
+    sb.slice.resize(s0 + n_sl);
+    for (int sl = 0; sl < n_sl; ++sl) sb.slice[s0 + sl] = static_cast<int>(start[sl + 1]);
 }
 
 // CSR under construction on the host (global rows of a level; padding rows are empty).
@@ -111,27 +127,37 @@ struct CsrBuild {
 };
 
 void csr_append(CsrBuild& cb, int n_rows, int n_pad, const int* rp, const int* ci, const double* va, int col_off) {
+    const long long base = static_cast<long long>(cb.col.size());
+    const long long nnz = n_rows > 0 ? rp[n_rows] - rp[0] : 0;
+    if (base + nnz > INT_MAX) fail(1, "operator too large for 32-bit offsets");
+    cb.col.resize(static_cast<size_t>(base + nnz));
+    cb.val.resize(static_cast<size_t>(base + nnz));
+    const size_t r0 = cb.rp.size();
+    cb.rp.resize(r0 + n_pad);
+#pragma omp parallel for schedule(static) if (n_rows > 16384)
     for (int i = 0; i < n_pad; ++i) {
         if (i < n_rows) {
+            const long long o = base + rp[i] - rp[0];
             for (int k = rp[i]; k < rp[i + 1]; ++k) {
-                cb.col.push_back(ci[k] + col_off);
-                cb.val.push_back(va[k]);
+                cb.col[static_cast<size_t>(o + k - rp[i])] = ci[k] + col_off;
+                cb.val[static_cast<size_t>(o + k - rp[i])] = va[k];
             }
         }
-        if (cb.col.size() > static_cast<size_t>(INT_MAX)) fail(1, "operator too large for 32-bit offsets");
-        cb.rp.push_back(static_cast<int>(cb.col.size()));
+        cb.rp[r0 + i] = static_cast<int>(base + (i < n_rows ? rp[i + 1] - rp[0] : nnz));
     }
 }
 
 std::vector<float> to_float(const std::vector<double>& v) {
     std::vector<float> f(v.size());
-    for (size_t i = 0; i < v.size(); ++i) f[i] = static_cast<float>(v[i]);
+#pragma omp parallel for schedule(static) if (v.size() > (1u << 20))
+    for (long long i = 0; i < static_cast<long long>(v.size()); ++i) f[i] = static_cast<float>(v[i]);
     return f;
 }
 
 // krylov_openmp.cpp:147-157 / krylov_cuda.cu:345-352: last nonzero diagonal entry, default 1.
 std::vector<double> inverse_diagonal(const HostCsr& a) {
     std::vector<double> d(static_cast<size_t>(a.n_rows), 1.0);
+#pragma omp parallel for schedule(static) if (a.n_rows > 65536)
     for (int i = 0; i < a.n_rows; ++i)
         for (int k = a.rp[i]; k < a.rp[i + 1]; ++k)
             if (a.ci[k] == i && a.va[k] != 0.0) d[i] = 1.0 / a.va[k];

@@ -35,7 +35,7 @@ struct Tuning {
     int fuse_first = 0;         // first two smoothing sweeps in one kernel (x1 recomputed)
     int sell_rows = kSellRows;  // rows per CTA of SELL operators (multiple of kSellRows)
     int krylov_pair = 1;        // level-0 Krylov SpMV kernels: two rows per thread per pass
-    int col16 = 1;              // FP32 operators store 16-bit column offsets where they fit
+    int col16 = 0;              // FP32 operators store 16-bit column offsets where they fit
     int tail_rows = 0;          // coarse levels of at most this many rows (and everything below
                                 // them) run as one persistent tail kernel; 0 disables it
 };

@@ -252,7 +252,7 @@ typedef struct {
     int tail_rows;    /* coarse levels of at most this many rows, with all coarser ones, run as one
                          persistent kernel; 0 (default) disables it */
     int col16;        /* FP32 operators keep 16-bit column offsets from a per-slice / per-row base
-                         where every slice / row spans fewer than 65536 columns, default 1 */
+                         where every slice / row spans fewer than 65536 columns, default 0 */
 } cfdb_tuning;
 void cfdb_default_tuning(cfdb_tuning* t);
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t);

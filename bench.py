@@ -269,7 +269,11 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
                     dg=torch.empty(n, dtype=torch.float64, device=dev),
                     src=torch.empty(n, dtype=torch.float64, device=dev),
                     x=torch.zeros(n, dtype=torch.float64, device=dev)) for k in solvers}
-    setup_s = {}
+    # the hierarchy is built twice: on the host from host copies of the coefficients (the
+    # reference's AmgPreconditioner::setup structure), then on the device from the device
+    # arrays (the product path; bit-identical result, which stays installed). Device setup is
+    # timed on its second run (the first includes loading the setup kernels).
+    setup_s, setup_dev_s, setup_prof = {}, {}, {}
     for k, ds in solvers.items():
         b = bufs[k]
         ds.assemble_pressure_device(flux, gamma, delta, src0, b["up"], b["lo"], b["dg"], b["src"])
@@ -278,6 +282,12 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
         ds.setup_amg(b["dg"].cpu().numpy(), b["up"].cpu().numpy(), b["lo"].cpu().numpy(),
                      cb.AmgSettings(strength_threshold=THETA))
         setup_s[k] = time.perf_counter() - t0
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ds.setup_amg(b["dg"], b["up"], b["lo"], cb.AmgSettings(strength_threshold=THETA), device=True)
+            setup_dev_s[k] = time.perf_counter() - t0
+        setup_prof[k] = ds.setup_profile()
     bnorm_ref = float(torch.linalg.norm(bufs["mixed"]["src"]).item())
     tol = 1e-8 * bnorm_ref
 
@@ -366,6 +376,8 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
             "solve_bytes": by, "hbm_gbs_solve": by / 1e9 / (ms_solve / 1e3),
             "kernel_ms_per_solve": ms_k,
             "setup_s_host": setup_s[k],
+            "setup_s_device": setup_dev_s[k],
+            "setup_phases_device": setup_prof[k],
             "device_bytes": solvers[k].device_bytes(),
         }
     by, ms_k, top, shares = summarise(prof["mixed"], results["mixed"]["iterations"])
@@ -401,6 +413,8 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
         # the reference rebuilds the hierarchy every 20 solves (ldu_matrix.cpp:314): per-solve
         # time with that host setup amortised in, for context (not the headline)
         "ms_per_solve_with_rebuild_every_20": {
+            k: out_prec[k]["ms_per_solve"] + 1e3 * out_prec[k]["setup_s_device"] / 20.0 for k in out_prec},
+        "ms_per_solve_with_host_rebuild_every_20": {
             k: out_prec[k]["ms_per_solve"] + 1e3 * out_prec[k]["setup_s_host"] / 20.0 for k in out_prec},
         "hbm_gbs": out_prec["mixed"]["hbm_gbs_solve"],
         "roofline": roofline, "clocks": results["mixed"]["clocks"],

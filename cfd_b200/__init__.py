@@ -68,7 +68,7 @@ class KernelRecordStruct(C.Structure):
 
 class AmgSettingsStruct(C.Structure):
     _fields_ = [("strength_threshold", _d), ("max_levels", _i), ("coarse_size", _i),
-                ("smooth_sweeps", _i), ("jacobi_weight", _d)]
+                ("smooth_sweeps", _i), ("jacobi_weight", _d), ("device_table_limit", _i)]
 
 
 def _proto(name, args, res=_i):
@@ -92,6 +92,7 @@ _proto("cfdb_build_pattern", [_i, _i, _pi, _pi, _pi, _pi, _pi, _pi, _pi, _pi])
 _proto("cfdb_solve_device_noalloc", [_P(CsrStruct), _vp, _vp, _i, _P(ControlStruct),
                                      _P(StatsStruct)])
 _proto("cfdb_amg_setup", [_P(CsrStruct), _P(AmgSettingsStruct), _P(_vp)])
+_proto("cfdb_amg_setup_device", [_P(CsrStruct), _P(AmgSettingsStruct), _P(_vp)])
 _proto("cfdb_hierarchy_destroy", [_vp])
 _proto("cfdb_hierarchy_levels", [_vp, _pi])
 _proto("cfdb_hierarchy_level", [_vp, _i, _i, _pi, _pi, _P(CsrStruct)])
@@ -105,6 +106,8 @@ _proto("cfdb_system_destroy", [_vp])
 _proto("cfdb_system_on_device", [_vp])
 _proto("cfdb_system_set_amg", [_vp, _P(AmgViewStruct)])
 _proto("cfdb_system_setup_amg", [_vp, _pd, _pd, _pd, _P(AmgSettingsStruct)])
+_proto("cfdb_system_setup_amg_device", [_vp, _vp, _vp, _vp, _P(AmgSettingsStruct), _i])
+_proto("cfdb_system_setup_profile", [_vp, C.c_char_p, C.c_size_t])
 _proto("cfdb_system_set_precision", [_vp, _i])
 _proto("cfdb_system_solve", [_vp, _pd, _pd, _pd, _pd, _pd, _i, _i, _P(ControlStruct),
                              _P(StatsStruct)])
@@ -468,21 +471,25 @@ class AmgSettings:
     coarse_size: int = 400
     smooth_sweeps: int = 2
     jacobi_weight: float = 0.7
+    # device setup only: rows longer than this use device-memory tables (0: the default 6144)
+    device_table_limit: int = 0
 
     def _c(self):
         return AmgSettingsStruct(float(self.strength_threshold), int(self.max_levels),
                                  int(self.coarse_size), int(self.smooth_sweeps),
-                                 float(self.jacobi_weight))
+                                 float(self.jacobi_weight), int(self.device_table_limit))
 
 
 class AmgHierarchy:
-    """Smoothed-aggregation hierarchy built on the host by the library (amg.cpp:122-190)."""
+    """Smoothed-aggregation hierarchy (amg.cpp:122-190) built by the library, on the host or
+    (device=True) with the sparse algebra on the GPU; both builds are bit-identical."""
 
-    def __init__(self, a: CsrView, settings: AmgSettings | None = None):
+    def __init__(self, a: CsrView, settings: AmgSettings | None = None, device: bool = False):
         self.settings = settings or AmgSettings()
         h = _vp()
         cs, ss = a._c(), self.settings._c()
-        _check(_lib.cfdb_amg_setup(C.byref(cs), C.byref(ss), C.byref(h)))
+        fn = _lib.cfdb_amg_setup_device if device else _lib.cfdb_amg_setup
+        _check(fn(C.byref(cs), C.byref(ss), C.byref(h)))
         self._h = h
 
     def __del__(self):
@@ -584,10 +591,36 @@ class DeviceSolver:
         v = amg._c()
         _check(_lib.cfdb_system_set_amg(self._h, C.byref(v)))
 
-    def setup_amg(self, diag, upper, lower, settings: AmgSettings | None = None) -> None:
+    def setup_amg(self, diag, upper, lower, settings: AmgSettings | None = None,
+                  device: bool = False) -> None:
+        """AmgPreconditioner::setup from LDU coefficients and installation of the hierarchy.
+        device=True builds it on the GPU (bit-identical); the coefficients may then also be
+        CUDA tensors (ready on the current stream)."""
         s = (settings or AmgSettings())._c()
-        _check(_lib.cfdb_system_setup_amg(self._h, _dp(_f64(diag)), _dp(_f64(upper)),
-                                          _dp(_f64(lower)), C.byref(s)))
+        if not device:
+            _check(_lib.cfdb_system_setup_amg(self._h, _dp(_f64(diag)), _dp(_f64(upper)),
+                                              _dp(_f64(lower)), C.byref(s)))
+            return
+        if hasattr(diag, "is_cuda") and diag.is_cuda:
+            import torch
+            torch.cuda.current_stream().synchronize()
+            _check(_lib.cfdb_system_setup_amg_device(self._h, _devptr(diag), _devptr(upper),
+                                                     _devptr(lower), C.byref(s), 1))
+            return
+        d, u, lo = _f64(diag), _f64(upper), _f64(lower)
+        _check(_lib.cfdb_system_setup_amg_device(self._h, d.ctypes.data, u.ctypes.data,
+                                                 lo.ctypes.data, C.byref(s), 0))
+
+    def setup_profile(self) -> dict:
+        """Seconds per phase of the last hierarchy setup."""
+        buf = C.create_string_buffer(1024)
+        _check(_lib.cfdb_system_setup_profile(self._h, buf, len(buf)))
+        out = {}
+        for item in buf.value.decode().split(";"):
+            if item:
+                k, v = item.split("=")
+                out[k] = float(v)
+        return out
 
     def set_precision(self, precision: Precision) -> None:
         _check(_lib.cfdb_system_set_precision(self._h, int(precision)))

@@ -8,6 +8,7 @@
 #include <new>
 #include <string>
 
+#include "dsetup.hpp"
 #include "engine.hpp"
 #include "host_algos.hpp"
 
@@ -97,6 +98,32 @@ std::shared_ptr<Hierarchy> hierarchy_from(const cfdb_amg_view& v, int n0, bool s
     return h;
 }
 
+AmgSettings settings_from(const cfdb_amg_settings* settings) {
+    AmgSettings s;
+    if (settings != nullptr) {
+        s.theta = settings->strength_threshold;
+        s.max_levels = settings->max_levels;
+        s.coarse_size = settings->coarse_size;
+        s.sweeps = settings->smooth_sweeps;
+        s.weight = settings->jacobi_weight;
+        s.table_limit = settings->device_table_limit;
+    }
+    if (s.max_levels < 1) fail(CFDB_ERR_BAD_ARG, "max_levels must be >= 1");
+    if (s.table_limit < 0) fail(CFDB_ERR_BAD_ARG, "device_table_limit must be >= 0");
+    return s;
+}
+
+// A non-blocking stream for the duration of one call.
+struct CallStream {
+    cudaStream_t s = nullptr;
+    CallStream() { CFDB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+    ~CallStream() {
+        if (s != nullptr) cudaStreamDestroy(s);
+    }
+    CallStream(const CallStream&) = delete;
+    CallStream& operator=(const CallStream&) = delete;
+};
+
 } // namespace
 
 namespace cfdb {
@@ -126,6 +153,7 @@ struct cfdb_system {
     std::vector<int> owner, neighbour; // kept when created from mesh addressing
     std::unique_ptr<Engine> eng;
     std::shared_ptr<const Hierarchy> h;
+    std::shared_ptr<const DeviceLevels> dl; // device-resident levels of a device setup
     int sweeps = 2;
     double weight = 0.7;
     int precision = CFDB_PRECISION_FP64;
@@ -140,6 +168,14 @@ struct cfdb_system {
     int* d_cf_face = nullptr;
     double* h_asm = nullptr; // device staging of cfdb_system_assemble (host-array variant)
     unsigned long long launches = 0;
+    // device copy of the pattern for the device AMG setup (uploaded on first use)
+    DeviceArena pat_arena;
+    int* d_rp = nullptr;
+    int* d_ci = nullptr;
+    int* d_dpos = nullptr;
+    int* d_upos = nullptr;
+    int* d_lpos = nullptr;
+    std::string setup_profile; // phase times of the last hierarchy setup
 };
 
 namespace {
@@ -168,6 +204,7 @@ void ensure_engine(cfdb_system* s) {
     sp.diag_src = s->diag_src;
     sp.vs_len = s->pat.n + 2 * s->pat.n_faces;
     sp.h = s->h;
+    sp.dl = s->h ? s->dl : nullptr;
     const bool mixed = s->precision == CFDB_PRECISION_MIXED;
     std::vector<SystemSpec> v;
     v.push_back(std::move(sp));
@@ -290,6 +327,7 @@ void cfdb_default_amg_settings(cfdb_amg_settings* s) {
     s->coarse_size = 400;
     s->smooth_sweeps = 2;
     s->jacobi_weight = 0.7;
+    s->device_table_limit = 0;
 }
 
 int cfdb_build_pattern(int n, int n_faces, const int* owner, const int* neighbour, int* row_ptr, int* col,
@@ -517,6 +555,37 @@ int cfdb_amg_setup(const cfdb_csr* a, const cfdb_amg_settings* settings, cfdb_hi
     });
 }
 
+int cfdb_amg_setup_device(const cfdb_csr* a, const cfdb_amg_settings* settings, cfdb_hierarchy** out) {
+    return guarded([&] {
+        require_device();
+        if (a == nullptr || out == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
+        const AmgSettings s = settings_from(settings);
+        const HostCsr m = csr_from(*a, a->n);
+        CallStream cs;
+        DeviceHierarchy dh;
+        DevCsr a0;
+        a0.n_rows = a0.n_cols = m.n_rows;
+        a0.nnz = m.nnz();
+        a0.rp = dh.mem.alloc<int>(m.rp.size());
+        a0.ci = dh.mem.alloc<int>(m.ci.size());
+        a0.va = dh.mem.alloc<double>(m.va.size());
+        CFDB_CUDA(cudaMemcpyAsync(a0.rp, m.rp.data(), sizeof(int) * m.rp.size(), cudaMemcpyHostToDevice, cs.s));
+        if (a0.nnz > 0) {
+            CFDB_CUDA(cudaMemcpyAsync(a0.ci, m.ci.data(), sizeof(int) * m.ci.size(), cudaMemcpyHostToDevice, cs.s));
+            CFDB_CUDA(cudaMemcpyAsync(a0.va, m.va.data(), sizeof(double) * m.va.size(), cudaMemcpyHostToDevice, cs.s));
+        }
+        amg_setup_device(a0, s, cs.s, dh);
+        auto* h = new cfdb_hierarchy;
+        try {
+            h->h = download_hierarchy(dh, /*with_a0=*/true, cs.s);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
 int cfdb_hierarchy_destroy(cfdb_hierarchy* h) {
     delete h;
     return CFDB_OK;
@@ -649,6 +718,7 @@ int cfdb_system_set_amg(cfdb_system* sys, const cfdb_amg_view* amg) {
         if (amg->n_levels <= 0 || amg->levels == nullptr)
             fail(CFDB_ERR_BAD_ARG, "DeviceSolver::set_amg: empty hierarchy");
         sys->h = hierarchy_from(*amg, sys->pat.n, /*skip_a0=*/true);
+        sys->dl.reset();
         sys->sweeps = amg->smooth_sweeps;
         sys->weight = amg->jacobi_weight;
         sys->dirty = true;
@@ -679,7 +749,10 @@ int cfdb_system_setup_amg(cfdb_system* sys, const double* diag, const double* up
             s.sweeps = settings->smooth_sweeps;
             s.weight = settings->jacobi_weight;
         }
+        const double t0 = PhaseTimes::now();
         auto h = std::make_shared<Hierarchy>(amg_setup(a, s));
+        const double t1 = PhaseTimes::now();
+        sys->dl.reset();
         if (h->levels() <= 1) {
             // ldu_matrix.cpp:358: a single-level hierarchy runs Jacobi CG instead of AMG
             sys->h.reset();
@@ -690,7 +763,81 @@ int cfdb_system_setup_amg(cfdb_system* sys, const double* diag, const double* up
         sys->weight = s.weight;
         sys->dirty = true;
         ensure_engine(sys);
+        PhaseTimes pt;
+        pt.add("hierarchy", t1 - t0);
+        pt.add("plan", PhaseTimes::now() - t1);
+        sys->setup_profile = pt.text();
     });
+}
+
+int cfdb_system_setup_amg_device(cfdb_system* sys, const double* diag, const double* upper, const double* lower,
+                                 const cfdb_amg_settings* settings, int device_arrays) {
+    return guarded([&] {
+        if (sys == nullptr || diag == nullptr || (sys->pat.n_faces > 0 && (upper == nullptr || lower == nullptr)))
+            fail(CFDB_ERR_BAD_ARG, "null argument");
+        const double t_in = PhaseTimes::now();
+        const AmgSettings s = settings_from(settings);
+        const LduPatternHost& p = sys->pat;
+        CFDB_CUDA(cudaSetDevice(sys->device));
+        CallStream cs;
+        if (sys->d_rp == nullptr) {
+            sys->d_rp = sys->pat_arena.upload(p.row_ptr, cs.s);
+            sys->d_ci = sys->pat_arena.upload(p.col, cs.s);
+            sys->d_dpos = sys->pat_arena.upload(p.diag_pos, cs.s);
+            sys->d_upos = sys->pat_arena.upload(p.upper_pos, cs.s);
+            sys->d_lpos = sys->pat_arena.upload(p.lower_pos, cs.s);
+        }
+        DeviceHierarchy dh;
+        const double *dd = diag, *du = upper, *dl = lower;
+        if (!device_arrays) {
+            double* ldu = dh.mem.alloc<double>(static_cast<size_t>(p.n) + 2 * static_cast<size_t>(p.n_faces));
+            CFDB_CUDA(cudaMemcpyAsync(ldu, diag, sizeof(double) * p.n, cudaMemcpyHostToDevice, cs.s));
+            if (p.n_faces > 0) {
+                CFDB_CUDA(cudaMemcpyAsync(ldu + p.n, upper, sizeof(double) * p.n_faces, cudaMemcpyHostToDevice, cs.s));
+                CFDB_CUDA(cudaMemcpyAsync(ldu + p.n + p.n_faces, lower, sizeof(double) * p.n_faces,
+                                          cudaMemcpyHostToDevice, cs.s));
+            }
+            dd = ldu;
+            du = ldu + p.n;
+            dl = ldu + p.n + p.n_faces;
+        }
+        DevCsr a0;
+        a0.n_rows = a0.n_cols = p.n;
+        a0.nnz = p.nnz();
+        a0.rp = sys->d_rp;
+        a0.ci = sys->d_ci;
+        a0.va = dh.mem.alloc<double>(static_cast<size_t>(p.nnz()));
+        CFDB_CUDA(cudaMemsetAsync(a0.va, 0, sizeof(double) * p.nnz(), cs.s));
+        ldu_to_csr_values(p.n, p.n_faces, sys->d_dpos, sys->d_upos, sys->d_lpos, dd, du, dl, a0.va, cs.s);
+        const double t0 = PhaseTimes::now();
+        amg_setup_device(a0, s, cs.s, dh);
+        const double t1 = PhaseTimes::now();
+        dh.times.add("input", t0 - t_in);
+        // the plan is laid out on the device from compact copies of the levels, which the
+        // system keeps (plan rebuilds need no host copy)
+        auto kept = keep_levels(dh, cs.s);
+        auto h = std::make_shared<Hierarchy>(hierarchy_shape(dh));
+        const double t2 = PhaseTimes::now();
+        dh.times.add("keep", t2 - t1);
+        if (h->levels() <= 1) {
+            sys->h.reset(); // ldu_matrix.cpp:358: one level runs Jacobi CG
+            sys->dl.reset();
+        } else {
+            sys->h = h;
+            sys->dl = kept;
+        }
+        sys->sweeps = s.sweeps;
+        sys->weight = s.weight;
+        sys->dirty = true;
+        ensure_engine(sys);
+        dh.times.add("plan", PhaseTimes::now() - t2);
+        sys->setup_profile = dh.times.text();
+    });
+}
+
+int cfdb_system_setup_profile(const cfdb_system* sys, char* buf, size_t len) {
+    if (sys == nullptr) return set_error(CFDB_ERR_BAD_ARG, "null system");
+    return copy_str(sys->setup_profile, buf, len);
 }
 
 int cfdb_system_set_precision(cfdb_system* sys, int precision) {
@@ -904,7 +1051,8 @@ int cfdb_system_stream(const cfdb_system* sys, void** stream) {
 
 int cfdb_system_device_bytes(const cfdb_system* sys, size_t* bytes) {
     if (sys == nullptr || bytes == nullptr) return set_error(CFDB_ERR_BAD_ARG, "null argument");
-    *bytes = (sys->eng ? sys->eng->device_bytes() : 0) + sys->asm_arena.bytes();
+    *bytes = (sys->eng ? sys->eng->device_bytes() : 0) + sys->asm_arena.bytes() + sys->pat_arena.bytes() +
+             (sys->dl ? sys->dl->bytes() : 0);
     return CFDB_OK;
 }
 

@@ -221,6 +221,7 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
     for (const auto& s : systems) {
         if (!s.h) has_amg_ = false;
         if (s.n <= 0) fail(1, "engine: empty system");
+        if (s.dl && (n_sys_ != 1 || !s.h)) fail(1, "engine: device-resident levels need a single-system plan");
     }
     if (!has_amg_) {
         for (auto& s : systems) s.h.reset();
@@ -393,12 +394,13 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         // `pick(s)`, columns shifted into the target level's concatenated index space. Wide
         // operators (more than kWideRow entries per row on average) are stored as CSR for the
         // warp-per-row kernels unless the engine is in ordered (bit-reproducible) mode.
-        auto build_op = [&](auto pick, int col_level, int row_level, DevSell64_32& m) {
+        // dsrc: the operator as a device CSR (single-system plans with device-resident levels)
+        auto build_op = [&](auto pick, const DevCsr* dsrc, int col_level, int row_level, DevSell64_32& m) {
             long long nnz = 0, rows = 0;
             for (int k = 0; k < n_sys_; ++k) {
                 const int s = perm_[k];
                 if (L[s] - 1 <= l) continue;
-                nnz += pick(s).nnz();
+                nnz += dsrc != nullptr ? dsrc->nnz : pick(s).nnz();
                 rows += pick(s).n_rows;
             }
             // lanes per row: about lanes_div entries per lane, and enough lanes in all to keep
@@ -415,6 +417,39 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
             // thread per row; SELL (rows sorted by length within 256-row windows) otherwise
             const bool wide = !ordered_ && rows > 0 &&
                               (avg > tuning_.wide_row || static_cast<double>(rows) < kFillThreads);
+            if (dsrc != nullptr) {
+                // the same layouts built on the device (columns offset 0: one system)
+                const DevCsr& a = *dsrc;
+                const int n_pad = round_up(a.n_rows, 32);
+                if (wide) {
+                    int* dp = arena_.alloc<int>(static_cast<size_t>(n_pad) + 1);
+                    csr_rows_padded(a, n_pad, dp, st);
+                    int* dc = arena_.alloc<int>(static_cast<size_t>(a.nnz) + 4);
+                    double* v64 = need64_ ? arena_.alloc<double>(static_cast<size_t>(a.nnz) + 4) : nullptr;
+                    float* v32 = need32_ ? arena_.alloc<float>(static_cast<size_t>(a.nnz) + 4) : nullptr;
+                    csr_copy_values(a, dc, v64, v32, st);
+                    m.n_slices = n_pad;
+                    m.slots = a.nnz;
+                    if (need64_) m.s64 = {dp, dc, v64, lanes};
+                    if (need32_) m.s32 = {dp, dc, v32, lanes};
+                    op_tiles(m, lanes, row_level, [&](int s) { return L[s] - 1 > l; }, [](int) { return true; });
+                } else {
+                    int* dperm = arena_.alloc<int>(std::max(n_pad, 1));
+                    int* dp = arena_.alloc<int>(static_cast<size_t>(n_pad / 32) + 1);
+                    const long long slots = sell_shape(a, n_pad, kSellRows, dperm, dp, st);
+                    int* dc = arena_.alloc<int>(static_cast<size_t>(slots));
+                    double* v64 = need64_ ? arena_.alloc<double>(static_cast<size_t>(slots)) : nullptr;
+                    float* v32 = need32_ ? arena_.alloc<float>(static_cast<size_t>(slots)) : nullptr;
+                    sell_fill(a, n_pad, dperm, dp, 0, dc, v64, v32, st);
+                    m.n_slices = n_pad / 32;
+                    m.slots = slots;
+                    if (need64_) m.s64 = {dp, dc, v64, kFmtSell, dperm};
+                    if (need32_) m.s32 = {dp, dc, v32, kFmtSell, dperm};
+                    op_tiles(m, kFmtSell, row_level, [&](int s) { return L[s] - 1 > l; }, [](int) { return true; });
+                }
+                m.nnz = nnz;
+                return;
+            }
             if (wide) {
                 CsrBuild cbd;
                 for (int k = 0; k < n_sys_; ++k) {
@@ -474,22 +509,34 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
             }
             m.nnz = nnz;
         };
+        const DeviceLevels* dl = systems[perm_[0]].dl.get();
+        const bool dev_l = dl != nullptr && L[perm_[0]] - 1 > l;
         if (l > 0) {
-            std::vector<double> wd(static_cast<size_t>(d.n_rows_nc), weight_);
-            for (int k = 0; k < n_sys_; ++k) {
-                const int s = perm_[k];
-                if (L[s] - 1 <= l) continue; // only systems with a coarser level need A_l here
-                const HostCsr& a = systems[s].h->a[l];
-                const std::vector<double> dinv = inverse_diagonal(a);
-                for (int i = 0; i < a.n_rows; ++i) wd[off[l][s] + i] = weight_ * dinv[i];
+            if (dev_l) {
+                // weight / diagonal on the device from A_l (rows padded to the level's block)
+                if (need64_) d.wd64 = arena_.alloc<double>(std::max(d.n_rows_nc, 1));
+                if (need32_) d.wd32 = arena_.alloc<float>(std::max(d.n_rows_nc, 1));
+                weighted_inverse_diagonal(dl->a[l], d.n_rows_nc, weight_, d.wd64, d.wd32, st);
+            } else {
+                std::vector<double> wd(static_cast<size_t>(d.n_rows_nc), weight_);
+                for (int k = 0; k < n_sys_; ++k) {
+                    const int s = perm_[k];
+                    if (L[s] - 1 <= l) continue; // only systems with a coarser level need A_l here
+                    const HostCsr& a = systems[s].h->a[l];
+                    const std::vector<double> dinv = inverse_diagonal(a);
+                    for (int i = 0; i < a.n_rows; ++i) wd[off[l][s] + i] = weight_ * dinv[i];
+                }
+                if (need64_) d.wd64 = arena_.upload(wd, st);
+                if (need32_) d.wd32 = arena_.upload(to_float(wd), st);
             }
-            build_op([&](int s) -> const HostCsr& { return systems[s].h->a[l]; }, l, l, d.a);
-            if (need64_) d.wd64 = arena_.upload(wd, st);
-            if (need32_) d.wd32 = arena_.upload(to_float(wd), st);
+            build_op([&](int s) -> const HostCsr& { return systems[s].h->a[l]; }, dev_l ? &dl->a[l] : nullptr, l, l,
+                     d.a);
         }
         if (l + 1 < n_levels_) {
-            build_op([&](int s) -> const HostCsr& { return systems[s].h->p[l]; }, l + 1, l, d.p);
-            build_op([&](int s) -> const HostCsr& { return systems[s].h->r[l]; }, l, l + 1, d.r);
+            build_op([&](int s) -> const HostCsr& { return systems[s].h->p[l]; }, dev_l ? &dl->p[l] : nullptr, l + 1,
+                     l, d.p);
+            build_op([&](int s) -> const HostCsr& { return systems[s].h->r[l]; }, dev_l ? &dl->r[l] : nullptr, l,
+                     l + 1, d.r);
         }
         // vectors (zero-initialised)
         auto vec64 = [&](int n) {

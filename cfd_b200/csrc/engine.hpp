@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "common.hpp"
+#include "dsetup.hpp"
 #include "host_algos.hpp"
 #include "kernels.cuh"
 
@@ -23,6 +24,9 @@ struct SystemSpec {
     int vs_len = 0;                   // length of this system's value source
     bool absolute_src = false;        // src already indexes the batch-wide value source
     std::shared_ptr<const Hierarchy> h; // levels >= 1, transfers, coarse inverse (null: none)
+    // Device-resident levels (single-system plans): when set, h holds only the shapes and the
+    // coarse inverse, and the operators of levels >= 1 are laid out on the device from dl.
+    std::shared_ptr<const DeviceLevels> dl;
 };
 
 // Launch-shape and schedule knobs (no effect on the arithmetic of a row sum except that wide

@@ -369,6 +369,49 @@ int aggregate(const HostCsr& a, const std::vector<double>& d, double theta, std:
     return n_agg;
 }
 
+int aggregate_strong(int n, const int* srp, const int* sci, const double* sav, std::vector<int>& agg) {
+    agg.assign(static_cast<size_t>(n), -1);
+    int n_agg = 0;
+    // pass 1: seeds whose strong neighbourhood is non-empty and entirely unaggregated
+    for (int i = 0; i < n; ++i) {
+        if (agg[i] >= 0 || srp[i] == srp[i + 1]) continue;
+        bool is_free = true;
+        for (int k = srp[i]; k < srp[i + 1]; ++k) {
+            if (agg[sci[k]] >= 0) {
+                is_free = false;
+                break;
+            }
+        }
+        if (!is_free) continue;
+        agg[i] = n_agg;
+        for (int k = srp[i]; k < srp[i + 1]; ++k) agg[sci[k]] = n_agg;
+        ++n_agg;
+    }
+    // pass 2: join the pass-1 aggregate of the strongest strong neighbour (strictly larger wins)
+    const std::vector<int> pass1 = agg;
+    for (int i = 0; i < n; ++i) {
+        if (agg[i] >= 0) continue;
+        double best = 0.0;
+        for (int k = srp[i]; k < srp[i + 1]; ++k) {
+            const int j = sci[k];
+            if (pass1[j] >= 0 && sav[k] > best) {
+                best = sav[k];
+                agg[i] = pass1[j];
+            }
+        }
+    }
+    // pass 3: leftovers seed new aggregates with their unaggregated strong neighbours
+    for (int i = 0; i < n; ++i) {
+        if (agg[i] < 0) {
+            agg[i] = n_agg;
+            for (int k = srp[i]; k < srp[i + 1]; ++k)
+                if (agg[sci[k]] < 0) agg[sci[k]] = n_agg;
+            ++n_agg;
+        }
+    }
+    return n_agg;
+}
+
 bool dense_inverse(int n, const std::vector<double>& a, std::vector<double>& inv) {
     std::vector<double> f;
     if (!ldlt_factor(n, a, f)) {

@@ -13,6 +13,7 @@ struct AmgSettings {
     int coarse_size = 400; // amg.hpp:20
     int sweeps = 2;       // krylov.hpp:56
     double weight = 0.7;  // krylov.hpp:57
+    int table_limit = 0;  // device setup: largest row kept in shared-memory tables (0: default)
 };
 
 struct LduPatternHost {
@@ -39,6 +40,11 @@ struct Hierarchy {
 
 // Aggregation of amg.cpp:12-78 (serial, order dependent by design).
 int aggregate(const HostCsr& a, const std::vector<double>& diag, double theta, std::vector<int>& agg);
+
+// The same aggregation from the strength graph alone: row i's strong connections (i != j and
+// |a_ij| > theta sqrt|d_i d_j|) in CSR order, columns sci[srp[i]..srp[i+1]) with |a_ij| in sav.
+// Every test of amg.cpp:12-78 reads only strong entries, so the result equals aggregate().
+int aggregate_strong(int n, const int* srp, const int* sci, const double* sav, std::vector<int>& agg);
 
 // Full setup. Sparse products use Gustavson order (row i: k ascending in A(i,:), j ascending
 // in B(k,:), first touch assigns), run row-parallel, so the result is independent of threads.

@@ -94,6 +94,9 @@ typedef struct {
     int coarse_size;           /* 400 */
     int smooth_sweeps;         /* 2 */
     double jacobi_weight;      /* 0.7 */
+    /* device setup only (no effect on results): rows of a sparse product or transpose with
+     * more entries than this use device-memory tables instead of shared memory (0: 6144) */
+    int device_table_limit;
 } cfdb_amg_settings;
 
 /* ---- backend queries: krylov.hpp:118-123 ---- */
@@ -150,6 +153,11 @@ int cfdb_build_pattern(int n, int n_faces, const int* owner, const int* neighbou
 typedef struct cfdb_hierarchy cfdb_hierarchy;
 int cfdb_amg_setup(const cfdb_csr* a, const cfdb_amg_settings* settings,
                    cfdb_hierarchy** out);
+/* The same hierarchy built on the device (sparse products, strength graph, transfers and
+ * Galerkin operators in CUDA kernels; the sequential aggregation on the host), bit-identical
+ * to cfdb_amg_setup. */
+int cfdb_amg_setup_device(const cfdb_csr* a, const cfdb_amg_settings* settings,
+                          cfdb_hierarchy** out);
 int cfdb_hierarchy_destroy(cfdb_hierarchy* h);
 /* levels() / level_matrix / level_prolongation / level_restriction (amg.hpp:37-54);
  * which: 0 = a, 1 = p, 2 = r. Pointers stay valid while h lives. */
@@ -182,6 +190,15 @@ int cfdb_system_set_amg(cfdb_system* sys, const cfdb_amg_view* amg);
  * installs it, as LduMatrix::solve_persistent does on an AMG rebuild (ldu_matrix.cpp:314-353).*/
 int cfdb_system_setup_amg(cfdb_system* sys, const double* diag, const double* upper,
                           const double* lower, const cfdb_amg_settings* settings);
+/* cfdb_system_setup_amg with the hierarchy built on the device (as cfdb_amg_setup_device);
+ * device_arrays: diag/upper/lower are device pointers (ready when the call is made). */
+int cfdb_system_setup_amg_device(cfdb_system* sys, const double* diag, const double* upper,
+                                 const double* lower, const cfdb_amg_settings* settings,
+                                 int device_arrays);
+/* Wall-clock seconds of the phases of the last hierarchy setup of sys, as text
+ * "phase=seconds;..." (host setup: hierarchy, plan; device setup: strength, aggregate,
+ * prolongation, transpose, AP, RAP, coarse_inverse, input, keep, plan). */
+int cfdb_system_setup_profile(const cfdb_system* sys, char* buf, size_t len);
 int cfdb_system_set_precision(cfdb_system* sys, int precision);
 /* solve(diag, upper, lower, b, x, method, use_amg, control): assembles A from LDU on the
  * device and solves A x = b; x is the initial guess in and the solution out. */

@@ -280,7 +280,7 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ds.setup_amg(b["dg"].cpu().numpy(), b["up"].cpu().numpy(), b["lo"].cpu().numpy(),
-                     cb.AmgSettings(strength_threshold=THETA))
+                     cb.AmgSettings(strength_threshold=THETA), device=False)
         setup_s[k] = time.perf_counter() - t0
         for _ in range(2):
             torch.cuda.synchronize()

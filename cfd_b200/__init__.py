@@ -108,6 +108,7 @@ _proto("cfdb_system_set_amg", [_vp, _P(AmgViewStruct)])
 _proto("cfdb_system_setup_amg", [_vp, _pd, _pd, _pd, _P(AmgSettingsStruct)])
 _proto("cfdb_system_setup_amg_device", [_vp, _vp, _vp, _vp, _P(AmgSettingsStruct), _i])
 _proto("cfdb_system_setup_profile", [_vp, C.c_char_p, C.c_size_t])
+_proto("cfdb_system_set_keep_levels", [_vp, _i])
 _proto("cfdb_system_set_precision", [_vp, _i])
 _proto("cfdb_system_solve", [_vp, _pd, _pd, _pd, _pd, _pd, _i, _i, _P(ControlStruct),
                              _P(StatsStruct)])
@@ -592,10 +593,10 @@ class DeviceSolver:
         _check(_lib.cfdb_system_set_amg(self._h, C.byref(v)))
 
     def setup_amg(self, diag, upper, lower, settings: AmgSettings | None = None,
-                  device: bool = False) -> None:
-        """AmgPreconditioner::setup from LDU coefficients and installation of the hierarchy.
-        device=True builds it on the GPU (bit-identical); the coefficients may then also be
-        CUDA tensors (ready on the current stream)."""
+                  device: bool = True) -> None:
+        """AmgPreconditioner::setup from LDU coefficients and installation of the hierarchy:
+        built on the GPU (device=True, the default; the coefficients may also be CUDA tensors
+        ready on the current stream) or on the host (device=False); both are bit-identical."""
         s = (settings or AmgSettings())._c()
         if not device:
             _check(_lib.cfdb_system_setup_amg(self._h, _dp(_f64(diag)), _dp(_f64(upper)),
@@ -610,6 +611,11 @@ class DeviceSolver:
         d, u, lo = _f64(diag), _f64(upper), _f64(lower)
         _check(_lib.cfdb_system_setup_amg_device(self._h, d.ctypes.data, u.ctypes.data,
                                                  lo.ctypes.data, C.byref(s), 0))
+
+    def set_keep_levels(self, keep: bool) -> None:
+        """Keep a device setup's levels on the device so that later precision or tuning changes
+        can rebuild the plan (default True)."""
+        _check(_lib.cfdb_system_set_keep_levels(self._h, 1 if keep else 0))
 
     def setup_profile(self) -> dict:
         """Seconds per phase of the last hierarchy setup."""

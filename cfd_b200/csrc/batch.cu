@@ -177,6 +177,8 @@ int cfdb_batch_create(int n_systems, const int* n_cells, const int* n_faces, con
 int cfdb_batch_destroy(cfdb_batch* b) {
     if (b != nullptr) {
         cudaSetDevice(b->device);
+        // device buffers go back to the pool at once: let the work that uses them finish
+        if (b->eng) cudaStreamSynchronize(b->eng->stream());
         delete b;
     }
     return CFDB_OK;

@@ -154,6 +154,8 @@ struct cfdb_system {
     std::unique_ptr<Engine> eng;
     std::shared_ptr<const Hierarchy> h;
     std::shared_ptr<const DeviceLevels> dl; // device-resident levels of a device setup
+    bool h_shapes_only = false;             // h came from a device setup (matrices on the device)
+    bool keep_levels = true;                // keep dl after a device setup (plan rebuilds)
     int sweeps = 2;
     double weight = 0.7;
     int precision = CFDB_PRECISION_FP64;
@@ -176,6 +178,7 @@ struct cfdb_system {
     int* d_upos = nullptr;
     int* d_lpos = nullptr;
     std::string setup_profile; // phase times of the last hierarchy setup
+    PinnedBuffer stage;        // page-locked staging of the device setup's read-backs
 };
 
 namespace {
@@ -194,6 +197,9 @@ void build_value_map(cfdb_system* s) {
 
 void ensure_engine(cfdb_system* s) {
     if (!s->dirty && s->eng) return;
+    if (s->h && s->h_shapes_only && !s->dl)
+        fail(CFDB_ERR_NOT_READY, "the hierarchy was built on the device without keeping its levels "
+                                 "(cfdb_system_set_keep_levels): set it up again before changing the plan");
     CFDB_CUDA(cudaSetDevice(s->device));
     if (!s->eng) s->eng = std::make_unique<Engine>(s->device);
     SystemSpec sp;
@@ -376,13 +382,13 @@ static int assemble_impl(int n_cells, int n_faces, const int* owner, const int* 
         }
         std::vector<int> ptr, face;
         cell_faces(n_cells, n_faces, own_h, nei_h, ptr, face);
+        DeviceArena ar; // released after the guard has drained the stream
         cudaStream_t st = nullptr;
         CFDB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         struct StreamGuard {
             cudaStream_t s;
             ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
         } guard{st};
-        DeviceArena ar;
         const int* d_ptr = ar.upload(ptr, st);
         const int* d_face = ar.upload(face, st);
         const int* d_own;
@@ -706,6 +712,8 @@ int cfdb_system_destroy(cfdb_system* sys) {
     return guarded([&] {
         if (sys == nullptr) return;
         cudaSetDevice(sys->device);
+        // device buffers go back to the pool at once: let the work that uses them finish
+        if (sys->eng) cudaStreamSynchronize(sys->eng->stream());
         delete sys;
     });
 }
@@ -719,6 +727,7 @@ int cfdb_system_set_amg(cfdb_system* sys, const cfdb_amg_view* amg) {
             fail(CFDB_ERR_BAD_ARG, "DeviceSolver::set_amg: empty hierarchy");
         sys->h = hierarchy_from(*amg, sys->pat.n, /*skip_a0=*/true);
         sys->dl.reset();
+        sys->h_shapes_only = false;
         sys->sweeps = amg->smooth_sweeps;
         sys->weight = amg->jacobi_weight;
         sys->dirty = true;
@@ -753,6 +762,7 @@ int cfdb_system_setup_amg(cfdb_system* sys, const double* diag, const double* up
         auto h = std::make_shared<Hierarchy>(amg_setup(a, s));
         const double t1 = PhaseTimes::now();
         sys->dl.reset();
+        sys->h_shapes_only = false;
         if (h->levels() <= 1) {
             // ldu_matrix.cpp:358: a single-level hierarchy runs Jacobi CG instead of AMG
             sys->h.reset();
@@ -810,7 +820,7 @@ int cfdb_system_setup_amg_device(cfdb_system* sys, const double* diag, const dou
         CFDB_CUDA(cudaMemsetAsync(a0.va, 0, sizeof(double) * p.nnz(), cs.s));
         ldu_to_csr_values(p.n, p.n_faces, sys->d_dpos, sys->d_upos, sys->d_lpos, dd, du, dl, a0.va, cs.s);
         const double t0 = PhaseTimes::now();
-        amg_setup_device(a0, s, cs.s, dh);
+        amg_setup_device(a0, s, cs.s, dh, &sys->stage);
         const double t1 = PhaseTimes::now();
         dh.times.add("input", t0 - t_in);
         // the plan is laid out on the device from compact copies of the levels, which the
@@ -822,17 +832,27 @@ int cfdb_system_setup_amg_device(cfdb_system* sys, const double* diag, const dou
         if (h->levels() <= 1) {
             sys->h.reset(); // ldu_matrix.cpp:358: one level runs Jacobi CG
             sys->dl.reset();
+            sys->h_shapes_only = false;
         } else {
             sys->h = h;
             sys->dl = kept;
+            sys->h_shapes_only = true;
         }
         sys->sweeps = s.sweeps;
         sys->weight = s.weight;
         sys->dirty = true;
         ensure_engine(sys);
+        if (!sys->keep_levels) sys->dl.reset();
         dh.times.add("plan", PhaseTimes::now() - t2);
+        for (const auto& pt : sys->eng->build_times().t) dh.times.add(pt.first, pt.second);
         sys->setup_profile = dh.times.text();
     });
+}
+
+int cfdb_system_set_keep_levels(cfdb_system* sys, int keep) {
+    if (sys == nullptr) return set_error(CFDB_ERR_BAD_ARG, "null system");
+    sys->keep_levels = keep != 0;
+    return CFDB_OK;
 }
 
 int cfdb_system_setup_profile(const cfdb_system* sys, char* buf, size_t len) {

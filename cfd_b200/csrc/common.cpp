@@ -1,5 +1,10 @@
 #include "common.hpp"
 
+#include <algorithm>
+#include <cstdint>
+#include <map>
+#include <mutex>
+
 namespace cfdb {
 
 void fail(int code, const std::string& msg) { throw Error(code, msg); }
@@ -11,21 +16,79 @@ void check_cuda(cudaError_t e, const char* what) {
     }
 }
 
+namespace {
+
+// One pool per device, created on first use; freed blocks stay in the pool (no release
+// threshold) and are reused by later allocations of any thread.
+cudaMemPool_t device_pool(int device) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    check_cuda(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+    uint64_t keep = UINT64_MAX;
+    check_cuda(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+    pools[device] = pool;
+    return pool;
+}
+
+} // namespace
+
 void DeviceBuffer::allocate(size_t bytes) {
     release();
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
     void* p = nullptr;
-    const cudaError_t e = cudaMalloc(&p, bytes);
+    // allocated in the order of this thread's default stream, then completed, so the block
+    // can be used from any stream
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, device_pool(dev), cudaStreamPerThread);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
         throw Error(3, "CUDA malloc of " + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
     }
     ptr_ = p;
     bytes_ = bytes;
+    device_ = dev;
+}
+
+PinnedBuffer::~PinnedBuffer() {
+    if (ptr_ != nullptr) cudaFreeHost(ptr_);
+}
+
+void* PinnedBuffer::get(size_t bytes) {
+    if (bytes <= bytes_ && ptr_ != nullptr) return ptr_;
+    if (ptr_ != nullptr) {
+        cudaFreeHost(ptr_);
+        ptr_ = nullptr;
+        bytes_ = 0;
+    }
+    const size_t want = std::max(bytes, static_cast<size_t>(1) << 20);
+    void* p = nullptr;
+    const cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        throw Error(3, "CUDA host allocation of " + std::to_string(want) + " bytes: " + cudaGetErrorString(e));
+    }
+    ptr_ = p;
+    bytes_ = want;
+    return ptr_;
 }
 
 void DeviceBuffer::release() {
+    // callers release a buffer only once the work that used it has completed
     if (ptr_ != nullptr) {
-        cudaFree(ptr_);
+        int cur = 0;
+        cudaGetDevice(&cur);
+        if (cur != device_) cudaSetDevice(device_);
+        cudaFreeAsync(ptr_, cudaStreamPerThread);
+        if (cur != device_) cudaSetDevice(cur);
         ptr_ = nullptr;
         bytes_ = 0;
     }

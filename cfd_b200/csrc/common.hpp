@@ -33,7 +33,10 @@ struct HostCsr {
     [[nodiscard]] bool empty() const { return n_rows == 0; }
 };
 
-// Owning device allocation (256-byte aligned by cudaMalloc).
+// Owning device allocation (256-byte aligned), from the library's stream-ordered memory pool of
+// the current device: the pool keeps freed memory for reuse, so a plan rebuild, which frees
+// one plan and allocates the next, neither returns memory to the driver nor waits for the
+// device to go idle as cudaFree does.
 class DeviceBuffer {
 public:
     DeviceBuffer() = default;
@@ -59,6 +62,23 @@ public:
     void release();
     [[nodiscard]] void* get() const { return ptr_; }
     template <class T> [[nodiscard]] T* as() const { return static_cast<T*>(ptr_); }
+    [[nodiscard]] size_t bytes() const { return bytes_; }
+
+private:
+    void* ptr_ = nullptr;
+    size_t bytes_ = 0;
+    int device_ = 0;
+};
+
+// Grow-only page-locked host buffer (staging of device-to-host reads).
+class PinnedBuffer {
+public:
+    PinnedBuffer() = default;
+    ~PinnedBuffer();
+    PinnedBuffer(const PinnedBuffer&) = delete;
+    PinnedBuffer& operator=(const PinnedBuffer&) = delete;
+    // at least `bytes` bytes (contents not kept when it grows)
+    void* get(size_t bytes);
     [[nodiscard]] size_t bytes() const { return bytes_; }
 
 private:

@@ -63,6 +63,8 @@ int grid_for(long long n, int threads = kThreads) {
     return static_cast<int>(std::max<long long>(1, (n + threads - 1) / threads));
 }
 
+size_t aligned(size_t bytes) { return (bytes + 255) & ~static_cast<size_t>(255); }
+
 int next_pow2(long long v) {
     long long p = 1;
     while (p < v) p <<= 1;
@@ -191,6 +193,28 @@ __global__ void k_strong(int n, const int* __restrict__ rp, const int* __restric
         }
     }
     if (!FILL) cnt[i] = c;
+}
+
+// rank of each strong entry within its row by (|a| descending, position ascending); rows have
+// at most 4096 strong entries (checked by the host)
+__global__ void k_strong_rank(int n, const int* __restrict__ srp, const double* __restrict__ sav, uint16_t* rank) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int b = srp[i], e = srp[i + 1];
+    for (int k = b; k < e; ++k) {
+        const double v = sav[k];
+        int r = 0;
+        for (int q = b; q < e; ++q) {
+            const double w = sav[q];
+            r += (w > v) || (w == v && q < k);
+        }
+        rank[k] = static_cast<uint16_t>(r);
+    }
+}
+
+__global__ void k_max_degree(int n, const int* __restrict__ srp, int* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicMax(out, srp[i + 1] - srp[i]);
 }
 
 // inv = 1/d (0 where d == 0); rho = max_i |inv_i| sum_j |a_ij| (bits of a non-negative double)
@@ -827,7 +851,10 @@ void ldu_to_csr_values(int n, int nf, const int* diag_pos, const int* upper_pos,
     CFDB_CUDA(cudaGetLastError());
 }
 
-void amg_setup_device(const DevCsr& a0, const AmgSettings& s, cudaStream_t st, DeviceHierarchy& h) {
+void amg_setup_device(const DevCsr& a0, const AmgSettings& s, cudaStream_t st, DeviceHierarchy& h,
+                      PinnedBuffer* stage) {
+    PinnedBuffer own_stage;
+    if (stage == nullptr) stage = &own_stage;
     if (a0.n_rows != a0.n_cols) fail(1, "AmgPreconditioner: matrix must be square");
     if (a0.n_rows <= 0) fail(1, "amg_setup: empty matrix");
     Ctx cx{st, &h.mem, nullptr, nullptr, nullptr, s.table_limit > 0 ? s.table_limit : INT_MAX};
@@ -864,15 +891,36 @@ void amg_setup_device(const DevCsr& a0, const AmgSettings& s, cudaStream_t st, D
         k_strong<true><<<grid_for(nl), kThreads, 0, st>>>(nl, cur.rp, cur.ci, cur.va, d, s.theta, nullptr, srp, sci,
                                                           sav);
         CFDB_CUDA(cudaGetLastError());
-        std::vector<int> srp_h, sci_h;
-        std::vector<double> sav_h;
-        to_host(srp_h, srp, static_cast<size_t>(nl) + 1, st);
-        to_host(sci_h, sci, static_cast<size_t>(ns), st);
-        to_host(sav_h, sav, static_cast<size_t>(ns), st);
+        // read back: offsets, columns and, per entry, its strength rank within the row (2
+        // bytes; the |a_ij| themselves when a row has more than 65536 strong entries)
+        CFDB_CUDA(cudaMemsetAsync(cx.d_counts, 0, sizeof(int), st));
+        k_max_degree<<<grid_for(nl), kThreads, 0, st>>>(nl, srp, cx.d_counts);
+        int max_deg = 0;
+        CFDB_CUDA(cudaMemcpyAsync(&max_deg, cx.d_counts, sizeof(int), cudaMemcpyDeviceToHost, st));
         sync(st);
+        const bool ranked = max_deg <= std::min(4096, cx.lim); // ranks cost O(degree^2) per row
+        const size_t b_rp = aligned(sizeof(int) * (static_cast<size_t>(nl) + 1));
+        const size_t b_ci = aligned(sizeof(int) * static_cast<size_t>(ns));
+        const size_t b_key = aligned((ranked ? sizeof(uint16_t) : sizeof(double)) * static_cast<size_t>(ns));
+        char* host = static_cast<char*>(stage->get(b_rp + b_ci + b_key));
+        const int* srp_h = reinterpret_cast<const int*>(host);
+        const int* sci_h = reinterpret_cast<const int*>(host + b_rp);
+        CFDB_CUDA(cudaMemcpyAsync(host, srp, sizeof(int) * (static_cast<size_t>(nl) + 1), cudaMemcpyDeviceToHost, st));
+        if (ns > 0) CFDB_CUDA(cudaMemcpyAsync(host + b_rp, sci, sizeof(int) * ns, cudaMemcpyDeviceToHost, st));
+        if (ranked) {
+            uint16_t* rank = h.mem.alloc<uint16_t>(ns);
+            k_strong_rank<<<grid_for(nl), kThreads, 0, st>>>(nl, srp, sav, rank);
+            if (ns > 0)
+                CFDB_CUDA(cudaMemcpyAsync(host + b_rp + b_ci, rank, sizeof(uint16_t) * ns, cudaMemcpyDeviceToHost, st));
+        } else if (ns > 0) {
+            CFDB_CUDA(cudaMemcpyAsync(host + b_rp + b_ci, sav, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
+        }
+        CFDB_CUDA(cudaGetLastError());
         phase("strength");
         std::vector<int> agg;
-        const int n_agg = aggregate_strong(nl, srp_h.data(), sci_h.data(), sav_h.data(), agg);
+        const int n_agg =
+            ranked ? aggregate_strong_ranked(nl, srp_h, sci_h, reinterpret_cast<const uint16_t*>(host + b_rp + b_ci), agg)
+                   : aggregate_strong(nl, srp_h, sci_h, reinterpret_cast<const double*>(host + b_rp + b_ci), agg);
         phase("aggregate");
         if (n_agg >= nl || n_agg == 0) {
             h.a.push_back(cur);
@@ -1046,11 +1094,20 @@ __global__ void k_weighted_inv_diag(int n, int n_pad, const int* __restrict__ rp
     if (wd32 != nullptr) wd32[i] = __double2float_rn(w);
 }
 
-DevCsr keep_csr(const DevCsr& m, DeviceArena& mem, cudaStream_t st) {
+size_t csr_bytes(const DevCsr& m) {
+    return aligned(sizeof(int) * (static_cast<size_t>(m.n_rows) + 1)) + aligned(sizeof(int) * m.nnz) +
+           aligned(sizeof(double) * m.nnz);
+}
+
+// copy of m carved out of the block at `cursor` (advanced)
+DevCsr keep_csr(const DevCsr& m, char*& cursor, cudaStream_t st) {
     DevCsr k = m;
-    k.rp = mem.alloc<int>(static_cast<size_t>(m.n_rows) + 1);
-    k.ci = mem.alloc<int>(static_cast<size_t>(m.nnz));
-    k.va = mem.alloc<double>(static_cast<size_t>(m.nnz));
+    k.rp = reinterpret_cast<int*>(cursor);
+    cursor += aligned(sizeof(int) * (static_cast<size_t>(m.n_rows) + 1));
+    k.ci = reinterpret_cast<int*>(cursor);
+    cursor += aligned(sizeof(int) * m.nnz);
+    k.va = reinterpret_cast<double*>(cursor);
+    cursor += aligned(sizeof(double) * m.nnz);
     CFDB_CUDA(cudaMemcpyAsync(k.rp, m.rp, sizeof(int) * (static_cast<size_t>(m.n_rows) + 1), cudaMemcpyDeviceToDevice, st));
     if (m.nnz > 0) {
         CFDB_CUDA(cudaMemcpyAsync(k.ci, m.ci, sizeof(int) * m.nnz, cudaMemcpyDeviceToDevice, st));
@@ -1063,18 +1120,22 @@ DevCsr keep_csr(const DevCsr& m, DeviceArena& mem, cudaStream_t st) {
 
 std::shared_ptr<DeviceLevels> keep_levels(const DeviceHierarchy& d, cudaStream_t st) {
     auto k = std::make_shared<DeviceLevels>();
+    size_t total = 0; // one allocation for all levels
+    for (int l = 1; l < d.levels(); ++l) total += csr_bytes(d.a[l]);
+    for (size_t l = 0; l < d.p.size(); ++l) total += csr_bytes(d.p[l]) + csr_bytes(d.r[l]);
+    char* cursor = k->mem.alloc<char>(total);
     for (int l = 0; l < d.levels(); ++l) {
         if (l == 0) {
             DevCsr e;
             e.n_rows = e.n_cols = d.a[0].n_rows;
             k->a.push_back(e);
         } else {
-            k->a.push_back(keep_csr(d.a[l], k->mem, st));
+            k->a.push_back(keep_csr(d.a[l], cursor, st));
         }
     }
     for (size_t l = 0; l < d.p.size(); ++l) {
-        k->p.push_back(keep_csr(d.p[l], k->mem, st));
-        k->r.push_back(keep_csr(d.r[l], k->mem, st));
+        k->p.push_back(keep_csr(d.p[l], cursor, st));
+        k->r.push_back(keep_csr(d.r[l], cursor, st));
     }
     sync(st);
     return k;

@@ -87,8 +87,10 @@ struct DeviceHierarchy {
 };
 
 // Builds the hierarchy of a0 (device CSR, already in h.mem or caller-owned and alive for the
-// call) with settings s on stream st. Synchronises st.
-void amg_setup_device(const DevCsr& a0, const AmgSettings& s, cudaStream_t st, DeviceHierarchy& h);
+// call) with settings s on stream st. Synchronises st. stage: page-locked staging of the
+// strength graphs read back for aggregation (null: a temporary one).
+void amg_setup_device(const DevCsr& a0, const AmgSettings& s, cudaStream_t st, DeviceHierarchy& h,
+                      PinnedBuffer* stage = nullptr);
 
 // Host copy of a device hierarchy; level 0's matrix is copied only when with_a0.
 Hierarchy download_hierarchy(const DeviceHierarchy& d, bool with_a0, cudaStream_t st);

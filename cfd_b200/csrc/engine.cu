@@ -200,10 +200,19 @@ long long Engine::level_slots(int l) const { return l < n_levels_ ? lv_[l].a.slo
 
 void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, bool need64,
                    bool need32) {
+    build_times_ = PhaseTimes{};
+    double t_mark = PhaseTimes::now();
+    auto phase = [&](const char* name) {
+        CFDB_CUDA(cudaStreamSynchronize(stream_));
+        const double t = PhaseTimes::now();
+        build_times_.add(name, t - t_mark);
+        t_mark = t;
+    };
     CFDB_CUDA(cudaSetDevice(device_));
     CFDB_CUDA(cudaStreamSynchronize(stream_));
     release_graphs();
     arena_.clear();
+    phase("plan_release");
     lv_.clear();
     tail32_ = nullptr;
     tail64_ = nullptr;
@@ -337,8 +346,40 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         m.tiles.row = arena_.upload(trow, st);
         m.tiles.sys = n_sys_ > 1 ? arena_.upload(tsys, st) : nullptr;
     };
-    // level-0 operator (values filled per solve) + value maps
-    {
+    // level-0 operator (values filled per solve) + value maps. Its layout depends only on the
+    // systems' patterns, so a single-system plan rebuilt over the same pattern (a new
+    // hierarchy, precision or tuning) reuses it from the previous build.
+    L0Key key;
+    key.n_sys = n_sys_;
+    if (n_sys_ == 1) {
+        const SystemSpec& sp = systems[0];
+        key.rp = sp.rp;
+        key.ci = sp.ci;
+        key.n = sp.n;
+        key.nnz = sp.rp[sp.n];
+        key.vs_len = sp.vs_len;
+        key.absolute_src = sp.absolute_src;
+        long long h = 0;
+        for (size_t k = 0; k < sp.src.size(); ++k) h = h * 1000003 + sp.src[k];
+        for (size_t k = 0; k < sp.diag_src.size(); ++k) h = h * 1000003 + sp.diag_src[k];
+        key.map_hash = h;
+    }
+    key.need32 = need32_;
+    key.col16 = tuning_.col16 != 0;
+    if (n_sys_ == 1 && l0_valid_ && key == l0_key_) {
+        DevLevel& d = lv_[0];
+        d.a = l0_.a;
+        d.wd64 = l0_.wd64;
+        d.wd32 = l0_.wd32;
+        src0_ = l0_.src0;
+        diag_src0_ = l0_.diag_src0;
+        row_map_ = l0_.row_map;
+        dinv0_ = l0_.dinv0;
+        user_rows_ = l0_.user_rows;
+        op_tiles(d.a, kFmtSell, 0, [](int) { return true; }, [&](int s) { return L[s] > 1; });
+    } else {
+        l0_valid_ = false;
+        arena0_.clear();
         SellBuild sb;
         sb.with_src = true;
         std::vector<int> dsrc(static_cast<size_t>(lv_[0].n_rows), -1);
@@ -357,23 +398,23 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         DevLevel& d = lv_[0];
         d.a.n_slices = static_cast<int>(sb.slice.size()) - 1;
         d.a.slots = sb.slice.back();
-        const int* dslice = arena_.upload(sb.slice, st);
-        const int* dcol = arena_.upload(sb.col, st);
-        d.a.s64 = {dslice, dcol, arena_.alloc<double>(d.a.slots), kFmtSell};
+        const int* dslice = arena0_.upload(sb.slice, st);
+        const int* dcol = arena0_.upload(sb.col, st);
+        d.a.s64 = {dslice, dcol, arena0_.alloc<double>(d.a.slots), kFmtSell};
         if (need32_) {
-            d.a.s32 = {dslice, dcol, arena_.alloc<float>(d.a.slots), kFmtSell};
+            d.a.s32 = {dslice, dcol, arena0_.alloc<float>(d.a.slots), kFmtSell};
             std::vector<uint16_t> c16;
             std::vector<int> cbase;
             if (tuning_.col16 && compress_cols(sb.slice, sb.col, &sb.pad, c16, cbase)) {
-                d.a.s32.c16 = arena_.upload(c16, st);
-                d.a.s32.cbase = arena_.upload(cbase, st);
+                d.a.s32.c16 = arena0_.upload(c16, st);
+                d.a.s32.cbase = arena0_.upload(cbase, st);
             }
         }
         long long nnz0 = 0;
         for (int s = 0; s < n_sys_; ++s) nnz0 += systems[s].rp[systems[s].n];
         d.a.nnz = nnz0;
-        src0_ = arena_.upload(sb.src, st);
-        diag_src0_ = arena_.upload(dsrc, st);
+        src0_ = arena0_.upload(sb.src, st);
+        diag_src0_ = arena0_.upload(dsrc, st);
         std::vector<int> rmap(static_cast<size_t>(lv_[0].n_rows), -1);
         long long uo = 0;
         for (int s = 0; s < n_sys_; ++s) {
@@ -381,12 +422,18 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
             uo += systems[s].n;
         }
         user_rows_ = uo;
-        row_map_ = arena_.upload(rmap, st);
-        d.wd64 = arena_.alloc<double>(d.n_rows);
-        if (need32_) d.wd32 = arena_.alloc<float>(d.n_rows);
-        dinv0_ = arena_.alloc<double>(d.n_rows);
+        row_map_ = arena0_.upload(rmap, st);
+        d.wd64 = arena0_.alloc<double>(d.n_rows);
+        if (need32_) d.wd32 = arena0_.alloc<float>(d.n_rows);
+        dinv0_ = arena0_.alloc<double>(d.n_rows);
         op_tiles(d.a, kFmtSell, 0, [](int) { return true; }, [&](int s) { return L[s] > 1; });
+        if (n_sys_ == 1) {
+            l0_key_ = key;
+            l0_ = L0Cache{d.a, d.wd64, d.wd32, src0_, diag_src0_, row_map_, dinv0_, user_rows_};
+            l0_valid_ = true;
+        }
     }
+    phase("plan_level0");
     // coarser levels, transfers
     for (int l = 0; l < n_levels_; ++l) {
         DevLevel& d = lv_[l];
@@ -562,6 +609,7 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
             if (l > 0) d.b32 = vec32(d.n_rows);
         }
     }
+    phase("plan_levels");
     // Krylov vectors and state
     {
         const int n0 = lv_[0].n_rows;
@@ -681,7 +729,7 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
                                            static_cast<int>(coarse_smem32_)));
         }
     }
-    CFDB_CUDA(cudaStreamSynchronize(st));
+    phase("plan_rest");
 }
 
 void Engine::set_values_device(const double* p0, const double* p1, const double* p2, int n1, int n2) {

@@ -79,7 +79,7 @@ public:
     [[nodiscard]] bool has_amg() const { return has_amg_; }
     [[nodiscard]] bool has32() const { return need32_; }
     [[nodiscard]] bool has64() const { return need64_; }
-    [[nodiscard]] size_t device_bytes() const { return arena_.bytes(); }
+    [[nodiscard]] size_t device_bytes() const { return arena_.bytes() + arena0_.bytes(); }
     [[nodiscard]] cudaStream_t stream() const { return stream_; }
     [[nodiscard]] int device() const { return device_; }
     [[nodiscard]] int levels() const { return n_levels_; }
@@ -135,6 +135,8 @@ public:
     // Kernels launched by this engine so far (graph kernel nodes counted per graph launch).
     [[nodiscard]] unsigned long long kernel_launches() const { return launches_; }
     [[nodiscard]] bool ordered() const { return ordered_; }
+    // wall-clock seconds of the phases of the last build()
+    [[nodiscard]] const PhaseTimes& build_times() const { return build_times_; }
 
 private:
     struct DevSell64_32 {
@@ -244,6 +246,35 @@ private:
     cudaGraphExec_t graphs_[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
     int graph_kernels_[3][2] = {{0, 0}, {0, 0}, {0, 0}};
     unsigned long long launches_ = 0;
+    PhaseTimes build_times_;
+    // level-0 layout kept across builds of a single-system plan over the same pattern
+    struct L0Key {
+        int n_sys = 0;
+        const int* rp = nullptr;
+        const int* ci = nullptr;
+        int n = 0, nnz = 0, vs_len = 0;
+        bool absolute_src = false;
+        long long map_hash = 0;
+        bool need32 = false, col16 = false;
+        bool operator==(const L0Key& o) const {
+            return n_sys == o.n_sys && rp == o.rp && ci == o.ci && n == o.n && nnz == o.nnz && vs_len == o.vs_len &&
+                   absolute_src == o.absolute_src && map_hash == o.map_hash && need32 == o.need32 && col16 == o.col16;
+        }
+    };
+    struct L0Cache {
+        DevSell64_32 a;
+        double* wd64;
+        float* wd32;
+        int* src0;
+        int* diag_src0;
+        int* row_map;
+        double* dinv0;
+        long long user_rows;
+    };
+    DeviceArena arena0_;
+    L0Key l0_key_{};
+    L0Cache l0_{};
+    bool l0_valid_ = false;
 };
 
 } // namespace cfdb

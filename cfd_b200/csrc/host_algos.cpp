@@ -1,6 +1,7 @@
 #include "host_algos.hpp"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 
@@ -401,6 +402,46 @@ int aggregate_strong(int n, const int* srp, const int* sci, const double* sav, s
         }
     }
     // pass 3: leftovers seed new aggregates with their unaggregated strong neighbours
+    for (int i = 0; i < n; ++i) {
+        if (agg[i] < 0) {
+            agg[i] = n_agg;
+            for (int k = srp[i]; k < srp[i + 1]; ++k)
+                if (agg[sci[k]] < 0) agg[sci[k]] = n_agg;
+            ++n_agg;
+        }
+    }
+    return n_agg;
+}
+
+int aggregate_strong_ranked(int n, const int* srp, const int* sci, const uint16_t* rank, std::vector<int>& agg) {
+    agg.assign(static_cast<size_t>(n), -1);
+    int n_agg = 0;
+    for (int i = 0; i < n; ++i) {
+        if (agg[i] >= 0 || srp[i] == srp[i + 1]) continue;
+        bool is_free = true;
+        for (int k = srp[i]; k < srp[i + 1]; ++k) {
+            if (agg[sci[k]] >= 0) {
+                is_free = false;
+                break;
+            }
+        }
+        if (!is_free) continue;
+        agg[i] = n_agg;
+        for (int k = srp[i]; k < srp[i + 1]; ++k) agg[sci[k]] = n_agg;
+        ++n_agg;
+    }
+    const std::vector<int> pass1 = agg;
+    for (int i = 0; i < n; ++i) {
+        if (agg[i] >= 0) continue;
+        int best = INT_MAX;
+        for (int k = srp[i]; k < srp[i + 1]; ++k) {
+            const int j = sci[k];
+            if (pass1[j] >= 0 && rank[k] < best) {
+                best = rank[k];
+                agg[i] = pass1[j];
+            }
+        }
+    }
     for (int i = 0; i < n; ++i) {
         if (agg[i] < 0) {
             agg[i] = n_agg;

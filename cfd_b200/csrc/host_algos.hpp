@@ -45,6 +45,9 @@ int aggregate(const HostCsr& a, const std::vector<double>& diag, double theta, s
 // |a_ij| > theta sqrt|d_i d_j|) in CSR order, columns sci[srp[i]..srp[i+1]) with |a_ij| in sav.
 // Every test of amg.cpp:12-78 reads only strong entries, so the result equals aggregate().
 int aggregate_strong(int n, const int* srp, const int* sci, const double* sav, std::vector<int>& agg);
+// The same with sav replaced by each strong entry's rank within its row by (|a_ij| descending,
+// position ascending): the strict-maximum choice of pass 2 is then the smallest eligible rank.
+int aggregate_strong_ranked(int n, const int* srp, const int* sci, const uint16_t* rank, std::vector<int>& agg);
 
 // Full setup. Sparse products use Gustavson order (row i: k ascending in A(i,:), j ascending
 // in B(k,:), first touch assigns), run row-parallel, so the result is independent of threads.

@@ -152,6 +152,7 @@ void execute(cfdb_server& s, Resident& r, const Mesh& m, Request& q, bool create
     if (created) {
         check(cfdb_system_create_mesh(m.n, m.nf, m.owner.data(), m.neighbour.data(), &r.sys));
         check(cfdb_system_set_precision(r.sys, s.cfg.precision));
+        check(cfdb_system_set_keep_levels(r.sys, 0)); // the plan of a resident system never changes
         dmalloc(&r.d_diag, m.n);
         dmalloc(&r.d_upper, m.nf);
         dmalloc(&r.d_lower, m.nf);
@@ -162,11 +163,6 @@ void execute(cfdb_server& s, Resident& r, const Mesh& m, Request& q, bool create
     check(cfdb_system_stream(r.sys, &stream_v));
     cudaStream_t st = static_cast<cudaStream_t>(stream_v);
     const bool new_matrix = r.matrix_key != q.key || q.key < 0;
-    if (created || (s.cfg.max_age > 0 && r.age >= s.cfg.max_age)) {
-        // hierarchy (re)build from this request's matrix, as the reference's AmgCache does
-        check(cfdb_system_setup_amg(r.sys, q.diag, q.upper, q.lower, &s.cfg.settings));
-        r.age = 0;
-    }
     if (new_matrix) {
         CFDB_CUDA(cudaMemcpyAsync(r.d_diag, q.diag, sizeof(double) * m.n, cudaMemcpyHostToDevice, st));
         if (m.nf > 0) {
@@ -174,6 +170,13 @@ void execute(cfdb_server& s, Resident& r, const Mesh& m, Request& q, bool create
             CFDB_CUDA(cudaMemcpyAsync(r.d_lower, q.lower, sizeof(double) * m.nf, cudaMemcpyHostToDevice, st));
         }
         r.matrix_key = q.key;
+    }
+    if (created || (s.cfg.max_age > 0 && r.age >= s.cfg.max_age)) {
+        // hierarchy (re)build from this request's matrix (already on the device), as the
+        // reference's AmgCache does, with the sparse algebra on the GPU
+        CFDB_CUDA(cudaStreamSynchronize(st));
+        check(cfdb_system_setup_amg_device(r.sys, r.d_diag, r.d_upper, r.d_lower, &s.cfg.settings, 1));
+        r.age = 0;
     }
     CFDB_CUDA(cudaMemcpyAsync(r.d_rhs, q.rhs, sizeof(double) * m.n, cudaMemcpyHostToDevice, st));
     if (!(q.warm && r.solution_key == q.key && q.key >= 0)) {

@@ -195,6 +195,10 @@ int cfdb_system_setup_amg(cfdb_system* sys, const double* diag, const double* up
 int cfdb_system_setup_amg_device(cfdb_system* sys, const double* diag, const double* upper,
                                  const double* lower, const cfdb_amg_settings* settings,
                                  int device_arrays);
+/* Whether a device setup keeps its levels on the device (default 1). They let the plan be
+ * rebuilt (set_precision, set_tuning, set_ordered) without a new setup; without them such a
+ * change after a device setup fails with CFDB_ERR_NOT_READY until the next setup. */
+int cfdb_system_set_keep_levels(cfdb_system* sys, int keep);
 /* Wall-clock seconds of the phases of the last hierarchy setup of sys, as text
  * "phase=seconds;..." (host setup: hierarchy, plan; device setup: strength, aggregate,
  * prolongation, transpose, AP, RAP, coarse_inverse, input, keep, plan). */

@@ -109,7 +109,7 @@ def test_solve_after_device_setup_is_identical(gpu, precision):
         ds.set_precision(getattr(cb.Precision, precision))
         s = cb.AmgSettings(strength_threshold=0.04)
         if how == "host":
-            ds.setup_amg(diag, up, lo, s)
+            ds.setup_amg(diag, up, lo, s, device=False)
         elif how == "device":
             ds.setup_amg(diag, up, lo, s, device=True)
         else:
@@ -147,3 +147,21 @@ def test_plan_rebuild_from_device_levels(gpu):
         it_h, x_h = run(False, tuning)
         it_d, x_d = run(True, tuning)
         assert it_h == it_d and np.array_equal(x_h, x_d)
+
+
+def test_dropped_levels_refuse_replan(gpu):
+    """Without kept levels, a plan change after a device setup is refused until the next setup
+    (it cannot rebuild the operators), and a new setup restores it."""
+    cb = gpu
+    case = W.graded(10)
+    up, lo, diag, src = _pressure(case)
+    ds = cb.DeviceSolver(cb.build_csr_pattern(case.n, case.owner, case.neighbour))
+    ds.set_keep_levels(False)
+    ds.setup_amg(diag, up, lo)
+    x = np.zeros(case.n)
+    assert ds.solve(diag, up, lo, src, x, cb.Method.Cg, True, cb.SolveControl(1e-9, 100)).converged
+    with pytest.raises(cb.CfdbError):
+        ds.set_precision(cb.Precision.MIXED)
+    ds.setup_amg(diag, up, lo)
+    x[:] = 0.0
+    assert ds.solve(diag, up, lo, src, x, cb.Method.Cg, True, cb.SolveControl(1e-9, 100)).converged

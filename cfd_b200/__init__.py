@@ -66,6 +66,16 @@ class KernelRecordStruct(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("level", _i), ("ms", _d), ("bytes", _d)]
 
 
+class LduSettingsStruct(C.Structure):
+    _fields_ = [("method", _i), ("tolerance", _d), ("rel_tolerance", _d), ("max_iterations", _i),
+                ("max_age", _i)]
+
+
+class LduResultStruct(C.Structure):
+    _fields_ = [("initial_residual", _d), ("final_residual", _d), ("iterations", _i),
+                ("amg_rebuilt", _i)]
+
+
 class AmgSettingsStruct(C.Structure):
     _fields_ = [("strength_threshold", _d), ("max_levels", _i), ("coarse_size", _i),
                 ("smooth_sweeps", _i), ("jacobi_weight", _d), ("device_table_limit", _i)]
@@ -109,6 +119,8 @@ _proto("cfdb_system_setup_amg", [_vp, _pd, _pd, _pd, _P(AmgSettingsStruct)])
 _proto("cfdb_system_setup_amg_device", [_vp, _vp, _vp, _vp, _P(AmgSettingsStruct), _i])
 _proto("cfdb_system_setup_profile", [_vp, C.c_char_p, C.c_size_t])
 _proto("cfdb_system_set_keep_levels", [_vp, _i])
+_proto("cfdb_system_solve_ldu", [_vp, _vp, _vp, _vp, _vp, _vp, _P(LduSettingsStruct),
+                                 _P(AmgSettingsStruct), _i, _P(LduResultStruct)])
 _proto("cfdb_system_set_precision", [_vp, _i])
 _proto("cfdb_system_solve", [_vp, _pd, _pd, _pd, _pd, _pd, _i, _i, _P(ControlStruct),
                              _P(StatsStruct)])
@@ -447,6 +459,29 @@ def solve_device_noalloc(n, nnz, row_ptr, col, val, b, x, method: Method,
     return SolveStats._from(st)
 
 
+@dataclass
+class LduSettings:
+    """LinearSolverSettings (ldu_matrix.hpp:23-28) of the GPU path, with AmgCache::max_age."""
+    method: int = 0  # Method.Cg (GpuCg) or Method.BiCgStab (GpuBiCgStab)
+    tolerance: float = 1e-10
+    rel_tolerance: float = 0.01
+    max_iterations: int = 1000
+    max_age: int = 20
+
+    def _c(self):
+        return LduSettingsStruct(int(self.method), float(self.tolerance), float(self.rel_tolerance),
+                                 int(self.max_iterations), int(self.max_age))
+
+
+@dataclass
+class LduResult:
+    """LinearSolveResult (ldu_matrix.hpp:30-34) plus whether the call rebuilt the hierarchy."""
+    initial_residual: float
+    final_residual: float
+    iterations: int
+    amg_rebuilt: bool
+
+
 def build_csr_pattern(n, owner, neighbour) -> LduPattern:
     """fv::build_csr_pattern (ldu_matrix.cpp:572-612) from internal-face addressing."""
     nei = _i32(neighbour)
@@ -654,6 +689,32 @@ class DeviceSolver:
                                              _devptr(lower), _devptr(b), _devptr(x), int(method),
                                              1 if use_amg else 0, C.byref(ctl), C.byref(st)))
         return SolveStats._from(st)
+
+    def solve_ldu(self, diag, upper, lower, source, x, settings: LduSettings | None = None,
+                  amg: AmgSettings | None = None) -> LduResult:
+        """LduMatrix::solve on the GPU path with the AmgCache rule (ldu_matrix.cpp:111-131,
+        287-366): normalised residuals before and after, hierarchy (re)built on the device at
+        the first CG call and every max_age calls. Host numpy arrays (x updated in place) or
+        CUDA tensors (ready on the current stream)."""
+        s = (settings or LduSettings())._c()
+        a = (amg or AmgSettings())._c()
+        r = LduResultStruct()
+        if hasattr(diag, "is_cuda") and diag.is_cuda:
+            import torch
+            torch.cuda.current_stream().synchronize()
+            _check(_lib.cfdb_system_solve_ldu(self._h, _devptr(diag), _devptr(upper), _devptr(lower),
+                                              _devptr(source), _devptr(x), C.byref(s), C.byref(a), 1,
+                                              C.byref(r)))
+        else:
+            d, u, lo, b = _f64(diag), _f64(upper), _f64(lower), _f64(source)
+            _out_f64(x, "x")
+            if len(d) != self.n or len(b) != self.n or len(x) != self.n or \
+                    len(u) != self.n_faces or len(lo) != self.n_faces:
+                raise InvalidArgument("array sizes do not match the pattern")
+            _check(_lib.cfdb_system_solve_ldu(self._h, d.ctypes.data, u.ctypes.data, lo.ctypes.data,
+                                              b.ctypes.data, x.ctypes.data, C.byref(s), C.byref(a), 0,
+                                              C.byref(r)))
+        return LduResult(r.initial_residual, r.final_residual, r.iterations, bool(r.amg_rebuilt))
 
     def assemble_device(self, flux, gamma, delta, convection, upper, lower, diag, div) -> None:
         _check(_lib.cfdb_system_assemble_device(self._h, _devptr(flux), _devptr(gamma),

@@ -2,6 +2,7 @@
 #include "../../include/cfdb.h"
 
 #include <algorithm>
+#include <cmath>
 #include <climits>
 #include <cstring>
 #include <memory>
@@ -10,6 +11,7 @@
 
 #include "dsetup.hpp"
 #include "engine.hpp"
+#include "ldu_solve.hpp"
 #include "host_algos.hpp"
 
 using namespace cfdb;
@@ -179,6 +181,13 @@ struct cfdb_system {
     int* d_lpos = nullptr;
     std::string setup_profile; // phase times of the last hierarchy setup
     PinnedBuffer stage;        // page-locked staging of the device setup's read-backs
+    // persistent LDU solve (cfdb_system_solve_ldu): AmgCache state and device staging
+    int age = 0;               // CG solves since the last hierarchy setup
+    bool amg_built = false;    // a setup has run (its hierarchy may have one level)
+    int* d_src = nullptr;      // value map of the pattern entries (pat_arena)
+    DeviceArena ldu_arena;
+    double* ldu_stage = nullptr; // diag | upper | lower | source | x (host-array calls)
+    double* norm_part = nullptr;
 };
 
 namespace {
@@ -216,6 +225,19 @@ void ensure_engine(cfdb_system* s) {
     v.push_back(std::move(sp));
     s->eng->build(std::move(v), s->sweeps, s->weight, /*need64=*/!mixed, /*need32=*/mixed);
     s->dirty = false;
+}
+
+// Device copy of the system's pattern (uploaded once).
+void pattern_on_device(cfdb_system* sys, cudaStream_t st) {
+    if (sys->d_rp != nullptr) return;
+    const LduPatternHost& p = sys->pat;
+    sys->d_rp = sys->pat_arena.upload(p.row_ptr, st);
+    sys->d_ci = sys->pat_arena.upload(p.col, st);
+    sys->d_dpos = sys->pat_arena.upload(p.diag_pos, st);
+    sys->d_upos = sys->pat_arena.upload(p.upper_pos, st);
+    sys->d_lpos = sys->pat_arena.upload(p.lower_pos, st);
+    sys->d_src = sys->pat_arena.upload(sys->src, st);
+    CFDB_CUDA(cudaStreamSynchronize(st));
 }
 
 void validate_pattern(const cfdb_ldu_pattern& p) {
@@ -790,13 +812,7 @@ int cfdb_system_setup_amg_device(cfdb_system* sys, const double* diag, const dou
         const LduPatternHost& p = sys->pat;
         CFDB_CUDA(cudaSetDevice(sys->device));
         CallStream cs;
-        if (sys->d_rp == nullptr) {
-            sys->d_rp = sys->pat_arena.upload(p.row_ptr, cs.s);
-            sys->d_ci = sys->pat_arena.upload(p.col, cs.s);
-            sys->d_dpos = sys->pat_arena.upload(p.diag_pos, cs.s);
-            sys->d_upos = sys->pat_arena.upload(p.upper_pos, cs.s);
-            sys->d_lpos = sys->pat_arena.upload(p.lower_pos, cs.s);
-        }
+        pattern_on_device(sys, cs.s);
         DeviceHierarchy dh;
         const double *dd = diag, *du = upper, *dl = lower;
         if (!device_arrays) {
@@ -889,6 +905,87 @@ int cfdb_system_solve_device(cfdb_system* sys, const double* diag, const double*
         if (sys == nullptr) fail(CFDB_ERR_BAD_ARG, "null system");
         CFDB_CUDA(cudaSetDevice(sys->device));
         put_stats(stats, run_single(sys, diag, upper, lower, b, x, method, use_amg, control, true));
+    });
+}
+
+void cfdb_default_ldu_settings(cfdb_ldu_settings* s) {
+    if (s == nullptr) return;
+    s->method = CFDB_METHOD_CG;
+    s->tolerance = 1e-10;
+    s->rel_tolerance = 0.01;
+    s->max_iterations = 1000;
+    s->max_age = 20;
+}
+
+int cfdb_system_solve_ldu(cfdb_system* sys, const double* diag, const double* upper, const double* lower,
+                          const double* source, double* x, const cfdb_ldu_settings* settings,
+                          const cfdb_amg_settings* amg, int device_arrays, cfdb_ldu_result* result) {
+    return guarded([&] {
+        if (sys == nullptr || settings == nullptr || result == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
+        const LduPatternHost& p = sys->pat;
+        const int n = p.n, nf = p.n_faces;
+        if (diag == nullptr || source == nullptr || x == nullptr || (nf > 0 && (upper == nullptr || lower == nullptr)))
+            fail(CFDB_ERR_BAD_ARG, "null array");
+        if (settings->method != CFDB_METHOD_CG && settings->method != CFDB_METHOD_BICGSTAB)
+            fail(CFDB_ERR_BAD_ARG, "unknown method");
+        CFDB_CUDA(cudaSetDevice(sys->device));
+        ensure_engine(sys);
+        cudaStream_t st = sys->eng->stream();
+        pattern_on_device(sys, st);
+        if (sys->norm_part == nullptr) sys->norm_part = sys->ldu_arena.alloc<double>(3 * static_cast<size_t>(kLduNormBlocks));
+        const double *dd = diag, *du = upper, *dl = lower, *db = source;
+        double* dx = x;
+        if (!device_arrays) {
+            if (sys->ldu_stage == nullptr)
+                sys->ldu_stage = sys->ldu_arena.alloc<double>(4 * static_cast<size_t>(n) + 2 * static_cast<size_t>(nf));
+            double* s = sys->ldu_stage;
+            auto put = [&](double* dst, const double* src, int cnt) {
+                if (cnt > 0) CFDB_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * cnt, cudaMemcpyHostToDevice, st));
+            };
+            put(s, diag, n);
+            put(s + n, upper, nf);
+            put(s + n + nf, lower, nf);
+            put(s + n + 2 * nf, source, n);
+            put(s + 2 * n + 2 * nf, x, n);
+            dd = s;
+            du = s + n;
+            dl = s + n + nf;
+            db = s + n + 2 * nf;
+            dx = s + 2 * n + 2 * nf;
+        }
+        const LduDevice m{n, nf, sys->d_rp, sys->d_ci, sys->d_src};
+        // ldu_matrix.cpp:118-125: initial normalised residual; nothing to do below the tolerance
+        const LduNorms n0 = ldu_residual_norms(m, dd, du, dl, db, dx, sys->norm_part, st);
+        constexpr double kSmall = 1e-20; // ldu_matrix.cpp:22
+        *result = cfdb_ldu_result{};
+        result->initial_residual = n0.res / (n0.norm + kSmall);
+        result->final_residual = result->initial_residual;
+        if (result->initial_residual < settings->tolerance) return;
+        // ldu_matrix.cpp:293-301: absolute CG target from the relative and absolute tolerances
+        const double target = std::max(settings->rel_tolerance,
+                                       settings->tolerance / std::max(result->initial_residual, kSmall)) *
+                              std::sqrt(n0.r2);
+        const bool cg = settings->method == CFDB_METHOD_CG;
+        // ldu_matrix.cpp:314-353: (re)build the hierarchy at the first CG solve and after
+        // max_age solves, here on the device from this matrix
+        if (cg && (!sys->amg_built || sys->age >= settings->max_age)) {
+            const int rc = cfdb_system_setup_amg_device(sys, dd, du, dl, amg, 1);
+            if (rc != CFDB_OK) fail(rc, g_last_error);
+            sys->age = 0;
+            sys->amg_built = true;
+            result->amg_rebuilt = 1;
+        }
+        if (cg) ++sys->age;
+        const bool use_amg = cg && sys->h != nullptr;
+        const cfdb_control ctl{std::max(target, 1e-300), settings->max_iterations};
+        const SolveResult r = run_single(sys, dd, du, dl, db, dx, settings->method, use_amg ? 1 : 0, &ctl, true);
+        result->iterations = r.iterations;
+        const LduNorms n1 = ldu_residual_norms(m, dd, du, dl, db, dx, sys->norm_part, st);
+        result->final_residual = n1.res / (n1.norm + kSmall);
+        if (!device_arrays) {
+            CFDB_CUDA(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+            CFDB_CUDA(cudaStreamSynchronize(st));
+        }
     });
 }
 

@@ -110,6 +110,43 @@ void DeviceSolver::set_mixed_precision(bool mixed) {
 
 void* DeviceSolver::handle() const { return impl_->sys; }
 
+namespace {
+cfdb_amg_settings amg_c(const AmgSetupSettings& a) {
+    cfdb_amg_settings s{};
+    cfdb_default_amg_settings(&s);
+    s.strength_threshold = a.strength_threshold;
+    s.max_levels = a.max_levels;
+    s.coarse_size = a.coarse_size;
+    return s;
+}
+} // namespace
+
+void DeviceSolver::setup_amg(const double* diag, const double* upper, const double* lower,
+                             const AmgSetupSettings& settings) {
+    const cfdb_amg_settings s = amg_c(settings);
+    check(cfdb_system_setup_amg_device(impl_->sys, diag, upper, lower, &s, 0));
+}
+
+LduSolveResult DeviceSolver::solve_ldu(const double* diag, const double* upper, const double* lower,
+                                       const double* source, double* x, const LduSolveSettings& settings,
+                                       const AmgSetupSettings& amg) {
+    cfdb_ldu_settings ls{};
+    ls.method = method_c(settings.method);
+    ls.tolerance = settings.tolerance;
+    ls.rel_tolerance = settings.rel_tolerance;
+    ls.max_iterations = settings.max_iterations;
+    ls.max_age = settings.max_age;
+    const cfdb_amg_settings as = amg_c(amg);
+    cfdb_ldu_result r{};
+    check(cfdb_system_solve_ldu(impl_->sys, diag, upper, lower, source, x, &ls, &as, 0, &r));
+    LduSolveResult o;
+    o.initial_residual = r.initial_residual;
+    o.final_residual = r.final_residual;
+    o.iterations = r.iterations;
+    o.amg_rebuilt = r.amg_rebuilt != 0;
+    return o;
+}
+
 void assemble_convection_diffusion(int n_cells, int n_faces, const int* owner, const int* neighbour,
                                    const double* flux, const double* gamma, const double* delta_coeff,
                                    double convection, double* upper, double* lower, double* diag,

@@ -76,6 +76,29 @@ struct LduPattern {
     const int* lower_pos = nullptr;
 };
 
+// Extensions (no reference counterpart) used by DeviceSolver::setup_amg / solve_ldu below.
+// amg.hpp:17-23 AmgSettings.
+struct AmgSetupSettings {
+    double strength_threshold = 0.08;
+    int max_levels = 25;
+    int coarse_size = 400;
+};
+// ldu_matrix.hpp:23-28 LinearSolverSettings of the GPU path, with AmgCache::max_age.
+struct LduSolveSettings {
+    Method method = Method::Cg;  // LinearSolverType::GpuCg (AMG-CG) or GpuBiCgStab
+    double tolerance = 1e-10;    // absolute, on the normalised residual
+    double rel_tolerance = 0.01; // relative to the initial normalised residual
+    int max_iterations = 1000;
+    int max_age = 20;            // hierarchy rebuilt after this many CG solves
+};
+// ldu_matrix.hpp:30-34 LinearSolveResult.
+struct LduSolveResult {
+    double initial_residual = 0.0;
+    double final_residual = 0.0;
+    int iterations = 0;
+    bool amg_rebuilt = false;
+};
+
 // krylov.hpp:83-103: persistent solver on one pattern; the device matrix is assembled from
 // LDU coefficients on every solve and the AMG hierarchy stays resident between set_amg calls.
 class DeviceSolver {
@@ -97,6 +120,16 @@ public:
     // reference algorithm; true: FP32 V-cycle inside FP64 flexible CG) and the C handle.
     void set_mixed_precision(bool mixed);
     [[nodiscard]] void* handle() const;
+    // AmgPreconditioner::setup of the LDU matrix on the GPU and installation of the hierarchy
+    // (replaces the host setup + set_amg of LduMatrix::solve_persistent, ldu_matrix.cpp:314-353).
+    void setup_amg(const double* diag, const double* upper, const double* lower,
+                   const AmgSetupSettings& settings = {});
+    // LduMatrix::solve with the GPU path and its AmgCache (ldu_matrix.cpp:111-131, 287-366):
+    // normalised residuals on the device, hierarchy (re)built on the device every max_age CG
+    // solves. Host arrays; x is the initial guess in and the solution out.
+    LduSolveResult solve_ldu(const double* diag, const double* upper, const double* lower,
+                             const double* source, double* x, const LduSolveSettings& settings,
+                             const AmgSetupSettings& amg = {});
 
 private:
     struct Impl;

@@ -213,6 +213,33 @@ int cfdb_system_solve(cfdb_system* sys, const double* diag, const double* upper,
 int cfdb_system_solve_device(cfdb_system* sys, const double* diag, const double* upper,
                              const double* lower, const double* b, double* x, int method,
                              int use_amg, const cfdb_control* control, cfdb_stats* stats);
+/* ---- persistent LDU solve: LduMatrix::solve with "solver": {"device": "gpu"}
+ * (ldu_matrix.cpp:111-131 with solve_persistent, ldu_matrix.cpp:287-366) ---- */
+typedef struct {
+    int method;           /* CFDB_METHOD_CG (LinearSolverType::GpuCg: AMG-CG) or
+                             CFDB_METHOD_BICGSTAB (GpuBiCgStab: Jacobi BiCGStab) */
+    double tolerance;     /* absolute, on the normalised residual (1e-10) */
+    double rel_tolerance; /* relative to the initial normalised residual (0.01) */
+    int max_iterations;   /* 1000 */
+    int max_age;          /* AmgCache::max_age: hierarchy rebuilt after this many CG solves (20) */
+} cfdb_ldu_settings;
+typedef struct {
+    double initial_residual; /* LinearSolveResult: normalised residuals before and after */
+    double final_residual;
+    int iterations;
+    int amg_rebuilt;         /* 1 when this call (re)built the hierarchy */
+} cfdb_ldu_result;
+void cfdb_default_ldu_settings(cfdb_ldu_settings* s);
+/* Solves A x = source for the LDU matrix (x: initial guess in, solution out) with the
+ * reference's stopping rule: returns at once when the normalised residual of x is below
+ * `tolerance`; otherwise CG/BiCGStab runs to max(rel_tolerance, tolerance / initial) times the
+ * initial residual 2-norm. With CG the hierarchy is built (on the device) at the first call and
+ * again every max_age solves; a one-level hierarchy runs Jacobi CG (ldu_matrix.cpp:358).
+ * device_arrays: all arrays are device pointers (else host arrays, copied once per call). */
+int cfdb_system_solve_ldu(cfdb_system* sys, const double* diag, const double* upper,
+                          const double* lower, const double* source, double* x,
+                          const cfdb_ldu_settings* settings, const cfdb_amg_settings* amg,
+                          int device_arrays, cfdb_ldu_result* result);
 /* Fused pressure assembly on device arrays (flow_solver.cpp:757-783 with the face loop of
  * krylov_cuda.cu:681-697): from face flux / gamma / delta (n_faces) builds the device matrix
  * directly and returns upper, lower (n_faces) and diag, divergence (n_cells, accumulated)

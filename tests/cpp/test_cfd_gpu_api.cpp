@@ -208,6 +208,32 @@ static void check_device() {
         const g::SolveStats s3 = ds.solve(dg.data(), up.data(), lo.data(), rhs.data(), xj.data(), g::Method::Cg, false, c2);
         CHECK(s3.converged && s3.iterations > s2.iterations);
     }
+    // extensions: hierarchy built on the device, and LduMatrix::solve with its AmgCache
+    {
+        g::DeviceSolver dd(pat);
+        g::AmgSetupSettings as;
+        as.strength_threshold = 0.04;
+        dd.setup_amg(dg.data(), up.data(), lo.data(), as);
+        std::vector<double> xd(m.n_cells, 0.0);
+        g::SolveControl c4;
+        c4.abs_tolerance = 1e-8 * norm(rhs);
+        c4.max_iterations = 200;
+        const g::SolveStats s4 = dd.solve(dg.data(), up.data(), lo.data(), rhs.data(), xd.data(), g::Method::Cg, true, c4);
+        CHECK(s4.converged && s4.iterations < 60);
+        g::LduSolveSettings ls;
+        ls.tolerance = 1e-14;
+        ls.rel_tolerance = 1e-8;
+        ls.max_age = 2;
+        bool pattern_ok = true;
+        for (int call = 0; call < 3; ++call) {
+            std::vector<double> xl(m.n_cells, 0.0);
+            const g::LduSolveResult r = dd.solve_ldu(dg.data(), up.data(), lo.data(), rhs.data(), xl.data(), ls, as);
+            pattern_ok = pattern_ok && r.amg_rebuilt == (call != 1) && r.iterations > 0;
+            CHECK(r.initial_residual > 0.0 && r.final_residual < 1e-6 * r.initial_residual);
+            CHECK(residual(A, rhs, xl) <= 1.01e-8 * norm(rhs));
+        }
+        CHECK(pattern_ok);
+    }
     cfdb_hierarchy_destroy(h);
 }
 

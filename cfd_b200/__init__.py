@@ -119,6 +119,7 @@ _proto("cfdb_system_setup_amg", [_vp, _pd, _pd, _pd, _P(AmgSettingsStruct)])
 _proto("cfdb_system_setup_amg_device", [_vp, _vp, _vp, _vp, _P(AmgSettingsStruct), _i])
 _proto("cfdb_system_setup_profile", [_vp, C.c_char_p, C.c_size_t])
 _proto("cfdb_system_set_keep_levels", [_vp, _i])
+_proto("cfdb_system_time_sweep", [_vp, _i, _i, _pd, _pd])
 _proto("cfdb_system_solve_ldu", [_vp, _vp, _vp, _vp, _vp, _vp, _P(LduSettingsStruct),
                                  _P(AmgSettingsStruct), _i, _P(LduResultStruct)])
 _proto("cfdb_system_set_precision", [_vp, _i])
@@ -530,7 +531,7 @@ class AmgHierarchy:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:  # the library may be gone at interpreter exit
             _lib.cfdb_hierarchy_destroy(h)
             self._h = None
 
@@ -614,7 +615,7 @@ class DeviceSolver:
 
     def close(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:  # the library may be gone at interpreter exit
             _lib.cfdb_system_destroy(h)
             self._h = None
 
@@ -646,6 +647,13 @@ class DeviceSolver:
         d, u, lo = _f64(diag), _f64(upper), _f64(lower)
         _check(_lib.cfdb_system_setup_amg_device(self._h, d.ctypes.data, u.ctypes.data,
                                                  lo.ctypes.data, C.byref(s), 0))
+
+    def time_sweep(self, level: int, reps: int = 20):
+        """(ms, algorithmic bytes) of one Jacobi sweep of `level`, timed over `reps`
+        back-to-back launches with CUDA events."""
+        ms, by = C.c_double(), C.c_double()
+        _check(_lib.cfdb_system_time_sweep(self._h, int(level), int(reps), C.byref(ms), C.byref(by)))
+        return ms.value, by.value
 
     def set_keep_levels(self, keep: bool) -> None:
         """Keep a device setup's levels on the device so that later precision or tuning changes
@@ -829,7 +837,7 @@ class Batch:
 
     def close(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:  # the library may be gone at interpreter exit
             _lib.cfdb_batch_destroy(h)
             self._h = None
 
@@ -958,7 +966,7 @@ class Mesh:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:  # the library may be gone at interpreter exit
             _lib.cfdb_mesh_destroy(h)
             self._h = None
 

@@ -2,6 +2,7 @@
 #include "../../include/cfdb.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <climits>
 #include <cstring>
@@ -149,10 +150,18 @@ Tuning tuning_from(const cfdb_tuning* t) {
 // system object
 // ------------------------------------------------------------------------------------------------
 
+namespace {
+long long next_layout_id() {
+    static std::atomic<long long> next{1};
+    return next++;
+}
+} // namespace
+
 struct cfdb_system {
     int device = 0;
     LduPatternHost pat;
     std::vector<int> owner, neighbour; // kept when created from mesh addressing
+    long long layout_id = next_layout_id(); // the pattern and value maps never change
     std::unique_ptr<Engine> eng;
     std::shared_ptr<const Hierarchy> h;
     std::shared_ptr<const DeviceLevels> dl; // device-resident levels of a device setup
@@ -215,8 +224,9 @@ void ensure_engine(cfdb_system* s) {
     sp.n = s->pat.n;
     sp.rp = s->pat.row_ptr.data();
     sp.ci = s->pat.col.data();
-    sp.src = s->src;
-    sp.diag_src = s->diag_src;
+    sp.src_ref = &s->src;
+    sp.diag_src_ref = &s->diag_src;
+    sp.layout_id = s->layout_id;
     sp.vs_len = s->pat.n + 2 * s->pat.n_faces;
     sp.h = s->h;
     sp.dl = s->h ? s->dl : nullptr;
@@ -836,12 +846,13 @@ int cfdb_system_setup_amg_device(cfdb_system* sys, const double* diag, const dou
         CFDB_CUDA(cudaMemsetAsync(a0.va, 0, sizeof(double) * p.nnz(), cs.s));
         ldu_to_csr_values(p.n, p.n_faces, sys->d_dpos, sys->d_upos, sys->d_lpos, dd, du, dl, a0.va, cs.s);
         const double t0 = PhaseTimes::now();
-        amg_setup_device(a0, s, cs.s, dh, &sys->stage);
+        // the hierarchy's own arrays go to an arena the system keeps: the plan is laid out on
+        // the device from them, and plan rebuilds need no host copy
+        auto kept = std::make_shared<DeviceLevels>();
+        amg_setup_device(a0, s, cs.s, dh, &sys->stage, &kept->mem);
         const double t1 = PhaseTimes::now();
         dh.times.add("input", t0 - t_in);
-        // the plan is laid out on the device from compact copies of the levels, which the
-        // system keeps (plan rebuilds need no host copy)
-        auto kept = keep_levels(dh, cs.s);
+        adopt_levels(dh, *kept);
         auto h = std::make_shared<Hierarchy>(hierarchy_shape(dh));
         const double t2 = PhaseTimes::now();
         dh.times.add("keep", t2 - t1);
@@ -862,6 +873,15 @@ int cfdb_system_setup_amg_device(cfdb_system* sys, const double* diag, const dou
         dh.times.add("plan", PhaseTimes::now() - t2);
         for (const auto& pt : sys->eng->build_times().t) dh.times.add(pt.first, pt.second);
         sys->setup_profile = dh.times.text();
+    });
+}
+
+int cfdb_system_time_sweep(cfdb_system* sys, int level, int reps, double* ms, double* bytes) {
+    return guarded([&] {
+        if (sys == nullptr || ms == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
+        CFDB_CUDA(cudaSetDevice(sys->device));
+        ensure_engine(sys);
+        *ms = sys->eng->time_sweep(level, reps, bytes);
     });
 }
 

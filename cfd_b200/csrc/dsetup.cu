@@ -406,15 +406,25 @@ __global__ void k_gemm_bound(int n, const int* __restrict__ arp, const int* __re
     ub[i] = static_cast<int>(u < n_cols ? u : n_cols);
 }
 
-// rows into four classes by measure: <= lim0, <= lim1, <= lim2, larger (lists[c * n + ...])
-__global__ void k_classify(int n, const int* __restrict__ m, int lim0, int lim1, int lim2, int* lists, int* counts) {
+// Table-size classes of a row (distinct columns, or entries of a row to sort), smallest first:
+// (threads per row, shared-memory slots, rows per CTA); the last class uses device memory.
+constexpr int kClasses = 6;
+struct Limits {
+    int lim[kClasses - 1]; // class q holds measures <= lim[q] (and > lim[q - 1])
+};
+
+// rows into classes by measure (lists[c * n + ...]); counts[c] rows in class c
+__global__ void k_classify(int n, const int* __restrict__ m, Limits L, int* lists, int* counts) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int v = m[i];
-    const int c = v <= lim0 ? 0 : v <= lim1 ? 1 : v <= lim2 ? 2 : 3;
+    int c = kClasses - 1;
+    for (int q = kClasses - 2; q >= 0; --q)
+        if (v <= L.lim[q]) c = q;
     lists[static_cast<size_t>(c) * n + atomicAdd(&counts[c], 1)] = i;
 }
 
+// rows of a list whose count is at most `lim` (symbolic retry: rows a smaller table rejected)
 // smoothed prolongator rows from C = (D^-1 A) P_tent (sorted): count (FILL = false) or write
 template <bool FILL>
 __global__ void k_p_emit(int n, const int* __restrict__ crp, const int* __restrict__ cci,
@@ -537,11 +547,9 @@ __global__ void k_nz_compact(int n, const int* __restrict__ rp, const int* __res
 // host drivers
 // ---------------------------------------------------------------------------------------------
 
-// Table-size classes: (threads per row, shared slots, rows per CTA)
-constexpr int kCap0 = 64, kCap1 = 512, kCap2 = 8192;
-constexpr int kPer0 = 8, kPer1 = 4;
-// a class holds rows with at most 3/4 of its slots filled
-constexpr int kLim0 = kCap0 - kCap0 / 4, kLim1 = kCap1 - kCap1 / 4, kLim2 = kCap2 - kCap2 / 4;
+// Shared-memory table classes: slots per table, and the largest measure each takes (3/4 full)
+constexpr int kCap[kClasses - 1] = {64, 128, 512, 2048, 8192};
+constexpr int kFill[kClasses - 1] = {48, 96, 384, 1536, 6144};
 // device-memory tables are processed in batches of at most this many slots
 constexpr long long kGlobalSlots = 64LL << 20;
 
@@ -549,9 +557,11 @@ struct Ctx {
     cudaStream_t st;
     Scratch* mem;
     long long* d_total;
-    int* d_counts; // 4 class counters + overflow counter
+    int* d_counts; // class counters (kClasses) + one spare
     int* d_err;
     int lim;       // largest row (distinct columns / entries) given a shared-memory table
+    DeviceArena* keep = nullptr; // where the hierarchy's own arrays go (null: mem)
+    template <class T> T* out(size_t count) { return keep != nullptr ? keep->alloc<T>(count) : mem->alloc<T>(count); }
 };
 
 template <class T> void to_host(std::vector<T>& h, const T* d, size_t n, cudaStream_t st) {
@@ -586,15 +596,18 @@ int checked_nnz(long long total, const char* what) {
 // Rows of class lists: counts after k_classify (host copy).
 struct Classes {
     int* lists = nullptr;
-    int count[4] = {0, 0, 0, 0};
+    int count[kClasses] = {};
 };
 
-Classes classify(Ctx& cx, int n, const int* measure, int lim0, int lim1, int lim2) {
+// limits lim[q] = min(base[q], cx.lim); classes above the limit stay empty
+Classes classify(Ctx& cx, int n, const int* measure, const int (&base)[kClasses - 1]) {
+    Limits L;
+    for (int q = 0; q < kClasses - 1; ++q) L.lim[q] = std::min(base[q], cx.lim);
     Classes c;
-    c.lists = cx.mem->alloc<int>(4 * static_cast<size_t>(std::max(n, 1)));
-    CFDB_CUDA(cudaMemsetAsync(cx.d_counts, 0, 5 * sizeof(int), cx.st));
-    if (n > 0) k_classify<<<grid_for(n), kThreads, 0, cx.st>>>(n, measure, lim0, lim1, lim2, c.lists, cx.d_counts);
-    CFDB_CUDA(cudaMemcpyAsync(c.count, cx.d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, cx.st));
+    c.lists = cx.mem->alloc<int>(kClasses * static_cast<size_t>(std::max(n, 1)));
+    CFDB_CUDA(cudaMemsetAsync(cx.d_counts, 0, (kClasses + 1) * sizeof(int), cx.st));
+    if (n > 0) k_classify<<<grid_for(n), kThreads, 0, cx.st>>>(n, measure, L, c.lists, cx.d_counts);
+    CFDB_CUDA(cudaMemcpyAsync(c.count, cx.d_counts, kClasses * sizeof(int), cudaMemcpyDeviceToHost, cx.st));
     sync(cx.st);
     return c;
 }
@@ -637,6 +650,34 @@ template <class K> void set_smem(K kernel, size_t bytes) {
     }
 }
 
+// One Gustavson kernel launch over the rows of a list, with the table class `cls` (0..4).
+template <bool NUMERIC> void gemm_launch(Ctx& cx, GemmArgs g, int cls, const int* rows, int n_list) {
+    if (n_list <= 0) return;
+    g.rows = rows;
+    g.n_list = n_list;
+    const size_t b = NUMERIC ? 12 : 4; // bytes per slot
+    cudaStream_t st = cx.st;
+    switch (cls) {
+    case 0:
+        k_gemm_rows<NUMERIC, 32, 64, 8><<<(n_list + 7) / 8, 256, 8 * 64 * b, st>>>(g);
+        break;
+    case 1:
+        k_gemm_rows<NUMERIC, 32, 128, 8><<<(n_list + 7) / 8, 256, 8 * 128 * b, st>>>(g);
+        break;
+    case 2:
+        k_gemm_rows<NUMERIC, 32, 512, 4><<<(n_list + 3) / 4, 128, 4 * 512 * b, st>>>(g);
+        break;
+    case 3:
+        k_gemm_rows<NUMERIC, kThreads, 2048, 1><<<n_list, kThreads, 2048 * b, st>>>(g);
+        break;
+    default:
+        set_smem(k_gemm_rows<NUMERIC, kThreads, 8192, 1>, 8192 * b);
+        k_gemm_rows<NUMERIC, kThreads, 8192, 1><<<n_list, kThreads, 8192 * b, st>>>(g);
+        break;
+    }
+    CFDB_CUDA(cudaGetLastError());
+}
+
 // C = diag(ascale) A B (B explicit, or the tentative prolongator of `tent` when b == null).
 DevCsr spgemm(Ctx& cx, const DevCsr& a, const double* ascale, const DevCsr* b, const int* tent, int n_cols) {
     const int n = a.n_rows;
@@ -654,49 +695,43 @@ DevCsr spgemm(Ctx& cx, const DevCsr& a, const double* ascale, const DevCsr* b, c
     g.bva = b != nullptr ? b->va : nullptr;
     g.tent = tent;
     g.err = cx.d_err;
-    // symbolic: classes by the bound min(sum |B(k,:)|, n_cols)
+    // symbolic: rows whose bound min(sum_k |B(k,:)|, n_cols) fits the two smallest tables go
+    // there; the others start in the 512-slot warp tables and move to larger tables when they
+    // fill up (the bound is loose: most such rows have far fewer distinct columns)
     int* ub = cx.mem->alloc<int>(std::max(n, 1));
     if (n > 0) k_gemm_bound<<<grid_for(n), kThreads, 0, st>>>(n, a.rp, a.ci, g.brp, n_cols, ub);
     int* cnt = cx.mem->alloc<int>(static_cast<size_t>(n) + 1);
-    const Classes sc = classify(cx, n, ub, std::min(kLim0, cx.lim), std::min(kLim1, cx.lim), INT_MAX);
     g.cnt = cnt;
-    g.limit = std::min(kLim2, cx.lim);
-    int* over_rows = cx.mem->alloc<int>(std::max(sc.count[2], 1));
-    int* n_over = cx.d_counts + 4;
-    CFDB_CUDA(cudaMemsetAsync(n_over, 0, sizeof(int), st));
-    if (sc.count[0] > 0) {
-        g.rows = sc.lists;
-        g.n_list = sc.count[0];
-        k_gemm_rows<false, 32, kCap0, kPer0><<<(g.n_list + kPer0 - 1) / kPer0, 32 * kPer0, kPer0 * kCap0 * sizeof(int), st>>>(g);
-    }
-    if (sc.count[1] > 0) {
-        g.rows = sc.lists + n;
-        g.n_list = sc.count[1];
-        k_gemm_rows<false, 32, kCap1, kPer1><<<(g.n_list + kPer1 - 1) / kPer1, 32 * kPer1, kPer1 * kCap1 * sizeof(int), st>>>(g);
-    }
-    if (sc.count[2] > 0) {
-        g.rows = sc.lists + 2 * static_cast<size_t>(n);
-        g.n_list = sc.count[2];
-        g.over_rows = over_rows;
-        g.n_over = n_over;
-        k_gemm_rows<false, kThreads, kCap2, 1><<<g.n_list, kThreads, kCap2 * sizeof(int), st>>>(g);
-        g.over_rows = nullptr;
-        g.n_over = nullptr;
-    }
-    CFDB_CUDA(cudaGetLastError());
-    int h_over = 0;
-    CFDB_CUDA(cudaMemcpyAsync(&h_over, n_over, sizeof(int), cudaMemcpyDeviceToHost, st));
-    sync(st);
-    if (h_over > 0) {
-        std::vector<int> rows, bound;
-        to_host(rows, over_rows, static_cast<size_t>(h_over), st);
+    const Classes sc = classify(cx, n, ub, kFill);
+    g.limit = INT_MAX;
+    gemm_launch<false>(cx, g, 0, sc.lists, sc.count[0]);
+    gemm_launch<false>(cx, g, 1, sc.lists + n, sc.count[1]);
+    int* over[2] = {cx.mem->alloc<int>(std::max(n, 1)), cx.mem->alloc<int>(std::max(n, 1))};
+    int* n_over = cx.mem->alloc<int>(2);
+    int pending = 0, cur = 0;
+    for (int q = 2; q < kClasses; ++q) pending += sc.count[q];
+    for (int cls = 2; cls < kClasses - 1 && pending > 0; ++cls) {
+        CFDB_CUDA(cudaMemsetAsync(n_over + cur, 0, sizeof(int), st));
+        GemmArgs h = g;
+        h.limit = std::min(kFill[cls], cx.lim);
+        h.over_rows = over[cur];
+        h.n_over = n_over + cur;
+        if (cls == 2) {
+            for (int q = 2; q < kClasses; ++q) gemm_launch<false>(cx, h, 2, sc.lists + static_cast<size_t>(q) * n, sc.count[q]);
+        } else {
+            gemm_launch<false>(cx, h, cls, over[1 - cur], pending);
+        }
+        CFDB_CUDA(cudaMemcpyAsync(&pending, n_over + cur, sizeof(int), cudaMemcpyDeviceToHost, st));
         sync(st);
-        std::vector<int> ub_h(rows.size());
-        for (size_t q = 0; q < rows.size(); ++q)
-            CFDB_CUDA(cudaMemcpyAsync(&ub_h[q], ub + rows[q], sizeof(int), cudaMemcpyDeviceToHost, st));
+        cur = 1 - cur;
+    }
+    if (pending > 0) { // rows beyond every shared-memory table: device-memory tables
+        std::vector<int> rows, ub_h;
+        to_host(rows, over[1 - cur], static_cast<size_t>(pending), st);
+        to_host(ub_h, ub, static_cast<size_t>(n), st);
         sync(st);
         std::vector<int> caps(rows.size());
-        for (size_t q = 0; q < rows.size(); ++q) caps[q] = next_pow2(2LL * std::max(ub_h[q], 1));
+        for (size_t q = 0; q < rows.size(); ++q) caps[q] = next_pow2(2LL * std::max(ub_h[rows[q]], 1));
         global_batches(cx, rows, caps, false, [&](int* d_rows, int nb, long long* d_off, int* d_cap, int* keys, double*) {
             GemmArgs h = g;
             h.rows = d_rows;
@@ -714,37 +749,20 @@ DevCsr spgemm(Ctx& cx, const DevCsr& a, const double* ascale, const DevCsr* b, c
     c.ci = cx.mem->alloc<int>(static_cast<size_t>(c.nnz) + 4);
     c.va = cx.mem->alloc<double>(static_cast<size_t>(c.nnz) + 4);
     // numeric: classes by the exact count
-    const Classes nc = classify(cx, n, cnt, std::min(kLim0, cx.lim), std::min(kLim1, cx.lim), std::min(kLim2, cx.lim));
+    const Classes nc = classify(cx, n, cnt, kFill);
     g.crp = c.rp;
     g.cci = c.ci;
     g.cva = c.va;
-    if (nc.count[0] > 0) {
-        g.rows = nc.lists;
-        g.n_list = nc.count[0];
-        k_gemm_rows<true, 32, kCap0, kPer0><<<(g.n_list + kPer0 - 1) / kPer0, 32 * kPer0, kPer0 * kCap0 * 12, st>>>(g);
-    }
-    if (nc.count[1] > 0) {
-        g.rows = nc.lists + n;
-        g.n_list = nc.count[1];
-        k_gemm_rows<true, 32, kCap1, kPer1><<<(g.n_list + kPer1 - 1) / kPer1, 32 * kPer1, kPer1 * kCap1 * 12, st>>>(g);
-    }
-    if (nc.count[2] > 0) {
-        g.rows = nc.lists + 2 * static_cast<size_t>(n);
-        g.n_list = nc.count[2];
-        set_smem(k_gemm_rows<true, kThreads, kCap2, 1>, kCap2 * 12);
-        k_gemm_rows<true, kThreads, kCap2, 1><<<g.n_list, kThreads, kCap2 * 12, st>>>(g);
-    }
-    CFDB_CUDA(cudaGetLastError());
-    if (nc.count[3] > 0) {
-        std::vector<int> rows;
-        to_host(rows, nc.lists + 3 * static_cast<size_t>(n), static_cast<size_t>(nc.count[3]), st);
+    for (int q = 0; q < kClasses - 1; ++q) gemm_launch<true>(cx, g, q, nc.lists + static_cast<size_t>(q) * n, nc.count[q]);
+    if (nc.count[kClasses - 1] > 0) {
+        std::vector<int> rows, rp_h;
+        to_host(rows, nc.lists + static_cast<size_t>(kClasses - 1) * n, static_cast<size_t>(nc.count[kClasses - 1]), st);
+        to_host(rp_h, c.rp, static_cast<size_t>(n) + 1, st);
         sync(st);
         std::vector<int> caps(rows.size());
-        std::vector<int> rp_h(2);
         for (size_t q = 0; q < rows.size(); ++q) {
-            CFDB_CUDA(cudaMemcpyAsync(rp_h.data(), c.rp + rows[q], 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
-            sync(st);
-            caps[q] = next_pow2((4LL * (rp_h[1] - rp_h[0]) + 2) / 3 + 1);
+            const long long len = rp_h[rows[q] + 1] - rp_h[rows[q]];
+            caps[q] = next_pow2((4 * len + 2) / 3 + 1);
         }
         global_batches(cx, rows, caps, true, [&](int* d_rows, int nb, long long* d_off, int* d_cap, int* keys, double* vals) {
             GemmArgs h = g;
@@ -761,40 +779,31 @@ DevCsr spgemm(Ctx& cx, const DevCsr& a, const double* ascale, const DevCsr* b, c
     return c;
 }
 
-DevCsr transpose(Ctx& cx, const DevCsr& a) {
+// Sorts every row of t by column, with the table class of its length.
+void sort_rows(Ctx& cx, DevCsr& t) {
     cudaStream_t st = cx.st;
-    DevCsr t;
-    t.n_rows = a.n_cols;
-    t.n_cols = a.n_rows;
-    const int m = a.n_cols;
-    int* cnt = cx.mem->alloc<int>(static_cast<size_t>(m) + 1);
-    CFDB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (static_cast<size_t>(m) + 1), st));
-    if (a.nnz > 0) k_col_count<<<grid_for(a.nnz), kThreads, 0, st>>>(a.nnz, a.ci, cnt);
-    t.rp = cx.mem->alloc<int>(static_cast<size_t>(m) + 1);
-    t.nnz = checked_nnz(scan(cx, cnt, m, t.rp), "a transpose");
-    t.ci = cx.mem->alloc<int>(static_cast<size_t>(t.nnz) + 4);
-    t.va = cx.mem->alloc<double>(static_cast<size_t>(t.nnz) + 4);
-    CFDB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (static_cast<size_t>(m) + 1), st));
-    if (a.n_rows > 0) k_t_fill<<<grid_for(a.n_rows), kThreads, 0, st>>>(a.n_rows, a.rp, a.ci, a.va, t.rp, cnt, t.ci, t.va);
-    // sort each row by column: classes by length
+    const int m = t.n_rows;
     int* len = cx.mem->alloc<int>(std::max(m, 1));
     if (m > 0) k_row_len<<<grid_for(m), kThreads, 0, st>>>(m, t.rp, len);
-    const Classes c = classify(cx, m, len, std::min(kCap0, cx.lim), std::min(kCap1, cx.lim), std::min(kCap2, cx.lim));
+    const Classes c = classify(cx, m, len, kCap);
+    auto lst = [&](int q) { return c.lists + static_cast<size_t>(q) * m; };
+    const size_t b = 12;
     if (c.count[0] > 0)
-        k_seg_sort<32, kCap0, kPer0><<<(c.count[0] + kPer0 - 1) / kPer0, 32 * kPer0, kPer0 * kCap0 * 12, st>>>(
-            c.lists, c.count[0], t.rp, t.ci, t.va, nullptr, nullptr, nullptr, nullptr);
+        k_seg_sort<32, 64, 8><<<(c.count[0] + 7) / 8, 256, 8 * 64 * b, st>>>(lst(0), c.count[0], t.rp, t.ci, t.va, nullptr, nullptr, nullptr, nullptr);
     if (c.count[1] > 0)
-        k_seg_sort<32, kCap1, kPer1><<<(c.count[1] + kPer1 - 1) / kPer1, 32 * kPer1, kPer1 * kCap1 * 12, st>>>(
-            c.lists + m, c.count[1], t.rp, t.ci, t.va, nullptr, nullptr, nullptr, nullptr);
-    if (c.count[2] > 0) {
-        set_smem(k_seg_sort<kThreads, kCap2, 1>, kCap2 * 12);
-        k_seg_sort<kThreads, kCap2, 1><<<c.count[2], kThreads, kCap2 * 12, st>>>(
-            c.lists + 2 * static_cast<size_t>(m), c.count[2], t.rp, t.ci, t.va, nullptr, nullptr, nullptr, nullptr);
+        k_seg_sort<32, 128, 8><<<(c.count[1] + 7) / 8, 256, 8 * 128 * b, st>>>(lst(1), c.count[1], t.rp, t.ci, t.va, nullptr, nullptr, nullptr, nullptr);
+    if (c.count[2] > 0)
+        k_seg_sort<32, 512, 4><<<(c.count[2] + 3) / 4, 128, 4 * 512 * b, st>>>(lst(2), c.count[2], t.rp, t.ci, t.va, nullptr, nullptr, nullptr, nullptr);
+    if (c.count[3] > 0)
+        k_seg_sort<kThreads, 2048, 1><<<c.count[3], kThreads, 2048 * b, st>>>(lst(3), c.count[3], t.rp, t.ci, t.va, nullptr, nullptr, nullptr, nullptr);
+    if (c.count[4] > 0) {
+        set_smem(k_seg_sort<kThreads, 8192, 1>, 8192 * b);
+        k_seg_sort<kThreads, 8192, 1><<<c.count[4], kThreads, 8192 * b, st>>>(lst(4), c.count[4], t.rp, t.ci, t.va, nullptr, nullptr, nullptr, nullptr);
     }
     CFDB_CUDA(cudaGetLastError());
-    if (c.count[3] > 0) {
+    if (c.count[5] > 0) {
         std::vector<int> rows, len_h;
-        to_host(rows, c.lists + 3 * static_cast<size_t>(m), static_cast<size_t>(c.count[3]), st);
+        to_host(rows, lst(5), static_cast<size_t>(c.count[5]), st);
         to_host(len_h, len, static_cast<size_t>(m), st);
         sync(st);
         std::vector<int> caps(rows.size());
@@ -804,6 +813,24 @@ DevCsr transpose(Ctx& cx, const DevCsr& a) {
             CFDB_CUDA(cudaGetLastError());
         });
     }
+}
+
+DevCsr transpose(Ctx& cx, const DevCsr& a) {
+    cudaStream_t st = cx.st;
+    DevCsr t;
+    t.n_rows = a.n_cols;
+    t.n_cols = a.n_rows;
+    const int m = a.n_cols;
+    int* cnt = cx.mem->alloc<int>(static_cast<size_t>(m) + 1);
+    CFDB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (static_cast<size_t>(m) + 1), st));
+    if (a.nnz > 0) k_col_count<<<grid_for(a.nnz), kThreads, 0, st>>>(a.nnz, a.ci, cnt);
+    t.rp = cx.out<int>(static_cast<size_t>(m) + 1);
+    t.nnz = checked_nnz(scan(cx, cnt, m, t.rp), "a transpose");
+    t.ci = cx.out<int>(static_cast<size_t>(t.nnz) + 4);
+    t.va = cx.out<double>(static_cast<size_t>(t.nnz) + 4);
+    CFDB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (static_cast<size_t>(m) + 1), st));
+    if (a.n_rows > 0) k_t_fill<<<grid_for(a.n_rows), kThreads, 0, st>>>(a.n_rows, a.rp, a.ci, a.va, t.rp, cnt, t.ci, t.va);
+    sort_rows(cx, t);
     return t;
 }
 
@@ -814,10 +841,10 @@ DevCsr prune_zeros(Ctx& cx, const DevCsr& a) {
     o.n_cols = a.n_cols;
     int* cnt = cx.mem->alloc<int>(static_cast<size_t>(a.n_rows) + 1);
     if (a.n_rows > 0) k_nz_count<<<grid_for(a.n_rows), kThreads, 0, st>>>(a.n_rows, a.rp, a.va, cnt);
-    o.rp = cx.mem->alloc<int>(static_cast<size_t>(a.n_rows) + 1);
+    o.rp = cx.out<int>(static_cast<size_t>(a.n_rows) + 1);
     o.nnz = checked_nnz(scan(cx, cnt, a.n_rows, o.rp), "a coarse operator");
-    o.ci = cx.mem->alloc<int>(static_cast<size_t>(o.nnz) + 4);
-    o.va = cx.mem->alloc<double>(static_cast<size_t>(o.nnz) + 4);
+    o.ci = cx.out<int>(static_cast<size_t>(o.nnz) + 4);
+    o.va = cx.out<double>(static_cast<size_t>(o.nnz) + 4);
     if (a.n_rows > 0)
         k_nz_compact<<<grid_for(a.n_rows), kThreads, 0, st>>>(a.n_rows, a.rp, a.ci, a.va, o.rp, o.ci, o.va);
     CFDB_CUDA(cudaGetLastError());
@@ -852,14 +879,14 @@ void ldu_to_csr_values(int n, int nf, const int* diag_pos, const int* upper_pos,
 }
 
 void amg_setup_device(const DevCsr& a0, const AmgSettings& s, cudaStream_t st, DeviceHierarchy& h,
-                      PinnedBuffer* stage) {
+                      PinnedBuffer* stage, DeviceArena* keep) {
     PinnedBuffer own_stage;
     if (stage == nullptr) stage = &own_stage;
     if (a0.n_rows != a0.n_cols) fail(1, "AmgPreconditioner: matrix must be square");
     if (a0.n_rows <= 0) fail(1, "amg_setup: empty matrix");
-    Ctx cx{st, &h.mem, nullptr, nullptr, nullptr, s.table_limit > 0 ? s.table_limit : INT_MAX};
+    Ctx cx{st, &h.mem, nullptr, nullptr, nullptr, s.table_limit > 0 ? s.table_limit : INT_MAX, keep};
     cx.d_total = h.mem.alloc<long long>(1);
-    cx.d_counts = h.mem.alloc<int>(5);
+    cx.d_counts = h.mem.alloc<int>(kClasses + 1);
     cx.d_err = h.mem.alloc<int>(1);
     CFDB_CUDA(cudaMemsetAsync(cx.d_err, 0, sizeof(int), st));
     unsigned long long* rho_bits = h.mem.alloc<unsigned long long>(1);
@@ -946,10 +973,10 @@ void amg_setup_device(const DevCsr& a0, const AmgSettings& s, cudaStream_t st, D
         int* pcnt = h.mem.alloc<int>(static_cast<size_t>(nl) + 1);
         k_p_emit<false><<<grid_for(nl), kThreads, 0, st>>>(nl, c.rp, c.ci, c.va, dagg, omega, pcnt, nullptr, nullptr,
                                                            nullptr);
-        p.rp = h.mem.alloc<int>(static_cast<size_t>(nl) + 1);
+        p.rp = cx.out<int>(static_cast<size_t>(nl) + 1);
         p.nnz = checked_nnz(scan(cx, pcnt, nl, p.rp), "a prolongation");
-        p.ci = h.mem.alloc<int>(static_cast<size_t>(p.nnz) + 4);
-        p.va = h.mem.alloc<double>(static_cast<size_t>(p.nnz) + 4);
+        p.ci = cx.out<int>(static_cast<size_t>(p.nnz) + 4);
+        p.va = cx.out<double>(static_cast<size_t>(p.nnz) + 4);
         k_p_emit<true><<<grid_for(nl), kThreads, 0, st>>>(nl, c.rp, c.ci, c.va, dagg, omega, nullptr, p.rp, p.ci, p.va);
         CFDB_CUDA(cudaGetLastError());
         phase("prolongation");
@@ -1094,51 +1121,23 @@ __global__ void k_weighted_inv_diag(int n, int n_pad, const int* __restrict__ rp
     if (wd32 != nullptr) wd32[i] = __double2float_rn(w);
 }
 
-size_t csr_bytes(const DevCsr& m) {
-    return aligned(sizeof(int) * (static_cast<size_t>(m.n_rows) + 1)) + aligned(sizeof(int) * m.nnz) +
-           aligned(sizeof(double) * m.nnz);
-}
-
-// copy of m carved out of the block at `cursor` (advanced)
-DevCsr keep_csr(const DevCsr& m, char*& cursor, cudaStream_t st) {
-    DevCsr k = m;
-    k.rp = reinterpret_cast<int*>(cursor);
-    cursor += aligned(sizeof(int) * (static_cast<size_t>(m.n_rows) + 1));
-    k.ci = reinterpret_cast<int*>(cursor);
-    cursor += aligned(sizeof(int) * m.nnz);
-    k.va = reinterpret_cast<double*>(cursor);
-    cursor += aligned(sizeof(double) * m.nnz);
-    CFDB_CUDA(cudaMemcpyAsync(k.rp, m.rp, sizeof(int) * (static_cast<size_t>(m.n_rows) + 1), cudaMemcpyDeviceToDevice, st));
-    if (m.nnz > 0) {
-        CFDB_CUDA(cudaMemcpyAsync(k.ci, m.ci, sizeof(int) * m.nnz, cudaMemcpyDeviceToDevice, st));
-        CFDB_CUDA(cudaMemcpyAsync(k.va, m.va, sizeof(double) * m.nnz, cudaMemcpyDeviceToDevice, st));
-    }
-    return k;
-}
-
 } // namespace
 
-std::shared_ptr<DeviceLevels> keep_levels(const DeviceHierarchy& d, cudaStream_t st) {
-    auto k = std::make_shared<DeviceLevels>();
-    size_t total = 0; // one allocation for all levels
-    for (int l = 1; l < d.levels(); ++l) total += csr_bytes(d.a[l]);
-    for (size_t l = 0; l < d.p.size(); ++l) total += csr_bytes(d.p[l]) + csr_bytes(d.r[l]);
-    char* cursor = k->mem.alloc<char>(total);
+void adopt_levels(const DeviceHierarchy& d, DeviceLevels& k) {
+    k.a.clear();
+    k.p.clear();
+    k.r.clear();
     for (int l = 0; l < d.levels(); ++l) {
         if (l == 0) {
             DevCsr e;
             e.n_rows = e.n_cols = d.a[0].n_rows;
-            k->a.push_back(e);
+            k.a.push_back(e);
         } else {
-            k->a.push_back(keep_csr(d.a[l], cursor, st));
+            k.a.push_back(d.a[l]);
         }
     }
-    for (size_t l = 0; l < d.p.size(); ++l) {
-        k->p.push_back(keep_csr(d.p[l], cursor, st));
-        k->r.push_back(keep_csr(d.r[l], cursor, st));
-    }
-    sync(st);
-    return k;
+    k.p = d.p;
+    k.r = d.r;
 }
 
 Hierarchy hierarchy_shape(const DeviceHierarchy& d) {
@@ -1175,7 +1174,7 @@ long long sell_shape(const DevCsr& m, int n_pad, int window, int* perm, int* sli
     if (n_pad % 32 != 0 || n_pad < m.n_rows) fail(1, "sell_shape: bad padding");
     const int n_sl = n_pad / 32;
     Scratch tmp;
-    Ctx cx{st, &tmp, tmp.alloc<long long>(1), tmp.alloc<int>(5), tmp.alloc<int>(1), INT_MAX};
+    Ctx cx{st, &tmp, tmp.alloc<long long>(1), tmp.alloc<int>(kClasses + 1), tmp.alloc<int>(1), INT_MAX};
     int* width32 = tmp.alloc<int>(std::max(n_sl, 1));
     if (n_pad > 0)
         k_sell_order<<<(n_pad + kSellWindow - 1) / kSellWindow, kSellWindow, 0, st>>>(m.n_rows, n_pad, m.rp, perm, width32);

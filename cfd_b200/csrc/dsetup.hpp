@@ -89,21 +89,24 @@ struct DeviceHierarchy {
 // Builds the hierarchy of a0 (device CSR, already in h.mem or caller-owned and alive for the
 // call) with settings s on stream st. Synchronises st. stage: page-locked staging of the
 // strength graphs read back for aggregation (null: a temporary one).
+// keep: where the hierarchy's own arrays (P_l, R_l, A_l for l >= 1) are allocated, so that a
+// caller can hold them after h's scratch is released (null: in h.mem).
 void amg_setup_device(const DevCsr& a0, const AmgSettings& s, cudaStream_t st, DeviceHierarchy& h,
-                      PinnedBuffer* stage = nullptr);
+                      PinnedBuffer* stage = nullptr, DeviceArena* keep = nullptr);
 
 // Host copy of a device hierarchy; level 0's matrix is copied only when with_a0.
 Hierarchy download_hierarchy(const DeviceHierarchy& d, bool with_a0, cudaStream_t st);
 
-// The levels a device plan is built from (A_l for l >= 1, P_l, R_l), compacted out of the
-// setup's scratch into their own allocation and kept with the system, so that the plan can be
-// rebuilt (precision or tuning changes) without the host.
+// The levels a device plan is built from (A_l for l >= 1, P_l, R_l), allocated by the setup
+// in their own arena (amg_setup_device's `keep`) and kept with the system, so that the plan can
+// be rebuilt (precision or tuning changes) without the host.
 struct DeviceLevels {
     DeviceArena mem;
     std::vector<DevCsr> a, p, r; // a[0] is empty (level 0 comes from the system's pattern)
     [[nodiscard]] size_t bytes() const { return mem.bytes(); }
 };
-std::shared_ptr<DeviceLevels> keep_levels(const DeviceHierarchy& d, cudaStream_t st);
+// Points k's level views at the arrays of d (which the setup allocated in k.mem).
+void adopt_levels(const DeviceHierarchy& d, DeviceLevels& k);
 
 // Shape-only host copy of a device hierarchy (sizes, aggregates, coarse inverse; matrix arrays
 // empty) for plan construction from the device levels.

@@ -359,10 +359,16 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         key.nnz = sp.rp[sp.n];
         key.vs_len = sp.vs_len;
         key.absolute_src = sp.absolute_src;
-        long long h = 0;
-        for (size_t k = 0; k < sp.src.size(); ++k) h = h * 1000003 + sp.src[k];
-        for (size_t k = 0; k < sp.diag_src.size(); ++k) h = h * 1000003 + sp.diag_src[k];
-        key.map_hash = h;
+        if (sp.layout_id != 0) {
+            key.map_hash = sp.layout_id;
+        } else {
+            const std::vector<int>& sv = sp.src_ref ? *sp.src_ref : sp.src;
+            const std::vector<int>& dv = sp.diag_src_ref ? *sp.diag_src_ref : sp.diag_src;
+            long long h = 0;
+            for (size_t k = 0; k < sv.size(); ++k) h = h * 1000003 + sv[k];
+            for (size_t k = 0; k < dv.size(); ++k) h = h * 1000003 + dv[k];
+            key.map_hash = h;
+        }
     }
     key.need32 = need32_;
     key.col16 = tuning_.col16 != 0;
@@ -386,14 +392,15 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         for (int k = 0; k < n_sys_; ++k) {
             const int s = perm_[k];
             const SystemSpec& sp = systems[s];
-            if (static_cast<int>(sp.src.size()) != sp.rp[sp.n] ||
-                static_cast<int>(sp.diag_src.size()) != sp.n) {
+            const std::vector<int>& sv = sp.src_ref ? *sp.src_ref : sp.src;
+            const std::vector<int>& dv = sp.diag_src_ref ? *sp.diag_src_ref : sp.diag_src;
+            if (static_cast<int>(sv.size()) != sp.rp[sp.n] || static_cast<int>(dv.size()) != sp.n) {
                 fail(1, "engine: level-0 value map size mismatch");
             }
             const int so = sp.absolute_src ? 0 : vs_off_[s];
-            sell_append(sb, sp.n, round_up(sp.n, 32), sp.rp, sp.ci, nullptr, sp.src.data(), off[0][s], so,
+            sell_append(sb, sp.n, round_up(sp.n, 32), sp.rp, sp.ci, nullptr, sv.data(), off[0][s], so,
                         off[0][s]);
-            for (int i = 0; i < sp.n; ++i) dsrc[off[0][s] + i] = sp.diag_src[i] >= 0 ? sp.diag_src[i] + so : -1;
+            for (int i = 0; i < sp.n; ++i) dsrc[off[0][s] + i] = dv[i] >= 0 ? dv[i] + so : -1;
         }
         DevLevel& d = lv_[0];
         d.a.n_slices = static_cast<int>(sb.slice.size()) - 1;
@@ -1471,6 +1478,62 @@ void Engine::apply_vcycle(Mode mode, const std::vector<int>&) {
     st_ = keep;
     CFDB_CUDA(cudaGetLastError());
     CFDB_CUDA(cudaStreamSynchronize(stream_));
+}
+
+double Engine::time_sweep(int level, int reps, double* bytes) {
+    if (level < 0 || level >= n_levels_ || reps < 1) fail(1, "time_sweep: bad level or reps");
+    const DevLevel& d = lv_[level];
+    const bool fp32 = need32_;
+    const DevSell64_32& m = d.a;
+    const bool nc = level + 1 < n_levels_;
+    const Tiles tiles = m.tiles;
+    const int grid = nc ? m.n_tiles_nc : m.n_tiles;
+    if (grid == 0) fail(1, "time_sweep: level has no operator tiles");
+    const int visit = visit_of(m.s64.val != nullptr ? m.s64.fmt : m.s32.fmt);
+    const double sv = fp32 ? 4.0 : 8.0;
+    const double sb = level == 0 ? 8.0 : sv;
+    const double n = d.n_rows_nc;
+    const double cb = fp32 && m.s32.c16 != nullptr ? 2.0 : 4.0;
+    if (bytes != nullptr) *bytes = static_cast<double>(m.nnz) * (sv + cb) + 4.0 * (n + 1.0) + 3.0 * sv * n + sb * n;
+    cudaEvent_t a, b;
+    CFDB_CUDA(cudaEventCreate(&a));
+    CFDB_CUDA(cudaEventCreate(&b));
+    auto launch = [&](auto tag) {
+        using T = decltype(tag);
+        const Sell<T> op = vs_sel<T>(m.s64, m.s32);
+        const T* wd = nullptr;
+        T *x, *y;
+        if constexpr (sizeof(T) == 8) {
+            wd = d.wd64;
+            x = d.x64;
+            y = d.y64;
+        } else {
+            wd = d.wd32;
+            x = d.x32;
+            y = d.y32;
+        }
+        with_visit(visit, [&](auto V) {
+            if (level == 0) {
+                k_vc_jacobi<T, double, decltype(V)::value><<<grid, m.block, 0, stream_>>>(op, tiles, nullptr, wd, r_, x, y);
+            } else {
+                const T* bv;
+                if constexpr (sizeof(T) == 8) bv = d.b64;
+                else bv = d.b32;
+                k_vc_jacobi<T, T, decltype(V)::value><<<grid, m.block, 0, stream_>>>(op, tiles, nullptr, wd, bv, x, y);
+            }
+        });
+    };
+    for (int w = 0; w < 2; ++w) fp32 ? launch(0.0f) : launch(0.0); // warm-up
+    CFDB_CUDA(cudaEventRecord(a, stream_));
+    for (int i = 0; i < reps; ++i) fp32 ? launch(0.0f) : launch(0.0);
+    CFDB_CUDA(cudaEventRecord(b, stream_));
+    CFDB_CUDA(cudaEventSynchronize(b));
+    CFDB_CUDA(cudaGetLastError());
+    float ms = 0.f;
+    CFDB_CUDA(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms / reps;
 }
 
 double Engine::time_level0_sweep(bool fp32, int reps) {

@@ -21,6 +21,11 @@ struct SystemSpec {
     const int* ci = nullptr;
     std::vector<int> src;             // per pattern entry: index into this system's value source
     std::vector<int> diag_src;        // per row: value-source index of the diagonal, or -1
+    // the same maps owned by the caller (used instead of src / diag_src when set; no copy)
+    const std::vector<int>* src_ref = nullptr;
+    const std::vector<int>* diag_src_ref = nullptr;
+    // identifies the pattern and value maps (0: unknown); equal ids mean equal level-0 layouts
+    long long layout_id = 0;
     int vs_len = 0;                   // length of this system's value source
     bool absolute_src = false;        // src already indexes the batch-wide value source
     std::shared_ptr<const Hierarchy> h; // levels >= 1, transfers, coarse inverse (null: none)
@@ -113,6 +118,10 @@ public:
 
     // Kernel timing probe: average device time (ms) of the level-0 FP64/FP32 smoother sweep.
     double time_level0_sweep(bool fp32, int reps);
+    // Average device time (ms) of `reps` back-to-back Jacobi sweeps of level l in the plan's
+    // precision and launch shape (level 0 reads the Krylov residual); *bytes = algorithmic bytes
+    // of one sweep (operator, weights, right-hand side, iterate in and out).
+    double time_sweep(int level, int reps, double* bytes);
 
     // Runs the initial preconditioning and one full iteration eagerly with CUDA events around
     // every kernel (all systems kept active); returns per-kernel device time averaged over reps

@@ -236,6 +236,8 @@ bool ldlt_factor(int n, const std::vector<double>& a, std::vector<double>& f) {
         }
         if (d == 0.0 || !std::isfinite(d)) return false;
         f[static_cast<size_t>(j) * n + j] = d;
+        // rows below the pivot are independent
+#pragma omp parallel for schedule(static) if (n - j > 128)
         for (int i = j + 1; i < n; ++i) {
             double s = f[static_cast<size_t>(i) * n + j];
             for (int k = 0; k < j; ++k) {
@@ -390,6 +392,7 @@ int aggregate_strong(int n, const int* srp, const int* sci, const double* sav, s
     }
     // pass 2: join the pass-1 aggregate of the strongest strong neighbour (strictly larger wins)
     const std::vector<int> pass1 = agg;
+#pragma omp parallel for schedule(static) if (n > 65536)
     for (int i = 0; i < n; ++i) {
         if (agg[i] >= 0) continue;
         double best = 0.0;
@@ -431,6 +434,8 @@ int aggregate_strong_ranked(int n, const int* srp, const int* sci, const uint16_
         ++n_agg;
     }
     const std::vector<int> pass1 = agg;
+    // pass 2 reads only pass 1's result: rows are independent
+#pragma omp parallel for schedule(static) if (n > 65536)
     for (int i = 0; i < n; ++i) {
         if (agg[i] >= 0) continue;
         int best = INT_MAX;
@@ -460,12 +465,17 @@ bool dense_inverse(int n, const std::vector<double>& a, std::vector<double>& inv
         return false;
     }
     inv.assign(static_cast<size_t>(n) * n, 0.0);
-    std::vector<double> e(static_cast<size_t>(n), 0.0), col(static_cast<size_t>(n));
-    for (int j = 0; j < n; ++j) {
-        e[j] = 1.0;
-        ldlt_solve(n, f, e.data(), col.data());
-        e[j] = 0.0;
-        for (int i = 0; i < n; ++i) inv[static_cast<size_t>(i) * n + j] = col[i];
+    // one independent solve per column
+#pragma omp parallel if (n > 64)
+    {
+        std::vector<double> e(static_cast<size_t>(n), 0.0), col(static_cast<size_t>(n));
+#pragma omp for schedule(static)
+        for (int j = 0; j < n; ++j) {
+            e[j] = 1.0;
+            ldlt_solve(n, f, e.data(), col.data());
+            e[j] = 0.0;
+            for (int i = 0; i < n; ++i) inv[static_cast<size_t>(i) * n + j] = col[i];
+        }
     }
     return true;
 }

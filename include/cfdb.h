@@ -195,6 +195,10 @@ int cfdb_system_setup_amg(cfdb_system* sys, const double* diag, const double* up
 int cfdb_system_setup_amg_device(cfdb_system* sys, const double* diag, const double* upper,
                                  const double* lower, const cfdb_amg_settings* settings,
                                  int device_arrays);
+/* Kernel timing: average device time (ms) of `reps` back-to-back Jacobi sweeps of level
+ * `level` in the installed plan (its precision and launch shape) and the algorithmic bytes of
+ * one sweep. The sweep reads the level's current vectors; solve results are not affected. */
+int cfdb_system_time_sweep(cfdb_system* sys, int level, int reps, double* ms, double* bytes);
 /* Whether a device setup keeps its levels on the device (default 1). They let the plan be
  * rebuilt (set_precision, set_tuning, set_ordered) without a new setup; without them such a
  * change after a device setup fails with CFDB_ERR_NOT_READY until the next setup. */

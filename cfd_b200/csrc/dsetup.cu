@@ -285,6 +285,45 @@ template <int G> __device__ void bitonic_sort(int* keys, double* vals, int cap, 
     }
 }
 
+// Moves the occupied slots (key != kEmpty) of a table to its front, keeping their order, and
+// returns their number. wc: G / 32 ints of shared memory (G > 32).
+template <int G> __device__ int compact_front(int* keys, double* vals, int cap, int t, int* wc) {
+    int base = 0;
+    const int lane = t & 31, w = t >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    for (int s0 = 0; s0 < cap; s0 += G) {
+        const int s = s0 + t;
+        const int key = s < cap ? keys[s] : kEmpty;
+        const bool occ = key != kEmpty;
+        const double val = occ ? vals[s] : 0.0;
+        const unsigned bal = __ballot_sync(0xffffffffu, occ);
+        int pos, total;
+        if constexpr (G == 32) {
+            pos = base + __popc(bal & below);
+            total = __popc(bal);
+        } else {
+            if (lane == 0) wc[w] = __popc(bal);
+            __syncthreads();
+            int before = 0;
+            total = 0;
+            for (int q = 0; q < G / 32; ++q) {
+                const int c = wc[q];
+                if (q < w) before += c;
+                total += c;
+            }
+            pos = base + before + __popc(bal & below);
+        }
+        group_sync<G>(); // the chunk is read before any of it is overwritten (pos <= s)
+        if (occ) {
+            keys[pos] = key;
+            vals[pos] = val;
+        }
+        base += total;
+        group_sync<G>();
+    }
+    return base;
+}
+
 // One row per group of G threads, PER groups per CTA. CAP > 0: table of CAP slots in shared
 // memory; CAP == 0: table in device memory (g.gkeys / g.gvals at g.goff, g.gcap slots).
 // Symbolic (NUMERIC = false): counts distinct columns; with LIMIT, a row whose count passes
@@ -295,6 +334,7 @@ __global__ void __launch_bounds__(G* PER) k_gemm_rows(GemmArgs g) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_count[PER];
     __shared__ int s_over[PER];
+    __shared__ int s_wc[G > 32 ? G / 32 : 1];
     const int grp = threadIdx.x / G, t = threadIdx.x % G;
     const int pos = blockIdx.x * PER + grp;
     if (pos >= g.n_list) return; // whole groups only
@@ -379,9 +419,15 @@ __global__ void __launch_bounds__(G* PER) k_gemm_rows(GemmArgs g) {
             if (t == 0) atomicExch(g.err, 2);
             return;
         }
-        bitonic_sort<G>(keys, vals, cap, t);
+        // sort only the occupied slots: compact them, pad to a power of two, bitonic sort
+        const int used = compact_front<G>(keys, vals, cap, t, s_wc);
+        int p2 = 1;
+        while (p2 < used) p2 <<= 1;
+        for (int s = used + t; s < p2; s += G) keys[s] = kEmpty;
+        group_sync<G>();
+        bitonic_sort<G>(keys, vals, p2, t);
         const int c0 = g.crp[i], len = g.crp[i + 1] - c0;
-        if (len > cap) {
+        if (len != used) {
             if (t == 0) atomicExch(g.err, 3);
             return;
         }
@@ -389,7 +435,6 @@ __global__ void __launch_bounds__(G* PER) k_gemm_rows(GemmArgs g) {
             g.cci[c0 + s] = keys[s];
             g.cva[c0 + s] = vals[s];
         }
-        if (t == 0 && ((len > 0 && keys[len - 1] == kEmpty) || (len < cap && keys[len] != kEmpty))) atomicExch(g.err, 4);
     }
 }
 
@@ -421,7 +466,14 @@ __global__ void k_classify(int n, const int* __restrict__ m, Limits L, int* list
     int c = kClasses - 1;
     for (int q = kClasses - 2; q >= 0; --q)
         if (v <= L.lim[q]) c = q;
-    lists[static_cast<size_t>(c) * n + atomicAdd(&counts[c], 1)] = i;
+    // one atomic per class present in the warp
+    const int lane = threadIdx.x & 31;
+    const unsigned same = __match_any_sync(__activemask(), c);
+    const int leader = __ffs(same) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&counts[c], __popc(same));
+    base = __shfl_sync(same, base, leader);
+    lists[static_cast<size_t>(c) * n + base + __popc(same & ((1u << lane) - 1u))] = i;
 }
 
 // rows of a list whose count is at most `lim` (symbolic retry: rows a smaller table rejected)
@@ -509,12 +561,14 @@ __global__ void __launch_bounds__(G* PER) k_seg_sort(const int* __restrict__ row
     }
     const int r0 = rp[i], len = rp[i + 1] - r0;
     if (len > cap) return; // classified by length: cannot happen
-    for (int s = t; s < cap; s += G) {
+    int p2 = 1;
+    while (p2 < len) p2 <<= 1;
+    for (int s = t; s < p2; s += G) {
         keys[s] = s < len ? ci[r0 + s] : kEmpty;
         vals[s] = s < len ? va[r0 + s] : 0.0;
     }
     group_sync<G>();
-    bitonic_sort<G>(keys, vals, cap, t);
+    bitonic_sort<G>(keys, vals, p2, t);
     for (int s = t; s < len; s += G) {
         ci[r0 + s] = keys[s];
         va[r0 + s] = vals[s];

@@ -139,7 +139,7 @@ _proto("cfdb_system_kernel_launches", [_vp, _P(C.c_ulonglong)])
 class TuningStruct(C.Structure):
     _fields_ = [("target_tiles", _i), ("wide_row", _i), ("lanes_div", _i), ("fuse_first", _i),
                 ("sell_rows", _i), ("krylov_pair", _i), ("tail_rows", _i),
-                ("col16", _i)]
+                ("col16", _i), ("pdl", _i)]
 
 
 _proto("cfdb_default_tuning", [_P(TuningStruct)], None)
@@ -795,11 +795,12 @@ class Tuning:
     krylov_pair: int = 1
     tail_rows: int = 0
     col16: int = 0
+    pdl: int = 1
 
     def _c(self):
         return TuningStruct(int(self.target_tiles), int(self.wide_row), int(self.lanes_div),
                             int(self.fuse_first), int(self.sell_rows), int(self.krylov_pair),
-                            int(self.tail_rows), int(self.col16))
+                            int(self.tail_rows), int(self.col16), int(self.pdl))
 
 
 def _set_system_tuning(self, t: Tuning) -> None:

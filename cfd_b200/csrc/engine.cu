@@ -166,6 +166,24 @@ std::vector<double> inverse_diagonal(const HostCsr& a) {
 
 int grid_of(long long n) { return static_cast<int>(std::max<long long>(1, (n + 255) / 256)); }
 
+// Kernel launch, with programmatic dependent launch when pdl: the kernel may be scheduled while
+// its predecessor in the stream finishes (every kernel of kernels.cuh starts with pdl_entry(),
+// which lets its own successor be scheduled and then waits for its predecessor's completion).
+template <class... P, class... A>
+void launch_k(bool pdl, void (*kernel)(P...), int grid, int block, size_t smem, cudaStream_t s, A&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid));
+    cfg.blockDim = dim3(static_cast<unsigned>(block));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    CFDB_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...));
+}
+
 } // namespace
 
 Engine::Engine(int device) : device_(device) {
@@ -743,12 +761,12 @@ void Engine::set_values_device(const double* p0, const double* p1, const double*
     const DevLevel& d = lv_[0];
     ValueSource vs{p0, p1, p2, n1, n2};
     const long long n = std::max<long long>(d.a.slots, d.n_rows);
-    k_fill_level0<<<grid_of(n), 256, 0, stream_>>>(static_cast<int>(d.a.slots), d.n_rows, src0_, diag_src0_, vs,
+    launch_k(tuning_.pdl != 0, k_fill_level0, grid_of(n), 256, 0, stream_, static_cast<int>(d.a.slots), d.n_rows, src0_, diag_src0_, vs,
                                                    weight_, d.a.s64.val ? const_cast<double*>(d.a.s64.val) : nullptr,
                                                    d.a.s32.val ? const_cast<float*>(d.a.s32.val) : nullptr, d.wd64,
                                                    d.wd32);
     // plain inverse diagonal for Jacobi preconditioning: weight 1
-    k_fill_level0<<<grid_of(d.n_rows), 256, 0, stream_>>>(0, d.n_rows, src0_, diag_src0_, vs, 1.0, nullptr,
+    launch_k(tuning_.pdl != 0, k_fill_level0, grid_of(d.n_rows), 256, 0, stream_, 0, d.n_rows, src0_, diag_src0_, vs, 1.0, nullptr,
                                                           nullptr, dinv0_, nullptr);
     launches_ += 2;
     CFDB_CUDA(cudaGetLastError());
@@ -799,15 +817,15 @@ void Engine::upload_values_device_concat(const std::vector<const double*>& dev_s
 
 void Engine::set_rhs_guess_concat(const double* b, const double* x0) {
     const int n = lv_[0].n_rows;
-    k_gather_rows<<<grid_of(n), 256, 0, stream_>>>(n, row_map_, b, b_);
-    k_gather_rows<<<grid_of(n), 256, 0, stream_>>>(n, row_map_, x0, x_);
+    launch_k(tuning_.pdl != 0, k_gather_rows, grid_of(n), 256, 0, stream_, n, row_map_, b, b_);
+    launch_k(tuning_.pdl != 0, k_gather_rows, grid_of(n), 256, 0, stream_, n, row_map_, x0, x_);
     launches_ += 2;
     CFDB_CUDA(cudaGetLastError());
 }
 
 void Engine::get_solution_concat(double* x) {
     const int n = lv_[0].n_rows;
-    k_scatter_rows<<<grid_of(n), 256, 0, stream_>>>(n, row_map_, x_, x);
+    launch_k(tuning_.pdl != 0, k_scatter_rows, grid_of(n), 256, 0, stream_, n, row_map_, x_, x);
     ++launches_;
     CFDB_CUDA(cudaGetLastError());
     CFDB_CUDA(cudaStreamSynchronize(stream_));
@@ -1105,8 +1123,8 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
             T* c = start;
             for (int k = 1; k < sweeps_; ++k) {
                 T* o = c == x ? y : x;
-                if (l == 0) with_visit(ta.visit, [&](auto V) { k_vc_jacobi<T, double, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, c, o); });
-                else with_visit(ta.visit, [&](auto V) { k_vc_jacobi<T, T, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), c, o); });
+                if (l == 0) with_visit(ta.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_jacobi<T, double, decltype(V)::value>, ta.second, ta.block, 0, s, A(l), ta.first, stv, WD(l), r_, c, o); });
+                else with_visit(ta.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_jacobi<T, T, decltype(V)::value>, ta.second, ta.block, 0, s, A(l), ta.first, stv, WD(l), Bv(l), c, o); });
                 mark("smooth", l, spmv_b(d.a, n, n) + sv * n + sb * n);
                 c = o;
             }
@@ -1114,30 +1132,30 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
         } else {
             const auto ta = TL(l, d.a, true);
             if (l == 0) {
-                with_visit(ta.visit, [&](auto V) { k_vc_first<T, double, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, start, fuse); });
+                with_visit(ta.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_first<T, double, decltype(V)::value>, ta.second, ta.block, 0, s, A(l), ta.first, stv, WD(l), r_, start, fuse); });
             } else {
-                with_visit(ta.visit, [&](auto V) { k_vc_first<T, T, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), start, fuse); });
+                with_visit(ta.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_first<T, T, decltype(V)::value>, ta.second, ta.block, 0, s, A(l), ta.first, stv, WD(l), Bv(l), start, fuse); });
             }
             mark("smooth_first", l, fuse ? spmv_b(d.a, n, n) - sv * n + sv * n + sb * n : 2.0 * sv * n + sb * n);
             T* c = start;
             for (int k = fuse ? 2 : 1; k < sweeps_; ++k) {
                 T* o = c == x ? y : x;
-                if (l == 0) with_visit(ta.visit, [&](auto V) { k_vc_jacobi<T, double, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, c, o); });
-                else with_visit(ta.visit, [&](auto V) { k_vc_jacobi<T, T, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), c, o); });
+                if (l == 0) with_visit(ta.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_jacobi<T, double, decltype(V)::value>, ta.second, ta.block, 0, s, A(l), ta.first, stv, WD(l), r_, c, o); });
+                else with_visit(ta.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_jacobi<T, T, decltype(V)::value>, ta.second, ta.block, 0, s, A(l), ta.first, stv, WD(l), Bv(l), c, o); });
                 mark("smooth", l, spmv_b(d.a, n, n) + sv * n + sb * n);
                 c = o;
             }
             cur[l] = c;
         }
         const auto tr = TL(l, d.a, true);
-        if (l == 0) with_visit(tr.visit, [&](auto V) { k_vc_residual<T, double, decltype(V)::value><<<tr.second, tr.block, 0, s>>>(A(l), tr.first, stv, r_, cur[l], Tv(l)); });
-        else with_visit(tr.visit, [&](auto V) { k_vc_residual<T, T, decltype(V)::value><<<tr.second, tr.block, 0, s>>>(A(l), tr.first, stv, Bv(l), cur[l], Tv(l)); });
+        if (l == 0) with_visit(tr.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_residual<T, double, decltype(V)::value>, tr.second, tr.block, 0, s, A(l), tr.first, stv, r_, cur[l], Tv(l)); });
+        else with_visit(tr.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_residual<T, T, decltype(V)::value>, tr.second, tr.block, 0, s, A(l), tr.first, stv, Bv(l), cur[l], Tv(l)); });
         mark("residual", l, spmv_b(d.a, n, n) + sb * n);
         const DevLevel& nx = lv_[l + 1];
         const auto tq = TL(l + 1, d.r, false);
         const bool next_x1 = x1_by_restrict && l + 2 < L && nx.n_rows_nc > 0;
         with_visit(tq.visit, [&](auto V) {
-            k_vc_spmv<T, decltype(V)::value><<<tq.second, tq.block, 0, s>>>(
+            launch_k(tuning_.pdl != 0, k_vc_spmv<T, decltype(V)::value>, tq.second, tq.block, 0, s, 
                 R(l), tq.first, stv, Tv(l), Bv(l + 1), next_x1 ? WD(l + 1) : nullptr,
                 next_x1 ? start_buffer<T>(l + 1) : nullptr, next_x1 ? nx.n_rows_nc : 0);
         });
@@ -1151,10 +1169,10 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
         mark("tail", lt, sizeof(T) == 8 ? tail_bytes64_ : tail_bytes32_);
     } else if (n_ctiles_ > 0) {
         if constexpr (sizeof(T) == 8) {
-            k_vc_coarse<double, double><<<n_ctiles_, kBlock, coarse_smem64_, s>>>(cb_, stv, b_level64_, x_level64_,
+            launch_k(tuning_.pdl != 0, k_vc_coarse<double, double>, n_ctiles_, kBlock, coarse_smem64_, s, cb_, stv, b_level64_, x_level64_,
                                                                                   block_level_, ctl, ord);
         } else {
-            k_vc_coarse<float, float><<<n_ctiles_, kBlock, coarse_smem32_, s>>>(cb_, stv, b_level32_, x_level32_,
+            launch_k(tuning_.pdl != 0, k_vc_coarse<float, float>, n_ctiles_, kBlock, coarse_smem32_, s, cb_, stv, b_level32_, x_level32_,
                                                                                 block_level_, ctl, ord);
         }
         mark("coarse", L - 1, coarse_bytes_ + 2.0 * sv * coarse_rows_);
@@ -1170,7 +1188,7 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
         T* c = cur[l];
         const auto tp = TL(l, d.p, true);
         with_visit(tp.visit, [&](auto V) {
-            k_vc_prolong<T, decltype(V)::value><<<tp.second, tp.block, 0, s>>>(P(l), tp.first, stv, X(l + 1), c);
+            launch_k(tuning_.pdl != 0, k_vc_prolong<T, decltype(V)::value>, tp.second, tp.block, 0, s, P(l), tp.first, stv, X(l + 1), c);
         });
         const auto ta = TL(l, d.a, true);
         mark("prolong", l, spmv_b(d.p, n, lv_[l + 1].n_rows) + sv * n);
@@ -1179,15 +1197,15 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
             const bool last = k + 1 == sweeps_;
             if (l == 0 && last && fused_final) {
                 with_visit(krylov_visit(), [&](auto V) {
-                    k_vc_jacobi_final<T, decltype(V)::value><<<d.n_tiles_nc, kBlock, 0, s>>>(
+                    launch_k(tuning_.pdl != 0, k_vc_jacobi_final<T, decltype(V)::value>, d.n_tiles_nc, kBlock, 0, s, 
                         A(0), d.tiles, st_, WD(0), r_, c, o, q_, red_, Control{n_active_, error_}, flexible);
                 });
                 mark("smooth_dot", l, spmv_b(d.a, n, n) + sv * n + sb * n + (flexible ? 8.0 * n : 0.0));
             } else if (l == 0) {
-                with_visit(ta.visit, [&](auto V) { k_vc_jacobi<T, double, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), r_, c, o); });
+                with_visit(ta.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_jacobi<T, double, decltype(V)::value>, ta.second, ta.block, 0, s, A(l), ta.first, stv, WD(l), r_, c, o); });
                 mark("smooth", l, spmv_b(d.a, n, n) + sv * n + sb * n);
             } else {
-                with_visit(ta.visit, [&](auto V) { k_vc_jacobi<T, T, decltype(V)::value><<<ta.second, ta.block, 0, s>>>(A(l), ta.first, stv, WD(l), Bv(l), c, o); });
+                with_visit(ta.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_jacobi<T, T, decltype(V)::value>, ta.second, ta.block, 0, s, A(l), ta.first, stv, WD(l), Bv(l), c, o); });
                 mark("smooth", l, spmv_b(d.a, n, n) + sv * n + sb * n);
             }
             c = o;
@@ -1209,12 +1227,12 @@ void Engine::enqueue_init(Mode mode) {
     const X1Out x1o = x1_out(mode);
     const double x1b = (mode == Mode::AmgMixed ? 8.0 : 16.0) * x1o.n;
     with_visit(krylov_visit(), [&](auto V) {
-        k_cg_init<decltype(V)::value><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, r_, red_, ctl, x1o);
+        launch_k(tuning_.pdl != 0, k_cg_init<decltype(V)::value>, d.n_tiles, kBlock, 0, stream_, d.a.s64, d.tiles, st_, b_, x_, r_, red_, ctl, x1o);
     });
     mark("cg_init", 0, a0 + 16.0 * n + x1b);
     const int flexible = mode == Mode::AmgMixed ? 1 : 0;
     if (mode == Mode::Jacobi) {
-        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, nullptr, q_, red_, ctl, 0);
+        launch_k(tuning_.pdl != 0, k_cg_rz<double>, d.n_tiles, kBlock, 0, stream_, d.tiles, st_, r_, d.x64, dinv0_, nullptr, q_, red_, ctl, 0);
         mark("cg_rz", 0, 24.0 * n);
         return;
     }
@@ -1227,10 +1245,10 @@ void Engine::enqueue_rz(Mode mode, int flexible) {
     const Control ctl{n_active_, error_};
     const double n = d.n_rows;
     if (mode == Mode::AmgMixed) {
-        k_cg_rz<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x32, nullptr, dinv0_, q_, red_, ctl, flexible);
+        launch_k(tuning_.pdl != 0, k_cg_rz<float>, d.n_tiles, kBlock, 0, stream_, d.tiles, st_, r_, d.x32, nullptr, dinv0_, q_, red_, ctl, flexible);
         mark("cg_rz", 0, 12.0 * n + (flexible ? 8.0 * n : 0.0));
     } else {
-        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, nullptr, dinv0_, q_, red_, ctl, flexible);
+        launch_k(tuning_.pdl != 0, k_cg_rz<double>, d.n_tiles, kBlock, 0, stream_, d.tiles, st_, r_, d.x64, nullptr, dinv0_, q_, red_, ctl, flexible);
         mark("cg_rz", 0, 16.0 * n + (flexible ? 8.0 * n : 0.0));
     }
 }
@@ -1241,31 +1259,31 @@ void Engine::enqueue_iteration(Mode mode) {
     const double n = d.n_rows;
     const double a0 = static_cast<double>(d.a.nnz) * 12.0 + 4.0 * (n + 1.0) + 16.0 * n;
     if (mode == Mode::AmgMixed) {
-        k_cg_pupdate<float><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, d.x32, r_, dinv0_, p_);
+        launch_k(tuning_.pdl != 0, k_cg_pupdate<float>, d.n_tiles, kBlock, 0, stream_, d.tiles, st_, d.x32, r_, dinv0_, p_);
         mark("cg_p_update", 0, 20.0 * n);
     } else {
-        k_cg_pupdate<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, d.x64, r_, dinv0_, p_);
+        launch_k(tuning_.pdl != 0, k_cg_pupdate<double>, d.n_tiles, kBlock, 0, stream_, d.tiles, st_, d.x64, r_, dinv0_, p_);
         mark("cg_p_update", 0, 24.0 * n);
     }
     with_visit(krylov_visit(), [&](auto V) {
-        k_cg_spmv_pq<decltype(V)::value><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, p_, q_, red_, ctl);
+        launch_k(tuning_.pdl != 0, k_cg_spmv_pq<decltype(V)::value>, d.n_tiles, kBlock, 0, stream_, d.a.s64, d.tiles, st_, p_, q_, red_, ctl);
     });
     mark("cg_spmv_pq", 0, a0);
     const X1Out x1o = x1_out(mode);
     const double x1b = (mode == Mode::AmgMixed ? 8.0 : 16.0) * x1o.n;
-    k_cg_xr<<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, x_, r_, p_, q_, red_,
+    launch_k(tuning_.pdl != 0, k_cg_xr, d.n_tiles, kBlock, 0, stream_, d.tiles, st_, x_, r_, p_, q_, red_,
                                                 ctl, mode == Mode::AmgMixed ? 1 : 0, x1o);
     mark("cg_xr", 0, 48.0 * n + x1b);
     if (mode == Mode::AmgMixed) {
         with_visit(krylov_visit(), [&](auto V) {
-            k_cg_true_check<decltype(V)::value><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, r_,
+            launch_k(tuning_.pdl != 0, k_cg_true_check<decltype(V)::value>, d.n_tiles, kBlock, 0, stream_, d.a.s64, d.tiles, st_, b_, x_, r_,
                                                                                red_, ctl, x1o);
         });
         mark("cg_true_check", 0, 0.0);
     }
     const int flexible = mode == Mode::AmgMixed ? 1 : 0;
     if (mode == Mode::Jacobi) {
-        k_cg_rz<double><<<d.n_tiles, kBlock, 0, stream_>>>(d.tiles, st_, r_, d.x64, dinv0_, nullptr, q_, red_, ctl, 0);
+        launch_k(tuning_.pdl != 0, k_cg_rz<double>, d.n_tiles, kBlock, 0, stream_, d.tiles, st_, r_, d.x64, dinv0_, nullptr, q_, red_, ctl, 0);
         mark("cg_rz", 0, 24.0 * n);
         return;
     }
@@ -1296,7 +1314,7 @@ std::vector<ProfRecord> Engine::profile(Mode mode, int reps) {
     // right-hand side and the guess are overwritten by the next solve anyway)
     {
         const int n = lv_[0].n_rows;
-        k_fill_rows<<<grid_of(n), 256, 0, stream_>>>(n, row_map_, 1.0, b_);
+        launch_k(tuning_.pdl != 0, k_fill_rows, grid_of(n), 256, 0, stream_, n, row_map_, 1.0, b_);
         CFDB_CUDA(cudaMemsetAsync(x_, 0, sizeof(double) * n, stream_));
         launches_ += 1;
     }
@@ -1443,7 +1461,7 @@ std::vector<SolveResult> Engine::solve(Mode mode, const std::vector<SolveRequest
     // true residual for reporting
     const DevLevel& d = lv_[0];
     with_visit(krylov_visit(), [&](auto V) {
-        k_true_residual<decltype(V)::value><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, st_, b_, x_, red_);
+        launch_k(tuning_.pdl != 0, k_true_residual<decltype(V)::value>, d.n_tiles, kBlock, 0, stream_, d.a.s64, d.tiles, st_, b_, x_, red_);
     });
     ++launches_;
     CFDB_CUDA(cudaGetLastError());
@@ -1514,12 +1532,12 @@ double Engine::time_sweep(int level, int reps, double* bytes) {
         }
         with_visit(visit, [&](auto V) {
             if (level == 0) {
-                k_vc_jacobi<T, double, decltype(V)::value><<<grid, m.block, 0, stream_>>>(op, tiles, nullptr, wd, r_, x, y);
+                launch_k(tuning_.pdl != 0, k_vc_jacobi<T, double, decltype(V)::value>, grid, m.block, 0, stream_, op, tiles, nullptr, wd, r_, x, y);
             } else {
                 const T* bv;
                 if constexpr (sizeof(T) == 8) bv = d.b64;
                 else bv = d.b32;
-                k_vc_jacobi<T, T, decltype(V)::value><<<grid, m.block, 0, stream_>>>(op, tiles, nullptr, wd, bv, x, y);
+                launch_k(tuning_.pdl != 0, k_vc_jacobi<T, T, decltype(V)::value>, grid, m.block, 0, stream_, op, tiles, nullptr, wd, bv, x, y);
             }
         });
     };
@@ -1544,10 +1562,10 @@ double Engine::time_level0_sweep(bool fp32, int reps) {
     CFDB_CUDA(cudaEventRecord(a, stream_));
     for (int i = 0; i < reps; ++i) {
         if (fp32) {
-            k_vc_jacobi<float, double, kVisitSell2><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s32, d.tiles, nullptr, d.wd32, r_,
+            launch_k(tuning_.pdl != 0, k_vc_jacobi<float, double, kVisitSell2>, d.n_tiles, kBlock, 0, stream_, d.a.s32, d.tiles, nullptr, d.wd32, r_,
                                                                          d.x32, d.y32);
         } else {
-            k_vc_jacobi<double, double, kVisitSell2><<<d.n_tiles, kBlock, 0, stream_>>>(d.a.s64, d.tiles, nullptr, d.wd64, r_,
+            launch_k(tuning_.pdl != 0, k_vc_jacobi<double, double, kVisitSell2>, d.n_tiles, kBlock, 0, stream_, d.a.s64, d.tiles, nullptr, d.wd64, r_,
                                                                           d.x64, d.y64);
         }
     }

@@ -47,6 +47,7 @@ struct Tuning {
     int col16 = 0;              // FP32 operators store 16-bit column offsets where they fit
     int tail_rows = 0;          // coarse levels of at most this many rows (and everything below
                                 // them) run as one persistent tail kernel; 0 disables it
+    int pdl = 1;                // programmatic dependent launch between consecutive kernels
 };
 
 struct SolveRequest {

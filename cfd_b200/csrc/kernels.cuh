@@ -28,6 +28,15 @@ constexpr int kBlock = 256;
 // a SELL operator's rows may be reordered by length.
 constexpr int kSellRows = kBlock;
 
+// Programmatic dependent launch (sm_90+): let the next kernel of the stream be scheduled once
+// every CTA of this one has started, then wait until the previous kernel has completed and its
+// writes are visible. Both are no-ops for a kernel launched without the attribute. Every kernel
+// below except the persistent tail calls it first, before touching global memory.
+__device__ __forceinline__ void pdl_entry() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // Storage of one sparse operator of a level, selected by `fmt`:
 //  0 (kFmtSell): SELL-32, one thread per row; `slice` = slice offsets. Row sums keep the CSR
 //     order.
@@ -506,6 +515,7 @@ static __global__ void k_fill_level0(int n_slots, int n_rows, const int* __restr
                               const int* __restrict__ diag_src, ValueSource vs, double weight,
                               double* __restrict__ val64, float* __restrict__ val32,
                               double* __restrict__ wd64, float* __restrict__ wd32) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n_slots) {
         const int s = __ldg(&src[i]);
@@ -526,6 +536,7 @@ static __global__ void k_fill_level0(int n_slots, int n_rows, const int* __restr
 // Engine layout <-> caller's concatenated vectors (map[i] = caller index of engine row i, or -1).
 static __global__ void k_gather_rows(int n, const int* __restrict__ map, const double* __restrict__ src,
                                      double* __restrict__ dst) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
         const int s = map[i];
@@ -535,12 +546,14 @@ static __global__ void k_gather_rows(int n, const int* __restrict__ map, const d
 
 // dst[i] = value on the caller's rows, 0 on padding rows.
 static __global__ void k_fill_rows(int n, const int* __restrict__ map, double value, double* __restrict__ dst) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = map[i] >= 0 ? value : 0.0;
 }
 
 static __global__ void k_scatter_rows(int n, const int* __restrict__ map, const double* __restrict__ src,
                                       double* __restrict__ dst) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
         const int s = map[i];
@@ -592,6 +605,7 @@ static __global__ void __launch_bounds__(kBlock, (kMinBlocks<T, V>)) k_vc_first(
                                                      const T* __restrict__ wd,
                                                      const B* __restrict__ b, T* __restrict__ y,
                                                      int fused2) {
+    pdl_entry();
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     auto x1 = [&](int j) -> T {
@@ -613,6 +627,7 @@ static __global__ void __launch_bounds__(kBlock, (kMinBlocks<T, V>)) k_vc_jacobi
                                                       const T* __restrict__ wd,
                                                       const B* __restrict__ b,
                                                       const T* __restrict__ x, T* __restrict__ y) {
+    pdl_entry();
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     visit_rows_v<V>(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
@@ -626,6 +641,7 @@ static __global__ void __launch_bounds__(kBlock, (kMinBlocks<T, V>)) k_vc_residu
                                                         const B* __restrict__ b,
                                                         const T* __restrict__ x,
                                                         T* __restrict__ t) {
+    pdl_entry();
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     visit_rows_v<V>(a, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
@@ -640,6 +656,7 @@ static __global__ void __launch_bounds__(kBlock, (kMinBlocks<T, V>)) k_vc_spmv(S
                                                     const T* __restrict__ x, T* __restrict__ y,
                                                     const T* __restrict__ wd1, T* __restrict__ x1,
                                                     int n1) {
+    pdl_entry();
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     visit_rows_v<V>(m, c.r0, c.r1, [x](int j) { return x[j]; }, [&](int row, T s) {
@@ -654,6 +671,7 @@ template <class T, int V>
 static __global__ void __launch_bounds__(kBlock, (kMinBlocks<T, V>)) k_vc_prolong(Sell<T> p, Tiles tiles, const SysState* st,
                                                        const T* __restrict__ xc,
                                                        T* __restrict__ x) {
+    pdl_entry();
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     visit_rows_v<V>(p, c.r0, c.r1, [xc](int j) { return xc[j]; }, [&](int row, T s) {
@@ -695,6 +713,7 @@ static __global__ void __launch_bounds__(kBlock) k_vc_coarse(CoarseBlocks cb, co
                                                       TX* const* __restrict__ x_level,
                                                       const int* __restrict__ block_level,
                                                       Control ctl, int ordered) {
+    pdl_entry();
     using T = TB;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar;
@@ -783,6 +802,7 @@ static __global__ void __launch_bounds__(kBlock) k_cg_init(Sell<double> a, Tiles
                                                     const double* __restrict__ x,
                                                     double* __restrict__ r, Reduce red,
                                                     Control ctl, X1Out x1o) {
+    pdl_entry();
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     double rr = 0.0, unused = 0.0;
@@ -815,6 +835,7 @@ static __global__ void __launch_bounds__(kBlock) k_cg_pupdate(Tiles tiles, const
                                                        const double* __restrict__ r,
                                                        const double* __restrict__ jac0,
                                                        double* __restrict__ p) {
+    pdl_entry();
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     const bool first = st[c.s].first != 0;
@@ -844,6 +865,7 @@ static __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(Sell<double> a, Ti
                                                        const double* __restrict__ p,
                                                        double* __restrict__ q, Reduce red,
                                                        Control ctl) {
+    pdl_entry();
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     double pq = 0.0, unused = 0.0;
@@ -872,6 +894,7 @@ static __global__ void __launch_bounds__(kBlock) k_cg_xr(Tiles tiles, SysState* 
                                                   const double* __restrict__ p,
                                                   const double* __restrict__ q, Reduce red,
                                                   Control ctl, int verify_true, X1Out x1o) {
+    pdl_entry();
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     const double alpha = st[c.s].alpha;
@@ -922,6 +945,7 @@ static __global__ void __launch_bounds__(kBlock) k_cg_true_check(Sell<double> a,
                                                           const double* __restrict__ x,
                                                           double* __restrict__ r, Reduce red,
                                                           Control ctl, X1Out x1o) {
+    pdl_entry();
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     if (st[c.s].check == 0) return;
@@ -978,6 +1002,7 @@ static __global__ void __launch_bounds__(kBlock) k_vc_jacobi_final(Sell<T> a, Ti
                                                             const double* __restrict__ q,
                                                             Reduce red, Control ctl,
                                                             int flexible) {
+    pdl_entry();
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     double rz = 0.0, zq = 0.0;
@@ -1004,6 +1029,7 @@ static __global__ void __launch_bounds__(kBlock) k_cg_rz(Tiles tiles, SysState* 
                                                   const double* __restrict__ jac0,
                                                   const double* __restrict__ q, Reduce red,
                                                   Control ctl, int flexible) {
+    pdl_entry();
     TileCtx c;
     if (!tile_begin(tiles, st, c)) return;
     const bool jsys = st[c.s].jacobi != 0;
@@ -1048,6 +1074,7 @@ static __global__ void __launch_bounds__(kBlock) k_true_residual(Sell<double> a,
                                                           const double* __restrict__ b,
                                                           const double* __restrict__ x,
                                                           Reduce red) {
+    pdl_entry();
     TileCtx c;
     tile_begin(tiles, nullptr, c);
     double rr = 0.0, unused = 0.0;
@@ -1069,6 +1096,7 @@ static __global__ void k_assemble_faces(int nf, const double* __restrict__ flux,
                                  const double* __restrict__ gamma,
                                  const double* __restrict__ delta, double convection,
                                  double* __restrict__ upper, double* __restrict__ lower) {
+    pdl_entry();
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nf) return;
     const double fl = flux[f];
@@ -1094,6 +1122,7 @@ static __global__ void k_assemble_pressure_cells(int n, const int* __restrict__ 
                                                  const int* __restrict__ ref_mask, double ref_value,
                                                  double* __restrict__ diag,
                                                  double* __restrict__ source) {
+    pdl_entry();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     double d = diag0 != nullptr ? diag0[c] : 0.0;
@@ -1122,6 +1151,7 @@ static __global__ void k_assemble_cells(int n, const int* __restrict__ cf_ptr,
                                  const double* __restrict__ delta, const int* __restrict__ owner,
                                  double convection, double* __restrict__ diag,
                                  double* __restrict__ div) {
+    pdl_entry();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     double d = diag[c];

@@ -305,6 +305,8 @@ typedef struct {
                          persistent kernel; 0 (default) disables it */
     int col16;        /* FP32 operators keep 16-bit column offsets from a per-slice / per-row base
                          where every slice / row spans fewer than 65536 columns, default 0 */
+    int pdl;          /* programmatic dependent launch between consecutive kernels (a kernel is
+                         scheduled while its predecessor drains), default 1 */
 } cfdb_tuning;
 void cfdb_default_tuning(cfdb_tuning* t);
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t);

@@ -18,13 +18,16 @@ void check_cuda(cudaError_t e, const char* what) {
 
 namespace {
 
-// One pool per device, created on first use; freed blocks stay in the pool (no release
-// threshold) and are reused by later allocations of any thread.
-cudaMemPool_t device_pool(int device) {
+// Two pools per device, created on first use: one for long-lived plan arrays and one for
+// transient setup scratch, so that the scratch of one setup finds the blocks of the previous
+// setup free instead of interleaved with arrays that stay. Freed blocks stay in their pool (no
+// release threshold) and are reused by later allocations of any thread.
+cudaMemPool_t device_pool(int device, bool transient) {
     static std::mutex mu;
     static std::map<int, cudaMemPool_t> pools;
     std::lock_guard<std::mutex> lock(mu);
-    auto it = pools.find(device);
+    const int key = 2 * device + (transient ? 1 : 0);
+    auto it = pools.find(key);
     if (it != pools.end()) return it->second;
     cudaMemPoolProps props{};
     props.allocType = cudaMemAllocationTypePinned;
@@ -34,20 +37,20 @@ cudaMemPool_t device_pool(int device) {
     check_cuda(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
     uint64_t keep = UINT64_MAX;
     check_cuda(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
-    pools[device] = pool;
+    pools[key] = pool;
     return pool;
 }
 
 } // namespace
 
-void DeviceBuffer::allocate(size_t bytes) {
+void DeviceBuffer::allocate(size_t bytes, bool transient) {
     release();
     int dev = 0;
     check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
     void* p = nullptr;
     // allocated in the order of this thread's default stream, then completed, so the block
     // can be used from any stream
-    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, device_pool(dev), cudaStreamPerThread);
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, device_pool(dev, transient), cudaStreamPerThread);
     if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();

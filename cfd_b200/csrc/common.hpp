@@ -40,7 +40,7 @@ struct HostCsr {
 class DeviceBuffer {
 public:
     DeviceBuffer() = default;
-    explicit DeviceBuffer(size_t bytes) { allocate(bytes); }
+    explicit DeviceBuffer(size_t bytes) { allocate(bytes, false); }
     ~DeviceBuffer() { release(); }
     DeviceBuffer(const DeviceBuffer&) = delete;
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
@@ -58,7 +58,8 @@ public:
         }
         return *this;
     }
-    void allocate(size_t bytes);
+    // transient: from the pool of short-lived setup scratch
+    void allocate(size_t bytes, bool transient = false);
     void release();
     [[nodiscard]] void* get() const { return ptr_; }
     template <class T> [[nodiscard]] T* as() const { return static_cast<T*>(ptr_); }

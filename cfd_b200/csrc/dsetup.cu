@@ -32,7 +32,7 @@ void* Scratch::raw(size_t bytes) {
         const size_t last = chunks_.empty() ? 0 : chunks_.back().buf.bytes();
         const size_t sz = std::max({bytes, 2 * last, static_cast<size_t>(4) << 20});
         chunks_.emplace_back();
-        chunks_.back().buf.allocate(sz);
+        chunks_.back().buf.allocate(sz, /*transient=*/true);
         total_ += sz;
     }
     Chunk& c = chunks_.back();
@@ -342,10 +342,17 @@ __global__ void __launch_bounds__(G* PER) k_gemm_rows(GemmArgs g) {
     int cap = CAP;
     int* keys;
     double* vals = nullptr;
+    double* sv = nullptr; // warp groups, numeric: the chunk's contributions, one per lane
     if constexpr (CAP > 0) {
         if constexpr (NUMERIC) {
-            vals = reinterpret_cast<double*>(smem) + static_cast<size_t>(grp) * CAP;
-            keys = reinterpret_cast<int*>(reinterpret_cast<double*>(smem) + static_cast<size_t>(PER) * CAP) + grp * CAP;
+            double* base = reinterpret_cast<double*>(smem);
+            vals = base + static_cast<size_t>(grp) * CAP;
+            if constexpr (G == 32) {
+                sv = base + static_cast<size_t>(PER) * CAP + grp * 32;
+                keys = reinterpret_cast<int*>(base + static_cast<size_t>(PER) * (CAP + 32)) + grp * CAP;
+            } else {
+                keys = reinterpret_cast<int*>(base + static_cast<size_t>(PER) * CAP) + grp * CAP;
+            }
         } else {
             keys = reinterpret_cast<int*>(smem) + grp * CAP;
         }
@@ -362,44 +369,127 @@ __global__ void __launch_bounds__(G* PER) k_gemm_rows(GemmArgs g) {
     group_sync<G>();
     const int limit = min(g.limit, cap - cap / 4);
     const int a0 = g.arp[i], a1 = g.arp[i + 1];
-    for (int ka = a0; ka < a1; ++ka) {
-        const int k = g.aci[ka];
-        double av = 0.0;
-        if constexpr (NUMERIC) {
-            av = g.ava[ka];
-            if (g.ascale != nullptr) av = __dmul_rn(g.ascale[i], av);
+    // slot of key j (inserted when absent; fresh = inserted now), or -1 when the table is full
+    auto find = [&](int j, bool& fresh) -> int {
+        unsigned h = slot_of(j, cap);
+        for (int probes = 0; probes < cap; ++probes) {
+            const int prev = atomicCAS(&keys[h], kEmpty, j);
+            if (prev == kEmpty || prev == j) {
+                fresh = prev == kEmpty;
+                return static_cast<int>(h);
+            }
+            h = (h + 1) & static_cast<unsigned>(cap - 1);
         }
-        const int b0 = g.brp != nullptr ? g.brp[k] : k;
-        const int b1 = g.brp != nullptr ? g.brp[k + 1] : k + 1;
-        for (int kb = b0 + t; kb < b1; kb += G) {
-            const int j = g.brp != nullptr ? g.bci[kb] : g.tent[kb];
-            unsigned h = slot_of(j, cap);
-            int probes = 0;
-            for (;;) {
-                const int prev = atomicCAS(&keys[h], kEmpty, j);
-                if (prev == kEmpty) {
-                    if constexpr (NUMERIC) {
-                        vals[h] = __dmul_rn(av, g.brp != nullptr ? g.bva[kb] : 1.0);
-                    } else {
-                        atomicAdd(&s_count[grp], 1);
-                    }
-                    break;
+        return -1;
+    };
+    if constexpr (G == 32 && CAP > 0) {
+        // Warp groups take the row's contributions 32 at a time in their order (k ascending
+        // over A(i,:), then B(k,:)), whatever k-groups a chunk spans. Within a chunk, the lanes
+        // holding one column are matched; the lowest of them adds their values in lane order.
+        const unsigned full = 0xffffffffu;
+        const int lane = t;
+        for (int w0 = a0; w0 < a1; w0 += 32) {
+            const int q = w0 + lane;
+            int len = 0, bstart = 0;
+            double av = 0.0;
+            if (q < a1) {
+                const int kk = g.aci[q];
+                if (g.brp != nullptr) {
+                    bstart = g.brp[kk];
+                    len = g.brp[kk + 1] - bstart;
+                } else {
+                    bstart = kk;
+                    len = 1;
                 }
-                if (prev == j) {
-                    if constexpr (NUMERIC) vals[h] = __dadd_rn(vals[h], __dmul_rn(av, g.brp != nullptr ? g.bva[kb] : 1.0));
-                    break;
-                }
-                h = (h + 1) & static_cast<unsigned>(cap - 1);
-                if (++probes >= cap) { // full table: symbolic overflow, numeric error
-                    s_over[grp] = 1;
-                    break;
+                if constexpr (NUMERIC) {
+                    av = g.ava[q];
+                    if (g.ascale != nullptr) av = __dmul_rn(g.ascale[i], av);
                 }
             }
+            int inc = len;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(full, inc, o);
+                if (lane >= o) inc += y;
+            }
+            const int total = __shfl_sync(full, inc, 31);
+            const int exc = inc - len;
+            bool stop = false;
+            for (int f0 = 0; f0 < total && !stop; f0 += 32) {
+                const int f = f0 + lane;
+                const bool active = f < total;
+                int src = 0; // first lane whose inclusive prefix exceeds f
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int v = __shfl_sync(full, inc, src + step - 1);
+                    if (v <= f) src += step;
+                }
+                const int off = f - __shfl_sync(full, exc, src);
+                const int kb = __shfl_sync(full, bstart, src) + off;
+                const double avs = __shfl_sync(full, av, src);
+                const int j = active ? (g.brp != nullptr ? g.bci[kb] : g.tent[kb]) : -1 - lane;
+                if constexpr (NUMERIC) {
+                    sv[lane] = active ? __dmul_rn(avs, g.brp != nullptr ? g.bva[kb] : 1.0) : 0.0;
+                    const unsigned same = __match_any_sync(full, j);
+                    __syncwarp();
+                    if (active && lane == __ffs(same) - 1) {
+                        bool fresh = false;
+                        const int h = find(j, fresh);
+                        if (h < 0) {
+                            s_over[grp] = 1;
+                        } else {
+                            unsigned m = same & (same - 1u); // the others, ascending
+                            double acc = fresh ? sv[lane] : __dadd_rn(vals[h], sv[lane]);
+                            while (m != 0u) {
+                                const int b = __ffs(m) - 1;
+                                m &= m - 1u;
+                                acc = __dadd_rn(acc, sv[b]);
+                            }
+                            vals[h] = acc;
+                        }
+                    }
+                } else {
+                    if (active) {
+                        bool fresh = false;
+                        const int h = find(j, fresh);
+                        if (h < 0) s_over[grp] = 1;
+                        else if (fresh) atomicAdd(&s_count[grp], 1);
+                    }
+                }
+                __syncwarp();
+                stop = s_over[grp] || (!NUMERIC && s_count[grp] > limit);
+                __syncwarp(); // every lane has read the flags before any lane updates them again
+            }
+            if (stop) break; // uniform within the warp
         }
-        group_sync<G>();
-        const bool stop = s_over[grp] || (!NUMERIC && s_count[grp] > limit);
-        group_sync<G>(); // every thread has read the flags before any thread updates them again
-        if (stop) break; // uniform within the group
+    } else {
+        for (int ka = a0; ka < a1; ++ka) {
+            const int k = g.aci[ka];
+            double av = 0.0;
+            if constexpr (NUMERIC) {
+                av = g.ava[ka];
+                if (g.ascale != nullptr) av = __dmul_rn(g.ascale[i], av);
+            }
+            const int b0 = g.brp != nullptr ? g.brp[k] : k;
+            const int b1 = g.brp != nullptr ? g.brp[k + 1] : k + 1;
+            for (int kb = b0 + t; kb < b1; kb += G) {
+                const int j = g.brp != nullptr ? g.bci[kb] : g.tent[kb];
+                bool fresh = false;
+                const int h = find(j, fresh);
+                if (h < 0) { // full table: symbolic overflow, numeric error
+                    s_over[grp] = 1;
+                    continue;
+                }
+                if constexpr (NUMERIC) {
+                    const double c = __dmul_rn(av, g.brp != nullptr ? g.bva[kb] : 1.0);
+                    vals[h] = fresh ? c : __dadd_rn(vals[h], c);
+                } else {
+                    if (fresh) atomicAdd(&s_count[grp], 1);
+                }
+            }
+            group_sync<G>();
+            const bool stop = s_over[grp] || (!NUMERIC && s_count[grp] > limit);
+            group_sync<G>(); // every thread has read the flags before any thread updates them again
+            if (stop) break; // uniform within the group
+        }
     }
     if constexpr (!NUMERIC) {
         if (t == 0) {
@@ -709,17 +799,18 @@ template <bool NUMERIC> void gemm_launch(Ctx& cx, GemmArgs g, int cls, const int
     if (n_list <= 0) return;
     g.rows = rows;
     g.n_list = n_list;
-    const size_t b = NUMERIC ? 12 : 4; // bytes per slot
+    const size_t b = NUMERIC ? 12 : 4;      // bytes per slot
+    const size_t chunk = NUMERIC ? 32 * 8 : 0; // warp groups: one chunk of contributions
     cudaStream_t st = cx.st;
     switch (cls) {
     case 0:
-        k_gemm_rows<NUMERIC, 32, 64, 8><<<(n_list + 7) / 8, 256, 8 * 64 * b, st>>>(g);
+        k_gemm_rows<NUMERIC, 32, 64, 8><<<(n_list + 7) / 8, 256, 8 * (64 * b + chunk), st>>>(g);
         break;
     case 1:
-        k_gemm_rows<NUMERIC, 32, 128, 8><<<(n_list + 7) / 8, 256, 8 * 128 * b, st>>>(g);
+        k_gemm_rows<NUMERIC, 32, 128, 8><<<(n_list + 7) / 8, 256, 8 * (128 * b + chunk), st>>>(g);
         break;
     case 2:
-        k_gemm_rows<NUMERIC, 32, 512, 4><<<(n_list + 3) / 4, 128, 4 * 512 * b, st>>>(g);
+        k_gemm_rows<NUMERIC, 32, 512, 4><<<(n_list + 3) / 4, 128, 4 * (512 * b + chunk), st>>>(g);
         break;
     case 3:
         k_gemm_rows<NUMERIC, kThreads, 2048, 1><<<n_list, kThreads, 2048 * b, st>>>(g);

@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serve: arrival rates (1/s)")
     ap.add_argument("--requests", type=int, default=200, help="serve: requests per rate")
     ap.add_argument("--slots", type=int, default=4, help="serve: worker slots")
+    ap.add_argument("--serve-pdl", type=int, default=0, help="serve: programmatic dependent launch (0/1)")
+    ap.add_argument("--max-age", type=int, default=20,
+                    help="serve: hierarchy rebuilt after this many solves of a mesh (AmgCache::max_age; 0: never)")
     ap.add_argument("--size", type=int, default=0, help="override the mesh edge length")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -667,7 +670,8 @@ def run_serve(args, rank, world, local_rank):
     res = {}
 
     def server(prec, slots):
-        srv = S.Server(slots=slots, hbm_budget_bytes=150e9, precision=prec, settings=settings)
+        srv = S.Server(slots=slots, hbm_budget_bytes=150e9, precision=prec, settings=settings,
+                       max_age=args.max_age, pdl=args.serve_pdl)
         pool = S.make_pool(srv, pool_cases, variants=3, seed=7)
         t0 = time.perf_counter()
         for e in pool:  # hierarchy builds (AmgCache setup), not timed below
@@ -702,8 +706,10 @@ def run_serve(args, rank, world, local_rank):
         "config": {"workload": "serve box/tet pool", "box_edges": list(W.SERVE_BOX_EDGES),
                    "tet_edges": list(W.SERVE_TET_EDGES), "tet_share": 0.25, "repeat_share": 0.3,
                    "slots": args.slots, "hbm_budget_gb": 150, "rates_hz": rates,
+                   "max_age": args.max_age,
                    "requests_per_rate": n_req, "strength_threshold": THETA,
-                   "step": "one request: H2D of its matrix (new key) and rhs, AMG-PCG to 1e-8, D2H of x",
+                   "step": "one request: H2D of its matrix (new key) and rhs, hierarchy rebuilt on the "
+                           "device when the mesh has served max_age solves, AMG-PCG to 1e-8, D2H of x",
                    "parallelism": f"replicas x{world}"},
         "mixed": res["mixed"], "fp64": res["fp64"], "one_at_a_time_fp64": res["one_at_a_time_fp64"],
         "served_mixed_vs_one_at_a_time_fp64": value / res["one_at_a_time_fp64"]["solves_per_s"],

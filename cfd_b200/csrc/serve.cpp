@@ -153,6 +153,10 @@ void execute(cfdb_server& s, Resident& r, const Mesh& m, Request& q, bool create
         check(cfdb_system_create_mesh(m.n, m.nf, m.owner.data(), m.neighbour.data(), &r.sys));
         check(cfdb_system_set_precision(r.sys, s.cfg.precision));
         check(cfdb_system_set_keep_levels(r.sys, 0)); // the plan of a resident system never changes
+        cfdb_tuning tun;
+        cfdb_default_tuning(&tun);
+        tun.pdl = s.cfg.pdl;
+        check(cfdb_system_set_tuning(r.sys, &tun));
         dmalloc(&r.d_diag, m.n);
         dmalloc(&r.d_upper, m.nf);
         dmalloc(&r.d_lower, m.nf);
@@ -295,6 +299,7 @@ void cfdb_default_server_config(cfdb_server_config* c) {
     c->precision = CFDB_PRECISION_MIXED;
     cfdb_default_amg_settings(&c->settings);
     c->max_age = 0;
+    c->pdl = 0;
 }
 
 int cfdb_server_create(const cfdb_server_config* cfg, cfdb_server** out) {

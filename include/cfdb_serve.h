@@ -25,6 +25,10 @@ typedef struct {
     int precision;              /* cfdb_precision of the solves, default MIXED */
     cfdb_amg_settings settings; /* hierarchy settings */
     int max_age;                /* rebuild the hierarchy after this many solves (0: never) */
+    int pdl;                    /* programmatic dependent launch in the resident systems' solves
+                                   (cfdb_tuning.pdl), default 0: with requests overlapping on
+                                   the GPU, kernels scheduled early would hold SM slots that
+                                   other requests' kernels can use */
 } cfdb_server_config;
 
 typedef struct {

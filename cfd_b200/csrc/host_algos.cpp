@@ -173,17 +173,21 @@ HostCsr transpose(const HostCsr& a) {
     t.ci.resize(static_cast<size_t>(a.nnz()));
     t.va.resize(static_cast<size_t>(a.nnz()));
     const int nt = a.n_rows > 4096 ? omp_get_max_threads() : 1;
-    std::vector<std::vector<int>> cnt(static_cast<size_t>(nt));
-    auto block = [&](int tid, int& r0, int& r1) {
-        const long long n = a.n_rows;
-        r0 = static_cast<int>(n * tid / nt);
-        r1 = static_cast<int>(n * (tid + 1) / nt);
-    };
+    // The rows are split over the threads the team actually has: inside another parallel
+    // region (a batch of systems set up in parallel) a nested team has one thread.
+    std::vector<std::vector<int>> cnt;
+    int team = 1;
 #pragma omp parallel num_threads(nt) if (nt > 1)
     {
+#pragma omp single
+        {
+            team = omp_get_num_threads();
+            cnt.resize(static_cast<size_t>(team));
+        }
         const int tid = omp_get_thread_num();
-        int r0, r1;
-        block(tid, r0, r1);
+        const long long n_rows = a.n_rows;
+        const int r0 = static_cast<int>(n_rows * tid / team);
+        const int r1 = static_cast<int>(n_rows * (tid + 1) / team);
         std::vector<int>& c = cnt[static_cast<size_t>(tid)];
         c.assign(static_cast<size_t>(m), 0);
         for (int i = r0; i < r1; ++i)
@@ -194,7 +198,7 @@ HostCsr transpose(const HostCsr& a) {
             // row lengths, then each thread's starting offset within every row
             for (int j = 0; j < m; ++j) {
                 int len = 0;
-                for (int q = 0; q < nt; ++q) {
+                for (int q = 0; q < team; ++q) {
                     const int v = cnt[static_cast<size_t>(q)][j];
                     cnt[static_cast<size_t>(q)][j] = len;
                     len += v;

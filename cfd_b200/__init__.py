@@ -134,6 +134,7 @@ _proto("cfdb_system_assemble", [_vp, _pd, _pd, _pd, _d, _pd, _pd, _pd, _pd])
 _proto("cfdb_system_assemble_pressure_device", [_vp, _vp, _vp, _vp, _vp, _vp, _i, _d, _vp, _vp,
                                                 _vp, _vp])
 _proto("cfdb_system_kernel_launches", [_vp, _P(C.c_ulonglong)])
+_proto("cfdb_system_correct_pressure_device", [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _vp, _vp])
 
 
 class TuningStruct(C.Structure):
@@ -753,6 +754,15 @@ class DeviceSolver:
             self._h, _devptr(flux), _devptr(gamma), _devptr(delta),
             _devptr(diag0) if diag0 is not None else None, _devptr(source0), int(ref_cell),
             float(ref_value), _devptr(upper), _devptr(lower), _devptr(diag), _devptr(source)))
+
+    def correct_pressure_device(self, flux, gamma, delta, p_new, phi, p, p_prev=None, alpha=1.0,
+                                non_orth=None) -> None:
+        """Conservative face flux phi and under-relaxed pressure p after the pressure solve
+        (flow_solver.cpp:821-840), on device arrays; enqueued on the solver's stream."""
+        _check(_lib.cfdb_system_correct_pressure_device(
+            self._h, _devptr(flux), _devptr(gamma), _devptr(delta),
+            _devptr(non_orth) if non_orth is not None else None, _devptr(p_new),
+            _devptr(p_prev) if p_prev is not None else None, float(alpha), _devptr(phi), _devptr(p)))
 
     def kernel_launches(self) -> int:
         c = C.c_ulonglong()

@@ -177,6 +177,7 @@ struct cfdb_system {
     // device copies for the fused face assembly
     DeviceArena asm_arena;
     int* d_owner = nullptr;
+    int* d_neighbour = nullptr; // uploaded on first use (flux correction)
     int* d_cf_ptr = nullptr;
     int* d_cf_face = nullptr;
     double* h_asm = nullptr; // device staging of cfdb_system_assemble (host-array variant)
@@ -1144,6 +1145,32 @@ int cfdb_system_assemble_pressure_device(cfdb_system* sys, const double* flux, c
         k_assemble_pressure_cells<<<(n + 255) / 256, 256, 0, st>>>(n, sys->d_cf_ptr, sys->d_cf_face, flux, gamma,
                                                                    delta, sys->d_owner, diag0, source0, ref_cell,
                                                                    nullptr, ref_value, diag, source);
+        ++sys->launches;
+        CFDB_CUDA(cudaGetLastError());
+    });
+}
+
+int cfdb_system_correct_pressure_device(cfdb_system* sys, const double* flux, const double* gamma,
+                                        const double* delta, const double* non_orth, const double* p_new,
+                                        const double* p_prev, double alpha, double* phi, double* p) {
+    return guarded([&] {
+        if (sys == nullptr) fail(CFDB_ERR_BAD_ARG, "null system");
+        if (sys->d_cf_ptr == nullptr) fail(CFDB_ERR_BAD_ARG, "system was not created from mesh addressing");
+        const int n = sys->pat.n, nf = sys->pat.n_faces;
+        if (p_new == nullptr || p == nullptr || (nf > 0 && (!flux || !gamma || !delta || !phi)))
+            fail(CFDB_ERR_BAD_ARG, "null array");
+        CFDB_CUDA(cudaSetDevice(sys->device));
+        ensure_engine(sys);
+        cudaStream_t st = sys->eng->stream();
+        if (nf > 0) {
+            if (sys->d_neighbour == nullptr) {
+                sys->d_neighbour = sys->asm_arena.upload(sys->neighbour, st);
+            }
+            k_correct_flux<<<(nf + 255) / 256, 256, 0, st>>>(nf, sys->d_owner, sys->d_neighbour, flux, gamma, delta,
+                                                             non_orth, p_new, phi);
+            ++sys->launches;
+        }
+        k_relax<<<(n + 255) / 256, 256, 0, st>>>(n, p_prev, p_new, alpha, p);
         ++sys->launches;
         CFDB_CUDA(cudaGetLastError());
     });

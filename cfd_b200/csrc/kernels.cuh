@@ -1107,6 +1107,31 @@ static __global__ void k_assemble_faces(int nf, const double* __restrict__ flux,
     lower[f] = __dsub_rn(-pos, g);
 }
 
+// Conservative face flux from the pressure solution (flow_solver.cpp:821-826):
+// phi = flux - (gamma * delta) * (p[N] - p[P]) - non_orth (non_orth may be null: zero),
+// rounded in that order.
+static __global__ void k_correct_flux(int nf, const int* __restrict__ owner, const int* __restrict__ neighbour,
+                                      const double* __restrict__ flux, const double* __restrict__ gamma,
+                                      const double* __restrict__ delta, const double* __restrict__ non_orth,
+                                      const double* __restrict__ p, double* __restrict__ phi) {
+    pdl_entry();
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const double dp = __dsub_rn(p[neighbour[f]], p[owner[f]]);
+    const double v = __dsub_rn(flux[f], __dmul_rn(__dmul_rn(gamma[f], delta[f]), dp));
+    phi[f] = __dsub_rn(v, non_orth != nullptr ? non_orth[f] : 0.0);
+}
+
+// Pressure under-relaxation (flow_solver.cpp:837-840): p = p_prev + alpha (p_new - p_prev), or
+// p = p_new when p_prev is null.
+static __global__ void k_relax(int n, const double* __restrict__ p_prev, const double* __restrict__ p_new,
+                               double alpha, double* __restrict__ p) {
+    pdl_entry();
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    p[c] = p_prev != nullptr ? __dadd_rn(p_prev[c], __dmul_rn(alpha, __dsub_rn(p_new[c], p_prev[c]))) : p_new[c];
+}
+
 // Pressure assembly epilogue fused into the cell gather (flow_solver.cpp:768-770 and 794-796):
 // diag = diag0 + sum of face coefficients, source = source0 - div(flux), then
 // set_reference(ref_cell, ref_value): source += diag * value, diag += diag (for the cell

@@ -281,6 +281,15 @@ int cfdb_system_assemble(cfdb_system* sys, const double* flux, const double* gam
  * diag = diag0 + sum of gamma*delta (diag0 may be NULL: zero), source = source0 - div(flux),
  * then set_reference(ref_cell, ref_value) unless ref_cell < 0. Requires
  * cfdb_system_create_mesh. */
+/* The steps of FlowSolver::pressure_correction after the pressure solve, for internal faces on
+ * device arrays: the conservative face flux phi = flux - gamma*delta*(p_new[N] - p_new[P]) -
+ * non_orth (flow_solver.cpp:821-826; non_orth may be NULL: zero) and the under-relaxed
+ * pressure p = p_prev + alpha (p_new - p_prev) (flow_solver.cpp:837-840; p_prev NULL: p =
+ * p_new). Enqueued on the system's stream. Requires cfdb_system_create_mesh. */
+int cfdb_system_correct_pressure_device(cfdb_system* sys, const double* flux, const double* gamma,
+                                        const double* delta, const double* non_orth,
+                                        const double* p_new, const double* p_prev, double alpha,
+                                        double* phi, double* p);
 int cfdb_system_assemble_pressure_device(cfdb_system* sys, const double* flux,
                                          const double* gamma, const double* delta_coeff,
                                          const double* diag0, const double* source0,

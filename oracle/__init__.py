@@ -237,6 +237,22 @@ def normalised_residual(owner, neighbour, diag, upper, lower, source, x):
     return res / (norm + 1e-20)
 
 
+def correct_flux(owner, neighbour, flux, gamma, delta, p, non_orth=None):
+    """Conservative internal-face flux of FlowSolver::pressure_correction
+    (flow_solver.cpp:821-826): phi_hbya - rau_f * dc * (p[N] - p[P]) - non_orth, elementwise in
+    that rounding order (numpy float64 rounds each operation; no fused multiply-add)."""
+    own, nei = np.asarray(owner), np.asarray(neighbour)
+    no = np.zeros(len(nei)) if non_orth is None else np.asarray(non_orth, np.float64)
+    return (np.asarray(flux, np.float64) - (np.asarray(gamma, np.float64) * np.asarray(delta, np.float64))
+            * (np.asarray(p)[nei] - np.asarray(p)[own])) - no
+
+
+def relax(p_prev, p_new, alpha):
+    """Pressure under-relaxation of FlowSolver::pressure_correction (flow_solver.cpp:837-840)."""
+    p_prev, p_new = np.asarray(p_prev, np.float64), np.asarray(p_new, np.float64)
+    return p_prev + alpha * (p_new - p_prev)
+
+
 def set_reference(diag, source, cell, value):
     """In place, like LduMatrix::set_reference."""
     assert diag.dtype == np.float64 and source.dtype == np.float64

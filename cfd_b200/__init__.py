@@ -135,6 +135,10 @@ _proto("cfdb_system_assemble_pressure_device", [_vp, _vp, _vp, _vp, _vp, _vp, _i
                                                 _vp, _vp])
 _proto("cfdb_system_kernel_launches", [_vp, _P(C.c_ulonglong)])
 _proto("cfdb_system_correct_pressure_device", [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _vp, _vp])
+_proto("cfdb_fv_create", [_i, _i, _i, _pi, _pi, _pd, _pd, _pd, _pd, _pd, _pi, _pd, _P(_vp)])
+_proto("cfdb_fv_destroy", [_vp])
+_proto("cfdb_fv_pressure_gradient_device", [_vp, _vp, _vp])
+_proto("cfdb_fv_correct_velocity_device", [_vp, _vp, _vp, _vp, _vp])
 
 
 class TuningStruct(C.Structure):
@@ -980,6 +984,52 @@ class Mesh:
         if h and _lib is not None:  # the library may be gone at interpreter exit
             _lib.cfdb_mesh_destroy(h)
             self._h = None
+
+
+class BoundaryKind(enum.IntEnum):
+    """flow_solver.hpp:16 FlowBoundary."""
+    VelocityInlet = 0
+    Wall = 1
+    PressureOutlet = 2
+    Symmetry = 3
+    Empty = 4
+
+
+class FvGeometry:
+    """Device copy of a mesh's geometry for the pressure gradient and velocity correction of
+    FlowSolver::pressure_correction (flow_solver.cpp:339-372, 843-846)."""
+
+    def __init__(self, mesh: "Mesh", boundary_kind, boundary_pressure=None):
+        nb = mesh.n_faces - mesh.n_internal_faces
+        kinds = _i32(boundary_kind)
+        pout = _f64(boundary_pressure if boundary_pressure is not None else np.zeros(nb))
+        if len(kinds) != nb or len(pout) != nb:
+            raise InvalidArgument("one boundary kind and pressure per boundary face")
+        self.n_cells = mesh.n_cells
+        own, nei = _i32(mesh.owner), _i32(mesh.neighbour)
+        sf, cf = _f64(mesh.face_areas).ravel(), _f64(mesh.face_centres).ravel()
+        cc, vol, w = _f64(mesh.cell_centres).ravel(), _f64(mesh.cell_volumes), _f64(mesh.weights)
+        h = _vp()
+        _check(_lib.cfdb_fv_create(mesh.n_cells, mesh.n_faces, mesh.n_internal_faces, _ip(own), _ip(nei),
+                                   _dp(sf), _dp(cf), _dp(cc), _dp(vol), _dp(w), _ip(kinds), _dp(pout),
+                                   C.byref(h)))
+        self._h = h
+
+    def pressure_gradient_device(self, p, grad) -> None:
+        """grad (n_cells x 3, CUDA float64) of the cell pressure p (CUDA float64)."""
+        _check(_lib.cfdb_fv_pressure_gradient_device(self._h, _devptr(p), _devptr(grad)))
+
+    def correct_velocity_device(self, hbya, rau, grad, u) -> None:
+        _check(_lib.cfdb_fv_correct_velocity_device(self._h, _devptr(hbya), _devptr(rau),
+                                                    _devptr(grad), _devptr(u)))
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:  # the library may be gone at interpreter exit
+            _lib.cfdb_fv_destroy(h)
+            self._h = None
+
+    __del__ = close
 
 
 from . import workloads  # noqa: E402,F401  (configs of the pressure systems)

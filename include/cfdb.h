@@ -217,6 +217,35 @@ int cfdb_system_solve(cfdb_system* sys, const double* diag, const double* upper,
 int cfdb_system_solve_device(cfdb_system* sys, const double* diag, const double* upper,
                              const double* lower, const double* b, double* x, int method,
                              int use_amg, const cfdb_control* control, cfdb_stats* stats);
+/* ---- pressure gradient and velocity correction (FlowSolver::pressure_correction after the
+ * solve: pressure_gradient's Gauss branch, flow_solver.cpp:339-372, and u = HbyA - rAU grad p,
+ * flow_solver.cpp:843-846) on device arrays ---- */
+typedef enum { /* flow_solver.hpp:16 FlowBoundary */
+    CFDB_BC_VELOCITY_INLET = 0,
+    CFDB_BC_WALL = 1,
+    CFDB_BC_PRESSURE_OUTLET = 2,
+    CFDB_BC_SYMMETRY = 3,
+    CFDB_BC_EMPTY = 4
+} cfdb_boundary_kind;
+typedef struct cfdb_fv cfdb_fv;
+/* Mesh geometry in the reference's contract (host arrays, copied): owner (n_faces), neighbour
+ * and interpolation weights (internal faces), face area vectors and face centres (3 n_faces,
+ * xyz-interleaved), cell centres (3 n_cells), cell volumes; per boundary face (n_faces -
+ * n_internal_faces, in face order) its cfdb_boundary_kind and, for pressure outlets, the
+ * fixed pressure. */
+int cfdb_fv_create(int n_cells, int n_faces, int n_internal_faces, const int* owner,
+                   const int* neighbour, const double* face_areas, const double* face_centres,
+                   const double* cell_centres, const double* cell_volumes, const double* weights,
+                   const int* boundary_kind, const double* boundary_pressure, cfdb_fv** out);
+int cfdb_fv_destroy(cfdb_fv* fv);
+/* grad (3 n_cells) of the cell pressure p (n_cells): Gauss sums with boundary values p_P, or
+ * the outlet pressure, in two passes, the second extrapolating zero-gradient boundary values
+ * tangentially with the first pass's gradient. Device arrays; returns when done. */
+int cfdb_fv_pressure_gradient_device(cfdb_fv* fv, const double* p, double* grad);
+/* u = hbya - rau * grad (u, hbya, grad: 3 n_cells; rau: n_cells). Device arrays. */
+int cfdb_fv_correct_velocity_device(cfdb_fv* fv, const double* hbya, const double* rau,
+                                    const double* grad, double* u);
+
 /* ---- persistent LDU solve: LduMatrix::solve with "solver": {"device": "gpu"}
  * (ldu_matrix.cpp:111-131 with solve_persistent, ldu_matrix.cpp:287-366) ---- */
 typedef struct {

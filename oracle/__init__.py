@@ -9,6 +9,7 @@ The product package ``cfd_b200`` never imports it.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 from dataclasses import dataclass
 
@@ -245,6 +246,54 @@ def correct_flux(owner, neighbour, flux, gamma, delta, p, non_orth=None):
     no = np.zeros(len(nei)) if non_orth is None else np.asarray(non_orth, np.float64)
     return (np.asarray(flux, np.float64) - (np.asarray(gamma, np.float64) * np.asarray(delta, np.float64))
             * (np.asarray(p)[nei] - np.asarray(p)[own])) - no
+
+
+def pressure_gradient(n_cells, n_internal, owner, neighbour, weights, face_areas, face_centres,
+                      cell_centres, cell_volumes, kinds, outlet_pressure, p):
+    """FlowSolver::pressure_gradient, Gauss branch (flow_solver.cpp:339-372), face by face in the
+    reference's order: internal faces add S_f (w p_P + (1 - w) p_N) to the owner and subtract
+    it from the neighbour; two passes over the boundary faces add S_f p_b (p_b = outlet
+    pressure, else p_P; the second pass adds the tangential extrapolation prev_P . (d - (d.n) n)
+    to every non-outlet face); the sums are divided by the cell volume. Every product and sum
+    is rounded separately (Python floats). Small meshes only: plain loops. kinds: 2 = outlet."""
+    nf = len(owner)
+    internal = [[0.0, 0.0, 0.0] for _ in range(n_cells)]
+    for f in range(n_internal):
+        o, n = int(owner[f]), int(neighbour[f])
+        w = float(weights[f])
+        s = w * float(p[o]) + (1.0 - w) * float(p[n])
+        for i in range(3):
+            fl = float(face_areas[f][i]) * s
+            internal[o][i] = internal[o][i] + fl
+            internal[n][i] = internal[n][i] - fl
+    prev = None
+    for pas in range(2):
+        grad = [list(g) for g in internal]
+        for f in range(n_internal, nf):
+            c = int(owner[f])
+            b = f - n_internal
+            outlet = int(kinds[b]) == 2
+            pb = float(outlet_pressure[b]) if outlet else float(p[c])
+            sf = [float(v) for v in face_areas[f]]
+            if pas > 0 and not outlet:
+                area = math.sqrt((sf[0] * sf[0] + sf[1] * sf[1]) + sf[2] * sf[2])
+                nrm = [v / area for v in sf]
+                d = [float(face_centres[f][i]) - float(cell_centres[c][i]) for i in range(3)]
+                dn = (d[0] * nrm[0] + d[1] * nrm[1]) + d[2] * nrm[2]
+                t = [d[i] - dn * nrm[i] for i in range(3)]
+                pb = pb + ((prev[c][0] * t[0] + prev[c][1] * t[1]) + prev[c][2] * t[2])
+            for i in range(3):
+                grad[c][i] = grad[c][i] + sf[i] * pb
+        for c in range(n_cells):
+            v = float(cell_volumes[c])
+            grad[c] = [g / v for g in grad[c]]
+        prev = grad
+    return np.array(grad)
+
+
+def correct_velocity(hbya, rau, grad):
+    """u = HbyA - rAU grad p (flow_solver.cpp:843-846)."""
+    return np.asarray(hbya, np.float64) - np.asarray(rau, np.float64)[:, None] * np.asarray(grad, np.float64)
 
 
 def relax(p_prev, p_new, alpha):

@@ -264,3 +264,36 @@ def test_flux_correction_and_relaxation_bitwise(gpu):
         want_p = p_new if prev is None else O.relax(prev, p_new, alpha)
         assert np.array_equal(phi.cpu().numpy(), want_phi)
         assert np.array_equal(p.cpu().numpy(), want_p)
+
+
+@pytest.mark.parametrize("kind", ["box", "tet"])
+def test_pressure_gradient_and_velocity_correction_bitwise(gpu, kind):
+    """Gauss pressure gradient with the two-pass tangential boundary extrapolation and the
+    velocity correction on the device (flow_solver.cpp:339-372, 843-846), against the oracle's
+    face-by-face restatement, bit for bit; one wall is a pressure outlet."""
+    import torch
+    cb = gpu
+    m = cb.Mesh.box(6, 5, 4, xs=np.array([0.0, 0.1, 0.25, 0.45, 0.7, 0.85, 1.0])) if kind == "box" \
+        else cb.Mesh.tet(4, 3, 3, jitter=0.2, seed=9)
+    nb = m.n_faces - m.n_internal_faces
+    fc_b = m.face_centres[m.n_internal_faces:]
+    kinds = np.where(np.isclose(fc_b[:, 0], 1.0), int(cb.BoundaryKind.PressureOutlet),
+                     int(cb.BoundaryKind.Wall)).astype(np.int32)
+    kinds[np.isclose(fc_b[:, 0], 0.0)] = int(cb.BoundaryKind.VelocityInlet)
+    pout = np.where(kinds == int(cb.BoundaryKind.PressureOutlet), 0.25, 0.0)
+    rng = np.random.default_rng(5)
+    p = rng.standard_normal(m.n_cells)
+    hbya = rng.standard_normal((m.n_cells, 3))
+    rau = rng.uniform(0.5, 2.0, m.n_cells)
+    fv = cb.FvGeometry(m, kinds, pout)
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")  # noqa: E731
+    grad = torch.empty((m.n_cells, 3), dtype=torch.float64, device="cuda")
+    u = torch.empty((m.n_cells, 3), dtype=torch.float64, device="cuda")
+    fv.pressure_gradient_device(T(p), grad)
+    fv.correct_velocity_device(T(hbya), T(rau), grad, u)
+    want = O.pressure_gradient(m.n_cells, m.n_internal_faces, m.owner, m.neighbour, m.weights,
+                               m.face_areas, m.face_centres, m.cell_centres, m.cell_volumes, kinds,
+                               pout, p)
+    assert nb > 0 and np.array_equal(grad.cpu().numpy(), want)
+    assert np.array_equal(u.cpu().numpy(), O.correct_velocity(hbya, rau, want))
+    fv.close()

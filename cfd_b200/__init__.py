@@ -139,6 +139,13 @@ _proto("cfdb_fv_create", [_i, _i, _i, _pi, _pi, _pd, _pd, _pd, _pd, _pd, _pi, _p
 _proto("cfdb_fv_destroy", [_vp])
 _proto("cfdb_fv_pressure_gradient_device", [_vp, _vp, _vp])
 _proto("cfdb_fv_correct_velocity_device", [_vp, _vp, _vp, _vp, _vp])
+_proto("cfdb_fv_delta_device", [_vp, _P(_vp)])
+_proto("cfdb_fv_hbya_rau_device", [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp])
+_proto("cfdb_fv_face_flux_device", [_vp, _vp, _vp, _vp, _vp, _vp, _d, _vp, _vp])
+_proto("cfdb_fv_pressure_boundary_device", [_vp, _vp, _vp, _i, _d, _vp, _vp])
+_proto("cfdb_fv_non_orth_device", [_vp, _vp, _vp, _vp, _vp, _vp])
+_proto("cfdb_fv_correct_flux_device", [_vp, _vp, _vp, _vp, _vp, _vp])
+_proto("cfdb_fv_relax_device", [_vp, _vp, _vp, _d, _vp])
 
 
 class TuningStruct(C.Structure):
@@ -1005,7 +1012,7 @@ class FvGeometry:
         pout = _f64(boundary_pressure if boundary_pressure is not None else np.zeros(nb))
         if len(kinds) != nb or len(pout) != nb:
             raise InvalidArgument("one boundary kind and pressure per boundary face")
-        self.n_cells = mesh.n_cells
+        self.n_cells, self.n_faces, self.n_internal_faces = mesh.n_cells, mesh.n_faces, mesh.n_internal_faces
         own, nei = _i32(mesh.owner), _i32(mesh.neighbour)
         sf, cf = _f64(mesh.face_areas).ravel(), _f64(mesh.face_centres).ravel()
         cc, vol, w = _f64(mesh.cell_centres).ravel(), _f64(mesh.cell_volumes), _f64(mesh.weights)
@@ -1022,6 +1029,43 @@ class FvGeometry:
     def correct_velocity_device(self, hbya, rau, grad, u) -> None:
         _check(_lib.cfdb_fv_correct_velocity_device(self._h, _devptr(hbya), _devptr(rau),
                                                     _devptr(grad), _devptr(u)))
+
+    def delta_device(self) -> int:
+        """Device pointer of the delta coefficients of all faces (owned by this object)."""
+        d = _vp()
+        _check(_lib.cfdb_fv_delta_device(self._h, C.byref(d)))
+        return int(d.value)
+
+    def hbya_rau_device(self, mom_diag, mom_upper, mom_lower, mom_source, u, hbya, rau) -> None:
+        _check(_lib.cfdb_fv_hbya_rau_device(self._h, _devptr(mom_diag), _devptr(mom_upper),
+                                            _devptr(mom_lower), _devptr(mom_source), _devptr(u),
+                                            _devptr(hbya), _devptr(rau)))
+
+    def face_flux_device(self, hbya, rau, fixed_velocity, phi_hbya, rau_f, u_prev=None,
+                         phi_prev=None, beta=0.0) -> None:
+        _check(_lib.cfdb_fv_face_flux_device(
+            self._h, _devptr(hbya), _devptr(rau), _devptr(fixed_velocity),
+            _devptr(u_prev) if u_prev is not None else None,
+            _devptr(phi_prev) if phi_prev is not None else None, float(beta), _devptr(phi_hbya),
+            _devptr(rau_f)))
+
+    def pressure_boundary_device(self, phi_hbya, rau_f, diag, source, ref_cell=-1, ref_value=0.0):
+        _check(_lib.cfdb_fv_pressure_boundary_device(self._h, _devptr(phi_hbya), _devptr(rau_f),
+                                                     int(ref_cell), float(ref_value), _devptr(diag),
+                                                     _devptr(source)))
+
+    def non_orth_device(self, grad, rau_f, base_source, non_orth, source) -> None:
+        _check(_lib.cfdb_fv_non_orth_device(self._h, _devptr(grad), _devptr(rau_f),
+                                            _devptr(base_source), _devptr(non_orth), _devptr(source)))
+
+    def correct_flux_device(self, phi_hbya, rau_f, p_new, phi, non_orth=None) -> None:
+        _check(_lib.cfdb_fv_correct_flux_device(
+            self._h, _devptr(phi_hbya), _devptr(rau_f),
+            _devptr(non_orth) if non_orth is not None else None, _devptr(p_new), _devptr(phi)))
+
+    def relax_device(self, p_prev, p_new, alpha, p) -> None:
+        _check(_lib.cfdb_fv_relax_device(self._h, _devptr(p_prev), _devptr(p_new), float(alpha),
+                                         _devptr(p)))
 
     def close(self):
         h = getattr(self, "_h", None)

@@ -245,6 +245,39 @@ int cfdb_fv_pressure_gradient_device(cfdb_fv* fv, const double* p, double* grad)
 /* u = hbya - rau * grad (u, hbya, grad: 3 n_cells; rau: n_cells). Device arrays. */
 int cfdb_fv_correct_velocity_device(cfdb_fv* fv, const double* hbya, const double* rau,
                                     const double* grad, double* u);
+/* The delta coefficients of all faces (device array of n_faces, owned by fv;
+ * fv_geometry.cpp:43-50), e.g. the internal prefix for cfdb_system_assemble_pressure_device. */
+int cfdb_fv_delta_device(const cfdb_fv* fv, const double** delta);
+/* HbyA = (source - offdiag(U)) / diag per component and rAU = V / mean(diag)
+ * (flow_solver.cpp:688-707) from the momentum system: diag, source 3 n_cells, shared
+ * off-diagonal upper / lower (internal faces), velocity u 3 n_cells. */
+int cfdb_fv_hbya_rau_device(cfdb_fv* fv, const double* mom_diag, const double* mom_upper,
+                            const double* mom_lower, const double* mom_source, const double* u,
+                            double* hbya, double* rau);
+/* Predicted face flux phi_hbya and face rAU (n_faces each; flow_solver.cpp:709-733): linear
+ * interpolation on internal faces; on boundary faces rAU_P and, by kind, the fixed velocity
+ * (fixed_velocity: 3 per boundary face; inlets and walls), HbyA_P (outlets) or 0. With u_prev
+ * and phi_prev (else both NULL) the relaxation-independent term beta (phi_prev - u_prev_f . S)
+ * is added (flow_solver.cpp:735-752). */
+int cfdb_fv_face_flux_device(cfdb_fv* fv, const double* hbya, const double* rau,
+                             const double* fixed_velocity, const double* u_prev,
+                             const double* phi_prev, double beta, double* phi_hbya, double* rau_f);
+/* Boundary terms of the pressure equation after the internal assembly (flow_solver.cpp:
+ * 784-796): source -= phi_hbya on every boundary face, outlets add rAU_f delta to diag and
+ * rAU_f delta p_out to source; then set_reference(ref_cell, ref_value) unless ref_cell < 0. */
+int cfdb_fv_pressure_boundary_device(cfdb_fv* fv, const double* phi_hbya, const double* rau_f,
+                                     int ref_cell, double ref_value, double* diag, double* source);
+/* Non-orthogonal corrector (flow_solver.cpp:805-816): non_orth = rAU_f k . (w grad_P +
+ * (1 - w) grad_N) per internal face; source = base_source + sum of +-non_orth per cell. */
+int cfdb_fv_non_orth_device(cfdb_fv* fv, const double* grad, const double* rau_f,
+                            const double* base_source, double* non_orth, double* source);
+/* Conservative flux on every face from the pressure solution (flow_solver.cpp:818-833);
+ * non_orth may be NULL (zero). */
+int cfdb_fv_correct_flux_device(cfdb_fv* fv, const double* phi_hbya, const double* rau_f,
+                                const double* non_orth, const double* p_new, double* phi);
+/* p = p_prev + alpha (p_new - p_prev) (flow_solver.cpp:837-840). */
+int cfdb_fv_relax_device(cfdb_fv* fv, const double* p_prev, const double* p_new, double alpha,
+                         double* p);
 
 /* ---- persistent LDU solve: LduMatrix::solve with "solver": {"device": "gpu"}
  * (ldu_matrix.cpp:111-131 with solve_persistent, ldu_matrix.cpp:287-366) ---- */

@@ -291,6 +291,123 @@ def pressure_gradient(n_cells, n_internal, owner, neighbour, weights, face_areas
     return np.array(grad)
 
 
+def fv_delta_corrections(n_internal, owner, neighbour, face_areas, face_centres, cell_centres):
+    """Delta coefficients of every face and non-orthogonal corrections of the internal faces
+    (fv_geometry.cpp:34-50): delta = |S|^2 / max(S.d, 0.05 |S||d|), k = S - d delta."""
+    nf = len(owner)
+    delta = np.zeros(nf)
+    corr = np.zeros((n_internal, 3))
+    dot = lambda a, b: (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]  # noqa: E731
+    for f in range(nf):
+        s = [float(v) for v in face_areas[f]]
+        cp = [float(v) for v in cell_centres[int(owner[f])]]
+        to = cell_centres[int(neighbour[f])] if f < n_internal else face_centres[f]
+        d = [float(to[i]) - cp[i] for i in range(3)]
+        area = math.sqrt(dot(s, s))
+        sd = max(dot(s, d), 0.05 * area * math.sqrt(dot(d, d)))
+        delta[f] = area * area / sd
+        if f < n_internal:
+            corr[f] = [s[i] - d[i] * delta[f] for i in range(3)]
+    return delta, corr
+
+
+def pressure_step_parts(m, kinds, outlet_pressure, mom_diag, mom_upper, mom_lower, mom_source, u,
+                        fixed_velocity, u_prev=None, phi_prev=None, alpha_u=1.0, ref_cell=-1,
+                        ref_value=0.0):
+    """FlowSolver::pressure_correction up to the solve, face by face in the reference's order
+    (flow_solver.cpp:688-796, GpuCg branch): HbyA, rAU, predicted flux phi_hbya and rau_f on
+    every face (with the relaxation-independent term when u_prev / phi_prev are given and
+    alpha_u < 1), the pressure matrix (internal assembly as krylov_openmp.cpp:289-300, then
+    source = -divergence) with the boundary terms and set_reference. Returns a dict."""
+    n, nf, ni = m.n_cells, m.n_faces, m.n_internal_faces
+    own, nei, w, sf = m.owner, m.neighbour, m.weights, m.face_areas
+    delta, _ = fv_delta_corrections(ni, own, nei, sf, m.face_centres, m.cell_centres)
+    dot = lambda a, b: (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]  # noqa: E731
+    hbya = np.zeros((n, 3))
+    for i in range(3):
+        off = [0.0] * n
+        for f in range(ni):
+            p, q = int(own[f]), int(nei[f])
+            off[p] = off[p] + float(mom_upper[f]) * float(u[q][i])
+            off[q] = off[q] + float(mom_lower[f]) * float(u[p][i])
+        for c in range(n):
+            hbya[c][i] = (float(mom_source[c][i]) - off[c]) / float(mom_diag[c][i])
+    rau = np.array([float(m.cell_volumes[c]) / (((float(mom_diag[c][0]) + float(mom_diag[c][1]))
+                    + float(mom_diag[c][2])) / 3.0) for c in range(n)])
+    phi = np.zeros(nf)
+    rau_f = np.zeros(nf)
+    for f in range(ni):
+        p, q = int(own[f]), int(nei[f])
+        wf = float(w[f])
+        v = [wf * hbya[p][i] + (1.0 - wf) * hbya[q][i] for i in range(3)]
+        phi[f] = dot(v, sf[f])
+        rau_f[f] = wf * rau[p] + (1.0 - wf) * rau[q]
+    for f in range(ni, nf):
+        p, b = int(own[f]), f - ni
+        rau_f[f] = rau[p]
+        k = int(kinds[b])
+        phi[f] = dot(fixed_velocity[b], sf[f]) if k in (0, 1) else (dot(hbya[p], sf[f]) if k == 2 else 0.0)
+    if u_prev is not None and phi_prev is not None and alpha_u < 1.0:
+        beta = 1.0 - alpha_u
+        for f in range(ni):
+            p, q = int(own[f]), int(nei[f])
+            wf = float(w[f])
+            uf = [wf * float(u_prev[p][i]) + (1.0 - wf) * float(u_prev[q][i]) for i in range(3)]
+            phi[f] = phi[f] + beta * (float(phi_prev[f]) - dot(uf, sf[f]))
+        for f in range(ni, nf):
+            if int(kinds[f - ni]) == 2:
+                p = int(own[f])
+                phi[f] = phi[f] + beta * (float(phi_prev[f]) - dot(u_prev[p], sf[f]))
+    up, lo, dg, dv = assemble(n, own[:ni], nei, phi[:ni], rau_f[:ni], delta[:ni], 0.0)
+    source = 0.0 - dv
+    for f in range(ni, nf):
+        p, b = int(own[f]), f - ni
+        source[p] = source[p] - phi[f]
+        if int(kinds[b]) == 2:
+            coeff = rau_f[f] * delta[f]
+            dg[p] = dg[p] + coeff
+            source[p] = source[p] + coeff * float(outlet_pressure[b])
+    if ref_cell >= 0:
+        source[ref_cell] = source[ref_cell] + dg[ref_cell] * ref_value
+        dg[ref_cell] = dg[ref_cell] + dg[ref_cell]
+    return dict(hbya=hbya, rau=rau, phi_hbya=phi, rau_f=rau_f, upper=up, lower=lo, diag=dg,
+                source=source, delta=delta)
+
+
+def non_orth_source(m, grad, rau_f, base_source):
+    """Non-orthogonal corrector terms (flow_solver.cpp:805-816): (non_orth, source)."""
+    ni = m.n_internal_faces
+    _, corr = fv_delta_corrections(ni, m.owner, m.neighbour, m.face_areas, m.face_centres,
+                                   m.cell_centres)
+    non_orth = np.zeros(ni)
+    source = np.array(base_source, np.float64)
+    for f in range(ni):
+        p, q = int(m.owner[f]), int(m.neighbour[f])
+        wf = float(m.weights[f])
+        v = [wf * float(grad[p][i]) + (1.0 - wf) * float(grad[q][i]) for i in range(3)]
+        non_orth[f] = float(rau_f[f]) * ((corr[f][0] * v[0] + corr[f][1] * v[1]) + corr[f][2] * v[2])
+        source[p] = source[p] + non_orth[f]
+        source[q] = source[q] - non_orth[f]
+    return non_orth, source
+
+
+def correct_flux_all(m, kinds, outlet_pressure, phi_hbya, rau_f, delta, non_orth, p_new):
+    """Conservative flux on every face (flow_solver.cpp:818-833)."""
+    ni = m.n_internal_faces
+    phi = np.zeros(m.n_faces)
+    for f in range(m.n_faces):
+        p = int(m.owner[f])
+        coeff = float(rau_f[f]) * float(delta[f])
+        if f < ni:
+            q = int(m.neighbour[f])
+            phi[f] = (float(phi_hbya[f]) - coeff * (float(p_new[q]) - float(p_new[p]))) - float(non_orth[f])
+        else:
+            phi[f] = float(phi_hbya[f])
+            if int(kinds[f - ni]) == 2:
+                phi[f] = phi[f] - coeff * (float(outlet_pressure[f - ni]) - float(p_new[p]))
+    return phi
+
+
 def correct_velocity(hbya, rau, grad):
     """u = HbyA - rAU grad p (flow_solver.cpp:843-846)."""
     return np.asarray(hbya, np.float64) - np.asarray(rau, np.float64)[:, None] * np.asarray(grad, np.float64)

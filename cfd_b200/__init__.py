@@ -119,6 +119,7 @@ _proto("cfdb_system_setup_amg", [_vp, _pd, _pd, _pd, _P(AmgSettingsStruct)])
 _proto("cfdb_system_setup_amg_device", [_vp, _vp, _vp, _vp, _P(AmgSettingsStruct), _i])
 _proto("cfdb_system_setup_profile", [_vp, C.c_char_p, C.c_size_t])
 _proto("cfdb_system_set_keep_levels", [_vp, _i])
+_proto("cfdb_release_cached_memory", [])
 _proto("cfdb_system_time_sweep", [_vp, _i, _i, _pd, _pd])
 _proto("cfdb_system_solve_ldu", [_vp, _vp, _vp, _vp, _vp, _vp, _P(LduSettingsStruct),
                                  _P(AmgSettingsStruct), _i, _P(LduResultStruct)])
@@ -399,6 +400,11 @@ def backend_name() -> str:
 
 def device_available() -> bool:
     return bool(_lib.cfdb_device_available())
+
+
+def release_cached_memory() -> None:
+    """Return device memory cached in the library's pools to the driver (current device)."""
+    _check(_lib.cfdb_release_cached_memory())
 
 
 def device_description() -> str:

@@ -359,6 +359,15 @@ int cfdb_device_description(char* buf, size_t len) {
 
 int cfdb_last_error(char* buf, size_t len) { return copy_str(g_last_error, buf, len); }
 
+int cfdb_release_cached_memory(void) {
+    return guarded([&] {
+        require_device();
+        int dev = 0;
+        CFDB_CUDA(cudaGetDevice(&dev));
+        trim_device_pools(dev);
+    });
+}
+
 void cfdb_default_amg_settings(cfdb_amg_settings* s) {
     if (s == nullptr) return;
     s->strength_threshold = 0.08;

@@ -43,6 +43,12 @@ cudaMemPool_t device_pool(int device, bool transient) {
 
 } // namespace
 
+void trim_device_pools(int device) {
+    for (const bool transient : {false, true}) {
+        check_cuda(cudaMemPoolTrimTo(device_pool(device, transient), 0), "cudaMemPoolTrimTo");
+    }
+}
+
 void DeviceBuffer::allocate(size_t bytes, bool transient) {
     release();
     int dev = 0;

@@ -71,6 +71,9 @@ private:
     int device_ = 0;
 };
 
+// Returns the freed blocks of the library's device pools on `device` to the driver.
+void trim_device_pools(int device);
+
 // Grow-only page-locked host buffer (staging of device-to-host reads).
 class PinnedBuffer {
 public:

@@ -126,6 +126,7 @@ bool make_room(cfdb_server& s, size_t need, int keep_mesh) {
         release(s, *s.resident[victim]);
         s.resident.erase(victim);
         ++s.evictions;
+        cfdb_release_cached_memory(); // the evicted system's blocks go back to the driver
     }
     return true;
 }

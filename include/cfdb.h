@@ -104,6 +104,9 @@ int cfdb_backend_name(char* buf, size_t len);        /* backend_name(): "cuda" *
 int cfdb_device_available(void);                    /* device_available() */
 int cfdb_device_description(char* buf, size_t len); /* device_description() */
 int cfdb_last_error(char* buf, size_t len);          /* message of the last failed call */
+/* Device memory freed by destroyed systems, plans and setups stays cached in the library's
+ * stream-ordered pools for reuse; this returns it to the driver (current device). */
+int cfdb_release_cached_memory(void);
 void cfdb_default_amg_settings(cfdb_amg_settings* s);
 
 /* ---- one-shot calls ---- */

@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="graded", choices=["graded", "tet", "cavity", "batch", "serve"])
+    ap.add_argument("--config", default="graded", choices=["graded", "tet", "cavity", "batch", "serve", "fv"])
     ap.add_argument("--systems", type=int, default=256, help="batch: number of systems")
     ap.add_argument("--tune-cache", default=None, help="batch: autotuner cache file")
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serve: arrival rates (1/s)")
@@ -720,6 +720,194 @@ def run_serve(args, rank, world, local_rank):
         print(json.dumps(line))
 
 
+# ------------------------------------------------------------------------------------------
+# DeviceFv cell kernels (fv_device.hpp): the explicit parts of the momentum predictor
+# ------------------------------------------------------------------------------------------
+
+FV_METRIC = ("DeviceFv cells/s per momentum-predictor pass (LSQ vector gradient, Venkatakrishnan-"
+             "limited linear-upwind momentum corrections with the transpose term, LSQ pressure gradient)")
+
+
+def fv_inputs(size):
+    """The jittered 6-tet box (edge 95: 5.14M cells) with smooth velocity / pressure fields."""
+    import numpy as np
+
+    import cfd_b200 as cb
+    from cfd_b200 import fv_device as D
+    mesh = cb.Mesh.tet(size, size, size, jitter=0.2, seed=7)
+    pv = D.mesh_view_of(mesh)
+    nc, nif, nb = pv.n_cells, pv.n_internal_faces, pv.n_boundary_faces
+    x, xb = pv.cell_centre, pv.face_centre[nif:]
+    vel = lambda q: np.stack([np.sin(3 * q[:, 1]) * np.cos(2 * q[:, 2]), q[:, 0] * q[:, 2],  # noqa: E731
+                              np.cos(q[:, 0] + q[:, 1])], axis=1)
+    u, ub = vel(x), vel(xb)
+    p, pb = np.sin(2 * x[:, 0]) + x[:, 1] ** 2, np.sin(2 * xb[:, 0]) + xb[:, 1] ** 2
+    rng = np.random.default_rng(5)
+    flux = rng.standard_normal(nif) * 1e-3
+    nu = 1e-3 * (1.0 + 0.5 * rng.random(nif))
+    return mesh, pv, dict(u=u, ub=ub, p=p, pb=pb, flux=flux, nu=nu, eps2=np.array([1e-4, 1e-4, 1e-4]))
+
+
+def fv_bytes(kind, pv):
+    """Algorithmic bytes of one launch: every array the kernel needs, read or written once."""
+    nc, nif, nf = pv.n_cells, pv.n_internal_faces, pv.n_faces
+    nb, ns = nf - nif, len(pv.cell_faces)
+    topo = 4 * (nc + 1) + 4 * ns + 4 * nf + 4 * nif  # offsets, cell faces, owner, neighbour
+    return {
+        "vector_gradient_lsq": topo + 24 * nf + 72 * nc + 24 * nc + 24 * nb + 72 * nc,
+        "gradient_lsq": topo + 24 * nf + 72 * nc + 8 * nc + 8 * nb + 24 * nc,
+        "limiter": topo + 24 * nc + 24 * nb + 72 * nc + 24 * nc + 24 * nf + 24 * nc,
+        # internal faces only: flux, w, nu, own, nei (8+8+8+4+4) and cf, kv, sf (3 x 24)
+        "momentum": 4 * (nc + 1) + 4 * ns + 104 * nif + 24 * nc + 72 * nc + 24 * nc + 24 * nc + 48 * nc,
+    }[kind]
+
+
+def run_fv(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    from cfd_b200 import fv_device as D
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    size = args.size or 95
+    mesh, pv, f = fv_inputs(size)
+    nc, nif, nb = pv.n_cells, pv.n_internal_faces, pv.n_boundary_faces
+    fv = D.DeviceFv(pv)
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)  # noqa: E731
+    u, ub, p, pb, flux, nu = T(f["u"]), T(f["ub"]), T(f["p"]), T(f["pb"]), T(f["flux"]), T(f["nu"])
+    g = torch.empty((nc, 9), dtype=torch.float64, device=dev)
+    gp = torch.empty((nc, 3), dtype=torch.float64, device=dev)
+    src = torch.zeros((nc, 3), dtype=torch.float64, device=dev)
+    st = torch.cuda.ExternalStream(fv.stream(), device=dev)
+    eps2 = f["eps2"]
+
+    def step():
+        fv.vector_gradient_device(u, ub, D.GradientScheme.LeastSquares, g)
+        fv.momentum_corrections_device(u, ub, g, flux, nu, True, True, True, eps2, 0.0, True, src)
+        fv.gradient_device(p, pb, D.GradientScheme.LeastSquares, gp)
+
+    def timed(fn, k):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(k):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    ms = timed(step, args.steps)
+    clocks = sampler.stop()
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * nc / (ms_step / 1e3)
+    # per kernel: back-to-back launches (inputs larger than L2)
+    reps = 20
+    peak, peak_kind = hbm_peak()
+    per = {}
+    t_vg = timed(lambda: fv.vector_gradient_device(u, ub, 1, g), reps) / reps
+    t_g = timed(lambda: fv.gradient_device(p, pb, 1, gp), reps) / reps
+    t_m = timed(lambda: fv.momentum_corrections_device(u, ub, g, flux, nu, True, False, False, None, 0.0, True,
+                                                       src), reps) / reps
+    t_ml = timed(lambda: fv.momentum_corrections_device(u, ub, g, flux, nu, True, True, True, eps2, 0.0, True,
+                                                        src), reps) / reps
+    for name, t in (("vector_gradient_lsq", t_vg), ("gradient_lsq", t_g), ("momentum", t_m),
+                    ("limiter", max(t_ml - t_m, 1e-6))):
+        b = fv_bytes(name, pv)
+        per[name] = {"us": t * 1e3, "algorithmic_bytes": b, "gbs": b / 1e9 / (t / 1e3),
+                     "frac": b / 1e9 / (t / 1e3) / peak, "traffic": traffic_for(f"fv_{name}")}
+    top = max(per, key=lambda k: per[k]["us"])
+    roofline = {"bound": "hbm", "kernel": top, "achieved": per[top]["gbs"], "peak": peak, "unit": "GB/s",
+                "frac": per[top]["frac"], "peak_source": peak_kind, "traffic": per[top]["traffic"]}
+    # end to end through the reference's host-array signatures (copies inside the timed region)
+    e2e = None
+    if not args.no_e2e:
+        hu, hub, hp, hpb = f["u"], f["ub"], f["p"], f["pb"]
+        hflux, hnu = f["flux"], f["nu"]
+        hsrc = np.zeros((nc, 3))
+
+        def host_step():
+            fv.vector_gradient(hu, hub, 1)
+            fv.momentum_corrections(hflux, hnu, True, True, True, eps2, 0.0, True, hsrc)
+            return fv.gradient(hp, hpb, 1)
+
+        host_step()
+        t0 = time.perf_counter()
+        k = max(2, args.steps // 2)
+        for _ in range(k):
+            host_step()
+        dt = (time.perf_counter() - t0) / k
+        e2e = {"value": nc / dt, "unit": "cells/s", "ms_per_step": dt * 1e3,
+               "h2d_bytes_per_step": 8 * (3 * nc + 3 * nb + nif + nif + 3 * nc + nc + nb),
+               "d2h_bytes_per_step": 8 * (9 * nc + 3 * nc + 3 * nc)}
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = fv_reference_time(pv, f, reps=1)
+    line = {
+        "metric": FV_METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"tet{size}^3 jittered 6-tet box", "cells": nc, "internal_faces": nif,
+                   "boundary_faces": nb, "step": "vector_gradient(LSQ) + momentum_corrections(limited LU, "
+                   "Venkatakrishnan, transpose) + gradient(LSQ) on device arrays",
+                   "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+        "kernels": per, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
+        "gpu_launches": 4 * args.steps, "device_bytes": fv.device_bytes(),
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    fv.close()
+
+
+def fv_reference_time(pv, f, reps=1):
+    """The reference's DeviceFv host path (fv_openmp.cpp on host threads) on the same step."""
+    import numpy as np
+
+    import oracle.fvcells as F
+    if F._ref_lib() is None:
+        return None
+    v = F.FvView(pv.n_cells, pv.owner, pv.neighbour, pv.cell_offsets, pv.cell_faces, pv.weight, pv.sf,
+                 pv.face_centre, pv.cell_centre, pv.volume, pv.correction, pv.lsq_d, pv.lsq_inverse)
+    ref = F.RefFv(v)
+    s = np.zeros((pv.n_cells, 3))
+    ref.vector_gradient(f["u"], f["ub"], 1)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ref.vector_gradient(f["u"], f["ub"], 1)
+        s = ref.momentum_corrections(f["flux"], f["nu"], True, True, True, f["eps2"], 0.0, True, s)
+        ref.gradient(f["p"], f["pb"], 1)
+    dt = (time.perf_counter() - t0) / reps
+    ref.close()
+    return {"value": pv.n_cells / dt, "unit": "cells/s", "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+            "kind": "reference", "ms_per_step": dt * 1e3,
+            "sample": f"{reps} full pass(es) of the same step on the same mesh"}
+
+
+def run_fv_reference(args):
+    size = args.size or 95
+    mesh, pv, f = fv_inputs(size)
+    cpu = fv_reference_time(pv, f, reps=max(1, min(args.steps, 3)))
+    if cpu is None:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's host path was not built"}))
+        return
+    print(json.dumps({
+        "impl": "reference", "metric": FV_METRIC, "value": cpu["value"], "unit": "cells/s", "n_gpus": 1,
+        "steps": max(1, min(args.steps, 3)), "warmup": 1, "ms_per_step": cpu["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": f"tet{size}^3 jittered 6-tet box", "cells": pv.n_cells},
+        "cpu_baseline": cpu,
+        "e2e": {"value": cpu["value"], "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+
 def main():
     args = parse()
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
@@ -729,6 +917,9 @@ def main():
     size = args.size
     if args.impl == "reference":
         if rank != 0:
+            return
+        if args.config == "fv":
+            run_fv_reference(args)
             return
         if args.config in ("batch", "serve"):
             print(json.dumps({"impl": "reference", "unavailable": "the reference solves one system at a "
@@ -747,6 +938,8 @@ def main():
         run_batch(args, rank, world, local_rank)
     elif args.config == "serve":
         run_serve(args, rank, world, local_rank)
+    elif args.config == "fv":
+        run_fv(args, rank, world, local_rank)
     else:
         run_case(args, rank, world, local_rank, size)
     if world > 1:

@@ -1,0 +1,679 @@
+// cfd::gpu::DeviceFv on the device: cell gradients (Green-Gauss, weighted least squares,
+// skewness-corrected Gauss) and the explicit internal-face corrections of the scalar and
+// momentum equations (linear upwind, LUST blending, Barth-Jespersen / Venkatakrishnan limiter,
+// non-orthogonal correction, transpose viscous term). Interface: fv_device.hpp:33-72 (DeviceFv,
+// FvMeshView); per-cell arithmetic: fv_cell.inc:24-261; call sequence: fv_openmp.cpp:158-305.
+//
+// One thread per cell gathers over the cell's faces in ascending face order (the cell_faces
+// CSR of the mesh view), so every cell sums the same terms in the same order as the
+// reference's per-cell loops; every product and sum is rounded separately (no FMA contraction:
+// this file is compiled with --fmad=false), so the results are bit-identical to the
+// reference's host build. The vector gradient computes the three components in one pass over
+// the mesh (the reference makes three passes); each component's arithmetic is unchanged.
+// Mesh arrays stay resident on the device for the life of the object; vectors are
+// xyz-interleaved, gradients of vectors are 9 values per cell with g[3 i + j] = du_i / dx_j.
+#include "../../include/cfdb.h"
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+
+namespace cfdb {
+void set_thread_error(const std::string& msg);
+} // namespace cfdb
+
+using namespace cfdb;
+
+namespace {
+
+// Device copy of an FvMeshView (fv_device.hpp:15-31).
+struct FvMesh {
+    int nc = 0, nif = 0, nf = 0;
+    const int* own = nullptr;     // n_faces
+    const int* nei = nullptr;     // n_internal_faces
+    const int* start = nullptr;   // n_cells + 1
+    const int* faces = nullptr;   // start[n_cells], ascending per cell
+    const double* w = nullptr;    // n_internal_faces
+    const double* sf = nullptr;   // 3 n_faces
+    const double* cf = nullptr;   // 3 n_faces
+    const double* cc = nullptr;   // 3 n_cells
+    const double* vol = nullptr;  // n_cells
+    const double* kv = nullptr;   // 3 n_faces: non-orthogonal correction vectors
+    const double* lsq_d = nullptr; // 3 n_faces: d / |d|^2
+    const double* lsq = nullptr;  // 9 n_cells: column-major inverse of sum d d^T / |d|^2
+};
+
+} // namespace
+
+struct cfdb_device_fv {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    DeviceArena mem;
+    FvMesh m;
+    // resident fields of the host-array entry points (fv_openmp.cpp:326-337)
+    double* phi = nullptr;   // n_cells
+    double* bv = nullptr;    // boundary faces
+    double* sgrad = nullptr; // 3 n_cells
+    double* vphi = nullptr;  // 3 n_cells
+    double* vbv = nullptr;   // 3 boundary faces
+    double* vgrad = nullptr; // 9 n_cells
+    double* lim = nullptr;   // 3 n_cells
+    double* flux = nullptr;  // internal faces
+    double* coef = nullptr;  // internal faces
+    double* src = nullptr;   // 3 n_cells
+    double* tmp = nullptr;   // 9 n_cells: least-squares gradient of the corrected scheme
+    bool have_vector = false;
+    ~cfdb_device_fv() {
+        if (st != nullptr) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+    }
+};
+
+namespace {
+
+constexpr int kThreads = 256;
+
+int grid(int n) { return std::max(1, (n + kThreads - 1) / kThreads); }
+
+// Gradient of NC components (stride NC per cell / boundary face) of phi: Green-Gauss with
+// linear face interpolation, or weighted least squares (fv_cell.inc:24-74). out: 3 NC per cell.
+template <int NC, bool LSQ>
+__global__ void __launch_bounds__(kThreads) k_cell_gradient(FvMesh m, const double* __restrict__ phi,
+                                                            const double* __restrict__ bv,
+                                                            double* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    double g[NC][3];
+    double pc[NC];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) {
+        g[i][0] = g[i][1] = g[i][2] = 0.0;
+        pc[i] = phi[c * NC + i];
+    }
+    const int k1 = m.start[c + 1];
+    for (int k = m.start[c]; k < k1; ++k) {
+        const int f = m.faces[k];
+        if (LSQ) {
+            const double d0 = m.lsq_d[3 * f], d1 = m.lsq_d[3 * f + 1], d2 = m.lsq_d[3 * f + 2];
+            if (f < m.nif) {
+                const int o = m.own[f], n = m.nei[f];
+#pragma unroll
+                for (int i = 0; i < NC; ++i) {
+                    const double dv = phi[n * NC + i] - phi[o * NC + i];
+                    g[i][0] += d0 * dv;
+                    g[i][1] += d1 * dv;
+                    g[i][2] += d2 * dv;
+                }
+            } else {
+                const double* b = bv + (f - m.nif) * NC;
+#pragma unroll
+                for (int i = 0; i < NC; ++i) {
+                    const double dv = b[i] - pc[i];
+                    g[i][0] += d0 * dv;
+                    g[i][1] += d1 * dv;
+                    g[i][2] += d2 * dv;
+                }
+            }
+        } else if (f < m.nif) {
+            const double wf = m.w[f];
+            const int o = m.own[f], n = m.nei[f];
+            const double s0 = m.sf[3 * f], s1 = m.sf[3 * f + 1], s2 = m.sf[3 * f + 2];
+#pragma unroll
+            for (int i = 0; i < NC; ++i) {
+                const double pf = wf * phi[o * NC + i] + (1.0 - wf) * phi[n * NC + i];
+                if (o == c) {
+                    g[i][0] += s0 * pf;
+                    g[i][1] += s1 * pf;
+                    g[i][2] += s2 * pf;
+                } else {
+                    g[i][0] -= s0 * pf;
+                    g[i][1] -= s1 * pf;
+                    g[i][2] -= s2 * pf;
+                }
+            }
+        } else {
+            const double* b = bv + (f - m.nif) * NC;
+            const double s0 = m.sf[3 * f], s1 = m.sf[3 * f + 1], s2 = m.sf[3 * f + 2];
+#pragma unroll
+            for (int i = 0; i < NC; ++i) {
+                g[i][0] += s0 * b[i];
+                g[i][1] += s1 * b[i];
+                g[i][2] += s2 * b[i];
+            }
+        }
+    }
+    double* o = out + static_cast<size_t>(c) * (3 * NC);
+    if (LSQ) {
+        const double* a = m.lsq + 9 * static_cast<size_t>(c); // column-major
+        const double a0 = a[0], a1 = a[1], a2 = a[2], a3 = a[3], a4 = a[4], a5 = a[5], a6 = a[6],
+                     a7 = a[7], a8 = a[8];
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            o[3 * i] = a0 * g[i][0] + a3 * g[i][1] + a6 * g[i][2];
+            o[3 * i + 1] = a1 * g[i][0] + a4 * g[i][1] + a7 * g[i][2];
+            o[3 * i + 2] = a2 * g[i][0] + a5 * g[i][1] + a8 * g[i][2];
+        }
+    } else {
+        const double v = m.vol[c];
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            o[3 * i] = g[i][0] / v;
+            o[3 * i + 1] = g[i][1] / v;
+            o[3 * i + 2] = g[i][2] / v;
+        }
+    }
+}
+
+// Skewness-corrected Green-Gauss (fv_cell.inc:76-121): face values w phi_P + (1 - w) phi_N +
+// (w g_P + (1 - w) g_N) . (x_f - x_ip) with the least-squares gradient g (3 NC per cell).
+template <int NC>
+__global__ void __launch_bounds__(kThreads) k_cell_gradient_corrected(FvMesh m, const double* __restrict__ phi,
+                                                                      const double* __restrict__ bv,
+                                                                      const double* __restrict__ g,
+                                                                      double* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    double a[NC][3];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) a[i][0] = a[i][1] = a[i][2] = 0.0;
+    const int k1 = m.start[c + 1];
+    for (int k = m.start[c]; k < k1; ++k) {
+        const int f = m.faces[k];
+        const double s0 = m.sf[3 * f], s1 = m.sf[3 * f + 1], s2 = m.sf[3 * f + 2];
+        if (f < m.nif) {
+            const int p = m.own[f], n = m.nei[f];
+            const double wf = m.w[f];
+            double r[3]; // x_f - x_ip, x_ip = w x_P + (1 - w) x_N
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const double xip = wf * m.cc[3 * p + j] + (1.0 - wf) * m.cc[3 * n + j];
+                r[j] = m.cf[3 * f + j] - xip;
+            }
+            const double* gp = g + static_cast<size_t>(p) * (3 * NC);
+            const double* gn = g + static_cast<size_t>(n) * (3 * NC);
+#pragma unroll
+            for (int i = 0; i < NC; ++i) {
+                double pf = wf * phi[p * NC + i] + (1.0 - wf) * phi[n * NC + i];
+                double dot = 0.0;
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const double gf = wf * gp[3 * i + j] + (1.0 - wf) * gn[3 * i + j];
+                    dot = j == 0 ? gf * r[0] : dot + gf * r[j];
+                }
+                pf += dot;
+                if (p == c) {
+                    a[i][0] += s0 * pf;
+                    a[i][1] += s1 * pf;
+                    a[i][2] += s2 * pf;
+                } else {
+                    a[i][0] -= s0 * pf;
+                    a[i][1] -= s1 * pf;
+                    a[i][2] -= s2 * pf;
+                }
+            }
+        } else {
+            const double* b = bv + (f - m.nif) * NC;
+#pragma unroll
+            for (int i = 0; i < NC; ++i) {
+                a[i][0] += s0 * b[i];
+                a[i][1] += s1 * b[i];
+                a[i][2] += s2 * b[i];
+            }
+        }
+    }
+    double* o = out + static_cast<size_t>(c) * (3 * NC);
+    const double v = m.vol[c];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) {
+        o[3 * i] = a[i][0] / v;
+        o[3 * i + 1] = a[i][1] / v;
+        o[3 * i + 2] = a[i][2] / v;
+    }
+}
+
+// Barth-Jespersen / Venkatakrishnan limiter per component of the vector field u with boundary
+// values ub and gradient g (9 per cell) (fv_cell.inc:123-163).
+__global__ void __launch_bounds__(kThreads) k_cell_limiter(FvMesh m, const double* __restrict__ u,
+                                                           const double* __restrict__ ub,
+                                                           const double* __restrict__ g, int venkat,
+                                                           double e0, double e1, double e2,
+                                                           double* __restrict__ lim) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    const double eps2[3] = {e0, e1, e2};
+    double uc[3], lo[3], hi[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) uc[i] = lo[i] = hi[i] = u[3 * c + i];
+    const int k0 = m.start[c], k1 = m.start[c + 1];
+    for (int k = k0; k < k1; ++k) {
+        const int f = m.faces[k];
+        const double* v = f < m.nif ? u + 3 * (m.own[f] == c ? m.nei[f] : m.own[f]) : ub + 3 * (f - m.nif);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double vi = v[i];
+            lo[i] = vi < lo[i] ? vi : lo[i];
+            hi[i] = vi > hi[i] ? vi : hi[i];
+        }
+    }
+    double l[3] = {1.0, 1.0, 1.0};
+    const double* gc = g + 9 * static_cast<size_t>(c);
+    double gv[9];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) gv[j] = gc[j];
+    const double x0 = m.cc[3 * c], x1 = m.cc[3 * c + 1], x2 = m.cc[3 * c + 2];
+    for (int k = k0; k < k1; ++k) {
+        const int f = m.faces[k];
+        const double r0 = m.cf[3 * f] - x0;
+        const double r1 = m.cf[3 * f + 1] - x1;
+        const double r2 = m.cf[3 * f + 2] - x2;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double d = gv[3 * i] * r0 + gv[3 * i + 1] * r1 + gv[3 * i + 2] * r2;
+            if (d < 1e-300 && d > -1e-300) continue;
+            const double bound = d > 0.0 ? hi[i] - uc[i] : lo[i] - uc[i];
+            double q;
+            if (venkat) {
+                q = (bound * bound + eps2[i] + 2.0 * d * bound) / (bound * bound + 2.0 * d * d + d * bound + eps2[i]);
+            } else {
+                const double ratio = bound / d;
+                q = ratio > 0.0 ? ratio : 0.0;
+            }
+            l[i] = q < l[i] ? q : l[i];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) lim[3 * c + i] = l[i];
+}
+
+// Explicit internal-face fluxes of a scalar equation with the cell gradient g (3 per cell),
+// accumulated into source (fv_cell.inc:165-196).
+__global__ void __launch_bounds__(kThreads) k_scalar_corrections(FvMesh m, const double* __restrict__ g,
+                                                                 const double* __restrict__ flux,
+                                                                 const double* __restrict__ gamma,
+                                                                 int linear_upwind, double* __restrict__ source) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    double s = 0.0;
+    const int k1 = m.start[c + 1];
+    for (int k = m.start[c]; k < k1; ++k) {
+        const int f = m.faces[k];
+        if (f >= m.nif) break; // boundary faces follow the internal ones
+        const int p = m.own[f], n = m.nei[f];
+        const double fl = flux[f];
+        double e = 0.0;
+        if (linear_upwind) {
+            const int up = fl >= 0.0 ? p : n;
+            const double r0 = m.cf[3 * f] - m.cc[3 * up];
+            const double r1 = m.cf[3 * f + 1] - m.cc[3 * up + 1];
+            const double r2 = m.cf[3 * f + 2] - m.cc[3 * up + 2];
+            e -= fl * (g[3 * up] * r0 + g[3 * up + 1] * r1 + g[3 * up + 2] * r2);
+        }
+        const double wf = m.w[f];
+        const double gf0 = wf * g[3 * p] + (1.0 - wf) * g[3 * n];
+        const double gf1 = wf * g[3 * p + 1] + (1.0 - wf) * g[3 * n + 1];
+        const double gf2 = wf * g[3 * p + 2] + (1.0 - wf) * g[3 * n + 2];
+        e += gamma[f] * (m.kv[3 * f] * gf0 + m.kv[3 * f + 1] * gf1 + m.kv[3 * f + 2] * gf2);
+        s = p == c ? s + e : s - e;
+    }
+    source[c] += s;
+}
+
+// Explicit internal-face fluxes of the momentum equation (fv_cell.inc:198-259).
+__global__ void __launch_bounds__(kThreads) k_momentum_corrections(
+    FvMesh m, const double* __restrict__ g, const double* __restrict__ lim, int limited,
+    const double* __restrict__ flux, const double* __restrict__ nu_face, int linear_upwind, double central,
+    const double* __restrict__ u, int transpose_term, double* __restrict__ source) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    double s[3] = {0.0, 0.0, 0.0};
+    const int k1 = m.start[c + 1];
+    for (int k = m.start[c]; k < k1; ++k) {
+        const int f = m.faces[k];
+        if (f >= m.nif) break;
+        const int p = m.own[f], n = m.nei[f];
+        const double fl = flux[f];
+        const double wf = m.w[f];
+        double e[3] = {0.0, 0.0, 0.0};
+        if (linear_upwind) {
+            const int up = fl >= 0.0 ? p : n;
+            const double r0 = m.cf[3 * f] - m.cc[3 * up];
+            const double r1 = m.cf[3 * f + 1] - m.cc[3 * up + 1];
+            const double r2 = m.cf[3 * f + 2] - m.cc[3 * up + 2];
+            const double* gu = g + 9 * static_cast<size_t>(up);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                double d = gu[3 * i] * r0 + gu[3 * i + 1] * r1 + gu[3 * i + 2] * r2;
+                if (central > 0.0) {
+                    const double uf = wf * u[3 * p + i] + (1.0 - wf) * u[3 * n + i];
+                    d = (1.0 - central) * d + central * (uf - u[3 * up + i]);
+                }
+                if (limited) d = lim[3 * up + i] * d;
+                e[i] -= fl * d;
+            }
+        }
+        const double* gp = g + 9 * static_cast<size_t>(p);
+        const double* gn = g + 9 * static_cast<size_t>(n);
+        double gf[9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) gf[j] = wf * gp[j] + (1.0 - wf) * gn[j];
+        const double nu = nu_face[f];
+        const double k0 = m.kv[3 * f], kk1 = m.kv[3 * f + 1], k2 = m.kv[3 * f + 2];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) e[i] += nu * (gf[3 * i] * k0 + gf[3 * i + 1] * kk1 + gf[3 * i + 2] * k2);
+        if (transpose_term) {
+            const double a0 = m.sf[3 * f], a1 = m.sf[3 * f + 1], a2 = m.sf[3 * f + 2];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) e[i] += nu * (gf[i] * a0 + gf[i + 3] * a1 + gf[i + 6] * a2);
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) s[i] = p == c ? s[i] + e[i] : s[i] - e[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) source[3 * c + i] += s[i];
+}
+
+template <class F> int guarded(F&& f) {
+    try {
+        f();
+        return CFDB_OK;
+    } catch (const Error& e) {
+        set_thread_error(e.what());
+        return e.code;
+    } catch (const std::exception& e) {
+        set_thread_error(e.what());
+        return CFDB_ERR_INTERNAL;
+    }
+}
+
+void check_scheme(int scheme) {
+    if (scheme < CFDB_GRAD_GAUSS || scheme > CFDB_GRAD_GAUSS_CORRECTED)
+        fail(CFDB_ERR_BAD_ARG, "DeviceFv: unknown gradient scheme " + std::to_string(scheme));
+}
+
+// gradient_loop of fv_openmp.cpp:250-297 with all NC components in one pass
+template <int NC>
+void launch_gradient(cfdb_device_fv* fv, const double* phi, const double* bv, int scheme, double* out) {
+    const FvMesh& m = fv->m;
+    if (scheme == CFDB_GRAD_GAUSS_CORRECTED) {
+        k_cell_gradient<NC, true><<<grid(m.nc), kThreads, 0, fv->st>>>(m, phi, bv, fv->tmp);
+        k_cell_gradient_corrected<NC><<<grid(m.nc), kThreads, 0, fv->st>>>(m, phi, bv, fv->tmp, out);
+    } else if (scheme == CFDB_GRAD_LEAST_SQUARES) {
+        k_cell_gradient<NC, true><<<grid(m.nc), kThreads, 0, fv->st>>>(m, phi, bv, out);
+    } else {
+        k_cell_gradient<NC, false><<<grid(m.nc), kThreads, 0, fv->st>>>(m, phi, bv, out);
+    }
+    CFDB_CUDA(cudaGetLastError());
+}
+
+void launch_scalar_corrections(cfdb_device_fv* fv, const double* phi, const double* bv, int scheme,
+                               const double* flux, const double* gamma, int linear_upwind, double* source) {
+    launch_gradient<1>(fv, phi, bv, scheme, fv->sgrad);
+    k_scalar_corrections<<<grid(fv->m.nc), kThreads, 0, fv->st>>>(fv->m, fv->sgrad, flux, gamma,
+                                                                   linear_upwind != 0 ? 1 : 0, source);
+    CFDB_CUDA(cudaGetLastError());
+}
+
+void launch_momentum_corrections(cfdb_device_fv* fv, const double* u, const double* ub, const double* g,
+                                 const double* flux, const double* nu_face, int linear_upwind, int limited,
+                                 int venkat, const double* eps2, double central, int transpose_term,
+                                 double* source) {
+    // the limiter is used only with linear upwind (fv_openmp.cpp:216)
+    const int use_lim = limited != 0 && linear_upwind != 0 ? 1 : 0;
+    const double e0 = venkat ? eps2[0] : 0.0, e1 = venkat ? eps2[1] : 0.0, e2 = venkat ? eps2[2] : 0.0;
+    if (use_lim) {
+        k_cell_limiter<<<grid(fv->m.nc), kThreads, 0, fv->st>>>(fv->m, u, ub, g, venkat != 0 ? 1 : 0, e0, e1, e2,
+                                                               fv->lim);
+    }
+    k_momentum_corrections<<<grid(fv->m.nc), kThreads, 0, fv->st>>>(
+        fv->m, g, fv->lim, use_lim, flux, nu_face, linear_upwind != 0 ? 1 : 0, central, u,
+        transpose_term != 0 ? 1 : 0, source);
+    CFDB_CUDA(cudaGetLastError());
+}
+
+void h2d(cfdb_device_fv* fv, double* dst, const double* src, size_t n) {
+    if (n > 0) CFDB_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, fv->st));
+}
+
+void d2h(cfdb_device_fv* fv, double* dst, const double* src, size_t n) {
+    if (n > 0) CFDB_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, fv->st));
+}
+
+size_t ncells(const cfdb_device_fv* fv) { return static_cast<size_t>(fv->m.nc); }
+size_t nbound(const cfdb_device_fv* fv) { return static_cast<size_t>(fv->m.nf - fv->m.nif); }
+size_t ninternal(const cfdb_device_fv* fv) { return static_cast<size_t>(fv->m.nif); }
+
+void need(bool ok, const char* what) {
+    if (!ok) fail(CFDB_ERR_BAD_ARG, std::string("DeviceFv: missing argument ") + what);
+}
+
+} // namespace
+
+extern "C" {
+
+int cfdb_device_fv_create(const cfdb_fv_mesh_view* v, cfdb_device_fv** out) {
+    return guarded([&] {
+        if (v == nullptr || out == nullptr) fail(CFDB_ERR_BAD_ARG, "DeviceFv: null argument");
+        *out = nullptr;
+        const int nc = v->n_cells, nif = v->n_internal_faces, nf = v->n_faces;
+        // FvHostMesh (fv_device.cpp:22-50): sizes, then every array present
+        if (nc <= 0 || nif < 0 || nf < nif || v->cell_offsets == nullptr)
+            fail(CFDB_ERR_BAD_ARG, "DeviceFv: invalid mesh sizes");
+        const size_t c = static_cast<size_t>(nc), f = static_cast<size_t>(nf), fi = static_cast<size_t>(nif);
+        const int n_slots = v->cell_offsets[nc];
+        auto missing = [&](const void* p, size_t n, const char* what) {
+            if (n > 0 && p == nullptr) fail(CFDB_ERR_BAD_ARG, std::string("DeviceFv: missing mesh array ") + what);
+        };
+        missing(v->owner, f, "owner");
+        missing(v->neighbour, fi, "neighbour");
+        missing(v->cell_faces, n_slots > 0 ? static_cast<size_t>(n_slots) : 0, "cell_faces");
+        missing(v->weight, fi, "weight");
+        missing(v->sf, f, "sf");
+        missing(v->face_centre, f, "face_centre");
+        missing(v->cell_centre, c, "cell_centre");
+        missing(v->volume, c, "volume");
+        missing(v->correction, f, "correction");
+        missing(v->lsq_d, f, "lsq_d");
+        missing(v->lsq_inverse, c, "lsq_inverse");
+        // every index the kernels follow stays inside its array
+        if (v->cell_offsets[0] != 0) fail(CFDB_ERR_BAD_ARG, "DeviceFv: cell_offsets[0] != 0");
+        for (int i = 0; i < nc; ++i)
+            if (v->cell_offsets[i + 1] < v->cell_offsets[i])
+                fail(CFDB_ERR_BAD_ARG, "DeviceFv: cell_offsets decrease at cell " + std::to_string(i));
+        for (int k = 0; k < n_slots; ++k)
+            if (v->cell_faces[k] < 0 || v->cell_faces[k] >= nf)
+                fail(CFDB_ERR_BAD_ARG, "DeviceFv: cell_faces[" + std::to_string(k) + "] out of range");
+        for (int i = 0; i < nf; ++i)
+            if (v->owner[i] < 0 || v->owner[i] >= nc || (i < nif && (v->neighbour[i] < 0 || v->neighbour[i] >= nc)))
+                fail(CFDB_ERR_BAD_ARG, "DeviceFv: face " + std::to_string(i) + " addresses a cell out of range");
+        auto* fv = new cfdb_device_fv;
+        try {
+            CFDB_CUDA(cudaGetDevice(&fv->device));
+            CFDB_CUDA(cudaStreamCreateWithFlags(&fv->st, cudaStreamNonBlocking));
+            auto up = [&](const auto* p, size_t n) {
+                using T = std::remove_const_t<std::remove_pointer_t<decltype(p)>>;
+                std::vector<T> h(p, p + n);
+                return static_cast<const T*>(fv->mem.upload(h, fv->st));
+            };
+            FvMesh& m = fv->m;
+            m.nc = nc;
+            m.nif = nif;
+            m.nf = nf;
+            m.own = up(v->owner, f);
+            m.nei = up(v->neighbour, fi);
+            m.start = up(v->cell_offsets, c + 1);
+            m.faces = up(v->cell_faces, static_cast<size_t>(n_slots));
+            m.w = up(v->weight, fi);
+            m.sf = up(v->sf, 3 * f);
+            m.cf = up(v->face_centre, 3 * f);
+            m.cc = up(v->cell_centre, 3 * c);
+            m.vol = up(v->volume, c);
+            m.kv = up(v->correction, 3 * f);
+            m.lsq_d = up(v->lsq_d, 3 * f);
+            m.lsq = up(v->lsq_inverse, 9 * c);
+            const size_t nb = f - fi;
+            fv->phi = fv->mem.alloc<double>(c);
+            fv->bv = fv->mem.alloc<double>(nb);
+            fv->sgrad = fv->mem.alloc<double>(3 * c);
+            fv->vphi = fv->mem.alloc<double>(3 * c);
+            fv->vbv = fv->mem.alloc<double>(3 * nb);
+            fv->vgrad = fv->mem.alloc<double>(9 * c);
+            fv->lim = fv->mem.alloc<double>(3 * c);
+            fv->flux = fv->mem.alloc<double>(fi);
+            fv->coef = fv->mem.alloc<double>(fi);
+            fv->src = fv->mem.alloc<double>(3 * c);
+            fv->tmp = fv->mem.alloc<double>(9 * c);
+            CFDB_CUDA(cudaStreamSynchronize(fv->st));
+        } catch (...) {
+            delete fv;
+            throw;
+        }
+        *out = fv;
+    });
+}
+
+int cfdb_device_fv_destroy(cfdb_device_fv* fv) {
+    if (fv != nullptr) {
+        cudaSetDevice(fv->device);
+        delete fv;
+    }
+    return CFDB_OK;
+}
+
+int cfdb_device_fv_on_device(const cfdb_device_fv* fv) { return fv != nullptr ? 1 : 0; }
+
+int cfdb_device_fv_device_bytes(const cfdb_device_fv* fv, size_t* bytes) {
+    if (fv == nullptr || bytes == nullptr) return CFDB_ERR_BAD_ARG;
+    *bytes = fv->mem.bytes();
+    return CFDB_OK;
+}
+
+int cfdb_device_fv_stream(const cfdb_device_fv* fv, void** stream) {
+    if (fv == nullptr || stream == nullptr) return CFDB_ERR_BAD_ARG;
+    *stream = fv->st;
+    return CFDB_OK;
+}
+
+int cfdb_device_fv_gradient(cfdb_device_fv* fv, const double* phi, const double* bv, int scheme, double* grad) {
+    return guarded([&] {
+        need(fv != nullptr && phi != nullptr && grad != nullptr && (nbound(fv) == 0 || bv != nullptr), "");
+        check_scheme(scheme);
+        CFDB_CUDA(cudaSetDevice(fv->device));
+        h2d(fv, fv->phi, phi, ncells(fv));
+        h2d(fv, fv->bv, bv, nbound(fv));
+        launch_gradient<1>(fv, fv->phi, fv->bv, scheme, fv->sgrad);
+        d2h(fv, grad, fv->sgrad, 3 * ncells(fv));
+        CFDB_CUDA(cudaStreamSynchronize(fv->st));
+    });
+}
+
+int cfdb_device_fv_vector_gradient(cfdb_device_fv* fv, const double* u, const double* ub, int scheme, double* grad) {
+    return guarded([&] {
+        need(fv != nullptr && u != nullptr && grad != nullptr && (nbound(fv) == 0 || ub != nullptr), "");
+        check_scheme(scheme);
+        CFDB_CUDA(cudaSetDevice(fv->device));
+        fv->have_vector = false;
+        h2d(fv, fv->vphi, u, 3 * ncells(fv));
+        h2d(fv, fv->vbv, ub, 3 * nbound(fv));
+        launch_gradient<3>(fv, fv->vphi, fv->vbv, scheme, fv->vgrad);
+        d2h(fv, grad, fv->vgrad, 9 * ncells(fv));
+        CFDB_CUDA(cudaStreamSynchronize(fv->st));
+        fv->have_vector = true;
+    });
+}
+
+int cfdb_device_fv_scalar_corrections(cfdb_device_fv* fv, const double* phi, const double* bv, int scheme,
+                                      const double* flux, const double* gamma, int linear_upwind, double* source) {
+    return guarded([&] {
+        need(fv != nullptr && phi != nullptr && source != nullptr && (nbound(fv) == 0 || bv != nullptr) &&
+                 (ninternal(fv) == 0 || (flux != nullptr && gamma != nullptr)),
+             "");
+        check_scheme(scheme);
+        CFDB_CUDA(cudaSetDevice(fv->device));
+        h2d(fv, fv->phi, phi, ncells(fv));
+        h2d(fv, fv->bv, bv, nbound(fv));
+        h2d(fv, fv->flux, flux, ninternal(fv));
+        h2d(fv, fv->coef, gamma, ninternal(fv));
+        h2d(fv, fv->src, source, ncells(fv));
+        launch_scalar_corrections(fv, fv->phi, fv->bv, scheme, fv->flux, fv->coef, linear_upwind, fv->src);
+        d2h(fv, source, fv->src, ncells(fv));
+        CFDB_CUDA(cudaStreamSynchronize(fv->st));
+    });
+}
+
+int cfdb_device_fv_momentum_corrections(cfdb_device_fv* fv, const double* flux, const double* nu_face,
+                                        int linear_upwind, int limited, int venkat, const double* eps2,
+                                        double central, int transpose_term, double* source) {
+    return guarded([&] {
+        need(fv != nullptr && source != nullptr && (ninternal(fv) == 0 || (flux != nullptr && nu_face != nullptr)) &&
+                 (!venkat || eps2 != nullptr),
+             "");
+        // fv_openmp.cpp:205-207
+        if (!fv->have_vector) fail(CFDB_ERR_NOT_READY, "DeviceFv::momentum_corrections before vector_gradient");
+        CFDB_CUDA(cudaSetDevice(fv->device));
+        h2d(fv, fv->flux, flux, ninternal(fv));
+        h2d(fv, fv->coef, nu_face, ninternal(fv));
+        h2d(fv, fv->src, source, 3 * ncells(fv));
+        launch_momentum_corrections(fv, fv->vphi, fv->vbv, fv->vgrad, fv->flux, fv->coef, linear_upwind, limited,
+                                    venkat, eps2, central, transpose_term, fv->src);
+        d2h(fv, source, fv->src, 3 * ncells(fv));
+        CFDB_CUDA(cudaStreamSynchronize(fv->st));
+    });
+}
+
+int cfdb_device_fv_gradient_device(cfdb_device_fv* fv, const double* phi, const double* bv, int scheme,
+                                   double* grad) {
+    return guarded([&] {
+        need(fv != nullptr && phi != nullptr && grad != nullptr && (nbound(fv) == 0 || bv != nullptr), "");
+        check_scheme(scheme);
+        CFDB_CUDA(cudaSetDevice(fv->device));
+        launch_gradient<1>(fv, phi, bv, scheme, grad);
+        CFDB_CUDA(cudaStreamSynchronize(fv->st));
+    });
+}
+
+int cfdb_device_fv_vector_gradient_device(cfdb_device_fv* fv, const double* u, const double* ub, int scheme,
+                                          double* grad) {
+    return guarded([&] {
+        need(fv != nullptr && u != nullptr && grad != nullptr && (nbound(fv) == 0 || ub != nullptr), "");
+        check_scheme(scheme);
+        CFDB_CUDA(cudaSetDevice(fv->device));
+        launch_gradient<3>(fv, u, ub, scheme, grad);
+        CFDB_CUDA(cudaStreamSynchronize(fv->st));
+    });
+}
+
+int cfdb_device_fv_scalar_corrections_device(cfdb_device_fv* fv, const double* phi, const double* bv, int scheme,
+                                             const double* flux, const double* gamma, int linear_upwind,
+                                             double* source) {
+    return guarded([&] {
+        need(fv != nullptr && phi != nullptr && source != nullptr && (nbound(fv) == 0 || bv != nullptr) &&
+                 (ninternal(fv) == 0 || (flux != nullptr && gamma != nullptr)),
+             "");
+        check_scheme(scheme);
+        CFDB_CUDA(cudaSetDevice(fv->device));
+        launch_scalar_corrections(fv, phi, bv, scheme, flux, gamma, linear_upwind, source);
+        CFDB_CUDA(cudaStreamSynchronize(fv->st));
+    });
+}
+
+int cfdb_device_fv_momentum_corrections_device(cfdb_device_fv* fv, const double* u, const double* ub,
+                                               const double* grad, const double* flux, const double* nu_face,
+                                               int linear_upwind, int limited, int venkat, const double* eps2,
+                                               double central, int transpose_term, double* source) {
+    return guarded([&] {
+        need(fv != nullptr && u != nullptr && grad != nullptr && source != nullptr &&
+                 (nbound(fv) == 0 || ub != nullptr) &&
+                 (ninternal(fv) == 0 || (flux != nullptr && nu_face != nullptr)) && (!venkat || eps2 != nullptr),
+             "");
+        CFDB_CUDA(cudaSetDevice(fv->device));
+        launch_momentum_corrections(fv, u, ub, grad, flux, nu_face, linear_upwind, limited, venkat, eps2, central,
+                                    transpose_term, source);
+        CFDB_CUDA(cudaStreamSynchronize(fv->st));
+    });
+}
+
+} // extern "C"

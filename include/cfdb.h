@@ -424,6 +424,73 @@ int cfdb_batch_stream(const cfdb_batch* b, void** stream);
 int cfdb_batch_device_bytes(const cfdb_batch* b, size_t* bytes);
 int cfdb_batch_kernel_launches(const cfdb_batch* b, unsigned long long* count);
 
+/* ---- finite-volume cell kernels: cfd::gpu::DeviceFv (fv_device.hpp:33-72) ---- */
+typedef enum { /* fv_geometry.hpp:31 GradientScheme */
+    CFDB_GRAD_GAUSS = 0,
+    CFDB_GRAD_LEAST_SQUARES = 1,
+    CFDB_GRAD_GAUSS_CORRECTED = 2
+} cfdb_gradient_scheme;
+/* FvMeshView (fv_device.hpp:15-31): host arrays, copied to the device by cfdb_device_fv_create.
+ * Faces [0, n_internal_faces) are internal; vectors are 3 doubles per entry (xyz). */
+typedef struct {
+    int n_cells;
+    int n_internal_faces;
+    int n_faces;
+    const int* owner;          /* n_faces */
+    const int* neighbour;      /* n_internal_faces */
+    const int* cell_offsets;   /* n_cells + 1: faces of each cell (CSR) ... */
+    const int* cell_faces;     /* ... in ascending face order */
+    const double* weight;      /* n_internal_faces: phi_f = w phi_P + (1 - w) phi_N */
+    const double* sf;          /* 3 n_faces: face area vectors */
+    const double* face_centre; /* 3 n_faces */
+    const double* cell_centre; /* 3 n_cells */
+    const double* volume;      /* n_cells */
+    const double* correction;  /* 3 n_faces: non-orthogonal correction vectors */
+    const double* lsq_d;       /* 3 n_faces: d / |d|^2 (d = C_N - C_P or C_f - C_P) */
+    const double* lsq_inverse; /* 9 n_cells: (sum d d^T / |d|^2)^-1, column-major */
+} cfdb_fv_mesh_view;
+typedef struct cfdb_device_fv cfdb_device_fv;
+/* DeviceFv::DeviceFv: checks the sizes and that every array is present (fv_device.cpp:22-50)
+ * and that every index stays in range, then keeps the mesh resident on the current device. */
+int cfdb_device_fv_create(const cfdb_fv_mesh_view* view, cfdb_device_fv** out);
+int cfdb_device_fv_destroy(cfdb_device_fv* fv);
+int cfdb_device_fv_on_device(const cfdb_device_fv* fv); /* 1: there is no host path */
+int cfdb_device_fv_device_bytes(const cfdb_device_fv* fv, size_t* bytes);
+int cfdb_device_fv_stream(const cfdb_device_fv* fv, void** stream);
+/* The four DeviceFv calls on HOST arrays, with the reference's semantics: grad (3 n_cells) of
+ * phi (n_cells) with boundary face values bv (n_boundary); the vector gradient (9 n_cells,
+ * grad[9 c + 3 i + j] = du_i / dx_j) of u (3 n_cells) with ub (3 n_boundary), kept on the
+ * device for momentum_corrections; scalar and momentum explicit face corrections accumulated
+ * into source (n_cells / 3 n_cells). momentum_corrections before a vector_gradient fails with
+ * CFDB_ERR_NOT_READY; eps2 (3 values) is read only when venkat != 0. */
+int cfdb_device_fv_gradient(cfdb_device_fv* fv, const double* phi, const double* bv, int scheme,
+                            double* grad);
+int cfdb_device_fv_vector_gradient(cfdb_device_fv* fv, const double* u, const double* ub,
+                                   int scheme, double* grad);
+int cfdb_device_fv_scalar_corrections(cfdb_device_fv* fv, const double* phi, const double* bv,
+                                      int scheme, const double* flux, const double* gamma,
+                                      int linear_upwind, double* source);
+int cfdb_device_fv_momentum_corrections(cfdb_device_fv* fv, const double* flux,
+                                        const double* nu_face, int linear_upwind, int limited,
+                                        int venkat, const double* eps2, double central,
+                                        int transpose_term, double* source);
+/* The same on DEVICE arrays (no copies); momentum corrections take the field, its boundary
+ * values and its vector gradient explicitly. Each returns when its kernels are done. */
+int cfdb_device_fv_gradient_device(cfdb_device_fv* fv, const double* phi, const double* bv,
+                                   int scheme, double* grad);
+int cfdb_device_fv_vector_gradient_device(cfdb_device_fv* fv, const double* u, const double* ub,
+                                          int scheme, double* grad);
+int cfdb_device_fv_scalar_corrections_device(cfdb_device_fv* fv, const double* phi,
+                                             const double* bv, int scheme, const double* flux,
+                                             const double* gamma, int linear_upwind,
+                                             double* source);
+int cfdb_device_fv_momentum_corrections_device(cfdb_device_fv* fv, const double* u,
+                                               const double* ub, const double* grad,
+                                               const double* flux, const double* nu_face,
+                                               int linear_upwind, int limited, int venkat,
+                                               const double* eps2, double central,
+                                               int transpose_term, double* source);
+
 #ifdef __cplusplus
 }
 #endif

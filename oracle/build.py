@@ -27,6 +27,8 @@ REF_SOURCES = [
     "src/gpu/src/krylov_openmp.cpp",
     "src/gpu/src/device_solver.cpp",
     "src/gpu/src/dispatch.cpp",
+    "src/gpu/src/fv_openmp.cpp",
+    "src/gpu/src/fv_device.cpp",
 ]
 
 
@@ -61,7 +63,10 @@ def build_ref(force: bool = False) -> str | None:
     srcs = [os.path.join(REFERENCE_ROOT, s) for s in REF_SOURCES]
     shim = os.path.join(HERE, "ref_shim.cpp")
     deps = srcs + [shim, os.path.join(REFERENCE_ROOT, "src/gpu/src/krylov_kernels.inc"),
-                   os.path.join(REFERENCE_ROOT, "src/gpu/include/cfd/gpu/krylov.hpp")]
+                   os.path.join(REFERENCE_ROOT, "src/gpu/include/cfd/gpu/krylov.hpp"),
+                   os.path.join(REFERENCE_ROOT, "src/gpu/src/fv_cell.inc"),
+                   os.path.join(REFERENCE_ROOT, "src/gpu/src/fv_impl.hpp"),
+                   os.path.join(REFERENCE_ROOT, "src/gpu/include/cfd/gpu/fv_device.hpp")]
     if force or _stale(REF_SO, deps):
         if shutil.which("g++") is None:
             return None

@@ -1,10 +1,12 @@
 // C-ABI shim over the reference's own host implementation of the accelerator path
 // (TEST INFRASTRUCTURE ONLY). It is compiled together with the reference's unchanged sources
 // src/gpu/src/{krylov_openmp.cpp, device_solver.cpp, dispatch.cpp} (which include
-// krylov_kernels.inc) into oracle/_ref/libcfdref.so by oracle/build.py. Without CFD_GPU_CUDA
+// krylov_kernels.inc) and src/gpu/src/{fv_openmp.cpp, fv_device.cpp} (which include
+// fv_cell.inc) into oracle/_ref/libcfdref.so by oracle/build.py. Without CFD_GPU_CUDA
 // those sources run the accelerator algorithm on host threads, exactly as the reference's CI
 // does (.github/workflows/ci.yml:157-169). Used to pin the C oracle and as the timed
 // reference CPU baseline.
+#include <cfd/gpu/fv_device.hpp>
 #include <cfd/gpu/krylov.hpp>
 
 #include <exception>
@@ -184,6 +186,84 @@ void ref_ds_destroy(void* h) {
 
 int ref_backend_is_host() {
     return cfd::gpu::backend_name() == "host" ? 1 : 0;
+}
+
+// cfd::gpu::DeviceFv (fv_device.hpp:33-72) over an FvMeshView of host arrays. Without an
+// accelerator the reference runs the per-cell kernels of fv_cell.inc on host threads.
+void* ref_fv_create(int n_cells, int n_internal_faces, int n_faces, const int* owner,
+                    const int* neighbour, const int* cell_offsets, const int* cell_faces,
+                    const double* weight, const double* sf, const double* face_centre,
+                    const double* cell_centre, const double* volume, const double* correction,
+                    const double* lsq_d, const double* lsq_inverse) {
+    try {
+        cfd::gpu::FvMeshView v;
+        v.n_cells = n_cells;
+        v.n_internal_faces = n_internal_faces;
+        v.n_faces = n_faces;
+        v.owner = owner;
+        v.neighbour = neighbour;
+        v.cell_offsets = cell_offsets;
+        v.cell_faces = cell_faces;
+        v.weight = weight;
+        v.sf = sf;
+        v.face_centre = face_centre;
+        v.cell_centre = cell_centre;
+        v.volume = volume;
+        v.correction = correction;
+        v.lsq_d = lsq_d;
+        v.lsq_inverse = lsq_inverse;
+        return new cfd::gpu::DeviceFv(v);
+    } catch (const std::exception&) {
+        return nullptr;
+    }
+}
+
+void ref_fv_destroy(void* h) {
+    delete static_cast<cfd::gpu::DeviceFv*>(h);
+}
+
+int ref_fv_gradient(void* h, const double* phi, const double* bv, int scheme, double* grad) {
+    try {
+        static_cast<cfd::gpu::DeviceFv*>(h)->gradient(phi, bv, scheme, grad);
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
+int ref_fv_vector_gradient(void* h, const double* u, const double* ub, int scheme,
+                           double* grad) {
+    try {
+        static_cast<cfd::gpu::DeviceFv*>(h)->vector_gradient(u, ub, scheme, grad);
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
+int ref_fv_scalar_corrections(void* h, const double* phi, const double* bv, int scheme,
+                              const double* flux, const double* gamma, int linear_upwind,
+                              double* source) {
+    try {
+        static_cast<cfd::gpu::DeviceFv*>(h)->scalar_corrections(phi, bv, scheme, flux, gamma,
+                                                               linear_upwind != 0, source);
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
+int ref_fv_momentum_corrections(void* h, const double* flux, const double* nu_face,
+                                int linear_upwind, int limited, int venkat, const double* eps2,
+                                double central, int transpose_term, double* source) {
+    try {
+        static_cast<cfd::gpu::DeviceFv*>(h)->momentum_corrections(
+            flux, nu_face, linear_upwind != 0, limited != 0, venkat != 0, eps2, central,
+            transpose_term != 0, source);
+        return 0;
+    } catch (const std::exception&) {
+        return 2;
+    }
 }
 
 } // extern "C"

@@ -970,7 +970,7 @@ int cfdb_system_solve_ldu(cfdb_system* sys, const double* diag, const double* up
                 sys->ldu_stage = sys->ldu_arena.alloc<double>(4 * static_cast<size_t>(n) + 2 * static_cast<size_t>(nf));
             double* s = sys->ldu_stage;
             auto put = [&](double* dst, const double* src, int cnt) {
-                if (cnt > 0) CFDB_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * cnt, cudaMemcpyHostToDevice, st));
+                if (cnt > 0) sys->eng->copier().to_device(dst, src, sizeof(double) * cnt, st);
             };
             put(s, diag, n);
             put(s + n, upper, nf);
@@ -1012,10 +1012,7 @@ int cfdb_system_solve_ldu(cfdb_system* sys, const double* diag, const double* up
         result->iterations = r.iterations;
         const LduNorms n1 = ldu_residual_norms(m, dd, du, dl, db, dx, sys->norm_part, st);
         result->final_residual = n1.res / (n1.norm + kSmall);
-        if (!device_arrays) {
-            CFDB_CUDA(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
-            CFDB_CUDA(cudaStreamSynchronize(st));
-        }
+        if (!device_arrays) sys->eng->copier().to_host(x, dx, sizeof(double) * n, st);
     });
 }
 

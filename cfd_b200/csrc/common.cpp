@@ -1,6 +1,7 @@
 #include "common.hpp"
 
 #include <algorithm>
+#include <cstring>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -100,6 +101,100 @@ void DeviceBuffer::release() {
         if (cur != device_) cudaSetDevice(cur);
         ptr_ = nullptr;
         bytes_ = 0;
+    }
+}
+
+
+namespace {
+
+// host memcpy by all OpenMP threads, in blocks of at least 256 KB
+void parallel_copy(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kBlock = size_t(256) << 10;
+    const long long nblk = static_cast<long long>((bytes + kBlock - 1) / kBlock);
+    auto* d = static_cast<char*>(dst);
+    const auto* s = static_cast<const char*>(src);
+#pragma omp parallel for schedule(static) if (nblk > 1)
+    for (long long b = 0; b < nblk; ++b) {
+        const size_t off = static_cast<size_t>(b) * kBlock;
+        std::memcpy(d + off, s + off, std::min(kBlock, bytes - off));
+    }
+}
+
+} // namespace
+
+StagedCopier::~StagedCopier() {
+    for (int b = 0; b < 2; ++b) {
+        if (ev_[b] != nullptr) {
+            cudaEventSynchronize(ev_[b]);
+            cudaEventDestroy(ev_[b]);
+        }
+    }
+}
+
+void StagedCopier::ready(int b) {
+    if (ev_[b] == nullptr) CFDB_CUDA(cudaEventCreateWithFlags(&ev_[b], cudaEventDisableTiming));
+    if (pending_[b]) {
+        CFDB_CUDA(cudaEventSynchronize(ev_[b]));
+        pending_[b] = false;
+    }
+}
+
+bool StagedCopier::page_locked(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+void StagedCopier::to_device(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    if (bytes == 0) return;
+    if (bytes < kDirect || page_locked(src)) {
+        CFDB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+        return;
+    }
+    auto* d = static_cast<char*>(dst);
+    const auto* s = static_cast<const char*>(src);
+    for (size_t off = 0, k = 0; off < bytes; off += kChunk, ++k) {
+        const int b = static_cast<int>(k & 1);
+        const size_t len = std::min(kChunk, bytes - off);
+        ready(b);
+        void* pin = buf_[b].get(kChunk);
+        parallel_copy(pin, s + off, len);
+        CFDB_CUDA(cudaMemcpyAsync(d + off, pin, len, cudaMemcpyHostToDevice, st));
+        CFDB_CUDA(cudaEventRecord(ev_[b], st));
+        pending_[b] = true;
+    }
+}
+
+void StagedCopier::to_host(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    if (bytes == 0) return;
+    if (bytes < kDirect || page_locked(dst)) {
+        CFDB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+        CFDB_CUDA(cudaStreamSynchronize(st));
+        return;
+    }
+    auto* d = static_cast<char*>(dst);
+    const auto* s = static_cast<const char*>(src);
+    const size_t nchunks = (bytes + kChunk - 1) / kChunk;
+    auto issue = [&](size_t k) {
+        const int b = static_cast<int>(k & 1);
+        const size_t off = k * kChunk;
+        ready(b);
+        CFDB_CUDA(cudaMemcpyAsync(buf_[b].get(kChunk), s + off, std::min(kChunk, bytes - off),
+                                  cudaMemcpyDeviceToHost, st));
+        CFDB_CUDA(cudaEventRecord(ev_[b], st));
+        pending_[b] = true;
+    };
+    issue(0);
+    if (nchunks > 1) issue(1);
+    for (size_t k = 0; k < nchunks; ++k) {
+        const int b = static_cast<int>(k & 1);
+        ready(b); // chunk k has arrived
+        const size_t off = k * kChunk;
+        parallel_copy(d + off, buf_[b].get(kChunk), std::min(kChunk, bytes - off));
+        if (k + 2 < nchunks) issue(k + 2);
     }
 }
 

@@ -90,6 +90,34 @@ private:
     size_t bytes_ = 0;
 };
 
+// Copies between pageable host arrays and device arrays through two page-locked chunks:
+// all host threads copy one chunk between the caller's array and page-locked memory while
+// the DMA of the other chunk runs, so a large copy moves at the DMA rate instead of the
+// driver's single-threaded staging rate. Copies below kDirect bytes go straight through
+// cudaMemcpyAsync, and so do copies from or to page-locked host memory. The chunks are
+// reused after their last DMA has completed (events).
+class StagedCopier {
+public:
+    StagedCopier() = default;
+    ~StagedCopier();
+    StagedCopier(const StagedCopier&) = delete;
+    StagedCopier& operator=(const StagedCopier&) = delete;
+    // enqueues the copy on st; src may be reused when this returns
+    void to_device(void* dst, const void* src, size_t bytes, cudaStream_t st);
+    // waits for the work already on st, then copies; returns when dst holds the data
+    void to_host(void* dst, const void* src, size_t bytes, cudaStream_t st);
+
+    static constexpr size_t kChunk = size_t(8) << 20;
+    static constexpr size_t kDirect = size_t(4) << 20;
+
+private:
+    static bool page_locked(const void* p);
+    void ready(int b);
+    PinnedBuffer buf_[2];
+    cudaEvent_t ev_[2] = {nullptr, nullptr};
+    bool pending_[2] = {false, false};
+};
+
 // Device arrays are grouped in an arena per engine so their footprint can be reported.
 class DeviceArena {
 public:

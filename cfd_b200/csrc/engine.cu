@@ -781,20 +781,17 @@ void Engine::upload_values(const std::vector<const double*>& host_src) {
         lens[s] = next - vs_off_[s];
     }
     for (int s = 0; s < n_sys_; ++s) {
-        if (lens[s] > 0) {
-            CFDB_CUDA(cudaMemcpyAsync(vs_ + vs_off_[s], host_src[s], sizeof(double) * lens[s],
-                                      cudaMemcpyHostToDevice, stream_));
-        }
+        if (lens[s] > 0) copier_.to_device(vs_ + vs_off_[s], host_src[s], sizeof(double) * lens[s], stream_);
     }
     set_values_device(vs_, vs_, vs_, INT_MAX, INT_MAX);
 }
 
 void Engine::upload_values_ldu(const double* diag, const double* upper, const double* lower, int n, int nf) {
     if (n_sys_ != 1 || vs_total_ != static_cast<long long>(n) + 2LL * nf) fail(1, "upload_values_ldu: layout mismatch");
-    CFDB_CUDA(cudaMemcpyAsync(vs_, diag, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
+    copier_.to_device(vs_, diag, sizeof(double) * n, stream_);
     if (nf > 0) {
-        CFDB_CUDA(cudaMemcpyAsync(vs_ + n, upper, sizeof(double) * nf, cudaMemcpyHostToDevice, stream_));
-        CFDB_CUDA(cudaMemcpyAsync(vs_ + n + nf, lower, sizeof(double) * nf, cudaMemcpyHostToDevice, stream_));
+        copier_.to_device(vs_ + n, upper, sizeof(double) * nf, stream_);
+        copier_.to_device(vs_ + n + nf, lower, sizeof(double) * nf, stream_);
     }
     set_values_device(vs_, vs_, vs_, INT_MAX, INT_MAX);
 }
@@ -832,19 +829,24 @@ void Engine::get_solution_concat(double* x) {
 }
 
 void Engine::set_rhs(int s, const double* b, bool dev) {
-    CFDB_CUDA(cudaMemcpyAsync(b_ + off0_[s], b, sizeof(double) * n_of_[s],
-                              dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
+    if (dev)
+        CFDB_CUDA(cudaMemcpyAsync(b_ + off0_[s], b, sizeof(double) * n_of_[s], cudaMemcpyDeviceToDevice, stream_));
+    else
+        copier_.to_device(b_ + off0_[s], b, sizeof(double) * n_of_[s], stream_);
 }
 
 void Engine::set_guess(int s, const double* x, bool dev) {
-    CFDB_CUDA(cudaMemcpyAsync(x_ + off0_[s], x, sizeof(double) * n_of_[s],
-                              dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
+    if (dev)
+        CFDB_CUDA(cudaMemcpyAsync(x_ + off0_[s], x, sizeof(double) * n_of_[s], cudaMemcpyDeviceToDevice, stream_));
+    else
+        copier_.to_device(x_ + off0_[s], x, sizeof(double) * n_of_[s], stream_);
 }
 
 void Engine::get_solution(int s, double* x, bool dev) {
-    CFDB_CUDA(cudaMemcpyAsync(x, x_ + off0_[s], sizeof(double) * n_of_[s],
-                              dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream_));
-    if (!dev) CFDB_CUDA(cudaStreamSynchronize(stream_));
+    if (dev)
+        CFDB_CUDA(cudaMemcpyAsync(x, x_ + off0_[s], sizeof(double) * n_of_[s], cudaMemcpyDeviceToDevice, stream_));
+    else
+        copier_.to_host(x, x_ + off0_[s], sizeof(double) * n_of_[s], stream_);
 }
 
 void Engine::set_residual(int s, const double* r, bool dev) {

@@ -87,6 +87,7 @@ public:
     [[nodiscard]] bool has64() const { return need64_; }
     [[nodiscard]] size_t device_bytes() const { return arena_.bytes() + arena0_.bytes(); }
     [[nodiscard]] cudaStream_t stream() const { return stream_; }
+    StagedCopier& copier() { return copier_; }
     [[nodiscard]] int device() const { return device_; }
     [[nodiscard]] int levels() const { return n_levels_; }
     [[nodiscard]] int level_rows(int l) const;
@@ -197,6 +198,7 @@ private:
 
     int device_;
     cudaStream_t stream_ = nullptr;
+    StagedCopier copier_; // host-array uploads and downloads
     DeviceArena arena_;
     int n_sys_ = 0;
     int n_levels_ = 0;

@@ -4,14 +4,16 @@
 // non-orthogonal correction, transpose viscous term). Interface: fv_device.hpp:33-72 (DeviceFv,
 // FvMeshView); per-cell arithmetic: fv_cell.inc:24-261; call sequence: fv_openmp.cpp:158-305.
 //
-// One thread per cell gathers over the cell's faces in ascending face order (the cell_faces
-// CSR of the mesh view), so every cell sums the same terms in the same order as the
-// reference's per-cell loops; every product and sum is rounded separately (no FMA contraction:
-// this file is compiled with --fmad=false), so the results are bit-identical to the
-// reference's host build. The vector gradient computes the three components in one pass over
-// the mesh (the reference makes three passes); each component's arithmetic is unchanged.
-// Mesh arrays stay resident on the device for the life of the object; vectors are
-// xyz-interleaved, gradients of vectors are 9 values per cell with g[3 i + j] = du_i / dx_j.
+// Every cell sums the same terms in the same order as the reference's per-cell loops (its
+// faces in ascending order, the cell_faces CSR of the mesh view), and every product and sum is
+// rounded separately (no FMA contraction: this file is compiled with --fmad=false), so the
+// results are bit-identical to the reference's host build. Gradients: one thread per (cell,
+// component), all components of a vector field in one launch (the reference makes one pass
+// per component). Explicit corrections: a face's flux does not depend on which of its cells
+// sums it, so it is computed once per internal face (coalesced over faces) and then summed
+// per cell in face order. Limiter: one thread per cell. Mesh arrays stay resident on the
+// device for the life of the object; vectors are xyz-interleaved, gradients of vectors are 9
+// values per cell with g[3 i + j] = du_i / dx_j.
 #include "../../include/cfdb.h"
 
 #include <algorithm>
@@ -64,7 +66,10 @@ struct cfdb_device_fv {
     double* coef = nullptr;  // internal faces
     double* src = nullptr;   // 3 n_cells
     double* tmp = nullptr;   // 9 n_cells: least-squares gradient of the corrected scheme
+    double* eface = nullptr; // 3 internal faces: explicit face fluxes before the cell sums
+    int maxf = 0;            // 4, 6 or 8: no cell has more faces (batched face sums); 0: any
     bool have_vector = false;
+    StagedCopier copier;     // host-array entry points
     ~cfdb_device_fv() {
         if (st != nullptr) {
             cudaStreamSynchronize(st);
@@ -79,164 +84,119 @@ constexpr int kThreads = 256;
 
 int grid(int n) { return std::max(1, (n + kThreads - 1) / kThreads); }
 
-// Gradient of NC components (stride NC per cell / boundary face) of phi: Green-Gauss with
-// linear face interpolation, or weighted least squares (fv_cell.inc:24-74). out: 3 NC per cell.
+// Gradient of component i of a field with NC values per cell / boundary face: Green-Gauss
+// with linear face interpolation, or weighted least squares (fv_cell.inc:24-74). One thread
+// per (cell, component), t = NC c + i, so a vector field's three components are three
+// independent threads with the scalar kernel's register footprint; the components share
+// their face-index and face-vector loads in L1. out[3 (NC c + i) + j] = d phi_i / dx_j.
 template <int NC, bool LSQ>
 __global__ void __launch_bounds__(kThreads) k_cell_gradient(FvMesh m, const double* __restrict__ phi,
                                                             const double* __restrict__ bv,
                                                             double* __restrict__ out) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.nc) return;
-    double g[NC][3];
-    double pc[NC];
-#pragma unroll
-    for (int i = 0; i < NC; ++i) {
-        g[i][0] = g[i][1] = g[i][2] = 0.0;
-        pc[i] = phi[c * NC + i];
-    }
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m.nc * NC) return;
+    const int c = NC == 1 ? t : t / NC;
+    const int i = NC == 1 ? 0 : t - c * NC;
+    double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    const double pc = phi[t];
     const int k1 = m.start[c + 1];
     for (int k = m.start[c]; k < k1; ++k) {
         const int f = m.faces[k];
         if (LSQ) {
-            const double d0 = m.lsq_d[3 * f], d1 = m.lsq_d[3 * f + 1], d2 = m.lsq_d[3 * f + 2];
-            if (f < m.nif) {
-                const int o = m.own[f], n = m.nei[f];
-#pragma unroll
-                for (int i = 0; i < NC; ++i) {
-                    const double dv = phi[n * NC + i] - phi[o * NC + i];
-                    g[i][0] += d0 * dv;
-                    g[i][1] += d1 * dv;
-                    g[i][2] += d2 * dv;
-                }
-            } else {
-                const double* b = bv + (f - m.nif) * NC;
-#pragma unroll
-                for (int i = 0; i < NC; ++i) {
-                    const double dv = b[i] - pc[i];
-                    g[i][0] += d0 * dv;
-                    g[i][1] += d1 * dv;
-                    g[i][2] += d2 * dv;
-                }
-            }
+            const double dv = f < m.nif ? phi[m.nei[f] * NC + i] - phi[m.own[f] * NC + i]
+                                        : bv[(f - m.nif) * NC + i] - pc;
+            g0 += m.lsq_d[3 * f] * dv;
+            g1 += m.lsq_d[3 * f + 1] * dv;
+            g2 += m.lsq_d[3 * f + 2] * dv;
         } else if (f < m.nif) {
             const double wf = m.w[f];
-            const int o = m.own[f], n = m.nei[f];
-            const double s0 = m.sf[3 * f], s1 = m.sf[3 * f + 1], s2 = m.sf[3 * f + 2];
-#pragma unroll
-            for (int i = 0; i < NC; ++i) {
-                const double pf = wf * phi[o * NC + i] + (1.0 - wf) * phi[n * NC + i];
-                if (o == c) {
-                    g[i][0] += s0 * pf;
-                    g[i][1] += s1 * pf;
-                    g[i][2] += s2 * pf;
-                } else {
-                    g[i][0] -= s0 * pf;
-                    g[i][1] -= s1 * pf;
-                    g[i][2] -= s2 * pf;
-                }
+            const int o = m.own[f];
+            const double pf = wf * phi[o * NC + i] + (1.0 - wf) * phi[m.nei[f] * NC + i];
+            if (o == c) {
+                g0 += m.sf[3 * f] * pf;
+                g1 += m.sf[3 * f + 1] * pf;
+                g2 += m.sf[3 * f + 2] * pf;
+            } else {
+                g0 -= m.sf[3 * f] * pf;
+                g1 -= m.sf[3 * f + 1] * pf;
+                g2 -= m.sf[3 * f + 2] * pf;
             }
         } else {
-            const double* b = bv + (f - m.nif) * NC;
-            const double s0 = m.sf[3 * f], s1 = m.sf[3 * f + 1], s2 = m.sf[3 * f + 2];
-#pragma unroll
-            for (int i = 0; i < NC; ++i) {
-                g[i][0] += s0 * b[i];
-                g[i][1] += s1 * b[i];
-                g[i][2] += s2 * b[i];
-            }
+            const double b = bv[(f - m.nif) * NC + i];
+            g0 += m.sf[3 * f] * b;
+            g1 += m.sf[3 * f + 1] * b;
+            g2 += m.sf[3 * f + 2] * b;
         }
     }
-    double* o = out + static_cast<size_t>(c) * (3 * NC);
+    double* o = out + 3 * static_cast<size_t>(t);
     if (LSQ) {
         const double* a = m.lsq + 9 * static_cast<size_t>(c); // column-major
-        const double a0 = a[0], a1 = a[1], a2 = a[2], a3 = a[3], a4 = a[4], a5 = a[5], a6 = a[6],
-                     a7 = a[7], a8 = a[8];
-#pragma unroll
-        for (int i = 0; i < NC; ++i) {
-            o[3 * i] = a0 * g[i][0] + a3 * g[i][1] + a6 * g[i][2];
-            o[3 * i + 1] = a1 * g[i][0] + a4 * g[i][1] + a7 * g[i][2];
-            o[3 * i + 2] = a2 * g[i][0] + a5 * g[i][1] + a8 * g[i][2];
-        }
+        o[0] = a[0] * g0 + a[3] * g1 + a[6] * g2;
+        o[1] = a[1] * g0 + a[4] * g1 + a[7] * g2;
+        o[2] = a[2] * g0 + a[5] * g1 + a[8] * g2;
     } else {
         const double v = m.vol[c];
-#pragma unroll
-        for (int i = 0; i < NC; ++i) {
-            o[3 * i] = g[i][0] / v;
-            o[3 * i + 1] = g[i][1] / v;
-            o[3 * i + 2] = g[i][2] / v;
-        }
+        o[0] = g0 / v;
+        o[1] = g1 / v;
+        o[2] = g2 / v;
     }
 }
 
-// Skewness-corrected Green-Gauss (fv_cell.inc:76-121): face values w phi_P + (1 - w) phi_N +
-// (w g_P + (1 - w) g_N) . (x_f - x_ip) with the least-squares gradient g (3 NC per cell).
+// Skewness-corrected Green-Gauss (fv_cell.inc:76-121) of component i, one thread per
+// (cell, component): face values w phi_P + (1 - w) phi_N + (w g_P + (1 - w) g_N) . (x_f - x_ip)
+// with the least-squares gradient g (layout of k_cell_gradient's output).
 template <int NC>
 __global__ void __launch_bounds__(kThreads) k_cell_gradient_corrected(FvMesh m, const double* __restrict__ phi,
                                                                       const double* __restrict__ bv,
                                                                       const double* __restrict__ g,
                                                                       double* __restrict__ out) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.nc) return;
-    double a[NC][3];
-#pragma unroll
-    for (int i = 0; i < NC; ++i) a[i][0] = a[i][1] = a[i][2] = 0.0;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m.nc * NC) return;
+    const int c = NC == 1 ? t : t / NC;
+    const int i = NC == 1 ? 0 : t - c * NC;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     const int k1 = m.start[c + 1];
     for (int k = m.start[c]; k < k1; ++k) {
         const int f = m.faces[k];
-        const double s0 = m.sf[3 * f], s1 = m.sf[3 * f + 1], s2 = m.sf[3 * f + 2];
         if (f < m.nif) {
             const int p = m.own[f], n = m.nei[f];
             const double wf = m.w[f];
-            double r[3]; // x_f - x_ip, x_ip = w x_P + (1 - w) x_N
+            double pf = wf * phi[p * NC + i] + (1.0 - wf) * phi[n * NC + i];
+            const double* gp = g + 3 * (static_cast<size_t>(p) * NC + i);
+            const double* gn = g + 3 * (static_cast<size_t>(n) * NC + i);
+            double dot = 0.0;
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
                 const double xip = wf * m.cc[3 * p + j] + (1.0 - wf) * m.cc[3 * n + j];
-                r[j] = m.cf[3 * f + j] - xip;
+                const double gf = wf * gp[j] + (1.0 - wf) * gn[j];
+                dot = j == 0 ? gf * (m.cf[3 * f] - xip) : dot + gf * (m.cf[3 * f + j] - xip);
             }
-            const double* gp = g + static_cast<size_t>(p) * (3 * NC);
-            const double* gn = g + static_cast<size_t>(n) * (3 * NC);
-#pragma unroll
-            for (int i = 0; i < NC; ++i) {
-                double pf = wf * phi[p * NC + i] + (1.0 - wf) * phi[n * NC + i];
-                double dot = 0.0;
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const double gf = wf * gp[3 * i + j] + (1.0 - wf) * gn[3 * i + j];
-                    dot = j == 0 ? gf * r[0] : dot + gf * r[j];
-                }
-                pf += dot;
-                if (p == c) {
-                    a[i][0] += s0 * pf;
-                    a[i][1] += s1 * pf;
-                    a[i][2] += s2 * pf;
-                } else {
-                    a[i][0] -= s0 * pf;
-                    a[i][1] -= s1 * pf;
-                    a[i][2] -= s2 * pf;
-                }
+            pf += dot;
+            if (p == c) {
+                a0 += m.sf[3 * f] * pf;
+                a1 += m.sf[3 * f + 1] * pf;
+                a2 += m.sf[3 * f + 2] * pf;
+            } else {
+                a0 -= m.sf[3 * f] * pf;
+                a1 -= m.sf[3 * f + 1] * pf;
+                a2 -= m.sf[3 * f + 2] * pf;
             }
         } else {
-            const double* b = bv + (f - m.nif) * NC;
-#pragma unroll
-            for (int i = 0; i < NC; ++i) {
-                a[i][0] += s0 * b[i];
-                a[i][1] += s1 * b[i];
-                a[i][2] += s2 * b[i];
-            }
+            const double b = bv[(f - m.nif) * NC + i];
+            a0 += m.sf[3 * f] * b;
+            a1 += m.sf[3 * f + 1] * b;
+            a2 += m.sf[3 * f + 2] * b;
         }
     }
-    double* o = out + static_cast<size_t>(c) * (3 * NC);
+    double* o = out + 3 * static_cast<size_t>(t);
     const double v = m.vol[c];
-#pragma unroll
-    for (int i = 0; i < NC; ++i) {
-        o[3 * i] = a[i][0] / v;
-        o[3 * i + 1] = a[i][1] / v;
-        o[3 * i + 2] = a[i][2] / v;
-    }
+    o[0] = a0 / v;
+    o[1] = a1 / v;
+    o[2] = a2 / v;
 }
 
 // Barth-Jespersen / Venkatakrishnan limiter per component of the vector field u with boundary
-// values ub and gradient g (9 per cell) (fv_cell.inc:123-163).
+// values ub and gradient g (9 per cell) (fv_cell.inc:123-163), one thread per cell.
 __global__ void __launch_bounds__(kThreads) k_cell_limiter(FvMesh m, const double* __restrict__ u,
                                                            const double* __restrict__ ub,
                                                            const double* __restrict__ g, int venkat,
@@ -289,91 +249,132 @@ __global__ void __launch_bounds__(kThreads) k_cell_limiter(FvMesh m, const doubl
     for (int i = 0; i < 3; ++i) lim[3 * c + i] = l[i];
 }
 
-// Explicit internal-face fluxes of a scalar equation with the cell gradient g (3 per cell),
-// accumulated into source (fv_cell.inc:165-196).
-__global__ void __launch_bounds__(kThreads) k_scalar_corrections(FvMesh m, const double* __restrict__ g,
-                                                                 const double* __restrict__ flux,
-                                                                 const double* __restrict__ gamma,
-                                                                 int linear_upwind, double* __restrict__ source) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.nc) return;
-    double s = 0.0;
-    const int k1 = m.start[c + 1];
-    for (int k = m.start[c]; k < k1; ++k) {
-        const int f = m.faces[k];
-        if (f >= m.nif) break; // boundary faces follow the internal ones
-        const int p = m.own[f], n = m.nei[f];
-        const double fl = flux[f];
-        double e = 0.0;
-        if (linear_upwind) {
-            const int up = fl >= 0.0 ? p : n;
-            const double r0 = m.cf[3 * f] - m.cc[3 * up];
-            const double r1 = m.cf[3 * f + 1] - m.cc[3 * up + 1];
-            const double r2 = m.cf[3 * f + 2] - m.cc[3 * up + 2];
-            e -= fl * (g[3 * up] * r0 + g[3 * up + 1] * r1 + g[3 * up + 2] * r2);
-        }
-        const double wf = m.w[f];
-        const double gf0 = wf * g[3 * p] + (1.0 - wf) * g[3 * n];
-        const double gf1 = wf * g[3 * p + 1] + (1.0 - wf) * g[3 * n + 1];
-        const double gf2 = wf * g[3 * p + 2] + (1.0 - wf) * g[3 * n + 2];
-        e += gamma[f] * (m.kv[3 * f] * gf0 + m.kv[3 * f + 1] * gf1 + m.kv[3 * f + 2] * gf2);
-        s = p == c ? s + e : s - e;
+// Explicit internal-face flux of a scalar equation with the cell gradient g (3 per cell)
+// (fv_cell.inc:165-196). The flux e_f depends on the face alone, so it is computed once per
+// internal face (one thread per face); k_cell_face_sums then adds +-e_f over each cell's faces
+// in the reference's order. The two cells of a face receive the same rounded e_f as in the
+// reference, which computes it once from each side.
+__global__ void __launch_bounds__(kThreads) k_scalar_face_terms(FvMesh m, const double* __restrict__ g,
+                                                                const double* __restrict__ flux,
+                                                                const double* __restrict__ gamma,
+                                                                int linear_upwind, double* __restrict__ e_out) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nif) return;
+    const int p = m.own[f], n = m.nei[f];
+    const double fl = flux[f];
+    double e = 0.0;
+    if (linear_upwind) {
+        const int up = fl >= 0.0 ? p : n;
+        const double r0 = m.cf[3 * f] - m.cc[3 * up];
+        const double r1 = m.cf[3 * f + 1] - m.cc[3 * up + 1];
+        const double r2 = m.cf[3 * f + 2] - m.cc[3 * up + 2];
+        e -= fl * (g[3 * up] * r0 + g[3 * up + 1] * r1 + g[3 * up + 2] * r2);
     }
-    source[c] += s;
+    const double wf = m.w[f];
+    const double gf0 = wf * g[3 * p] + (1.0 - wf) * g[3 * n];
+    const double gf1 = wf * g[3 * p + 1] + (1.0 - wf) * g[3 * n + 1];
+    const double gf2 = wf * g[3 * p + 2] + (1.0 - wf) * g[3 * n + 2];
+    e += gamma[f] * (m.kv[3 * f] * gf0 + m.kv[3 * f + 1] * gf1 + m.kv[3 * f + 2] * gf2);
+    e_out[f] = e;
 }
 
-// Explicit internal-face fluxes of the momentum equation (fv_cell.inc:198-259).
-__global__ void __launch_bounds__(kThreads) k_momentum_corrections(
+// Explicit internal-face flux of the momentum equation (fv_cell.inc:198-259), once per face.
+__global__ void __launch_bounds__(kThreads) k_momentum_face_terms(
     FvMesh m, const double* __restrict__ g, const double* __restrict__ lim, int limited,
     const double* __restrict__ flux, const double* __restrict__ nu_face, int linear_upwind, double central,
-    const double* __restrict__ u, int transpose_term, double* __restrict__ source) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.nc) return;
-    double s[3] = {0.0, 0.0, 0.0};
-    const int k1 = m.start[c + 1];
-    for (int k = m.start[c]; k < k1; ++k) {
-        const int f = m.faces[k];
-        if (f >= m.nif) break;
-        const int p = m.own[f], n = m.nei[f];
-        const double fl = flux[f];
-        const double wf = m.w[f];
-        double e[3] = {0.0, 0.0, 0.0};
-        if (linear_upwind) {
-            const int up = fl >= 0.0 ? p : n;
-            const double r0 = m.cf[3 * f] - m.cc[3 * up];
-            const double r1 = m.cf[3 * f + 1] - m.cc[3 * up + 1];
-            const double r2 = m.cf[3 * f + 2] - m.cc[3 * up + 2];
-            const double* gu = g + 9 * static_cast<size_t>(up);
+    const double* __restrict__ u, int transpose_term, double* __restrict__ e_out) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nif) return;
+    const int p = m.own[f], n = m.nei[f];
+    const double fl = flux[f];
+    const double wf = m.w[f];
+    double e[3] = {0.0, 0.0, 0.0};
+    if (linear_upwind) {
+        const int up = fl >= 0.0 ? p : n;
+        const double r0 = m.cf[3 * f] - m.cc[3 * up];
+        const double r1 = m.cf[3 * f + 1] - m.cc[3 * up + 1];
+        const double r2 = m.cf[3 * f + 2] - m.cc[3 * up + 2];
+        const double* gu = g + 9 * static_cast<size_t>(up);
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                double d = gu[3 * i] * r0 + gu[3 * i + 1] * r1 + gu[3 * i + 2] * r2;
-                if (central > 0.0) {
-                    const double uf = wf * u[3 * p + i] + (1.0 - wf) * u[3 * n + i];
-                    d = (1.0 - central) * d + central * (uf - u[3 * up + i]);
-                }
-                if (limited) d = lim[3 * up + i] * d;
-                e[i] -= fl * d;
+        for (int i = 0; i < 3; ++i) {
+            double d = gu[3 * i] * r0 + gu[3 * i + 1] * r1 + gu[3 * i + 2] * r2;
+            if (central > 0.0) {
+                const double uf = wf * u[3 * p + i] + (1.0 - wf) * u[3 * n + i];
+                d = (1.0 - central) * d + central * (uf - u[3 * up + i]);
             }
+            if (limited) d = lim[3 * up + i] * d;
+            e[i] -= fl * d;
         }
-        const double* gp = g + 9 * static_cast<size_t>(p);
-        const double* gn = g + 9 * static_cast<size_t>(n);
-        double gf[9];
+    }
+    const double* gp = g + 9 * static_cast<size_t>(p);
+    const double* gn = g + 9 * static_cast<size_t>(n);
+    double gf[9];
 #pragma unroll
-        for (int j = 0; j < 9; ++j) gf[j] = wf * gp[j] + (1.0 - wf) * gn[j];
-        const double nu = nu_face[f];
-        const double k0 = m.kv[3 * f], kk1 = m.kv[3 * f + 1], k2 = m.kv[3 * f + 2];
+    for (int j = 0; j < 9; ++j) gf[j] = wf * gp[j] + (1.0 - wf) * gn[j];
+    const double nu = nu_face[f];
+    const double k0 = m.kv[3 * f], k1 = m.kv[3 * f + 1], k2 = m.kv[3 * f + 2];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) e[i] += nu * (gf[3 * i] * k0 + gf[3 * i + 1] * kk1 + gf[3 * i + 2] * k2);
-        if (transpose_term) {
-            const double a0 = m.sf[3 * f], a1 = m.sf[3 * f + 1], a2 = m.sf[3 * f + 2];
+    for (int i = 0; i < 3; ++i) e[i] += nu * (gf[3 * i] * k0 + gf[3 * i + 1] * k1 + gf[3 * i + 2] * k2);
+    if (transpose_term) {
+        const double a0 = m.sf[3 * f], a1 = m.sf[3 * f + 1], a2 = m.sf[3 * f + 2];
 #pragma unroll
-            for (int i = 0; i < 3; ++i) e[i] += nu * (gf[i] * a0 + gf[i + 3] * a1 + gf[i + 6] * a2);
-        }
-#pragma unroll
-        for (int i = 0; i < 3; ++i) s[i] = p == c ? s[i] + e[i] : s[i] - e[i];
+        for (int i = 0; i < 3; ++i) e[i] += nu * (gf[i] * a0 + gf[i + 3] * a1 + gf[i + 6] * a2);
     }
 #pragma unroll
-    for (int i = 0; i < 3; ++i) source[3 * c + i] += s[i];
+    for (int i = 0; i < 3; ++i) e_out[3 * static_cast<size_t>(f) + i] = e[i];
+}
+
+// source[c] += sum over the cell's faces, in ascending order up to its first boundary face
+// (fv_cell.inc:172-174, 210-212), of +e_f (owner) or -e_f (neighbour); NC values per face.
+// MAXF > 0: every cell has at most MAXF faces; the indices, owners and face terms of all its
+// faces are loaded before the (unchanged, ordered) sums.
+template <int NC, int MAXF>
+__global__ void __launch_bounds__(kThreads) k_cell_face_sums(FvMesh m, const double* __restrict__ e,
+                                                             double* __restrict__ source) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    double s[NC];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) s[i] = 0.0;
+    const int k0 = m.start[c], k1 = m.start[c + 1];
+    if (MAXF > 0) {
+        constexpr int F = MAXF > 0 ? MAXF : 1;
+        int f[F];
+        bool mine[F];
+        double ev[F][NC];
+        bool live = true;
+#pragma unroll
+        for (int j = 0; j < F; ++j) {
+            const int fj = k0 + j < k1 ? m.faces[k0 + j] : m.nif; // past the end: a stop marker
+            live = live && fj < m.nif;
+            f[j] = live ? fj : -1;
+        }
+#pragma unroll
+        for (int j = 0; j < F; ++j) {
+            mine[j] = f[j] >= 0 ? m.own[f[j]] == c : false;
+#pragma unroll
+            for (int i = 0; i < NC; ++i) ev[j][i] = f[j] >= 0 ? e[static_cast<size_t>(f[j]) * NC + i] : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < F; ++j) {
+            if (f[j] < 0) break;
+#pragma unroll
+            for (int i = 0; i < NC; ++i) s[i] = mine[j] ? s[i] + ev[j][i] : s[i] - ev[j][i];
+        }
+    } else {
+        for (int k = k0; k < k1; ++k) {
+            const int f = m.faces[k];
+            if (f >= m.nif) break;
+            const bool mine = m.own[f] == c;
+#pragma unroll
+            for (int i = 0; i < NC; ++i) {
+                const double ev = e[static_cast<size_t>(f) * NC + i];
+                s[i] = mine ? s[i] + ev : s[i] - ev;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NC; ++i) source[static_cast<size_t>(c) * NC + i] += s[i];
 }
 
 template <class F> int guarded(F&& f) {
@@ -394,26 +395,47 @@ void check_scheme(int scheme) {
         fail(CFDB_ERR_BAD_ARG, "DeviceFv: unknown gradient scheme " + std::to_string(scheme));
 }
 
-// gradient_loop of fv_openmp.cpp:250-297 with all NC components in one pass
+// Launches K<..., MAXF> with the mesh's face-count class (0: any number of faces).
+#define CFDB_FV_BY_MAXF(fv, LAUNCH)          \
+    switch ((fv)->maxf) {                   \
+    case 4: LAUNCH(4); break;               \
+    case 6: LAUNCH(6); break;               \
+    case 8: LAUNCH(8); break;               \
+    default: LAUNCH(0); break;              \
+    }
+
+int grid_of(long long threads) { return static_cast<int>(std::max(1LL, (threads + kThreads - 1) / kThreads)); }
+
+// gradient_loop of fv_openmp.cpp:250-297: all NC components in one launch
 template <int NC>
 void launch_gradient(cfdb_device_fv* fv, const double* phi, const double* bv, int scheme, double* out) {
     const FvMesh& m = fv->m;
+    if (bv == nullptr) bv = fv->vbv; // no boundary faces: never read, but a valid address
+    const int blocks = grid_of(static_cast<long long>(m.nc) * NC);
     if (scheme == CFDB_GRAD_GAUSS_CORRECTED) {
-        k_cell_gradient<NC, true><<<grid(m.nc), kThreads, 0, fv->st>>>(m, phi, bv, fv->tmp);
-        k_cell_gradient_corrected<NC><<<grid(m.nc), kThreads, 0, fv->st>>>(m, phi, bv, fv->tmp, out);
+        k_cell_gradient<NC, true><<<blocks, kThreads, 0, fv->st>>>(m, phi, bv, fv->tmp);
+        k_cell_gradient_corrected<NC><<<blocks, kThreads, 0, fv->st>>>(m, phi, bv, fv->tmp, out);
     } else if (scheme == CFDB_GRAD_LEAST_SQUARES) {
-        k_cell_gradient<NC, true><<<grid(m.nc), kThreads, 0, fv->st>>>(m, phi, bv, out);
+        k_cell_gradient<NC, true><<<blocks, kThreads, 0, fv->st>>>(m, phi, bv, out);
     } else {
-        k_cell_gradient<NC, false><<<grid(m.nc), kThreads, 0, fv->st>>>(m, phi, bv, out);
+        k_cell_gradient<NC, false><<<blocks, kThreads, 0, fv->st>>>(m, phi, bv, out);
     }
     CFDB_CUDA(cudaGetLastError());
+}
+
+template <int NC, int MAXF> void launch_face_sums(const cfdb_device_fv* fv, double* source) {
+    k_cell_face_sums<NC, MAXF><<<grid(fv->m.nc), kThreads, 0, fv->st>>>(fv->m, fv->eface, source);
 }
 
 void launch_scalar_corrections(cfdb_device_fv* fv, const double* phi, const double* bv, int scheme,
                                const double* flux, const double* gamma, int linear_upwind, double* source) {
     launch_gradient<1>(fv, phi, bv, scheme, fv->sgrad);
-    k_scalar_corrections<<<grid(fv->m.nc), kThreads, 0, fv->st>>>(fv->m, fv->sgrad, flux, gamma,
-                                                                   linear_upwind != 0 ? 1 : 0, source);
+    if (fv->m.nif > 0)
+        k_scalar_face_terms<<<grid(fv->m.nif), kThreads, 0, fv->st>>>(fv->m, fv->sgrad, flux, gamma,
+                                                                      linear_upwind != 0 ? 1 : 0, fv->eface);
+#define L(F) launch_face_sums<1, F>(fv, source)
+    CFDB_FV_BY_MAXF(fv, L)
+#undef L
     CFDB_CUDA(cudaGetLastError());
 }
 
@@ -424,22 +446,26 @@ void launch_momentum_corrections(cfdb_device_fv* fv, const double* u, const doub
     // the limiter is used only with linear upwind (fv_openmp.cpp:216)
     const int use_lim = limited != 0 && linear_upwind != 0 ? 1 : 0;
     const double e0 = venkat ? eps2[0] : 0.0, e1 = venkat ? eps2[1] : 0.0, e2 = venkat ? eps2[2] : 0.0;
-    if (use_lim) {
-        k_cell_limiter<<<grid(fv->m.nc), kThreads, 0, fv->st>>>(fv->m, u, ub, g, venkat != 0 ? 1 : 0, e0, e1, e2,
-                                                               fv->lim);
-    }
-    k_momentum_corrections<<<grid(fv->m.nc), kThreads, 0, fv->st>>>(
-        fv->m, g, fv->lim, use_lim, flux, nu_face, linear_upwind != 0 ? 1 : 0, central, u,
-        transpose_term != 0 ? 1 : 0, source);
+    const int vk = venkat != 0 ? 1 : 0;
+    if (ub == nullptr) ub = fv->vbv; // no boundary faces: never read, but a valid address
+    if (use_lim)
+        k_cell_limiter<<<grid(fv->m.nc), kThreads, 0, fv->st>>>(fv->m, u, ub, g, vk, e0, e1, e2, fv->lim);
+    if (fv->m.nif > 0)
+        k_momentum_face_terms<<<grid(fv->m.nif), kThreads, 0, fv->st>>>(
+            fv->m, g, fv->lim, use_lim, flux, nu_face, linear_upwind != 0 ? 1 : 0, central, u,
+            transpose_term != 0 ? 1 : 0, fv->eface);
+#define L(F) launch_face_sums<3, F>(fv, source)
+    CFDB_FV_BY_MAXF(fv, L)
+#undef L
     CFDB_CUDA(cudaGetLastError());
 }
 
 void h2d(cfdb_device_fv* fv, double* dst, const double* src, size_t n) {
-    if (n > 0) CFDB_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, fv->st));
+    fv->copier.to_device(dst, src, n * sizeof(double), fv->st);
 }
 
 void d2h(cfdb_device_fv* fv, double* dst, const double* src, size_t n) {
-    if (n > 0) CFDB_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, fv->st));
+    fv->copier.to_host(dst, src, n * sizeof(double), fv->st);
 }
 
 size_t ncells(const cfdb_device_fv* fv) { return static_cast<size_t>(fv->m.nc); }
@@ -526,6 +552,10 @@ int cfdb_device_fv_create(const cfdb_fv_mesh_view* v, cfdb_device_fv** out) {
             fv->coef = fv->mem.alloc<double>(fi);
             fv->src = fv->mem.alloc<double>(3 * c);
             fv->tmp = fv->mem.alloc<double>(9 * c);
+            fv->eface = fv->mem.alloc<double>(3 * fi);
+            int deg = 0;
+            for (int i = 0; i < nc; ++i) deg = std::max(deg, v->cell_offsets[i + 1] - v->cell_offsets[i]);
+            fv->maxf = deg <= 4 ? 4 : deg <= 6 ? 6 : deg <= 8 ? 8 : 0;
             CFDB_CUDA(cudaStreamSynchronize(fv->st));
         } catch (...) {
             delete fv;

@@ -22,21 +22,24 @@
 
 using cfdb::fail;
 
-namespace {
+namespace cfdb {
+void set_thread_error(const std::string& msg); // capi.cu: the message of cfdb_last_error
+} // namespace cfdb
 
-thread_local std::string g_synth_error;
+namespace {
 
 template <class F> int guarded_synth(F&& f) {
     try {
         f();
         return CFDB_OK;
     } catch (const cfdb::Error& e) {
-        g_synth_error = e.what();
+        cfdb::set_thread_error(e.what());
         return e.code;
     } catch (const std::bad_alloc&) {
+        cfdb::set_thread_error("out of host memory");
         return CFDB_ERR_OOM;
     } catch (const std::exception& e) {
-        g_synth_error = e.what();
+        cfdb::set_thread_error(e.what());
         return CFDB_ERR_INTERNAL;
     }
 }

@@ -5,6 +5,7 @@
 //
 //   test_cfd_gpu_api            checks on the GPU
 //   test_cfd_gpu_api --no-device  checks the no-device behaviour (no host fallback)
+#include <cfd_gpu_fv.hpp>
 #include <cfd_gpu_krylov.hpp>
 #include <cfdb.h>
 
@@ -101,12 +102,150 @@ static Box box(int m) {
     return b;
 }
 
+// A row of n unit cubes along x (cell c centred at (c + 0.5, 0.5, 0.5)) as an FvMeshView: the
+// n - 1 internal faces first, then per cell its boundary faces. Least-squares matrices are
+// inverted by cofactors.
+struct FvRow {
+    int n, nif, nf;
+    std::vector<int> own, nei, off, faces;
+    std::vector<double> w, sf, cf, cc, vol, kv, lsq_d, lsq;
+    explicit FvRow(int cells) : n(cells), nif(cells - 1) {
+        for (int c = 0; c + 1 < n; ++c) face(c, c + 1, {1, 0, 0}, {c + 1.0, 0.5, 0.5});
+        for (int c = 0; c < n; ++c) {
+            if (c == 0) face(c, -1, {-1, 0, 0}, {0.0, 0.5, 0.5});
+            if (c == n - 1) face(c, -1, {1, 0, 0}, {double(n), 0.5, 0.5});
+            face(c, -1, {0, -1, 0}, {c + 0.5, 0.0, 0.5});
+            face(c, -1, {0, 1, 0}, {c + 0.5, 1.0, 0.5});
+            face(c, -1, {0, 0, -1}, {c + 0.5, 0.5, 0.0});
+            face(c, -1, {0, 0, 1}, {c + 0.5, 0.5, 1.0});
+        }
+        nf = static_cast<int>(own.size());
+        for (int c = 0; c < n; ++c) {
+            cc.insert(cc.end(), {c + 0.5, 0.5, 0.5});
+            vol.push_back(1.0);
+        }
+        std::vector<std::vector<int>> lists(n);
+        std::vector<double> m(9 * n, 0.0);
+        for (int f = 0; f < nf; ++f) {
+            const int p = own[f];
+            double d[3];
+            for (int i = 0; i < 3; ++i) d[i] = (f < nif ? cc[3 * nei[f] + i] : cf[3 * f + i]) - cc[3 * p + i];
+            const double dd = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            for (int i = 0; i < 3; ++i) {
+                lsq_d.push_back(d[i] / dd);
+                kv.push_back(0.0); // orthogonal: S = d delta
+            }
+            for (int c : {p, f < nif ? nei[f] : -1}) {
+                if (c < 0) continue;
+                lists[c].push_back(f);
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) m[9 * c + 3 * j + i] += d[i] * d[j] / dd;
+            }
+        }
+        off.push_back(0);
+        for (int c = 0; c < n; ++c) {
+            faces.insert(faces.end(), lists[c].begin(), lists[c].end());
+            off.push_back(static_cast<int>(faces.size()));
+            const double* a = &m[9 * c];
+            auto at = [&](int r, int k) { return a[3 * k + r]; };
+            double inv[9];
+            const double det = at(0, 0) * (at(1, 1) * at(2, 2) - at(1, 2) * at(2, 1)) -
+                               at(0, 1) * (at(1, 0) * at(2, 2) - at(1, 2) * at(2, 0)) +
+                               at(0, 2) * (at(1, 0) * at(2, 1) - at(1, 1) * at(2, 0));
+            for (int r = 0; r < 3; ++r)
+                for (int k = 0; k < 3; ++k) {
+                    const int r1 = (k + 1) % 3, r2 = (k + 2) % 3, k1 = (r + 1) % 3, k2 = (r + 2) % 3;
+                    inv[3 * k + r] = (at(r1, k1) * at(r2, k2) - at(r1, k2) * at(r2, k1)) / det;
+                }
+            lsq.insert(lsq.end(), inv, inv + 9);
+        }
+    }
+    void face(int p, int q, std::initializer_list<double> s, std::initializer_list<double> x) {
+        own.push_back(p);
+        if (q >= 0) {
+            nei.push_back(q);
+            w.push_back(0.5);
+        }
+        sf.insert(sf.end(), s);
+        cf.insert(cf.end(), x);
+    }
+    g::FvMeshView view() const {
+        g::FvMeshView v;
+        v.n_cells = n;
+        v.n_internal_faces = nif;
+        v.n_faces = nf;
+        v.owner = own.data();
+        v.neighbour = nei.data();
+        v.cell_offsets = off.data();
+        v.cell_faces = faces.data();
+        v.weight = w.data();
+        v.sf = sf.data();
+        v.face_centre = cf.data();
+        v.cell_centre = cc.data();
+        v.volume = vol.data();
+        v.correction = kv.data();
+        v.lsq_d = lsq_d.data();
+        v.lsq_inverse = lsq.data();
+        return v;
+    }
+};
+
+// DeviceFv (fv_device.hpp): linear fields have exact gradients with every scheme on this
+// orthogonal row; errors are the reference's exception types.
+static void check_device_fv() {
+    const FvRow row(5);
+    g::DeviceFv fv(row.view());
+    CHECK(fv.on_device());
+    const double a[3] = {2.0, 3.0, -1.0};
+    auto lin = [&](const double* x) { return a[0] * x[0] + a[1] * x[1] + a[2] * x[2] + 0.5; };
+    std::vector<double> phi(row.n), bv(row.nf - row.nif), u(3 * row.n), ub(3 * (row.nf - row.nif));
+    for (int c = 0; c < row.n; ++c) {
+        phi[c] = lin(&row.cc[3 * c]);
+        for (int i = 0; i < 3; ++i) u[3 * c + i] = (i + 1) * phi[c];
+    }
+    for (int f = row.nif; f < row.nf; ++f) {
+        bv[f - row.nif] = lin(&row.cf[3 * f]);
+        for (int i = 0; i < 3; ++i) ub[3 * (f - row.nif) + i] = (i + 1) * bv[f - row.nif];
+    }
+    std::vector<double> nu(row.nif, 0.1), flux(row.nif, 1.0);
+    std::vector<double> src(3 * row.n, 0.0);
+    CHECK(throws<std::logic_error>([&] {
+        fv.momentum_corrections(flux.data(), nu.data(), true, false, false, nullptr, 0.0, false, src.data());
+    }));
+    for (int scheme = 0; scheme < 3; ++scheme) {
+        std::vector<double> grad(3 * row.n), vg(9 * row.n);
+        fv.gradient(phi.data(), bv.data(), scheme, grad.data());
+        fv.vector_gradient(u.data(), ub.data(), scheme, vg.data());
+        double err = 0.0;
+        for (int c = 0; c < row.n; ++c)
+            for (int j = 0; j < 3; ++j) {
+                err = std::fmax(err, std::fabs(grad[3 * c + j] - a[j]));
+                for (int i = 0; i < 3; ++i) err = std::fmax(err, std::fabs(vg[9 * c + 3 * i + j] - (i + 1) * a[j]));
+            }
+        CHECK(err < 1e-12);
+    }
+    // uniform flux through orthogonal faces with a linear field: the linear-upwind corrections
+    // telescope to F (phi_f - phi_up) differences; the interior cells receive the same source
+    std::vector<double> s(row.n, 0.0);
+    fv.scalar_corrections(phi.data(), bv.data(), 1, flux.data(), nu.data(), true, s.data());
+    CHECK(std::fabs(s[0] + 1.0) < 1e-12 && std::fabs(s[row.n - 1] - 1.0) < 1e-12);
+    for (int c = 1; c + 1 < row.n; ++c) CHECK(std::fabs(s[c]) < 1e-12);
+    fv.momentum_corrections(flux.data(), nu.data(), true, true, false, nullptr, 0.0, true, src.data());
+    CHECK(std::isfinite(src[0]));
+    CHECK(throws<std::invalid_argument>([&] { fv.gradient(phi.data(), bv.data(), 7, phi.data()); }));
+    g::FvMeshView bad = row.view();
+    bad.n_faces = bad.n_internal_faces - 1;
+    CHECK(throws<std::invalid_argument>([&] { g::DeviceFv x(bad); }));
+}
+
 static void check_no_device() {
     CHECK(g::backend_name() == "cuda");
     CHECK(!g::device_available());
     Csr a = five_point(4);
     std::vector<double> b(a.n, 1.0), x(a.n, 0.0);
     CHECK(throws<std::runtime_error>([&] { g::solve(a.view(), b.data(), x.data(), g::Method::Cg, {}); }));
+    const FvRow row(3);
+    CHECK(throws<std::runtime_error>([&] { g::DeviceFv fv(row.view()); }));
 }
 
 static void check_device() {
@@ -241,7 +380,10 @@ int main(int argc, char** argv) {
     const bool no_device = argc > 1 && std::strcmp(argv[1], "--no-device") == 0;
     try {
         if (no_device) check_no_device();
-        else check_device();
+        else {
+            check_device();
+            check_device_fv();
+        }
     } catch (const std::exception& e) {
         std::fprintf(stderr, "unexpected exception: %s\n", e.what());
         return 2;

@@ -70,6 +70,10 @@ struct cfdb_device_fv {
     int maxf = 0;            // 4, 6 or 8: no cell has more faces (batched face sums); 0: any
     bool have_vector = false;
     StagedCopier copier;     // host-array entry points
+    // FvGeometry's face factors for the scalar equation (cfdb_device_fv_set_face_geometry)
+    double* dc = nullptr;    // n_faces: delta coefficients
+    double* un = nullptr;    // 3 n_faces: unit normals
+    double* area = nullptr;  // n_faces: face areas
     ~cfdb_device_fv() {
         if (st != nullptr) {
             cudaStreamSynchronize(st);
@@ -375,6 +379,150 @@ __global__ void __launch_bounds__(kThreads) k_cell_face_sums(FvMesh m, const dou
     }
 #pragma unroll
     for (int i = 0; i < NC; ++i) source[static_cast<size_t>(c) * NC + i] += s[i];
+}
+
+// ---- the scalar equation of solve_scalar (scalar_transport.cpp:50-176, GPU path) ----------
+
+// std::min / std::max of the reference: (b < a) ? b : a and (a < b) ? b : a (signed zeros kept)
+__device__ __forceinline__ double ref_min(double a, double b) { return b < a ? b : a; }
+__device__ __forceinline__ double ref_max(double a, double b) { return a < b ? b : a; }
+
+// |(x_f - x_P) . n_f| (scalar_transport.cpp:27-28, 133, 140)
+__device__ __forceinline__ double normal_distance(const FvMesh& m, const double* __restrict__ un, int f, int p) {
+    const double d0 = m.cf[3 * f] - m.cc[3 * p];
+    const double d1 = m.cf[3 * f + 1] - m.cc[3 * p + 1];
+    const double d2 = m.cf[3 * f + 2] - m.cc[3 * p + 2];
+    return fabs(d0 * un[3 * f] + d1 * un[3 * f + 1] + d2 * un[3 * f + 2]);
+}
+
+// boundary_values (scalar_transport.cpp:10-40), one thread per boundary face
+__global__ void __launch_bounds__(kThreads) k_scalar_boundary_values(FvMesh m, const double* __restrict__ un,
+                                                                     const int* __restrict__ kind,
+                                                                     const double* __restrict__ value,
+                                                                     const double* __restrict__ coef,
+                                                                     const double* __restrict__ field,
+                                                                     double* __restrict__ bv) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m.nf - m.nif) return;
+    const int f = m.nif + b;
+    const int p = m.own[f];
+    switch (kind[b]) {
+    case CFDB_SCALAR_FIXED_VALUE: bv[b] = value[b]; break;
+    case CFDB_SCALAR_FIXED_GRADIENT: bv[b] = field[p] + value[b] * normal_distance(m, un, f, p); break;
+    case CFDB_SCALAR_MIXED: {
+        const double rd = coef[b] * normal_distance(m, un, f, p);
+        bv[b] = (field[p] + rd * value[b]) / (1.0 + rd);
+        break;
+    }
+    default: bv[b] = field[p]; break; // zero gradient
+    }
+}
+
+// Internal-face coefficients of assemble_convection_diffusion with convection = 1
+// (krylov.hpp:105-116) and the fixed-cell rule (scalar_transport.cpp:162-170).
+__global__ void __launch_bounds__(kThreads) k_scalar_face_coeffs(FvMesh m, const double* __restrict__ flux,
+                                                                 const double* __restrict__ gamma,
+                                                                 const double* __restrict__ dc,
+                                                                 const unsigned char* __restrict__ fixed,
+                                                                 double* __restrict__ upper, double* __restrict__ lower) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nif) return;
+    const double fl = flux[f];
+    const double g = gamma[f] * dc[f];
+    const double pos = fl > 0.0 ? 1.0 * fl : 0.0;
+    const double neg = fl < 0.0 ? 1.0 * fl : 0.0;
+    upper[f] = fixed != nullptr && fixed[m.own[f]] != 0 ? 0.0 : neg - g;
+    lower[f] = fixed != nullptr && fixed[m.nei[f]] != 0 ? 0.0 : -pos - g;
+}
+
+struct ScalarCellTerms {
+    const double* su;
+    const double* sp;
+    const double* old_value;
+    const double* capacity;
+    const unsigned char* fixed;
+    const double* fixed_value;
+    double relaxation;
+    double dt;
+};
+
+// Per cell, in the reference's order: the internal faces' diagonal and divergence
+// (assemble_convection_diffusion), the boundary faces (scalar_transport.cpp:127-148), then the
+// cell terms (:150-161) and fixed cells (:171-177). source holds the explicit face corrections
+// on entry. One thread per cell over its faces in ascending order (internal before boundary).
+__global__ void __launch_bounds__(kThreads) k_scalar_cells(FvMesh m, const double* __restrict__ flux,
+                                                           const double* __restrict__ gamma,
+                                                           const double* __restrict__ dc,
+                                                           const double* __restrict__ un,
+                                                           const double* __restrict__ area,
+                                                           const int* __restrict__ kind,
+                                                           const double* __restrict__ value,
+                                                           const double* __restrict__ coef, ScalarCellTerms t,
+                                                           double* __restrict__ field, double* __restrict__ diag,
+                                                           double* __restrict__ source) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    double d = 0.0, div = 0.0, src = source[c];
+    const int k1 = m.start[c + 1];
+    for (int k = m.start[c]; k < k1; ++k) {
+        const int f = m.faces[k];
+        const double fl = flux[f];
+        if (f < m.nif) {
+            const double g = gamma[f] * dc[f];
+            if (m.own[f] == c) {
+                const double pos = fl > 0.0 ? 1.0 * fl : 0.0;
+                d = d + (pos + g);
+                div = div + fl;
+            } else {
+                const double neg = fl < 0.0 ? 1.0 * fl : 0.0;
+                d = d + (-neg + g);
+                div = div - fl;
+            }
+            continue;
+        }
+        const int b = f - m.nif;
+        div += fl;
+        const int kb = kind[b];
+        if (kb == CFDB_SCALAR_FIXED_VALUE) {
+            const double diff = gamma[f] * dc[f];
+            d += diff + ref_max(fl, 0.0);
+            src += (diff - ref_min(fl, 0.0)) * value[b];
+        } else if (kb == CFDB_SCALAR_MIXED) {
+            const double dn = normal_distance(m, un, f, c);
+            const double rd = coef[b] * dn;
+            const double cm = gamma[f] * dc[f] * rd / (1.0 + rd);
+            d += cm + fl;
+            src += cm * value[b];
+        } else {
+            d += fl;
+            if (kb == CFDB_SCALAR_FIXED_GRADIENT) {
+                const double dn = normal_distance(m, un, f, c);
+                src += gamma[f] * value[b] * area[f] - fl * value[b] * dn;
+            }
+        }
+    }
+    const double vol = m.vol[c];
+    const double phi = field[c];
+    d -= div; // bounded convection form
+    d -= ref_min(t.sp[c], 0.0) * vol;
+    src += t.su[c] * vol + ref_max(t.sp[c], 0.0) * phi * vol;
+    if (t.dt > 0.0) {
+        const double ddt = vol / t.dt * (t.capacity != nullptr ? t.capacity[c] : 1.0);
+        d += ddt;
+        src += ddt * (t.old_value != nullptr ? t.old_value[c] : phi);
+    }
+    if (t.relaxation < 1.0) {
+        const double d1 = d / t.relaxation;
+        src += (d1 - d) * phi;
+        d = d1;
+    }
+    if (t.fixed != nullptr && t.fixed[c] != 0) {
+        d = 1.0;
+        src = t.fixed_value[c];
+        field[c] = t.fixed_value[c];
+    }
+    diag[c] = d;
+    source[c] = src;
 }
 
 template <class F> int guarded(F&& f) {
@@ -706,4 +854,64 @@ int cfdb_device_fv_momentum_corrections_device(cfdb_device_fv* fv, const double*
     });
 }
 
+int cfdb_device_fv_set_face_geometry(cfdb_device_fv* fv, const double* delta_coeffs, const double* unit_normals,
+                                     const double* face_areas) {
+    return guarded([&] {
+        if (fv == nullptr || (fv->m.nf > 0 && (!delta_coeffs || !unit_normals || !face_areas)))
+            fail(CFDB_ERR_BAD_ARG, "DeviceFv: null face geometry");
+        CFDB_CUDA(cudaSetDevice(fv->device));
+        const size_t nf = static_cast<size_t>(fv->m.nf);
+        if (fv->dc == nullptr) {
+            fv->dc = fv->mem.alloc<double>(nf);
+            fv->un = fv->mem.alloc<double>(3 * nf);
+            fv->area = fv->mem.alloc<double>(nf);
+        }
+        if (nf > 0) {
+            CFDB_CUDA(cudaMemcpyAsync(fv->dc, delta_coeffs, sizeof(double) * nf, cudaMemcpyHostToDevice, fv->st));
+            CFDB_CUDA(cudaMemcpyAsync(fv->un, unit_normals, sizeof(double) * 3 * nf, cudaMemcpyHostToDevice, fv->st));
+            CFDB_CUDA(cudaMemcpyAsync(fv->area, face_areas, sizeof(double) * nf, cudaMemcpyHostToDevice, fv->st));
+        }
+        CFDB_CUDA(cudaStreamSynchronize(fv->st));
+    });
+}
+
+int cfdb_device_fv_scalar_system_device(cfdb_device_fv* fv, const cfdb_scalar_equation* eq, const double* face_flux,
+                                        double* field, double* upper, double* lower, double* diag, double* source) {
+    return guarded([&] {
+        if (fv == nullptr || eq == nullptr || face_flux == nullptr || field == nullptr || diag == nullptr ||
+            source == nullptr || eq->gamma_face == nullptr || eq->su == nullptr || eq->sp == nullptr)
+            fail(CFDB_ERR_BAD_ARG, "scalar system: null argument");
+        const FvMesh& m = fv->m;
+        const int nb = m.nf - m.nif;
+        if (m.nif > 0 && (upper == nullptr || lower == nullptr)) fail(CFDB_ERR_BAD_ARG, "scalar system: null upper/lower");
+        if (nb > 0 && (!eq->bc_kind || !eq->bc_value || !eq->bc_coefficient))
+            fail(CFDB_ERR_BAD_ARG, "scalar system: boundary conditions missing");
+        if (eq->fixed_cell != nullptr && eq->fixed_value == nullptr)
+            fail(CFDB_ERR_BAD_ARG, "scalar system: fixed cells without values");
+        if (!(eq->relaxation > 0.0)) fail(CFDB_ERR_BAD_ARG, "scalar system: relaxation must be positive");
+        if (fv->dc == nullptr) fail(CFDB_ERR_NOT_READY, "scalar system: cfdb_device_fv_set_face_geometry first");
+        check_scheme(eq->gradient);
+        CFDB_CUDA(cudaSetDevice(fv->device));
+        // bv = boundary_values(field) (scalar_transport.cpp:80), into the resident buffer
+        if (nb > 0)
+            k_scalar_boundary_values<<<grid(nb), kThreads, 0, fv->st>>>(m, fv->un, eq->bc_kind, eq->bc_value,
+                                                                        eq->bc_coefficient, field, fv->bv);
+        // a.source = 0, then the explicit face corrections (scalar_transport.cpp:81-83)
+        CFDB_CUDA(cudaMemsetAsync(source, 0, sizeof(double) * m.nc, fv->st));
+        launch_scalar_corrections(fv, field, fv->bv, eq->gradient, face_flux, eq->gamma_face, eq->linear_upwind,
+                                  source);
+        if (m.nif > 0)
+            k_scalar_face_coeffs<<<grid(m.nif), kThreads, 0, fv->st>>>(m, face_flux, eq->gamma_face, fv->dc,
+                                                                       eq->fixed_cell, upper, lower);
+        const ScalarCellTerms t{eq->su, eq->sp, eq->old_value, eq->capacity, eq->fixed_cell, eq->fixed_value,
+                                eq->relaxation, eq->dt};
+        k_scalar_cells<<<grid(m.nc), kThreads, 0, fv->st>>>(m, face_flux, eq->gamma_face, fv->dc, fv->un, fv->area,
+                                                            eq->bc_kind, eq->bc_value, eq->bc_coefficient, t, field,
+                                                            diag, source);
+        CFDB_CUDA(cudaGetLastError());
+        CFDB_CUDA(cudaStreamSynchronize(fv->st));
+    });
+}
+
 } // extern "C"
+

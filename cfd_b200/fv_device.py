@@ -50,6 +50,7 @@ _proto("cfdb_device_fv_vector_gradient_device", [_vp, _vp, _vp, _i, _vp])
 _proto("cfdb_device_fv_scalar_corrections_device", [_vp, _vp, _vp, _i, _vp, _vp, _i, _vp])
 _proto("cfdb_device_fv_momentum_corrections_device",
        [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _pd, _d, _i, _vp])
+_proto("cfdb_device_fv_set_face_geometry", [_vp, _pd, _pd, _pd])
 
 
 class MeshView:
@@ -144,8 +145,13 @@ def mesh_view(n_cells, owner, neighbour, face_areas, face_centres, cell_centres,
                             np.bincount(nei, dd[:nif, a, b], minlength=int(n_cells)))
     inv = np.linalg.inv(mat)
     offsets, faces = cell_face_lists(n_cells, own, nei)
-    return MeshView(n_cells, own, nei, offsets, faces, weights, sf, cf, cc, cell_volumes, correction,
+    view = MeshView(n_cells, own, nei, offsets, faces, weights, sf, cf, cc, cell_volumes, correction,
                     q, inv.transpose(0, 2, 1).reshape(-1, 9))
+    # FvGeometry's other face factors (fv_geometry.cpp:36-50), for the scalar equation
+    view.delta_coeffs = delta
+    view.face_areas = area
+    view.unit_normals = sf / area[:, None]
+    return view
 
 
 def mesh_view_of(mesh) -> MeshView:
@@ -255,6 +261,15 @@ class DeviceFv:
             self._h, _devptr(u), _devptr(ub) if ub is not None else None, _devptr(grad), _devptr(flux),
             _devptr(nu_face), 1 if linear_upwind else 0, 1 if limited else 0, 1 if venkat else 0, _dp(e),
             float(central), 1 if transpose_term else 0, _devptr(source)))
+
+    def set_face_geometry(self, delta_coeffs=None, unit_normals=None, face_areas=None) -> None:
+        """FvGeometry's delta coefficients, unit normals and face areas (all faces) for the
+        scalar equation; by default those :func:`mesh_view` computed."""
+        dc = _host_in(self.view.delta_coeffs if delta_coeffs is None else delta_coeffs, self.n_faces, "delta_coeffs")
+        un = _host_in(self.view.unit_normals if unit_normals is None else unit_normals, 3 * self.n_faces,
+                      "unit_normals")
+        ar = _host_in(self.view.face_areas if face_areas is None else face_areas, self.n_faces, "face_areas")
+        _check(_lib.cfdb_device_fv_set_face_geometry(self._h, _dp(dc), _dp(un), _dp(ar)))
 
     def close(self):
         h = getattr(self, "_h", None)

@@ -491,6 +491,43 @@ int cfdb_device_fv_momentum_corrections_device(cfdb_device_fv* fv, const double*
                                                const double* eps2, double central,
                                                int transpose_term, double* source);
 
+/* ---- the scalar transport equation on the device: solve_scalar's GPU path
+ * (scalar_transport.cpp:50-176) up to a.solve, which is cfdb_system_solve_ldu ---- */
+typedef enum { /* scalar_transport.hpp:14 ScalarBoundary::Kind */
+    CFDB_SCALAR_FIXED_VALUE = 0,
+    CFDB_SCALAR_ZERO_GRADIENT = 1,
+    CFDB_SCALAR_FIXED_GRADIENT = 2,
+    CFDB_SCALAR_MIXED = 3
+} cfdb_scalar_bc_kind;
+/* ScalarEquation (scalar_transport.hpp:24-37); every array on the device. */
+typedef struct {
+    const double* gamma_face;          /* n_faces: diffusivity */
+    const double* su;                  /* n_cells: explicit source per unit volume */
+    const double* sp;                  /* n_cells: implicit source coefficient */
+    const int* bc_kind;                /* n_boundary: cfdb_scalar_bc_kind */
+    const double* bc_value;            /* n_boundary */
+    const double* bc_coefficient;      /* n_boundary: Mixed h / gamma */
+    const unsigned char* fixed_cell;   /* optional n_cells: 1 = value fixed */
+    const double* fixed_value;         /* with fixed_cell */
+    double relaxation;                 /* implicit under-relaxation (1: none) */
+    double dt;                         /* > 0: implicit Euler with old_value (else the field) */
+    const double* old_value;           /* optional */
+    const double* capacity;            /* optional factor of the time term */
+    int linear_upwind;
+    int gradient;                      /* cfdb_gradient_scheme of the explicit corrections */
+} cfdb_scalar_equation;
+/* FvGeometry's delta coefficients (n_faces), unit normals (3 n_faces) and face areas (n_faces)
+ * (fv_geometry.cpp:33-50), host arrays copied to the device, for the scalar equation. */
+int cfdb_device_fv_set_face_geometry(cfdb_device_fv* fv, const double* delta_coeffs,
+                                     const double* unit_normals, const double* face_areas);
+/* The LDU system of solve_scalar on device arrays: boundary values of field, the explicit
+ * face corrections, the convection-diffusion coefficients (convection 1), boundary-face terms,
+ * sources, time term, under-relaxation and fixed cells (field takes the fixed values). upper /
+ * lower: internal faces; diag, source: cells. Bit-identical to the face-by-face host loops. */
+int cfdb_device_fv_scalar_system_device(cfdb_device_fv* fv, const cfdb_scalar_equation* eq,
+                                        const double* face_flux, double* field, double* upper,
+                                        double* lower, double* diag, double* source);
+
 #ifdef __cplusplus
 }
 #endif

@@ -150,3 +150,34 @@ def test_product_mesh_view_matches_the_oracle(case):
     assert np.array_equal(pv.cell_offsets, v.start) and np.array_equal(pv.cell_faces, v.faces)
     for a, b in ((pv.correction, v.kv), (pv.lsq_d, v.lsq_d), (pv.lsq_inverse, v.lsq)):
         assert np.allclose(a, b, rtol=1e-12, atol=1e-12 * np.abs(b).max())
+
+
+def test_scalar_restatement_conserves_and_holds_constants():
+    """oracle/scalar.py (the restatement of solve_scalar's assembly): with no flux and
+    zero-gradient walls the rows sum to zero; with fixed-value walls at c and no sources the
+    constant field c satisfies A c = b exactly up to rounding."""
+    import oracle.scalar as OS
+    mesh = _skewed_tet(4, 3, 3)
+    mesh.weights = mesh.fv_geometry()[1]
+    v = F.view_of(mesh)
+    nb = v.nf - v.nif
+    area = np.sqrt((v.sf ** 2).sum(axis=1))
+    un = v.sf / area[:, None]
+    d = np.concatenate([v.cc[v.nei] - v.cc[v.own[: v.nif]], v.cf[v.nif:] - v.cc[v.own[v.nif:]]])
+    dc = area * area / np.maximum((v.sf * d).sum(axis=1), 0.05 * area * np.sqrt((d * d).sum(axis=1)))
+    eq = {"gamma_face": np.full(v.nf, 0.1), "su": np.zeros(v.nc), "sp": np.zeros(v.nc),
+          "bc_kind": np.full(nb, OS.ZERO_GRADIENT, np.int32), "bc_value": np.zeros(nb),
+          "bc_coefficient": np.zeros(nb), "linear_upwind": False, "gradient": 0}
+    field = np.zeros(v.nc)
+    up, lo, dg, src, _ = OS.scalar_system(v, dc, un, area, eq, np.zeros(v.nf), field)
+    rows = dg.copy()
+    np.add.at(rows, v.own[: v.nif], up)
+    np.add.at(rows, v.nei, lo)
+    assert np.abs(rows).max() < 1e-12 * np.abs(dg).max()
+    eq["bc_kind"] = np.full(nb, OS.FIXED_VALUE, np.int32)
+    eq["bc_value"] = np.full(nb, 2.5)
+    up, lo, dg, src, _ = OS.scalar_system(v, dc, un, area, eq, np.zeros(v.nf), np.full(v.nc, 2.5))
+    ax = 2.5 * dg
+    np.add.at(ax, v.own[: v.nif], 2.5 * up)
+    np.add.at(ax, v.nei, 2.5 * lo)
+    assert np.allclose(ax, src, rtol=0, atol=1e-12 * np.abs(src).max())

@@ -12,6 +12,8 @@ plain FP64 path is reported beside it. Inputs are resident in HBM and larger tha
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config graded|tet|cavity]
   python bench.py --config batch    # 256 uneven boxes in one device plan, autotuned
   python bench.py --config serve    # serving loop, Poisson arrivals, p50/p99
+  python bench.py --config fv       # DeviceFv kernels of the momentum predictor, 5.14M-cell tet box
+  python bench.py --config step     # the whole pressure-correction step on the device, tet box
 
 Multi-GPU: the path does not shard (one pressure system per GPU); N ranks run independent
 replicas (weak scaling, no collective on the data path); value = total solves/s, time = max
@@ -41,7 +43,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="graded", choices=["graded", "tet", "cavity", "batch", "serve", "fv"])
+    ap.add_argument("--config", default="graded", choices=["graded", "tet", "cavity", "batch", "serve", "fv", "step"])
     ap.add_argument("--systems", type=int, default=256, help="batch: number of systems")
     ap.add_argument("--tune-cache", default=None, help="batch: autotuner cache file")
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serve: arrival rates (1/s)")
@@ -908,6 +910,85 @@ def run_fv_reference(args):
 
 
 
+# ------------------------------------------------------------------------------------------
+# the whole pressure-correction step on the device (FlowSolver::pressure_correction)
+# ------------------------------------------------------------------------------------------
+
+STEP_METRIC = ("pressure-correction steps/s on the device (HbyA/rAU, face flux, pressure matrix, 1 "
+               "non-orthogonal corrector, persistent AMG-CG with the AmgCache rule, flux, relaxation, "
+               "velocity correction)")
+
+
+def run_step(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import cfd_b200 as cb
+    from cfd_b200 import pressure as P
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    size = args.size or 95
+    m = cb.Mesh.tet(size, size, size, jitter=0.2, seed=7)
+    n, ni = m.n_cells, m.n_internal_faces
+    fc_b = m.face_centres[ni:]
+    kinds = np.full(m.n_faces - ni, int(cb.BoundaryKind.Wall), np.int32)
+    kinds[np.isclose(fc_b[:, 0], 0.0)] = int(cb.BoundaryKind.VelocityInlet)
+    kinds[np.isclose(fc_b[:, 0], 1.0)] = int(cb.BoundaryKind.PressureOutlet)
+    kinds[np.isclose(fc_b[:, 2], 0.0)] = int(cb.BoundaryKind.Symmetry)
+    ufix = np.zeros((m.n_faces - ni, 3))
+    ufix[kinds == int(cb.BoundaryKind.VelocityInlet)] = [1.0, 0.0, 0.0]
+    rng = np.random.default_rng(17)
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)  # noqa: E731
+    mom = [T(rng.uniform(2.0, 4.0, (n, 3))), T(-rng.uniform(0.1, 0.5, ni)), T(-rng.uniform(0.1, 0.5, ni)),
+           T(rng.standard_normal((n, 3)))]
+    u, p = T(rng.standard_normal((n, 3))), T(np.zeros(n))
+    u_prev, phi_prev = u.clone(), T(rng.standard_normal(m.n_faces))
+    phi = torch.zeros(m.n_faces, dtype=torch.float64, device=dev)
+    ds = cb.DeviceSolver(mesh=(n, m.owner[:ni], m.neighbour))
+    ds.set_precision(cb.Precision.MIXED)
+    fv = cb.FvGeometry(m, kinds, np.zeros(m.n_faces - ni))
+    s = P.PressureSettings(alpha_u=0.7, alpha_p=0.3, n_non_orth_correctors=1, ref_cell=-1,
+                           p_solver=cb.LduSettings(tolerance=1e-8, rel_tolerance=0.01, max_iterations=1000,
+                                                   max_age=20),
+                           amg=cb.AmgSettings(strength_threshold=THETA))
+    fix = T(ufix)
+
+    def step():
+        P.pressure_correction(ds, fv, *mom, u, p, fix, s, u_prev=u_prev, phi_prev=phi_prev, phi=phi)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    times = []
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        step()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
+    ms = sum(times) / len(times)
+    line = {
+        "metric": STEP_METRIC, "value": 1e3 / ms, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 outer, f32 V-cycle", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"tet{size}^3 jittered 6-tet box", "cells": n, "internal_faces": ni,
+                   "step": "cfd_b200.pressure.pressure_correction, 1 non-orthogonal corrector, Majumdar term, "
+                           "p solver tolerance 1e-8 / rel 0.01, hierarchy rebuilt on the device every 20 CG solves",
+                   "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+        "ms_min": min(times), "ms_median": sorted(times)[len(times) // 2], "ms_max": max(times),
+        "cpu_baseline": None,
+        "cpu_baseline_note": "the reference's FlowSolver needs Eigen and is not built here",
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+
+
+
 def main():
     args = parse()
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
@@ -920,6 +1001,10 @@ def main():
             return
         if args.config == "fv":
             run_fv_reference(args)
+            return
+        if args.config == "step":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference's FlowSolver (pressure_correction) "
+                              "needs Eigen and the fv library, which are not built here"}))
             return
         if args.config in ("batch", "serve"):
             print(json.dumps({"impl": "reference", "unavailable": "the reference solves one system at a "
@@ -940,6 +1025,8 @@ def main():
         run_serve(args, rank, world, local_rank)
     elif args.config == "fv":
         run_fv(args, rank, world, local_rank)
+    elif args.config == "step":
+        run_step(args, rank, world, local_rank)
     else:
         run_case(args, rank, world, local_rank, size)
     if world > 1:

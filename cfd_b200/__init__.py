@@ -18,7 +18,9 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
+import functools
 import os
+import sys
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -263,6 +265,25 @@ def _out_f64(a, name):
     return a
 
 
+def _torch_ready() -> None:
+    """The library's kernels run on its own CUDA streams. Before a call that reads or writes
+    CUDA tensors, the work already queued on torch's current stream (tensor creation, zero
+    fills, copies) must be finished, or the two could overlap on the same buffers."""
+    torch = sys.modules.get("torch")
+    if torch is not None and torch.cuda.is_initialized():
+        torch.cuda.current_stream().synchronize()
+
+
+def _stream_ordered(fn):
+    """Decorator for the device-array entry points: torch's queued work first (_torch_ready);
+    the library call itself returns when its own kernels are done."""
+    @functools.wraps(fn)
+    def call(*args, **kwargs):
+        _torch_ready()
+        return fn(*args, **kwargs)
+    return call
+
+
 def _devptr(t):
     """Device pointer of a torch CUDA tensor / object with data_ptr(), or a raw int."""
     if isinstance(t, int):
@@ -433,6 +454,7 @@ def assemble_convection_diffusion(n_cells, n_faces, owner, neighbour, flux, gamm
                               _dp(diag), _dp(divergence)))
 
 
+@_stream_ordered
 def assemble_convection_diffusion_device(n_cells, n_faces, owner, neighbour, flux, gamma,
                                          delta_coeff, convection, upper, lower, diag,
                                          divergence) -> None:
@@ -464,6 +486,7 @@ def solve_amg_cg(amg: AmgView, b, x, control: SolveControl) -> SolveStats:
     return SolveStats._from(st)
 
 
+@_stream_ordered
 def solve_device_noalloc(n, nnz, row_ptr, col, val, b, x, method: Method,
                          control: SolveControl) -> SolveStats:
     """Jacobi-preconditioned CG that allocates no device memory: every array is the caller's
@@ -706,6 +729,7 @@ class DeviceSolver:
                                       C.byref(st)))
         return SolveStats._from(st)
 
+    @_stream_ordered
     def solve_device(self, diag, upper, lower, b, x, method: Method = Method.Cg,
                      use_amg: bool = True, control: SolveControl | None = None) -> SolveStats:
         """All arrays device-resident (torch CUDA float64 tensors or raw pointers)."""
@@ -742,6 +766,7 @@ class DeviceSolver:
                                               C.byref(r)))
         return LduResult(r.initial_residual, r.final_residual, r.iterations, bool(r.amg_rebuilt))
 
+    @_stream_ordered
     def assemble_device(self, flux, gamma, delta, convection, upper, lower, diag, div) -> None:
         _check(_lib.cfdb_system_assemble_device(self._h, _devptr(flux), _devptr(gamma),
                                                 _devptr(delta), float(convection),
@@ -764,6 +789,7 @@ class DeviceSolver:
                                          float(convection), _dp(upper), _dp(lower), _dp(diag),
                                          _dp(div)))
 
+    @_stream_ordered
     def assemble_pressure_device(self, flux, gamma, delta, source0, upper, lower, diag, source,
                                  diag0=None, ref_cell=0, ref_value=0.0) -> None:
         """Pressure-equation assembly on device arrays (flow_solver.cpp:757-796)."""
@@ -772,6 +798,7 @@ class DeviceSolver:
             _devptr(diag0) if diag0 is not None else None, _devptr(source0), int(ref_cell),
             float(ref_value), _devptr(upper), _devptr(lower), _devptr(diag), _devptr(source)))
 
+    @_stream_ordered
     def correct_pressure_device(self, flux, gamma, delta, p_new, phi, p, p_prev=None, alpha=1.0,
                                 non_orth=None) -> None:
         """Conservative face flux phi and under-relaxed pressure p after the pressure solve
@@ -883,6 +910,7 @@ class Batch:
         ts = t._c()
         _check(_lib.cfdb_batch_set_tuning(self._h, C.byref(ts)))
 
+    @_stream_ordered
     def assemble_pressure_device(self, flux, gamma, delta, source0, upper, lower, diag, source,
                                  ref_cells=None, ref_value=0.0) -> None:
         refs = _i32(ref_cells if ref_cells is not None else np.zeros(self.n_systems))
@@ -890,6 +918,7 @@ class Batch:
             self._h, _devptr(flux), _devptr(gamma), _devptr(delta), _devptr(source0), _ip(refs),
             float(ref_value), _devptr(upper), _devptr(lower), _devptr(diag), _devptr(source)))
 
+    @_stream_ordered
     def solve_device(self, diag, upper, lower, rhs, x, controls, use_amg=True):
         ctl = (ControlStruct * self.n_systems)(*[c._c() for c in controls])
         st = (StatsStruct * self.n_systems)()
@@ -1028,10 +1057,12 @@ class FvGeometry:
                                    C.byref(h)))
         self._h = h
 
+    @_stream_ordered
     def pressure_gradient_device(self, p, grad) -> None:
         """grad (n_cells x 3, CUDA float64) of the cell pressure p (CUDA float64)."""
         _check(_lib.cfdb_fv_pressure_gradient_device(self._h, _devptr(p), _devptr(grad)))
 
+    @_stream_ordered
     def correct_velocity_device(self, hbya, rau, grad, u) -> None:
         _check(_lib.cfdb_fv_correct_velocity_device(self._h, _devptr(hbya), _devptr(rau),
                                                     _devptr(grad), _devptr(u)))
@@ -1042,11 +1073,13 @@ class FvGeometry:
         _check(_lib.cfdb_fv_delta_device(self._h, C.byref(d)))
         return int(d.value)
 
+    @_stream_ordered
     def hbya_rau_device(self, mom_diag, mom_upper, mom_lower, mom_source, u, hbya, rau) -> None:
         _check(_lib.cfdb_fv_hbya_rau_device(self._h, _devptr(mom_diag), _devptr(mom_upper),
                                             _devptr(mom_lower), _devptr(mom_source), _devptr(u),
                                             _devptr(hbya), _devptr(rau)))
 
+    @_stream_ordered
     def face_flux_device(self, hbya, rau, fixed_velocity, phi_hbya, rau_f, u_prev=None,
                          phi_prev=None, beta=0.0) -> None:
         _check(_lib.cfdb_fv_face_flux_device(
@@ -1055,20 +1088,24 @@ class FvGeometry:
             _devptr(phi_prev) if phi_prev is not None else None, float(beta), _devptr(phi_hbya),
             _devptr(rau_f)))
 
+    @_stream_ordered
     def pressure_boundary_device(self, phi_hbya, rau_f, diag, source, ref_cell=-1, ref_value=0.0):
         _check(_lib.cfdb_fv_pressure_boundary_device(self._h, _devptr(phi_hbya), _devptr(rau_f),
                                                      int(ref_cell), float(ref_value), _devptr(diag),
                                                      _devptr(source)))
 
+    @_stream_ordered
     def non_orth_device(self, grad, rau_f, base_source, non_orth, source) -> None:
         _check(_lib.cfdb_fv_non_orth_device(self._h, _devptr(grad), _devptr(rau_f),
                                             _devptr(base_source), _devptr(non_orth), _devptr(source)))
 
+    @_stream_ordered
     def correct_flux_device(self, phi_hbya, rau_f, p_new, phi, non_orth=None) -> None:
         _check(_lib.cfdb_fv_correct_flux_device(
             self._h, _devptr(phi_hbya), _devptr(rau_f),
             _devptr(non_orth) if non_orth is not None else None, _devptr(p_new), _devptr(phi)))
 
+    @_stream_ordered
     def relax_device(self, p_prev, p_new, alpha, p) -> None:
         _check(_lib.cfdb_fv_relax_device(self._h, _devptr(p_prev), _devptr(p_new), float(alpha),
                                          _devptr(p)))

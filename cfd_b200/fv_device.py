@@ -16,7 +16,7 @@ import enum
 
 import numpy as np
 
-from . import (InvalidArgument, _check, _devptr, _dp, _f64, _i32, _ip, _lib, _proto)
+from . import (InvalidArgument, _check, _devptr, _dp, _f64, _i32, _ip, _lib, _proto, _stream_ordered)
 
 _i, _d, _vp, _sz = C.c_int, C.c_double, C.c_void_p, C.c_size_t
 _pi, _pd = C.POINTER(C.c_int), C.POINTER(C.c_double)
@@ -241,19 +241,23 @@ class DeviceFv:
         return a
 
     # -- device arrays (CUDA tensors, no copies) ----------------------------------------------
+    @_stream_ordered
     def gradient_device(self, phi, bv, scheme, grad) -> None:
         _check(_lib.cfdb_device_fv_gradient_device(self._h, _devptr(phi), _devptr(bv) if bv is not None else None,
                                                    int(scheme), _devptr(grad)))
 
+    @_stream_ordered
     def vector_gradient_device(self, u, ub, scheme, grad) -> None:
         _check(_lib.cfdb_device_fv_vector_gradient_device(
             self._h, _devptr(u), _devptr(ub) if ub is not None else None, int(scheme), _devptr(grad)))
 
+    @_stream_ordered
     def scalar_corrections_device(self, phi, bv, scheme, flux, gamma, linear_upwind, source) -> None:
         _check(_lib.cfdb_device_fv_scalar_corrections_device(
             self._h, _devptr(phi), _devptr(bv) if bv is not None else None, int(scheme), _devptr(flux),
             _devptr(gamma), 1 if linear_upwind else 0, _devptr(source)))
 
+    @_stream_ordered
     def momentum_corrections_device(self, u, ub, grad, flux, nu_face, linear_upwind, limited, venkat,
                                     eps2, central, transpose_term, source) -> None:
         e = _f64(eps2 if eps2 is not None else np.zeros(3))

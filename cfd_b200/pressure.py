@@ -39,9 +39,10 @@ def pressure_correction(ds: DeviceSolver, fv: FvGeometry, mom_diag, mom_upper, m
     dev, f64 = p.device, torch.float64
     z = lambda *shape: torch.zeros(*shape, dtype=f64, device=dev)  # noqa: E731
     torch.cuda.current_stream().synchronize()
-    hbya, rau = z(n, 3), z(n)
+    e = lambda *shape: torch.empty(*shape, dtype=f64, device=dev)  # noqa: E731  (fully written)
+    hbya, rau = e(n, 3), e(n)
     fv.hbya_rau_device(mom_diag, mom_upper, mom_lower, mom_source, u, hbya, rau)
-    phi_hbya, rau_f = z(nf), z(nf)
+    phi_hbya, rau_f = e(nf), e(nf)
     majumdar = u_prev is not None and phi_prev is not None and s.alpha_u < 1.0
     fv.face_flux_device(hbya, rau, fixed_velocity, phi_hbya, rau_f,
                         u_prev if majumdar else None, phi_prev if majumdar else None,

@@ -15,7 +15,7 @@ import ctypes as C
 import enum
 from dataclasses import dataclass
 
-from . import InvalidArgument, LduResult, LduSettings, _check, _devptr, _lib, _proto
+from . import InvalidArgument, LduResult, LduSettings, _check, _devptr, _lib, _proto, _stream_ordered
 from .fv_device import DeviceFv
 
 
@@ -68,6 +68,7 @@ class ScalarEquation:
                                     int(self.gradient))
 
 
+@_stream_ordered
 def scalar_system_device(fv: DeviceFv, eq: ScalarEquation, face_flux, field, upper, lower, diag,
                          source) -> None:
     """The LDU system of solve_scalar into device arrays (field takes fixed values)."""

@@ -56,3 +56,21 @@ def test_argument_errors_before_device_work(cb):
         cb.assemble_convection_diffusion(4, 3, [0, 1, 2], [1, 2, 3], np.zeros(3), np.ones(3),
                                          np.ones(3), 0.0, [0.0] * 3, np.zeros(3), np.zeros(4),
                                          np.zeros(4))
+
+
+def test_device_array_wrappers_wait_for_torch_first(cb):
+    """The library's kernels run on its own streams, so every Python entry point that takes CUDA
+    tensors first drains torch's current stream (zero fills and copies queued there must not
+    land on a buffer the library is writing)."""
+    from cfd_b200 import fv_device, scalar
+    owners = [cb.DeviceSolver, cb.Batch, cb.FvGeometry, fv_device.DeviceFv]
+    getters = {"delta_device", "device_bytes", "on_device"}
+    checked = []
+    for cls in owners:
+        for name, fn in vars(cls).items():
+            if name.endswith("_device") and name not in getters and callable(fn):
+                assert hasattr(fn, "__wrapped__"), f"{cls.__name__}.{name} is not stream-ordered"
+                checked.append(name)
+    for fn in (cb.assemble_convection_diffusion_device, cb.solve_device_noalloc, scalar.scalar_system_device):
+        assert hasattr(fn, "__wrapped__"), fn.__name__
+    assert len(checked) >= 18

@@ -825,6 +825,25 @@ def run_fv(args, rank, world, local_rank):
         b = fv_bytes(name, pv)
         per[name] = {"us": t * 1e3, "algorithmic_bytes": b, "gbs": b / 1e9 / (t / 1e3),
                      "frac": b / 1e9 / (t / 1e3) / peak, "traffic": traffic_for(f"fv_{name}")}
+    # the scalar transport system of solve_scalar (Gauss corrections, linear upwind, every
+    # boundary-condition kind, sources, time term, under-relaxation) in one device call
+    from cfd_b200 import scalar as S
+    fv.set_face_geometry()
+    rng = np.random.default_rng(11)
+    nf = pv.n_faces
+    eq = S.ScalarEquation(gamma_face=T(0.01 + 0.05 * rng.random(nf)), su=T(rng.standard_normal(nc)),
+                          sp=T(-rng.random(nc)), bc_kind=torch.as_tensor((np.arange(nb) % 4).astype(np.int32),
+                                                                       device=dev),
+                          bc_value=T(rng.standard_normal(nb)), bc_coefficient=T(0.5 + rng.random(nb)),
+                          relaxation=0.8, dt=0.05, old_value=T(rng.standard_normal(nc)), linear_upwind=True,
+                          gradient=0)
+    sflux, sfield = T(0.1 * rng.standard_normal(nf)), T(rng.standard_normal(nc))
+    s_up, s_lo = torch.empty(nif, dtype=torch.float64, device=dev), torch.empty(nif, dtype=torch.float64, device=dev)
+    s_dg, s_src = torch.empty(nc, dtype=torch.float64, device=dev), torch.empty(nc, dtype=torch.float64, device=dev)
+    t_sc = timed(lambda: S.scalar_system_device(fv, eq, sflux, sfield, s_up, s_lo, s_dg, s_src), reps) / reps
+    scalar_system = {"us": t_sc * 1e3, "cells_per_s": nc / (t_sc / 1e3),
+                     "step": "boundary values, Gauss gradient, linear-upwind + non-orthogonal face fluxes, "
+                             "convection-diffusion coefficients, boundary terms, sources, time term, relaxation"}
     top = max(per, key=lambda k: per[k]["us"])
     roofline = {"bound": "hbm", "kernel": top, "achieved": per[top]["gbs"], "peak": peak, "unit": "GB/s",
                 "frac": per[top]["frac"], "peak_source": peak_kind, "traffic": per[top]["traffic"]}
@@ -860,7 +879,8 @@ def run_fv(args, rank, world, local_rank):
                    "boundary_faces": nb, "step": "vector_gradient(LSQ) + momentum_corrections(limited LU, "
                    "Venkatakrishnan, transpose) + gradient(LSQ) on device arrays",
                    "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
-        "kernels": per, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
+        "kernels": per, "scalar_system": scalar_system, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
+        "clocks": clocks,
         "gpu_launches": 4 * args.steps, "device_bytes": fv.device_bytes(),
     }
     if rank == 0:

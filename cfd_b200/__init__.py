@@ -961,6 +961,13 @@ def positions_two_sided(n: int, ratio: float) -> np.ndarray:
     return out
 
 
+def _view_copy(ptr, shape, dtype):
+    """Copy of a library-owned array; an empty array may come back as a null pointer."""
+    if int(np.prod(shape)) == 0:
+        return np.zeros(shape, dtype)
+    return np.ctypeslib.as_array(ptr, shape).copy()
+
+
 class Mesh:
     """Box (hex) or jittered 6-tet mesh in the reference's face ordering, with geometry."""
 
@@ -973,23 +980,23 @@ class Mesh:
             nc.value, nf.value, ni.value, npn.value)
         o, n = _pi(), _pi()
         _check(_lib.cfdb_mesh_addressing(h, C.byref(o), C.byref(n)))
-        self.owner = np.ctypeslib.as_array(o, (self.n_faces,)).copy()
-        self.neighbour = np.ctypeslib.as_array(n, (self.n_internal_faces,)).copy()
+        self.owner = _view_copy(o, (self.n_faces,), np.int32)
+        self.neighbour = _view_copy(n, (self.n_internal_faces,), np.int32)
         pts, fc, sf, cc, vol = _pd(), _pd(), _pd(), _pd(), _pd()
         _check(_lib.cfdb_mesh_geometry(h, C.byref(pts), C.byref(fc), C.byref(sf), C.byref(cc),
                                        C.byref(vol)))
-        self.points = np.ctypeslib.as_array(pts, (self.n_points, 3)).copy()
-        self.face_centres = np.ctypeslib.as_array(fc, (self.n_faces, 3)).copy()
-        self.face_areas = np.ctypeslib.as_array(sf, (self.n_faces, 3)).copy()
-        self.cell_centres = np.ctypeslib.as_array(cc, (self.n_cells, 3)).copy()
-        self.cell_volumes = np.ctypeslib.as_array(vol, (self.n_cells,)).copy()
+        self.points = _view_copy(pts, (self.n_points, 3), np.float64)
+        self.face_centres = _view_copy(fc, (self.n_faces, 3), np.float64)
+        self.face_areas = _view_copy(sf, (self.n_faces, 3), np.float64)
+        self.cell_centres = _view_copy(cc, (self.n_cells, 3), np.float64)
+        self.cell_volumes = _view_copy(vol, (self.n_cells,), np.float64)
         dl, w = _pd(), _pd()
         _check(_lib.cfdb_mesh_fv(h, C.byref(dl), C.byref(w)))
-        self.delta = np.ctypeslib.as_array(dl, (self.n_internal_faces,)).copy()
-        self.weights = np.ctypeslib.as_array(w, (self.n_internal_faces,)).copy()
+        self.delta = _view_copy(dl, (self.n_internal_faces,), np.float64)
+        self.weights = _view_copy(w, (self.n_internal_faces,), np.float64)
         fo, fn = _pi(), _pi()
         _check(_lib.cfdb_mesh_faces(h, C.byref(fo), C.byref(fn)))
-        self.face_offsets = np.ctypeslib.as_array(fo, (self.n_faces + 1,)).copy()
+        self.face_offsets = _view_copy(fo, (self.n_faces + 1,), np.int32)
         self.face_nodes = np.ctypeslib.as_array(fn, (int(self.face_offsets[-1]),)).copy()
 
     @staticmethod

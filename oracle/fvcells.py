@@ -353,3 +353,32 @@ class RefFv:
             self.h = None
 
     __del__ = close
+
+
+def random_view(n_cells: int, n_internal: int, n_boundary: int, seed: int = 0) -> FvView:
+    """A consistent FvMeshView with random addressing and data (no geometry behind it): cells
+    with anything from no faces to many, to exercise ragged face counts. Internal faces are
+    ordered by (owner, neighbour) with owner < neighbour, boundary faces follow."""
+    rng = np.random.default_rng(seed)
+    pairs = set()
+    inner = max(2, (4 * n_cells) // 5)  # the last fifth of the cells get no internal faces
+    while len(pairs) < n_internal:
+        a, b = rng.integers(0, inner, 2)
+        if a != b:
+            pairs.add((min(a, b), max(a, b)))
+    pairs = sorted(pairs)
+    own = np.array([p[0] for p in pairs] + list(rng.integers(0, n_cells, n_boundary)), np.int32)
+    nei = np.array([p[1] for p in pairs], np.int32)
+    nf = len(own)
+    lists = [[] for _ in range(n_cells)]
+    for f in range(nf):
+        lists[own[f]].append(f)
+        if f < n_internal:
+            lists[nei[f]].append(f)
+    start = np.zeros(n_cells + 1, np.int32)
+    start[1:] = np.cumsum([len(x) for x in lists])
+    faces = np.array([f for x in lists for f in sorted(x)], np.int32)
+    return FvView(n_cells, own, nei, start, faces, rng.uniform(0.05, 0.95, n_internal),
+                  rng.standard_normal((nf, 3)), rng.standard_normal((nf, 3)), rng.standard_normal((n_cells, 3)),
+                  rng.uniform(0.5, 2.0, n_cells), rng.standard_normal((nf, 3)), rng.standard_normal((nf, 3)),
+                  rng.standard_normal((n_cells, 9)))

@@ -181,3 +181,30 @@ def test_scalar_restatement_conserves_and_holds_constants():
     np.add.at(ax, v.own[: v.nif], 2.5 * up)
     np.add.at(ax, v.nei, 2.5 * lo)
     assert np.allclose(ax, src, rtol=0, atol=1e-12 * np.abs(src).max())
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_ragged_random_view_bit_identical_to_reference(seed):
+    """Random addressing: cells with no faces, only boundary faces, or up to ~20 faces."""
+    v = F.random_view(150, 700, 120, seed)
+    deg = np.diff(v.start)
+    assert deg.min() <= 3 and deg.max() > 8
+    if F._ref_lib() is None:
+        pytest.skip("reference not built")
+    ref = F.RefFv(v)
+    rng = np.random.default_rng(seed)
+    phi, bv = rng.standard_normal(v.nc), rng.standard_normal(v.nf - v.nif)
+    u, ub = rng.standard_normal((v.nc, 3)), rng.standard_normal((v.nf - v.nif, 3))
+    flux, gamma, nu = rng.standard_normal(v.nf), rng.random(v.nf), rng.random(v.nif)
+    for scheme in (0, 1, 2):
+        assert np.array_equal(F.gradient(v, phi, bv, scheme), ref.gradient(phi, bv, scheme))
+        g = ref.vector_gradient(u, ub, scheme)
+        assert np.array_equal(F.vector_gradient(v, u, ub, scheme), g)
+        src = np.full(v.nc, 0.5)
+        assert np.array_equal(F.scalar_corrections(v, phi, bv, scheme, flux, gamma, True, src),
+                              ref.scalar_corrections(phi, bv, scheme, flux, gamma, True, src))
+        for venkat in (0, 1):
+            m0 = np.full((v.nc, 3), 0.25)
+            assert np.array_equal(F.momentum_corrections(v, u, ub, g, flux[: v.nif], nu, 1, 1, venkat, (1e-3,) * 3,
+                                                         0.75, 1, m0),
+                                  ref.momentum_corrections(flux[: v.nif], nu, 1, 1, venkat, (1e-3,) * 3, 0.75, 1, m0))

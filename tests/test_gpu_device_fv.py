@@ -160,3 +160,50 @@ def test_errors_follow_the_reference(gpu):
                       pv.face_centre, pv.cell_centre, pv.volume, pv.correction, pv.lsq_d, pv.lsq_inverse)
     with pytest.raises(gpu.InvalidArgument):  # fv_device.cpp:25-27
         D.DeviceFv(bad2)
+
+
+@pytest.mark.parametrize("sizes,seed", [((150, 700, 120), 0), ((300, 350, 100), 0), ((400, 380, 120), 1)])
+def test_ragged_views_bit_identical(gpu, sizes, seed):
+    """Random addressing with cells of 0 to ~20 faces: the face sums take their generic loop
+    (more than 8 faces) or the 8-face batch, and every call still equals the oracle."""
+    from cfd_b200 import fv_device as D
+    v = F.random_view(*sizes, seed)
+    pv = D.MeshView(v.nc, v.own, v.nei, v.start, v.faces, v.w, v.sf, v.cf, v.cc, v.vol, v.kv, v.lsq_d, v.lsq)
+    fv = D.DeviceFv(pv)
+    rng = np.random.default_rng(seed + 100)
+    nb = v.nf - v.nif
+    phi, bv = rng.standard_normal(v.nc), rng.standard_normal(nb)
+    u, ub = rng.standard_normal((v.nc, 3)), rng.standard_normal((nb, 3))
+    flux, gamma, nu = rng.standard_normal(v.nf), rng.random(v.nf), rng.random(v.nif)
+    for scheme in (0, 1, 2):
+        assert np.array_equal(fv.gradient(phi, bv, scheme), F.gradient(v, phi, bv, scheme))
+        g = fv.vector_gradient(u, ub, scheme)
+        assert np.array_equal(g, F.vector_gradient(v, u, ub, scheme))
+        src = np.linspace(-1.0, 1.0, v.nc)
+        want = F.scalar_corrections(v, phi, bv, scheme, flux, gamma, True, src)
+        fv.scalar_corrections(phi, bv, scheme, flux, gamma, True, src)
+        assert np.array_equal(src, want)
+        for venkat in (False, True):
+            m = np.full((v.nc, 3), 0.25)
+            want = F.momentum_corrections(v, u, ub, g, flux[: v.nif], nu, True, True, venkat, [1e-3] * 3, 0.75,
+                                          True, m)
+            fv.momentum_corrections(flux, nu, True, True, venkat, [1e-3] * 3, 0.75, True, m)
+            assert np.array_equal(m, want)
+
+
+def test_single_cell_mesh(gpu):
+    """No internal faces (the reference pads its empty neighbour array, fv_device.cpp:45-49)."""
+    from cfd_b200 import fv_device as D
+    pv = D.mesh_view_of(gpu.Mesh.box(1, 1, 1))
+    assert pv.n_internal_faces == 0 and pv.n_faces == 6
+    v = _oracle_view(pv)
+    fv = D.DeviceFv(pv)
+    bv = pv.face_centre[:, 0] * 2.0 - pv.face_centre[:, 1]
+    for scheme in (0, 1, 2):
+        assert np.array_equal(fv.gradient(np.array([0.3]), bv, scheme), F.gradient(v, [0.3], bv, scheme))
+    u, ub = np.array([[1.0, 2.0, 3.0]]), np.stack([bv, -bv, 2 * bv], axis=1)
+    g = fv.vector_gradient(u, ub, 1)
+    m = np.zeros((1, 3))
+    fv.momentum_corrections(np.zeros(0), np.zeros(0), True, True, True, [1e-3] * 3, 0.0, True, m)
+    assert np.array_equal(m, F.momentum_corrections(v, u, ub, g, np.zeros(0), np.zeros(0), True, True, True,
+                                                    [1e-3] * 3, 0.0, True, np.zeros((1, 3))))

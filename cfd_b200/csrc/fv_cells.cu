@@ -621,7 +621,7 @@ size_t nbound(const cfdb_device_fv* fv) { return static_cast<size_t>(fv->m.nf - 
 size_t ninternal(const cfdb_device_fv* fv) { return static_cast<size_t>(fv->m.nif); }
 
 void need(bool ok, const char* what) {
-    if (!ok) fail(CFDB_ERR_BAD_ARG, std::string("DeviceFv: missing argument ") + what);
+    if (!ok) fail(CFDB_ERR_BAD_ARG, std::string("DeviceFv: null argument among ") + what);
 }
 
 } // namespace
@@ -737,7 +737,7 @@ int cfdb_device_fv_stream(const cfdb_device_fv* fv, void** stream) {
 
 int cfdb_device_fv_gradient(cfdb_device_fv* fv, const double* phi, const double* bv, int scheme, double* grad) {
     return guarded([&] {
-        need(fv != nullptr && phi != nullptr && grad != nullptr && (nbound(fv) == 0 || bv != nullptr), "");
+        need(fv != nullptr && phi != nullptr && grad != nullptr && (nbound(fv) == 0 || bv != nullptr), "phi, bv, grad");
         check_scheme(scheme);
         CFDB_CUDA(cudaSetDevice(fv->device));
         h2d(fv, fv->phi, phi, ncells(fv));
@@ -750,7 +750,7 @@ int cfdb_device_fv_gradient(cfdb_device_fv* fv, const double* phi, const double*
 
 int cfdb_device_fv_vector_gradient(cfdb_device_fv* fv, const double* u, const double* ub, int scheme, double* grad) {
     return guarded([&] {
-        need(fv != nullptr && u != nullptr && grad != nullptr && (nbound(fv) == 0 || ub != nullptr), "");
+        need(fv != nullptr && u != nullptr && grad != nullptr && (nbound(fv) == 0 || ub != nullptr), "u, ub, grad");
         check_scheme(scheme);
         CFDB_CUDA(cudaSetDevice(fv->device));
         fv->have_vector = false;
@@ -767,8 +767,7 @@ int cfdb_device_fv_scalar_corrections(cfdb_device_fv* fv, const double* phi, con
                                       const double* flux, const double* gamma, int linear_upwind, double* source) {
     return guarded([&] {
         need(fv != nullptr && phi != nullptr && source != nullptr && (nbound(fv) == 0 || bv != nullptr) &&
-                 (ninternal(fv) == 0 || (flux != nullptr && gamma != nullptr)),
-             "");
+                 (ninternal(fv) == 0 || (flux != nullptr && gamma != nullptr)), "phi, bv, flux, gamma, source");
         check_scheme(scheme);
         CFDB_CUDA(cudaSetDevice(fv->device));
         h2d(fv, fv->phi, phi, ncells(fv));
@@ -787,8 +786,7 @@ int cfdb_device_fv_momentum_corrections(cfdb_device_fv* fv, const double* flux, 
                                         double central, int transpose_term, double* source) {
     return guarded([&] {
         need(fv != nullptr && source != nullptr && (ninternal(fv) == 0 || (flux != nullptr && nu_face != nullptr)) &&
-                 (!venkat || eps2 != nullptr),
-             "");
+                 (!venkat || eps2 != nullptr), "flux, nu_face, eps2, source");
         // fv_openmp.cpp:205-207
         if (!fv->have_vector) fail(CFDB_ERR_NOT_READY, "DeviceFv::momentum_corrections before vector_gradient");
         CFDB_CUDA(cudaSetDevice(fv->device));
@@ -805,7 +803,7 @@ int cfdb_device_fv_momentum_corrections(cfdb_device_fv* fv, const double* flux, 
 int cfdb_device_fv_gradient_device(cfdb_device_fv* fv, const double* phi, const double* bv, int scheme,
                                    double* grad) {
     return guarded([&] {
-        need(fv != nullptr && phi != nullptr && grad != nullptr && (nbound(fv) == 0 || bv != nullptr), "");
+        need(fv != nullptr && phi != nullptr && grad != nullptr && (nbound(fv) == 0 || bv != nullptr), "phi, bv, grad");
         check_scheme(scheme);
         CFDB_CUDA(cudaSetDevice(fv->device));
         launch_gradient<1>(fv, phi, bv, scheme, grad);
@@ -816,7 +814,7 @@ int cfdb_device_fv_gradient_device(cfdb_device_fv* fv, const double* phi, const 
 int cfdb_device_fv_vector_gradient_device(cfdb_device_fv* fv, const double* u, const double* ub, int scheme,
                                           double* grad) {
     return guarded([&] {
-        need(fv != nullptr && u != nullptr && grad != nullptr && (nbound(fv) == 0 || ub != nullptr), "");
+        need(fv != nullptr && u != nullptr && grad != nullptr && (nbound(fv) == 0 || ub != nullptr), "u, ub, grad");
         check_scheme(scheme);
         CFDB_CUDA(cudaSetDevice(fv->device));
         launch_gradient<3>(fv, u, ub, scheme, grad);
@@ -829,8 +827,7 @@ int cfdb_device_fv_scalar_corrections_device(cfdb_device_fv* fv, const double* p
                                              double* source) {
     return guarded([&] {
         need(fv != nullptr && phi != nullptr && source != nullptr && (nbound(fv) == 0 || bv != nullptr) &&
-                 (ninternal(fv) == 0 || (flux != nullptr && gamma != nullptr)),
-             "");
+                 (ninternal(fv) == 0 || (flux != nullptr && gamma != nullptr)), "phi, bv, flux, gamma, source");
         check_scheme(scheme);
         CFDB_CUDA(cudaSetDevice(fv->device));
         launch_scalar_corrections(fv, phi, bv, scheme, flux, gamma, linear_upwind, source);
@@ -845,8 +842,7 @@ int cfdb_device_fv_momentum_corrections_device(cfdb_device_fv* fv, const double*
     return guarded([&] {
         need(fv != nullptr && u != nullptr && grad != nullptr && source != nullptr &&
                  (nbound(fv) == 0 || ub != nullptr) &&
-                 (ninternal(fv) == 0 || (flux != nullptr && nu_face != nullptr)) && (!venkat || eps2 != nullptr),
-             "");
+                 (ninternal(fv) == 0 || (flux != nullptr && nu_face != nullptr)) && (!venkat || eps2 != nullptr), "u, ub, grad, flux, nu_face, eps2, source");
         CFDB_CUDA(cudaSetDevice(fv->device));
         launch_momentum_corrections(fv, u, ub, grad, flux, nu_face, linear_upwind, limited, venkat, eps2, central,
                                     transpose_term, source);

@@ -37,6 +37,10 @@ struct FvMesh {
     const int* nei = nullptr;     // n_internal_faces
     const int* start = nullptr;   // n_cells + 1
     const int* faces = nullptr;   // start[n_cells], ascending per cell
+    // per slot of faces: the cell across an internal face, c' >= 0 when this cell owns it and
+    // -2 - c' when this cell is its neighbour; -1 for a boundary face (built at create, so the
+    // gathers need no owner / neighbour loads)
+    const int* across = nullptr;
     const double* w = nullptr;    // n_internal_faces
     const double* sf = nullptr;   // 3 n_faces
     const double* cf = nullptr;   // 3 n_faces
@@ -94,7 +98,7 @@ int grid(int n) { return std::max(1, (n + kThreads - 1) / kThreads); }
 // independent threads with the scalar kernel's register footprint; the components share
 // their face-index and face-vector loads in L1. out[3 (NC c + i) + j] = d phi_i / dx_j.
 template <int NC, bool LSQ>
-__global__ void __launch_bounds__(kThreads) k_cell_gradient(FvMesh m, const double* __restrict__ phi,
+__global__ void __launch_bounds__(kThreads, LSQ ? 8 : 6) k_cell_gradient(FvMesh m, const double* __restrict__ phi,
                                                             const double* __restrict__ bv,
                                                             double* __restrict__ out) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -106,30 +110,41 @@ __global__ void __launch_bounds__(kThreads) k_cell_gradient(FvMesh m, const doub
     const int k1 = m.start[c + 1];
     for (int k = m.start[c]; k < k1; ++k) {
         const int f = m.faces[k];
-        if (LSQ) {
-            const double dv = f < m.nif ? phi[m.nei[f] * NC + i] - phi[m.own[f] * NC + i]
-                                        : bv[(f - m.nif) * NC + i] - pc;
-            g0 += m.lsq_d[3 * f] * dv;
-            g1 += m.lsq_d[3 * f + 1] * dv;
-            g2 += m.lsq_d[3 * f + 2] * dv;
-        } else if (f < m.nif) {
-            const double wf = m.w[f];
-            const int o = m.own[f];
-            const double pf = wf * phi[o * NC + i] + (1.0 - wf) * phi[m.nei[f] * NC + i];
-            if (o == c) {
-                g0 += m.sf[3 * f] * pf;
-                g1 += m.sf[3 * f + 1] * pf;
-                g2 += m.sf[3 * f + 2] * pf;
+        const int x = m.across[k];
+        if (x != -1) {
+            // phi_P and phi_N of the face: this cell's value and the one across
+            const bool mine = x >= 0;
+            const double pa = phi[(mine ? x : -2 - x) * NC + i];
+            if (LSQ) {
+                const double dv = mine ? pa - pc : pc - pa; // phi_N - phi_P
+                g0 += m.lsq_d[3 * f] * dv;
+                g1 += m.lsq_d[3 * f + 1] * dv;
+                g2 += m.lsq_d[3 * f + 2] * dv;
             } else {
-                g0 -= m.sf[3 * f] * pf;
-                g1 -= m.sf[3 * f + 1] * pf;
-                g2 -= m.sf[3 * f + 2] * pf;
+                const double wf = m.w[f];
+                const double pf = mine ? wf * pc + (1.0 - wf) * pa : wf * pa + (1.0 - wf) * pc;
+                if (mine) {
+                    g0 += m.sf[3 * f] * pf;
+                    g1 += m.sf[3 * f + 1] * pf;
+                    g2 += m.sf[3 * f + 2] * pf;
+                } else {
+                    g0 -= m.sf[3 * f] * pf;
+                    g1 -= m.sf[3 * f + 1] * pf;
+                    g2 -= m.sf[3 * f + 2] * pf;
+                }
             }
         } else {
             const double b = bv[(f - m.nif) * NC + i];
-            g0 += m.sf[3 * f] * b;
-            g1 += m.sf[3 * f + 1] * b;
-            g2 += m.sf[3 * f + 2] * b;
+            if (LSQ) {
+                const double dv = b - pc;
+                g0 += m.lsq_d[3 * f] * dv;
+                g1 += m.lsq_d[3 * f + 1] * dv;
+                g2 += m.lsq_d[3 * f + 2] * dv;
+            } else {
+                g0 += m.sf[3 * f] * b;
+                g1 += m.sf[3 * f + 1] * b;
+                g2 += m.sf[3 * f + 2] * b;
+            }
         }
     }
     double* o = out + 3 * static_cast<size_t>(t);
@@ -162,8 +177,9 @@ __global__ void __launch_bounds__(kThreads) k_cell_gradient_corrected(FvMesh m, 
     const int k1 = m.start[c + 1];
     for (int k = m.start[c]; k < k1; ++k) {
         const int f = m.faces[k];
-        if (f < m.nif) {
-            const int p = m.own[f], n = m.nei[f];
+        const int x = m.across[k];
+        if (x != -1) {
+            const int p = x >= 0 ? c : -2 - x, n = x >= 0 ? x : c;
             const double wf = m.w[f];
             double pf = wf * phi[p * NC + i] + (1.0 - wf) * phi[n * NC + i];
             const double* gp = g + 3 * (static_cast<size_t>(p) * NC + i);
@@ -214,8 +230,8 @@ __global__ void __launch_bounds__(kThreads) k_cell_limiter(FvMesh m, const doubl
     for (int i = 0; i < 3; ++i) uc[i] = lo[i] = hi[i] = u[3 * c + i];
     const int k0 = m.start[c], k1 = m.start[c + 1];
     for (int k = k0; k < k1; ++k) {
-        const int f = m.faces[k];
-        const double* v = f < m.nif ? u + 3 * (m.own[f] == c ? m.nei[f] : m.own[f]) : ub + 3 * (f - m.nif);
+        const int x = m.across[k];
+        const double* v = x != -1 ? u + 3 * (x >= 0 ? x : -2 - x) : ub + 3 * (m.faces[k] - m.nif);
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
             const double vi = v[i];
@@ -347,15 +363,17 @@ __global__ void __launch_bounds__(kThreads) k_cell_face_sums(FvMesh m, const dou
         bool mine[F];
         double ev[F][NC];
         bool live = true;
+        int x[F];
+#pragma unroll
+        for (int j = 0; j < F; ++j) x[j] = k0 + j < k1 ? m.across[k0 + j] : -1; // past the end: a stop
 #pragma unroll
         for (int j = 0; j < F; ++j) {
-            const int fj = k0 + j < k1 ? m.faces[k0 + j] : m.nif; // past the end: a stop marker
-            live = live && fj < m.nif;
-            f[j] = live ? fj : -1;
+            live = live && x[j] != -1;
+            f[j] = live ? m.faces[k0 + j] : -1;
         }
 #pragma unroll
         for (int j = 0; j < F; ++j) {
-            mine[j] = f[j] >= 0 ? m.own[f[j]] == c : false;
+            mine[j] = x[j] >= 0;
 #pragma unroll
             for (int i = 0; i < NC; ++i) ev[j][i] = f[j] >= 0 ? e[static_cast<size_t>(f[j]) * NC + i] : 0.0;
         }
@@ -367,9 +385,10 @@ __global__ void __launch_bounds__(kThreads) k_cell_face_sums(FvMesh m, const dou
         }
     } else {
         for (int k = k0; k < k1; ++k) {
+            const int x = m.across[k];
+            if (x == -1) break; // the first boundary face
             const int f = m.faces[k];
-            if (f >= m.nif) break;
-            const bool mine = m.own[f] == c;
+            const bool mine = x >= 0;
 #pragma unroll
             for (int i = 0; i < NC; ++i) {
                 const double ev = e[static_cast<size_t>(f) * NC + i];
@@ -680,6 +699,15 @@ int cfdb_device_fv_create(const cfdb_fv_mesh_view* v, cfdb_device_fv** out) {
             m.nei = up(v->neighbour, fi);
             m.start = up(v->cell_offsets, c + 1);
             m.faces = up(v->cell_faces, static_cast<size_t>(n_slots));
+            {
+                std::vector<int> across(static_cast<size_t>(n_slots));
+                for (int cc = 0; cc < nc; ++cc)
+                    for (int k = v->cell_offsets[cc]; k < v->cell_offsets[cc + 1]; ++k) {
+                        const int f = v->cell_faces[k];
+                        across[k] = f >= nif ? -1 : v->owner[f] == cc ? v->neighbour[f] : -2 - v->owner[f];
+                    }
+                m.across = fv->mem.upload(across, fv->st);
+            }
             m.w = up(v->weight, fi);
             m.sf = up(v->sf, 3 * f);
             m.cf = up(v->face_centre, 3 * f);

@@ -486,9 +486,10 @@ __global__ void __launch_bounds__(kThreads) k_scalar_cells(FvMesh m, const doubl
     for (int k = m.start[c]; k < k1; ++k) {
         const int f = m.faces[k];
         const double fl = flux[f];
-        if (f < m.nif) {
+        const int x = m.across[k];
+        if (x != -1) {
             const double g = gamma[f] * dc[f];
-            if (m.own[f] == c) {
+            if (x >= 0) { // this cell owns the face
                 const double pos = fl > 0.0 ? 1.0 * fl : 0.0;
                 d = d + (pos + g);
                 div = div + fl;

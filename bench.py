@@ -454,18 +454,22 @@ def run_e2e(args, case, ds, tol, dev):
     dg, dv, x, src = pin(np.zeros(n)), pin(np.zeros(n)), pin(np.zeros(n)), pin(np.zeros(n))
     src0 = case.source0
     c = case.ref_cell
+    # The caller's host loops (zeroing the accumulated arrays, flow_solver.cpp:768-770 and
+    # 794-796, the norm for the tolerance) run as torch CPU ops on views of the same pinned
+    # buffers, so they use the host's threads as a caller's OpenMP loops would.
+    t_dg, t_dv, t_x, t_src = (torch.from_numpy(a) for a in (dg, dv, x, src))
+    t_src0 = torch.from_numpy(np.ascontiguousarray(src0, dtype=np.float64))
 
     def step():
-        dg[:] = 0.0
-        dv[:] = 0.0
+        t_dg.zero_()
+        t_dv.zero_()
         ds.assemble(flux, gamma, delta, 0.0, up, lo, dg, dv)
-        # flow_solver.cpp:768-770, 794-796 on the host, in place in pinned buffers
-        np.subtract(src0, dv, out=src)
+        torch.sub(t_src0, t_dv, out=t_src)
         src[c] += dg[c] * case.ref_value
         dg[c] += dg[c]
-        x[:] = 0.0
+        t_x.zero_()
         return ds.solve(dg, up, lo, src, x, cb.Method.Cg, True,
-                        cb.SolveControl(1e-8 * float(np.linalg.norm(src)), 500))
+                        cb.SolveControl(1e-8 * float(torch.linalg.vector_norm(t_src)), 500))
 
     for _ in range(max(args.warmup, 0)):
         step()

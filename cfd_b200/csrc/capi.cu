@@ -127,6 +127,29 @@ struct CallStream {
     CallStream& operator=(const CallStream&) = delete;
 };
 
+// A second stream with one event per slice, kept for an object's life: the read-backs of a
+// pipelined host-array call run on it while the next slice's uploads and kernels run on the
+// engine's stream.
+struct SliceStream {
+    cudaStream_t s = nullptr;
+    std::vector<cudaEvent_t> ev;
+    void ensure(size_t n_events) {
+        if (s == nullptr) CFDB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        while (ev.size() < n_events) {
+            cudaEvent_t e = nullptr;
+            CFDB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            ev.push_back(e);
+        }
+    }
+    SliceStream() = default;
+    ~SliceStream() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+        if (s != nullptr) cudaStreamDestroy(s);
+    }
+    SliceStream(const SliceStream&) = delete;
+    SliceStream& operator=(const SliceStream&) = delete;
+};
+
 } // namespace
 
 namespace cfdb {
@@ -181,6 +204,10 @@ struct cfdb_system {
     int* d_cf_ptr = nullptr;
     int* d_cf_face = nullptr;
     double* h_asm = nullptr; // device staging of cfdb_system_assemble (host-array variant)
+    // slices of cfdb_system_assemble: cells [asm_cells[j], asm_cells[j+1]) need the faces
+    // [0, asm_faces[j+1]), so slice j's read-back overlaps slice j+1's upload
+    std::vector<int> asm_cells, asm_faces;
+    SliceStream asm_d2h;
     unsigned long long launches = 0;
     // device copy of the pattern for the device AMG setup (uploaded on first use)
     DeviceArena pat_arena;
@@ -212,6 +239,31 @@ void build_value_map(cfdb_system* s) {
     }
     s->diag_src.resize(static_cast<size_t>(p.n));
     for (int i = 0; i < p.n; ++i) s->diag_src[i] = i;
+}
+
+// Cell slices of the host-array assembly and, per slice, the face prefix its cells need: the
+// largest face index of any cell up to the slice's end, plus one. With faces ordered by owner
+// (owner < neighbour) the prefixes grow evenly; any other order stays correct, with fewer
+// copies overlapped.
+void plan_assembly_slices(cfdb_system* s) {
+    constexpr int kSliceCells = 1 << 18;
+    constexpr int kMaxSlices = 8;
+    const int n = s->pat.n, nf = s->pat.n_faces;
+    const int k = std::max(1, std::min(kMaxSlices, n / kSliceCells));
+    std::vector<int> last(static_cast<size_t>(n), -1); // largest face index of each cell
+    for (int f = 0; f < nf; ++f) {
+        last[s->owner[f]] = std::max(last[s->owner[f]], f);
+        last[s->neighbour[f]] = std::max(last[s->neighbour[f]], f);
+    }
+    s->asm_cells.assign(1, 0);
+    s->asm_faces.assign(1, 0);
+    int upto = -1, c = 0;
+    for (int j = 0; j < k; ++j) {
+        const int c1 = j + 1 == k ? n : static_cast<int>(static_cast<long long>(n) * (j + 1) / k);
+        for (; c < c1; ++c) upto = std::max(upto, last[c]);
+        s->asm_cells.push_back(c1);
+        s->asm_faces.push_back(j + 1 == k ? nf : upto + 1);
+    }
 }
 
 void ensure_engine(cfdb_system* s) {
@@ -1104,28 +1156,50 @@ int cfdb_system_assemble(cfdb_system* sys, const double* flux, const double* gam
         double* d_lo = d_up + nf;
         double* d_dg = d_lo + nf;
         double* d_dv = d_dg + n;
-        const size_t bf = sizeof(double) * nf, bc = sizeof(double) * n;
-        if (nf > 0) {
-            CFDB_CUDA(cudaMemcpyAsync(d_fl, flux, bf, cudaMemcpyHostToDevice, st));
-            CFDB_CUDA(cudaMemcpyAsync(d_ga, gamma, bf, cudaMemcpyHostToDevice, st));
-            CFDB_CUDA(cudaMemcpyAsync(d_de, delta, bf, cudaMemcpyHostToDevice, st));
+        if (sys->asm_cells.empty()) plan_assembly_slices(sys);
+        const int n_slices = static_cast<int>(sys->asm_cells.size()) - 1;
+        sys->asm_d2h.ensure(static_cast<size_t>(n_slices) + 1);
+        cudaStream_t rb = sys->asm_d2h.s;
+        // Slice j: upload the faces it adds to the prefix and its cells' diag / div, compute
+        // those faces' coefficients and those cells' sums, then read them back on the second
+        // stream while slice j+1 uploads (the copy engines run both directions at once).
+        auto h2d = [&](double* dst, const double* src, int off, int cnt) {
+            if (cnt > 0)
+                CFDB_CUDA(cudaMemcpyAsync(dst + off, src + off, sizeof(double) * cnt, cudaMemcpyHostToDevice, st));
+        };
+        auto d2h = [&](double* dst, const double* src, int off, int cnt) {
+            if (cnt > 0)
+                CFDB_CUDA(cudaMemcpyAsync(dst + off, src + off, sizeof(double) * cnt, cudaMemcpyDeviceToHost, rb));
+        };
+        for (int j = 0; j < n_slices; ++j) {
+            const int f0 = sys->asm_faces[j], f1 = sys->asm_faces[j + 1];
+            const int c0 = sys->asm_cells[j], c1 = sys->asm_cells[j + 1];
+            h2d(d_fl, flux, f0, f1 - f0);
+            h2d(d_ga, gamma, f0, f1 - f0);
+            h2d(d_de, delta, f0, f1 - f0);
+            h2d(d_dg, diag, c0, c1 - c0);
+            h2d(d_dv, div, c0, c1 - c0);
+            if (f1 > f0) {
+                k_assemble_faces<<<(f1 - f0 + 255) / 256, 256, 0, st>>>(f1 - f0, d_fl + f0, d_ga + f0, d_de + f0,
+                                                                        convection, d_up + f0, d_lo + f0);
+                ++sys->launches;
+            }
+            if (c1 > c0) {
+                k_assemble_cell_range<<<(c1 - c0 + 255) / 256, 256, 0, st>>>(
+                    c0, c1, sys->d_cf_ptr, sys->d_cf_face, d_fl, d_ga, d_de, sys->d_owner, convection, d_dg, d_dv);
+                ++sys->launches;
+            }
+            CFDB_CUDA(cudaGetLastError());
+            CFDB_CUDA(cudaEventRecord(sys->asm_d2h.ev[j], st));
+            CFDB_CUDA(cudaStreamWaitEvent(rb, sys->asm_d2h.ev[j], 0));
+            d2h(upper, d_up, f0, f1 - f0);
+            d2h(lower, d_lo, f0, f1 - f0);
+            d2h(diag, d_dg, c0, c1 - c0);
+            d2h(div, d_dv, c0, c1 - c0);
         }
-        CFDB_CUDA(cudaMemcpyAsync(d_dg, diag, bc, cudaMemcpyHostToDevice, st));
-        CFDB_CUDA(cudaMemcpyAsync(d_dv, div, bc, cudaMemcpyHostToDevice, st));
-        if (nf > 0) {
-            k_assemble_faces<<<(nf + 255) / 256, 256, 0, st>>>(nf, d_fl, d_ga, d_de, convection, d_up, d_lo);
-            ++sys->launches;
-        }
-        k_assemble_cells<<<(n + 255) / 256, 256, 0, st>>>(n, sys->d_cf_ptr, sys->d_cf_face, d_fl, d_ga, d_de,
-                                                          sys->d_owner, convection, d_dg, d_dv);
-        ++sys->launches;
-        CFDB_CUDA(cudaGetLastError());
-        if (nf > 0) {
-            CFDB_CUDA(cudaMemcpyAsync(upper, d_up, bf, cudaMemcpyDeviceToHost, st));
-            CFDB_CUDA(cudaMemcpyAsync(lower, d_lo, bf, cudaMemcpyDeviceToHost, st));
-        }
-        CFDB_CUDA(cudaMemcpyAsync(diag, d_dg, bc, cudaMemcpyDeviceToHost, st));
-        CFDB_CUDA(cudaMemcpyAsync(div, d_dv, bc, cudaMemcpyDeviceToHost, st));
+        // the engine's stream resumes only after the last read-back
+        CFDB_CUDA(cudaEventRecord(sys->asm_d2h.ev[n_slices], rb));
+        CFDB_CUDA(cudaStreamWaitEvent(st, sys->asm_d2h.ev[n_slices], 0));
         CFDB_CUDA(cudaStreamSynchronize(st));
     });
 }

@@ -1170,6 +1170,16 @@ static __global__ void k_assemble_pressure_cells(int n, const int* __restrict__ 
     source[c] = src;
 }
 
+// Diagonal and divergence of cell c: its faces in ascending order, added to what diag and div
+// hold (assemble_convection_diffusion accumulates).
+static __device__ __forceinline__ void assemble_cell(int c, const int* __restrict__ cf_ptr,
+                                                     const int* __restrict__ cf_face,
+                                                     const double* __restrict__ flux,
+                                                     const double* __restrict__ gamma,
+                                                     const double* __restrict__ delta,
+                                                     const int* __restrict__ owner, double convection,
+                                                     double* __restrict__ diag, double* __restrict__ div);
+
 static __global__ void k_assemble_cells(int n, const int* __restrict__ cf_ptr,
                                  const int* __restrict__ cf_face, const double* __restrict__ flux,
                                  const double* __restrict__ gamma,
@@ -1179,6 +1189,27 @@ static __global__ void k_assemble_cells(int n, const int* __restrict__ cf_ptr,
     pdl_entry();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
+    assemble_cell(c, cf_ptr, cf_face, flux, gamma, delta, owner, convection, diag, div);
+}
+
+// Cells [c0, c1) only: one slice of a host-array assembly whose copies are pipelined.
+static __global__ void k_assemble_cell_range(int c0, int c1, const int* __restrict__ cf_ptr,
+                                             const int* __restrict__ cf_face, const double* __restrict__ flux,
+                                             const double* __restrict__ gamma, const double* __restrict__ delta,
+                                             const int* __restrict__ owner, double convection,
+                                             double* __restrict__ diag, double* __restrict__ div) {
+    const int c = c0 + static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (c >= c1) return;
+    assemble_cell(c, cf_ptr, cf_face, flux, gamma, delta, owner, convection, diag, div);
+}
+
+static __device__ __forceinline__ void assemble_cell(int c, const int* __restrict__ cf_ptr,
+                                                     const int* __restrict__ cf_face,
+                                                     const double* __restrict__ flux,
+                                                     const double* __restrict__ gamma,
+                                                     const double* __restrict__ delta,
+                                                     const int* __restrict__ owner, double convection,
+                                                     double* __restrict__ diag, double* __restrict__ div) {
     double d = diag[c];
     double v = div[c];
     const int end = cf_ptr[c + 1];

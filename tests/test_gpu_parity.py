@@ -63,6 +63,35 @@ def test_assembly_bitwise(gpu, make):
         assert np.array_equal(dg, d2) and np.array_equal(dv, v2)
 
 
+@pytest.mark.parametrize("size,permute", [(12, False), (100, False), (82, True)],
+                         ids=["graded12-one-slice", "graded100-three-slices", "graded82-faces-shuffled"])
+def test_system_assembly_host_arrays_bitwise(gpu, size, permute):
+    """DeviceSolver.assemble on host arrays (the call the e2e sequence makes): the copies are
+    pipelined over cell slices once a mesh has 2^19 cells or more; diag and div accumulate.
+    With the faces shuffled (no owner order) each slice needs a long face prefix, which must
+    stay correct."""
+    cb = gpu
+    case = W.graded(size)
+    own, nei = np.asarray(case.owner), np.asarray(case.neighbour)
+    flux, gamma, delta = case.flux, case.gamma, case.delta
+    nf = case.n_faces
+    if permute:
+        p = np.random.default_rng(7).permutation(nf)
+        own, nei, flux, gamma, delta = own[p], nei[p], flux[p], gamma[p], delta[p]
+    ds = cb.DeviceSolver(mesh=(case.n, own, nei))
+    try:
+        for conv, d0 in ((0.0, 0.0), (1.0, 0.25), (0.0, 0.0)):
+            up, lo = np.zeros(nf), np.zeros(nf)
+            dg, dv = np.full(case.n, d0), np.full(case.n, -d0)
+            ds.assemble(flux, gamma, delta, conv, up, lo, dg, dv)
+            u2, l2, d2, v2 = O.assemble(case.n, own, nei, flux, gamma, delta, conv,
+                                        diag=np.full(case.n, d0), div=np.full(case.n, -d0))
+            assert np.array_equal(up, u2) and np.array_equal(lo, l2)
+            assert np.array_equal(dg, d2) and np.array_equal(dv, v2)
+    finally:
+        ds.close()
+
+
 def test_assembly_matches_reference_kat(gpu):
     """test_gpu.cpp:274-309 (AssemblyMatchesCpu): 7x5x3 box, convection 1."""
     cb = gpu

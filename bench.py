@@ -487,7 +487,28 @@ def run_e2e(args, case, ds, tol, dev):
     d2h = (16 * nf + 16 * n) + 8 * n
     return {"value": args.steps / (ms / 1e3), "unit": "solves/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": ms / args.steps,
-            "path": "cfdb_system_assemble + host finalize + cfdb_system_solve (host arrays)"}
+            "path": "cfdb_system_assemble + host finalize + cfdb_system_solve (host arrays)",
+            "host_copy_gbs": host_copy_rates(stream, dev)}
+
+
+def host_copy_rates(stream, dev, nbytes=64 << 20):
+    """This machine's page-locked copy rates (GB/s, each way, one 64 MB copy timed with CUDA
+    events after a warm-up): the e2e figure depends on them, and they differ between hosts."""
+    import torch
+    h = torch.empty(nbytes // 8, dtype=torch.float64).pin_memory()
+    d = torch.empty(nbytes // 8, dtype=torch.float64, device=dev)
+    out = {}
+    with torch.cuda.stream(stream):
+        for name, dst, src in (("h2d", d, h), ("d2h", h, d)):
+            dst.copy_(src, non_blocking=True)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(5):
+                dst.copy_(src, non_blocking=True)
+            e1.record(stream)
+            e1.synchronize()
+            out[name] = 5 * nbytes / 1e9 / (e0.elapsed_time(e1) / 1e3)
+    return out
 
 
 def cpu_baseline(case):

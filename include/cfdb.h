@@ -337,7 +337,10 @@ int cfdb_system_profile(cfdb_system* sys, int use_amg, int reps, cfdb_kernel_rec
                         int max_records, int* n_records);
 
 /* cfdb_system_assemble_device with host arrays (the reference's assemble call on a persistent
- * mesh: inputs copied to the device, results copied back). */
+ * mesh: inputs copied to the device, results copied back). On meshes of 2^19 cells or more the
+ * copies run in up to 8 cell slices, each slice's results copied back while the next slice
+ * uploads; page-locked arrays let the two directions overlap. Returns when every result is in
+ * the host arrays. */
 int cfdb_system_assemble(cfdb_system* sys, const double* flux, const double* gamma,
                          const double* delta_coeff, double convection, double* upper,
                          double* lower, double* diag, double* divergence);

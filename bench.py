@@ -455,9 +455,8 @@ def run_e2e(args, case, ds, tol, dev):
     src0 = case.source0
     c = case.ref_cell
     # The caller's host loops (zeroing the accumulated arrays, flow_solver.cpp:768-770 and
-    # 794-796) run as torch CPU ops on views of the same pinned buffers, so they use the host's
-    # threads as a caller's OpenMP loops would; the norm for the tolerance is numpy's (BLAS),
-    # which measured faster than torch's here (0.11 vs 0.66 ms for 2.1M values).
+    # 794-796, the norm for the tolerance) run as torch CPU ops on views of the same pinned
+    # buffers, so they use the host's threads as a caller's OpenMP loops would.
     t_dg, t_dv, t_x, t_src = (torch.from_numpy(a) for a in (dg, dv, x, src))
     t_src0 = torch.from_numpy(np.ascontiguousarray(src0, dtype=np.float64))
 
@@ -470,7 +469,7 @@ def run_e2e(args, case, ds, tol, dev):
         dg[c] += dg[c]
         t_x.zero_()
         return ds.solve(dg, up, lo, src, x, cb.Method.Cg, True,
-                        cb.SolveControl(1e-8 * float(np.linalg.norm(src)), 500))
+                        cb.SolveControl(1e-8 * float(torch.linalg.vector_norm(t_src)), 500))
 
     for _ in range(max(args.warmup, 0)):
         step()

@@ -1,15 +1,16 @@
 #!/usr/bin/env python3
 """Benchmark: pressure solves/s of the B200 pressure-correction path.
 
-Workload (default): the 128^3 two-sided graded hex box (2,097,152 cells, 6,242,304 internal
-faces, grading ratio 1.05, rAU log-normal sigma 0.5, seeded), one GPU. One step = one pressure
+Workload (default): the jittered 6-tet box, 95^3 cubes split into 6 tets each (5,144,250 cells,
+10,234,350 internal faces, interior nodes jittered by +-20% of the spacing, over-relaxed delta
+coefficients, rAU log-normal sigma 1, seeded), one GPU. One step = one pressure
 solve as FlowSolver::pressure_correction issues it: face-loop assembly of the LDU pressure
 matrix and right-hand side on the device, then AMG-PCG from x0 = 0 to relative residual 1e-8
 with the resident hierarchy (rebuilt only every 20 solves in the reference; setup time reported
 separately). `value` is the mixed-precision path (FP32 V-cycle inside FP64 flexible CG); the
 plain FP64 path is reported beside it. Inputs are resident in HBM and larger than L2.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config graded|tet|cavity]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config tet|graded|cavity]
   python bench.py --config batch    # 256 uneven boxes in one device plan, autotuned
   python bench.py --config serve    # serving loop, Poisson arrivals, p50/p99
   python bench.py --config fv       # DeviceFv kernels of the momentum predictor, 5.14M-cell tet box
@@ -43,7 +44,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="graded", choices=["graded", "tet", "cavity", "batch", "serve", "fv", "step"])
+    ap.add_argument("--config", default="tet", choices=["graded", "tet", "cavity", "batch", "serve", "fv", "step"])
     ap.add_argument("--systems", type=int, default=256, help="batch: number of systems")
     ap.add_argument("--tune-cache", default=None, help="batch: autotuner cache file")
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serve: arrival rates (1/s)")
@@ -60,6 +61,14 @@ def parse():
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="build and time one precision only (profiling runs)")
     return ap.parse_args()
+
+
+def case_config(cfg_name, case, desc, world):
+    """The `config` object of both arms' lines (identical keys and values)."""
+    return {"workload": cfg_name, "cells": case.n, "internal_faces": case.n_faces,
+            "description": desc, "tolerance": "true relative residual <= 1e-8, x0 = 0",
+            "strength_threshold": THETA, "l2": "inputs larger than L2 (no flush)",
+            "parallelism": f"replicas x{world}"}
 
 
 def make_case(config, size):
@@ -182,14 +191,14 @@ def reference_solver(case, hier):
     ci = np.ascontiguousarray(hier.coarse_inverse)
     assert R.ref_ds_set_amg(h, nl, A, P, RR, dp(ci), 2, 0.7) == 0
 
-    def step():
+    def step(rel_tol=1e-8, out=None):
         up, lo, dg, dv = O.ref_assemble(case.n, case.owner, case.neighbour, case.flux, case.gamma,
                                         case.delta, 0.0)
         diag, src = case.finalize(up, lo, dg, dv)
-        x = np.zeros(case.n)
+        x = np.zeros(case.n) if out is None else out
         it, res, conv = C.c_int(), C.c_double(), C.c_int()
-        tol = 1e-8 * float(np.linalg.norm(src))
-        rc = R.ref_ds_solve(h, dp(diag), dp(up), dp(lo), dp(src), dp(x), 0, 1, tol, 500,
+        tol = rel_tol * float(np.linalg.norm(src))
+        rc = R.ref_ds_solve(h, dp(diag), dp(up), dp(lo), dp(src), dp(x), 0, 1, tol, 1000,
                             C.byref(it), C.byref(res), C.byref(conv))
         assert rc == 0 and conv.value == 1
         return it.value
@@ -232,8 +241,7 @@ def run_reference(args, cfg_name, case, desc):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-        "config": {"workload": cfg_name, "cells": case.n, "faces": case.n_faces,
-                   "description": desc, "strength_threshold": THETA},
+        "config": case_config(cfg_name, case, desc, args.gpus),
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores,
                          "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
@@ -384,6 +392,12 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
             "setup_s_device": setup_dev_s[k],
             "setup_phases_device": setup_prof[k],
             "device_bytes": solvers[k].device_bytes(),
+            # every kernel class of one CG iteration: launches, CUDA-event time per launch,
+            # algorithmic bytes per launch and the fraction of the measured HBM peak
+            "kernel_table": {key: {"launches": c, "us_per_launch": 1e3 * t / c,
+                                   "alg_bytes_per_launch": b / c,
+                                   "frac_of_peak": (b / 1e9) / (t / 1e3) / peak if t > 0 else None}
+                             for key, (t, b, c) in shares.items()},
         }
     by, ms_k, top, shares = summarise(prof["mixed"], results["mixed"]["iterations"])
     key, (tms, tbytes, cnt) = top
@@ -409,7 +423,12 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
         e2e = run_e2e(args, case, solvers["mixed"], tol, dev)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(case)
+        cpu, x_star = cpu_baseline(case)
+        if x_star is not None:
+            xs = torch.as_tensor(x_star, device=dev)
+            for k in out_prec:
+                out_prec[k]["rel_error_vs_reference_fp64_1e-12"] = float(
+                    torch.linalg.norm(bufs[k]["x"] - xs).item() / torch.linalg.norm(xs).item())
     value = out_prec["mixed"]["solves_per_s"]
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
@@ -417,10 +436,7 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
         "ms_per_step": results["mixed"]["ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32 (FP64 outer, FP32 V-cycle)",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": cfg_name, "cells": n, "internal_faces": nf, "description": desc,
-                   "tolerance": "true relative residual <= 1e-8, x0 = 0",
-                   "strength_threshold": THETA, "l2": "inputs larger than L2 (no flush)",
-                   "parallelism": f"replicas x{world}"},
+        "config": case_config(cfg_name, case, desc, world),
         "fp64": out_prec["fp64"], "mixed": out_prec["mixed"],
         "mixed_vs_fp64_time": out_prec["mixed"]["ms_per_solve"] / out_prec["fp64"]["ms_per_solve"],
         # the reference rebuilds the hierarchy every 20 solves (ldu_matrix.cpp:314): per-solve
@@ -513,12 +529,13 @@ def host_copy_rates(stream, dev, nbytes=64 << 20):
 
 def cpu_baseline(case):
     """The reference's host implementation (oracle/_ref) timed on this machine's cores on a
-    bounded sample: two pressure solves of the same workload."""
+    bounded sample: two pressure solves of the same workload. Also returns the reference's
+    solution at relative residual 1e-12 (untimed), the FP64 yardstick for the stated errors."""
     try:
         import numpy as np
         import oracle as O
         if O.ref() is None:
-            return None
+            return None, None
         hier = oracle_hierarchy(case)
         step = reference_solver(case, hier)
         step()
@@ -527,14 +544,17 @@ def cpu_baseline(case):
         for _ in range(k):
             step()
         dt = time.perf_counter() - t0
+        x_star = np.zeros(case.n)
+        it_star = step(1e-12, x_star)
         step.close()
-        del np
         return {"value": k / dt, "unit": "solves/s", "cores": os.cpu_count() or 1,
                 "kind": "reference",
-                "sample": f"{k} pressure solves (assembly + AMG-PCG to 1e-8) after one warm-up"}
+                "sample": f"{k} pressure solves (assembly + AMG-PCG to 1e-8) after one warm-up",
+                "fp64_yardstick": f"reference host path to relative residual 1e-12 ({it_star} "
+                                  "iterations), untimed"}, x_star
     except Exception as e:  # the baseline is reported, never required
         return {"value": None, "unit": "solves/s", "cores": os.cpu_count() or 1,
-                "kind": "reference", "sample": f"failed: {e}"}
+                "kind": "reference", "sample": f"failed: {e}"}, None
 
 
 # ------------------------------------------------------------------------------------------

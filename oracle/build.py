@@ -21,8 +21,10 @@ REF_DIR = os.path.join(HERE, "_ref")
 ORACLE_SO = os.path.join(BUILD_DIR, "liboracle.so")
 REF_SO = os.path.join(REF_DIR, "libcfdref.so")
 
-# Where the reference checkout lives in the build container (read-only).
-REFERENCE_ROOT = os.environ.get("CFD_REFERENCE_ROOT", "/root/reference")
+# The reference checkout: CFD_REFERENCE_ROOT, else a directory named "reference" beside the
+# repository (read-only; only this recipe reads it).
+REFERENCE_ROOT = os.environ.get(
+    "CFD_REFERENCE_ROOT", os.path.normpath(os.path.join(HERE, os.pardir, os.pardir, "reference")))
 REF_SOURCES = [
     "src/gpu/src/krylov_openmp.cpp",
     "src/gpu/src/device_solver.cpp",
@@ -30,6 +32,19 @@ REF_SOURCES = [
     "src/gpu/src/fv_openmp.cpp",
     "src/gpu/src/fv_device.cpp",
 ]
+# Eigen-dependent sources, compiled unchanged against the Eigen stand-in (oracle/eigen_standin).
+REF_EIGEN_SOURCES = [
+    "src/mesh/src/mesh.cpp",
+    "src/mesh/src/mesh_builder.cpp",
+    "src/mesh/src/box_mesher.cpp",
+    "src/fv/src/fv_geometry.cpp",
+    "src/fv/src/ldu_matrix.cpp",
+    "src/fv/src/amg.cpp",
+    "src/fv/src/parallel_amg.cpp",
+    "src/parallel/src/comm.cpp",
+]
+REF_INCLUDES = ["src/gpu/include", "src/core/include", "src/mesh/include", "src/fv/include",
+                "src/parallel/include"]
 
 
 def _stale(target: str, sources: list[str]) -> bool:
@@ -53,29 +68,45 @@ def build_oracle(force: bool = False) -> str:
 
 
 def reference_available() -> bool:
-    return all(os.path.exists(os.path.join(REFERENCE_ROOT, s)) for s in REF_SOURCES)
+    return all(os.path.exists(os.path.join(REFERENCE_ROOT, s)) for s in REF_SOURCES + REF_EIGEN_SOURCES)
 
 
 def build_ref(force: bool = False) -> str | None:
     """Compile the reference's host path (unchanged sources) + our shim into oracle/_ref."""
     if not reference_available():
         return REF_SO if os.path.exists(REF_SO) else None
-    srcs = [os.path.join(REFERENCE_ROOT, s) for s in REF_SOURCES]
-    shim = os.path.join(HERE, "ref_shim.cpp")
-    deps = srcs + [shim, os.path.join(REFERENCE_ROOT, "src/gpu/src/krylov_kernels.inc"),
-                   os.path.join(REFERENCE_ROOT, "src/gpu/include/cfd/gpu/krylov.hpp"),
-                   os.path.join(REFERENCE_ROOT, "src/gpu/src/fv_cell.inc"),
-                   os.path.join(REFERENCE_ROOT, "src/gpu/src/fv_impl.hpp"),
-                   os.path.join(REFERENCE_ROOT, "src/gpu/include/cfd/gpu/fv_device.hpp")]
+    srcs = [os.path.join(REFERENCE_ROOT, s) for s in REF_SOURCES + REF_EIGEN_SOURCES]
+    shims = [os.path.join(HERE, "ref_shim.cpp"), os.path.join(HERE, "ref_eigen_shim.cpp")]
+    standin = os.path.join(HERE, "eigen_standin")
+    deps = srcs + shims + [os.path.join(REFERENCE_ROOT, "src/gpu/src/krylov_kernels.inc"),
+                           os.path.join(REFERENCE_ROOT, "src/gpu/src/fv_cell.inc"),
+                           os.path.join(REFERENCE_ROOT, "src/gpu/src/fv_impl.hpp")]
+    for inc in REF_INCLUDES:
+        for dirpath, _, files in os.walk(os.path.join(REFERENCE_ROOT, inc)):
+            deps += [os.path.join(dirpath, f) for f in files]
+    deps += [os.path.join(standin, "Eigen", f) for f in os.listdir(os.path.join(standin, "Eigen"))]
     if force or _stale(REF_SO, deps):
         if shutil.which("g++") is None:
             return None
         os.makedirs(REF_DIR, exist_ok=True)
+        objdir = os.path.join(REF_DIR, "obj")
+        os.makedirs(objdir, exist_ok=True)
+        # No -march: plain x86-64 (SSE2, no FMA), so the host path rounds every product and sum
+        # separately, as a default build of the reference does.
+        flags = ["g++", "-std=c++20", "-O3", "-fopenmp", "-fPIC", "-I", standin]
+        for inc in REF_INCLUDES:
+            flags += ["-I", os.path.join(REFERENCE_ROOT, inc)]
+        from concurrent.futures import ThreadPoolExecutor
+        objs = [os.path.join(objdir, f"{i:02d}_{os.path.basename(src)}.o") for i, src in enumerate(srcs + shims)]
+
+        def compile_one(pair):
+            src, obj = pair
+            subprocess.run(flags + ["-c", src, "-o", obj], check=True)
+
+        with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+            list(ex.map(compile_one, zip(srcs + shims, objs)))
         tmp = REF_SO + f".tmp{os.getpid()}"
-        # No -march: plain x86-64 has no FMA, so the host path rounds every product and sum.
-        cmd = ["g++", "-std=c++20", "-O3", "-fopenmp", "-fPIC", "-shared",
-               "-I", os.path.join(REFERENCE_ROOT, "src/gpu/include"), *srcs, shim, "-o", tmp]
-        subprocess.run(cmd, check=True)
+        subprocess.run(["g++", "-shared", "-fopenmp", *objs, "-o", tmp], check=True)
         os.replace(tmp, REF_SO)
     return REF_SO
 

@@ -1,0 +1,191 @@
+"""Parity at the sizes of the benchmark configurations, through the C ABI.
+
+* cavity32: the lid-driven cavity pressure system, uniform 32^3 hex box (32,768 cells, 95,232
+  internal faces), rAU = 1, pure Neumann walls with cell 0 pinned.
+* tet95: the jittered 6-tet box, 95^3 cubes (5,144,250 cells, 10,234,350 internal faces),
+  over-relaxed delta coefficients, rAU log-normal sigma 1.
+
+Checks per configuration:
+* the device assembly (fused pressure assembly into the resident system, and the host-array
+  assemble_convection_diffusion) equals the reference's own compiled serial assembly
+  (krylov_openmp.cpp:289-300, oracle/_ref) bit for bit; source -= div (flow_solver.cpp:768-770)
+  and set_reference (ldu_matrix.cpp:105-109) applied by the oracle;
+* the hierarchy built on the device equals the oracle's restated AmgPreconditioner::setup
+  (amg.cpp:12-240) bit for bit: aggregates, P, R, Galerkin operators, coarse inverse;
+* FP64 AMG-PCG on the oracle's hierarchy takes the iterations of the reference's compiled
+  DeviceSolver host path (device_solver.cpp:58-150, krylov_kernels.inc:240-301) within 1 and
+  reaches the true relative residual 1e-8;
+* the product path as the benchmark runs it (device setup, FP64 and mixed precision) reaches
+  the true relative residual 1e-8 in FP64, and its error against a tight FP64 solution of the
+  reference's host path (relative residual 1e-12) is bounded and recorded.
+
+Set CFDB_PARITY_RECORD=<file.json> to append the measured errors and iteration counts.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from cfd_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+THETA = 0.04
+CONFIGS = {"cavity32": lambda: W.cavity(32), "tet95": lambda: W.tet(95)}
+
+
+def _record(name, **fields):
+    path = os.environ.get("CFDB_PARITY_RECORD")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps({"config": name, **fields}) + "\n")
+
+
+@pytest.fixture(scope="module", params=list(CONFIGS))
+def system(request):
+    if O.ref() is None:
+        pytest.skip("reference host library (oracle/_ref) not built")
+    name = request.param
+    case = CONFIGS[name]()
+    up, lo, dg, dv = O.ref_assemble(case.n, case.owner, case.neighbour, case.flux, case.gamma,
+                                    case.delta, 0.0)
+    src = case.source0 - dv
+    diag = dg.copy()
+    O.set_reference(diag, src, case.ref_cell, case.ref_value)
+    pat = O.build_pattern(case.n, case.owner, case.neighbour)
+    a = O.ldu_to_csr(pat, diag, up, lo)
+    hier = O.Hierarchy(a, theta=THETA)
+    bnorm = float(np.linalg.norm(src))
+    # tight FP64 solution of the reference's host path, the yardstick for the stated errors
+    x_star, st = O.ref_device_solver(pat, hier, diag, up, lo, src, abs_tol=1e-12 * bnorm,
+                                     max_iterations=1000)
+    assert st["converged"]
+    return dict(name=name, case=case, up=up, lo=lo, dg=dg, dv=dv, diag=diag, src=src, pat=pat,
+                a=a, hier=hier, bnorm=bnorm, x_star=x_star)
+
+
+def _view(cb, h):
+    lv = []
+    for l in range(h.levels):
+        A = cb.CsrView(h.a[l].n_rows, h.a[l].rp, h.a[l].ci, h.a[l].va)
+        P = R = None
+        if l + 1 < h.levels:
+            P = cb.CsrView(h.p[l].n_rows, h.p[l].rp, h.p[l].ci, h.p[l].va)
+            R = cb.CsrView(h.r[l].n_rows, h.r[l].rp, h.r[l].ci, h.r[l].va)
+        lv.append(cb.AmgLevelView(A, P, R))
+    return cb.AmgView(lv, h.coarse_inverse, 2, 0.7)
+
+
+def test_assembly_matches_reference(gpu, system):
+    import torch
+    cb, s = gpu, system
+    case = s["case"]
+    n, nf = case.n, case.n_faces
+    # host-array entry point (assemble_convection_diffusion, convection 0)
+    up, lo, dg, dv = np.zeros(nf), np.zeros(nf), np.zeros(n), np.zeros(n)
+    cb.assemble_convection_diffusion(n, nf, case.owner, case.neighbour, case.flux, case.gamma,
+                                     case.delta, 0.0, up, lo, dg, dv)
+    for got, want in ((up, s["up"]), (lo, s["lo"]), (dg, s["dg"]), (dv, s["dv"])):
+        assert np.array_equal(got, want)
+    # fused device assembly into the resident system: upper, lower, diag with the reference
+    # cell, source0 - div with the reference cell
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")  # noqa: E731
+    ds = cb.DeviceSolver(mesh=(n, case.owner, case.neighbour))
+    try:
+        out = [torch.empty(k, dtype=torch.float64, device="cuda") for k in (nf, nf, n, n)]
+        ds.assemble_pressure_device(T(case.flux), T(case.gamma), T(case.delta), T(case.source0),
+                                    *out, ref_cell=case.ref_cell, ref_value=case.ref_value)
+        torch.cuda.synchronize()
+        for got, want in zip(out, (s["up"], s["lo"], s["diag"], s["src"])):
+            assert np.array_equal(got.cpu().numpy(), want)
+    finally:
+        ds.close()
+
+
+def test_device_hierarchy_matches_oracle(gpu, system):
+    cb, s = gpu, system
+    a, o = s["a"], s["hier"]
+    h = cb.AmgHierarchy(cb.CsrView(a.n_rows, a.rp, a.ci, a.va),
+                        cb.AmgSettings(strength_threshold=THETA), device=True)
+    assert h.levels() == o.levels
+    for l in range(o.levels):
+        got = h.level_matrix(l)
+        for x, y in zip((got.row_ptr, got.col, got.val), (o.a[l].rp, o.a[l].ci, o.a[l].va)):
+            assert np.array_equal(x, y), f"A[{l}]"
+        if l + 1 < o.levels:
+            agg, n_agg = h.aggregates(l)
+            assert np.array_equal(agg, o.aggregates[l]) and n_agg == o.a[l + 1].n_rows, f"aggregates[{l}]"
+            for nm, g, w in (("P", h.level_prolongation(l), o.p[l]), ("R", h.level_restriction(l), o.r[l])):
+                for x, y in zip((g.row_ptr, g.col, g.val), (w.rp, w.ci, w.va)):
+                    assert np.array_equal(x, y), f"{nm}[{l}]"
+    assert np.array_equal(h.coarse_inverse(), o.coarse_inverse)
+    _record(s["name"], levels=o.levels, level_rows=[o.a[l].n_rows for l in range(o.levels)],
+            operator_complexity=sum(o.a[l].nnz for l in range(o.levels)) / o.a[0].nnz)
+
+
+def test_fp64_amg_pcg_matches_reference(gpu, system):
+    """Same hierarchy on both sides: iterations of the GPU FP64 path within 1 of the reference's
+    compiled DeviceSolver host path, true relative residual <= 1e-8."""
+    cb, s = gpu, system
+    tol = 1e-8 * s["bnorm"]
+    x_ref, st_ref = O.ref_device_solver(s["pat"], s["hier"], s["diag"], s["up"], s["lo"], s["src"],
+                                        abs_tol=tol, max_iterations=500)
+    p = s["pat"]
+    ds = cb.DeviceSolver(cb.LduPattern(p.n, p.n_faces, p.row_ptr, p.col, p.diag_pos, p.upper_pos,
+                                       p.lower_pos))
+    try:
+        ds.set_amg(_view(cb, s["hier"]))
+        x = np.zeros(p.n)
+        st = ds.solve(s["diag"], s["up"], s["lo"], s["src"], x, cb.Method.Cg, True,
+                      cb.SolveControl(tol, 500))
+    finally:
+        ds.close()
+    assert st.converged and st.on_device and st_ref["converged"]
+    assert abs(st.iterations - st_ref["iterations"]) <= 1
+    true_res = float(np.linalg.norm(s["src"] - s["a"].matvec(x)))
+    assert true_res <= 1.05 * tol
+    xs = s["x_star"]
+    err = float(np.linalg.norm(x - xs) / np.linalg.norm(xs))
+    err_ref = float(np.linalg.norm(x_ref - xs) / np.linalg.norm(xs))
+    # both stop at the same residual target; the GPU's error is of the reference's own size
+    assert err <= max(10.0 * err_ref, 1e-9)
+    _record(s["name"], path="fp64, oracle hierarchy", iterations=st.iterations,
+            reference_iterations=st_ref["iterations"], true_rel_residual=true_res / s["bnorm"],
+            rel_error_vs_fp64_reference_1e12=err, reference_rel_error=err_ref)
+
+
+@pytest.mark.parametrize("precision", ["FP64", "MIXED"])
+def test_product_path_reaches_target(gpu, system, precision):
+    """The benchmark's path: device assembly, hierarchy built on the device, FP64 or mixed
+    (FP32 V-cycle inside FP64 flexible CG), to a true FP64 relative residual of 1e-8."""
+    import torch
+    cb, s = gpu, system
+    case = s["case"]
+    n, nf = case.n, case.n_faces
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")  # noqa: E731
+    ds = cb.DeviceSolver(mesh=(n, case.owner, case.neighbour))
+    try:
+        ds.set_precision(getattr(cb.Precision, precision))
+        up, lo, dg, src = [torch.empty(k, dtype=torch.float64, device="cuda") for k in (nf, nf, n, n)]
+        ds.assemble_pressure_device(T(case.flux), T(case.gamma), T(case.delta), T(case.source0),
+                                    up, lo, dg, src, ref_cell=case.ref_cell, ref_value=case.ref_value)
+        ds.setup_amg(dg, up, lo, cb.AmgSettings(strength_threshold=THETA), device=True)
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        tol = 1e-8 * s["bnorm"]
+        st = ds.solve_device(dg, up, lo, src, x, cb.Method.Cg, True, cb.SolveControl(tol, 500))
+        torch.cuda.synchronize()
+        xh = x.cpu().numpy()
+    finally:
+        ds.close()
+    assert st.converged
+    true_res = float(np.linalg.norm(s["src"] - s["a"].matvec(xh)))
+    # mixed precision converges on the FP64 true residual; FP64 CG stops on its recursively
+    # updated residual, as the reference does, which tracks the true one to round-off
+    assert true_res <= (1.0 if precision == "MIXED" else 1.05) * tol
+    xs = s["x_star"]
+    err = float(np.linalg.norm(xh - xs) / np.linalg.norm(xs))
+    assert err <= 1e-6
+    _record(s["name"], path=f"{precision.lower()}, device setup", iterations=st.iterations,
+            true_rel_residual=true_res / s["bnorm"], rel_error_vs_fp64_reference_1e12=err)

@@ -71,13 +71,38 @@ def case_config(cfg_name, case, desc, world):
             "parallelism": f"replicas x{world}"}
 
 
+DEFAULT_SIZE = {"graded": 128, "tet": 95, "cavity": 32}
+DESCRIPTION = {"graded": "graded hex box, two-sided ratio 1.05, rAU lognormal 0.5",
+               "tet": "jittered 6-tet box (+-20% h), over-relaxed delta, rAU lognormal 1",
+               "cavity": "uniform cavity hex box, rAU = 1"}
+
+
 def make_case(config, size):
+    """The configuration from the product's generator (our arm)."""
     from cfd_b200 import workloads as W
-    if config == "graded":
-        return W.graded(size or 128), "graded hex box, two-sided ratio 1.05, rAU lognormal 0.5"
-    if config == "tet":
-        return W.tet(size or 95), "jittered 6-tet box (+-20% h), over-relaxed delta, rAU lognormal 1"
-    return W.cavity(size or 32), "uniform cavity hex box, rAU = 1"
+    make = {"graded": W.graded, "tet": W.tet, "cavity": W.cavity}[config]
+    return make(size or DEFAULT_SIZE[config]), DESCRIPTION[config]
+
+
+def make_reference_case(config, size):
+    """The same configuration built by the reference's own mesh pipeline and FvGeometry
+    (oracle/_ref; the seeded inputs restated there), so that the reference arm never loads
+    the product library. Equal to make_case's bit for bit (tests/test_reference_eigen_pinned.py)."""
+    import oracle.reference as RX
+    if not RX.available():
+        return None, DESCRIPTION[config]
+    make = {"graded": RX.graded, "tet": RX.tet, "cavity": RX.cavity}[config]
+    return make(size or DEFAULT_SIZE[config]), DESCRIPTION[config]
+
+
+def finalize(case, up, lo, dg, dv):
+    """flow_solver.cpp:768-770 (source -= div) and LduMatrix::set_reference
+    (ldu_matrix.cpp:105-109) on copies: returns (diag, source)."""
+    import oracle as O
+    src = case.source0 - dv
+    diag = dg.copy()
+    O.set_reference(diag, src, case.ref_cell, case.ref_value)
+    return diag, src
 
 
 class ClockSampler:
@@ -194,7 +219,7 @@ def reference_solver(case, hier):
     def step(rel_tol=1e-8, out=None):
         up, lo, dg, dv = O.ref_assemble(case.n, case.owner, case.neighbour, case.flux, case.gamma,
                                         case.delta, 0.0)
-        diag, src = case.finalize(up, lo, dg, dv)
+        diag, src = finalize(case, up, lo, dg, dv)
         x = np.zeros(case.n) if out is None else out
         it, res, conv = C.c_int(), C.c_double(), C.c_int()
         tol = rel_tol * float(np.linalg.norm(src))
@@ -208,18 +233,27 @@ def reference_solver(case, hier):
     return step
 
 
-def oracle_hierarchy(case):
+def reference_hierarchy(case):
+    """AmgPreconditioner::setup of the reference (amg.cpp, compiled against the Eigen stand-in)
+    on the assembled pressure matrix, at the benchmark's strength threshold."""
     import oracle as O
-    up, lo, dg, dv = O.assemble(case.n, case.owner, case.neighbour, case.flux, case.gamma,
-                                case.delta, 0.0)
-    diag, src = case.finalize(up, lo, dg, dv)
+    import oracle.reference as RX
+    up, lo, dg, dv = O.ref_assemble(case.n, case.owner, case.neighbour, case.flux, case.gamma,
+                                    case.delta, 0.0)
+    diag, src = finalize(case, up, lo, dg, dv)
     pat = O.build_pattern(case.n, case.owner, case.neighbour)
-    return O.Hierarchy(O.ldu_to_csr(pat, diag, up, lo), theta=THETA)
+    a = O.ldu_to_csr(pat, diag, up, lo)
+    if RX.available():
+        return RX.RefAmg(a, theta=THETA)
+    return O.Hierarchy(a, theta=THETA)
 
 
 def run_reference(args, cfg_name, case, desc):
     cores = os.cpu_count() or 1
-    hier = oracle_hierarchy(case)
+    if case is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference host library (oracle/_ref) not built"}))
+        return
+    hier = reference_hierarchy(case)
     step = reference_solver(case, hier)
     if step is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference host library not built"}))
@@ -235,7 +269,8 @@ def run_reference(args, cfg_name, case, desc):
     total = sum(times)
     value = args.steps / total
     sample = (f"{args.steps} full pressure solves (assembly + AMG-PCG to 1e-8) of the "
-              f"{cfg_name} workload, {iters[-1]} iterations each")
+              f"{cfg_name} workload, {iters[-1]} iterations each; mesh, FV geometry and AMG setup "
+              "by the reference's own sources (untimed)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -536,7 +571,7 @@ def cpu_baseline(case):
         import oracle as O
         if O.ref() is None:
             return None, None
-        hier = oracle_hierarchy(case)
+        hier = reference_hierarchy(case)
         step = reference_solver(case, hier)
         step()
         t0 = time.perf_counter()
@@ -1075,8 +1110,8 @@ def main():
             print(json.dumps({"impl": "reference", "unavailable": "the reference solves one system at a "
                               "time; its host solver is timed per system by --config graded|tet|cavity"}))
             return
-        case, desc = make_case(args.config, size)
-        run_reference(args, f"{args.config}{case.mesh.shape[0]}^3", case, desc)
+        case, desc = make_reference_case(args.config, size)
+        run_reference(args, f"{args.config}{size or DEFAULT_SIZE[args.config]}^3", case, desc)
         return
     if world > 1:
         import datetime
@@ -1101,7 +1136,7 @@ def main():
 
 def run_case(args, rank, world, local_rank, size):
     case, desc = make_case(args.config, size)
-    cfg_name = f"{args.config}{case.mesh.shape[0]}^3"
+    cfg_name = f"{args.config}{size or DEFAULT_SIZE[args.config]}^3"
     if args.profile_only:
         args.no_e2e = True
         args.no_cpu_baseline = True

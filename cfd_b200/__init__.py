@@ -486,12 +486,41 @@ def solve_amg_cg(amg: AmgView, b, x, control: SolveControl) -> SolveStats:
     return SolveStats._from(st)
 
 
+def _noalloc_args(args):
+    """The torch tensor arguments of solve_device_noalloc, (tensor, name, dtype, length), checked
+    for the element type the kernels read, then layout, then device, then length. Raw integer
+    pointers are the caller's responsibility (the library still checks where they point and the
+    CSR structure)."""
+    import torch
+    ts = [a for a in args if not isinstance(a[0], int)]
+    for t, name, _, _ in ts:
+        if not isinstance(t, torch.Tensor):
+            raise InvalidArgument(f"{name}: a torch CUDA tensor or a raw device pointer is required")
+    for t, name, dt, _ in ts:
+        if t.dtype != getattr(torch, dt):
+            raise InvalidArgument(f"{name} must be torch.{dt}, got {t.dtype}")
+    for t, name, _, _ in ts:
+        if not t.is_contiguous():
+            raise InvalidArgument(f"{name} must be contiguous")
+    for t, name, _, _ in ts:
+        if not t.is_cuda or t.device.index != torch.cuda.current_device():
+            raise InvalidArgument(f"{name} must be on the current CUDA device")
+    for t, name, _, ln in ts:
+        if t.numel() < ln:
+            raise InvalidArgument(f"{name} holds {t.numel()} elements, {ln} needed")
+
+
 @_stream_ordered
 def solve_device_noalloc(n, nnz, row_ptr, col, val, b, x, method: Method,
                          control: SolveControl) -> SolveStats:
     """Jacobi-preconditioned CG that allocates no device memory: every array is the caller's
     device memory (torch CUDA tensors or raw pointers), work vectors live in the library's
-    static device array (at most 65,536 rows). For callers that cannot call cudaMalloc."""
+    static device array (at most 65,536 rows). For callers that cannot call cudaMalloc.
+    Tensors must be row_ptr / col int32, val / b / x float64, contiguous, on the current
+    device; the call runs on the legacy default stream after torch's current stream is done."""
+    n, nnz = int(n), int(nnz)
+    _noalloc_args(((row_ptr, "row_ptr", "int32", n + 1), (col, "col", "int32", nnz),
+                   (val, "val", "float64", nnz), (b, "b", "float64", n), (x, "x", "float64", n)))
     cs = CsrStruct(int(n), int(nnz), C.cast(_devptr(row_ptr), _pi), C.cast(_devptr(col), _pi),
                    C.cast(_devptr(val), _pd))
     st = StatsStruct()

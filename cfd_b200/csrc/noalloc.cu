@@ -16,14 +16,26 @@
 //    cudaGetSymbolAddress (host code must not pass the symbol itself to a kernel); make that
 //    first call before any stream capture;
 //  * every call shares the array and leaves its last contents there; calls that overlap on the
-//    GPU (for example from two host threads at once) race and must be serialised by the caller.
+//    GPU (for example from two host threads at once) race and must be serialised by the caller;
+//  * it runs on the legacy default stream: a caller that wrote a, b or x on a non-blocking
+//    stream must finish those writes (synchronise that stream) before the call;
+//  * the arrays must be device memory of the current device (or managed memory), and the CSR
+//    structure is checked on the device before use (row offsets, then column indices).
 #include "../../include/cfdb.h"
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 #include <string>
 
 #include "common.hpp"
+#include "pointer_rule.hpp"
+
+static_assert(static_cast<int>(cudaMemoryTypeUnregistered) == cfdb::kPtrUnregistered &&
+                  static_cast<int>(cudaMemoryTypeHost) == cfdb::kPtrHost &&
+                  static_cast<int>(cudaMemoryTypeDevice) == cfdb::kPtrDevice &&
+                  static_cast<int>(cudaMemoryTypeManaged) == cfdb::kPtrManaged,
+              "cudaMemoryType values");
 
 namespace cfdb {
 void set_thread_error(const std::string& msg); // capi.cu
@@ -34,11 +46,13 @@ namespace {
 constexpr int kNaMaxRows = 65536;
 constexpr int kNaBlock = 256;
 constexpr int kNaMaxBlocks = kNaMaxRows / kNaBlock;
-// Layout in doubles: dinv | r | z | p | q | partial sums (one per block) | spare.
+// Layout in doubles: dinv | r | z | p | q | partial sums (one per block) | scalars (32 slots:
+// slot 0 the reduced scalar, slots 8.. the validation flags as ints).
 constexpr size_t kNaVec = static_cast<size_t>(kNaMaxRows);
 constexpr size_t kNaOffPart = 5 * kNaVec;
 constexpr size_t kNaOffScalar = kNaOffPart + kNaMaxBlocks;
 constexpr size_t kNaDoubles = kNaOffScalar + 32;
+constexpr size_t kNaFlagSlot = 8;
 
 static __device__ __align__(256) double g_na_scratch[kNaDoubles];
 
@@ -85,6 +99,28 @@ __device__ __forceinline__ void na_block_sum(double v, double* part) {
         v = threadIdx.x < kNaBlock / 32 ? sh[threadIdx.x] : 0.0;
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (threadIdx.x == 0) part[blockIdx.x] = v;
+    }
+}
+
+// CSR structure checks before any kernel reads through the caller's indices. Rows: every
+// row_ptr entry in [0, nnz], non-decreasing, row_ptr[0] = 0 and row_ptr[n] = nnz (flag bit 1).
+__global__ void k_na_check_rows(int n, int nnz, const int* __restrict__ rp, int* flag) {
+    const int i = blockIdx.x * kNaBlock + threadIdx.x;
+    if (i > n) return;
+    const int v = rp[i];
+    bool bad = v < 0 || v > nnz || (i == 0 && v != 0) || (i == n && v != nnz);
+    if (i < n) bad = bad || rp[i + 1] < v;
+    if (bad) atomicOr(flag, 1);
+}
+
+// Columns (run only once the rows passed): every column index in [0, n) (flag bit 2).
+__global__ void k_na_check_cols(int n, int nnz, const int* __restrict__ ci, int* flag) {
+    for (int k = blockIdx.x * kNaBlock + threadIdx.x; k < nnz; k += gridDim.x * kNaBlock) {
+        const int c = ci[k];
+        if (c < 0 || c >= n) {
+            atomicOr(flag, 2);
+            return;
+        }
     }
 }
 
@@ -179,13 +215,14 @@ void check(cudaError_t e, const char* what) {
     }
 }
 
-bool is_device_pointer(const void* p) {
+// Device memory of the current device, or managed memory.
+bool usable_here(const void* p, int dev) {
     cudaPointerAttributes at{};
     if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
         (void)cudaGetLastError();
         return false;
     }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+    return cfdb::pointer_usable_on(static_cast<int>(at.type), at.device, dev);
 }
 
 } // namespace
@@ -212,12 +249,13 @@ extern "C" int cfdb_solve_device_noalloc(const cfdb_csr* a, const double* b, dou
             if (stats) *stats = cfdb_stats{0, 0.0, 1, 1, 0.0};
             return CFDB_OK;
         }
-        if (!is_device_pointer(a->row_ptr) || !is_device_pointer(a->col) || !is_device_pointer(a->val) ||
-            !is_device_pointer(b) || !is_device_pointer(x)) {
-            cfdb::fail(CFDB_ERR_BAD_ARG, "cfdb_solve_device_noalloc: every array must be device memory");
-        }
         int dev = 0;
         check(cudaGetDevice(&dev), "cudaGetDevice");
+        if (!usable_here(a->row_ptr, dev) || !usable_here(a->col, dev) || !usable_here(a->val, dev) ||
+            !usable_here(b, dev) || !usable_here(x, dev)) {
+            cfdb::fail(CFDB_ERR_BAD_ARG, "cfdb_solve_device_noalloc: every array must be device memory of the "
+                                         "current device (device " + std::to_string(dev) + ") or managed memory");
+        }
         double* base = scratch_base(dev);
         const int n = a->n;
         double* dinv = base;
@@ -237,6 +275,23 @@ extern "C" int cfdb_solve_device_noalloc(const cfdb_csr* a, const double* b, dou
             check(cudaStreamSynchronize(s), "synchronize");
             return h;
         };
+        // validate the CSR structure on the device (flags in the scratch; no allocation)
+        int* flag = reinterpret_cast<int*>(scalar + kNaFlagSlot);
+        check(cudaMemsetAsync(flag, 0, sizeof(int), s), "clear flag");
+        k_na_check_rows<<<(n + kNaBlock) / kNaBlock, kNaBlock, 0, s>>>(n, a->nnz, a->row_ptr, flag);
+        int hflag = 0;
+        check(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s), "copy flag");
+        check(cudaStreamSynchronize(s), "synchronize");
+        if (hflag == 0 && a->nnz > 0) {
+            const int cblocks = std::min((a->nnz + kNaBlock - 1) / kNaBlock, 1184);
+            k_na_check_cols<<<cblocks, kNaBlock, 0, s>>>(n, a->nnz, a->col, flag);
+            check(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s), "copy flag");
+            check(cudaStreamSynchronize(s), "synchronize");
+        }
+        if (hflag & 1)
+            cfdb::fail(CFDB_ERR_BAD_ARG, "cfdb_solve_device_noalloc: row_ptr is not a valid CSR row offset array "
+                                         "(row_ptr[0] = 0, non-decreasing, row_ptr[n] = nnz)");
+        if (hflag & 2) cfdb::fail(CFDB_ERR_BAD_ARG, "cfdb_solve_device_noalloc: a column index is outside [0, n)");
         cfdb_stats st{0, 0.0, 0, 1, 0.0};
         // krylov_kernels.inc:44-95
         k_na_init<<<blocks, kNaBlock, 0, s>>>(m, b, x, dinv, r, part);

@@ -142,7 +142,10 @@ int cfdb_solve_amg_cg(const cfdb_amg_view* amg, const double* b, double* x,
  * rejected with CFDB_ERR_BAD_ARG). The first call on each device resolves that array's address
  * and should come before any stream capture. Calls share the array: calls that overlap on the
  * GPU race. Same iteration and stopping rule as cfdb_solve; runs on the legacy default
- * stream and returns when the solve is done. */
+ * stream and returns when the solve is done, so a caller that wrote a, b or x on a
+ * non-blocking stream must finish those writes first. Every array must be device memory of the
+ * current device (or managed memory); the CSR structure (row offsets, column range) is checked
+ * on the device before use, and a bad one is rejected with CFDB_ERR_BAD_ARG. */
 int cfdb_solve_device_noalloc(const cfdb_csr* a, const double* b, double* x, int method,
                               const cfdb_control* control, cfdb_stats* stats);
 

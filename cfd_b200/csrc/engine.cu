@@ -1062,7 +1062,7 @@ template <class T> void Engine::launch_tail(cudaStream_t s) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     CFDB_CUDA(cudaLaunchKernelEx(&cfg, k_vc_tail<T>, ph, count, cb_, n_ctiles_, b_lv, x_lv,
-                                 static_cast<const int*>(block_level_), tail_bar_, error_));
+                                 static_cast<const int*>(block_level_), tail_bar_, error_, tuning_.wait_polls));
 }
 
 template <class T>
@@ -1164,7 +1164,7 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
         mark("restrict", l, spmv_b(d.r, nx.n_rows, n) + (next_x1 ? 2.0 * sv * nx.n_rows_nc : 0.0));
     }
     // ---- coarsest blocks (dense inverse of each multi-level system's coarsest operator) ----
-    const Control ctl{n_active_, error_};
+    const Control ctl{n_active_, error_, tuning_.wait_polls};
     const int ord = ordered_ ? 1 : 0;
     if (lt < L) {
         launch_tail<T>(s);
@@ -1200,7 +1200,7 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
             if (l == 0 && last && fused_final) {
                 with_visit(krylov_visit(), [&](auto V) {
                     launch_k(tuning_.pdl != 0, k_vc_jacobi_final<T, decltype(V)::value>, d.n_tiles_nc, kBlock, 0, s, 
-                        A(0), d.tiles, st_, WD(0), r_, c, o, q_, red_, Control{n_active_, error_}, flexible);
+                        A(0), d.tiles, st_, WD(0), r_, c, o, q_, red_, Control{n_active_, error_, tuning_.wait_polls}, flexible);
                 });
                 mark("smooth_dot", l, spmv_b(d.a, n, n) + sv * n + sb * n + (flexible ? 8.0 * n : 0.0));
             } else if (l == 0) {
@@ -1223,7 +1223,7 @@ void Engine::enqueue_vcycle(Mode mode, bool fused_final, int flexible, bool x1_r
 // Preconditioner output z (level-0 iterate) in the precision of the mode.
 void Engine::enqueue_init(Mode mode) {
     const DevLevel& d = lv_[0];
-    const Control ctl{n_active_, error_};
+    const Control ctl{n_active_, error_, tuning_.wait_polls};
     const double n = d.n_rows;
     const double a0 = static_cast<double>(d.a.nnz) * 12.0 + 4.0 * (n + 1.0) + 16.0 * n;
     const X1Out x1o = x1_out(mode);
@@ -1244,7 +1244,7 @@ void Engine::enqueue_init(Mode mode) {
 
 void Engine::enqueue_rz(Mode mode, int flexible) {
     const DevLevel& d = lv_[0];
-    const Control ctl{n_active_, error_};
+    const Control ctl{n_active_, error_, tuning_.wait_polls};
     const double n = d.n_rows;
     if (mode == Mode::AmgMixed) {
         launch_k(tuning_.pdl != 0, k_cg_rz<float>, d.n_tiles, kBlock, 0, stream_, d.tiles, st_, r_, d.x32, nullptr, dinv0_, q_, red_, ctl, flexible);
@@ -1257,7 +1257,7 @@ void Engine::enqueue_rz(Mode mode, int flexible) {
 
 void Engine::enqueue_iteration(Mode mode) {
     const DevLevel& d = lv_[0];
-    const Control ctl{n_active_, error_};
+    const Control ctl{n_active_, error_, tuning_.wait_polls};
     const double n = d.n_rows;
     const double a0 = static_cast<double>(d.a.nnz) * 12.0 + 4.0 * (n + 1.0) + 16.0 * n;
     if (mode == Mode::AmgMixed) {
@@ -1457,8 +1457,12 @@ std::vector<SolveResult> Engine::solve(Mode mode, const std::vector<SolveRequest
     int err = 0;
     CFDB_CUDA(cudaMemcpy(&err, error_, sizeof(int), cudaMemcpyDeviceToHost));
     if (err != 0) {
+        // an expired grid barrier leaves stale arrival counts: reset them with the flag, so
+        // the next solve starts from a clean state
         CFDB_CUDA(cudaMemset(error_, 0, sizeof(int)));
-        fail(6, "solve: a bounded device wait expired (coarse-level staging)");
+        if (tail_bar_ != nullptr) CFDB_CUDA(cudaMemset(tail_bar_, 0, 2 * sizeof(unsigned)));
+        fail(6, err == 2 ? "solve: a bounded device wait expired (persistent-tail grid barrier)"
+                         : "solve: a bounded device wait expired (coarse-level staging)");
     }
     // true residual for reporting
     const DevLevel& d = lv_[0];

@@ -48,6 +48,7 @@ struct Tuning {
     int tail_rows = 0;          // coarse levels of at most this many rows (and everything below
                                 // them) run as one persistent tail kernel; 0 disables it
     int pdl = 1;                // programmatic dependent launch between consecutive kernels
+    int wait_polls = 1 << 22;   // poll limit of the bounded device waits (< 0: give up at once)
 };
 
 struct SolveRequest {

@@ -92,7 +92,12 @@ struct SysState {
 struct Control {
     int* n_active;   // number of active systems (device)
     int* error;      // device error flag (bounded waits)
+    int wait_polls = 1 << 22; // poll limit of the bounded waits (< 0: give up at once)
 };
+
+// Polls allowed to drain a CTA's own bulk copy after its bounded wait expired: the CTA must
+// not exit while the copy can still write its shared memory.
+constexpr int kDrainPolls = 1 << 22;
 
 // ---------------------------------------------------------------------------------------------
 // helpers
@@ -750,16 +755,22 @@ static __global__ void __launch_bounds__(kBlock) k_vc_coarse(CoarseBlocks cb, co
         }
     }
     // bounded wait on phase 0
-    uint32_t ok = 0;
-    for (int spin = 0; spin < (1 << 22) && !ok; ++spin) {
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(ok)
-            : "r"(smem_u32(&bar)), "r"(0)
-            : "memory");
-    }
-    if (!ok) {
+    auto wait_phase0 = [&](int polls) {
+        uint32_t done = 0;
+        for (int spin = 0; spin < polls && !done; ++spin) {
+            asm volatile(
+                "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                : "=r"(done)
+                : "r"(smem_u32(&bar)), "r"(0)
+                : "memory");
+        }
+        return done != 0;
+    };
+    if (!wait_phase0(ctl.wait_polls)) {
         if (threadIdx.x == 0) atomicExch(ctl.error, 1);
+        // the expired wait must not leave the bulk copy writing this CTA's shared memory after
+        // it exits: drain it (bounded too), then return
+        (void)wait_phase0(kDrainPolls);
         return;
     }
     if (ordered) {
@@ -1255,11 +1266,10 @@ template <class T> struct TailPhase {
     int n1;
 };
 
-constexpr int kTailSpinLimit = 1 << 22;
-
 // Grid-wide barrier over `nblocks` co-resident CTAs: bar[0] counts arrivals, bar[1] is the
-// generation. Bounded: returns false (error flag set) if the generation does not move.
-__device__ __forceinline__ bool tail_barrier(unsigned* bar, unsigned nblocks, int* error) {
+// generation. Bounded by `limit` polls (< 0: none): returns false (error flag set) if the
+// generation does not move. After an expiry the counters are stale; the host resets them.
+__device__ __forceinline__ bool tail_barrier(unsigned* bar, unsigned nblocks, int* error, int limit) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1273,7 +1283,7 @@ __device__ __forceinline__ bool tail_barrier(unsigned* bar, unsigned nblocks, in
             atomicAdd(&bar[1], 1u);
         } else {
             for (int spin = 0; *gen == g0; ++spin) {
-                if (spin >= kTailSpinLimit) {
+                if (spin >= limit) {
                     good = 0;
                     atomicExch(error, 2);
                     break;
@@ -1310,7 +1320,7 @@ static __global__ void __launch_bounds__(kBlock, 4) k_vc_tail(const TailPhase<T>
                                                     CoarseBlocks cb, int n_ctiles, T* const* __restrict__ b_level,
                                                     T* const* __restrict__ x_level,
                                                     const int* __restrict__ block_level, unsigned* bar,
-                                                    int* error) {
+                                                    int* error, int wait_polls) {
     extern __shared__ __align__(16) unsigned char tail_smem[];
     for (int ph = 0; ph < n_phases; ++ph) {
         const TailPhase<T> P = phases[ph];
@@ -1358,7 +1368,7 @@ static __global__ void __launch_bounds__(kBlock, 4) k_vc_tail(const TailPhase<T>
                 }
             });
         }
-        if (ph + 1 < n_phases && !tail_barrier(bar, gridDim.x, error)) return;
+        if (ph + 1 < n_phases && !tail_barrier(bar, gridDim.x, error, wait_polls)) return;
     }
 }
 

@@ -8,7 +8,12 @@
 // Errors are thrown as the reference throws them: std::invalid_argument for bad arguments
 // (krylov.hpp callers rely on it for an empty hierarchy, device_solver.cpp:89) and
 // std::runtime_error("CUDA ...") for device failures (krylov_cuda.cu:18-22).
-// Not provided: solve_host / solve_amg_cg_host (the reference's host-thread path).
+//
+// The reference's host-thread path (solve_host, solve_amg_cg_host and the detail:: host
+// functions, krylov.hpp:41-42, 63-64, 125-136) is the reference's CPU code, not a GPU fallback:
+// libcfdb.so does not implement it. A drop-in build links the reference's own
+// src/gpu/src/krylov_openmp.cpp object beside libcfdb.so; it defines solve_host and the
+// detail:: functions, and solve_amg_cg_host below forwards to it as dispatch.cpp:25-28 does.
 #pragma once
 
 #include <memory>
@@ -47,6 +52,11 @@ struct SolveStats {
 SolveStats solve(const CsrView& a, const double* b, double* x, Method method,
                  const SolveControl& control);
 
+// krylov.hpp:41-42: the same algorithms on host threads -- defined by the reference's
+// krylov_openmp.cpp (linked beside libcfdb.so), not by libcfdb.so.
+SolveStats solve_host(const CsrView& a, const double* b, double* x, Method method,
+                      const SolveControl& control);
+
 // krylov.hpp:48-58
 struct AmgLevelView {
     CsrView a;
@@ -63,6 +73,28 @@ struct AmgView {
 // krylov.hpp:61-62
 SolveStats solve_amg_cg(const AmgView& amg, const double* b, double* x,
                         const SolveControl& control);
+
+// krylov.hpp:125-136: the reference's host implementation, defined by its krylov_openmp.cpp.
+namespace detail {
+SolveStats solve_openmp(const CsrView& a, const double* b, double* x, Method method,
+                        const SolveControl& control);
+SolveStats solve_openmp(const CsrView& a, const double* b, double* x, Method method,
+                        const SolveControl& control, bool allow_device);
+bool openmp_device_available();
+SolveStats solve_amg_openmp(const AmgView& amg, const double* b, double* x,
+                            const SolveControl& control, bool allow_device);
+void assemble_openmp(int n_cells, int n_faces, const int* owner, const int* neighbour,
+                     const double* flux, const double* gamma, const double* delta_coeff,
+                     double convection, double* upper, double* lower, double* diag,
+                     double* divergence);
+} // namespace detail
+
+// krylov.hpp:63-64: AMG-PCG on host threads, through the reference's krylov_openmp.cpp (the
+// one-line forwarder of dispatch.cpp:25-28).
+inline SolveStats solve_amg_cg_host(const AmgView& amg, const double* b, double* x,
+                                    const SolveControl& control) {
+    return detail::solve_amg_openmp(amg, b, x, control, false);
+}
 
 // krylov.hpp:68-77
 struct LduPattern {

@@ -387,6 +387,11 @@ typedef struct {
                          where every slice / row spans fewer than 65536 columns, default 0 */
     int pdl;          /* programmatic dependent launch between consecutive kernels (a kernel is
                          scheduled while its predecessor drains), default 1 */
+    int wait_polls;   /* poll limit of the bounded device waits (coarse-level staging barrier,
+                         persistent-tail grid barrier), default 2^22 (0 = default); a negative value
+                         makes every such wait give up at once, which the tests of the expiry path
+                         (CFDB_ERR_TIMEOUT) use. An expired staging wait still drains its own
+                         copy before the CTA exits. */
 } cfdb_tuning;
 void cfdb_default_tuning(cfdb_tuning* t);
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t);

@@ -124,3 +124,34 @@ def test_ragged_batch_with_converged_and_tiny_systems(gpu):
         c = cases[i]
         a = O.ldu_to_csr(O.build_pattern(c.n, c.owner, c.neighbour), sysd[i][2], sysd[i][0], sysd[i][1])
         assert np.linalg.norm(src[i] - a.matvec(xs[off[i]:off[i + 1]])) <= 1.05e-8 * np.linalg.norm(src[i])
+
+
+@pytest.mark.parametrize("precision", ["FP64", "MIXED"])
+@pytest.mark.parametrize("tail", [0, 10 ** 6], ids=["coarse-staging-wait", "tail-grid-barrier"])
+def test_expired_device_wait_reports_timeout_and_recovers(gpu, tail, precision):
+    """Every device-side wait is bounded. With the poll limit set to give up at once
+    (Tuning.wait_polls < 0) the waits expire -- the coarse kernel's wait for its bulk copy
+    (which it still drains before it exits) or the persistent tail's grid barrier -- and the
+    solve reports CFDB_ERR_TIMEOUT. With the default limit restored, the next solve is
+    bit-identical to one that never timed out (error flag and barrier counters reset)."""
+    cb = gpu
+    case = W.graded(20)
+    up, lo, diag, src = _system(case)
+    ds = cb.DeviceSolver(cb.build_csr_pattern(case.n, case.owner, case.neighbour))
+    ds.set_precision(getattr(cb.Precision, precision))
+    ds.setup_amg(diag, up, lo, cb.AmgSettings(strength_threshold=0.04))
+    ctl = cb.SolveControl(1e-8 * np.linalg.norm(src), 200)
+    ds.set_tuning(cb.Tuning(tail_rows=tail))
+    x_ref = np.zeros(case.n)
+    st_ref = ds.solve(diag, up, lo, src, x_ref, cb.Method.Cg, True, ctl)
+    assert st_ref.converged
+    ds.set_tuning(cb.Tuning(tail_rows=tail, wait_polls=-1))
+    with pytest.raises(cb.Timeout, match="bounded device wait expired"):
+        ds.solve(diag, up, lo, src, np.zeros(case.n), cb.Method.Cg, True, ctl)
+    ds.set_tuning(cb.Tuning(tail_rows=tail))
+    for _ in range(2):
+        x = np.zeros(case.n)
+        st = ds.solve(diag, up, lo, src, x, cb.Method.Cg, True, ctl)
+        assert st.converged and st.iterations == st_ref.iterations
+        assert np.array_equal(x, x_ref)
+    ds.close()

@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true",
                     help="timed solves only (no e2e / CPU baseline), e.g. under ncu")
+    ap.add_argument("--pipe", type=int, default=None,
+                    help="persistent SELL V-cycle kernels, CTAs per SM (Tuning.pipe; 0: one CTA per tile)")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="build and time one precision only (profiling runs)")
     return ap.parse_args()
@@ -307,6 +309,8 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
     def make_solver(precision):
         ds = cb.DeviceSolver(mesh=(n, case.owner, case.neighbour))
         ds.set_precision(precision)
+        if args.pipe is not None:
+            ds.set_tuning(cb.Tuning(pipe=args.pipe))
         return ds
 
     # setup: assemble once, build the hierarchy on the host (AmgPreconditioner::setup)

@@ -154,7 +154,7 @@ _proto("cfdb_fv_relax_device", [_vp, _vp, _vp, _d, _vp])
 class TuningStruct(C.Structure):
     _fields_ = [("target_tiles", _i), ("wide_row", _i), ("lanes_div", _i), ("fuse_first", _i),
                 ("sell_rows", _i), ("krylov_pair", _i), ("tail_rows", _i),
-                ("col16", _i), ("pdl", _i), ("wait_polls", _i)]
+                ("col16", _i), ("pdl", _i), ("wait_polls", _i), ("pipe", _i)]
 
 
 _proto("cfdb_default_tuning", [_P(TuningStruct)], None)
@@ -880,11 +880,13 @@ class Tuning:
     col16: int = 0
     pdl: int = 1
     wait_polls: int = 1 << 22  # bounded device waits; < 0 makes them give up at once (tests)
+    pipe: int = 0  # persistent SELL V-cycle kernels, CTAs per SM (0: one CTA per tile)
 
     def _c(self):
         return TuningStruct(int(self.target_tiles), int(self.wide_row), int(self.lanes_div),
                             int(self.fuse_first), int(self.sell_rows), int(self.krylov_pair),
-                            int(self.tail_rows), int(self.col16), int(self.pdl), int(self.wait_polls))
+                            int(self.tail_rows), int(self.col16), int(self.pdl), int(self.wait_polls),
+                            int(self.pipe))
 
 
 def _set_system_tuning(self, t: Tuning) -> None:

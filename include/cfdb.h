@@ -392,6 +392,10 @@ typedef struct {
                          makes every such wait give up at once, which the tests of the expiry path
                          (CFDB_ERR_TIMEOUT) use. An expired staging wait still drains its own
                          copy before the CTA exits. */
+    int pipe;         /* SELL V-cycle kernels (sweeps, residuals, restriction, prolongation) as
+                         persistent kernels of this many CTAs per SM that load the next row's
+                         columns and values while gathering for the current one; 0 (default):
+                         one CTA per tile. Results are bit-identical either way. */
 } cfdb_tuning;
 void cfdb_default_tuning(cfdb_tuning* t);
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t);

@@ -163,6 +163,7 @@ _proto("cfdb_batch_create", [_i, _pi, _pi, _pi, _pi, _P(_vp)])
 _proto("cfdb_batch_destroy", [_vp])
 _proto("cfdb_batch_sizes", [_vp, _P(C.c_longlong), _P(C.c_longlong)])
 _proto("cfdb_batch_setup_amg", [_vp, _pd, _pd, _pd, _P(AmgSettingsStruct)])
+_proto("cfdb_batch_setup_amg_device", [_vp, _vp, _vp, _vp, _P(AmgSettingsStruct), _i])
 _proto("cfdb_batch_set_precision", [_vp, _i])
 _proto("cfdb_batch_set_tuning", [_vp, _P(TuningStruct)])
 _proto("cfdb_batch_assemble_pressure_device", [_vp, _vp, _vp, _vp, _vp, _pi, _d, _vp, _vp, _vp,
@@ -930,8 +931,17 @@ class Batch:
 
     __del__ = close
 
-    def setup_amg(self, diag, upper, lower, settings: AmgSettings | None = None) -> None:
+    def setup_amg(self, diag, upper, lower, settings: AmgSettings | None = None, device: bool = False,
+                  concurrency: int = 0) -> None:
+        """AmgPreconditioner::setup of every system: on the host (OpenMP over systems; host
+        arrays) or on the device (device setup per system, `concurrency` systems at a time; CUDA
+        tensors), bit-identical either way."""
         s = (settings or AmgSettings())._c()
+        if device:
+            _torch_ready()
+            _check(_lib.cfdb_batch_setup_amg_device(self._h, _devptr(diag), _devptr(upper), _devptr(lower),
+                                                    C.byref(s), int(concurrency)))
+            return
         _check(_lib.cfdb_batch_setup_amg(self._h, _dp(_f64(diag)), _dp(_f64(upper)),
                                          _dp(_f64(lower)), C.byref(s)))
 

@@ -7,6 +7,7 @@
 #include <memory>
 #include <string>
 
+#include "dsetup.hpp"
 #include "engine.hpp"
 #include "host_algos.hpp"
 
@@ -223,6 +224,73 @@ int cfdb_batch_setup_amg(cfdb_batch* b, const double* diag, const double* upper,
             } catch (const std::exception& e) {
                 errs[s] = e.what();
             }
+        }
+        for (int s = 0; s < b->n_sys; ++s)
+            if (!errs[s].empty()) fail(CFDB_ERR_BAD_ARG, "system " + std::to_string(s) + ": " + errs[s]);
+        b->sweeps = st.sweeps;
+        b->weight = st.weight;
+        b->dirty = true;
+        ensure_batch_engine(b);
+    });
+}
+
+// The hierarchies of every system built on the device (amg_setup_device per system: strength
+// graph, smoothed prolongation, transpose and Galerkin products in CUDA kernels, aggregation on
+// the host), several systems at a time on their own streams and host threads, then copied into
+// the plan as the host build's are. Bit-identical to cfdb_batch_setup_amg. diag / upper / lower
+// are device arrays, concatenated in system order.
+int cfdb_batch_setup_amg_device(cfdb_batch* b, const double* diag, const double* upper, const double* lower,
+                                const cfdb_amg_settings* settings, int concurrency) {
+    return guarded_b([&] {
+        if (b == nullptr || diag == nullptr || (b->tf > 0 && (upper == nullptr || lower == nullptr)))
+            fail(CFDB_ERR_BAD_ARG, "cfdb_batch_setup_amg_device: null argument");
+        CFDB_CUDA(cudaSetDevice(b->device));
+        AmgSettings st;
+        if (settings != nullptr) {
+            st.theta = settings->strength_threshold;
+            st.max_levels = settings->max_levels;
+            st.coarse_size = settings->coarse_size;
+            st.sweeps = settings->smooth_sweeps;
+            st.weight = settings->jacobi_weight;
+            st.table_limit = settings->device_table_limit;
+        }
+        if (st.max_levels < 1) fail(CFDB_ERR_BAD_ARG, "max_levels must be >= 1");
+        const int workers = std::max(1, std::min(concurrency > 0 ? concurrency : 8, b->n_sys));
+        std::vector<std::string> errs(b->n_sys);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(workers)
+        for (int s = 0; s < b->n_sys; ++s) {
+            cudaStream_t cs = nullptr;
+            try {
+                CFDB_CUDA(cudaSetDevice(b->device));
+                CFDB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+                const LduPatternHost& p = b->pats[s];
+                DeviceHierarchy dh;
+                DevCsr a0;
+                a0.n_rows = a0.n_cols = p.n;
+                a0.nnz = p.nnz();
+                a0.rp = dh.mem.alloc<int>(p.row_ptr.size());
+                a0.ci = dh.mem.alloc<int>(std::max<size_t>(p.col.size(), 1));
+                a0.va = dh.mem.alloc<double>(std::max<size_t>(p.col.size(), 1));
+                int* pos = dh.mem.alloc<int>(static_cast<size_t>(p.n + 2 * p.n_faces) + 1);
+                CFDB_CUDA(cudaMemcpyAsync(a0.rp, p.row_ptr.data(), sizeof(int) * p.row_ptr.size(), cudaMemcpyHostToDevice, cs));
+                if (a0.nnz > 0)
+                    CFDB_CUDA(cudaMemcpyAsync(a0.ci, p.col.data(), sizeof(int) * p.col.size(), cudaMemcpyHostToDevice, cs));
+                CFDB_CUDA(cudaMemcpyAsync(pos, p.diag_pos.data(), sizeof(int) * p.n, cudaMemcpyHostToDevice, cs));
+                if (p.n_faces > 0) {
+                    CFDB_CUDA(cudaMemcpyAsync(pos + p.n, p.upper_pos.data(), sizeof(int) * p.n_faces, cudaMemcpyHostToDevice, cs));
+                    CFDB_CUDA(cudaMemcpyAsync(pos + p.n + p.n_faces, p.lower_pos.data(), sizeof(int) * p.n_faces,
+                                              cudaMemcpyHostToDevice, cs));
+                }
+                ldu_to_csr_values(p.n, p.n_faces, pos, pos + p.n, pos + p.n + p.n_faces, diag + b->coff[s],
+                                  p.n_faces > 0 ? upper + b->foff[s] : nullptr, p.n_faces > 0 ? lower + b->foff[s] : nullptr,
+                                  a0.va, cs);
+                amg_setup_device(a0, st, cs, dh);
+                b->hs[s] = std::make_shared<Hierarchy>(download_hierarchy(dh, /*with_a0=*/true, cs));
+                CFDB_CUDA(cudaStreamSynchronize(cs));
+            } catch (const std::exception& e) {
+                errs[s] = e.what();
+            }
+            if (cs != nullptr) cudaStreamDestroy(cs);
         }
         for (int s = 0; s < b->n_sys; ++s)
             if (!errs[s].empty()) fail(CFDB_ERR_BAD_ARG, "system " + std::to_string(s) + ": " + errs[s]);

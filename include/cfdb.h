@@ -420,6 +420,12 @@ int cfdb_batch_sizes(const cfdb_batch* b, long long* total_cells, long long* tot
  * systems in parallel on the host). */
 int cfdb_batch_setup_amg(cfdb_batch* b, const double* diag, const double* upper,
                          const double* lower, const cfdb_amg_settings* settings);
+/* The same hierarchies built on the device (the device setup of cfdb_amg_setup_device per
+ * system, `concurrency` systems at a time on their own streams; 0: 8), bit-identical to
+ * cfdb_batch_setup_amg. diag / upper / lower are device arrays. */
+int cfdb_batch_setup_amg_device(cfdb_batch* b, const double* diag, const double* upper,
+                                const double* lower, const cfdb_amg_settings* settings,
+                                int concurrency);
 int cfdb_batch_set_precision(cfdb_batch* b, int precision);
 int cfdb_batch_set_tuning(cfdb_batch* b, const cfdb_tuning* t);
 /* cfdb_system_assemble_pressure_device for every system (device arrays); ref_cell: host array

@@ -73,3 +73,41 @@ def test_batch_matches_single_solves(gpu, precision):
         assert np.linalg.norm(xi - xs) <= 1e-5 * np.linalg.norm(xs)
         co += c.n
         fo += c.n_faces
+
+
+@pytest.mark.parametrize("precision", ["FP64", "MIXED"])
+def test_batch_device_setup_equals_host_setup(gpu, precision):
+    """Batch hierarchies built on the device (cfdb_batch_setup_amg_device, several systems at a
+    time) equal the host build: the batched solves that follow are bit-identical."""
+    import torch
+    cb = gpu
+    cases = _cases()
+    nc, nf, own, nei, flux, gamma, delta, src0 = _concat(cases)
+    dev = torch.device("cuda")
+    T = lambda a: torch.as_tensor(a, dtype=torch.float64, device=dev)  # noqa: E731
+    out = []
+    for how in ("host", "device", "device1"):
+        b = cb.Batch(nc, nf, own, nei)
+        d_up, d_lo = torch.empty(b.total_faces, dtype=torch.float64, device=dev), torch.empty(b.total_faces, dtype=torch.float64, device=dev)
+        d_dg, d_src = torch.empty(b.total_cells, dtype=torch.float64, device=dev), torch.empty(b.total_cells, dtype=torch.float64, device=dev)
+        b.assemble_pressure_device(T(flux), T(gamma), T(delta), T(src0), d_up, d_lo, d_dg, d_src,
+                                   ref_cells=[0] * len(cases))
+        torch.cuda.synchronize()
+        s = cb.AmgSettings(strength_threshold=0.04)
+        if how == "host":
+            b.setup_amg(d_dg.cpu().numpy(), d_up.cpu().numpy(), d_lo.cpu().numpy(), s)
+        else:
+            b.setup_amg(d_dg, d_up, d_lo, s, device=True, concurrency=1 if how == "device1" else 0)
+        b.set_precision(getattr(cb.Precision, precision))
+        src = d_src.cpu().numpy()
+        co, tols = 0, []
+        for c in cases:
+            tols.append(1e-8 * np.linalg.norm(src[co:co + c.n]))
+            co += c.n
+        x = torch.zeros(b.total_cells, dtype=torch.float64, device=dev)
+        stats = b.solve_device(d_dg, d_up, d_lo, d_src, x, [cb.SolveControl(t, 300) for t in tols])
+        torch.cuda.synchronize()
+        out.append(([st.iterations for st in stats], x.cpu().numpy()))
+        b.close()
+    for its, x in out[1:]:
+        assert its == out[0][0] and np.array_equal(x, out[0][1])

@@ -23,6 +23,7 @@ over ranks.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -49,17 +50,17 @@ def parse():
     ap.add_argument("--tune-cache", default=None, help="batch: autotuner cache file")
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serve: arrival rates (1/s)")
     ap.add_argument("--requests", type=int, default=200, help="serve: requests per rate")
+    ap.add_argument("--repeats", type=int, default=3, help="serve: runs of every load point (spread reported)")
     ap.add_argument("--slots", type=int, default=4, help="serve: worker slots")
     ap.add_argument("--serve-pdl", type=int, default=0, help="serve: programmatic dependent launch (0/1)")
     ap.add_argument("--max-age", type=int, default=20,
                     help="serve: hierarchy rebuilt after this many solves of a mesh (AmgCache::max_age; 0: never)")
     ap.add_argument("--size", type=int, default=0, help="override the mesh edge length")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="default launch knobs and smoother schedule")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true",
                     help="timed solves only (no e2e / CPU baseline), e.g. under ncu")
-    ap.add_argument("--pipe", type=int, default=None,
-                    help="persistent SELL V-cycle kernels, CTAs per SM (Tuning.pipe; 0: one CTA per tile)")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="build and time one precision only (profiling runs)")
     return ap.parse_args()
@@ -309,8 +310,6 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
     def make_solver(precision):
         ds = cb.DeviceSolver(mesh=(n, case.owner, case.neighbour))
         ds.set_precision(precision)
-        if args.pipe is not None:
-            ds.set_tuning(cb.Tuning(pipe=args.pipe))
         return ds
 
     # setup: assemble once, build the hierarchy on the host (AmgPreconditioner::setup)
@@ -340,7 +339,7 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
             ds.setup_amg(b["dg"], b["up"], b["lo"], cb.AmgSettings(strength_threshold=THETA), device=True)
             setup_dev_s[k] = time.perf_counter() - t0
         setup_prof[k] = ds.setup_profile()
-    bnorm_ref = float(torch.linalg.norm(bufs["mixed"]["src"]).item())
+    bnorm_ref = float(torch.linalg.norm(next(iter(bufs.values()))["src"]).item())
     tol = 1e-8 * bnorm_ref
 
     def step(k):
@@ -349,6 +348,29 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
         b["x"].zero_()
         return ds.solve_device(b["dg"], b["up"], b["lo"], b["src"], b["x"], cb.Method.Cg, True,
                                cb.SolveControl(tol, 500))
+
+    # autotuner (cfd_b200/autotune.py), untimed: the launch knobs of each precision's plan on a
+    # fixed number of iterations; then, for the mixed path only, its smoother schedule on whole
+    # solves to the tolerance (the FP64 path keeps the reference's 2 sweeps, weight 0.7)
+    tuning = {}
+    if not args.no_tune:
+        from cfd_b200.autotune import tune, tune_smoother
+        for k, ds in solvers.items():
+            b = bufs[k]
+            stream = torch.cuda.ExternalStream(ds.stream(), device=dev)
+
+            def run_iterations(it, ds=ds, b=b):
+                b["x"].zero_()
+                ds.solve_device(b["dg"], b["up"], b["lo"], b["src"], b["x"], cb.Method.Cg, True,
+                                cb.SolveControl(0.0, it))
+
+            with torch.cuda.stream(stream):
+                best, rec = tune(ds, run_iterations, ds.stream(), f"{cfg_name}:{k}")
+                if k == "mixed":
+                    best, srec = tune_smoother(ds, lambda k=k: step(k).iterations, ds.stream(), base=best)
+                    rec = dict(rec, smoother=srec)
+            tuning[k] = {"tuning": dataclasses.asdict(best), "default_ms": rec.get("default_ms"),
+                         "ms": rec.get("ms"), "smoother": rec.get("smoother")}
 
     results = {}
     for k in [k for k in ("fp64", "mixed") if k in solvers]:
@@ -485,6 +507,7 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
         "ms_per_solve_with_host_rebuild_every_20": {
             k: out_prec[k]["ms_per_solve"] + 1e3 * out_prec[k]["setup_s_host"] / 20.0 for k in out_prec},
         "hbm_gbs": out_prec["mixed"]["hbm_gbs_solve"],
+        "autotuned": tuning,
         "roofline": roofline, "clocks": results["mixed"]["clocks"],
         "gpu_launches": results["mixed"]["launches"],
         "e2e": e2e, "cpu_baseline": cpu,
@@ -749,6 +772,23 @@ def run_batch(args, rank, world, local_rank):
 SERVE_METRIC = "served pressure solves/s at saturation (box/tet mix, 1e-8, mixed, warm starts)"
 
 
+def spread(runs):
+    """Median of each figure over repeated runs of one load point, with min / max beside it."""
+    out = {}
+    for k in runs[0]:
+        vals = [r[k] for r in runs if isinstance(r.get(k), (int, float)) and not isinstance(r.get(k), bool)]
+        if len(vals) == len(runs):
+            out[k] = statistics.median(vals)
+            out[k + "_min"] = min(vals)
+            out[k + "_max"] = max(vals)
+        elif isinstance(runs[0][k], bool):
+            out[k] = all(r[k] for r in runs)
+        else:
+            out[k] = runs[0][k]
+    out["runs"] = len(runs)
+    return out
+
+
 def run_serve(args, rank, world, local_rank):
     import torch
 
@@ -784,10 +824,14 @@ def run_serve(args, rank, world, local_rank):
         sampler = ClockSampler(local_rank) if label == "mixed" else None
         if sampler:
             sampler.start()
-        _, sat = S.run_load(srv, pool, 1e6, n_req, seed=11)  # all requests queued at once
-        sweep = [S.run_load(srv, pool, r, n_req, seed=12 + k)[1] for k, r in enumerate(rates)]
+        # every load point `repeats` times (different arrival seeds): median and spread
+        sat_runs = [S.run_load(srv, pool, 1e6, n_req, seed=11 + 100 * k)[1] for k in range(args.repeats)]
+        sweep = []
+        for i, r in enumerate(rates):
+            runs = [S.run_load(srv, pool, r, n_req, seed=12 + i + 100 * k)[1] for k in range(args.repeats)]
+            sweep.append(spread(runs))
         clocks = sampler.stop() if sampler else None
-        res[label] = {"saturated": sat, "sweep": sweep, "setup_s": setup, "clocks": clocks,
+        res[label] = {"saturated": spread(sat_runs), "sweep": sweep, "setup_s": setup, "clocks": clocks,
                       "info": srv.info()}
         srv.close()
     value = res["mixed"]["saturated"]["solves_per_s"]
@@ -801,7 +845,7 @@ def run_serve(args, rank, world, local_rank):
                    "tet_edges": list(W.SERVE_TET_EDGES), "tet_share": 0.25, "repeat_share": 0.3,
                    "slots": args.slots, "hbm_budget_gb": 150, "rates_hz": rates,
                    "max_age": args.max_age,
-                   "requests_per_rate": n_req, "strength_threshold": THETA,
+                   "requests_per_rate": n_req, "repeats": args.repeats, "strength_threshold": THETA,
                    "step": "one request: H2D of its matrix (new key) and rhs, hierarchy rebuilt on the "
                            "device when the mesh has served max_age solves, AMG-PCG to 1e-8, D2H of x",
                    "parallelism": f"replicas x{world}"},
@@ -1152,6 +1196,7 @@ def run_case(args, rank, world, local_rank, size):
     if args.profile_only:
         args.no_e2e = True
         args.no_cpu_baseline = True
+        args.no_tune = True
     run_ours(args, rank, world, local_rank, cfg_name, case, desc)
 
 

@@ -154,7 +154,8 @@ _proto("cfdb_fv_relax_device", [_vp, _vp, _vp, _d, _vp])
 class TuningStruct(C.Structure):
     _fields_ = [("target_tiles", _i), ("wide_row", _i), ("lanes_div", _i), ("fuse_first", _i),
                 ("sell_rows", _i), ("krylov_pair", _i), ("tail_rows", _i),
-                ("col16", _i), ("pdl", _i), ("wait_polls", _i), ("pipe", _i)]
+                ("col16", _i), ("pdl", _i), ("wait_polls", _i), ("mixed_sweeps", _i),
+                ("mixed_weight", _d)]
 
 
 _proto("cfdb_default_tuning", [_P(TuningStruct)], None)
@@ -881,13 +882,14 @@ class Tuning:
     col16: int = 0
     pdl: int = 1
     wait_polls: int = 1 << 22  # bounded device waits; < 0 makes them give up at once (tests)
-    pipe: int = 0  # persistent SELL V-cycle kernels, CTAs per SM (0: one CTA per tile)
+    mixed_sweeps: int = 0  # mixed precision: Jacobi sweeps per level (0: the hierarchy's)
+    mixed_weight: float = 0.0  # mixed precision: Jacobi weight (0: the hierarchy's)
 
     def _c(self):
         return TuningStruct(int(self.target_tiles), int(self.wide_row), int(self.lanes_div),
                             int(self.fuse_first), int(self.sell_rows), int(self.krylov_pair),
                             int(self.tail_rows), int(self.col16), int(self.pdl), int(self.wait_polls),
-                            int(self.pipe))
+                            int(self.mixed_sweeps), float(self.mixed_weight))
 
 
 def _set_system_tuning(self, t: Tuning) -> None:

@@ -9,14 +9,19 @@ The knobs are those of `Tuning` (include/cfdb.h, cfdb_tuning):
 * fuse_first   - first two Jacobi sweeps of the pre-smoothing fused into one kernel,
 * sell_rows    - rows per CTA of SELL operators (one row per thread per pass),
 * krylov_pair  - level-0 Krylov SpMV kernels take two rows per thread per pass, or one,
-* tail_rows    - coarse levels of at most this many rows run in one persistent kernel.
+* tail_rows    - coarse levels of at most this many rows run in one persistent kernel,
+* mixed_sweeps, mixed_weight - the smoother schedule of the mixed-precision V-cycle (Jacobi
+                 sweeps per level before and after the coarse correction, and the weight); the
+                 FP64 path keeps the hierarchy's (the reference's 2 sweeps, weight 0.7).
 
-The search is a coordinate descent from the defaults: each knob in turn is swept over its
-candidate values with the others fixed, the best value kept, and the pass repeated until no
-knob changes (at most `passes` passes). The objective is the device time of a fixed number of
-CG iterations (tolerance 0, so every system runs exactly `iterations` iterations) through the
-captured graphs of the real solve path, median of `reps` runs. Results are cached in a JSON
-file keyed by a workload signature.
+The launch knobs are searched by coordinate descent from the defaults: each knob in turn is
+swept over its candidate values with the others fixed, the best value kept, and the pass
+repeated until no knob changes (at most `passes` passes). Their objective is the device time of
+a fixed number of CG iterations (tolerance 0, so every system runs exactly `iterations`
+iterations) through the captured graphs of the real solve path, median of `reps` runs. The
+smoother schedule changes the iteration count, so its objective is the device time of whole
+solves to the caller's tolerance (`tune_smoother`). Results are cached in a JSON file keyed by
+a workload signature.
 """
 from __future__ import annotations
 
@@ -126,3 +131,40 @@ def tune(target, run_iterations, stream_handle, signature: str, cache_path: str 
         with open(cache_path, "w") as f:
             json.dump(cache, f, indent=1)
     return best, dict(rec, cached=False)
+
+
+# (sweeps, weight) candidates of the mixed-precision smoother schedule; (2, 0.7) is the
+# reference's AmgView default
+SMOOTHER_CANDIDATES = [(2, 0.7), (2, 0.85), (1, 0.85), (1, 0.7), (3, 0.85)]
+
+
+def tune_smoother(target, solve: Callable[[], int], stream_handle: int, base: Tuning | None = None,
+                  candidates=None, reps: int = 3):
+    """Picks the mixed-precision smoother schedule with the shortest device time of a whole
+    solve to the caller's tolerance. solve() runs one solve on the target's stream and returns
+    its iteration count. Installs the best schedule on top of `base` and returns
+    (tuning, record)."""
+    import torch
+    base = base or Tuning()
+    trace = []
+    best, best_ms = None, float("inf")
+    for sweeps, weight in candidates or SMOOTHER_CANDIDATES:
+        t = dataclasses.replace(base, mixed_sweeps=sweeps, mixed_weight=weight)
+        target.set_tuning(t)
+        stream = torch.cuda.ExternalStream(stream_handle)
+        solve()  # warm: graph capture for the new plan
+        times, iters = [], 0
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            iters = solve()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms = statistics.median(times)
+        trace.append({"sweeps": sweeps, "weight": weight, "ms": ms, "iterations": iters})
+        if ms < best_ms:
+            best, best_ms = t, ms
+    target.set_tuning(best)
+    return best, {"ms": best_ms, "trace": trace}

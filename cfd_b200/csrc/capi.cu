@@ -165,7 +165,8 @@ Tuning tuning_from(const cfdb_tuning* t) {
         fail(CFDB_ERR_BAD_ARG, "tuning: sell_rows must be a multiple of 256 in 256..4096");
     return Tuning{t->target_tiles, t->wide_row, t->lanes_div, t->fuse_first != 0 ? 1 : 0, t->sell_rows,
                   t->krylov_pair != 0 ? 1 : 0, t->col16 != 0 ? 1 : 0, std::max(t->tail_rows, 0), t->pdl != 0 ? 1 : 0,
-                  t->wait_polls == 0 ? Tuning{}.wait_polls : t->wait_polls, std::max(t->pipe, 0)};
+                  t->wait_polls == 0 ? Tuning{}.wait_polls : t->wait_polls, std::max(t->mixed_sweeps, 0),
+                  t->mixed_weight > 0.0 ? t->mixed_weight : 0.0};
 }
 
 } // namespace cfdb
@@ -1276,7 +1277,8 @@ void cfdb_default_tuning(cfdb_tuning* t) {
     t->col16 = d.col16;
     t->pdl = d.pdl;
     t->wait_polls = d.wait_polls;
-    t->pipe = d.pipe;
+    t->mixed_sweeps = d.mixed_sweeps;
+    t->mixed_weight = d.mixed_weight;
 }
 
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t) {

@@ -242,6 +242,13 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
     if (sweeps < 0) fail(1, "engine: negative smoothing sweeps");
     sweeps_ = sweeps;
     weight_ = weight;
+    // mixed precision (the FP32 V-cycle alone): its smoother schedule may differ from the
+    // hierarchy's (Tuning.mixed_sweeps / mixed_weight, picked by the autotuner); the FP64 path
+    // keeps the reference's schedule
+    if (need32 && !need64) {
+        if (tuning_.mixed_sweeps > 0) sweeps_ = tuning_.mixed_sweeps;
+        if (tuning_.mixed_weight > 0.0) weight_ = tuning_.mixed_weight;
+    }
     need64_ = need64;
     need32_ = need32;
     has_amg_ = true;
@@ -883,7 +890,6 @@ template <> Sell<float> vs_sel<float>(const Sell<double>&, const Sell<float>& b)
 // Calls fn with the visiting strategy v as a compile-time constant.
 template <class Fn> void with_visit(int v, Fn&& fn) {
     if (v == kVisitSell2) fn(std::integral_constant<int, kVisitSell2>{});
-    else if (v == kVisitSellPipe) fn(std::integral_constant<int, kVisitSellPipe>{});
     else if (v == kVisitSell1) fn(std::integral_constant<int, kVisitSell1>{});
     else if (v == kVisitWarp) fn(std::integral_constant<int, kVisitWarp>{});
     else fn(std::integral_constant<int, kVisitBlock>{});
@@ -1100,20 +1106,7 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
         int block;
         int visit;  // row-visiting strategy of the operator's kernels
     };
-    if (sm_count_ == 0) CFDB_CUDA(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_));
-    // SELL operators run persistent (kVisitSellPipe, tuning.pipe CTAs per SM) when the knob is
-    // on; every other operator, and SELL with the knob off, one CTA per tile
     auto TL = [&](int, const DevSell64_32& m, bool nc) -> Launch {
-        const int fmt = m.s64.val != nullptr ? m.s64.fmt : m.s32.fmt;
-        const int nt = nc ? m.n_tiles_nc : m.n_tiles;
-        Tiles t = m.tiles;
-        t.n = nt;
-        if (fmt == kFmtSell && tuning_.pipe > 0 && nt > 0 && !ordered_)
-            return {t, std::min(nt, sm_count_ * tuning_.pipe), m.block, kVisitSellPipe};
-        return {t, nt, m.block, visit_of(fmt)};
-    };
-    // the first pre-smoothing sweep keeps one CTA per tile (its unfused form is a plain row loop)
-    auto TL1 = [&](int, const DevSell64_32& m, bool nc) -> Launch {
         return {m.tiles, nc ? m.n_tiles_nc : m.n_tiles, m.block, visit_of(m.s64.val != nullptr ? m.s64.fmt : m.s32.fmt)};
     };
     std::vector<T*> cur(L, nullptr);
@@ -1147,11 +1140,10 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
             cur[l] = c;
         } else {
             const auto ta = TL(l, d.a, true);
-            const auto tf = TL1(l, d.a, true);
             if (l == 0) {
-                with_visit(tf.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_first<T, double, decltype(V)::value>, tf.second, tf.block, 0, s, A(l), tf.first, stv, WD(l), r_, start, fuse); });
+                with_visit(ta.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_first<T, double, decltype(V)::value>, ta.second, ta.block, 0, s, A(l), ta.first, stv, WD(l), r_, start, fuse); });
             } else {
-                with_visit(tf.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_first<T, T, decltype(V)::value>, tf.second, tf.block, 0, s, A(l), tf.first, stv, WD(l), Bv(l), start, fuse); });
+                with_visit(ta.visit, [&](auto V) { launch_k(tuning_.pdl != 0, k_vc_first<T, T, decltype(V)::value>, ta.second, ta.block, 0, s, A(l), ta.first, stv, WD(l), Bv(l), start, fuse); });
             }
             mark("smooth_first", l, fuse ? spmv_b(d.a, n, n) - sv * n + sv * n + sb * n : 2.0 * sv * n + sb * n);
             T* c = start;
@@ -1525,16 +1517,10 @@ double Engine::time_sweep(int level, int reps, double* bytes) {
     const bool fp32 = need32_;
     const DevSell64_32& m = d.a;
     const bool nc = level + 1 < n_levels_;
-    Tiles tiles = m.tiles;
-    tiles.n = nc ? m.n_tiles_nc : m.n_tiles;
-    int grid = tiles.n;
+    const Tiles tiles = m.tiles;
+    const int grid = nc ? m.n_tiles_nc : m.n_tiles;
     if (grid == 0) fail(1, "time_sweep: level has no operator tiles");
-    int visit = visit_of(m.s64.val != nullptr ? m.s64.fmt : m.s32.fmt);
-    if (sm_count_ == 0) CFDB_CUDA(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_));
-    if (visit == kVisitSell1 && tuning_.pipe > 0 && !ordered_) {
-        visit = kVisitSellPipe;
-        grid = std::min(grid, sm_count_ * tuning_.pipe);
-    }
+    const int visit = visit_of(m.s64.val != nullptr ? m.s64.fmt : m.s32.fmt);
     const double sv = fp32 ? 4.0 : 8.0;
     const double sb = level == 0 ? 8.0 : sv;
     const double n = d.n_rows_nc;

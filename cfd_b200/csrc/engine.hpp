@@ -49,9 +49,8 @@ struct Tuning {
                                 // them) run as one persistent tail kernel; 0 disables it
     int pdl = 1;                // programmatic dependent launch between consecutive kernels
     int wait_polls = 1 << 22;   // poll limit of the bounded device waits (< 0: give up at once)
-    int pipe = 0;               // SELL V-cycle kernels persistent with this many CTAs per SM,
-                                // the next row's loads in flight during the current row's
-                                // gathers (0: one CTA per tile)
+    int mixed_sweeps = 0;       // mixed precision: Jacobi sweeps per level (0: the hierarchy's)
+    double mixed_weight = 0.0;  // mixed precision: Jacobi weight (0: the hierarchy's)
 };
 
 struct SolveRequest {
@@ -201,8 +200,6 @@ private:
     void release_graphs();
 
     int device_;
-
-    int sm_count_ = 0;  // multiprocessors of the device (persistent grids)
     cudaStream_t stream_ = nullptr;
     StagedCopier copier_; // host-array uploads and downloads
     DeviceArena arena_;

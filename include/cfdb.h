@@ -392,10 +392,12 @@ typedef struct {
                          makes every such wait give up at once, which the tests of the expiry path
                          (CFDB_ERR_TIMEOUT) use. An expired staging wait still drains its own
                          copy before the CTA exits. */
-    int pipe;         /* SELL V-cycle kernels (sweeps, residuals, restriction, prolongation) as
-                         persistent kernels of this many CTAs per SM that load the next row's
-                         columns and values while gathering for the current one; 0 (default):
-                         one CTA per tile. Results are bit-identical either way. */
+    int mixed_sweeps; /* mixed precision only: Jacobi sweeps before and after the coarse
+                         correction on every level (0, default: the hierarchy's, 2 for the
+                         reference's AmgView); the FP64 path always keeps the hierarchy's */
+    double mixed_weight; /* mixed precision only: Jacobi weight (0, default: the hierarchy's,
+                         0.7); flexible CG tolerates any fixed schedule, and the autotuner picks
+                         the one with the shortest time to the tolerance */
 } cfdb_tuning;
 void cfdb_default_tuning(cfdb_tuning* t);
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t);

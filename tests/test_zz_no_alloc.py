@@ -96,5 +96,8 @@ def test_noalloc_rejects_oversize(gpu):
     va = torch.ones(1, dtype=torch.float64, device=dev)
     b = torch.ones(1, dtype=torch.float64, device=dev)
     x = torch.zeros(1, dtype=torch.float64, device=dev)
+    # raw device pointers: the C entry point itself refuses the size (tensors would already be
+    # refused by the wrapper's length checks)
     with pytest.raises(cb.InvalidArgument, match="maximum of 65536 rows"):
-        cb.solve_device_noalloc(65537, 1, rp, ci, va, b, x, cb.Method.Cg, cb.SolveControl())
+        cb.solve_device_noalloc(65537, 1, rp.data_ptr(), ci.data_ptr(), va.data_ptr(), b.data_ptr(),
+                                x.data_ptr(), cb.Method.Cg, cb.SolveControl())

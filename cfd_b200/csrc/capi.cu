@@ -1293,6 +1293,13 @@ int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t) {
     });
 }
 
+int cfdb_system_sizes(const cfdb_system* sys, int* n_cells, int* n_faces) {
+    if (sys == nullptr) return set_error(CFDB_ERR_BAD_ARG, "null system");
+    if (n_cells) *n_cells = sys->pat.n;
+    if (n_faces) *n_faces = sys->pat.n_faces;
+    return CFDB_OK;
+}
+
 int cfdb_system_stream(const cfdb_system* sys, void** stream) {
     if (sys == nullptr || stream == nullptr || !sys->eng) return set_error(CFDB_ERR_BAD_ARG, "null argument");
     *stream = sys->eng->stream();

@@ -427,6 +427,14 @@ int cfdb_fv_pressure_gradient_device(cfdb_fv* fv, const double* p, double* grad)
     });
 }
 
+int cfdb_fv_sizes(const cfdb_fv* fv, int* n_cells, int* n_faces, int* n_internal_faces) {
+    if (fv == nullptr) return CFDB_ERR_BAD_ARG;
+    if (n_cells) *n_cells = fv->n;
+    if (n_faces) *n_faces = fv->nf;
+    if (n_internal_faces) *n_internal_faces = fv->ni;
+    return CFDB_OK;
+}
+
 int cfdb_fv_delta_device(const cfdb_fv* fv, const double** delta) {
     if (fv == nullptr || delta == nullptr) return CFDB_ERR_BAD_ARG;
     *delta = fv->delta;

@@ -243,6 +243,8 @@ int cfdb_fv_create(int n_cells, int n_faces, int n_internal_faces, const int* ow
                    const int* neighbour, const double* face_areas, const double* face_centres,
                    const double* cell_centres, const double* cell_volumes, const double* weights,
                    const int* boundary_kind, const double* boundary_pressure, cfdb_fv** out);
+/* Cells, faces and internal faces of the geometry (no reference counterpart). */
+int cfdb_fv_sizes(const cfdb_fv* fv, int* n_cells, int* n_faces, int* n_internal_faces);
 int cfdb_fv_destroy(cfdb_fv* fv);
 /* grad (3 n_cells) of the cell pressure p (n_cells): Gauss sums with boundary values p_P, or
  * the outlet pressure, in two passes, the second extrapolating zero-gradient boundary values
@@ -312,6 +314,55 @@ int cfdb_system_solve_ldu(cfdb_system* sys, const double* diag, const double* up
                           const double* lower, const double* source, double* x,
                           const cfdb_ldu_settings* settings, const cfdb_amg_settings* amg,
                           int device_arrays, cfdb_ldu_result* result);
+
+/* ---- the whole pressure correction: FlowSolver::pressure_correction
+ * (src/fv/src/flow_solver.cpp:673-847) with every array in device memory ----
+ * HbyA / rAU from the momentum system, the predicted face flux and face rAU (with the
+ * relaxation-independent term when u_prev and phi_prev are given and alpha_u < 1), the pressure
+ * equation with boundary terms and reference cell, n_non_orth_correctors + 1 persistent LDU
+ * solves (cfdb_system_solve_ldu, AmgCache rule) with the non-orthogonal corrector sources, the
+ * conservative face flux, pressure relaxation and the velocity correction, in the reference's
+ * order, each step the device kernel bit-identical to the reference's loop. u (n x 3) and p (n)
+ * are updated in place; ws->phi receives the conservative flux. sys and fv must describe the
+ * same mesh (sys over its internal faces). The workspace is the caller's device memory, so the
+ * call allocates none of its own. results (optional, n_non_orth_correctors + 1 entries, host)
+ * and ws->solve_p / ws->solve_source (optional, (n_non_orth_correctors + 1) x n each) record
+ * every solve. Returns when the step is done. */
+typedef struct {
+    double alpha_u;            /* momentum under-relaxation (for the relaxation-independent term) */
+    double alpha_p;            /* pressure under-relaxation */
+    int n_non_orth_correctors;
+    int ref_cell;              /* -1: none (a case with a pressure outlet) */
+    double ref_value;
+    int relax_p;               /* 1: p = p_prev + alpha_p (p_new - p_prev); 0: p = p_new */
+    cfdb_ldu_settings p_solver;
+    cfdb_amg_settings amg;
+} cfdb_pressure_settings;
+typedef struct {
+    double* hbya;         /* n x 3 */
+    double* rau;          /* n */
+    double* phi_hbya;     /* n_faces */
+    double* rau_f;        /* n_faces */
+    double* upper;        /* n_internal_faces */
+    double* lower;        /* n_internal_faces */
+    double* diag;         /* n */
+    double* source;       /* n: right-hand side of the current solve */
+    double* base_source;  /* n: right-hand side before the corrector terms */
+    double* p_prev;       /* n */
+    double* p_new;        /* n */
+    double* non_orth;     /* max(n_internal_faces, 1) */
+    double* grad;         /* n x 3 */
+    double* phi;          /* n_faces: conservative face flux (output) */
+    double* solve_p;      /* optional */
+    double* solve_source; /* optional */
+} cfdb_pressure_workspace;
+int cfdb_pressure_correction_device(cfdb_system* sys, cfdb_fv* fv, const double* mom_diag,
+                                    const double* mom_upper, const double* mom_lower,
+                                    const double* mom_source, double* u, double* p,
+                                    const double* fixed_velocity, const double* u_prev,
+                                    const double* phi_prev, const cfdb_pressure_settings* settings,
+                                    const cfdb_pressure_workspace* ws, cfdb_ldu_result* results,
+                                    double* initial_residual);
 /* Fused pressure assembly on device arrays (flow_solver.cpp:757-783 with the face loop of
  * krylov_cuda.cu:681-697): from face flux / gamma / delta (n_faces) builds the device matrix
  * directly and returns upper, lower (n_faces) and diag, divergence (n_cells, accumulated)
@@ -404,6 +455,8 @@ int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t);
 
 /* Stream of the system (cudaStream_t as void*), for callers that order their own work. */
 int cfdb_system_stream(const cfdb_system* sys, void** stream);
+/* Cells and internal faces of the system's pattern. */
+int cfdb_system_sizes(const cfdb_system* sys, int* n_cells, int* n_faces);
 /* Device bytes held by the system (pattern, hierarchy, work vectors). */
 int cfdb_system_device_bytes(const cfdb_system* sys, size_t* bytes);
 

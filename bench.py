@@ -1109,11 +1109,15 @@ def run_step(args, rank, world, local_rank):
                            amg=cb.AmgSettings(strength_threshold=THETA))
     fix = T(ufix)
 
+    solves = []
+
     def step():
-        P.pressure_correction(ds, fv, *mom, u, p, fix, s, u_prev=u_prev, phi_prev=phi_prev, phi=phi)
+        P.pressure_correction(ds, fv, *mom, u, p, fix, s, u_prev=u_prev, phi_prev=phi_prev, phi=phi,
+                              results=solves)
 
     for _ in range(max(3, args.warmup)):
         step()
+    solves.clear()
     times = []
     sampler = ClockSampler(local_rank)
     sampler.start()
@@ -1136,6 +1140,9 @@ def run_step(args, rank, world, local_rank):
                            "p solver tolerance 1e-8 / rel 0.01, hierarchy rebuilt on the device every 20 CG solves",
                    "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
         "ms_min": min(times), "ms_median": sorted(times)[len(times) // 2], "ms_max": max(times),
+        "ms_per_step_each": times, "pressure_solves": len(solves),
+        "hierarchy_rebuilds": sum(1 for r in solves if r.amg_rebuilt),
+        "iterations_per_solve": [r.iterations for r in solves],
         "cpu_baseline": None,
         "cpu_baseline_note": "the reference's FlowSolver needs Eigen and is not built here",
         "clocks": clocks,

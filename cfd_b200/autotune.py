@@ -40,7 +40,7 @@ CANDIDATES = {
     "fuse_first": [0, 1],
     "sell_rows": [256, 512, 1024],
     "krylov_pair": [0, 1],
-    "tail_rows": [0, 1024, 8192],
+    "tail_rows": [0, 1024, 8192, 65536],
 }
 
 

@@ -49,6 +49,7 @@ struct Resident {
     double *d_diag = nullptr, *d_upper = nullptr, *d_lower = nullptr, *d_rhs = nullptr, *d_x = nullptr;
     long long matrix_key = -1;   // key of the LDU values on the device
     long long solution_key = -1; // key of the matrix the device solution belongs to
+    long long hier_key = -1;     // key of the matrix the hierarchy was built from
     int age = 0;                 // solves since the hierarchy was built
     bool busy = false;
     Clock::time_point last_use{};
@@ -176,12 +177,17 @@ void execute(cfdb_server& s, Resident& r, const Mesh& m, Request& q, bool create
         }
         r.matrix_key = q.key;
     }
-    if (created || (s.cfg.max_age > 0 && r.age >= s.cfg.max_age)) {
-        // hierarchy (re)build from this request's matrix (already on the device), as the
-        // reference's AmgCache does, with the sparse algebra on the GPU
+    // hierarchy (re)build from this request's matrix (already on the device), as the
+    // reference's AmgCache does after max_age solves, with the sparse algebra on the GPU; when the
+    // request's matrix is the one the hierarchy was built from, the rebuild would reproduce it bit
+    // for bit, so it waits for the next new matrix
+    const bool same_as_hierarchy = q.key >= 0 && r.hier_key == q.key;
+    const bool aged = s.cfg.max_age > 0 && r.age >= s.cfg.max_age && !same_as_hierarchy;
+    if (created || aged) {
         CFDB_CUDA(cudaStreamSynchronize(st));
         check(cfdb_system_setup_amg_device(r.sys, r.d_diag, r.d_upper, r.d_lower, &s.cfg.settings, 1));
         r.age = 0;
+        r.hier_key = q.key;
     }
     CFDB_CUDA(cudaMemcpyAsync(r.d_rhs, q.rhs, sizeof(double) * m.n, cudaMemcpyHostToDevice, st));
     if (!(q.warm && r.solution_key == q.key && q.key >= 0)) {

@@ -50,11 +50,12 @@ _lib.cfdb_pressure_correction_device.restype = C.c_int
 @_stream_ordered
 def pressure_correction(ds: DeviceSolver, fv: FvGeometry, mom_diag, mom_upper, mom_lower, mom_source,
                         u, p, fixed_velocity, settings: PressureSettings | None = None, relax_p=True,
-                        u_prev=None, phi_prev=None, phi=None, keep=None):
+                        u_prev=None, phi_prev=None, phi=None, keep=None, results=None):
     """One pressure correction on CUDA float64 tensors: u (n_cells x 3) and p (n_cells) are
     updated in place, phi (n_faces, optional) receives the conservative face flux. Returns the
     initial normalised residual of the first pressure solve. keep: a dict that receives the
-    workspace arrays and, under "solves", (result, p after, right-hand side) of every solve."""
+    workspace arrays and, under "solves", (result, p after, right-hand side) of every solve.
+    results: a list that receives the LduResult of every solve."""
     import torch
     s = settings or PressureSettings()
     n, nf, ni = fv.n_cells, fv.n_faces, fv.n_internal_faces
@@ -70,15 +71,17 @@ def pressure_correction(ds: DeviceSolver, fv: FvGeometry, mom_diag, mom_upper, m
     cs = PressureSettingsStruct(float(s.alpha_u), float(s.alpha_p), int(s.n_non_orth_correctors), int(s.ref_cell),
                                 float(s.ref_value), 1 if relax_p else 0, (s.p_solver or LduSettings())._c(),
                                 (s.amg or AmgSettings())._c())
-    results = (LduResultStruct * n_solves)()
+    res = (LduResultStruct * n_solves)()
     initial = C.c_double()
     ptr = lambda t: None if t is None else _devptr(t)  # noqa: E731
     _check(_lib.cfdb_pressure_correction_device(
         ds._h, fv._h, _devptr(mom_diag), _devptr(mom_upper), _devptr(mom_lower), _devptr(mom_source),
         _devptr(u), _devptr(p), ptr(fixed_velocity), ptr(u_prev), ptr(phi_prev), C.byref(cs), C.byref(wst),
-        results, C.byref(initial)))
+        res, C.byref(initial)))
+    out = [LduResult(r.initial_residual, r.final_residual, r.iterations, bool(r.amg_rebuilt)) for r in res]
+    if results is not None:
+        results.extend(out)
     if keep is not None:
         keep.update({k: v for k, v in ws.items() if k not in ("solve_p", "solve_source")})
-        keep["solves"] = [(LduResult(r.initial_residual, r.final_residual, r.iterations, bool(r.amg_rebuilt)),
-                           ws["solve_p"][k], ws["solve_source"][k]) for k, r in enumerate(results)]
+        keep["solves"] = [(r, ws["solve_p"][k], ws["solve_source"][k]) for k, r in enumerate(out)]
     return initial.value

@@ -24,7 +24,10 @@ typedef struct {
     double hbm_budget_bytes;    /* device bytes the resident systems may hold, default 150e9 */
     int precision;              /* cfdb_precision of the solves, default MIXED */
     cfdb_amg_settings settings; /* hierarchy settings */
-    int max_age;                /* rebuild the hierarchy after this many solves (0: never) */
+    int max_age;                /* rebuild the hierarchy after this many solves (0: never), as
+                                   the reference's AmgCache does; a request whose matrix is the
+                                   one the hierarchy was built from (same matrix_key) does not
+                                   trigger it, since the rebuild would reproduce the hierarchy */
     int pdl;                    /* programmatic dependent launch in the resident systems' solves
                                    (cfdb_tuning.pdl), default 0: with requests overlapping on
                                    the GPU, kernels scheduled early would hold SM slots that

@@ -52,12 +52,17 @@ def parse():
     ap.add_argument("--requests", type=int, default=200, help="serve: requests per rate")
     ap.add_argument("--repeats", type=int, default=3, help="serve: runs of every load point (spread reported)")
     ap.add_argument("--slots", type=int, default=4, help="serve: worker slots")
+    ap.add_argument("--serve-schedule", default="1,0.85",
+                    help="serve: mixed smoother schedule 'sweeps,weight' (the autotuned one of the tet box; "
+                         "'0,0' keeps the reference's)")
     ap.add_argument("--serve-pdl", type=int, default=0, help="serve: programmatic dependent launch (0/1)")
     ap.add_argument("--max-age", type=int, default=20,
                     help="serve: hierarchy rebuilt after this many solves of a mesh (AmgCache::max_age; 0: never)")
     ap.add_argument("--size", type=int, default=0, help="override the mesh edge length")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default launch knobs and smoother schedule")
+    ap.add_argument("--schedule", default=None,
+                    help="mixed smoother schedule 'sweeps,weight' without the autotuner (e.g. 1,0.85)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true",
                     help="timed solves only (no e2e / CPU baseline), e.g. under ncu")
@@ -310,6 +315,9 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
     def make_solver(precision):
         ds = cb.DeviceSolver(mesh=(n, case.owner, case.neighbour))
         ds.set_precision(precision)
+        if args.schedule and precision == cb.Precision.MIXED:
+            sw, w = args.schedule.split(",")
+            ds.set_tuning(cb.Tuning(mixed_sweeps=int(sw), mixed_weight=float(w)))
         return ds
 
     # setup: assemble once, build the hierarchy on the host (AmgPreconditioner::setup)
@@ -804,8 +812,9 @@ def run_serve(args, rank, world, local_rank):
     res = {}
 
     def server(prec, slots):
+        sched = tuple(float(v) for v in args.serve_schedule.split(","))
         srv = S.Server(slots=slots, hbm_budget_bytes=150e9, precision=prec, settings=settings,
-                       max_age=args.max_age, pdl=args.serve_pdl)
+                       max_age=args.max_age, pdl=args.serve_pdl, mixed_schedule=(int(sched[0]), sched[1]))
         pool = S.make_pool(srv, pool_cases, variants=3, seed=7)
         t0 = time.perf_counter()
         for e in pool:  # hierarchy builds (AmgCache setup), not timed below
@@ -844,6 +853,7 @@ def run_serve(args, rank, world, local_rank):
         "config": {"workload": "serve box/tet pool", "box_edges": list(W.SERVE_BOX_EDGES),
                    "tet_edges": list(W.SERVE_TET_EDGES), "tet_share": 0.25, "repeat_share": 0.3,
                    "slots": args.slots, "hbm_budget_gb": 150, "rates_hz": rates,
+                   "mixed_schedule": args.serve_schedule,
                    "max_age": args.max_age,
                    "requests_per_rate": n_req, "repeats": args.repeats, "strength_threshold": THETA,
                    "step": "one request: H2D of its matrix (new key) and rhs, hierarchy rebuilt on the "

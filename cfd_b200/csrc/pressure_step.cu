@@ -85,6 +85,11 @@ extern "C" int cfdb_pressure_correction_device(cfdb_system* sys, cfdb_fv* fv, co
         ok(cfdb_system_assemble_pressure_device(sys, w->phi_hbya, w->rau_f, delta, nullptr, w->base_source, -1, 0.0,
                                                 w->upper, w->lower, w->diag, w->source),
            "pressure assembly");
+        // the assembly is enqueued on the system's stream and returns at once: it must be done
+        // before the geometry's stream adds the boundary terms to the same diag and source
+        void* sys_stream = nullptr;
+        ok(cfdb_system_stream(sys, &sys_stream), "system stream");
+        CFDB_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(sys_stream)));
         ok(cfdb_fv_pressure_boundary_device(fv, w->phi_hbya, w->rau_f, s->ref_cell, s->ref_value, w->diag, w->source),
            "pressure boundary");
         copy(w->base_source, w->source);

@@ -158,6 +158,8 @@ void execute(cfdb_server& s, Resident& r, const Mesh& m, Request& q, bool create
         cfdb_tuning tun;
         cfdb_default_tuning(&tun);
         tun.pdl = s.cfg.pdl;
+        tun.mixed_sweeps = s.cfg.mixed_sweeps;
+        tun.mixed_weight = s.cfg.mixed_weight;
         check(cfdb_system_set_tuning(r.sys, &tun));
         dmalloc(&r.d_diag, m.n);
         dmalloc(&r.d_upper, m.nf);
@@ -307,6 +309,8 @@ void cfdb_default_server_config(cfdb_server_config* c) {
     cfdb_default_amg_settings(&c->settings);
     c->max_age = 0;
     c->pdl = 0;
+    c->mixed_sweeps = 0;
+    c->mixed_weight = 0.0;
 }
 
 int cfdb_server_create(const cfdb_server_config* cfg, cfdb_server** out) {

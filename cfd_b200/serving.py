@@ -22,7 +22,8 @@ _pd = C.POINTER(C.c_double)
 
 class ServerConfigStruct(C.Structure):
     _fields_ = [("slots", _i), ("hbm_budget_bytes", _d), ("precision", _i),
-                ("settings", AmgSettingsStruct), ("max_age", _i), ("pdl", _i)]
+                ("settings", AmgSettingsStruct), ("max_age", _i), ("pdl", _i),
+                ("mixed_sweeps", _i), ("mixed_weight", _d)]
 
 
 class ServerInfoStruct(C.Structure):
@@ -47,13 +48,15 @@ _p("cfdb_server_info", [_vp, C.POINTER(ServerInfoStruct)])
 
 class Server:
     def __init__(self, slots=4, hbm_budget_bytes=150e9, precision=Precision.MIXED,
-                 settings: AmgSettings | None = None, max_age=0, pdl=0):
+                 settings: AmgSettings | None = None, max_age=0, pdl=0, mixed_schedule=None):
         cfg = ServerConfigStruct()
         _lib.cfdb_default_server_config(C.byref(cfg))
         cfg.slots, cfg.hbm_budget_bytes, cfg.precision = int(slots), float(hbm_budget_bytes), int(precision)
         cfg.settings = (settings or AmgSettings())._c()
         cfg.max_age = int(max_age)
         cfg.pdl = int(pdl)
+        if mixed_schedule is not None:  # (sweeps, weight) of the mixed V-cycle
+            cfg.mixed_sweeps, cfg.mixed_weight = int(mixed_schedule[0]), float(mixed_schedule[1])
         h = _vp()
         _check(_lib.cfdb_server_create(C.byref(cfg), C.byref(h)))
         self._h = h

@@ -402,7 +402,8 @@ int cfdb_system_assemble(cfdb_system* sys, const double* flux, const double* gam
  * on device arrays (flow_solver.cpp:757-796, convection 0): upper = lower = -gamma*delta,
  * diag = diag0 + sum of gamma*delta (diag0 may be NULL: zero), source = source0 - div(flux),
  * then set_reference(ref_cell, ref_value) unless ref_cell < 0. Requires
- * cfdb_system_create_mesh. */
+ * cfdb_system_create_mesh. Enqueued on the system's stream (cfdb_system_stream) and returns at
+ * once: work on other streams that reads or writes the outputs must wait for that stream. */
 /* The steps of FlowSolver::pressure_correction after the pressure solve, for internal faces on
  * device arrays: the conservative face flux phi = flux - gamma*delta*(p_new[N] - p_new[P]) -
  * non_orth (flow_solver.cpp:821-826; non_orth may be NULL: zero) and the under-relaxed

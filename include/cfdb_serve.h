@@ -32,6 +32,8 @@ typedef struct {
                                    (cfdb_tuning.pdl), default 0: with requests overlapping on
                                    the GPU, kernels scheduled early would hold SM slots that
                                    other requests' kernels can use */
+    int mixed_sweeps;           /* mixed precision: the V-cycle's smoother schedule */
+    double mixed_weight;        /* (cfdb_tuning.mixed_sweeps / mixed_weight; 0: the hierarchy's) */
 } cfdb_server_config;
 
 typedef struct {

@@ -20,8 +20,9 @@ repeated until no knob changes (at most `passes` passes). Their objective is the
 a fixed number of CG iterations (tolerance 0, so every system runs exactly `iterations`
 iterations) through the captured graphs of the real solve path, median of `reps` runs. The
 smoother schedule changes the iteration count, so its objective is the device time of whole
-solves to the caller's tolerance (`tune_smoother`). Results are cached in a JSON file keyed by
-a workload signature.
+solves to the caller's tolerance (`tune_smoother`); the knobs that interact with it are then
+searched once more under the chosen schedule (`retune_knobs`). Results of `tune` are cached in a
+JSON file keyed by a workload signature.
 """
 from __future__ import annotations
 
@@ -40,8 +41,13 @@ CANDIDATES = {
     "fuse_first": [0, 1],
     "sell_rows": [256, 512, 1024],
     "krylov_pair": [0, 1],
-    "tail_rows": [0, 1024, 8192, 65536],
+    "tail_rows": [0, 1024, 8192, 65536, 131072],
 }
+
+# knobs whose best value depends on the smoother schedule: with one sweep per level the first
+# sweeps are never fused, so the persistent tail (which needs the unfused schedule) and the
+# shapes of the kernels it replaces are searched again once the schedule is chosen
+SCHEDULE_KNOBS = ("tail_rows", "sell_rows", "target_tiles")
 
 
 def _key(t: Tuning) -> tuple:
@@ -168,3 +174,13 @@ def tune_smoother(target, solve: Callable[[], int], stream_handle: int, base: Tu
             best, best_ms = t, ms
     target.set_tuning(best)
     return best, {"ms": best_ms, "trace": trace}
+
+
+def retune_knobs(evaluate: Callable[[Tuning], float], base: Tuning, knobs=SCHEDULE_KNOBS):
+    """One coordinate-descent pass over `knobs` from `base` (a tuning that already carries the
+    chosen smoother schedule); evaluate is an objective such as solve_timer's, which also
+    installs the tuning it times. Returns (tuning, record); the caller installs the tuning."""
+    cand = {k: CANDIDATES[k] for k in knobs}
+    best, best_ms, trace = coordinate_search(evaluate, base, candidates=cand, passes=1)
+    return best, {"ms": best_ms, "start_ms": trace[0][1] if trace else None,
+                  "evaluations": len(trace), "trace": trace}

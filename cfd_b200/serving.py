@@ -229,8 +229,11 @@ def run_load(server: Server, pool: list, rate_hz: float, n_requests: int, repeat
             x = e.free_x.pop() if e.free_x else _pinned(e.n)
         ticket = server.submit(e.mesh_id, key, d, u, l, e.rhs[bi], x=x,
                                warm_start=bool(rep and warm_start), rel_tol=rel_tol)
+        # host-to-device bytes of the request: the matrix unless it repeats the resident key,
+        # and the right-hand side; the solution comes back
+        h2d = 8 * (e.n + (0 if rep else len(d) + len(u) + len(l)))
         pending.put((ticket, e, x, {"mesh": e.mesh_id, "kind": e.kind, "n": e.n,
-                                    "repeat": bool(rep)}))
+                                    "repeat": bool(rep), "h2d": h2d, "d2h": 8 * e.n}))
         if closed_loop:
             while True:
                 with lock:
@@ -253,4 +256,7 @@ def run_load(server: Server, pool: list, rate_hz: float, n_requests: int, repeat
         "repeat_frac": float(np.mean([r["repeat"] for r in records])) if records else None,
         "mean_iterations": float(np.mean([r["iterations"] for r in records])) if records else None,
         "all_converged": all(r["converged"] for r in records),
+        "h2d_gbs": sum(r["h2d"] for r in records) / wall / 1e9 if wall > 0 else 0.0,
+        "d2h_gbs": sum(r["d2h"] for r in records) / wall / 1e9 if wall > 0 else 0.0,
+        "mean_h2d_mb": float(np.mean([r["h2d"] for r in records]) / 1e6) if records else None,
     }

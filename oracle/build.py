@@ -3,7 +3,9 @@
 * ``oracle/_build/liboracle.so``: the C restatement in ``oracle/oracle.c`` (gcc, no FMA
   contraction so roundings match the reference's x86-64 host build).
 * ``oracle/_ref/libcfdref.so``: the reference's own host sources, compiled unchanged where
-  they lie under the reference checkout, plus ``oracle/ref_shim.cpp``. Only built when the
+  they lie under the reference checkout (the Eigen-dependent ones against
+  ``oracle/eigen_standin``), plus the shims ``oracle/ref_shim.cpp``,
+  ``oracle/ref_eigen_shim.cpp`` and ``oracle/ref_flow_shim.cpp``. Only built when the
   reference checkout is present; the built library is git-ignored and travels with the tree.
 
 Run ``python -m oracle.build`` (or call :func:`build_all`).
@@ -43,6 +45,8 @@ REF_EIGEN_SOURCES = [
     "src/fv/src/parallel_amg.cpp",
     "src/parallel/src/comm.cpp",
 ]
+# FlowSolver (the callers of the pressure path), in the reference build only
+REF_FLOW_SOURCES = ["src/fv/src/flow_solver.cpp"]
 REF_INCLUDES = ["src/gpu/include", "src/core/include", "src/mesh/include", "src/fv/include",
                 "src/parallel/include"]
 
@@ -68,15 +72,17 @@ def build_oracle(force: bool = False) -> str:
 
 
 def reference_available() -> bool:
-    return all(os.path.exists(os.path.join(REFERENCE_ROOT, s)) for s in REF_SOURCES + REF_EIGEN_SOURCES)
+    return all(os.path.exists(os.path.join(REFERENCE_ROOT, s))
+               for s in REF_SOURCES + REF_EIGEN_SOURCES + REF_FLOW_SOURCES)
 
 
 def build_ref(force: bool = False) -> str | None:
     """Compile the reference's host path (unchanged sources) + our shim into oracle/_ref."""
     if not reference_available():
         return REF_SO if os.path.exists(REF_SO) else None
-    srcs = [os.path.join(REFERENCE_ROOT, s) for s in REF_SOURCES + REF_EIGEN_SOURCES]
-    shims = [os.path.join(HERE, "ref_shim.cpp"), os.path.join(HERE, "ref_eigen_shim.cpp")]
+    srcs = [os.path.join(REFERENCE_ROOT, s) for s in REF_SOURCES + REF_EIGEN_SOURCES + REF_FLOW_SOURCES]
+    shims = [os.path.join(HERE, "ref_shim.cpp"), os.path.join(HERE, "ref_eigen_shim.cpp"),
+             os.path.join(HERE, "ref_flow_shim.cpp")]
     standin = os.path.join(HERE, "eigen_standin")
     deps = srcs + shims + [os.path.join(REFERENCE_ROOT, "src/gpu/src/krylov_kernels.inc"),
                            os.path.join(REFERENCE_ROOT, "src/gpu/src/fv_cell.inc"),

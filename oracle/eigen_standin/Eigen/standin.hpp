@@ -1,6 +1,6 @@
 // Header-only stand-in for the subset of Eigen 3.4 that the reference's pressure-path sources
 // use (amg.cpp, ldu_matrix.cpp, parallel_amg.cpp, mesh.cpp, mesh_builder.cpp, box_mesher.cpp,
-// fv_geometry.cpp). TEST INFRASTRUCTURE ONLY: it lets those sources compile unchanged into the
+// fv_geometry.cpp, flow_solver.cpp). TEST INFRASTRUCTURE ONLY: it lets those sources compile unchanged into the
 // oracle's reference build (oracle/_ref) in an image without Eigen. Nothing in the product
 // includes it.
 //
@@ -299,6 +299,19 @@ public:
         for (Index i = 0; i < size(); ++i) r.data()[i] = std::abs(data()[i]);
         return r;
     }
+    // element-wise min / max (std::min / std::max per element, Eigen's default NaN handling)
+    template <typename Other> Matrix cwiseMin(const Other& o) const {
+        Matrix r = *this;
+        for (Index i = 0; i < size(); ++i) r.data()[i] = std::min(data()[i], o.coeff(i));
+        return r;
+    }
+    template <typename Other> Matrix cwiseMax(const Other& o) const {
+        Matrix r = *this;
+        for (Index i = 0; i < size(); ++i) r.data()[i] = std::max(data()[i], o.coeff(i));
+        return r;
+    }
+    // mean = sum() / size(), the sum in the reduction order above
+    S mean() const { return sum() / static_cast<S>(size()); }
     template <typename F> Matrix unaryExpr(F f) const {
         Matrix r = *this;
         for (Index i = 0; i < size(); ++i) r.data()[i] = f(data()[i]);

@@ -1,9 +1,9 @@
 """Python front end of the reference's Eigen-dependent host sources -- TEST INFRASTRUCTURE ONLY.
 
 ``oracle/_ref/libcfdref.so`` holds the reference's unchanged mesh pipeline (``mesh.cpp``,
-``mesh_builder.cpp``, ``box_mesher.cpp``), ``fv_geometry.cpp``, ``ldu_matrix.cpp`` and
-``amg.cpp``, compiled against the Eigen stand-in in ``oracle/eigen_standin`` (see
-``oracle/ref_eigen_shim.cpp``). Integer results (face ordering, CSR pattern, aggregates) are the
+``mesh_builder.cpp``, ``box_mesher.cpp``), ``fv_geometry.cpp``, ``ldu_matrix.cpp``, ``amg.cpp``
+and ``flow_solver.cpp``, compiled against the Eigen stand-in in ``oracle/eigen_standin`` (see
+``oracle/ref_eigen_shim.cpp`` and ``oracle/ref_flow_shim.cpp``). Integer results (face ordering, CSR pattern, aggregates) are the
 reference's own; floating-point results follow Eigen as far as the stand-in does.
 
 The lattice helpers (cells and boundary tags of box meshes, the 6-tet split, the jittered nodes)
@@ -76,6 +76,19 @@ def lib():
         R.refx_jittered_lattice.argtypes = [_i, _i, _i, _pd, _pd, _pd, _d, _u64, _pd]
         R.refx_pressure_inputs.argtypes = [_i, _i, _pi, _pi, _pd, _pd, _pd, _d, _i, _i, _i, _u64, _pd,
                                            _pd, _pd]
+        if hasattr(R, "refx_flow_create"):
+            R.refx_flow_create.argtypes = [_vp, _i, _pi, _pd, _pd, _pd, _pi]
+            R.refx_flow_create.restype = _vp
+            R.refx_flow_destroy.argtypes = [_vp]
+            for name, args in (("refx_flow_set_state", [_vp, _pd, _pd, _pd]),
+                               ("refx_flow_get_state", [_vp, _pd, _pd, _pd]),
+                               ("refx_flow_boundary", [_vp, _pi, _pd, _pd]),
+                               ("refx_flow_momentum", [_vp, _d, _i]),
+                               ("refx_flow_momentum_arrays", [_vp, _pd, _pd, _pd, _pd]),
+                               ("refx_flow_solve_momentum", [_vp, _pd]),
+                               ("refx_flow_pressure_correction", [_vp, _i, _pd, _pd, _pd])):
+                getattr(R, name).argtypes = args
+                getattr(R, name).restype = _i
         _declared = True
     return R
 
@@ -490,6 +503,91 @@ class RefLdu:
     def close(self):
         if self._h:
             lib().refx_ldu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# FlowBoundary, LinearSolverType, ConvectionScheme and GradientScheme as the reference numbers
+# them (flow_solver.hpp:15, ldu_matrix.hpp:21, flow_solver.hpp:40, fv_geometry.hpp:32)
+FLOW_BOUNDARY = {"VelocityInlet": 0, "Wall": 1, "PressureOutlet": 2, "Symmetry": 3, "Empty": 4}
+CONVECTION = {"Upwind": 0, "LinearUpwind": 1, "LimitedLinearUpwind": 2, "Lust": 3, "LimitedLust": 4}
+GRADIENT = {"Gauss": 0, "LeastSquares": 1, "GaussCorrected": 2}
+
+
+class RefFlow:
+    """cfd::fv::FlowSolver on a reference mesh built by RefMesh.build (patches "p0", "p1", ...),
+    driven one SIMPLE step at a time (oracle/ref_flow_shim.cpp)."""
+
+    def __init__(self, mesh: RefMesh, patches, nu=1e-3, alpha_u=0.7, alpha_p=0.3, n_non_orth=0,
+                 p_solver=("GpuCg", 1e-10, 0.01, 500), u_solver=("GpuBiCgStab", 1e-10, 0.1, 1000),
+                 convection="LinearUpwind", gradient="Gauss"):
+        """patches: one (kind, velocity (3), pressure) per patch, kind a FLOW_BOUNDARY name."""
+        R = lib()
+        if R is None or not hasattr(R, "refx_flow_create"):
+            raise RuntimeError("the reference build has no FlowSolver")
+        self.mesh = mesh
+        kinds = _i32([FLOW_BOUNDARY[k] for k, _, _ in patches])
+        vel = _f64([v for _, v, _ in patches]).reshape(-1, 3)
+        pre = _f64([p for _, _, p in patches])
+        real = _f64([nu, alpha_u, alpha_p, p_solver[1], p_solver[2], u_solver[1], u_solver[2]])
+        ints = _i32([n_non_orth, LINEAR_SOLVER[p_solver[0]], p_solver[3], LINEAR_SOLVER[u_solver[0]],
+                     u_solver[3], CONVECTION[convection], GRADIENT[gradient]])
+        self._h = R.refx_flow_create(mesh._h, len(patches), _ip(kinds), _dp(vel), _dp(pre), _dp(real), _ip(ints))
+        if not self._h:
+            raise ValueError("FlowSolver construction failed")
+
+    def _call(self, name, *args):
+        if getattr(lib(), name)(self._h, *args) != 0:
+            raise ValueError(f"{name} failed")
+
+    def set_state(self, u, p, phi=None):
+        u, p = _f64(u), _f64(p)
+        self._call("refx_flow_set_state", _dp(u), _dp(p), None if phi is None else _dp(_f64(phi)))
+
+    def state(self):
+        m = self.mesh
+        u, p, phi = np.empty((m.n_cells, 3)), np.empty(m.n_cells), np.empty(m.n_faces)
+        self._call("refx_flow_get_state", _dp(u), _dp(p), _dp(phi))
+        return u, p, phi
+
+    def boundary(self):
+        """Per boundary face: (FlowBoundary kind, outlet pressure, fixed velocity)."""
+        nb = self.mesh.n_faces - self.mesh.n_internal_faces
+        k, p, v = np.empty(nb, np.int32), np.empty(nb), np.empty((nb, 3))
+        self._call("refx_flow_boundary", _ip(k), _dp(p), _dp(v))
+        return k, p, v
+
+    def momentum(self, dt=0.0, relax=True):
+        """assemble_momentum into the solver's momentum system; returns (diag (n, 3), upper,
+        lower, source (n, 3))."""
+        self._call("refx_flow_momentum", float(dt), 1 if relax else 0)
+        m = self.mesh
+        d, s = np.empty((m.n_cells, 3)), np.empty((m.n_cells, 3))
+        up, lo = np.empty(m.n_internal_faces), np.empty(m.n_internal_faces)
+        self._call("refx_flow_momentum_arrays", _dp(d), _dp(up), _dp(lo), _dp(s))
+        return d, up, lo, s
+
+    def solve_momentum(self):
+        r = np.empty(3)
+        self._call("refx_flow_solve_momentum", _dp(r))
+        return r
+
+    def pressure_correction(self, relax_p=True, u_prev=None, phi_prev=None):
+        """FlowSolver::pressure_correction on the momentum system; returns the initial residual."""
+        ini = _d()
+        self._call("refx_flow_pressure_correction", 1 if relax_p else 0,
+                   None if u_prev is None else _dp(_f64(u_prev)),
+                   None if phi_prev is None else _dp(_f64(phi_prev)), C.byref(ini))
+        return ini.value
+
+    def close(self):
+        if self._h:
+            lib().refx_flow_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -26,3 +26,20 @@ def test_coordinate_search_finds_separable_minimum():
 def test_coordinate_search_keeps_default_when_flat():
     best, val, trace = coordinate_search(lambda t: 1.0)
     assert best == Tuning() and val == 1.0
+
+
+def test_retune_knobs_keeps_the_schedule_and_searches_only_its_knobs():
+    from cfd_b200.autotune import SCHEDULE_KNOBS, retune_knobs
+    base = dataclasses.replace(Tuning(), mixed_sweeps=1, mixed_weight=0.85, wide_row=64)
+    seen = []
+
+    def cost(t):
+        seen.append(t)
+        return 2.0 - (t.tail_rows == 8192)  # the tail pays off only under this schedule
+
+    best, rec = retune_knobs(cost, base)
+    assert best.tail_rows == 8192 and rec["ms"] == 1.0 and rec["start_ms"] == 2.0
+    assert (best.mixed_sweeps, best.mixed_weight, best.wide_row) == (1, 0.85, 64)
+    for t in seen:  # every point differs from the base in the schedule knobs alone
+        diff = {k for k, v in dataclasses.asdict(t).items() if v != getattr(base, k)}
+        assert diff <= set(SCHEDULE_KNOBS)

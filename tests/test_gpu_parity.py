@@ -220,10 +220,13 @@ def test_mixed_precision_reaches_target(gpu, make):
     assert np.linalg.norm(x - xo) <= 1e-5 * np.linalg.norm(xo)
 
 
-@pytest.mark.parametrize("precision", ["FP64", "MIXED"])
-def test_persistent_tail_matches_separate_kernels(gpu, precision):
+@pytest.mark.parametrize("precision,schedule", [("FP64", (0, 0.0)), ("MIXED", (0, 0.0)), ("MIXED", (1, 0.85)),
+                                                 ("MIXED", (3, 0.85))],
+                         ids=["FP64", "MIXED", "MIXED-1sweep", "MIXED-3sweeps"])
+def test_persistent_tail_matches_separate_kernels(gpu, precision, schedule):
     """The persistent tail kernel (small coarse levels + coarse solve in one cooperative launch)
-    computes every row exactly as the separate per-level kernels do."""
+    computes every row exactly as the separate per-level kernels do, under the hierarchy's
+    smoother schedule and under the mixed path's tuned ones."""
     cb = gpu
     case = W.graded(24)
     up, lo, diag, src = _assembled(case)
@@ -233,7 +236,7 @@ def test_persistent_tail_matches_separate_kernels(gpu, precision):
     tol = 1e-10 * np.linalg.norm(src)
     out = []
     for tail in (0, 10**6):
-        ds.set_tuning(cb.Tuning(tail_rows=tail))
+        ds.set_tuning(cb.Tuning(tail_rows=tail, mixed_sweeps=schedule[0], mixed_weight=schedule[1]))
         x = np.zeros(case.n)
         st = ds.solve(diag, up, lo, src, x, cb.Method.Cg, True, cb.SolveControl(tol, 500))
         z = ds.apply_amg(np.random.default_rng(3).standard_normal(case.n))

@@ -58,6 +58,10 @@ def parse():
     ap.add_argument("--serve-pdl", type=int, default=0, help="serve: programmatic dependent launch (0/1)")
     ap.add_argument("--max-age", type=int, default=20,
                     help="serve: hierarchy rebuilt after this many solves of a mesh (AmgCache::max_age; 0: never)")
+    ap.add_argument("--serve-rebuild", choices=("background", "inline"), default="background",
+                    help="serve: aged hierarchies rebuilt by the server's rebuild thread while the mesh keeps "
+                         "serving, or before the triggering request's solve (the one-at-a-time baseline "
+                         "always rebuilds inline, as the reference's AmgCache does)")
     ap.add_argument("--size", type=int, default=0, help="override the mesh edge length")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default launch knobs and smoother schedule")
@@ -494,6 +498,7 @@ def run_ours(args, rank, world, local_rank, cfg_name, case, desc):
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(args, case, solvers["mixed"], tol, dev)
+        e2e["device_api"] = run_e2e_device_api(args, case, solvers["mixed"], dev)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, x_star = cpu_baseline(case)
@@ -579,6 +584,53 @@ def run_e2e(args, case, ds, tol, dev):
             "d2h_bytes_per_step": d2h, "ms_per_step": ms / args.steps,
             "path": "cfdb_system_assemble + host finalize + cfdb_system_solve (host arrays)",
             "host_copy_gbs": host_copy_rates(stream, dev)}
+
+
+def run_e2e_device_api(args, case, ds, dev):
+    """The product's device-array calls with the step's inputs copied in from page-locked host
+    memory every step: H2D of the face flux, face rAU, delta coefficients and source0, the fused
+    assembly with the finalize on the device (cfdb_system_assemble_pressure_device), the norm of
+    b for the tolerance, the solve (cfdb_system_solve_device), D2H of x. The LDU matrix stays on
+    the device between assembly and solve, where the reference-facing sequence (run_e2e) moves
+    it to the host and back."""
+    import numpy as np
+    import torch
+
+    import cfd_b200 as cb
+    n, nf = case.n, case.n_faces
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory()  # noqa: E731
+    h_in = [pin(case.flux), pin(case.gamma), pin(case.delta), pin(case.source0)]
+    h_x = pin(np.zeros(n))
+    d_in = [torch.empty_like(t, device=dev) for t in h_in]
+    e = lambda k: torch.empty(k, dtype=torch.float64, device=dev)  # noqa: E731
+    up, lo, dg, src, x = e(nf), e(nf), e(n), e(n), e(n)
+    stream = torch.cuda.ExternalStream(ds.stream(), device=dev)
+
+    def step():
+        for d, h in zip(d_in, h_in):
+            d.copy_(h, non_blocking=True)
+        flux, gamma, delta, src0 = d_in
+        ds.assemble_pressure_device(flux, gamma, delta, src0, up, lo, dg, src)
+        x.zero_()
+        tol = 1e-8 * float(torch.linalg.vector_norm(src))
+        st = ds.solve_device(dg, up, lo, src, x, cb.Method.Cg, True, cb.SolveControl(tol, 500))
+        h_x.copy_(x, non_blocking=True)
+        return st
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 0)):
+            step()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            assert step().converged
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"value": args.steps / (ms / 1e3), "unit": "solves/s", "h2d_bytes_per_step": 8 * (3 * nf + n),
+            "d2h_bytes_per_step": 8 * n, "ms_per_step": ms / args.steps,
+            "path": "H2D face data + cfdb_system_assemble_pressure_device + cfdb_system_solve_device + D2H x"}
 
 
 def host_copy_rates(stream, dev, nbytes=64 << 20):
@@ -815,10 +867,11 @@ def run_serve(args, rank, world, local_rank):
     n_req = args.requests
     res = {}
 
-    def server(prec, slots):
+    def server(prec, slots, background=False):
         sched = tuple(float(v) for v in args.serve_schedule.split(","))
         srv = S.Server(slots=slots, hbm_budget_bytes=150e9, precision=prec, settings=settings,
-                       max_age=args.max_age, pdl=args.serve_pdl, mixed_schedule=(int(sched[0]), sched[1]))
+                       max_age=args.max_age, pdl=args.serve_pdl, mixed_schedule=(int(sched[0]), sched[1]),
+                       background_rebuild=background)
         pool = S.make_pool(srv, pool_cases, variants=3, seed=7)
         t0 = time.perf_counter()
         for e in pool:  # hierarchy builds (AmgCache setup), not timed below
@@ -832,7 +885,7 @@ def run_serve(args, rank, world, local_rank):
     res["one_at_a_time_fp64"] = dict(base, setup_s=setup)
     srv.close()
     for label, prec in (("mixed", cb.Precision.MIXED), ("fp64", cb.Precision.FP64)):
-        srv, pool, setup = server(prec, args.slots)
+        srv, pool, setup = server(prec, args.slots, background=args.serve_rebuild == "background")
         S.run_load(srv, pool, 1e6, n_req, seed=10)  # warm-up: page-locked buffers, graphs
         sampler = ClockSampler(local_rank) if label == "mixed" else None
         if sampler:
@@ -858,10 +911,11 @@ def run_serve(args, rank, world, local_rank):
                    "tet_edges": list(W.SERVE_TET_EDGES), "tet_share": 0.25, "repeat_share": 0.3,
                    "slots": args.slots, "hbm_budget_gb": 150, "rates_hz": rates,
                    "mixed_schedule": args.serve_schedule,
-                   "max_age": args.max_age,
+                   "max_age": args.max_age, "served_rebuild": args.serve_rebuild,
                    "requests_per_rate": n_req, "repeats": args.repeats, "strength_threshold": THETA,
                    "step": "one request: H2D of its matrix (new key) and rhs, hierarchy rebuilt on the "
-                           "device when the mesh has served max_age solves, AMG-PCG to 1e-8, D2H of x",
+                           "device when the mesh has served max_age solves (served arms: by the rebuild "
+                           "thread when served_rebuild is background), AMG-PCG to 1e-8, D2H of x",
                    "parallelism": f"replicas x{world}"},
         "mixed": res["mixed"], "fp64": res["fp64"], "one_at_a_time_fp64": res["one_at_a_time_fp64"],
         "served_mixed_vs_one_at_a_time_fp64": value / res["one_at_a_time_fp64"]["solves_per_s"],

@@ -8,6 +8,9 @@
 // Residency is bounded by an HBM budget: a system is admitted only when its (estimated, then
 // measured) device footprint fits next to the resident ones, evicting idle systems in
 // least-recently-used order; requests that do not fit wait in the queue until memory frees up.
+// Hierarchies age as the reference's AmgCache does (rebuilt after max_age solves); with
+// background_rebuild a rebuild thread builds the new one on a spare system from a copy of the
+// triggering request's matrix while the mesh keeps serving with the old one.
 #include "../../include/cfdb_serve.h"
 
 #include <algorithm>
@@ -43,6 +46,11 @@ struct Mesh {
     std::vector<int> owner, neighbour;
 };
 
+// State of a mesh's background hierarchy rebuild (cfg.background_rebuild), guarded by the
+// server lock: queued for the rebuild thread, being built on the spare system, or ready to be
+// swapped in by the next request on the mesh.
+enum class Rebuild { Idle, Queued, Building, Ready };
+
 struct Resident {
     cfdb_system* sys = nullptr;
     size_t bytes = 0;
@@ -53,6 +61,15 @@ struct Resident {
     int age = 0;                 // solves since the hierarchy was built
     bool busy = false;
     Clock::time_point last_use{};
+    // background rebuild: a second system on the same mesh builds the new hierarchy from device
+    // copies of the triggering request's matrix while `sys` keeps serving; the two are swapped
+    // by the next request on the mesh once the build is done
+    cfdb_system* spare = nullptr;
+    double *s_diag = nullptr, *s_upper = nullptr, *s_lower = nullptr;
+    cudaEvent_t copied = nullptr; // the copies of the matrix are complete
+    long long spare_key = -1;     // key of the matrix the spare's hierarchy is built from
+    Rebuild rebuild = Rebuild::Idle;
+    bool background_failed = false; // a background build failed: rebuild on the request path
 };
 
 struct Request {
@@ -90,21 +107,31 @@ struct cfdb_server {
     std::vector<std::thread> workers;
     long long completed = 0;
     long long evictions = 0;
+    long long rebuilds = 0;            // hierarchy rebuilds on the request path
+    long long background_rebuilds = 0; // hierarchies built by the rebuild thread and swapped in
+    std::deque<int> rebuild_queue;     // meshes whose spare system is to be rebuilt
+    std::condition_variable cv_rebuild;
+    std::thread rebuilder;
 };
 
 namespace {
 
 size_t estimate_bytes(const cfdb_server& s, const Mesh& m) {
     // measured footprint of the persistent systems: about 800 bytes per cell (hierarchy, SELL
-    // copies, Krylov vectors) plus the server's device copies of one matrix and three vectors
+    // copies, Krylov vectors) plus the server's device copies of one matrix and three vectors;
+    // with background rebuilds, a spare system and a second copy of the matrix
     const size_t per_cell = s.cfg.precision == CFDB_PRECISION_MIXED ? 700 : 800;
-    return per_cell * static_cast<size_t>(m.n) + sizeof(double) * (static_cast<size_t>(m.n) * 3 + 2 * static_cast<size_t>(m.nf) + m.n);
+    const size_t matrix = sizeof(double) * (static_cast<size_t>(m.n) + 2 * static_cast<size_t>(m.nf));
+    const size_t one = per_cell * static_cast<size_t>(m.n) + matrix + sizeof(double) * 3 * static_cast<size_t>(m.n);
+    return s.cfg.background_rebuild ? one + per_cell * static_cast<size_t>(m.n) + matrix : one;
 }
 
 void release(cfdb_server& s, Resident& r) {
     if (r.sys != nullptr) cfdb_system_destroy(r.sys);
-    for (double* p : {r.d_diag, r.d_upper, r.d_lower, r.d_rhs, r.d_x})
+    if (r.spare != nullptr) cfdb_system_destroy(r.spare);
+    for (double* p : {r.d_diag, r.d_upper, r.d_lower, r.d_rhs, r.d_x, r.s_diag, r.s_upper, r.s_lower})
         if (p != nullptr) cudaFree(p);
+    if (r.copied != nullptr) cudaEventDestroy(r.copied);
     s.resident_bytes -= std::min(s.resident_bytes, r.bytes);
     r = Resident{};
 }
@@ -117,7 +144,9 @@ bool make_room(cfdb_server& s, size_t need, int keep_mesh) {
         int victim = -1;
         Clock::time_point oldest = Clock::time_point::max();
         for (auto& kv : s.resident) {
-            if (kv.first == keep_mesh || kv.second->busy || kv.second->sys == nullptr) continue;
+            const Resident& c = *kv.second;
+            const bool rebuilding = c.rebuild == Rebuild::Queued || c.rebuild == Rebuild::Building;
+            if (kv.first == keep_mesh || c.busy || rebuilding || c.sys == nullptr) continue;
             if (kv.second->last_use < oldest) {
                 oldest = kv.second->last_use;
                 victim = kv.first;
@@ -148,19 +177,35 @@ void dmalloc(double** p, size_t n) {
     }
 }
 
-// Runs one request on its (locked) resident system. No server lock held.
-void execute(cfdb_server& s, Resident& r, const Mesh& m, Request& q, bool created) {
-    cudaSetDevice(s.device);
-    if (created) {
-        check(cfdb_system_create_mesh(m.n, m.nf, m.owner.data(), m.neighbour.data(), &r.sys));
-        check(cfdb_system_set_precision(r.sys, s.cfg.precision));
-        check(cfdb_system_set_keep_levels(r.sys, 0)); // the plan of a resident system never changes
+// A persistent system on the mesh with the server's precision, plan and tuning.
+cfdb_system* new_system(const cfdb_server& s, const Mesh& m) {
+    cfdb_system* sys = nullptr;
+    check(cfdb_system_create_mesh(m.n, m.nf, m.owner.data(), m.neighbour.data(), &sys));
+    try {
+        check(cfdb_system_set_precision(sys, s.cfg.precision));
+        check(cfdb_system_set_keep_levels(sys, 0)); // the plan of a resident system never changes
         cfdb_tuning tun;
         cfdb_default_tuning(&tun);
         tun.pdl = s.cfg.pdl;
         tun.mixed_sweeps = s.cfg.mixed_sweeps;
         tun.mixed_weight = s.cfg.mixed_weight;
-        check(cfdb_system_set_tuning(r.sys, &tun));
+        check(cfdb_system_set_tuning(sys, &tun));
+    } catch (...) {
+        cfdb_system_destroy(sys);
+        throw;
+    }
+    return sys;
+}
+
+enum ExecuteOutcome { kRebuiltInline = 1, kQueueRebuild = 2 };
+
+// Runs one request on its (locked) resident system. No server lock held. may_queue: the
+// resident has no background rebuild in progress or waiting. Returns ExecuteOutcome bits.
+int execute(cfdb_server& s, Resident& r, const Mesh& m, Request& q, bool created, bool may_queue) {
+    cudaSetDevice(s.device);
+    int outcome = 0;
+    if (created) {
+        r.sys = new_system(s, m);
         dmalloc(&r.d_diag, m.n);
         dmalloc(&r.d_upper, m.nf);
         dmalloc(&r.d_lower, m.nf);
@@ -185,11 +230,31 @@ void execute(cfdb_server& s, Resident& r, const Mesh& m, Request& q, bool create
     // for bit, so it waits for the next new matrix
     const bool same_as_hierarchy = q.key >= 0 && r.hier_key == q.key;
     const bool aged = s.cfg.max_age > 0 && r.age >= s.cfg.max_age && !same_as_hierarchy;
-    if (created || aged) {
+    const bool background = s.cfg.background_rebuild != 0 && !r.background_failed;
+    if (created || (aged && !background)) {
         CFDB_CUDA(cudaStreamSynchronize(st));
         check(cfdb_system_setup_amg_device(r.sys, r.d_diag, r.d_upper, r.d_lower, &s.cfg.settings, 1));
         r.age = 0;
         r.hier_key = q.key;
+        if (!created) outcome |= kRebuiltInline;
+    } else if (aged && may_queue) {
+        // the rebuild thread builds the spare system's hierarchy from copies of this matrix
+        // (the next request on the mesh may overwrite d_diag / d_upper / d_lower); this
+        // request and the ones after it solve with the current hierarchy until the swap
+        if (r.s_diag == nullptr) {
+            dmalloc(&r.s_diag, m.n);
+            dmalloc(&r.s_upper, m.nf);
+            dmalloc(&r.s_lower, m.nf);
+            CFDB_CUDA(cudaEventCreateWithFlags(&r.copied, cudaEventDisableTiming));
+        }
+        CFDB_CUDA(cudaMemcpyAsync(r.s_diag, r.d_diag, sizeof(double) * m.n, cudaMemcpyDeviceToDevice, st));
+        if (m.nf > 0) {
+            CFDB_CUDA(cudaMemcpyAsync(r.s_upper, r.d_upper, sizeof(double) * m.nf, cudaMemcpyDeviceToDevice, st));
+            CFDB_CUDA(cudaMemcpyAsync(r.s_lower, r.d_lower, sizeof(double) * m.nf, cudaMemcpyDeviceToDevice, st));
+        }
+        CFDB_CUDA(cudaEventRecord(r.copied, st));
+        r.spare_key = q.key;
+        outcome |= kQueueRebuild;
     }
     CFDB_CUDA(cudaMemcpyAsync(r.d_rhs, q.rhs, sizeof(double) * m.n, cudaMemcpyHostToDevice, st));
     if (!(q.warm && r.solution_key == q.key && q.key >= 0)) {
@@ -204,6 +269,55 @@ void execute(cfdb_server& s, Resident& r, const Mesh& m, Request& q, bool create
     ++r.age;
     if (q.x != nullptr) CFDB_CUDA(cudaMemcpyAsync(q.x, r.d_x, sizeof(double) * m.n, cudaMemcpyDeviceToHost, st));
     CFDB_CUDA(cudaStreamSynchronize(st));
+    return outcome;
+}
+
+// The background rebuild thread: builds queued meshes' spare hierarchies one at a time on the
+// spare system's own stream, while the workers keep solving with the current ones.
+void rebuild_loop(cfdb_server* sp) {
+    cfdb_server& s = *sp;
+    cudaSetDevice(s.device);
+    std::unique_lock<std::mutex> lk(s.mu);
+    for (;;) {
+        s.cv_rebuild.wait(lk, [&] { return s.stopping || !s.rebuild_queue.empty(); });
+        if (s.stopping) {
+            for (int id : s.rebuild_queue) {
+                auto it = s.resident.find(id);
+                if (it != s.resident.end()) it->second->rebuild = Rebuild::Idle;
+            }
+            s.rebuild_queue.clear();
+            return;
+        }
+        const int mesh = s.rebuild_queue.front();
+        s.rebuild_queue.pop_front();
+        auto it = s.resident.find(mesh);
+        if (it == s.resident.end()) continue; // queued residents are never evicted; defensive
+        Resident& r = *it->second;
+        r.rebuild = Rebuild::Building;
+        const Mesh& m = s.meshes[mesh];
+        const bool first = r.spare == nullptr;
+        lk.unlock();
+        bool ok = true;
+        size_t spare_bytes = 0;
+        try {
+            // while Building, only this thread touches the spare system and its matrix copies
+            if (first) r.spare = new_system(s, m);
+            CFDB_CUDA(cudaEventSynchronize(r.copied));
+            check(cfdb_system_setup_amg_device(r.spare, r.s_diag, r.s_upper, r.s_lower, &s.cfg.settings, 1));
+            if (first) {
+                cfdb_system_device_bytes(r.spare, &spare_bytes);
+                spare_bytes += sizeof(double) * (static_cast<size_t>(m.n) + 2 * static_cast<size_t>(m.nf));
+            }
+        } catch (const std::exception&) {
+            ok = false;
+        }
+        lk.lock();
+        r.bytes += spare_bytes;
+        s.resident_bytes += spare_bytes;
+        r.rebuild = ok ? Rebuild::Ready : Rebuild::Idle;
+        if (!ok) r.background_failed = true;
+        s.cv_work.notify_all();
+    }
 }
 
 void worker_loop(cfdb_server* sp) {
@@ -242,10 +356,20 @@ void worker_loop(cfdb_server* sp) {
             s.cv_work.wait(lk);
         }
         r->busy = true;
+        if (r->rebuild == Rebuild::Ready) {
+            // the background build is done: its hierarchy serves from this request on
+            std::swap(r->sys, r->spare);
+            r->hier_key = r->spare_key;
+            r->age = 0;
+            r->rebuild = Rebuild::Idle;
+            ++s.background_rebuilds;
+        }
+        const bool may_queue = r->rebuild == Rebuild::Idle;
         q->started = Clock::now();
         lk.unlock();
+        int outcome = 0;
         try {
-            execute(s, *r, s.meshes[q->mesh], *q, created);
+            outcome = execute(s, *r, s.meshes[q->mesh], *q, created, may_queue);
         } catch (const cfdb::Error& e) {
             q->status = e.code;
             q->error = e.what();
@@ -255,6 +379,12 @@ void worker_loop(cfdb_server* sp) {
         }
         q->finished = Clock::now();
         lk.lock();
+        if (outcome & kRebuiltInline) ++s.rebuilds;
+        if ((outcome & kQueueRebuild) && q->status == CFDB_OK) {
+            r->rebuild = Rebuild::Queued;
+            s.rebuild_queue.push_back(q->mesh);
+            s.cv_rebuild.notify_one();
+        }
         if (created && r->sys != nullptr) {
             size_t b = 0;
             cfdb_system_device_bytes(r->sys, &b);
@@ -311,6 +441,7 @@ void cfdb_default_server_config(cfdb_server_config* c) {
     c->pdl = 0;
     c->mixed_sweeps = 0;
     c->mixed_weight = 0.0;
+    c->background_rebuild = 0;
 }
 
 int cfdb_server_create(const cfdb_server_config* cfg, cfdb_server** out) {
@@ -324,6 +455,7 @@ int cfdb_server_create(const cfdb_server_config* cfg, cfdb_server** out) {
         CFDB_CUDA(cudaGetDevice(&s->device));
         s->t0 = Clock::now();
         for (int i = 0; i < cfg->slots; ++i) s->workers.emplace_back(worker_loop, s.get());
+        if (cfg->background_rebuild) s->rebuilder = std::thread(rebuild_loop, s.get());
         *out = s.release();
     });
 }
@@ -336,6 +468,8 @@ int cfdb_server_destroy(cfdb_server* s) {
     }
     s->cv_work.notify_all();
     for (auto& t : s->workers) t.join();
+    s->cv_rebuild.notify_all();
+    if (s->rebuilder.joinable()) s->rebuilder.join();
     cudaSetDevice(s->device);
     for (auto& kv : s->resident) release(*s, *kv.second);
     delete s;
@@ -430,6 +564,8 @@ int cfdb_server_info(cfdb_server* s, cfdb_server_info_t* info) {
     info->queued = static_cast<int>(s->queue.size());
     info->completed = s->completed;
     info->evictions = s->evictions;
+    info->rebuilds = s->rebuilds;
+    info->background_rebuilds = s->background_rebuilds;
     return CFDB_OK;
 }
 

@@ -23,12 +23,12 @@ _pd = C.POINTER(C.c_double)
 class ServerConfigStruct(C.Structure):
     _fields_ = [("slots", _i), ("hbm_budget_bytes", _d), ("precision", _i),
                 ("settings", AmgSettingsStruct), ("max_age", _i), ("pdl", _i),
-                ("mixed_sweeps", _i), ("mixed_weight", _d)]
+                ("mixed_sweeps", _i), ("mixed_weight", _d), ("background_rebuild", _i)]
 
 
 class ServerInfoStruct(C.Structure):
     _fields_ = [("resident_systems", _i), ("resident_bytes", _d), ("queued", _i),
-                ("completed", _ll), ("evictions", _ll)]
+                ("completed", _ll), ("evictions", _ll), ("rebuilds", _ll), ("background_rebuilds", _ll)]
 
 
 def _p(name, args, res=_i):
@@ -48,7 +48,8 @@ _p("cfdb_server_info", [_vp, C.POINTER(ServerInfoStruct)])
 
 class Server:
     def __init__(self, slots=4, hbm_budget_bytes=150e9, precision=Precision.MIXED,
-                 settings: AmgSettings | None = None, max_age=0, pdl=0, mixed_schedule=None):
+                 settings: AmgSettings | None = None, max_age=0, pdl=0, mixed_schedule=None,
+                 background_rebuild=False):
         cfg = ServerConfigStruct()
         _lib.cfdb_default_server_config(C.byref(cfg))
         cfg.slots, cfg.hbm_budget_bytes, cfg.precision = int(slots), float(hbm_budget_bytes), int(precision)
@@ -57,6 +58,7 @@ class Server:
         cfg.pdl = int(pdl)
         if mixed_schedule is not None:  # (sweeps, weight) of the mixed V-cycle
             cfg.mixed_sweeps, cfg.mixed_weight = int(mixed_schedule[0]), float(mixed_schedule[1])
+        cfg.background_rebuild = 1 if background_rebuild else 0
         h = _vp()
         _check(_lib.cfdb_server_create(C.byref(cfg), C.byref(h)))
         self._h = h
@@ -115,7 +117,8 @@ class Server:
         i = ServerInfoStruct()
         _check(_lib.cfdb_server_info(self._h, C.byref(i)))
         return {"resident_systems": i.resident_systems, "resident_bytes": i.resident_bytes,
-                "queued": i.queued, "completed": i.completed, "evictions": i.evictions}
+                "queued": i.queued, "completed": i.completed, "evictions": i.evictions,
+                "rebuilds": i.rebuilds, "background_rebuilds": i.background_rebuilds}
 
 
 def _pinned(shape_or_array):

@@ -34,6 +34,12 @@ typedef struct {
                                    other requests' kernels can use */
     int mixed_sweeps;           /* mixed precision: the V-cycle's smoother schedule */
     double mixed_weight;        /* (cfdb_tuning.mixed_sweeps / mixed_weight; 0: the hierarchy's) */
+    int background_rebuild;     /* 1: an aged hierarchy is rebuilt off the request path, on a
+                                   spare system per mesh, from a device copy of the triggering
+                                   request's matrix; requests keep solving with the old one
+                                   until the new one is swapped in (results then depend on
+                                   timing, within the tolerance). 0 (default): rebuilt before
+                                   the triggering request's solve, as the reference does */
 } cfdb_server_config;
 
 typedef struct {
@@ -42,6 +48,8 @@ typedef struct {
     int queued;
     long long completed;
     long long evictions;
+    long long rebuilds;            /* hierarchy rebuilds on the request path (age rule) */
+    long long background_rebuilds; /* hierarchies built in the background and swapped in */
 } cfdb_server_info_t;
 
 typedef struct cfdb_server cfdb_server;

@@ -65,3 +65,31 @@ def test_warm_start_and_budget_eviction(gpu):
     info = s.info()
     assert info["evictions"] >= 1 and info["resident_systems"] < len(cases)
     s.close()
+
+
+@pytest.mark.parametrize("background", [False, True], ids=["inline", "background"])
+def test_age_rule_rebuilds(gpu, background):
+    """Hierarchies are rebuilt after max_age solves of new matrices, on the request path or by
+    the background rebuild thread (swapped in at a later request); every solve meets its
+    tolerance against the oracle's matrix-vector product either way."""
+    import time
+
+    from cfd_b200 import serving as S
+    case, d, u, l, b = _entry(W.tet(6, seed=2))
+    s = S.Server(slots=2, max_age=3, background_rebuild=background)
+    (e,) = S.make_pool(s, [("tet", case, d, u, l, b)], variants=3, seed=5)
+    pat = O.build_pattern(case.n, case.owner, case.neighbour)
+    for k in range(1, 16):
+        dk, uk, lk = e.matrices[k % 3]
+        rhs = e.rhs[k % 3]
+        x, st, _ = s.wait(s.submit(e.mesh_id, k, dk, uk, lk, rhs))
+        a = O.ldu_to_csr(pat, dk, uk, lk)
+        assert st.converged
+        assert np.linalg.norm(rhs - a.matvec(x)) <= 1.05e-8 * np.linalg.norm(rhs)
+        time.sleep(0.05)  # room for the background build between requests
+    info = s.info()
+    if background:
+        assert info["rebuilds"] == 0 and info["background_rebuilds"] >= 2
+    else:
+        assert info["rebuilds"] >= 3 and info["background_rebuilds"] == 0
+    s.close()

@@ -49,13 +49,15 @@ def parse():
     ap.add_argument("--systems", type=int, default=256, help="batch: number of systems")
     ap.add_argument("--tune-cache", default=None, help="batch: autotuner cache file")
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serve: arrival rates (1/s)")
-    ap.add_argument("--requests", type=int, default=200, help="serve: requests per rate")
+    ap.add_argument("--requests", type=int, default=300, help="serve: requests per rate")
+    ap.add_argument("--sat-requests", type=int, default=1000,
+                    help="serve: requests of the saturated trace (all queued at once; also the baseline's trace)")
     ap.add_argument("--repeats", type=int, default=3, help="serve: runs of every load point (spread reported)")
-    ap.add_argument("--slots", type=int, default=4, help="serve: worker slots")
+    ap.add_argument("--slots", type=int, default=6, help="serve: worker slots")
     ap.add_argument("--serve-schedule", default="1,0.85",
                     help="serve: mixed smoother schedule 'sweeps,weight' (the autotuned one of the tet box; "
                          "'0,0' keeps the reference's)")
-    ap.add_argument("--serve-pdl", type=int, default=0, help="serve: programmatic dependent launch (0/1)")
+    ap.add_argument("--serve-pdl", type=int, default=1, help="serve: programmatic dependent launch (0/1)")
     ap.add_argument("--max-age", type=int, default=20,
                     help="serve: hierarchy rebuilt after this many solves of a mesh (AmgCache::max_age; 0: never)")
     ap.add_argument("--serve-rebuild", choices=("background", "inline"), default="background",
@@ -881,8 +883,9 @@ def run_serve(args, rank, world, local_rank):
 
     # plain FP64 drop-in, one request at a time, no warm start
     srv, pool, setup = server(cb.Precision.FP64, 1)
+    n_sat = args.sat_requests
     S.run_load(srv, pool, 0.0, n_req // 2, seed=10, closed_loop=True, warm_start=False)
-    _, base = S.run_load(srv, pool, 0.0, n_req, seed=11, closed_loop=True, warm_start=False)
+    _, base = S.run_load(srv, pool, 0.0, n_sat, seed=11, closed_loop=True, warm_start=False)
     res["one_at_a_time_fp64"] = dict(base, setup_s=setup)
     srv.close()
     for label, prec in (("mixed", cb.Precision.MIXED), ("fp64", cb.Precision.FP64)):
@@ -891,11 +894,12 @@ def run_serve(args, rank, world, local_rank):
         sampler = ClockSampler(local_rank) if label == "mixed" else None
         if sampler:
             sampler.start()
-        # every load point `repeats` times (different arrival seeds): median and spread
-        sat_runs = [S.run_load(srv, pool, 1e6, n_req, seed=11 + 100 * k)[1] for k in range(args.repeats)]
+        # every load point `repeats` times over the same request trace (the saturated one is the
+        # baseline's), so that the spread is the server's and not that of the sampled mesh mix
+        sat_runs = [S.run_load(srv, pool, 1e6, n_sat, seed=11)[1] for _ in range(args.repeats)]
         sweep = []
         for i, r in enumerate(rates):
-            runs = [S.run_load(srv, pool, r, n_req, seed=12 + i + 100 * k)[1] for k in range(args.repeats)]
+            runs = [S.run_load(srv, pool, r, n_req, seed=12 + i)[1] for _ in range(args.repeats)]
             sweep.append(spread(runs))
         clocks = sampler.stop() if sampler else None
         res[label] = {"saturated": spread(sat_runs), "sweep": sweep, "setup_s": setup, "clocks": clocks,
@@ -904,7 +908,7 @@ def run_serve(args, rank, world, local_rank):
     value = res["mixed"]["saturated"]["solves_per_s"]
     line = {
         "metric": SERVE_METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
-        "steps": n_req, "warmup": len(pool_cases),
+        "steps": n_sat, "warmup": len(pool_cases),
         "ms_per_step": 1e3 / value if value else None, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32 (FP64 outer, FP32 V-cycle)",
         "data": "synthetic (seeded generator)",
@@ -913,7 +917,8 @@ def run_serve(args, rank, world, local_rank):
                    "slots": args.slots, "hbm_budget_gb": 150, "rates_hz": rates,
                    "mixed_schedule": args.serve_schedule,
                    "max_age": args.max_age, "served_rebuild": args.serve_rebuild,
-                   "requests_per_rate": n_req, "repeats": args.repeats, "strength_threshold": THETA,
+                   "requests_per_rate": n_req, "saturated_requests": n_sat, "repeats": args.repeats,
+                   "strength_threshold": THETA,
                    "step": "one request: H2D of its matrix (new key) and rhs, hierarchy rebuilt on the "
                            "device when the mesh has served max_age solves (served arms: by the rebuild "
                            "thread when served_rebuild is background), AMG-PCG to 1e-8, D2H of x",

@@ -29,9 +29,10 @@ typedef struct {
                                    one the hierarchy was built from (same matrix_key) does not
                                    trigger it, since the rebuild would reproduce the hierarchy */
     int pdl;                    /* programmatic dependent launch in the resident systems' solves
-                                   (cfdb_tuning.pdl), default 0: with requests overlapping on
-                                   the GPU, kernels scheduled early would hold SM slots that
-                                   other requests' kernels can use */
+                                   (cfdb_tuning.pdl), default 0 (kernels scheduled early hold
+                                   SM slots that other requests' kernels could use; on the
+                                   box/tet serving mix with 6 slots it measured 3-8 % faster,
+                                   and the benchmark turns it on) */
     int mixed_sweeps;           /* mixed precision: the V-cycle's smoother schedule */
     double mixed_weight;        /* (cfdb_tuning.mixed_sweeps / mixed_weight; 0: the hierarchy's) */
     int background_rebuild;     /* 1: an aged hierarchy is rebuilt off the request path, on a

@@ -64,6 +64,8 @@ def parse():
                     help="serve: aged hierarchies rebuilt by the server's rebuild thread while the mesh keeps "
                          "serving, or before the triggering request's solve (the one-at-a-time baseline "
                          "always rebuilds inline, as the reference's AmgCache does)")
+    ap.add_argument("--serve-policy", choices=("fifo", "most_work"), default="fifo",
+                    help="serve: order in which free slots take queued requests")
     ap.add_argument("--size", type=int, default=0, help="override the mesh edge length")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default launch knobs and smoother schedule")
@@ -874,7 +876,7 @@ def run_serve(args, rank, world, local_rank):
         sched = tuple(float(v) for v in args.serve_schedule.split(","))
         srv = S.Server(slots=slots, hbm_budget_bytes=150e9, precision=prec, settings=settings,
                        max_age=args.max_age, pdl=args.serve_pdl, mixed_schedule=(int(sched[0]), sched[1]),
-                       background_rebuild=background)
+                       background_rebuild=background, schedule=args.serve_policy)
         pool = S.make_pool(srv, pool_cases, variants=3, seed=7)
         t0 = time.perf_counter()
         for e in pool:  # hierarchy builds (AmgCache setup), not timed below
@@ -916,7 +918,7 @@ def run_serve(args, rank, world, local_rank):
                    "tet_edges": list(W.SERVE_TET_EDGES), "tet_share": 0.25, "repeat_share": 0.3,
                    "slots": args.slots, "hbm_budget_gb": 150, "rates_hz": rates,
                    "mixed_schedule": args.serve_schedule,
-                   "max_age": args.max_age, "served_rebuild": args.serve_rebuild,
+                   "max_age": args.max_age, "served_rebuild": args.serve_rebuild, "policy": args.serve_policy,
                    "requests_per_rate": n_req, "saturated_requests": n_sat, "repeats": args.repeats,
                    "strength_threshold": THETA,
                    "step": "one request: H2D of its matrix (new key) and rhs, hierarchy rebuilt on the "

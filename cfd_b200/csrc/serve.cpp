@@ -325,13 +325,35 @@ void worker_loop(cfdb_server* sp) {
     cudaSetDevice(s.device);
     std::unique_lock<std::mutex> lk(s.mu);
     for (;;) {
-        // first queued request whose mesh is idle and whose system is resident or fits
+        // the first queued request whose mesh is idle and whose system is resident or fits;
+        // with the most-work-first policy, the meshes' first queued requests are tried in
+        // order of the cells queued on each mesh (ties: queue order), so that at saturation
+        // the long per-mesh chains start first and the run does not end on one of them
         std::shared_ptr<Request> q;
         Resident* r = nullptr;
         bool created = false;
+        using QueueIt = std::deque<std::shared_ptr<Request>>::iterator;
+        std::vector<QueueIt> order;
         for (;;) {
             if (s.stopping && s.queue.empty()) return;
-            for (auto it = s.queue.begin(); it != s.queue.end(); ++it) {
+            order.clear();
+            if (s.cfg.schedule == CFDB_SCHEDULE_MOST_WORK) {
+                std::unordered_map<int, std::pair<double, QueueIt>> per_mesh;
+                for (auto it = s.queue.begin(); it != s.queue.end(); ++it) {
+                    auto ins = per_mesh.try_emplace((*it)->mesh, 0.0, it);
+                    ins.first->second.first += static_cast<double>(s.meshes[(*it)->mesh].n);
+                }
+                std::vector<std::pair<double, QueueIt>> by_work;
+                by_work.reserve(per_mesh.size());
+                for (auto& kv : per_mesh) by_work.push_back(kv.second);
+                std::sort(by_work.begin(), by_work.end(), [](const auto& a, const auto& b) {
+                    return a.first != b.first ? a.first > b.first : (*a.second)->ticket < (*b.second)->ticket;
+                });
+                for (auto& w : by_work) order.push_back(w.second);
+            } else {
+                for (auto it = s.queue.begin(); it != s.queue.end(); ++it) order.push_back(it);
+            }
+            for (QueueIt it : order) {
                 auto& cand = *it;
                 auto rit = s.resident.find(cand->mesh);
                 if (rit != s.resident.end()) {
@@ -442,12 +464,15 @@ void cfdb_default_server_config(cfdb_server_config* c) {
     c->mixed_sweeps = 0;
     c->mixed_weight = 0.0;
     c->background_rebuild = 0;
+    c->schedule = CFDB_SCHEDULE_FIFO;
 }
 
 int cfdb_server_create(const cfdb_server_config* cfg, cfdb_server** out) {
     return guarded_s([&] {
         if (cfg == nullptr || out == nullptr) fail(CFDB_ERR_BAD_ARG, "null argument");
         if (cfg->slots < 1 || cfg->slots > 64) fail(CFDB_ERR_BAD_ARG, "slots must be in 1..64");
+        if (cfg->schedule != CFDB_SCHEDULE_FIFO && cfg->schedule != CFDB_SCHEDULE_MOST_WORK)
+            fail(CFDB_ERR_BAD_ARG, "unknown schedule");
         if (!(cfg->hbm_budget_bytes > 0)) fail(CFDB_ERR_BAD_ARG, "HBM budget must be positive");
         if (!cfdb_device_available()) fail(CFDB_ERR_NO_DEVICE, "no CUDA device: this library has no host fallback");
         auto s = std::make_unique<cfdb_server>();

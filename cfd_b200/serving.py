@@ -23,7 +23,7 @@ _pd = C.POINTER(C.c_double)
 class ServerConfigStruct(C.Structure):
     _fields_ = [("slots", _i), ("hbm_budget_bytes", _d), ("precision", _i),
                 ("settings", AmgSettingsStruct), ("max_age", _i), ("pdl", _i),
-                ("mixed_sweeps", _i), ("mixed_weight", _d), ("background_rebuild", _i)]
+                ("mixed_sweeps", _i), ("mixed_weight", _d), ("background_rebuild", _i), ("schedule", _i)]
 
 
 class ServerInfoStruct(C.Structure):
@@ -49,7 +49,7 @@ _p("cfdb_server_info", [_vp, C.POINTER(ServerInfoStruct)])
 class Server:
     def __init__(self, slots=4, hbm_budget_bytes=150e9, precision=Precision.MIXED,
                  settings: AmgSettings | None = None, max_age=0, pdl=0, mixed_schedule=None,
-                 background_rebuild=False):
+                 background_rebuild=False, schedule="fifo"):
         cfg = ServerConfigStruct()
         _lib.cfdb_default_server_config(C.byref(cfg))
         cfg.slots, cfg.hbm_budget_bytes, cfg.precision = int(slots), float(hbm_budget_bytes), int(precision)
@@ -59,6 +59,7 @@ class Server:
         if mixed_schedule is not None:  # (sweeps, weight) of the mixed V-cycle
             cfg.mixed_sweeps, cfg.mixed_weight = int(mixed_schedule[0]), float(mixed_schedule[1])
         cfg.background_rebuild = 1 if background_rebuild else 0
+        cfg.schedule = {"fifo": 0, "most_work": 1}[schedule]
         h = _vp()
         _check(_lib.cfdb_server_create(C.byref(cfg), C.byref(h)))
         self._h = h
@@ -147,8 +148,9 @@ def make_pool(server: Server, pool_cases, variants=3, seed=0, coefficient_jitter
     """Registers the meshes of `pool_cases` [(kind, case, diag, upper, lower, source)] and
     prepares page-locked coefficient variants: the finalized matrix with its face coefficients
     scaled by LogNormal(0, coefficient_jitter) (diagonal adjusted so row sums are kept) and
-    zero-mean random right-hand sides; `x_buffers` page-locked solution buffers per mesh (more
-    are allocated on demand when more requests of one mesh are in flight)."""
+    zero-mean random right-hand sides; `x_buffers` page-locked solution buffers per mesh (run_load
+    adds more before its clock starts when its trace can have more requests of one mesh in
+    flight)."""
     rng = np.random.default_rng(seed)
     pool = []
     for kind, c, d, u, l, b in pool_cases:
@@ -203,17 +205,14 @@ def run_load(server: Server, pool: list, rate_hz: float, n_requests: int, repeat
                                     service=times[2] - times[1], iterations=st.iterations,
                                     converged=st.converged, residual=st.residual))
 
-    th = threading.Thread(target=collector, daemon=True)
-    th.start()
-    t0 = time.perf_counter()
+    # the request trace, drawn before the clock starts (arrival, entry, key, variant, rhs,
+    # repeat), and enough page-locked solution buffers for every request of a mesh to be in
+    # flight at once, so that no buffer is page-locked while the server runs
+    trace = []
     ta = 0.0
-    done_events = []
     for i in range(n_requests):
         if not closed_loop:
             ta += rng.exponential(1.0 / rate_hz)
-            now = time.perf_counter() - t0
-            if ta > now:
-                time.sleep(ta - now)
         kind = "tet" if ("tet" in by_kind and rng.random() < tet_frac) else \
             ("box" if "box" in by_kind else kinds[0])
         group = by_kind[kind]
@@ -227,6 +226,22 @@ def run_load(server: Server, pool: list, rate_hz: float, n_requests: int, repeat
             mi = key % len(e.matrices)
             last[e.mesh_id] = (key, mi)
         bi = int(rng.integers(len(e.rhs)))
+        trace.append((ta, e, key, mi, bi, bool(rep)))
+    if not closed_loop:
+        need = {}
+        for _, e, *_ in trace:
+            need[e.mesh_id] = need.get(e.mesh_id, 0) + 1
+        for e in pool:
+            while len(e.free_x) < need.get(e.mesh_id, 0):
+                e.free_x.append(_pinned(e.n))
+    th = threading.Thread(target=collector, daemon=True)
+    th.start()
+    t0 = time.perf_counter()
+    for i, (ta, e, key, mi, bi, rep) in enumerate(trace):
+        if not closed_loop:
+            now = time.perf_counter() - t0
+            if ta > now:
+                time.sleep(ta - now)
         d, u, l = e.matrices[mi]
         with lock:
             x = e.free_x.pop() if e.free_x else _pinned(e.n)
@@ -236,7 +251,7 @@ def run_load(server: Server, pool: list, rate_hz: float, n_requests: int, repeat
         # and the right-hand side; the solution comes back
         h2d = 8 * (e.n + (0 if rep else len(d) + len(u) + len(l)))
         pending.put((ticket, e, x, {"mesh": e.mesh_id, "kind": e.kind, "n": e.n,
-                                    "repeat": bool(rep), "h2d": h2d, "d2h": 8 * e.n}))
+                                    "repeat": rep, "h2d": h2d, "d2h": 8 * e.n}))
         if closed_loop:
             while True:
                 with lock:

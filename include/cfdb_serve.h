@@ -19,6 +19,13 @@
 extern "C" {
 #endif
 
+/* Order in which free worker slots take queued requests. */
+enum {
+    CFDB_SCHEDULE_FIFO = 0,      /* the first queued request whose mesh is free */
+    CFDB_SCHEDULE_MOST_WORK = 1  /* the first queued request of the free mesh with the most
+                                    queued cells (requests of one mesh stay in order) */
+};
+
 typedef struct {
     int slots;                  /* concurrent worker slots (streams), default 4 */
     double hbm_budget_bytes;    /* device bytes the resident systems may hold, default 150e9 */
@@ -41,6 +48,7 @@ typedef struct {
                                    until the new one is swapped in (results then depend on
                                    timing, within the tolerance). 0 (default): rebuilt before
                                    the triggering request's solve, as the reference does */
+    int schedule;               /* CFDB_SCHEDULE_*, default FIFO */
 } cfdb_server_config;
 
 typedef struct {

@@ -22,7 +22,8 @@ def _cases():
                                 W.graded(12, seed=4))]
 
 
-def test_same_result_alone_and_in_the_mix(gpu):
+@pytest.mark.parametrize("schedule", ["fifo", "most_work"])
+def test_same_result_alone_and_in_the_mix(gpu, schedule):
     from cfd_b200.serving import Server
     cases = _cases()
     alone = []
@@ -33,7 +34,7 @@ def test_same_result_alone_and_in_the_mix(gpu):
         assert st.converged
         alone.append(x)
         s.close()
-    s = Server(slots=4)
+    s = Server(slots=4, schedule=schedule)
     ids = [s.add_mesh(c.n, c.owner, c.neighbour) for c, *_ in cases]
     tickets = [s.submit(mid, 1, d, u, l, b) for mid, (c, d, u, l, b) in zip(ids, cases)]
     tickets += [s.submit(mid, 1, d, u, l, b) for mid, (c, d, u, l, b) in zip(ids, cases)]

@@ -22,6 +22,16 @@ struct Error : std::runtime_error {
 void check_cuda(cudaError_t e, const char* what);
 #define CFDB_CUDA(call) ::cfdb::check_cuda((call), #call)
 
+// Fails with status 4 (CFDB_ERR_NO_DEVICE of include/cfdb.h) when no CUDA device is visible:
+// the library has no host path to fall back to.
+inline void require_cuda_device() {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        (void)cudaGetLastError();
+        fail(4, "no CUDA device: this library has no host fallback");
+    }
+}
+
 // Host CSR matrix (int32 indices, FP64 values).
 struct HostCsr {
     int n_rows = 0;

@@ -16,6 +16,8 @@
 
 #include "common.hpp"
 
+static_assert(CFDB_ERR_NO_DEVICE == 4, "require_cuda_device (common.hpp) reports status 4");
+
 namespace cfdb {
 void set_thread_error(const std::string& msg);
 } // namespace cfdb
@@ -328,6 +330,7 @@ int cfdb_fv_create(int n_cells, int n_faces, int n_internal_faces, const int* ow
         for (int b = 0; b < nb; ++b)
             if (boundary_kind[b] < CFDB_BC_VELOCITY_INLET || boundary_kind[b] > CFDB_BC_EMPTY)
                 fail(CFDB_ERR_BAD_ARG, "cfdb_fv_create: unknown boundary kind");
+        require_cuda_device();
         auto* fv = new cfdb_fv;
         try {
             CFDB_CUDA(cudaGetDevice(&fv->device));

@@ -683,6 +683,7 @@ int cfdb_device_fv_create(const cfdb_fv_mesh_view* v, cfdb_device_fv** out) {
         for (int i = 0; i < nf; ++i)
             if (v->owner[i] < 0 || v->owner[i] >= nc || (i < nif && (v->neighbour[i] < 0 || v->neighbour[i] >= nc)))
                 fail(CFDB_ERR_BAD_ARG, "DeviceFv: face " + std::to_string(i) + " addresses a cell out of range");
+        require_cuda_device();
         auto* fv = new cfdb_device_fv;
         try {
             CFDB_CUDA(cudaGetDevice(&fv->device));

@@ -118,28 +118,34 @@ def build_ref(force: bool = False) -> str | None:
 
 
 DROPIN_EXE = os.path.join(REF_DIR, "dropin_ldu")
+DROPIN_FLOW_EXE = os.path.join(REF_DIR, "dropin_flow")
 DROPIN_SOURCES = [s for s in REF_EIGEN_SOURCES] + ["src/gpu/src/krylov_openmp.cpp"]
 
 
 def build_dropin(force: bool = False) -> str | None:
-    """tests/cpp/test_dropin_ldu.cpp with the reference's unchanged LduMatrix / AMG / mesh /
-    FvGeometry sources and its host path (krylov_openmp.cpp), compiled against this project's
-    C++ front end (include/cfd_gpu_krylov.hpp and include/cfd_gpu_fv.hpp in place of the
-    reference's cfd/gpu headers) and linked with libcfdb.so: the reference's callers driving the
-    product. Built where the reference checkout and the product library are present; the binary
-    travels with the tree (rpath to cfd_b200/)."""
+    """The drop-in programs: tests/cpp/test_dropin_ldu.cpp with the reference's unchanged
+    LduMatrix / AMG / mesh / FvGeometry sources and its host path (krylov_openmp.cpp), and
+    tests/cpp/test_dropin_flow.cpp with the same sources plus its unchanged flow_solver.cpp,
+    compiled against this project's C++ front end (include/cfd_gpu_krylov.hpp and
+    include/cfd_gpu_fv.hpp in place of the reference's cfd/gpu headers) and linked with
+    libcfdb.so: the reference's callers driving the product. Built where the reference checkout
+    and the product library are present; the binaries travel with the tree (rpath to
+    cfd_b200/). Returns the LDU program's path."""
     root = os.path.dirname(HERE)
     lib = os.path.join(root, "cfd_b200", "libcfdb.so")
     if not reference_available() or not os.path.exists(lib):
         return DROPIN_EXE if os.path.exists(DROPIN_EXE) else None
     srcs = [os.path.join(REFERENCE_ROOT, s) for s in DROPIN_SOURCES]
-    test = os.path.join(root, "tests", "cpp", "test_dropin_ldu.cpp")
+    flow_src = os.path.join(REFERENCE_ROOT, REF_FLOW_SOURCES[0])
+    tests = {DROPIN_EXE: os.path.join(root, "tests", "cpp", "test_dropin_ldu.cpp"),
+             DROPIN_FLOW_EXE: os.path.join(root, "tests", "cpp", "test_dropin_flow.cpp")}
     ours = {"krylov.hpp": os.path.join(root, "include", "cfd_gpu_krylov.hpp"),
             "fv_device.hpp": os.path.join(root, "include", "cfd_gpu_fv.hpp")}
     standin = os.path.join(HERE, "eigen_standin")
-    deps = srcs + [test, lib, os.path.join(REFERENCE_ROOT, "src/gpu/src/krylov_kernels.inc")] + list(ours.values())
+    deps = srcs + [flow_src, lib, os.path.join(REFERENCE_ROOT, "src/gpu/src/krylov_kernels.inc")] + list(ours.values())
+    deps += list(tests.values())
     deps += [os.path.join(standin, "Eigen", f) for f in os.listdir(os.path.join(standin, "Eigen"))]
-    if not (force or _stale(DROPIN_EXE, deps)):
+    if not (force or any(_stale(exe, deps) for exe in tests)):
         return DROPIN_EXE
     # <cfd/gpu/...> resolves to this project's headers; the other reference headers as they are
     shadow = os.path.join(REF_DIR, "dropin_include", "cfd", "gpu")
@@ -154,7 +160,7 @@ def build_dropin(force: bool = False) -> str | None:
     objdir = os.path.join(REF_DIR, "dropin_obj")
     os.makedirs(objdir, exist_ok=True)
     from concurrent.futures import ThreadPoolExecutor
-    units = srcs + [test]
+    units = srcs + [flow_src] + list(tests.values())
     objs = [os.path.join(objdir, f"{i:02d}_{os.path.basename(u)}.o") for i, u in enumerate(units)]
 
     def compile_one(pair):
@@ -162,10 +168,14 @@ def build_dropin(force: bool = False) -> str | None:
 
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         list(ex.map(compile_one, zip(units, objs)))
-    tmp = DROPIN_EXE + f".tmp{os.getpid()}"
-    subprocess.run(["g++", "-fopenmp", *objs, "-L", os.path.dirname(lib), "-lcfdb",
-                    "-Wl,-rpath,$ORIGIN/../../cfd_b200", "-o", tmp], check=True)
-    os.replace(tmp, DROPIN_EXE)
+    common = objs[:len(srcs)]
+    flow_obj = objs[len(srcs)]
+    test_objs = dict(zip(tests, objs[len(srcs) + 1:]))
+    for exe, extra in ((DROPIN_EXE, []), (DROPIN_FLOW_EXE, [flow_obj])):
+        tmp = exe + f".tmp{os.getpid()}"
+        subprocess.run(["g++", "-fopenmp", *common, *extra, test_objs[exe], "-L", os.path.dirname(lib), "-lcfdb",
+                        "-Wl,-rpath,$ORIGIN/../../cfd_b200", "-o", tmp], check=True)
+        os.replace(tmp, exe)
     return DROPIN_EXE
 
 

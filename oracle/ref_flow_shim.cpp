@@ -16,6 +16,7 @@
 #include <exception>
 #include <map>
 #include <memory>
+#include <stdexcept>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -83,8 +84,8 @@ void put_vec3s(const std::vector<Vec3>& v, double* out) {
 
 extern "C" {
 
-// FlowSolver(mesh, conditions, settings) (flow_solver.cpp:35-67) on a mesh whose patches are
-// named "p0".."p{n_patches-1}" (refx_mesh_build). Per patch: kind (FlowBoundary: 0 inlet,
+// FlowSolver(mesh, conditions, settings) (flow_solver.cpp:35-67), one condition per mesh patch
+// in the mesh's patch order (n_patches of them). Per patch: kind (FlowBoundary: 0 inlet,
 // 1 wall, 2 outlet, 3 symmetry, 4 empty), velocity (3), pressure. real = {nu, alpha_u, alpha_p,
 // p tolerance, p rel_tolerance, u tolerance, u rel_tolerance}; ints = {n_non_orth_correctors,
 // p solver type, p max_iterations, u solver type, u max_iterations, convection scheme,
@@ -93,13 +94,14 @@ void* refx_flow_create(const void* mesh, int n_patches, const int* kind, const d
                        const double* pressure, const double* real, const int* ints) {
     try {
         const auto& m = *static_cast<const cfd::mesh::Mesh*>(mesh);
+        if (n_patches != static_cast<int>(m.patches().size())) throw std::invalid_argument("one condition per patch");
         std::map<std::string, cfd::fv::BoundaryCondition> conditions;
         for (int p = 0; p < n_patches; ++p) {
             cfd::fv::BoundaryCondition c;
             c.kind = static_cast<cfd::fv::FlowBoundary>(kind[p]);
             c.velocity = Vec3(velocity[3 * p], velocity[3 * p + 1], velocity[3 * p + 2]);
             c.pressure = pressure[p];
-            conditions["p" + std::to_string(p)] = c;
+            conditions[m.patches()[static_cast<std::size_t>(p)].name] = c;
         }
         cfd::fv::FlowSettings s;
         s.nu = real[0];
@@ -214,6 +216,17 @@ int refx_flow_pressure_correction(void* h, int relax_p, const double* u_prev, co
         if (phi_prev != nullptr) pp.assign(phi_prev, phi_prev + f.n_faces);
         *initial_residual = ((*f.solver).*member_of(PressureCorrection{}))(
             *f.sys, relax_p != 0, u_prev != nullptr ? &up : nullptr, phi_prev != nullptr ? &pp : nullptr);
+    });
+}
+
+// FlowSolver::simple_iteration (flow_solver.cpp:849-866): residuals = {u (3), p, continuity}.
+int refx_flow_simple_iteration(void* h, double* residuals) {
+    return guarded([&] {
+        auto& f = *static_cast<FlowHandle*>(h);
+        const cfd::fv::Residuals r = f.solver->simple_iteration();
+        for (int k = 0; k < 3; ++k) residuals[k] = r.u[k];
+        residuals[3] = r.p;
+        residuals[4] = r.continuity;
     });
 }
 

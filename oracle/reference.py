@@ -86,7 +86,8 @@ def lib():
                                ("refx_flow_momentum", [_vp, _d, _i]),
                                ("refx_flow_momentum_arrays", [_vp, _pd, _pd, _pd, _pd]),
                                ("refx_flow_solve_momentum", [_vp, _pd]),
-                               ("refx_flow_pressure_correction", [_vp, _i, _pd, _pd, _pd])):
+                               ("refx_flow_pressure_correction", [_vp, _i, _pd, _pd, _pd]),
+                               ("refx_flow_simple_iteration", [_vp, _pd])):
                 getattr(R, name).argtypes = args
                 getattr(R, name).restype = _i
         _declared = True
@@ -520,8 +521,8 @@ GRADIENT = {"Gauss": 0, "LeastSquares": 1, "GaussCorrected": 2}
 
 
 class RefFlow:
-    """cfd::fv::FlowSolver on a reference mesh built by RefMesh.build (patches "p0", "p1", ...),
-    driven one SIMPLE step at a time (oracle/ref_flow_shim.cpp)."""
+    """cfd::fv::FlowSolver on a reference mesh (one condition per patch, in the mesh's patch
+    order), driven one SIMPLE step at a time (oracle/ref_flow_shim.cpp)."""
 
     def __init__(self, mesh: RefMesh, patches, nu=1e-3, alpha_u=0.7, alpha_p=0.3, n_non_orth=0,
                  p_solver=("GpuCg", 1e-10, 0.01, 500), u_solver=("GpuBiCgStab", 1e-10, 0.1, 1000),
@@ -576,6 +577,12 @@ class RefFlow:
         r = np.empty(3)
         self._call("refx_flow_solve_momentum", _dp(r))
         return r
+
+    def simple_iteration(self):
+        """FlowSolver::simple_iteration; returns (u residuals (3), p residual, continuity)."""
+        r = np.empty(5)
+        self._call("refx_flow_simple_iteration", _dp(r))
+        return r[:3].copy(), float(r[3]), float(r[4])
 
     def pressure_correction(self, relax_p=True, u_prev=None, phi_prev=None):
         """FlowSolver::pressure_correction on the momentum system; returns the initial residual."""

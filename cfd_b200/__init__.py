@@ -155,7 +155,7 @@ class TuningStruct(C.Structure):
     _fields_ = [("target_tiles", _i), ("wide_row", _i), ("lanes_div", _i), ("fuse_first", _i),
                 ("sell_rows", _i), ("krylov_pair", _i), ("tail_rows", _i),
                 ("col16", _i), ("pdl", _i), ("wait_polls", _i), ("mixed_sweeps", _i),
-                ("mixed_weight", _d)]
+                ("mixed_weight", _d), ("tail_cluster", _i)]
 
 
 _proto("cfdb_default_tuning", [_P(TuningStruct)], None)
@@ -884,12 +884,13 @@ class Tuning:
     wait_polls: int = 1 << 22  # bounded device waits; < 0 makes them give up at once (tests)
     mixed_sweeps: int = 0  # mixed precision: Jacobi sweeps per level (0: the hierarchy's)
     mixed_weight: float = 0.0  # mixed precision: Jacobi weight (0: the hierarchy's)
+    tail_cluster: int = 0  # tail as one cluster of this many CTAs (2..16); 0: cooperative grid
 
     def _c(self):
         return TuningStruct(int(self.target_tiles), int(self.wide_row), int(self.lanes_div),
                             int(self.fuse_first), int(self.sell_rows), int(self.krylov_pair),
                             int(self.tail_rows), int(self.col16), int(self.pdl), int(self.wait_polls),
-                            int(self.mixed_sweeps), float(self.mixed_weight))
+                            int(self.mixed_sweeps), float(self.mixed_weight), int(self.tail_cluster))
 
 
 def _set_system_tuning(self, t: Tuning) -> None:

@@ -10,12 +10,14 @@ The knobs are those of `Tuning` (include/cfdb.h, cfdb_tuning):
 * sell_rows    - rows per CTA of SELL operators (one row per thread per pass),
 * krylov_pair  - level-0 Krylov SpMV kernels take two rows per thread per pass, or one,
 * tail_rows    - coarse levels of at most this many rows run in one persistent kernel,
+* tail_cluster - that kernel as one thread-block cluster of this many CTAs (0: a cooperative
+                 grid); searched jointly with tail_rows,
 * mixed_sweeps, mixed_weight - the smoother schedule of the mixed-precision V-cycle (Jacobi
                  sweeps per level before and after the coarse correction, and the weight); the
                  FP64 path keeps the hierarchy's (the reference's 2 sweeps, weight 0.7).
 
-The launch knobs are searched by coordinate descent from the defaults: each knob in turn is
-swept over its candidate values with the others fixed, the best value kept, and the pass
+The launch knobs are searched by coordinate descent from the defaults: each knob (or a tuple
+of knobs searched jointly) in turn is swept over its candidate values with the others fixed, the best value kept, and the pass
 repeated until no knob changes (at most `passes` passes). Their objective is the device time of
 a fixed number of CG iterations (tolerance 0, so every system runs exactly `iterations`
 iterations) through the captured graphs of the real solve path, median of `reps` runs. The
@@ -41,13 +43,14 @@ CANDIDATES = {
     "fuse_first": [0, 1],
     "sell_rows": [256, 512, 1024],
     "krylov_pair": [0, 1],
-    "tail_rows": [0, 1024, 8192, 65536, 131072],
+    ("tail_rows", "tail_cluster"): [(0, 0), (1024, 0), (8192, 0), (65536, 0), (131072, 0),
+                                    (8192, 8), (8192, 16), (16384, 16)],
 }
 
 # knobs whose best value depends on the smoother schedule: with one sweep per level the first
 # sweeps are never fused, so the persistent tail (which needs the unfused schedule) and the
 # shapes of the kernels it replaces are searched again once the schedule is chosen
-SCHEDULE_KNOBS = ("tail_rows", "sell_rows", "target_tiles")
+SCHEDULE_KNOBS = (("tail_rows", "tail_cluster"), "sell_rows", "target_tiles")
 
 
 def _key(t: Tuning) -> tuple:
@@ -74,10 +77,12 @@ def coordinate_search(evaluate: Callable[[Tuning], float], start: Tuning | None 
     for _ in range(max(passes, 1)):
         changed = False
         for knob, values in cand.items():
+            names = knob if isinstance(knob, tuple) else (knob,)
             for v in values:
-                if getattr(best, knob) == v:
+                vals = v if isinstance(knob, tuple) else (v,)
+                if tuple(getattr(best, k) for k in names) == tuple(vals):
                     continue
-                t = dataclasses.replace(best, **{knob: v})
+                t = dataclasses.replace(best, **dict(zip(names, vals)))
                 val = ev(t)
                 if val < best_v:
                     best, best_v, changed = t, val, True

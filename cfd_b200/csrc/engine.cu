@@ -1028,14 +1028,40 @@ template <class T> void Engine::prepare_tail() {
             c = o;
         }
     }
-    // grid: co-resident CTAs (cooperative launch), no more than the largest phase can use
     const size_t smem = sizeof(T) == 8 ? coarse_smem64_ : coarse_smem32_;
-    CFDB_CUDA(cudaFuncSetAttribute(k_vc_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    int per_sm = 0, sms = 0;
-    CFDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vc_tail<T>, kBlock, smem));
-    CFDB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
-    if (per_sm <= 0) return;  // cannot be co-resident: keep the separate kernels
-    grid = std::max(1, std::min(per_sm * sms, max_blocks));
+    if (tuning_.tail_cluster > 0) {
+        // one cluster of tail_cluster CTAs; kept only if such a cluster can be resident
+        const int cs = std::min(std::max(tuning_.tail_cluster, 2), 16);
+        CFDB_CUDA(cudaFuncSetAttribute(k_vc_tail<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem)));
+        CFDB_CUDA(cudaFuncSetAttribute(k_vc_tail<T, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        cudaLaunchConfig_t q{};
+        q.gridDim = dim3(static_cast<unsigned>(cs));
+        q.blockDim = dim3(kBlock);
+        q.dynamicSmemBytes = smem;
+        cudaLaunchAttribute a[1];
+        a[0].id = cudaLaunchAttributeClusterDimension;
+        a[0].val.clusterDim.x = static_cast<unsigned>(cs);
+        a[0].val.clusterDim.y = 1;
+        a[0].val.clusterDim.z = 1;
+        q.attrs = a;
+        q.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, k_vc_tail<T, true>, &q) != cudaSuccess || clusters <= 0) {
+            (void)cudaGetLastError();
+            return; // no such cluster fits: keep the separate kernels
+        }
+        grid = cs;
+    } else {
+        // grid: co-resident CTAs (cooperative launch), no more than the largest phase can use
+        CFDB_CUDA(cudaFuncSetAttribute(k_vc_tail<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem)));
+        int per_sm = 0, sms = 0;
+        CFDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vc_tail<T, false>, kBlock, smem));
+        CFDB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+        if (per_sm <= 0) return;  // cannot be co-resident: keep the separate kernels
+        grid = std::max(1, std::min(per_sm * sms, max_blocks));
+    }
     TailPhase<T>* d = arena_.alloc<TailPhase<T>>(ph.size());
     CFDB_CUDA(cudaMemcpyAsync(d, ph.data(), sizeof(TailPhase<T>) * ph.size(), cudaMemcpyHostToDevice, stream_));
     CFDB_CUDA(cudaStreamSynchronize(stream_));
@@ -1064,12 +1090,21 @@ template <class T> void Engine::launch_tail(cudaStream_t s) {
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CFDB_CUDA(cudaLaunchKernelEx(&cfg, k_vc_tail<T>, ph, count, cb_, n_ctiles_, b_lv, x_lv,
-                                 static_cast<const int*>(block_level_), tail_bar_, error_, tuning_.wait_polls));
+    if (tuning_.tail_cluster > 0) {
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = static_cast<unsigned>(grid);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        CFDB_CUDA(cudaLaunchKernelEx(&cfg, k_vc_tail<T, true>, ph, count, cb_, n_ctiles_, b_lv, x_lv,
+                                     static_cast<const int*>(block_level_), tail_bar_, error_, tuning_.wait_polls));
+    } else {
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        CFDB_CUDA(cudaLaunchKernelEx(&cfg, k_vc_tail<T, false>, ph, count, cb_, n_ctiles_, b_lv, x_lv,
+                                     static_cast<const int*>(block_level_), tail_bar_, error_, tuning_.wait_polls));
+    }
 }
 
 template <class T>

@@ -51,6 +51,8 @@ struct Tuning {
     int wait_polls = 1 << 22;   // poll limit of the bounded device waits (< 0: give up at once)
     int mixed_sweeps = 0;       // mixed precision: Jacobi sweeps per level (0: the hierarchy's)
     double mixed_weight = 0.0;  // mixed precision: Jacobi weight (0: the hierarchy's)
+    int tail_cluster = 0;       // the tail as one thread-block cluster of this many CTAs (2..16)
+                                // separated by the cluster barrier; 0: a cooperative grid
 };
 
 struct SolveRequest {

@@ -1361,7 +1361,18 @@ __device__ __forceinline__ void tail_rows(const Sell<T>& m, int n, XA xa, F f) {
     }
 }
 
-template <class T>
+// Barrier over the CTAs of one thread-block cluster (all of them run every phase): the
+// hardware cluster barrier with release / acquire semantics at cluster scope, so the global
+// writes of one phase are visible to the loads of the next. No polling: it cannot time out.
+__device__ __forceinline__ void tail_cluster_barrier() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// The phases of the small coarse levels and the coarse solve in one launch. kCluster = false:
+// a cooperative grid of co-resident CTAs separated by the bounded grid barrier; kCluster =
+// true: a single thread-block cluster (gridDim.x = cluster size) separated by the cluster
+// barrier, for levels small enough that a few SMs keep up with them.
+template <class T, bool kCluster>
 static __global__ void __launch_bounds__(kBlock, 4) k_vc_tail(const TailPhase<T>* __restrict__ phases, int n_phases,
                                                     CoarseBlocks cb, int n_ctiles, T* const* __restrict__ b_level,
                                                     T* const* __restrict__ x_level,
@@ -1414,7 +1425,10 @@ static __global__ void __launch_bounds__(kBlock, 4) k_vc_tail(const TailPhase<T>
                 }
             });
         }
-        if (ph + 1 < n_phases && !tail_barrier(bar, gridDim.x, error, wait_polls)) return;
+        if (ph + 1 < n_phases) {
+            if constexpr (kCluster) tail_cluster_barrier();
+            else if (!tail_barrier(bar, gridDim.x, error, wait_polls)) return;
+        }
     }
 }
 

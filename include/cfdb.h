@@ -450,6 +450,9 @@ typedef struct {
     double mixed_weight; /* mixed precision only: Jacobi weight (0, default: the hierarchy's,
                          0.7); flexible CG tolerates any fixed schedule, and the autotuner picks
                          the one with the shortest time to the tolerance */
+    int tail_cluster; /* with tail_rows: run the tail as one thread-block cluster of this many CTAs
+                         (2..16), its phases separated by the hardware cluster barrier; 0
+                         (default): a cooperative grid with the bounded grid barrier */
 } cfdb_tuning;
 void cfdb_default_tuning(cfdb_tuning* t);
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t);

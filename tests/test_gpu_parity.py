@@ -220,13 +220,16 @@ def test_mixed_precision_reaches_target(gpu, make):
     assert np.linalg.norm(x - xo) <= 1e-5 * np.linalg.norm(xo)
 
 
-@pytest.mark.parametrize("precision,schedule", [("FP64", (0, 0.0)), ("MIXED", (0, 0.0)), ("MIXED", (1, 0.85)),
-                                                 ("MIXED", (3, 0.85))],
-                         ids=["FP64", "MIXED", "MIXED-1sweep", "MIXED-3sweeps"])
-def test_persistent_tail_matches_separate_kernels(gpu, precision, schedule):
-    """The persistent tail kernel (small coarse levels + coarse solve in one cooperative launch)
-    computes every row exactly as the separate per-level kernels do, under the hierarchy's
-    smoother schedule and under the mixed path's tuned ones."""
+@pytest.mark.parametrize("precision,schedule,cluster", [
+    ("FP64", (0, 0.0), 0), ("MIXED", (0, 0.0), 0), ("MIXED", (1, 0.85), 0), ("MIXED", (3, 0.85), 0),
+    ("FP64", (0, 0.0), 16), ("MIXED", (1, 0.85), 8), ("MIXED", (1, 0.85), 16)],
+    ids=["FP64", "MIXED", "MIXED-1sweep", "MIXED-3sweeps", "FP64-cluster16", "MIXED-1sweep-cluster8",
+         "MIXED-1sweep-cluster16"])
+def test_persistent_tail_matches_separate_kernels(gpu, precision, schedule, cluster):
+    """The persistent tail kernel (small coarse levels + coarse solve in one launch: a
+    cooperative grid, or one thread-block cluster) computes every row exactly as the separate
+    per-level kernels do, under the hierarchy's smoother schedule and under the mixed path's
+    tuned ones."""
     cb = gpu
     case = W.graded(24)
     up, lo, diag, src = _assembled(case)
@@ -236,7 +239,8 @@ def test_persistent_tail_matches_separate_kernels(gpu, precision, schedule):
     tol = 1e-10 * np.linalg.norm(src)
     out = []
     for tail in (0, 10**6):
-        ds.set_tuning(cb.Tuning(tail_rows=tail, mixed_sweeps=schedule[0], mixed_weight=schedule[1]))
+        ds.set_tuning(cb.Tuning(tail_rows=tail, mixed_sweeps=schedule[0], mixed_weight=schedule[1],
+                                tail_cluster=cluster if tail else 0))
         x = np.zeros(case.n)
         st = ds.solve(diag, up, lo, src, x, cb.Method.Cg, True, cb.SolveControl(tol, 500))
         z = ds.apply_amg(np.random.default_rng(3).standard_normal(case.n))

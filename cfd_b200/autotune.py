@@ -11,7 +11,7 @@ The knobs are those of `Tuning` (include/cfdb.h, cfdb_tuning):
 * krylov_pair  - level-0 Krylov SpMV kernels take two rows per thread per pass, or one,
 * tail_rows    - coarse levels of at most this many rows run in one persistent kernel,
 * tail_cluster - that kernel as one thread-block cluster of this many CTAs (0: a cooperative
-                 grid); searched jointly with tail_rows,
+                 grid), searched jointly with tail_rows (the candidates keep the grid form),
 * mixed_sweeps, mixed_weight - the smoother schedule of the mixed-precision V-cycle (Jacobi
                  sweeps per level before and after the coarse correction, and the weight); the
                  FP64 path keeps the hierarchy's (the reference's 2 sweeps, weight 0.7).
@@ -43,8 +43,9 @@ CANDIDATES = {
     "fuse_first": [0, 1],
     "sell_rows": [256, 512, 1024],
     "krylov_pair": [0, 1],
-    ("tail_rows", "tail_cluster"): [(0, 0), (1024, 0), (8192, 0), (65536, 0), (131072, 0),
-                                    (8192, 8), (8192, 16), (16384, 16)],
+    # the single-cluster tail (tail_cluster > 0) is not a candidate: on tet 95^3 x 6 it took
+    # 299 us (16 CTAs) to 1,103 us (4 CTAs) per V-cycle where the separate kernels take ~50 us
+    ("tail_rows", "tail_cluster"): [(0, 0), (1024, 0), (8192, 0), (65536, 0), (131072, 0)],
 }
 
 # knobs whose best value depends on the smoother schedule: with one sweep per level the first

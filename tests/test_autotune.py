@@ -12,7 +12,7 @@ def _value(t, knob):
 
 def test_coordinate_search_finds_separable_minimum():
     target = {"target_tiles": 148 * 16, "wide_row": 32, "lanes_div": 8, "fuse_first": 1, "sell_rows": 512,
-              "krylov_pair": 0, ("tail_rows", "tail_cluster"): (8192, 16)}
+              "krylov_pair": 0, ("tail_rows", "tail_cluster"): (65536, 0)}
     calls = []
 
     def cost(t):

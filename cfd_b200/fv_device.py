@@ -115,12 +115,46 @@ def cell_face_lists(n_cells, owner, neighbour):
     return offsets.astype(np.int32), faces[order].astype(np.int32)
 
 
+def _face_sums(n_cells, own, nei, per_face):
+    """Per cell, the sum of per_face[f] over its faces in ascending face order, as the face loop
+    of FvGeometry::build_least_squares (fv_geometry.cpp:78-87) adds them (each face to its
+    owner, then to its neighbour): the k-th contribution of every cell is added in round k."""
+    nf, nif = len(own), len(nei)
+    cell_of = np.concatenate([np.stack([own[:nif], nei], axis=1).ravel(), own[nif:]]).astype(np.int64)
+    face_of = np.concatenate([np.repeat(np.arange(nif), 2), np.arange(nif, nf)])
+    order = np.argsort(cell_of, kind="stable")  # by cell; each cell's faces stay in face order
+    c_sorted = cell_of[order]
+    rank = np.arange(len(order)) - np.searchsorted(c_sorted, np.arange(n_cells))[c_sorted]
+    out = np.zeros((n_cells,) + per_face.shape[1:])
+    for k in range(int(rank.max()) + 1 if len(rank) else 0):
+        e = order[rank == k]
+        out[cell_of[e]] += per_face[face_of[e]]
+    return out
+
+
+def _inverse3(m):
+    """Inverses of 3x3 matrices by cofactors, in the operation order of Eigen's fixed-size 3x3
+    inverse that FvGeometry calls (Matrix3d::inverse): the cofactors of column 0 give the
+    determinant (c00 m00 + c10 m10) + c20 m20, and entry (i, j) is cofactor (j, i) times 1 / det."""
+    def cof(i, j):
+        i1, i2, j1, j2 = (i + 1) % 3, (i + 2) % 3, (j + 1) % 3, (j + 2) % 3
+        return m[:, i1, j1] * m[:, i2, j2] - m[:, i1, j2] * m[:, i2, j1]
+    det = (cof(0, 0) * m[:, 0, 0] + cof(1, 0) * m[:, 1, 0]) + cof(2, 0) * m[:, 2, 0]
+    invdet = 1.0 / det
+    out = np.empty_like(m)
+    for i in range(3):
+        for j in range(3):
+            out[:, i, j] = cof(j, i) * invdet
+    return out
+
+
 def mesh_view(n_cells, owner, neighbour, face_areas, face_centres, cell_centres, cell_volumes,
               weights) -> MeshView:
     """The FvMeshView of FvGeometry::device() (fv_geometry.cpp:209-260) from a mesh's
     addressing and geometry: d = C_N - C_P (boundary: C_f - C_P), delta = |S|^2 / max(S.d,
     0.05 |S||d|), correction = S - d delta, lsq_d = d / |d|^2, lsq_inverse = (sum d d^T /
-    |d|^2)^-1 over each cell's faces (column-major)."""
+    |d|^2)^-1 over each cell's faces (column-major), each in the reference's operation order
+    (FvGeometry::build_least_squares, fv_geometry.cpp:70-92)."""
     own, nei = _i32(owner), _i32(neighbour)
     nf, nif = len(own), len(nei)
     sf = _f64(face_areas).reshape(-1, 3)
@@ -136,14 +170,11 @@ def mesh_view(n_cells, owner, neighbour, face_areas, face_centres, cell_centres,
         raise InvalidArgument("mesh_view: zero-area face or degenerate cell-to-face distance")
     delta = area * area / s_dot_d
     correction = sf - d * delta[:, None]
-    q = d / (d * d).sum(axis=1)[:, None]
-    dd = d[:, :, None] * q[:, None, :]  # d d^T / |d|^2
-    mat = np.empty((int(n_cells), 3, 3))
-    for a in range(3):
-        for b in range(3):
-            mat[:, a, b] = (np.bincount(own, dd[:, a, b], minlength=int(n_cells)) +
-                            np.bincount(nei, dd[:nif, a, b], minlength=int(n_cells)))
-    inv = np.linalg.inv(mat)
+    s2 = (d * d).sum(axis=1)  # |d|^2, x + y first, then z
+    q = d / s2[:, None]
+    dd = (d[:, :, None] * d[:, None, :]) / s2[:, None, None]  # d d^T / |d|^2 (fv_geometry.cpp:82)
+    mat = _face_sums(int(n_cells), own, nei, dd)
+    inv = _inverse3(mat)
     offsets, faces = cell_face_lists(n_cells, own, nei)
     view = MeshView(n_cells, own, nei, offsets, faces, weights, sf, cf, cc, cell_volumes, correction,
                     q, inv.transpose(0, 2, 1).reshape(-1, 9))

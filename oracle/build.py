@@ -45,8 +45,9 @@ REF_EIGEN_SOURCES = [
     "src/fv/src/parallel_amg.cpp",
     "src/parallel/src/comm.cpp",
 ]
-# FlowSolver (the callers of the pressure path), in the reference build only
-REF_FLOW_SOURCES = ["src/fv/src/flow_solver.cpp"]
+# FlowSolver (the callers of the pressure path) and the scalar transport step, in the
+# reference build only (the drop-in program links flow_solver.cpp alone)
+REF_FLOW_SOURCES = ["src/fv/src/flow_solver.cpp", "src/fv/src/scalar_transport.cpp"]
 REF_INCLUDES = ["src/gpu/include", "src/core/include", "src/mesh/include", "src/fv/include",
                 "src/parallel/include"]
 

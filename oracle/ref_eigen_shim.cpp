@@ -342,12 +342,13 @@ void refx_ldu_pattern(const void* h, int* row_ptr, int* col, int* diag_pos, int*
     std::copy(p.lower_pos.begin(), p.lower_pos.end(), lower_pos);
 }
 
-// LduMatrix::solve (ldu_matrix.cpp:111-282) with the handle's AmgCache; type is
-// LinearSolverType (0 ConjugateGradient, 1 BiCgStab, 2 AmgCg, 3 GpuCg, 4 GpuBiCgStab).
-// with_pattern = 0 detaches the CSR pattern (the non-persistent branches).
+// LduMatrix::solve (ldu_matrix.cpp:111-282) with the handle's AmgCache (with_cache = 0: none,
+// as solve_scalar calls it); type is LinearSolverType (0 ConjugateGradient, 1 BiCgStab,
+// 2 AmgCg, 3 GpuCg, 4 GpuBiCgStab). with_pattern = 0 detaches the CSR pattern (the
+// non-persistent branches).
 int refx_ldu_solve(void* h, int type, double tolerance, double rel_tolerance, int max_iterations, int max_age,
-                   int with_pattern, double* x, double* initial, double* final_residual, int* iterations,
-                   int* amg_age, int* amg_levels) {
+                   int with_pattern, int with_cache, double* x, double* initial, double* final_residual,
+                   int* iterations, int* amg_age, int* amg_levels) {
     return guarded([&] {
         auto* hh = static_cast<LduHandle*>(h);
         hh->ldu->pattern = with_pattern ? &hh->pattern : nullptr;
@@ -358,7 +359,7 @@ int refx_ldu_solve(void* h, int type, double tolerance, double rel_tolerance, in
         s.rel_tolerance = rel_tolerance;
         s.max_iterations = max_iterations;
         std::vector<Scalar> xv(x, x + hh->ldu->diag.size());
-        const auto r = hh->ldu->solve(xv, s, &hh->cache);
+        const auto r = hh->ldu->solve(xv, s, with_cache ? &hh->cache : nullptr);
         std::copy(xv.begin(), xv.end(), x);
         *initial = r.initial_residual;
         *final_residual = r.final_residual;

@@ -8,8 +8,9 @@
 // oracle's restatement and, through it, with the device step. Those three members are private;
 // their addresses are taken in explicit instantiations of a class template, where the language
 // does not check access (C++20 [temp.spec.general]/6), so the reference's sources stay as they
-// are.
+// are. It also runs the reference's solve_scalar (src/fv/src/scalar_transport.cpp) on a mesh.
 #include <cfd/fv/flow_solver.hpp>
+#include <cfd/fv/scalar_transport.hpp>
 #include <cfd/mesh/mesh.hpp>
 
 #include <algorithm>
@@ -227,6 +228,64 @@ int refx_flow_simple_iteration(void* h, double* residuals) {
         for (int k = 0; k < 3; ++k) residuals[k] = r.u[k];
         residuals[3] = r.p;
         residuals[4] = r.continuity;
+    });
+}
+
+// solve_scalar (scalar_transport.cpp:49-183) on a mesh with its own FvGeometry: the equation
+// given per face (gamma_face, n_faces), per cell (su, sp) and per boundary face (kind:
+// ScalarBoundary::Kind 0 fixed value, 1 zero gradient, 2 fixed gradient, 3 mixed; value;
+// coefficient); fixed_cell / fixed_value, old_value and capacity may be null. flags = {solver type
+// (LinearSolverType), max_iterations, linear_upwind, gradient scheme}; real = {relaxation, dt,
+// tolerance, rel_tolerance}. field is solved in place; result = {initial, final, iterations}.
+int refx_scalar_solve(const void* mesh, const double* face_flux, const double* gamma_face, const double* su,
+                      const double* sp, const int* bc_kind, const double* bc_value, const double* bc_coefficient,
+                      const unsigned char* fixed_cell, const double* fixed_value, const double* old_value,
+                      const double* capacity, const int* flags, const double* real, double* field, double* result) {
+    return guarded([&] {
+        const auto& m = *static_cast<const cfd::mesh::Mesh*>(mesh);
+        const auto nc = static_cast<std::size_t>(m.n_cells());
+        const auto nf = static_cast<std::size_t>(m.n_faces());
+        const auto nb = nf - static_cast<std::size_t>(m.n_internal_faces());
+        const cfd::fv::FvGeometry geo(m);
+        cfd::fv::ScalarEquation eq;
+        eq.gamma_face.assign(gamma_face, gamma_face + nf);
+        eq.su.assign(su, su + nc);
+        eq.sp.assign(sp, sp + nc);
+        eq.boundary.resize(nb);
+        for (std::size_t b = 0; b < nb; ++b) {
+            eq.boundary[b].kind = static_cast<cfd::fv::ScalarBoundary::Kind>(bc_kind[b]);
+            eq.boundary[b].value = bc_value[b];
+            eq.boundary[b].coefficient = bc_coefficient[b];
+        }
+        if (fixed_cell != nullptr) {
+            eq.fixed_cell.assign(fixed_cell, fixed_cell + nc);
+            eq.fixed_value.assign(fixed_value, fixed_value + nc);
+        }
+        std::vector<Scalar> old, cap;
+        if (old_value != nullptr) {
+            old.assign(old_value, old_value + nc);
+            eq.old_value = &old;
+        }
+        if (capacity != nullptr) {
+            cap.assign(capacity, capacity + nc);
+            eq.capacity = &cap;
+        }
+        eq.linear_upwind = flags[2] != 0;
+        eq.gradient = static_cast<cfd::fv::GradientScheme>(flags[3]);
+        eq.relaxation = real[0];
+        eq.dt = real[1];
+        cfd::fv::LinearSolverSettings s;
+        s.type = static_cast<cfd::fv::LinearSolverType>(flags[0]);
+        s.max_iterations = flags[1];
+        s.tolerance = real[2];
+        s.rel_tolerance = real[3];
+        std::vector<Scalar> flux(face_flux, face_flux + nf);
+        std::vector<Scalar> x(field, field + nc);
+        const auto r = cfd::fv::solve_scalar(geo, flux, eq, x, s);
+        std::copy(x.begin(), x.end(), field);
+        result[0] = r.initial_residual;
+        result[1] = r.final_residual;
+        result[2] = static_cast<double>(r.iterations);
     });
 }
 

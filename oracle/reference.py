@@ -71,7 +71,7 @@ def lib():
         R.refx_ldu_multiply.argtypes = [_vp, _pd, _pd]
         R.refx_ldu_residual_norms.argtypes = [_vp, _pd, _pd, _pd]
         R.refx_ldu_pattern.argtypes = [_vp, _pi, _pi, _pi, _pi, _pi]
-        R.refx_ldu_solve.argtypes = [_vp, _i, _d, _d, _i, _i, _i, _pd, _pd, _pd, _pi, _pi, _pi]
+        R.refx_ldu_solve.argtypes = [_vp, _i, _d, _d, _i, _i, _i, _i, _pd, _pd, _pd, _pi, _pi, _pi]
         R.refx_ldu_solve.restype = _i
         R.refx_jittered_lattice.argtypes = [_i, _i, _i, _pd, _pd, _pd, _d, _u64, _pd]
         R.refx_pressure_inputs.argtypes = [_i, _i, _pi, _pi, _pd, _pd, _pd, _d, _i, _i, _i, _u64, _pd,
@@ -87,7 +87,9 @@ def lib():
                                ("refx_flow_momentum_arrays", [_vp, _pd, _pd, _pd, _pd]),
                                ("refx_flow_solve_momentum", [_vp, _pd]),
                                ("refx_flow_pressure_correction", [_vp, _i, _pd, _pd, _pd]),
-                               ("refx_flow_simple_iteration", [_vp, _pd])):
+                               ("refx_flow_simple_iteration", [_vp, _pd]),
+                               ("refx_scalar_solve", [_vp, _pd, _pd, _pd, _pd, _pi, _pd, _pd, C.c_void_p,
+                                                      _pd, _pd, _pd, _pi, _pd, _pd, _pd])):
                 getattr(R, name).argtypes = args
                 getattr(R, name).restype = _i
         _declared = True
@@ -486,15 +488,17 @@ class RefLdu:
         return Pattern(n, nif, rp, col, d, u, lo)
 
     def solve(self, x, solver="GpuCg", tolerance=1e-10, rel_tolerance=0.01, max_iterations=1000,
-              max_age=20, with_pattern=True):
-        """LduMatrix::solve (ldu_matrix.cpp:111-282) in place on x; returns the result record."""
+              max_age=20, with_pattern=True, with_cache=True):
+        """LduMatrix::solve (ldu_matrix.cpp:111-282) in place on x, with the handle's AmgCache
+        or (with_cache False) none; returns the result record."""
         x_ = _f64(x)
         if x_ is not x:
             raise ValueError("x must be a contiguous float64 array (solved in place)")
         ini, fin = _d(), _d()
         it, age, lv = _i(), _i(), _i()
         rc = lib().refx_ldu_solve(self._h, LINEAR_SOLVER[solver], float(tolerance), float(rel_tolerance),
-                                  int(max_iterations), int(max_age), 1 if with_pattern else 0, _dp(x),
+                                  int(max_iterations), int(max_age), 1 if with_pattern else 0,
+                                  1 if with_cache else 0, _dp(x),
                                   C.byref(ini), C.byref(fin), C.byref(it), C.byref(age), C.byref(lv))
         if rc != 0:
             raise ValueError("LduMatrix::solve failed")
@@ -602,3 +606,27 @@ class RefFlow:
             self.close()
         except Exception:
             pass
+
+
+def scalar_solve(mesh: RefMesh, face_flux, eq: dict, field, solver=("GpuBiCgStab", 1e-12, 1e-9, 1000)):
+    """The reference's solve_scalar (scalar_transport.cpp:49-183) on `mesh` with its own
+    FvGeometry; eq as oracle.scalar.scalar_system takes it. Returns (field after the solve,
+    {initial_residual, final_residual, iterations})."""
+    R = lib()
+    fx = eq.get("fixed_cell")
+    fixed = None if fx is None else np.ascontiguousarray(fx, np.uint8)
+    opt = lambda k: None if eq.get(k) is None else _dp(_f64(eq[k]))  # noqa: E731
+    keep = [_f64(face_flux), _f64(eq["gamma_face"]), _f64(eq["su"]), _f64(eq["sp"]), _i32(eq["bc_kind"]),
+            _f64(eq["bc_value"]), _f64(eq["bc_coefficient"])]
+    flags = _i32([LINEAR_SOLVER[solver[0]], solver[3], 1 if eq.get("linear_upwind", True) else 0,
+                  int(eq.get("gradient", 0))])
+    real = _f64([eq.get("relaxation", 1.0), eq.get("dt", 0.0), solver[1], solver[2]])
+    x = np.array(field, np.float64)
+    res = np.empty(3)
+    rc = R.refx_scalar_solve(mesh._h, _dp(keep[0]), _dp(keep[1]), _dp(keep[2]), _dp(keep[3]), _ip(keep[4]),
+                             _dp(keep[5]), _dp(keep[6]), None if fixed is None else fixed.ctypes.data,
+                             opt("fixed_value") if fixed is not None else None, opt("old_value"), opt("capacity"),
+                             _ip(flags), _dp(real), _dp(x), _dp(res))
+    if rc != 0:
+        raise ValueError("solve_scalar failed")
+    return x, {"initial_residual": float(res[0]), "final_residual": float(res[1]), "iterations": int(res[2])}

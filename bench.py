@@ -724,6 +724,7 @@ def run_batch(args, rank, world, local_rank):
     settings = cb.AmgSettings(strength_threshold=THETA)
     b.setup_amg(h_dg, h_up, h_lo, settings)
     setup_s = time.perf_counter() - t0
+    setup_split_host = b.setup_times()
     # the same hierarchies built on the device (bit-identical); timed on its second run, the
     # first includes loading the setup kernels; the device build stays installed
     setup_dev_s = None
@@ -732,6 +733,7 @@ def run_batch(args, rank, world, local_rank):
         t0 = time.perf_counter()
         b.setup_amg(dg, up, lo, settings, device=True)
         setup_dev_s = time.perf_counter() - t0
+    setup_split_device = b.setup_times()
     offs = np.concatenate([[0], np.cumsum(nc)])
     tols = [1e-8 * float(np.linalg.norm(h_src[offs[i]:offs[i + 1]])) for i in range(len(cases))]
     ctl = [cb.SolveControl(t, 500) for t in tols]
@@ -826,7 +828,9 @@ def run_batch(args, rank, world, local_rank):
         "one_at_a_time_fp64": {"systems_per_s": len(cases) / (t_single / 1e3), "ms_total": t_single,
                                "iterations_max": max(it_single)},
         "batched_mixed_vs_one_at_a_time_fp64": value / (len(cases) / (t_single / 1e3)),
-        "setup_s_host": setup_s, "setup_s_device": setup_dev_s, "tuning": tuning, "clocks": out["mixed"]["clocks"],
+        "setup_s_host": setup_s, "setup_s_device": setup_dev_s,
+        "setup_split": {"host": setup_split_host, "device": setup_split_device},
+        "tuning": tuning, "clocks": out["mixed"]["clocks"],
         "gpu_launches": out["mixed"]["gpu_launches"],
     }
     if rank == 0:

@@ -174,6 +174,7 @@ _proto("cfdb_batch_solve_device", [_vp, _vp, _vp, _vp, _vp, _vp, _i, _P(ControlS
 _proto("cfdb_batch_profile", [_vp, _i, _P(KernelRecordStruct), _i, _pi])
 _proto("cfdb_batch_stream", [_vp, _P(_vp)])
 _proto("cfdb_batch_device_bytes", [_vp, _P(_sz)])
+_proto("cfdb_batch_setup_times", [_vp, _pd, _pd])
 _proto("cfdb_batch_kernel_launches", [_vp, _P(C.c_ulonglong)])
 
 
@@ -947,6 +948,12 @@ class Batch:
             return
         _check(_lib.cfdb_batch_setup_amg(self._h, _dp(_f64(diag)), _dp(_f64(upper)),
                                          _dp(_f64(lower)), C.byref(s)))
+
+    def setup_times(self) -> dict:
+        """Wall seconds of the last setup: per-system hierarchies and the batch plan."""
+        h, p = C.c_double(), C.c_double()
+        _check(_lib.cfdb_batch_setup_times(self._h, C.byref(h), C.byref(p)))
+        return {"hierarchies_s": h.value, "plan_s": p.value}
 
     def set_precision(self, precision: Precision) -> None:
         _check(_lib.cfdb_batch_set_precision(self._h, int(precision)))

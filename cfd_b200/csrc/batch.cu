@@ -2,6 +2,7 @@
 #include "../../include/cfdb.h"
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cstring>
 #include <memory>
@@ -41,6 +42,8 @@ struct cfdb_batch {
     int* d_ref = nullptr;
     std::vector<int> ref_cached;
     unsigned long long launches = 0;
+    double setup_hierarchies_s = 0.0; // last setup: the per-system hierarchies
+    double setup_plan_s = 0.0;        // last setup: the batch plan built from them
 };
 
 namespace {
@@ -206,6 +209,7 @@ int cfdb_batch_setup_amg(cfdb_batch* b, const double* diag, const double* upper,
             st.weight = settings->jacobi_weight;
         }
         std::vector<std::string> errs(b->n_sys);
+        const auto t0 = std::chrono::steady_clock::now();
 #pragma omp parallel for schedule(dynamic, 1)
         for (int s = 0; s < b->n_sys; ++s) {
             try {
@@ -230,7 +234,10 @@ int cfdb_batch_setup_amg(cfdb_batch* b, const double* diag, const double* upper,
         b->sweeps = st.sweeps;
         b->weight = st.weight;
         b->dirty = true;
+        const auto t1 = std::chrono::steady_clock::now();
         ensure_batch_engine(b);
+        b->setup_hierarchies_s = std::chrono::duration<double>(t1 - t0).count();
+        b->setup_plan_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
     });
 }
 
@@ -257,6 +264,7 @@ int cfdb_batch_setup_amg_device(cfdb_batch* b, const double* diag, const double*
         if (st.max_levels < 1) fail(CFDB_ERR_BAD_ARG, "max_levels must be >= 1");
         const int workers = std::max(1, std::min(concurrency > 0 ? concurrency : 8, b->n_sys));
         std::vector<std::string> errs(b->n_sys);
+        const auto t0 = std::chrono::steady_clock::now();
 #pragma omp parallel for schedule(dynamic, 1) num_threads(workers)
         for (int s = 0; s < b->n_sys; ++s) {
             cudaStream_t cs = nullptr;
@@ -297,7 +305,10 @@ int cfdb_batch_setup_amg_device(cfdb_batch* b, const double* diag, const double*
         b->sweeps = st.sweeps;
         b->weight = st.weight;
         b->dirty = true;
+        const auto t1 = std::chrono::steady_clock::now();
         ensure_batch_engine(b);
+        b->setup_hierarchies_s = std::chrono::duration<double>(t1 - t0).count();
+        b->setup_plan_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
     });
 }
 
@@ -409,6 +420,13 @@ int cfdb_batch_profile(cfdb_batch* b, int reps, cfdb_kernel_record* records, int
 int cfdb_batch_stream(const cfdb_batch* b, void** stream) {
     if (b == nullptr || stream == nullptr || !b->eng) return CFDB_ERR_BAD_ARG;
     *stream = b->eng->stream();
+    return CFDB_OK;
+}
+
+int cfdb_batch_setup_times(const cfdb_batch* b, double* hierarchies_s, double* plan_s) {
+    if (b == nullptr) return CFDB_ERR_BAD_ARG;
+    if (hierarchies_s != nullptr) *hierarchies_s = b->setup_hierarchies_s;
+    if (plan_s != nullptr) *plan_s = b->setup_plan_s;
     return CFDB_OK;
 }
 

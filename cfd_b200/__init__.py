@@ -175,6 +175,7 @@ _proto("cfdb_batch_profile", [_vp, _i, _P(KernelRecordStruct), _i, _pi])
 _proto("cfdb_batch_stream", [_vp, _P(_vp)])
 _proto("cfdb_batch_device_bytes", [_vp, _P(_sz)])
 _proto("cfdb_batch_setup_times", [_vp, _pd, _pd])
+_proto("cfdb_batch_setup_profile", [_vp, C.c_char_p, C.c_size_t])
 _proto("cfdb_batch_kernel_launches", [_vp, _P(C.c_ulonglong)])
 
 
@@ -953,7 +954,14 @@ class Batch:
         """Wall seconds of the last setup: per-system hierarchies and the batch plan."""
         h, p = C.c_double(), C.c_double()
         _check(_lib.cfdb_batch_setup_times(self._h, C.byref(h), C.byref(p)))
-        return {"hierarchies_s": h.value, "plan_s": p.value}
+        out = {"hierarchies_s": h.value, "plan_s": p.value}
+        buf = C.create_string_buffer(4096)
+        _check(_lib.cfdb_batch_setup_profile(self._h, buf, len(buf)))
+        for item in buf.value.decode().split(";"):
+            name, _, v = item.partition("=")
+            if v:
+                out[name if name.startswith("plan") else "plan_" + name] = float(v)
+        return out
 
     def set_precision(self, precision: Precision) -> None:
         _check(_lib.cfdb_batch_set_precision(self._h, int(precision)))

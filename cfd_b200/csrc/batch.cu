@@ -423,6 +423,15 @@ int cfdb_batch_stream(const cfdb_batch* b, void** stream) {
     return CFDB_OK;
 }
 
+int cfdb_batch_setup_profile(const cfdb_batch* b, char* buf, size_t len) {
+    if (b == nullptr || buf == nullptr || len == 0) return CFDB_ERR_BAD_ARG;
+    const std::string t = b->eng ? b->eng->build_times().text() : std::string();
+    const size_t n = std::min(len - 1, t.size());
+    std::memcpy(buf, t.data(), n);
+    buf[n] = '\0';
+    return CFDB_OK;
+}
+
 int cfdb_batch_setup_times(const cfdb_batch* b, double* hierarchies_s, double* plan_s) {
     if (b == nullptr) return CFDB_ERR_BAD_ARG;
     if (hierarchies_s != nullptr) *hierarchies_s = b->setup_hierarchies_s;

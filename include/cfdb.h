@@ -504,6 +504,8 @@ int cfdb_batch_stream(const cfdb_batch* b, void** stream);
 int cfdb_batch_device_bytes(const cfdb_batch* b, size_t* bytes);
 /* Wall time of the last setup: the per-system hierarchies, then the batch plan built from them. */
 int cfdb_batch_setup_times(const cfdb_batch* b, double* hierarchies_s, double* plan_s);
+/* Phase times of the last plan build, "name=seconds;..." (as cfdb_system_setup_profile). */
+int cfdb_batch_setup_profile(const cfdb_batch* b, char* buf, size_t len);
 int cfdb_batch_kernel_launches(const cfdb_batch* b, unsigned long long* count);
 
 /* ---- finite-volume cell kernels: cfd::gpu::DeviceFv (fv_device.hpp:33-72) ---- */

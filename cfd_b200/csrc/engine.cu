@@ -119,6 +119,105 @@ void sell_append(SellBuild& sb, int n_rows, int n_pad, const int* rp, const int*
     for (int sl = 0; sl < n_sl; ++sl) sb.slice[s0 + sl] = static_cast<int>(start[sl + 1]);
 }
 
+// One CSR block of a multi-system operator (the arguments of sell_append / csr_append).
+struct BlockSpec {
+    int n_rows = 0, n_pad = 0;
+    const int* rp = nullptr;
+    const int* ci = nullptr;
+    const double* va = nullptr;
+    const int* src_of = nullptr;
+    int col_off = 0, src_off = 0, pad_col = 0;
+};
+
+// sell_append over many blocks in order, with the same result as appending them one after
+// another: the blocks' row orders and slice widths are worked out in parallel (one block per
+// thread), the slot offsets follow from a prefix sum over the blocks, and the blocks are then
+// filled in parallel. A single block goes through sell_append and its own inner parallelism.
+void sell_append_blocks(SellBuild& sb, const std::vector<BlockSpec>& blocks) {
+    const int nb = static_cast<int>(blocks.size());
+    if (nb == 1) {
+        const BlockSpec& b = blocks[0];
+        sell_append(sb, b.n_rows, b.n_pad, b.rp, b.ci, b.va, b.src_of, b.col_off, b.src_off, b.pad_col);
+        return;
+    }
+    std::vector<std::vector<int>> order(static_cast<size_t>(nb)), width(static_cast<size_t>(nb));
+    std::vector<long long> slots(static_cast<size_t>(nb) + 1, 0), rows(static_cast<size_t>(nb) + 1, 0),
+        slices(static_cast<size_t>(nb) + 1, 0);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int bi = 0; bi < nb; ++bi) {
+        const BlockSpec& b = blocks[static_cast<size_t>(bi)];
+        auto len_of = [&](int i) { return i < b.n_rows ? b.rp[i + 1] - b.rp[i] : -1; };
+        std::vector<int>& o = order[static_cast<size_t>(bi)];
+        o.resize(static_cast<size_t>(b.n_pad));
+        std::iota(o.begin(), o.end(), 0);
+        if (sb.sort) {
+            for (int w0 = 0; w0 < b.n_pad; w0 += kSellRows) {
+                const int w1 = std::min(b.n_pad, w0 + kSellRows);
+                std::stable_sort(o.begin() + w0, o.begin() + w1, [&](int a, int c) { return len_of(a) > len_of(c); });
+            }
+        }
+        const int n_sl = b.n_pad / 32;
+        std::vector<int>& w = width[static_cast<size_t>(bi)];
+        w.assign(static_cast<size_t>(n_sl), 0);
+        long long total = 0;
+        for (int sl = 0; sl < n_sl; ++sl) {
+            int m = 0;
+            for (int q = sl * 32; q < sl * 32 + 32; ++q) m = std::max(m, len_of(o[q]));
+            w[static_cast<size_t>(sl)] = m;
+            total += 32LL * m;
+        }
+        slots[static_cast<size_t>(bi) + 1] = total;
+        rows[static_cast<size_t>(bi) + 1] = b.n_pad;
+        slices[static_cast<size_t>(bi) + 1] = n_sl;
+    }
+    const long long slot0 = sb.slice.back(), row0 = static_cast<long long>(sb.perm.size());
+    const long long slice0 = static_cast<long long>(sb.slice.size()) - 1;
+    for (int bi = 0; bi < nb; ++bi) {
+        slots[static_cast<size_t>(bi) + 1] += slots[static_cast<size_t>(bi)];
+        rows[static_cast<size_t>(bi) + 1] += rows[static_cast<size_t>(bi)];
+        slices[static_cast<size_t>(bi) + 1] += slices[static_cast<size_t>(bi)];
+    }
+    const long long total = slot0 + slots[static_cast<size_t>(nb)];
+    if (total > INT_MAX) fail(1, "operator too large for 32-bit slot offsets");
+    sb.col.resize(static_cast<size_t>(total), 0);
+    sb.val.resize(static_cast<size_t>(total), 0.0);
+    sb.pad.resize(static_cast<size_t>(total), 1);
+    if (sb.with_src) sb.src.resize(static_cast<size_t>(total), -1);
+    if (sb.sort) sb.perm.resize(static_cast<size_t>(row0 + rows[static_cast<size_t>(nb)]));
+    sb.slice.resize(static_cast<size_t>(slice0 + slices[static_cast<size_t>(nb)] + 1));
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int bi = 0; bi < nb; ++bi) {
+        const BlockSpec& b = blocks[static_cast<size_t>(bi)];
+        const std::vector<int>& o = order[static_cast<size_t>(bi)];
+        const std::vector<int>& w = width[static_cast<size_t>(bi)];
+        const long long r0 = row0 + rows[static_cast<size_t>(bi)];
+        if (sb.sort)
+            for (int q = 0; q < b.n_pad; ++q) sb.perm[static_cast<size_t>(r0 + q)] = static_cast<int>(r0 + o[q]);
+        long long base = slot0 + slots[static_cast<size_t>(bi)];
+        const long long s0 = slice0 + slices[static_cast<size_t>(bi)];
+        for (int sl = 0; sl < b.n_pad / 32; ++sl) {
+            for (int lane = 0; lane < 32; ++lane) {
+                const int i = o[static_cast<size_t>(sl) * 32 + lane];
+                const int len = i < b.n_rows ? b.rp[i + 1] - b.rp[i] : 0;
+                for (int k = 0; k < w[static_cast<size_t>(sl)]; ++k) {
+                    const size_t slot = static_cast<size_t>(base + static_cast<long long>(k) * 32 + lane);
+                    if (k < len) {
+                        const int e = b.rp[i] + k;
+                        sb.pad[slot] = 0;
+                        sb.col[slot] = b.ci[e] + b.col_off;
+                        sb.val[slot] = b.va != nullptr ? b.va[e] : 0.0;
+                        if (sb.with_src) sb.src[slot] = b.src_of != nullptr ? b.src_of[e] + b.src_off : -1;
+                    } else {
+                        sb.col[slot] = b.pad_col;
+                    }
+                }
+            }
+            base += 32LL * w[static_cast<size_t>(sl)];
+            sb.slice[static_cast<size_t>(s0 + sl + 1)] = static_cast<int>(base);
+        }
+    }
+}
+
 // CSR under construction on the host (global rows of a level; padding rows are empty).
 struct CsrBuild {
     std::vector<int> rp{0};
@@ -144,6 +243,46 @@ void csr_append(CsrBuild& cb, int n_rows, int n_pad, const int* rp, const int* c
             }
         }
         cb.rp[r0 + i] = static_cast<int>(base + (i < n_rows ? rp[i + 1] - rp[0] : nnz));
+    }
+}
+
+// csr_append over many blocks in order (one block per thread after a prefix sum of their
+// entries); a single block goes through csr_append.
+void csr_append_blocks(CsrBuild& cb, const std::vector<BlockSpec>& blocks) {
+    const int nb = static_cast<int>(blocks.size());
+    if (nb == 1) {
+        const BlockSpec& b = blocks[0];
+        csr_append(cb, b.n_rows, b.n_pad, b.rp, b.ci, b.va, b.col_off);
+        return;
+    }
+    std::vector<long long> ent(static_cast<size_t>(nb) + 1, 0), rows(static_cast<size_t>(nb) + 1, 0);
+    for (int bi = 0; bi < nb; ++bi) {
+        const BlockSpec& b = blocks[static_cast<size_t>(bi)];
+        ent[static_cast<size_t>(bi) + 1] = ent[static_cast<size_t>(bi)] + (b.n_rows > 0 ? b.rp[b.n_rows] - b.rp[0] : 0);
+        rows[static_cast<size_t>(bi) + 1] = rows[static_cast<size_t>(bi)] + b.n_pad;
+    }
+    const long long base0 = static_cast<long long>(cb.col.size());
+    if (base0 + ent[static_cast<size_t>(nb)] > INT_MAX) fail(1, "operator too large for 32-bit offsets");
+    const size_t r00 = cb.rp.size();
+    cb.col.resize(static_cast<size_t>(base0 + ent[static_cast<size_t>(nb)]));
+    cb.val.resize(static_cast<size_t>(base0 + ent[static_cast<size_t>(nb)]));
+    cb.rp.resize(r00 + static_cast<size_t>(rows[static_cast<size_t>(nb)]));
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int bi = 0; bi < nb; ++bi) {
+        const BlockSpec& b = blocks[static_cast<size_t>(bi)];
+        const long long base = base0 + ent[static_cast<size_t>(bi)];
+        const long long nnz = ent[static_cast<size_t>(bi) + 1] - ent[static_cast<size_t>(bi)];
+        const size_t r0 = r00 + static_cast<size_t>(rows[static_cast<size_t>(bi)]);
+        for (int i = 0; i < b.n_pad; ++i) {
+            if (i < b.n_rows) {
+                const long long o = base + b.rp[i] - b.rp[0];
+                for (int k = b.rp[i]; k < b.rp[i + 1]; ++k) {
+                    cb.col[static_cast<size_t>(o + k - b.rp[i])] = b.ci[k] + b.col_off;
+                    cb.val[static_cast<size_t>(o + k - b.rp[i])] = b.va[k];
+                }
+            }
+            cb.rp[r0 + static_cast<size_t>(i)] = static_cast<int>(base + (i < b.n_rows ? b.rp[i + 1] - b.rp[0] : nnz));
+        }
     }
 }
 
@@ -414,6 +553,8 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         SellBuild sb;
         sb.with_src = true;
         std::vector<int> dsrc(static_cast<size_t>(lv_[0].n_rows), -1);
+        std::vector<BlockSpec> blocks;
+        blocks.reserve(static_cast<size_t>(n_sys_));
         for (int k = 0; k < n_sys_; ++k) {
             const int s = perm_[k];
             const SystemSpec& sp = systems[s];
@@ -423,8 +564,16 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
                 fail(1, "engine: level-0 value map size mismatch");
             }
             const int so = sp.absolute_src ? 0 : vs_off_[s];
-            sell_append(sb, sp.n, round_up(sp.n, 32), sp.rp, sp.ci, nullptr, sv.data(), off[0][s], so,
-                        off[0][s]);
+            blocks.push_back(BlockSpec{sp.n, round_up(sp.n, 32), sp.rp, sp.ci, nullptr, sv.data(), off[0][s], so,
+                                       off[0][s]});
+        }
+        sell_append_blocks(sb, blocks);
+#pragma omp parallel for schedule(dynamic, 1) if (n_sys_ > 1)
+        for (int k = 0; k < n_sys_; ++k) {
+            const int s = perm_[k];
+            const SystemSpec& sp = systems[s];
+            const std::vector<int>& dv = sp.diag_src_ref ? *sp.diag_src_ref : sp.diag_src;
+            const int so = sp.absolute_src ? 0 : vs_off_[s];
             for (int i = 0; i < sp.n; ++i) dsrc[off[0][s] + i] = dv[i] >= 0 ? dv[i] + so : -1;
         }
         DevLevel& d = lv_[0];
@@ -531,13 +680,15 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
             }
             if (wide) {
                 CsrBuild cbd;
+                std::vector<BlockSpec> blocks;
                 for (int k = 0; k < n_sys_; ++k) {
                     const int s = perm_[k];
                     if (L[s] - 1 <= l) continue;
                     const HostCsr& a = pick(s);
-                    csr_append(cbd, a.n_rows, round_up(a.n_rows, 32), a.rp.data(), a.ci.data(), a.va.data(),
-                               off[col_level][s]);
+                    blocks.push_back(BlockSpec{a.n_rows, round_up(a.n_rows, 32), a.rp.data(), a.ci.data(), a.va.data(),
+                                               nullptr, off[col_level][s], 0, 0});
                 }
+                csr_append_blocks(cbd, blocks);
                 m.n_slices = static_cast<int>(cbd.rp.size()) - 1;
                 m.slots = cbd.rp.back();
                 // slack for the aligned quad loads of the last row
@@ -560,14 +711,18 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
             } else {
                 SellBuild sb;
                 sb.sort = true;
+                std::vector<BlockSpec> blocks;
+                int next_row = 0;
                 for (int k = 0; k < n_sys_; ++k) {
                     const int s = perm_[k];
                     if (L[s] - 1 <= l) continue;
                     const HostCsr& a = pick(s);
-                    if (static_cast<int>(sb.perm.size()) != off[row_level][s]) fail(1, "engine: operator rows out of order");
-                    sell_append(sb, a.n_rows, round_up(a.n_rows, 32), a.rp.data(), a.ci.data(), a.va.data(),
-                                nullptr, off[col_level][s], 0, off[col_level][s]);
+                    if (next_row != off[row_level][s]) fail(1, "engine: operator rows out of order");
+                    next_row += round_up(a.n_rows, 32);
+                    blocks.push_back(BlockSpec{a.n_rows, round_up(a.n_rows, 32), a.rp.data(), a.ci.data(), a.va.data(),
+                                               nullptr, off[col_level][s], 0, off[col_level][s]});
                 }
+                sell_append_blocks(sb, blocks);
                 m.n_slices = static_cast<int>(sb.slice.size()) - 1;
                 m.slots = sb.slice.back();
                 std::vector<uint16_t> c16;
@@ -598,6 +753,7 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
                 weighted_inverse_diagonal(dl->a[l], d.n_rows_nc, weight_, d.wd64, d.wd32, st);
             } else {
                 std::vector<double> wd(static_cast<size_t>(d.n_rows_nc), weight_);
+#pragma omp parallel for schedule(dynamic, 1) if (n_sys_ > 1)
                 for (int k = 0; k < n_sys_; ++k) {
                     const int s = perm_[k];
                     if (L[s] - 1 <= l) continue; // only systems with a coarser level need A_l here

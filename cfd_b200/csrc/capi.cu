@@ -888,6 +888,19 @@ int cfdb_system_setup_amg_device(cfdb_system* sys, const double* diag, const dou
         CFDB_CUDA(cudaSetDevice(sys->device));
         CallStream cs;
         pattern_on_device(sys, cs.s);
+        // The previous hierarchy's device levels serve only plan rebuilds (the plan holds its
+        // own copies), and this call replaces the plan: free them first, so that the new
+        // hierarchy takes over their blocks instead of growing the memory pool by a second
+        // hierarchy. Until the new one is installed the system has none.
+        if (sys->dl) {
+            CFDB_CUDA(cudaStreamSynchronize(sys->eng ? sys->eng->stream() : cs.s));
+            sys->dl.reset();
+            if (sys->h_shapes_only) {
+                sys->h.reset();
+                sys->h_shapes_only = false;
+                sys->dirty = true;
+            }
+        }
         DeviceHierarchy dh;
         const double *dd = diag, *du = upper, *dl = lower;
         if (!device_arrays) {

@@ -10,6 +10,7 @@ The knobs are those of `Tuning` (include/cfdb.h, cfdb_tuning):
 * sell_rows    - rows per CTA of SELL operators (one row per thread per pass),
 * krylov_pair  - level-0 Krylov SpMV kernels take two rows per thread per pass, or one,
 * tail_rows    - coarse levels of at most this many rows run in one persistent kernel,
+* vcycle_pair  - V-cycle kernels of SELL operators take two rows per thread per pass, or one,
 * tail_cluster - that kernel as one thread-block cluster of this many CTAs (0: a cooperative
                  grid), searched jointly with tail_rows (the candidates keep the grid form),
 * mixed_sweeps, mixed_weight - the smoother schedule of the mixed-precision V-cycle (Jacobi
@@ -43,6 +44,7 @@ CANDIDATES = {
     "fuse_first": [0, 1],
     "sell_rows": [256, 512, 1024],
     "krylov_pair": [0, 1],
+    "vcycle_pair": [0, 1],
     # the single-cluster tail (tail_cluster > 0) is not a candidate: on tet 95^3 x 6 it took
     # 299 us (16 CTAs) to 1,103 us (4 CTAs) per V-cycle where the separate kernels take ~50 us
     ("tail_rows", "tail_cluster"): [(0, 0), (1024, 0), (8192, 0), (65536, 0), (131072, 0)],
@@ -51,7 +53,7 @@ CANDIDATES = {
 # knobs whose best value depends on the smoother schedule: with one sweep per level the first
 # sweeps are never fused, so the persistent tail (which needs the unfused schedule) and the
 # shapes of the kernels it replaces are searched again once the schedule is chosen
-SCHEDULE_KNOBS = (("tail_rows", "tail_cluster"), "sell_rows", "target_tiles")
+SCHEDULE_KNOBS = (("tail_rows", "tail_cluster"), "sell_rows", "target_tiles", "vcycle_pair")
 
 
 def _key(t: Tuning) -> tuple:

@@ -1298,7 +1298,7 @@ void Engine::enqueue_vcycle_t(bool fused_final, int flexible, bool x1_ready0) {
         int visit;  // row-visiting strategy of the operator's kernels
     };
     auto TL = [&](int, const DevSell64_32& m, bool nc) -> Launch {
-        return {m.tiles, nc ? m.n_tiles_nc : m.n_tiles, m.block, visit_of(m.s64.val != nullptr ? m.s64.fmt : m.s32.fmt)};
+        return {m.tiles, nc ? m.n_tiles_nc : m.n_tiles, m.block, vcycle_visit(m)};
     };
     std::vector<T*> cur(L, nullptr);
     // levels lt and below run in the persistent tail kernel when its phases are prepared
@@ -1711,7 +1711,7 @@ double Engine::time_sweep(int level, int reps, double* bytes) {
     const Tiles tiles = m.tiles;
     const int grid = nc ? m.n_tiles_nc : m.n_tiles;
     if (grid == 0) fail(1, "time_sweep: level has no operator tiles");
-    const int visit = visit_of(m.s64.val != nullptr ? m.s64.fmt : m.s32.fmt);
+    const int visit = vcycle_visit(m);
     const double sv = fp32 ? 4.0 : 8.0;
     const double sb = level == 0 ? 8.0 : sv;
     const double n = d.n_rows_nc;

@@ -53,6 +53,8 @@ struct Tuning {
     double mixed_weight = 0.0;  // mixed precision: Jacobi weight (0: the hierarchy's)
     int tail_cluster = 0;       // the tail as one thread-block cluster of this many CTAs (2..16)
                                 // separated by the cluster barrier; 0: a cooperative grid
+    int vcycle_pair = 0;        // V-cycle kernels of SELL operators take two rows per thread per
+                                // pass (as the level-0 Krylov kernels with krylov_pair), or one
 };
 
 struct SolveRequest {
@@ -193,6 +195,11 @@ private:
     template <class T> void launch_tail(cudaStream_t s);
     // rows per thread per pass of the level-0 Krylov SpMV kernels (two, or one)
     int krylov_visit() const { return tuning_.krylov_pair ? kVisitSell2 : kVisitSell1; }
+    // row-visiting strategy of a V-cycle operator's kernels
+    int vcycle_visit(const DevSell64_32& m) const {
+        const int v = visit_of(m.s64.val != nullptr ? m.s64.fmt : m.s32.fmt);
+        return v == kVisitSell1 && tuning_.vcycle_pair ? kVisitSell2 : v;
+    }
     // where the residual producers of `mode` write the level-0 first sweep (n = 0: nowhere)
     X1Out x1_out(Mode mode) const;
     void enqueue_init(Mode mode);

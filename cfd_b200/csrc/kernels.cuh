@@ -434,7 +434,8 @@ constexpr int kFineRows = 8;
 
 // Row-visiting strategies of the tiled kernels, fixed at compile time so that each kernel
 // instance holds the registers of one strategy only:
-//  kVisitSell2  SELL, two rows per thread per pass (big tiles of the Krylov kernels);
+//  kVisitSell2  SELL, two rows per thread per pass (big tiles of the Krylov kernels, and the
+//               V-cycle kernels with Tuning.vcycle_pair), rows optionally reordered;
 //  kVisitSell1  SELL, one row per thread per pass, rows optionally reordered (V-cycle kernels);
 //  kVisitWarp   CSR, G <= 32 lanes per row (8 rows per tile);
 //  kVisitBlock  CSR, G = 64..256 lanes per row (256 / G rows per tile).
@@ -445,13 +446,14 @@ template <int V, class T, class XA, class F>
 __device__ __forceinline__ void visit_rows_v(const Sell<T>& m, int r0, int r1, XA xa, F f) {
     if constexpr (V == kVisitSell2) {
         int row = r0 + threadIdx.x;
+        auto at = [&](int q) { return m.perm != nullptr ? __ldg(&m.perm[q]) : q; };
         for (; row + kBlock < r1; row += 2 * kBlock) {
             T s0, s1;
             sell_row_sum2(m, row, row + kBlock, xa, s0, s1);
-            f(row, s0);
-            f(row + kBlock, s1);
+            f(at(row), s0);
+            f(at(row + kBlock), s1);
         }
-        if (row < r1) f(row, sell_row_sum(m, row, xa));
+        if (row < r1) f(at(row), sell_row_sum(m, row, xa));
     } else if constexpr (V == kVisitSell1) {
         // reordered operators: tiles are aligned windows of positions
         for (int row = r0 + threadIdx.x; row < r1; row += kBlock)
@@ -481,17 +483,20 @@ template <int V, class T, class XA, class P, class F>
 __device__ __forceinline__ void visit_rows_e(const Sell<T>& m, int r0, int r1, XA xa, P pre, F f) {
     if constexpr (V == kVisitSell2) {
         int row = r0 + threadIdx.x;
+        auto at = [&](int q) { return m.perm != nullptr ? __ldg(&m.perm[q]) : q; };
         for (; row + kBlock < r1; row += 2 * kBlock) {
-            const auto e0 = pre(row);
-            const auto e1 = pre(row + kBlock);
+            const int ra = at(row), rb = at(row + kBlock);
+            const auto e0 = pre(ra);
+            const auto e1 = pre(rb);
             T s0, s1;
             sell_row_sum2(m, row, row + kBlock, xa, s0, s1);
-            f(row, s0, e0);
-            f(row + kBlock, s1, e1);
+            f(ra, s0, e0);
+            f(rb, s1, e1);
         }
         if (row < r1) {
-            const auto e = pre(row);
-            f(row, sell_row_sum(m, row, xa), e);
+            const int ra = at(row);
+            const auto e = pre(ra);
+            f(ra, sell_row_sum(m, row, xa), e);
         }
     } else if constexpr (V == kVisitSell1) {
         for (int row = r0 + threadIdx.x; row < r1; row += kBlock) {

@@ -453,6 +453,8 @@ typedef struct {
     int tail_cluster; /* with tail_rows: run the tail as one thread-block cluster of this many CTAs
                          (2..16), its phases separated by the hardware cluster barrier; 0
                          (default): a cooperative grid with the bounded grid barrier */
+    int vcycle_pair;  /* V-cycle kernels of SELL operators take two rows per thread per pass (1)
+                         or one (0, default) */
 } cfdb_tuning;
 void cfdb_default_tuning(cfdb_tuning* t);
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t);

@@ -172,22 +172,51 @@ def make_pool(server: Server, pool_cases, variants=3, seed=0, coefficient_jitter
     return pool
 
 
-def run_load(server: Server, pool: list, rate_hz: float, n_requests: int, repeat_frac=0.3,
-             tet_frac=0.25, seed=0, rel_tol=1e-8, closed_loop=False, warm_start=True):
-    """Open-loop Poisson arrivals at rate_hz (closed_loop: each request submitted when the
-    previous one finished) of n_requests over the pool. A request picks tet meshes with
-    probability tet_frac, then a pool mesh of that kind uniformly. With probability repeat_frac
-    it repeats its mesh's previous matrix (same key: no re-upload) with a new right-hand side
-    and, if warm_start, starts from the resident solution; otherwise it carries the next
-    coefficient variant under a new key. Latency = finish - submit on the server clock."""
-    import queue as _q
+def request_trace(pool: list, rate_hz: float, n_requests: int, repeat_frac=0.3, tet_frac=0.25, seed=0,
+                  closed_loop=False):
+    """The requests run_load submits, drawn from `seed` before any clock starts: a list of
+    (arrival s, pool entry, matrix key, variant, right-hand side, repeat). A request picks tet
+    meshes with probability tet_frac, then a pool mesh of that kind uniformly; with probability
+    repeat_frac it repeats its mesh's previous key and variant, otherwise it carries the next
+    key and the variant key % variants. Arrivals are Poisson at rate_hz (all 0 in a closed
+    loop). The same arguments give the same trace."""
     rng = np.random.default_rng(seed)
     by_kind = {}
     for e in pool:
         by_kind.setdefault(e.kind, []).append(e)
     kinds = sorted(by_kind)
     last = {}
-    key_counter = [0]
+    key_counter = 0
+    trace = []
+    ta = 0.0
+    for _ in range(n_requests):
+        if not closed_loop:
+            ta += rng.exponential(1.0 / rate_hz)
+        kind = "tet" if ("tet" in by_kind and rng.random() < tet_frac) else \
+            ("box" if "box" in by_kind else kinds[0])
+        group = by_kind[kind]
+        e = group[int(rng.integers(len(group)))]
+        rep = e.mesh_id in last and rng.random() < repeat_frac
+        if rep:
+            key, mi = last[e.mesh_id]
+        else:
+            key_counter += 1
+            key = key_counter
+            mi = key % len(e.matrices)
+            last[e.mesh_id] = (key, mi)
+        bi = int(rng.integers(len(e.rhs)))
+        trace.append((ta, e, key, mi, bi, bool(rep)))
+    return trace
+
+
+def run_load(server: Server, pool: list, rate_hz: float, n_requests: int, repeat_frac=0.3,
+             tet_frac=0.25, seed=0, rel_tol=1e-8, closed_loop=False, warm_start=True):
+    """Open-loop Poisson arrivals at rate_hz (closed_loop: each request submitted when the
+    previous one finished) of the n_requests of request_trace over the pool. A repeat carries
+    its mesh's previous matrix (same key: no re-upload) with a new right-hand side and, if
+    warm_start, starts from the resident solution. Latency = finish - submit on the server
+    clock."""
+    import queue as _q
     records = []
     pending = _q.Queue()
     lock = threading.Lock()
@@ -205,28 +234,10 @@ def run_load(server: Server, pool: list, rate_hz: float, n_requests: int, repeat
                                     service=times[2] - times[1], iterations=st.iterations,
                                     converged=st.converged, residual=st.residual))
 
-    # the request trace, drawn before the clock starts (arrival, entry, key, variant, rhs,
-    # repeat), and enough page-locked solution buffers for every request of a mesh to be in
-    # flight at once, so that no buffer is page-locked while the server runs
-    trace = []
-    ta = 0.0
-    for i in range(n_requests):
-        if not closed_loop:
-            ta += rng.exponential(1.0 / rate_hz)
-        kind = "tet" if ("tet" in by_kind and rng.random() < tet_frac) else \
-            ("box" if "box" in by_kind else kinds[0])
-        group = by_kind[kind]
-        e = group[int(rng.integers(len(group)))]
-        rep = e.mesh_id in last and rng.random() < repeat_frac
-        if rep:
-            key, mi = last[e.mesh_id]
-        else:
-            key_counter[0] += 1
-            key = key_counter[0]
-            mi = key % len(e.matrices)
-            last[e.mesh_id] = (key, mi)
-        bi = int(rng.integers(len(e.rhs)))
-        trace.append((ta, e, key, mi, bi, bool(rep)))
+    # the request trace, drawn before the clock starts, and enough page-locked solution buffers
+    # for every request of a mesh to be in flight at once, so that no buffer is page-locked
+    # while the server runs
+    trace = request_trace(pool, rate_hz, n_requests, repeat_frac, tet_frac, seed, closed_loop)
     if not closed_loop:
         need = {}
         for _, e, *_ in trace:

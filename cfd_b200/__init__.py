@@ -155,7 +155,8 @@ class TuningStruct(C.Structure):
     _fields_ = [("target_tiles", _i), ("wide_row", _i), ("lanes_div", _i), ("fuse_first", _i),
                 ("sell_rows", _i), ("krylov_pair", _i), ("tail_rows", _i),
                 ("col16", _i), ("pdl", _i), ("wait_polls", _i), ("mixed_sweeps", _i),
-                ("mixed_weight", _d), ("tail_cluster", _i), ("vcycle_pair", _i)]
+                ("mixed_weight", _d), ("tail_cluster", _i), ("vcycle_pair", _i),
+                ("krylov_stage", _i)]
 
 
 _proto("cfdb_default_tuning", [_P(TuningStruct)], None)
@@ -888,13 +889,14 @@ class Tuning:
     mixed_weight: float = 0.0  # mixed precision: Jacobi weight (0: the hierarchy's)
     tail_cluster: int = 0  # tail as one cluster of this many CTAs (2..16); 0: cooperative grid
     vcycle_pair: int = 0  # V-cycle SELL kernels: two rows per thread per pass (1) or one (0)
+    krylov_stage: int = 0  # level-0 Krylov SpMV staged through shared memory in 2..4 buffers; 0: off
 
     def _c(self):
         return TuningStruct(int(self.target_tiles), int(self.wide_row), int(self.lanes_div),
                             int(self.fuse_first), int(self.sell_rows), int(self.krylov_pair),
                             int(self.tail_rows), int(self.col16), int(self.pdl), int(self.wait_polls),
                             int(self.mixed_sweeps), float(self.mixed_weight), int(self.tail_cluster),
-                            int(self.vcycle_pair))
+                            int(self.vcycle_pair), int(self.krylov_stage))
 
 
 def _set_system_tuning(self, t: Tuning) -> None:

@@ -9,6 +9,8 @@ The knobs are those of `Tuning` (include/cfdb.h, cfdb_tuning):
 * fuse_first   - first two Jacobi sweeps of the pre-smoothing fused into one kernel,
 * sell_rows    - rows per CTA of SELL operators (one row per thread per pass),
 * krylov_pair  - level-0 Krylov SpMV kernels take two rows per thread per pass, or one,
+* krylov_stage - the level-0 Krylov SpMV streams the operator through shared memory by bulk
+                 copies in this many buffers (0: the threads load it, as krylov_pair says),
 * tail_rows    - coarse levels of at most this many rows run in one persistent kernel,
 * vcycle_pair  - V-cycle kernels of SELL operators take two rows per thread per pass, or one,
 * tail_cluster - that kernel as one thread-block cluster of this many CTAs (0: a cooperative
@@ -44,6 +46,7 @@ CANDIDATES = {
     "fuse_first": [0, 1],
     "sell_rows": [256, 512, 1024],
     "krylov_pair": [0, 1],
+    "krylov_stage": [0, 2, 3, 4],
     "vcycle_pair": [0, 1],
     # the single-cluster tail (tail_cluster > 0) is not a candidate: on tet 95^3 x 6 it took
     # 299 us (16 CTAs) to 1,103 us (4 CTAs) per V-cycle where the separate kernels take ~50 us

@@ -167,7 +167,8 @@ Tuning tuning_from(const cfdb_tuning* t) {
                   t->krylov_pair != 0 ? 1 : 0, t->col16 != 0 ? 1 : 0, std::max(t->tail_rows, 0), t->pdl != 0 ? 1 : 0,
                   t->wait_polls == 0 ? Tuning{}.wait_polls : t->wait_polls, std::max(t->mixed_sweeps, 0),
                   t->mixed_weight > 0.0 ? t->mixed_weight : 0.0,
-                  t->tail_cluster > 0 ? std::min(std::max(t->tail_cluster, 2), 16) : 0, t->vcycle_pair != 0 ? 1 : 0};
+                  t->tail_cluster > 0 ? std::min(std::max(t->tail_cluster, 2), 16) : 0, t->vcycle_pair != 0 ? 1 : 0,
+                  t->krylov_stage > 0 ? std::min(std::max(t->krylov_stage, 2), 4) : 0};
 }
 
 } // namespace cfdb
@@ -1295,6 +1296,7 @@ void cfdb_default_tuning(cfdb_tuning* t) {
     t->mixed_weight = d.mixed_weight;
     t->tail_cluster = d.tail_cluster;
     t->vcycle_pair = d.vcycle_pair;
+    t->krylov_stage = d.krylov_stage;
 }
 
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t) {

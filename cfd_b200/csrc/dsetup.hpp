@@ -1,9 +1,11 @@
 // Smoothed-aggregation AMG setup on the device (fv::AmgPreconditioner::setup, amg.cpp:122-190).
 //
 // The sparse algebra of every level (strength graph, tentative and smoothed prolongation,
-// restriction, Galerkin products, zero pruning) runs in device kernels; the aggregation itself
-// (amg.cpp:12-78) is a sequential greedy pass whose result depends on the visiting order, so it
-// stays on the host, which receives only the strength graph of each level. Every product and
+// restriction, Galerkin products, zero pruning) runs in device kernels. The aggregation
+// (amg.cpp:12-78) is a sequence of greedy passes whose result depends on the visiting order:
+// passes 1 and 2 run on the device with the sequential result (pass 1 as the lexicographically
+// first independent set it is, resolved by sweeps); a level that leaves rows for pass 3 is
+// aggregated on the host from its strength graph. Every product and
 // sum is rounded in the order the host build (amg_setup, host_algos.cpp) uses, so the device
 // hierarchy is bit-identical to it: aggregates, P, R, coarse operators and coarse inverse.
 #pragma once
@@ -77,6 +79,9 @@ struct DevCsr {
 struct DeviceHierarchy {
     Scratch mem;
     std::vector<DevCsr> a, p, r;
+    // aggregates of each non-coarsest level on the device (in mem); the host copy `agg` is kept
+    // where the host aggregated, and made by download_hierarchy elsewhere
+    std::vector<const int*> dagg;
     std::vector<std::vector<int>> agg;
     std::vector<int> n_agg;
     int n_c = 0;
@@ -108,8 +113,9 @@ struct DeviceLevels {
 // Points k's level views at the arrays of d (which the setup allocated in k.mem).
 void adopt_levels(const DeviceHierarchy& d, DeviceLevels& k);
 
-// Shape-only host copy of a device hierarchy (sizes, aggregates, coarse inverse; matrix arrays
-// empty) for plan construction from the device levels.
+// Shape-only host copy of a device hierarchy (sizes, coarse inverse, and the aggregates of the
+// levels the host aggregated; matrix arrays and the device-aggregated levels' aggregates empty)
+// for plan construction from the device levels.
 Hierarchy hierarchy_shape(const DeviceHierarchy& d);
 
 // ---- engine operator layouts built from a device CSR block (one system, column offset 0) ----

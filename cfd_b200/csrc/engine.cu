@@ -579,6 +579,10 @@ void Engine::build(std::vector<SystemSpec> systems, int sweeps, double weight, b
         DevLevel& d = lv_[0];
         d.a.n_slices = static_cast<int>(sb.slice.size()) - 1;
         d.a.slots = sb.slice.back();
+        for (int sl = 0; sl < d.a.n_slices; ++sl) {
+            const int e = sb.slice[static_cast<size_t>(std::min(sl + 8, d.a.n_slices))];
+            d.a.max8_slots = std::max(d.a.max8_slots, e - sb.slice[static_cast<size_t>(sl)]);
+        }
         const int* dslice = arena0_.upload(sb.slice, st);
         const int* dcol = arena0_.upload(sb.col, st);
         d.a.s64 = {dslice, dcol, arena0_.alloc<double>(d.a.slots), kFmtSell};
@@ -1453,6 +1457,36 @@ void Engine::enqueue_rz(Mode mode, int flexible) {
     }
 }
 
+// Shared-memory budget of the staged SpMV's buffers: two CTAs per SM whatever the buffer count.
+constexpr int kStageBytes = 96 * 1024;
+
+template <int S> constexpr int stage_limit() { return kStageBytes / (S * 12) / 32 * 32; }
+
+// The staged level-0 Krylov SpMV runs when Tuning.krylov_stage asks for it and the operator
+// allows it: SELL, values and columns 16-byte aligned (bulk copies). Its buffers hold the
+// widest 8-slice chunk up to the budget (wider chunks are summed from global memory). The
+// kernels' shared-memory limit is always set to the budget, so that engines sharing them in one
+// process never lower it for one another.
+void Engine::prepare_stage() {
+    stage_cap_ = 0;
+    const int S = tuning_.krylov_stage;
+    const DevSell64_32& a = lv_[0].a;
+    if (S < 2 || S > 4 || a.s64.fmt != kFmtSell || a.max8_slots <= 0) return;
+    if ((reinterpret_cast<uintptr_t>(a.s64.val) | reinterpret_cast<uintptr_t>(a.s64.col)) % 16 != 0) return;
+    int limit = 0;
+    if (S == 2) {
+        limit = stage_limit<2>();
+        CFDB_CUDA(cudaFuncSetAttribute(k_cg_spmv_pq_staged<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * limit * 12));
+    } else if (S == 3) {
+        limit = stage_limit<3>();
+        CFDB_CUDA(cudaFuncSetAttribute(k_cg_spmv_pq_staged<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * limit * 12));
+    } else {
+        limit = stage_limit<4>();
+        CFDB_CUDA(cudaFuncSetAttribute(k_cg_spmv_pq_staged<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * limit * 12));
+    }
+    stage_cap_ = std::min(round_up(a.max8_slots, 32), limit);
+}
+
 void Engine::enqueue_iteration(Mode mode) {
     const DevLevel& d = lv_[0];
     const Control ctl{n_active_, error_, tuning_.wait_polls};
@@ -1465,9 +1499,20 @@ void Engine::enqueue_iteration(Mode mode) {
         launch_k(tuning_.pdl != 0, k_cg_pupdate<double>, d.n_tiles, kBlock, 0, stream_, d.tiles, st_, d.x64, r_, dinv0_, p_);
         mark("cg_p_update", 0, 24.0 * n);
     }
-    with_visit(krylov_visit(), [&](auto V) {
-        launch_k(tuning_.pdl != 0, k_cg_spmv_pq<decltype(V)::value>, d.n_tiles, kBlock, 0, stream_, d.a.s64, d.tiles, st_, p_, q_, red_, ctl);
-    });
+    if (stage_cap_ > 0) {
+        const size_t smem = static_cast<size_t>(tuning_.krylov_stage) * stage_cap_ * 12;
+        auto staged = [&](auto kernel) {
+            launch_k(tuning_.pdl != 0, kernel, d.n_tiles, kBlock, smem, stream_, d.a.s64, d.tiles, st_, p_, q_, red_, ctl,
+                     stage_cap_);
+        };
+        if (tuning_.krylov_stage == 2) staged(k_cg_spmv_pq_staged<2>);
+        else if (tuning_.krylov_stage == 3) staged(k_cg_spmv_pq_staged<3>);
+        else staged(k_cg_spmv_pq_staged<4>);
+    } else {
+        with_visit(krylov_visit(), [&](auto V) {
+            launch_k(tuning_.pdl != 0, k_cg_spmv_pq<decltype(V)::value>, d.n_tiles, kBlock, 0, stream_, d.a.s64, d.tiles, st_, p_, q_, red_, ctl);
+        });
+    }
     mark("cg_spmv_pq", 0, a0);
     const X1Out x1o = x1_out(mode);
     const double x1b = (mode == Mode::AmgMixed ? 8.0 : 16.0) * x1o.n;
@@ -1508,6 +1553,7 @@ std::vector<ProfRecord> Engine::profile(Mode mode, int reps) {
     if (mode != Mode::Jacobi && !has_amg_) fail(5, "profile: no AMG hierarchy set");
     if (mode == Mode::AmgMixed) prepare_tail<float>();
     else if (mode == Mode::AmgFp64) prepare_tail<double>();
+    prepare_stage();
     std::vector<ProfRecord> out;
     std::vector<int> count;
     // b = 1 on every real row, x = 0: a nonzero residual whatever the engine held before (the
@@ -1571,6 +1617,7 @@ void Engine::capture_graphs(Mode mode) {
     if (graphs_[m][0] != nullptr) return;
     if (mode == Mode::AmgMixed) prepare_tail<float>();
     else if (mode == Mode::AmgFp64) prepare_tail<double>();
+    prepare_stage();
     for (int which = 0; which < 2; ++which) {
         cudaGraph_t g = nullptr;
         CFDB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));

@@ -55,6 +55,8 @@ struct Tuning {
                                 // separated by the cluster barrier; 0: a cooperative grid
     int vcycle_pair = 0;        // V-cycle kernels of SELL operators take two rows per thread per
                                 // pass (as the level-0 Krylov kernels with krylov_pair), or one
+    int krylov_stage = 0;       // level-0 Krylov SpMV with the operator staged through shared
+                                // memory in this many buffers (2..4); 0: krylov_pair's kernels
 };
 
 struct SolveRequest {
@@ -163,6 +165,7 @@ private:
         int n_slices = 0;     // SELL slices, or CSR rows
         long long slots = 0;  // stored entries (SELL: with padding)
         long long nnz = 0;    // algorithmic nonzeros
+        int max8_slots = 0;   // SELL: most slots of any 8 consecutive slices (a staged chunk)
         // launch tiles of the operator's own row space: kSellRows rows (SELL), 8 rows (CSR,
         // G <= 32) or 256 / G rows (CSR, G > 32); block = threads per CTA
         Tiles tiles{};
@@ -191,6 +194,8 @@ private:
     template <class T> T* start_buffer(int l) const;
     // V-cycle tail (small coarse levels in one persistent kernel): first level, phases
     int tail_level() const;
+    // staged level-0 Krylov SpMV (Tuning.krylov_stage): buffer size in slots, 0 when off
+    void prepare_stage();
     template <class T> void prepare_tail();
     template <class T> void launch_tail(cudaStream_t s);
     // rows per thread per pass of the level-0 Krylov SpMV kernels (two, or one)
@@ -257,6 +262,7 @@ private:
     TailPhase<float>* tail32_ = nullptr;
     TailPhase<double>* tail64_ = nullptr;
     int tail_n32_ = 0, tail_n64_ = 0, tail_grid32_ = 0, tail_grid64_ = 0;
+    int stage_cap_ = 0;
     double tail_bytes32_ = 0.0, tail_bytes64_ = 0.0;
     unsigned* tail_bar_ = nullptr;
     CoarseBlocks cb_{};

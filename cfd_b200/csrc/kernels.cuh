@@ -850,6 +850,152 @@ static __global__ void __launch_bounds__(kBlock) k_vc_coarse(CoarseBlocks cb, co
     }
 }
 
+// ---- staged SELL visit: the operator stream through shared memory ----
+// The slots of a tile's rows are contiguous per chunk of kBlock positions (8 whole slices: the
+// tiles start on slice boundaries), so one thread moves a chunk's values and columns into
+// shared memory with two bulk copies (1-D cp.async.bulk, no multicast, mbarrier completion).
+// Thread 0 keeps S - 1 chunks in flight while the block sums the current one from shared
+// memory: a row's gathers then follow a shared-memory load of its columns instead of a DRAM
+// load, and the bytes in flight cost no registers. Each thread takes position c0 + threadIdx.x
+// of every chunk, the order in which kVisitSell1 and kVisitSell2 visit a tile, and sums each
+// row in CSR order, so rows, sums and the per-thread epilogue order are theirs bit for bit. A
+// chunk with more slots than a stage holds is summed from global memory as kVisitSell1 does.
+
+__device__ __forceinline__ void mbar_init1(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// 1-D bulk copy global -> this CTA's shared memory (both addresses 16-byte aligned, bytes a
+// multiple of 16), completing `bytes` transactions on bar.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Bounded wait for the phase of the given parity: true once it has completed, false after
+// `polls` unsuccessful tries (none when polls <= 0).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int polls) {
+    uint32_t done = 0;
+    for (int spin = 0; spin < polls && !done; ++spin) {
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+    }
+    return done != 0;
+}
+
+// Sum of one row of a staged chunk: k = the row's first slot and e = its slice's end, both
+// relative to the chunk's first slot. Eight entries per batch, their gathers in flight
+// together; entries in CSR order, padding (column -1) skipped, as sell_row_sum.
+template <class T, class XA>
+__device__ __forceinline__ T staged_row_sum(const T* sv, const int* sc, int k, int e, XA xa) {
+    T s = T(0);
+    for (; k < e; k += 8 * 32) {
+        int c[8];
+        T xv[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) c[u] = k + 32 * u < e ? sc[k + 32 * u] : -1;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) xv[u] = c[u] >= 0 ? xa(c[u]) : T(0);
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (c[u] >= 0) s = madd<T>(s, sv[k + 32 * u], xv[u]);
+    }
+    return s;
+}
+
+// As visit_rows_e over the SELL positions [r0, r1) (r0 a multiple of 32), with the operator
+// staged in S buffers of `cap` slots each (dynamic shared memory: S * cap * (sizeof(T) + 4)
+// bytes, cap a multiple of 32). Returns false when a bounded wait expired: ctl.error is set,
+// the CTA's copies in flight have been waited out (bounded too) and the remaining rows are
+// not visited; every thread returns together, so the caller's block reduction still runs.
+template <int S, class T, class XA, class P, class F>
+__device__ __forceinline__ bool visit_rows_staged(const Sell<T>& m, int r0, int r1, int cap, const Control& ctl,
+                                                  XA xa, P pre, F f) {
+    static_assert(S >= 2 && S <= 4, "stages");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar[S];
+    T* sval = reinterpret_cast<T*>(smem_raw);
+    int* scol = reinterpret_cast<int*>(smem_raw + static_cast<size_t>(S) * cap * sizeof(T));
+    const int n_chunks = (r1 - r0 + kBlock - 1) / kBlock;
+    // first slot and slot count of chunk j
+    auto span = [&](int j, int& first, int& count) {
+        const int c0 = r0 + j * kBlock;
+        const int c1 = min(c0 + kBlock, r1);
+        first = __ldg(&m.slice[c0 >> 5]);
+        count = __ldg(&m.slice[(c1 + 31) >> 5]) - first;
+    };
+    auto fits = [cap](int count) { return count > 0 && count <= cap; };
+    auto issue = [&](int j) {  // thread 0
+        int first, count;
+        span(j, first, count);
+        if (!fits(count)) return;
+        const int s = j % S;
+        // the block's reads of this buffer (ordered before this thread by the block barrier)
+        // precede the copy's writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect(&bar[s], static_cast<uint32_t>(count) * static_cast<uint32_t>(sizeof(T) + sizeof(int)));
+        bulk_load(sval + static_cast<size_t>(s) * cap, m.val + first, static_cast<uint32_t>(count * sizeof(T)), &bar[s]);
+        bulk_load(scol + static_cast<size_t>(s) * cap, m.col + first, static_cast<uint32_t>(count * sizeof(int)), &bar[s]);
+    };
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) mbar_init1(&bar[s]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int j = 0; j < S - 1 && j < n_chunks; ++j) issue(j);
+    uint32_t par = 0;  // bit s: parity of buffer s's next phase
+    for (int j = 0; j < n_chunks; ++j) {
+        int first, count;
+        span(j, first, count);
+        const bool staged = fits(count);
+        const int s = j % S;
+        const int pos = r0 + j * kBlock + static_cast<int>(threadIdx.x);
+        const bool has = pos < r1;
+        const int row = has ? (m.perm != nullptr ? __ldg(&m.perm[pos]) : pos) : 0;
+        decltype(pre(0)) e{};
+        if (has) e = pre(row);
+        const bool late = staged && !mbar_wait(&bar[s], (par >> s) & 1u, ctl.wait_polls);
+        if (__syncthreads_or(late)) {
+            if (threadIdx.x == 0) {
+                atomicExch(ctl.error, 1);
+                // the copies of chunks j .. j + S - 2 are in flight: let them land first
+                for (int q = j; q < min(j + S - 1, n_chunks); ++q) {
+                    int fq, nq;
+                    span(q, fq, nq);
+                    if (fits(nq)) (void)mbar_wait(&bar[q % S], (par >> (q % S)) & 1u, kDrainPolls);
+                }
+            }
+            __syncthreads();
+            return false;
+        }
+        if (staged) par ^= 1u << s;
+        if (threadIdx.x == 0 && j + S - 1 < n_chunks) issue(j + S - 1);
+        if (has) {
+            T sum;
+            if (staged) {
+                const int sl = pos >> 5;
+                sum = staged_row_sum(sval + static_cast<size_t>(s) * cap, scol + static_cast<size_t>(s) * cap,
+                                     __ldg(&m.slice[sl]) - first + (pos & 31), __ldg(&m.slice[sl + 1]) - first, xa);
+            } else {
+                sum = sell_row_sum(m, pos, xa);
+            }
+            f(row, sum, e);
+        }
+    }
+    return true;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Krylov kernels (krylov_kernels.inc:240-301 / krylov_cuda.cu:462-507), level-0 FP64
 // ---------------------------------------------------------------------------------------------
@@ -919,21 +1065,10 @@ static __global__ void __launch_bounds__(kBlock) k_cg_pupdate(Tiles tiles, const
     }
 }
 
-// q = A p ; p.q ; alpha = rz / pq (break if pq == 0)
-template <int V>
-static __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(Sell<double> a, Tiles tiles, SysState* st,
-                                                       const double* __restrict__ p,
-                                                       double* __restrict__ q, Reduce red,
-                                                       Control ctl) {
-    pdl_entry();
-    TileCtx c;
-    if (!tile_begin(tiles, st, c)) return;
-    double pq = 0.0, unused = 0.0;
-    visit_rows_e<V>(a, c.r0, c.r1, [p](int j) { return p[j]; }, [&](int row) { return p[row]; },
-                    [&](int row, double qi, double pi) {
-                        q[row] = qi;
-                        pq = __dadd_rn(pq, __dmul_rn(pi, qi));
-                    });
+// p.q of the tiles of one system ; alpha = rz / pq (break if pq == 0)
+__device__ __forceinline__ void cg_finish_pq(double pq, const TileCtx& c, SysState* st, const Reduce& red,
+                                             const Control& ctl) {
+    double unused = 0.0;
     if (reduce_system(pq, unused, c.tile, c.s, red) && threadIdx.x == 0) {
         SysState& s = st[c.s];
         s.first = 0;
@@ -946,6 +1081,43 @@ static __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(Sell<double> a, Ti
             s.alpha = s.rz / pq;
         }
     }
+}
+
+// k_cg_spmv_pq (below) with the operator staged through shared memory: S buffers of `cap`
+// slots (visit_rows_staged). Same q and p.q bit for bit.
+template <int S>
+static __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq_staged(Sell<double> a, Tiles tiles, SysState* st,
+                                                              const double* __restrict__ p,
+                                                              double* __restrict__ q, Reduce red,
+                                                              Control ctl, int cap) {
+    pdl_entry();
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    double pq = 0.0;
+    visit_rows_staged<S>(a, c.r0, c.r1, cap, ctl, [p](int j) { return p[j]; }, [&](int row) { return p[row]; },
+                         [&](int row, double qi, double pi) {
+                             q[row] = qi;
+                             pq = __dadd_rn(pq, __dmul_rn(pi, qi));
+                         });
+    cg_finish_pq(pq, c, st, red, ctl);
+}
+
+// q = A p ; p.q ; alpha = rz / pq (break if pq == 0)
+template <int V>
+static __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(Sell<double> a, Tiles tiles, SysState* st,
+                                                       const double* __restrict__ p,
+                                                       double* __restrict__ q, Reduce red,
+                                                       Control ctl) {
+    pdl_entry();
+    TileCtx c;
+    if (!tile_begin(tiles, st, c)) return;
+    double pq = 0.0;
+    visit_rows_e<V>(a, c.r0, c.r1, [p](int j) { return p[j]; }, [&](int row) { return p[row]; },
+                    [&](int row, double qi, double pi) {
+                        q[row] = qi;
+                        pq = __dadd_rn(pq, __dmul_rn(pi, qi));
+                    });
+    cg_finish_pq(pq, c, st, red, ctl);
 }
 
 // x += alpha p ; r -= alpha q ; |r|_2 ; converged?

@@ -455,6 +455,9 @@ typedef struct {
                          (default): a cooperative grid with the bounded grid barrier */
     int vcycle_pair;  /* V-cycle kernels of SELL operators take two rows per thread per pass (1)
                          or one (0, default) */
+    int krylov_stage; /* level-0 Krylov SpMV with the operator streamed through shared memory by
+                         bulk copies, in this many buffers (2..4); 0 (default): loaded by the
+                         threads (krylov_pair). Same results bit for bit. */
 } cfdb_tuning;
 void cfdb_default_tuning(cfdb_tuning* t);
 int cfdb_system_set_tuning(cfdb_system* sys, const cfdb_tuning* t);

@@ -79,6 +79,34 @@ def test_device_setup_matches_host_build(gpu, make, theta):
     _same(cb.AmgHierarchy(view, s, device=True), cb.AmgHierarchy(view, s))
 
 
+@pytest.mark.parametrize("size,every", [(36, 300), (36, 250)], ids=["pass3-device", "pass3-host"])
+def test_device_setup_with_rows_left_for_pass3(gpu, size, every):
+    """The fine level of tet 36 (279,936 rows, sparse) is aggregated on the device. Rows whose
+    every off-diagonal is weak have no strong connection: passes 1 and 2 leave them for pass 3
+    (amg.cpp:66-76), which one device thread runs when at most 1024 rows are left (every 300th
+    row: 934) and the host runs from the strength graph read back when more are (every 250th:
+    1,120). The hierarchy equals the oracle's either way."""
+    import dataclasses
+    theta = 0.04
+    cb = gpu
+    case = W.tet(size)
+    up, lo, diag, _ = _pressure(case)
+    a = O.ldu_to_csr(O.build_pattern(case.n, case.owner, case.neighbour), diag, up, lo)
+    rows = np.repeat(np.arange(a.n_rows), np.diff(a.rp))
+    iso = np.arange(a.n_rows) % every == 5
+    weak = (a.ci != rows) & (iso[rows] | iso[a.ci])
+    va = a.va.copy()
+    va[weak] *= 1e-6
+    a = dataclasses.replace(a, va=va)
+    d = np.zeros(a.n_rows)
+    d[rows[a.ci == rows]] = va[a.ci == rows]
+    strong = (a.ci != rows) & (np.abs(va) > theta * np.sqrt(np.abs(d[rows] * d[a.ci])))
+    assert not strong[iso[rows]].any() and strong.any()  # isolated rows exist at level 0
+    h = cb.AmgHierarchy(cb.CsrView(a.n_rows, a.rp, a.ci, a.va), cb.AmgSettings(strength_threshold=theta),
+                        device=True)
+    _same(h, O.Hierarchy(a, theta=theta))
+
+
 @pytest.mark.parametrize("limit", [24, 200])
 @pytest.mark.parametrize("name,theta", [("tet7_sigma", 0.0), ("graded12", 0.04)])
 def test_device_memory_tables_match_oracle(gpu, name, theta, limit):

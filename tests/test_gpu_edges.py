@@ -127,13 +127,16 @@ def test_ragged_batch_with_converged_and_tiny_systems(gpu):
 
 
 @pytest.mark.parametrize("precision", ["FP64", "MIXED"])
-@pytest.mark.parametrize("tail", [0, 10 ** 6], ids=["coarse-staging-wait", "tail-grid-barrier"])
-def test_expired_device_wait_reports_timeout_and_recovers(gpu, tail, precision):
+@pytest.mark.parametrize("knobs", [{"tail_rows": 0}, {"tail_rows": 10 ** 6}, {"krylov_stage": 3}],
+                         ids=["coarse-staging-wait", "tail-grid-barrier", "krylov-staging-wait"])
+def test_expired_device_wait_reports_timeout_and_recovers(gpu, knobs, precision):
     """Every device-side wait is bounded. With the poll limit set to give up at once
     (Tuning.wait_polls < 0) the waits expire -- the coarse kernel's wait for its bulk copy
-    (which it still drains before it exits) or the persistent tail's grid barrier -- and the
-    solve reports CFDB_ERR_TIMEOUT. With the default limit restored, the next solve is
-    bit-identical to one that never timed out (error flag and barrier counters reset)."""
+    (which it still drains before it exits), the persistent tail's grid barrier, or the staged
+    Krylov SpMV's wait for a chunk (the CTA drains its copies in flight and still joins the
+    block reduction) -- and the solve reports CFDB_ERR_TIMEOUT. With the default limit restored,
+    the next solve is bit-identical to one that never timed out (error flag and barrier and
+    reduction counters reset)."""
     cb = gpu
     case = W.graded(20)
     up, lo, diag, src = _system(case)
@@ -141,14 +144,14 @@ def test_expired_device_wait_reports_timeout_and_recovers(gpu, tail, precision):
     ds.set_precision(getattr(cb.Precision, precision))
     ds.setup_amg(diag, up, lo, cb.AmgSettings(strength_threshold=0.04))
     ctl = cb.SolveControl(1e-8 * np.linalg.norm(src), 200)
-    ds.set_tuning(cb.Tuning(tail_rows=tail))
+    ds.set_tuning(cb.Tuning(**knobs))
     x_ref = np.zeros(case.n)
     st_ref = ds.solve(diag, up, lo, src, x_ref, cb.Method.Cg, True, ctl)
     assert st_ref.converged
-    ds.set_tuning(cb.Tuning(tail_rows=tail, wait_polls=-1))
+    ds.set_tuning(cb.Tuning(**knobs, wait_polls=-1))
     with pytest.raises(cb.Timeout, match="bounded device wait expired"):
         ds.solve(diag, up, lo, src, np.zeros(case.n), cb.Method.Cg, True, ctl)
-    ds.set_tuning(cb.Tuning(tail_rows=tail))
+    ds.set_tuning(cb.Tuning(**knobs))
     for _ in range(2):
         x = np.zeros(case.n)
         st = ds.solve(diag, up, lo, src, x, cb.Method.Cg, True, ctl)

@@ -388,3 +388,63 @@ def test_two_row_vcycle_kernels_match_one_row(gpu, precision):
         out.append((x, st.iterations, z))
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][2], out[1][2])
+
+
+def _mixed_stencil(nx, ny, nz, wide_x):
+    """LDU system on an nx x ny x nz lattice: 6-neighbour couplings everywhere, and the 26
+    neighbours of the cells with x < wide_x (rows of 27 entries: their SELL chunks hold more
+    slots than a staging buffer, so the staged kernel sums them from global memory).
+    Symmetric, diagonally dominant."""
+    idx = np.arange(nx * ny * nz).reshape(nz, ny, nx)
+    pairs = []
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                if (dz, dy, dx) <= (0, 0, 0):
+                    continue
+                a = idx[max(0, -dz):nz - max(0, dz), max(0, -dy):ny - max(0, dy), max(0, -dx):nx - max(0, dx)]
+                b = idx[max(0, dz):nz - max(0, -dz) or None, max(0, dy):ny - max(0, -dy) or None,
+                        max(0, dx):nx - max(0, -dx) or None]
+                a, b = a.ravel(), b.ravel()
+                axis = abs(dz) + abs(dy) + abs(dx) == 1
+                keep = axis | ((a % nx < wide_x) & (b % nx < wide_x))
+                pairs.append(np.stack([np.minimum(a, b)[keep], np.maximum(a, b)[keep]], 1))
+    p = np.concatenate(pairs)
+    p = p[np.lexsort((p[:, 1], p[:, 0]))]
+    owner, neighbour = p[:, 0].astype(np.int32), p[:, 1].astype(np.int32)
+    n = nx * ny * nz
+    rng = np.random.default_rng(21)
+    w = rng.uniform(0.5, 1.5, len(owner))
+    diag = np.bincount(owner, w, n) + np.bincount(neighbour, w, n) + 0.05
+    src = rng.standard_normal(n)
+    return n, owner, neighbour, -w, -w.copy(), diag, src
+
+
+@pytest.mark.parametrize("precision", ["FP64", "MIXED"])
+@pytest.mark.parametrize("mesh", ["tet", "mixed-stencil"])
+def test_staged_krylov_spmv_matches_thread_loads(gpu, precision, mesh):
+    """The level-0 Krylov SpMV with the operator streamed through shared memory by bulk copies
+    (krylov_stage 2..4 buffers) visits and sums every row as the thread-load kernels do: solves
+    are bit-identical (iterations and x). Few tiles, so that each CTA pipelines many chunks
+    through its buffers; on the mixed stencil the wide chunks take the unstaged path."""
+    cb = gpu
+    if mesh == "tet":
+        case = W.tet(14)
+        up, lo, diag, src = _assembled(case)
+        n, owner, neighbour = case.n, case.owner, case.neighbour
+    else:
+        n, owner, neighbour, up, lo, diag, src = _mixed_stencil(40, 30, 24, 9)
+    ds = cb.DeviceSolver(cb.build_csr_pattern(n, owner, neighbour))
+    ds.set_precision(getattr(cb.Precision, precision))
+    ds.setup_amg(diag, up, lo, cb.AmgSettings(strength_threshold=0.04))
+    ctl = cb.SolveControl(1e-10 * np.linalg.norm(src), 500)
+    out = []
+    for pair, stage in ((1, 0), (0, 0), (1, 2), (1, 3), (1, 4)):
+        ds.set_tuning(cb.Tuning(krylov_pair=pair, krylov_stage=stage, target_tiles=3))
+        x = np.zeros(n)
+        st = ds.solve(diag, up, lo, src, x, cb.Method.Cg, True, ctl)
+        assert st.converged
+        out.append((st.iterations, x))
+    for it, x in out[1:]:
+        assert it == out[0][0] and np.array_equal(x, out[0][1])
+    ds.close()

@@ -111,3 +111,46 @@ def test_batch_device_setup_equals_host_setup(gpu, precision):
         b.close()
     for its, x in out[1:]:
         assert its == out[0][0] and np.array_equal(x, out[0][1])
+
+
+@pytest.mark.parametrize("precision", ["FP64", "MIXED"])
+def test_batch_staged_krylov_spmv_matches_thread_loads(gpu, precision):
+    """In a batch the level-0 Krylov tiles hold one system each, starting on the system's
+    32-row-aligned offset: the staged SpMV (krylov_stage, operator chunks through shared
+    memory) gives every system the same iterations and solution bit for bit as the
+    thread-load kernels, with tiles of many chunks (target_tiles 4) and of one."""
+    import torch
+    cb = gpu
+    cases = _cases()
+    nc, nf, own, nei, flux, gamma, delta, src0 = _concat(cases)
+    dev = torch.device("cuda")
+    T = lambda a: torch.as_tensor(a, dtype=torch.float64, device=dev)  # noqa: E731
+    b = cb.Batch(nc, nf, own, nei)
+    d_up, d_lo = torch.empty(b.total_faces, dtype=torch.float64, device=dev), torch.empty(b.total_faces, dtype=torch.float64, device=dev)
+    d_dg, d_src = torch.empty(b.total_cells, dtype=torch.float64, device=dev), torch.empty(b.total_cells, dtype=torch.float64, device=dev)
+    b.assemble_pressure_device(T(flux), T(gamma), T(delta), T(src0), d_up, d_lo, d_dg, d_src,
+                               ref_cells=[0] * len(cases))
+    b.setup_amg(d_dg, d_up, d_lo, cb.AmgSettings(strength_threshold=0.04), device=True)
+    b.set_precision(getattr(cb.Precision, precision))
+    src = d_src.cpu().numpy()
+    co, tols = 0, []
+    for c in cases:
+        tols.append(1e-8 * np.linalg.norm(src[co:co + c.n]))
+        co += c.n
+    out = []
+    for stage, tiles in ((0, 4), (3, 4), (2, 0), (4, 0)):
+        b.set_tuning(cb.Tuning(krylov_stage=stage, target_tiles=tiles))
+        x = torch.zeros(b.total_cells, dtype=torch.float64, device=dev)
+        stats = b.solve_device(d_dg, d_up, d_lo, d_src, x, [cb.SolveControl(t, 300) for t in tols])
+        torch.cuda.synchronize()
+        assert all(st.converged for st in stats)
+        out.append(([st.iterations for st in stats], x.cpu().numpy()))
+    # target_tiles changes the reduction tiles (the dot products' partial sums), so compare
+    # within each tiling: staged against thread loads with the same tiles
+    b.set_tuning(cb.Tuning(krylov_stage=0, target_tiles=0))
+    x = torch.zeros(b.total_cells, dtype=torch.float64, device=dev)
+    stats = b.solve_device(d_dg, d_up, d_lo, d_src, x, [cb.SolveControl(t, 300) for t in tols])
+    ref0 = ([st.iterations for st in stats], x.cpu().numpy())
+    assert out[0][0] == out[1][0] and np.array_equal(out[0][1], out[1][1])
+    for it, xs in out[2:]:
+        assert it == ref0[0] and np.array_equal(xs, ref0[1])

@@ -1224,6 +1224,8 @@ def run_step(args, rank, world, local_rank):
         "ms_min": min(times), "ms_median": sorted(times)[len(times) // 2], "ms_max": max(times),
         "ms_per_step_each": times, "pressure_solves": len(solves),
         "hierarchy_rebuilds": sum(1 for r in solves if r.amg_rebuilt),
+        # phases of the last device rebuild (cfdb_system_setup_profile), ms
+        "rebuild_phases_ms": {k: round(v * 1e3, 3) for k, v in ds.setup_profile().items()},
         "iterations_per_solve": [r.iterations for r in solves],
         "cpu_baseline": None,
         "cpu_baseline_note": ("the reference's FlowSolver is compiled here (oracle/_ref, through the Eigen "

@@ -902,6 +902,7 @@ int cfdb_system_setup_amg_device(cfdb_system* sys, const double* diag, const dou
                 sys->dirty = true;
             }
         }
+        const double t_wait = PhaseTimes::now();
         DeviceHierarchy dh;
         const double *dd = diag, *du = upper, *dl = lower;
         if (!device_arrays) {
@@ -930,7 +931,9 @@ int cfdb_system_setup_amg_device(cfdb_system* sys, const double* diag, const dou
         auto kept = std::make_shared<DeviceLevels>();
         amg_setup_device(a0, s, cs.s, dh, &sys->stage, &kept->mem);
         const double t1 = PhaseTimes::now();
-        dh.times.add("input", t0 - t_in);
+        // input_wait: the system's stream drained (its queued work) before the old levels go
+        dh.times.add("input_wait", t_wait - t_in);
+        dh.times.add("input", t0 - t_wait);
         adopt_levels(dh, *kept);
         auto h = std::make_shared<Hierarchy>(hierarchy_shape(dh));
         const double t2 = PhaseTimes::now();

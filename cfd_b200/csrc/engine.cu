@@ -1516,8 +1516,15 @@ void Engine::enqueue_iteration(Mode mode) {
     mark("cg_spmv_pq", 0, a0);
     const X1Out x1o = x1_out(mode);
     const double x1b = (mode == Mode::AmgMixed ? 8.0 : 16.0) * x1o.n;
-    launch_k(tuning_.pdl != 0, k_cg_xr, d.n_tiles, kBlock, 0, stream_, d.tiles, st_, x_, r_, p_, q_, red_,
-                                                ctl, mode == Mode::AmgMixed ? 1 : 0, x1o);
+    {
+        const int vt = mode == Mode::AmgMixed ? 1 : 0;
+        if (x1o.n > 0 && x1o.x32 != nullptr)
+            launch_k(tuning_.pdl != 0, k_cg_xr<1>, d.n_tiles, kBlock, 0, stream_, d.tiles, st_, x_, r_, p_, q_, red_, ctl, vt, x1o);
+        else if (x1o.n > 0 && x1o.x64 != nullptr)
+            launch_k(tuning_.pdl != 0, k_cg_xr<2>, d.n_tiles, kBlock, 0, stream_, d.tiles, st_, x_, r_, p_, q_, red_, ctl, vt, x1o);
+        else
+            launch_k(tuning_.pdl != 0, k_cg_xr<0>, d.n_tiles, kBlock, 0, stream_, d.tiles, st_, x_, r_, p_, q_, red_, ctl, vt, x1o);
+    }
     mark("cg_xr", 0, 48.0 * n + x1b);
     if (mode == Mode::AmgMixed) {
         with_visit(krylov_visit(), [&](auto V) {

@@ -1122,7 +1122,11 @@ static __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(Sell<double> a, Ti
 
 // x += alpha p ; r -= alpha q ; |r|_2 ; converged?
 // verify_true: mixed mode marks the system for an FP64 true-residual check instead.
-static __global__ void __launch_bounds__(kBlock) k_cg_xr(Tiles tiles, SysState* st,
+// X1: the V-cycle's first sweep written from the new r (x1o): 0 none, 1 FP32, 2 FP64; its
+// weights are loaded with the pass's other operands (an instance per form, so the instance
+// without it holds no registers for them).
+template <int X1>
+static __global__ void __launch_bounds__(kBlock, (X1 == 0 ? 5 : 4)) k_cg_xr(Tiles tiles, SysState* st,
                                                   double* __restrict__ x, double* __restrict__ r,
                                                   const double* __restrict__ p,
                                                   const double* __restrict__ q, Reduce red,
@@ -1134,7 +1138,8 @@ static __global__ void __launch_bounds__(kBlock) k_cg_xr(Tiles tiles, SysState* 
     double rr = 0.0, unused = 0.0;
     // four rows per thread per pass: all loads of the pass are issued before any store
     for (int r0 = c.r0 + threadIdx.x; r0 < c.r1; r0 += 4 * kBlock) {
-        double xi[4], pi[4], ri[4], qi[4];
+        double xi[4], pi[4], ri[4], qi[4], w64[4];
+        float w32[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int row = r0 + u * kBlock;
@@ -1143,6 +1148,8 @@ static __global__ void __launch_bounds__(kBlock) k_cg_xr(Tiles tiles, SysState* 
             pi[u] = ok ? p[row] : 0.0;
             ri[u] = ok ? r[row] : 0.0;
             qi[u] = ok ? q[row] : 0.0;
+            if constexpr (X1 == 1) w32[u] = ok && row < x1o.n ? x1o.wd32[row] : 0.0f;
+            if constexpr (X1 == 2) w64[u] = ok && row < x1o.n ? x1o.wd64[row] : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -1151,7 +1158,12 @@ static __global__ void __launch_bounds__(kBlock) k_cg_xr(Tiles tiles, SysState* 
             x[row] = __dadd_rn(xi[u], __dmul_rn(alpha, pi[u]));
             const double rn = __dsub_rn(ri[u], __dmul_rn(alpha, qi[u]));
             r[row] = rn;
-            x1o.put(row, rn);
+            if constexpr (X1 == 1) {
+                if (row < x1o.n) x1o.x32[row] = first_sweep<float>(w32[u], rn);
+            }
+            if constexpr (X1 == 2) {
+                if (row < x1o.n) x1o.x64[row] = first_sweep<double>(w64[u], rn);
+            }
             rr = __dadd_rn(rr, __dmul_rn(rn, rn));
         }
     }
